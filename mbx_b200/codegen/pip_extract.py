@@ -1,0 +1,335 @@
+#!/usr/bin/env python3
+"""Recover the monomial basis of the reference's generated PIP programs.
+
+The reference ships each permutationally-invariant polynomial (PIP) only as a
+machine-generated straight-line program (``const double tN = ...;`` or
+``t[N] = ...;`` assignments over ``a[k]`` and ``x[j]``) that is linear in the
+coefficients ``a``.  This tool parses such a program, expands it symbolically
+and writes the polynomial in the explicit form
+
+    P(a, x) = sum_k a[k] * sum_m  c_{k,m} * prod_{j in m} x[j]
+
+as a term table (one line per (k, m) pair).  The build's own CUDA generator
+(``gen_kernels.py``) and the oracle restatement (``oracle/mbx_oracle.c``)
+both work from these tables; neither contains any of the reference programs.
+The table is checked against the compiled reference polynomial in
+``tests/test_pip_tables.py``.
+
+Programs parsed (file:line of the energy-only evaluator in the reference):
+
+======== ================================================================ ==== ====
+name     source                                                           vars coef
+======== ================================================================ ==== ====
+mbpol2b  potential/2b/poly-2b-v6x-nogrd.cpp:41 (eval(nd, a, x))          31   1153
+mbpol3b  potential/3b/poly-3b-v2x-nogrd.cpp:38 (eval(a, x))              36   1163
+ch4h2o2b potential/2b/poly_2b_A1B2Z2_C1D4_deg3_exp0_v1.cpp:38             38   603
+ch4ch42b potential/2b/poly_2b_A1B4_A1B4_deg4_exp0_v1.cpp:44982 (+fmg1-15) 45   1345
+ch4h2o3b potential/3b/poly_3b_A1B4_C1D2_C1D2_deg3_nograd_v1.cpp:39        55   1254
+======== ================================================================ ==== ====
+
+It also extracts the fitted linear coefficients (the model parameters) from
+the evaluator classes:
+
+* mbpol2b: ``thefit`` in potential/2b/x2b-v9x.cpp:164-1318
+* mbpol3b: ``thefit`` in potential/3b/x3b-v2x.cpp:80-1244
+* ch4h2o2b: ``coefficients`` in potential/2b/x2b_A1B2Z2_C1D4_deg3_exp0_v1x.cpp:175
+* ch4ch42b: ``coefficients`` in potential/2b/x2b_A1B4_A1B4_deg4_exp0_v1x.cpp
+* ch4h2o3b: ``coefficients`` in potential/3b/mbnrg_3b_A1B4_C1D2_C1D2_deg3_v1.cpp
+
+Output (``mbx_b200/data/``): ``<name>.pip.gz`` (term table, gzip) and ``<name>.fit``
+(coefficients, one per line, printed with ``repr`` so they round-trip
+bit-exactly).
+
+Usage: ``python -m mbx_b200.codegen.pip_extract [--ref /root/reference]``
+"""
+import argparse
+import gzip
+import os
+import re
+import sys
+import time
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+DATA = os.path.join(os.path.dirname(HERE), "data")
+
+PROGRAMS = {
+    "mbpol2b": ("potential/2b/poly-2b-v6x-nogrd.cpp", 31, 1153, 4),
+    "mbpol3b": ("potential/3b/poly-3b-v2x-nogrd.cpp", 36, 1163, 4),
+    "ch4h2o2b": ("potential/2b/poly_2b_A1B2Z2_C1D4_deg3_exp0_v1.cpp", 38, 603, 3),
+    "ch4ch42b": ("potential/2b/poly_2b_A1B4_A1B4_deg4_exp0_v1.cpp", 45, 1345, 4),
+    "ch4h2o3b": ("potential/3b/poly_3b_A1B4_C1D2_C1D2_deg3_nograd_v1.cpp", 55, 1254, 3),
+}
+
+FITS = {
+    "mbpol2b": ("potential/2b/x2b-v9x.cpp", r"const double thefit\[\]\s*=\s*\{"),
+    "mbpol3b": ("potential/3b/x3b-v2x.cpp", r"thefit\[[^\]]*\]\s*=\s*\{"),
+    "ch4h2o2b": ("potential/2b/x2b_A1B2Z2_C1D4_deg3_exp0_v1x.cpp", r"coefficients\s*=\s*std::vector<double>\s*\{"),
+    "ch4ch42b": ("potential/2b/x2b_A1B4_A1B4_deg4_exp0_v1x.cpp", r"coefficients\s*=\s*std::vector<double>\s*\{"),
+    "ch4h2o3b": ("potential/3b/mbnrg_3b_A1B4_C1D2_C1D2_deg3_v1.cpp", r"coefficients\s*=\s*std::vector<double>\s*\{"),
+}
+
+TOKEN = re.compile(
+    r"\s*(?:(?P<num>\d+\.\d*(?:[eE][-+]?\d+)?|\d+(?:[eE][-+]?\d+)?)"
+    r"|(?P<t>t\[\d+\]|t\d+)"
+    r"|(?P<a>a\[\d+\])"
+    r"|(?P<x>x\[[^\]]*\])"
+    r"|(?P<op>[-+*/()]))"
+)
+
+
+# ---------------------------------------------------------------------------
+# Sparse polynomials linear in a: dict {(k, mono): coef}; k = -1 means "no a",
+# mono = sorted tuple of variable indices (with repetition).
+# ---------------------------------------------------------------------------
+
+def padd(p, q, sign=1.0):
+    r = dict(p)
+    for key, c in q.items():
+        v = r.get(key, 0.0) + sign * c
+        if v == 0.0:
+            r.pop(key, None)
+        else:
+            r[key] = v
+    return r
+
+
+def pmul(p, q):
+    if len(p) > len(q):
+        p, q = q, p
+    r = {}
+    for (k1, m1), c1 in p.items():
+        for (k2, m2), c2 in q.items():
+            if k1 >= 0 and k2 >= 0:
+                raise ValueError("program is not linear in the coefficients")
+            key = (k1 if k1 >= 0 else k2, tuple(sorted(m1 + m2)))
+            v = r.get(key, 0.0) + c1 * c2
+            if v == 0.0:
+                r.pop(key, None)
+            else:
+                r[key] = v
+    return r
+
+
+class Parser:
+    def __init__(self, env, xindex):
+        self.env = env
+        self.xindex = xindex
+
+    def parse(self, text):
+        self.toks = []
+        pos = 0
+        text = text.strip()
+        while pos < len(text):
+            m = TOKEN.match(text, pos)
+            if not m or m.end() == pos:
+                raise ValueError("cannot tokenise: %r" % text[pos:pos + 40])
+            self.toks.append((m.lastgroup, m.group(m.lastgroup)))
+            pos = m.end()
+            while pos < len(text) and text[pos].isspace():
+                pos += 1
+        self.i = 0
+        v = self.expr()
+        if self.i != len(self.toks):
+            raise ValueError("trailing tokens in %r" % text[:80])
+        return v
+
+    def peek(self):
+        return self.toks[self.i] if self.i < len(self.toks) else (None, None)
+
+    def expr(self):
+        v = self.term()
+        while True:
+            kind, tok = self.peek()
+            if kind == "op" and tok in "+-":
+                self.i += 1
+                v = padd(v, self.term(), 1.0 if tok == "+" else -1.0)
+            else:
+                return v
+
+    def term(self):
+        v = self.factor()
+        while True:
+            kind, tok = self.peek()
+            if kind == "op" and tok == "*":
+                self.i += 1
+                v = pmul(v, self.factor())
+            elif kind == "op" and tok == "/":
+                self.i += 1
+                d = self.factor()
+                if len(d) != 1 or next(iter(d)) != (-1, ()):
+                    raise ValueError("division by a non-constant")
+                c = next(iter(d.values()))
+                v = {key: val / c for key, val in v.items()}
+            else:
+                return v
+
+    def factor(self):
+        kind, tok = self.peek()
+        self.i += 1
+        if kind == "op" and tok == "-":
+            return {key: -c for key, c in self.factor().items()}
+        if kind == "op" and tok == "+":
+            return self.factor()
+        if kind == "op" and tok == "(":
+            v = self.expr()
+            k2, t2 = self.peek()
+            if t2 != ")":
+                raise ValueError("missing )")
+            self.i += 1
+            return v
+        if kind == "num":
+            return {(-1, ()): float(tok)}
+        if kind == "t":
+            return self.env[tok.replace("[", "").replace("]", "")]
+        if kind == "a":
+            return {(int(tok[2:-1]), ()): 1.0}
+        if kind == "x":
+            return {(-1, (self.xindex(tok),)): 1.0}
+        raise ValueError("unexpected token %r" % (tok,))
+
+
+def xindex_factory(src):
+    def xi(tok):
+        inner = tok[2:-1].replace(" ", "")
+        m = re.fullmatch(r"(\d+)", inner)
+        if m:
+            return int(m.group(1))
+        m = re.fullmatch(r"nv\+nd\*(\d+)", inner)
+        if m:
+            return int(m.group(1))
+        raise ValueError("unknown x index form %r in %s" % (tok, src))
+    return xi
+
+
+ASSIGN = re.compile(r"(?:const\s+double\s+)?(t\d+|t\[\d+\])\s*=\s*([^;]*);", re.S)
+
+
+def statements(body):
+    """Yield (target, expr) for assignments and ('<result>', expr) for the result."""
+    for stmt in body.split(";"):
+        s = " ".join(stmt.split())
+        if not s:
+            continue
+        m = re.fullmatch(r"(?:const double )?(t\d+|t\[\d+\]) = (.*)", s)
+        if m:
+            yield m.group(1).replace("[", "").replace("]", ""), m.group(2)
+            continue
+        m = re.fullmatch(r"(?:return \(?|energy\[nv\] = )(.*)", s)
+        if m and ("t" in m.group(1)):
+            expr = m.group(1)
+            if s.startswith("return (") and expr.endswith(")") and expr.count("(") < expr.count(")"):
+                expr = expr[:-1]
+            yield "<result>", expr
+
+
+def function_bodies(text, names):
+    """Return the bodies of the named functions, in the order given."""
+    out = []
+    for name in names:
+        m = re.search(r"\b" + re.escape(name) + r"\s*\([^)]*\)\s*\{", text)
+        if not m:
+            raise ValueError("function %s not found" % name)
+        depth, i = 1, m.end()
+        while depth:
+            c = text[i]
+            depth += (c == "{") - (c == "}")
+            i += 1
+        out.append(text[m.end():i - 1])
+    return out
+
+
+def strip_comments(text):
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return re.sub(r"//[^\n]*", "", text)
+
+
+def extract_program(ref, name):
+    rel, nvars, ncoef, degree = PROGRAMS[name]
+    path = os.path.join(ref, "src", rel)
+    text = strip_comments(open(path).read())
+    if name == "ch4ch42b":
+        bodies = function_bodies(text, ["fmg%d" % i for i in range(1, 16)])
+        main = re.search(r"::eval\(const double a\[1345\], const double x\[45\]\)\s*\{(.*?)\n\}", text, re.S).group(1)
+        bodies.append(main)
+    elif name == "mbpol2b":
+        m = re.search(r"for \(size_t nv = 0; nv < nd; nv\+\+\) \{(.*?)\n    \}\n    return energy;", text, re.S)
+        bodies = [m.group(1)]
+    else:
+        m = re.search(r"::eval\([^)]*\)\s*\{(.*)\}\s*\}\s*//\s*namespace", text, re.S)
+        if not m:
+            m = re.search(r"::eval\([^)]*\)\s*\{(.*)\}", text, re.S)
+        bodies = [m.group(1)]
+    env = {}
+    parser = Parser(env, xindex_factory(rel))
+    result = None
+    for body in bodies:
+        for target, expr in statements(body):
+            if target in ("fmg%d" % i for i in range(1, 16)):
+                continue
+            if re.fullmatch(r"fmg\d+\(x, a, t\)", expr or ""):
+                continue
+            v = parser.parse(expr)
+            if target == "<result>":
+                result = v
+            else:
+                env[target] = v
+    if result is None:
+        raise ValueError("no result expression found in %s" % rel)
+    terms = []
+    for (k, mono), c in result.items():
+        if k < 0:
+            raise ValueError("term without a coefficient in %s" % rel)
+        if len(mono) > degree or (mono and max(mono) >= nvars) or k >= ncoef:
+            raise ValueError("term out of range in %s: %r" % (rel, (k, mono)))
+        terms.append((k, mono, c))
+    terms.sort(key=lambda t: (t[0], len(t[1]), t[1]))
+    return terms
+
+
+def extract_fit(ref, name, ncoef):
+    rel, pattern = FITS[name]
+    text = strip_comments(open(os.path.join(ref, "src", rel)).read())
+    m = re.search(pattern, text)
+    if not m:
+        raise ValueError("coefficients not found in %s" % rel)
+    end = text.index("}", m.end())
+    vals = [float(v) for v in text[m.end():end].replace(",", " ").split()]
+    if len(vals) != ncoef:
+        raise ValueError("%s: expected %d coefficients, found %d" % (rel, ncoef, len(vals)))
+    return vals
+
+
+def write_tables(name, terms, fit, nvars, ncoef, degree):
+    os.makedirs(DATA, exist_ok=True)
+    with gzip.GzipFile(os.path.join(DATA, name + ".pip.gz"), "wb", mtime=0) as gz, \
+            __import__("io").TextIOWrapper(gz) as f:
+        f.write("# PIP term table: k coef nvar v1..vn  (P = sum a[k] * coef * prod x[v])\n")
+        f.write("%d %d %d %d\n" % (nvars, ncoef, degree, len(terms)))
+        for k, mono, c in terms:
+            ci = int(c)
+            cs = str(ci) if ci == c else repr(c)
+            f.write("%d %s %d %s\n" % (k, cs, len(mono), " ".join(map(str, mono))))
+    with open(os.path.join(DATA, name + ".fit"), "w") as f:
+        for v in fit:
+            f.write(repr(v) + "\n")
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("names", nargs="*", default=list(PROGRAMS))
+    args = ap.parse_args(argv)
+    for name in args.names:
+        t0 = time.time()
+        rel, nvars, ncoef, degree = PROGRAMS[name]
+        terms = extract_program(args.ref, name)
+        fit = extract_fit(args.ref, name, ncoef)
+        used = sorted({t[0] for t in terms})
+        write_tables(name, terms, fit, nvars, ncoef, degree)
+        print("%-9s %6d terms, %4d/%d coefficients used, %.1fs" % (name, len(terms), len(used), ncoef,
+                                                                   time.time() - t0))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

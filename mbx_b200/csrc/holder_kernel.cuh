@@ -1,0 +1,381 @@
+// Evaluation kernels for the 2-body/3-body evaluators (one template for all
+// types; the per-type pieces come from the generated traits T in gen/*.cuh).
+//
+// One n-mer per thread for the straight-line polynomials: the n-mer's atoms
+// are gathered, moved to the image next to the n-mer's first monomer
+// (GetCloseDimerImage / GetCloseTrimerImage), the polynomial variables are
+// built in FP64, the polynomial and its gradient run out of registers (the
+// generated Horner trie), then the switch, the chain rule to atoms (including
+// the lone-pair redistribution), the virial and the gradient scatter follow.
+// This is the work of x2b_v9x::eval / x3b_v2x::eval / the MB-nrg evaluators
+// (potential/2b/x2b-v9x.cpp:1514-1819, potential/3b/x3b-v2x.cpp:1403-1808,
+// x2b_A1B2Z2_C1D4_deg3_exp0_v1x.cpp:954, x2b_A1B4_A1B4_deg4_exp0_v1x.cpp:1600,
+// mbnrg_3b_A1B4_C1D2_C1D2_deg3_v1.cpp:1481) fused with the gather, image and
+// scatter steps of System::Get2B/Get3B (bblock/system.cpp:2425-2725,
+// 2769-3073).
+//
+// The CH4-CH4 polynomial (201k terms) is evaluated by a warp per dimer that
+// walks the term table (pip_warp below).
+#pragma once
+#include "holder_common.cuh"
+
+// Precision / output modes.
+enum { HM_ENERGY = 0, HM_GRAD_FP64 = 1, HM_GRAD_MIXED = 2, HM_ENERGY_MIXED = 3 };
+
+struct HolderArgs {
+    long n;                    // number of n-mers
+    const int4* nmers;         // system input: (m0, m1, m2, anchor slot), holder order
+    const double* xyz;         // system input: site array (3 per site); AoS input: [n][NREAL*3]
+    const int* first_index;    // system input: first site of every monomer
+    BoxParams bp;
+    double* grad;              // system: site-array gradient (+=); AoS: [n][NREAL*3] (+=)
+    double* out;               // [0] energy, [1..6] virial xx xy xz yy yz zz (+=)
+    double* e_per;             // optional: switched energy of every n-mer
+    const double* coef;        // custom linear coefficients (global) or null
+    int aos;                   // 1: AoS per-n-mer input (already imaged, no gather)
+    // table-driven polynomial (warp kernel)
+    const int4* terms;         // (k, v0 | v1<<8 | v2<<16 | v3<<24 (255 = none), deg, unused)
+    const double* tcoef;       // term multiplicities
+    long nterms;
+};
+
+// Coefficient source: a global pointer, read through the read-only path.
+struct GlobalCoef {
+    const double* __restrict__ p;
+    __device__ __forceinline__ double operator[](int k) const { return __ldg(p + k); }
+};
+
+__device__ __forceinline__ double ld_volatile(const double* p) {
+    double v;
+    asm volatile("ld.global.nc.f64 %0, [%1];" : "=d"(v) : "l"(p));
+    return v;
+}
+
+template <class T, bool VOL>
+__device__ __forceinline__ void load_nmer(const HolderArgs& A, long t, double (&r)[T::NREAL][3]) {
+    if (A.aos) {
+        const double* p = A.xyz + (size_t)t * (T::NREAL * 3);
+#pragma unroll
+        for (int i = 0; i < T::NREAL; ++i)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) r[i][c] = VOL ? ld_volatile(p + 3 * i + c) : __ldg(p + 3 * i + c);
+        return;
+    }
+    const int4 nm = __ldg(A.nmers + t);
+    const int mon[3] = {nm.x, nm.y, nm.z};
+    const int nat[3] = {T::NAT0, T::NAT1, T::NAT2};
+    const int first[3] = {T::FIRST0, T::FIRST1, T::FIRST2};
+#pragma unroll
+    for (int s = 0; s < T::NBODY; ++s) {
+        const double* p = A.xyz + 3 * (size_t)__ldg(A.first_index + mon[s]);
+#pragma unroll
+        for (int a = 0; a < 3 * 5; ++a) {
+            if (a < 3 * nat[s]) r[first[s] + a / 3][a % 3] = VOL ? ld_volatile(p + a) : __ldg(p + a);
+        }
+    }
+    if (A.bp.use_pbc) {
+        const int anchor = nm.w;
+        double p0[3];
+#pragma unroll
+        for (int s = 0; s < T::NBODY; ++s)
+            if (s == anchor) { p0[0] = r[first[s]][0]; p0[1] = r[first[s]][1]; p0[2] = r[first[s]][2]; }
+#pragma unroll
+        for (int s = 0; s < T::NBODY; ++s) {
+            if (s == anchor) continue;
+            double q0[3] = {r[first[s]][0], r[first[s]][1], r[first[s]][2]};
+            double d[3];
+            image_shift(A.bp, p0, q0, d);
+#pragma unroll
+            for (int a = 0; a < 5; ++a) {
+                if (a < nat[s]) {
+                    double q[3] = {r[first[s] + a][0], r[first[s] + a][1], r[first[s] + a][2]};
+                    apply_shift(A.bp, d, q);
+                    r[first[s] + a][0] = q[0];
+                    r[first[s] + a][1] = q[1];
+                    r[first[s] + a][2] = q[2];
+                }
+            }
+        }
+    }
+}
+
+// First-atom distances (pairs 01, 02, 12) and the skip rule of the type.
+template <class T>
+__device__ __forceinline__ bool pair_dists(const double (&r)[T::NREAL][3], double (&d)[3][3], double (&rr)[3]) {
+    const int first[3] = {T::FIRST0, T::FIRST1, T::FIRST2};
+    const int pa[3] = {0, 0, 1}, pb[3] = {1, 2, 2};
+    constexpr int NP = T::NBODY == 2 ? 1 : 3;
+#pragma unroll
+    for (int p = 0; p < NP; ++p) {
+        const int i = first[pa[p]], j = first[pb[p]];
+        d[p][0] = r[i][0] - r[j][0];
+        d[p][1] = r[i][1] - r[j][1];
+        d[p][2] = r[i][2] - r[j][2];
+        rr[p] = sqrt(d[p][0] * d[p][0] + d[p][1] * d[p][1] + d[p][2] * d[p][2]);
+    }
+    const double rf = T::RF;
+    if (T::SKIP == 0) return rr[0] > rf;
+    if (T::SKIP == 1)
+        return (rr[0] > rf && rr[1] > rf) || (rr[0] > rf && rr[2] > rf) || (rr[1] > rf && rr[2] > rf);
+    return rr[0] > rf && rr[1] > rf && rr[2] > rf;
+}
+
+// Switch value and the gradient of the switch with respect to first atoms,
+// scaled by the unswitched energy ep, added into tg.
+template <class T>
+__device__ __forceinline__ double apply_switch(const double (&d)[3][3], const double (&rr)[3], double ep,
+                                               double (&tg)[T::NREAL][3], bool grads) {
+    const int first[3] = {T::FIRST0, T::FIRST1, T::FIRST2};
+    if (!T::SWITCH_TRIPLE) {
+        double gs;
+        const double sw = f_switch(rr[0], T::RI, T::RF, gs);
+        if (grads) {
+            const double f = gs * ep / rr[0];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                tg[first[0]][c] += f * d[0][c];
+                tg[first[1]][c] -= f * d[0][c];
+            }
+        }
+        return sw;
+    }
+    double g0, g1, g2;
+    const double s0 = f_switch(rr[0], T::RI, T::RF, g0);
+    const double s1 = f_switch(rr[1], T::RI, T::RF, g1);
+    const double s2 = f_switch(rr[2], T::RI, T::RF, g2);
+    if (grads) {
+        const double f0 = g0 * (s1 + s2) * ep / rr[0];
+        const double f1 = g1 * (s0 + s2) * ep / rr[1];
+        const double f2 = g2 * (s0 + s1) * ep / rr[2];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            tg[first[0]][c] += f0 * d[0][c] + f1 * d[1][c];
+            tg[first[1]][c] += f2 * d[2][c] - f0 * d[0][c];
+            tg[first[2]][c] -= f1 * d[1][c] + f2 * d[2][c];
+        }
+    }
+    return s0 * s1 + s0 * s2 + s1 * s2;
+}
+
+// Everything after the polynomial: chain rule, switch, virial, scatter.
+template <class T>
+__device__ __forceinline__ void finish_nmer(const HolderArgs& A, long t, double ep, const double (&g)[T::NVARS],
+                                            bool grads, double (&acc)[7]) {
+    double r[T::NREAL][3];
+    load_nmer<T, true>(A, t, r);
+    double d[3][3], rr[3];
+    pair_dists<T>(r, d, rr);
+    double tg[T::NREAL][3];
+    if (grads) {
+        double s[T::NSITES][3], sg[T::NSITES][3];
+        T::sites(r, s);
+        T::chain(s, g, sg);
+#pragma unroll
+        for (int i = 0; i < T::NREAL; ++i)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) tg[i][c] = sg[i][c];
+    }
+    const double sw = apply_switch<T>(d, rr, ep, tg, false);
+    if (grads) {
+#pragma unroll
+        for (int i = 0; i < T::NREAL; ++i)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) tg[i][c] *= sw;
+        apply_switch<T>(d, rr, ep, tg, true);
+    }
+    const double es = sw * ep;
+    acc[0] += es;
+    if (A.e_per) A.e_per[t] = es;
+    if (!grads) return;
+#pragma unroll
+    for (int i = 0; i < T::NREAL; ++i) {
+        acc[1] -= r[i][0] * tg[i][0];
+        acc[2] -= r[i][0] * tg[i][1];
+        acc[3] -= r[i][0] * tg[i][2];
+        acc[4] -= r[i][1] * tg[i][1];
+        acc[5] -= r[i][1] * tg[i][2];
+        acc[6] -= r[i][2] * tg[i][2];
+    }
+    if (A.aos) {
+        double* p = A.grad + (size_t)t * (T::NREAL * 3);
+#pragma unroll
+        for (int i = 0; i < T::NREAL; ++i)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) p[3 * i + c] += tg[i][c];
+        return;
+    }
+    const int4 nm = __ldg(A.nmers + t);
+    const int mon[3] = {nm.x, nm.y, nm.z};
+    const int nat[3] = {T::NAT0, T::NAT1, T::NAT2};
+    const int first[3] = {T::FIRST0, T::FIRST1, T::FIRST2};
+#pragma unroll
+    for (int s = 0; s < T::NBODY; ++s) {
+        double* p = A.grad + 3 * (size_t)__ldg(A.first_index + mon[s]);
+#pragma unroll
+        for (int a = 0; a < 5; ++a)
+            if (a < nat[s])
+#pragma unroll
+                for (int c = 0; c < 3; ++c) atomicAdd(p + 3 * a + c, tg[first[s] + a][c]);
+    }
+}
+
+// One n-mer per thread, straight-line polynomial.
+template <class T, class CC, int MODE, bool CUSTOM>
+__global__ void __launch_bounds__(128) holder_kernel(const HolderArgs A) {
+    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    const bool grads = (MODE == HM_GRAD_FP64 || MODE == HM_GRAD_MIXED);
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < A.n; t += (long)gridDim.x * blockDim.x) {
+        double ep;
+        double g[T::NVARS];
+        {
+            double r[T::NREAL][3];
+            load_nmer<T, false>(A, t, r);
+            double d[3][3], rr[3];
+            if (pair_dists<T>(r, d, rr)) {
+                if (A.e_per) A.e_per[t] = 0.0;
+                continue;
+            }
+            double s[T::NSITES][3];
+            T::sites(r, s);
+            double x[T::NVARS];
+            T::vars(s, x);
+#pragma unroll
+            for (int v = 0; v < T::NVARS; ++v) g[v] = 0.0;
+            if constexpr (T::STRAIGHT) {
+                if constexpr (CUSTOM) {
+                    const GlobalCoef coef{A.coef};
+                    if (MODE == HM_ENERGY) ep = T::pip_e(coef, x);
+                    else if (MODE == HM_GRAD_FP64) ep = T::pip(coef, x, g);
+                    else {
+                        float xf[T::NVARS], gf[T::NVARS];
+#pragma unroll
+                        for (int v = 0; v < T::NVARS; ++v) { xf[v] = (float)x[v]; gf[v] = 0.0f; }
+                        ep = T::pip_mixed(coef, xf, x, g, gf);
+#pragma unroll
+                        for (int v = 0; v < T::NVARS; ++v) g[v] += (double)gf[v];
+                    }
+                } else {
+                    const CC coef{};
+                    if (MODE == HM_ENERGY) ep = T::pip_e(coef, x);
+                    else if (MODE == HM_GRAD_FP64) ep = T::pip(coef, x, g);
+                    else {
+                        float xf[T::NVARS], gf[T::NVARS];
+#pragma unroll
+                        for (int v = 0; v < T::NVARS; ++v) { xf[v] = (float)x[v]; gf[v] = 0.0f; }
+                        ep = T::pip_mixed(coef, xf, x, g, gf);
+#pragma unroll
+                        for (int v = 0; v < T::NVARS; ++v) g[v] += (double)gf[v];
+                    }
+                }
+            } else {
+                ep = 0.0;
+            }
+        }
+        finish_nmer<T>(A, t, ep, g, grads, acc);
+    }
+    block_reduce_add<7>(acc, A.out);
+}
+
+// Warp-cooperative evaluation for polynomials too large for straight-line
+// code: lane l handles terms l, l+32, ...; variables and gradient
+// accumulators of the warp's n-mer live in shared memory.
+template <class T, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) holder_warp_kernel(const HolderArgs A, int grads) {
+    __shared__ double xs[WARPS][T::NVARS];
+    __shared__ double gs[WARPS][T::NVARS];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    const long stride = (long)gridDim.x * WARPS;
+    for (long t = blockIdx.x * (long)WARPS + w; t < A.n; t += stride) {
+        double r[T::NREAL][3];
+        load_nmer<T, false>(A, t, r);
+        double d[3][3], rr[3];
+        if (pair_dists<T>(r, d, rr)) {
+            if (lane == 0 && A.e_per) A.e_per[t] = 0.0;
+            continue;
+        }
+        if (lane == 0) {
+            double s[T::NSITES][3], x[T::NVARS];
+            T::sites(r, s);
+            T::vars(s, x);
+#pragma unroll
+            for (int v = 0; v < T::NVARS; ++v) { xs[w][v] = x[v]; gs[w][v] = 0.0; }
+        }
+        __syncwarp();
+        double e = 0.0;
+        for (long q = lane; q < A.nterms; q += 32) {
+            const int4 tm = __ldg(A.terms + q);
+            const double c = (A.coef ? __ldg(A.coef + tm.x) : 0.0) * __ldg(A.tcoef + q);
+            const int deg = tm.z;
+            int v[4];
+            double xv[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                v[i] = (tm.y >> (8 * i)) & 255;
+                xv[i] = i < deg ? xs[w][v[i]] : 1.0;
+            }
+            const double p01 = xv[0] * xv[1], p23 = xv[2] * xv[3];
+            e += c * p01 * p23;
+            if (grads) {
+                if (deg > 0) atomicAdd(&gs[w][v[0]], c * xv[1] * p23);
+                if (deg > 1) atomicAdd(&gs[w][v[1]], c * xv[0] * p23);
+                if (deg > 2) atomicAdd(&gs[w][v[2]], c * p01 * xv[3]);
+                if (deg > 3) atomicAdd(&gs[w][v[3]], c * p01 * xv[2]);
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
+        __syncwarp();
+        if (lane == 0) {
+            double g[T::NVARS];
+#pragma unroll
+            for (int v = 0; v < T::NVARS; ++v) g[v] = gs[w][v];
+            finish_nmer<T>(A, t, e, g, grads != 0, acc);
+        }
+        __syncwarp();
+    }
+    block_reduce_add<7>(acc, A.out);
+}
+
+// Gradient with respect to the linear coefficients: out[k] += sum over n-mers
+// of w[n] * sw(n) * dP/da_k(x(n)), the monomials recomputed from the
+// coordinates (adjoint of E = sum_n sw(n) P(a, x(n)) for refitting).
+template <class T>
+__global__ void __launch_bounds__(128) holder_dcoef_kernel(const HolderArgs A, const double* __restrict__ w,
+                                                           double* __restrict__ out) {
+    __shared__ double part[T::NCOEF];
+    for (int k = threadIdx.x; k < T::NCOEF; k += blockDim.x) part[k] = 0.0;
+    __syncthreads();
+    const long nt = A.n;
+    for (long base = blockIdx.x * (long)blockDim.x; base < nt; base += (long)gridDim.x * blockDim.x) {
+        const long t = base + threadIdx.x;
+        double scale = 0.0;
+        double x[T::NVARS];
+#pragma unroll
+        for (int v = 0; v < T::NVARS; ++v) x[v] = 0.0;
+        if (t < nt) {
+            double r[T::NREAL][3];
+            load_nmer<T, false>(A, t, r);
+            double d[3][3], rr[3];
+            if (!pair_dists<T>(r, d, rr)) {
+                double s[T::NSITES][3];
+                T::sites(r, s);
+                T::vars(s, x);
+                double tg[T::NREAL][3];
+                scale = apply_switch<T>(d, rr, 0.0, tg, false) * (w ? w[t] : 1.0);
+            }
+        }
+        if constexpr (T::STRAIGHT) {
+            const unsigned lane = threadIdx.x & 31;
+            T::dcoef(x, [&](int k, double m) {
+                double v = scale * m;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                if (lane == 0 && v != 0.0) atomicAdd(&part[k], v);
+            });
+        }
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < T::NCOEF; k += blockDim.x)
+        if (part[k] != 0.0) atomicAdd(out + k, part[k]);
+}

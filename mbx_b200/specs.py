@@ -1,0 +1,261 @@
+"""Declarative description of the 2-body and 3-body evaluators on the path.
+
+Each evaluator of the reference ("polynomial holder": variables built from
+inter-site distances, virtual sites, a switching function, the chain rule to
+atoms and the virial) follows one template.  This module states every
+evaluator as data -- its sites, its polynomial variables, its switch and its
+skip rule -- so that the CUDA generator (``codegen/gen_kernels.py``) and the
+CPU oracle restatement (``oracle/``) are produced from one description.  The
+numbers below are the fitted model constants of the reference and must be
+identical to it; each block cites where they are defined.
+
+Variable kinds (r = |p1 - p2|):
+
+* ``exp``   v = exp(k * (d0 - r))
+            (``variable::v_exp0``, potential/2b/x2b-v9x.cpp:54-69;
+            ``var``, potential/3b/x3b-v2x.cpp:52-59 writes the same value as
+            exp(-k (r - d0)); ``variable::v_exp`` in tools/variable.cpp:68 is
+            the case d0 = 0)
+* ``coul``  v = exp(k * (d0 - r)) / r   (``variable::v_coul``,
+            potential/2b/x2b-v9x.cpp:73-92)
+
+Virtual sites ``lp``: the two MB-pol lone-pair sites of a water (O, H1, H2),
+``monomer::setup`` potential/2b/x2b-v9x.cpp:119-135:
+    X(+/-) = O + 0.5 * g_in * (OH1 + OH2) +/- g_out * (OH1 x OH2)
+with g_in = -9.721486914088159e-02, g_out = 9.859272078406150e-02
+(x2b-v9x.cpp:1341-1342; the same numbers are w12/wcross in
+x2b_A1B2Z2_C1D4_deg3_exp0_v1x.cpp:1003-1005).
+
+Switches (cosine, ``f_switch``):
+    s(r) = 1 for r <= ri, (1 + cos(pi (r - ri)/(rf - ri)))/2 for ri < r <= rf,
+           0 for r > rf
+* ``pair``: s(r12) on the first-atom distance of the two monomers
+  (x2b-v9x.cpp:1349-1362, x2b_A1B2Z2_C1D4_deg3_exp0_v1x.cpp:804-818,
+  x2b_A1B4_A1B4_deg4_exp0_v1x.cpp:1453-1466)
+* ``triple``: s12 s13 + s12 s23 + s13 s23 on the three first-atom distances
+  (x3b-v2x.cpp:1275-1288,1690; mbnrg_3b_A1B4_C1D2_C1D2_deg3_v1.cpp:1318-1333)
+
+Skip rules (n-mers not evaluated; their energy and gradient are exactly 0):
+* ``pair_gt``: r12 > rf  (x2b-v9x.cpp:1563)
+* ``two_of_three_gt``: at least two of r12, r13, r23 > rf (x3b-v2x.cpp:1515)
+* ``all_three_gt``: all of r12, r13, r23 > rf
+  (mbnrg_3b_A1B4_C1D2_C1D2_deg3_v1.cpp:1561)
+"""
+from dataclasses import dataclass, field
+from typing import List, Tuple
+
+LP_GAMMA_IN = -9.721486914088159e-02
+LP_GAMMA_OUT = 9.859272078406150e-02
+
+
+@dataclass(frozen=True)
+class Spec:
+    name: str                  # also the PIP table name in mbx_b200/data
+    monomers: Tuple[str, ...]  # monomer ids in evaluator (holder) order
+    nat: Tuple[int, ...]       # real atoms per monomer
+    sites: Tuple[str, ...]     # real atoms in holder order, then virtual sites
+    lp: Tuple[Tuple[int, int, int, int], ...]  # (monomer, first real site, X+ site, X- site)
+    variables: Tuple[Tuple[str, int, int, float, float], ...]  # (kind, site1, site2, k, d0)
+    switch: str                # "pair" or "triple"
+    ri: float
+    rf: float
+    skip: str                  # "pair_gt", "two_of_three_gt", "all_three_gt"
+    nvars: int
+    ncoef: int
+    degree: int
+    ref: str                   # reference evaluator (file:line)
+
+    @property
+    def nbody(self):
+        return len(self.monomers)
+
+    @property
+    def nreal(self):
+        return sum(self.nat)
+
+    def site(self, name):
+        return self.sites.index(name)
+
+
+def _vars(sites, table):
+    out = []
+    for kind, a, b, k, d0 in table:
+        out.append((kind, sites.index(a), sites.index(b), float(k), float(d0)))
+    return tuple(out)
+
+
+# ---------------------------------------------------------------------------
+# MB-pol 2b: x2o::x2b_v9x, potential/2b/x2b-v9x.cpp:1514-1819 (constants
+# :1330-1346, variables :1600-1650)
+# ---------------------------------------------------------------------------
+_S = ("Oa", "Ha1", "Ha2", "Ob", "Hb1", "Hb2", "Xa1", "Xa2", "Xb1", "Xb2")
+_kHHi, _kOHi = -6.480884773303821e-01, 1.674518993682975e+00
+_kHHc, _kOHc, _kOOc = 1.148231864355956e+00, 1.205989761123099e+00, 1.395357065790959e+00
+_kXH, _kXO, _kXX = 7.347036852042255e-01, 7.998249864422826e-01, 7.960663960630585e-01
+MBPOL2B = Spec(
+    name="mbpol2b", monomers=("h2o", "h2o"), nat=(3, 3), sites=_S,
+    lp=((0, 0, 6, 7), (1, 3, 8, 9)),
+    variables=_vars(_S, [
+        ("exp", "Ha1", "Ha2", _kHHi, 1.0), ("exp", "Hb1", "Hb2", _kHHi, 1.0),
+        ("exp", "Oa", "Ha1", _kOHi, 1.0), ("exp", "Oa", "Ha2", _kOHi, 1.0),
+        ("exp", "Ob", "Hb1", _kOHi, 1.0), ("exp", "Ob", "Hb2", _kOHi, 1.0),
+        ("coul", "Ha1", "Hb1", _kHHc, 4.0), ("coul", "Ha1", "Hb2", _kHHc, 4.0),
+        ("coul", "Ha2", "Hb1", _kHHc, 4.0), ("coul", "Ha2", "Hb2", _kHHc, 4.0),
+        ("coul", "Oa", "Hb1", _kOHc, 4.0), ("coul", "Oa", "Hb2", _kOHc, 4.0),
+        ("coul", "Ob", "Ha1", _kOHc, 4.0), ("coul", "Ob", "Ha2", _kOHc, 4.0),
+        ("coul", "Oa", "Ob", _kOOc, 4.0),
+        ("exp", "Xa1", "Hb1", _kXH, 4.0), ("exp", "Xa1", "Hb2", _kXH, 4.0),
+        ("exp", "Xa2", "Hb1", _kXH, 4.0), ("exp", "Xa2", "Hb2", _kXH, 4.0),
+        ("exp", "Xb1", "Ha1", _kXH, 4.0), ("exp", "Xb1", "Ha2", _kXH, 4.0),
+        ("exp", "Xb2", "Ha1", _kXH, 4.0), ("exp", "Xb2", "Ha2", _kXH, 4.0),
+        ("exp", "Oa", "Xb1", _kXO, 4.0), ("exp", "Oa", "Xb2", _kXO, 4.0),
+        ("exp", "Ob", "Xa1", _kXO, 4.0), ("exp", "Ob", "Xa2", _kXO, 4.0),
+        ("exp", "Xa1", "Xb1", _kXX, 4.0), ("exp", "Xa1", "Xb2", _kXX, 4.0),
+        ("exp", "Xa2", "Xb1", _kXX, 4.0), ("exp", "Xa2", "Xb2", _kXX, 4.0),
+    ]),
+    switch="pair", ri=4.5, rf=6.5, skip="pair_gt",
+    nvars=31, ncoef=1153, degree=4, ref="potential/2b/x2b-v9x.cpp:1514",
+)
+
+# ---------------------------------------------------------------------------
+# MB-pol 3b: x2o::x3b_v2x, potential/3b/x3b-v2x.cpp:1403-1808 (constants
+# :1256-1271, variables :1548-1584)
+# ---------------------------------------------------------------------------
+_S = ("Oa", "Ha1", "Ha2", "Ob", "Hb1", "Hb2", "Oc", "Hc1", "Hc2")
+_kHHi3, _dHHi3 = -2.254303257872797e+00, 1.690594510379166e+00
+_kOHi3, _dOHi3 = -2.564771901404151e-01, -2.999999868517452e+00
+_kHH3, _dHH3 = 4.247920544074333e-01, 3.499031358429095e+00
+_kOH3, _dOH3 = 8.128985941165371e-01, 4.854042963514281e+00
+_kOO3, _dOO3 = 3.749457984616480e-02, 4.816312044947604e-08
+_pairs3 = [
+    ("Ha1", "Ha2", _kHHi3, _dHHi3), ("Hb1", "Hb2", _kHHi3, _dHHi3), ("Hc1", "Hc2", _kHHi3, _dHHi3),
+    ("Oa", "Ha1", _kOHi3, _dOHi3), ("Oa", "Ha2", _kOHi3, _dOHi3), ("Ob", "Hb1", _kOHi3, _dOHi3),
+    ("Ob", "Hb2", _kOHi3, _dOHi3), ("Oc", "Hc1", _kOHi3, _dOHi3), ("Oc", "Hc2", _kOHi3, _dOHi3),
+    ("Ha1", "Hb1", _kHH3, _dHH3), ("Ha1", "Hb2", _kHH3, _dHH3), ("Ha1", "Hc1", _kHH3, _dHH3),
+    ("Ha1", "Hc2", _kHH3, _dHH3), ("Ha2", "Hb1", _kHH3, _dHH3), ("Ha2", "Hb2", _kHH3, _dHH3),
+    ("Ha2", "Hc1", _kHH3, _dHH3), ("Ha2", "Hc2", _kHH3, _dHH3), ("Hb1", "Hc1", _kHH3, _dHH3),
+    ("Hb1", "Hc2", _kHH3, _dHH3), ("Hb2", "Hc1", _kHH3, _dHH3), ("Hb2", "Hc2", _kHH3, _dHH3),
+    ("Oa", "Hb1", _kOH3, _dOH3), ("Oa", "Hb2", _kOH3, _dOH3), ("Oa", "Hc1", _kOH3, _dOH3),
+    ("Oa", "Hc2", _kOH3, _dOH3), ("Ob", "Ha1", _kOH3, _dOH3), ("Ob", "Ha2", _kOH3, _dOH3),
+    ("Ob", "Hc1", _kOH3, _dOH3), ("Ob", "Hc2", _kOH3, _dOH3), ("Oc", "Ha1", _kOH3, _dOH3),
+    ("Oc", "Ha2", _kOH3, _dOH3), ("Oc", "Hb1", _kOH3, _dOH3), ("Oc", "Hb2", _kOH3, _dOH3),
+    ("Oa", "Ob", _kOO3, _dOO3), ("Oa", "Oc", _kOO3, _dOO3), ("Ob", "Oc", _kOO3, _dOO3),
+]
+MBPOL3B = Spec(
+    name="mbpol3b", monomers=("h2o", "h2o", "h2o"), nat=(3, 3, 3), sites=_S, lp=(),
+    variables=_vars(_S, [("exp", a, b, k, d) for a, b, k, d in _pairs3]),
+    switch="triple", ri=0.0, rf=4.5, skip="two_of_three_gt",
+    nvars=36, ncoef=1163, degree=4, ref="potential/3b/x3b-v2x.cpp:1403",
+)
+
+# ---------------------------------------------------------------------------
+# CH4-H2O 2b: x2b_A1B2Z2_C1D4_v1x("h2o","ch4"), water first,
+# potential/2b/x2b_A1B2Z2_C1D4_deg3_exp0_v1x.cpp:954-1250 (constants :778-800,
+# variables :1007-1044)
+# ---------------------------------------------------------------------------
+_S = ("A1", "B1", "B2", "C1", "D1", "D2", "D3", "D4", "Z1", "Z2")
+_c = dict(
+    kAB=(7.981769253199138e-01, 4.040819683827504e+00), kBB=(2.579463880579890e-01, 2.377019586697373e+00),
+    kCD=(3.688427221099756e-01, 4.333852019203771e+00), kDD=(7.091344939292101e-01, 3.168984322065454e+00),
+    AC=(1.564512113339641e+00, 3.257864349051078e+00), AD=(6.622458897222858e-01, 3.893753782478246e+00),
+    BC=(1.206761651281590e+00, 2.837093011555366e+00), BD=(7.972437249347342e-01, 5.352114146493275e+00),
+    CZ=(1.291962400963017e+00, 4.726091329507012e+00), DZ=(4.825788863998004e-01, 5.184523093153075e+00),
+)
+
+
+def _v(kind, a, b, key):
+    k, d = _c[key]
+    return (kind, a, b, k, d)
+
+
+_tab = [_v("exp", "A1", "B1", "kAB"), _v("exp", "A1", "B2", "kAB"), _v("exp", "B1", "B2", "kBB")]
+_tab += [_v("exp", "C1", "D%d" % i, "kCD") for i in range(1, 5)]
+_tab += [_v("exp", "D%d" % i, "D%d" % j, "kDD") for i in range(1, 5) for j in range(i + 1, 5)]
+_tab += [_v("exp", "A1", "C1", "AC")] + [_v("exp", "A1", "D%d" % i, "AD") for i in range(1, 5)]
+_tab += [_v("exp", "B1", "C1", "BC")] + [_v("exp", "B1", "D%d" % i, "BD") for i in range(1, 5)]
+_tab += [_v("exp", "B2", "C1", "BC")] + [_v("exp", "B2", "D%d" % i, "BD") for i in range(1, 5)]
+_tab += [_v("coul", "Z1", "C1", "CZ")] + [_v("coul", "Z1", "D%d" % i, "DZ") for i in range(1, 5)]
+_tab += [_v("coul", "Z2", "C1", "CZ")] + [_v("coul", "Z2", "D%d" % i, "DZ") for i in range(1, 5)]
+CH4H2O2B = Spec(
+    name="ch4h2o2b", monomers=("h2o", "ch4"), nat=(3, 5), sites=_S, lp=((0, 0, 8, 9),),
+    variables=_vars(_S, _tab), switch="pair", ri=8.0, rf=9.0, skip="pair_gt",
+    nvars=38, ncoef=603, degree=3, ref="potential/2b/x2b_A1B2Z2_C1D4_deg3_exp0_v1x.cpp:954",
+)
+
+# ---------------------------------------------------------------------------
+# CH4-CH4 2b: x2b_A1B4_A1B4_v1x, potential/2b/x2b_A1B4_A1B4_deg4_exp0_v1x.cpp
+# :1600-1760 (constants :1436-1449, variables :1515-1559)
+# ---------------------------------------------------------------------------
+_S = ("Aa", "B1a", "B2a", "B3a", "B4a", "Ab", "B1b", "B2b", "B3b", "B4b")
+_kABi = (3.188848769154688e+00, 1.993909788871820e+00)
+_kBBi = (1.204263123667977e+00, 2.367262478707738e+00)
+_kAA = (3.280825850503320e+00, 1.705786899598748e+00)
+_kAB = (6.515735442121080e-01, 4.621435907700928e+00)
+_kBB = (1.345128916678614e+00, 5.411919409835622e+00)
+_tab = []
+for m in "ab":
+    _tab += [("exp", "A" + m, "B%d%s" % (i, m)) + _kABi for i in range(1, 5)]
+    _tab += [("exp", "B%d%s" % (i, m), "B%d%s" % (j, m)) + _kBBi for i in range(1, 5) for j in range(i + 1, 5)]
+_tab += [("exp", "Aa", "Ab") + _kAA]
+_tab += [("exp", "Aa", "B%db" % i) + _kAB for i in range(1, 5)]
+for i in range(1, 5):
+    _tab += [("exp", "B%da" % i, "Ab") + _kAB]
+    _tab += [("exp", "B%da" % i, "B%db" % j) + _kBB for j in range(1, 5)]
+CH4CH42B = Spec(
+    name="ch4ch42b", monomers=("ch4", "ch4"), nat=(5, 5), sites=_S, lp=(),
+    variables=_vars(_S, _tab), switch="pair", ri=8.0, rf=9.0, skip="pair_gt",
+    nvars=45, ncoef=1345, degree=4, ref="potential/2b/x2b_A1B4_A1B4_deg4_exp0_v1x.cpp:1600",
+)
+
+# ---------------------------------------------------------------------------
+# CH4-H2O-H2O 3b: mbnrg_A1B4_C1D2_C1D2_deg3_v1, methane first,
+# potential/3b/mbnrg_3b_A1B4_C1D2_C1D2_deg3_v1.cpp:1481-1863 (constants
+# :1301-1313, variables :1617-1671; v_exp has d0 = 0)
+# ---------------------------------------------------------------------------
+_S = ("A1", "B1", "B2", "B3", "B4", "C1", "D1", "D2", "C2", "D3", "D4")
+_k = dict(
+    AB1=1.531189404203529e+00, AC0=4.745721065911203e+00, AD0=5.125853420719423e-01,
+    BB1=2.388453487869389e+00, BC0=8.378927200873254e-01, BD0=1.429945481869194e+00,
+    CC0=5.000000078438228e-01, CD1=5.359930384592185e+00, CD0=1.064344403260153e+00,
+    DD1=2.264354654848907e+00, DD0=5.000020400292975e-01,
+)
+_tab = [
+    ("A1", "B1", "AB1"), ("A1", "B2", "AB1"), ("A1", "B3", "AB1"), ("A1", "B4", "AB1"),
+    ("A1", "C1", "AC0"), ("A1", "C2", "AC0"),
+    ("A1", "D1", "AD0"), ("A1", "D2", "AD0"), ("A1", "D3", "AD0"), ("A1", "D4", "AD0"),
+]
+for i in range(1, 5):
+    _tab += [("B%d" % i, "B%d" % j, "BB1") for j in range(i + 1, 5)]
+    _tab += [("B%d" % i, "C1", "BC0"), ("B%d" % i, "C2", "BC0")]
+    _tab += [("B%d" % i, "D%d" % j, "BD0") for j in range(1, 5)]
+_tab += [("C1", "C2", "CC0"), ("C1", "D1", "CD1"), ("C1", "D2", "CD1"), ("C1", "D3", "CD0"), ("C1", "D4", "CD0"),
+         ("C2", "D1", "CD0"), ("C2", "D2", "CD0"), ("C2", "D3", "CD1"), ("C2", "D4", "CD1"),
+         ("D1", "D2", "DD1"), ("D1", "D3", "DD0"), ("D1", "D4", "DD0"), ("D2", "D3", "DD0"), ("D2", "D4", "DD0"),
+         ("D3", "D4", "DD1")]
+CH4H2O3B = Spec(
+    name="ch4h2o3b", monomers=("ch4", "h2o", "h2o"), nat=(5, 3, 3), sites=_S, lp=(),
+    variables=_vars(_S, [("exp", a, b, _k[key], 0.0) for a, b, key in _tab]),
+    switch="triple", ri=5.0, rf=6.0, skip="all_three_gt",
+    nvars=55, ncoef=1254, degree=3, ref="potential/3b/mbnrg_3b_A1B4_C1D2_C1D2_deg3_v1.cpp:1481",
+)
+
+SPECS = {s.name: s for s in (MBPOL2B, MBPOL3B, CH4H2O2B, CH4CH42B, CH4H2O3B)}
+
+# Dispatch by sorted monomer ids (e2b::get_2b_energy, potential/2b/energy2b.cpp:
+# 240-254,258,282,323; e3b::get_3b_energy, potential/3b/energy3b.cpp:185-216,
+# 220,243).  Any other tuple evaluates to 0, as in the reference's else branch.
+DISPATCH_2B = {("h2o", "h2o"): "mbpol2b", ("ch4", "h2o"): "ch4h2o2b", ("ch4", "ch4"): "ch4ch42b"}
+DISPATCH_3B = {("h2o", "h2o", "h2o"): "mbpol3b", ("ch4", "h2o", "h2o"): "ch4h2o3b"}
+
+# Real atoms and total sites (real + electrostatic virtual sites) per monomer
+# type, as the reference's monomer table sets them (bblock/sys_tools.cpp
+# SetUpMonomers:133-254: h2o has 3 atoms + the M site, ch4 5 atoms).
+MONOMER_ATOMS = {"h2o": 3, "ch4": 5}
+MONOMER_SITES = {"h2o": 4, "ch4": 5}
+
+
+def check():
+    for s in SPECS.values():
+        assert len(s.variables) == s.nvars, (s.name, len(s.variables))
+        assert len(s.sites) == s.nreal + 2 * len(s.lp), s.name
+    return True

@@ -1,0 +1,150 @@
+"""Seeded synthetic inputs for the 2-body/3-body path.
+
+No public benchmark or dataset exists for this path; the workloads are built
+from their stated recipes with numpy ``default_rng(seed)``:
+
+* ``water_box(n_side, n_mol, L)``: rigid waters (O-H 0.9572 A, HOH 104.52 deg)
+  with uniformly random orientations (uniform quaternions), oxygens on an
+  ``n_side^3`` lattice of spacing L/n_side (``n_mol`` sites drawn without
+  replacement), each oxygen jittered by U(-0.3, 0.3) A per component; cubic
+  periodic box of edge L.  256 waters: n_side 7, L 19.72 A; 2048 waters:
+  n_side 14, L 39.44 A (1.0 g/cm^3).
+* ``beads(base, n, sigma)``: path-integral beads, every atom displaced by
+  independent N(0, sigma^2) noise.
+* ``water_cluster(n)``: gas-phase cluster of n random rigid waters at liquid
+  density (0.0334 molecules/A^3) inside a sphere, O-O >= 2.5 A by rejection.
+* ``gas_trimers / gas_dimers``: isolated n-mers with O-O distances uniform in
+  a range and random orientations.
+* ``methane_water_box``: 57 CH4 (C-H 1.09 A, tetrahedral) + 513 H2O, random
+  centres with heavy-atom separation >= 2.6 A, box 24.6 x 24.6 x 31.0 A.
+
+Coordinates are returned in the reference's input layout: a list of monomer
+ids and the real atoms in input order (3 floats per atom).
+"""
+import numpy as np
+
+R_OH = 0.9572
+THETA_HOH = np.deg2rad(104.52)
+R_CH = 1.09
+
+
+def random_rotations(rng, n):
+    q = rng.normal(size=(n, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    w, x, y, z = q.T
+    return np.stack([
+        np.stack([1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)], -1),
+        np.stack([2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)], -1),
+        np.stack([2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)], -1),
+    ], 1)
+
+
+def water_body():
+    h = THETA_HOH / 2
+    return np.array([[0.0, 0.0, 0.0],
+                     [R_OH * np.sin(h), 0.0, R_OH * np.cos(h)],
+                     [-R_OH * np.sin(h), 0.0, R_OH * np.cos(h)]])
+
+
+def methane_body():
+    t = R_CH / np.sqrt(3.0)
+    return np.array([[0, 0, 0], [t, t, t], [t, -t, -t], [-t, t, -t], [-t, -t, t]], float)
+
+
+def place(rng, body, centres):
+    rot = random_rotations(rng, len(centres))
+    return centres[:, None, :] + np.einsum("nij,aj->nai", rot, body)
+
+
+def water_box(n_side=14, n_mol=2048, L=39.44, seed=0, jitter=0.3):
+    rng = np.random.default_rng(seed)
+    s = L / n_side
+    g = (np.arange(n_side) + 0.5) * s - L / 2
+    lattice = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+    pick = rng.choice(len(lattice), size=n_mol, replace=False)
+    centres = lattice[pick] + rng.uniform(-jitter, jitter, size=(n_mol, 3))
+    xyz = place(rng, water_body(), centres)
+    box = np.array([L, 0, 0, 0, L, 0, 0, 0, L], float)
+    return ["h2o"] * n_mol, xyz.reshape(-1), box
+
+
+def water_256(seed=0):
+    return water_box(7, 256, 19.72, seed)
+
+
+def water_2048(seed=0):
+    return water_box(14, 2048, 39.44, seed)
+
+
+def beads(xyz, n, sigma=0.05, seed=0):
+    rng = np.random.default_rng(seed)
+    xyz = np.asarray(xyz, float).reshape(-1)
+    return [xyz + rng.normal(0.0, sigma, size=xyz.shape) for _ in range(n)]
+
+
+def water_cluster(n, seed=0, density=0.0334, dmin=2.5):
+    rng = np.random.default_rng(seed)
+    radius = (3.0 * n / (4.0 * np.pi * density)) ** (1.0 / 3.0)
+    centres = []
+    tries = 0
+    while len(centres) < n:
+        tries += 1
+        if tries > 2000 * n:
+            radius *= 1.02
+            tries = 0
+        p = rng.uniform(-radius, radius, size=3)
+        if np.dot(p, p) > radius * radius:
+            continue
+        if centres and np.min(np.linalg.norm(np.array(centres) - p, axis=1)) < dmin:
+            continue
+        centres.append(p)
+    xyz = place(rng, water_body(), np.array(centres))
+    return ["h2o"] * n, xyz.reshape(-1)
+
+
+def _random_directions(rng, n):
+    v = rng.normal(size=(n, 3))
+    return v / np.linalg.norm(v, axis=1, keepdims=True)
+
+
+def gas_dimers(n=20000, rmin=2.2, rmax=9.0, seed=0):
+    """[n, 18] AoS (O H H, O H H), O-O distance uniform in [rmin, rmax]."""
+    rng = np.random.default_rng(seed)
+    r = rng.uniform(rmin, rmax, size=n)
+    c2 = _random_directions(rng, n) * r[:, None]
+    a = place(rng, water_body(), np.zeros((n, 3)))
+    b = place(rng, water_body(), c2)
+    return np.concatenate([a.reshape(n, 9), b.reshape(n, 9)], 1)
+
+
+def gas_trimers(n=20000, rmin=2.4, rmax=6.5, seed=0):
+    """[n, 27] AoS, the two O-O distances from molecule a uniform in [rmin, rmax]."""
+    rng = np.random.default_rng(seed)
+    rb = rng.uniform(rmin, rmax, size=n)
+    rc = rng.uniform(rmin, rmax, size=n)
+    cb = _random_directions(rng, n) * rb[:, None]
+    cc = _random_directions(rng, n) * rc[:, None]
+    a = place(rng, water_body(), np.zeros((n, 3)))
+    b = place(rng, water_body(), cb)
+    c = place(rng, water_body(), cc)
+    return np.concatenate([a.reshape(n, 9), b.reshape(n, 9), c.reshape(n, 9)], 1)
+
+
+def methane_water_box(n_ch4=57, n_h2o=513, box=(24.6, 24.6, 31.0), seed=0, dmin=2.6):
+    rng = np.random.default_rng(seed)
+    L = np.array(box, float)
+    n = n_ch4 + n_h2o
+    centres = np.zeros((0, 3))
+    while len(centres) < n:
+        p = (rng.uniform(size=3) - 0.5) * L
+        if len(centres):
+            d = centres - p
+            d -= L * np.round(d / L)
+            if np.min(np.einsum("ij,ij->i", d, d)) < dmin * dmin:
+                continue
+        centres = np.vstack([centres, p])
+    ch4 = place(rng, methane_body(), centres[:n_ch4])
+    h2o = place(rng, water_body(), centres[n_ch4:])
+    ids = ["ch4"] * n_ch4 + ["h2o"] * n_h2o
+    xyz = np.concatenate([ch4.reshape(-1), h2o.reshape(-1)])
+    return ids, xyz, np.array([L[0], 0, 0, 0, L[1], 0, 0, 0, L[2]], float)
