@@ -1,0 +1,326 @@
+#!/usr/bin/env python3
+"""Throughput of the 2-body + 3-body path: dimers+trimers/s with forces, 2048 H2O.
+
+One step = one TwoBodyEnergy + one ThreeBodyEnergy (System::Get2B + Get3B) of
+the 2048-water box (cubic 39.44 A, 2b cutoff 9 A, 3b cutoff 7 A, seed 0):
+FixMonomerCoordinates, the n-mer search, every evaluator with energies,
+gradients and virial.  Units = listed n-mers (dimers within 9 A + trimers by
+the reference's AddClusters rule within 7 A), the reference's unit of work.
+
+* value: device-resident (coordinates and gradients in HBM), CUDA events on
+  the library's stream, L2 flushed between steps (inputs are far smaller than
+  the 126 MB L2), FP64 path;
+* e2e: the same through the public API (mbx_b200.system.System) with pinned
+  host buffers, host<->device copies inside, wall clock per step;
+* mixed: the FP32-monomial / FP64-accumulate path, its throughput and its
+  energy error against the FP64 path;
+* roofline: the MB-pol 3b evaluation kernel, algorithmic flops counted from
+  the reference's gradient program (mbx_b200/data/flops.json) over its
+  CUDA-event duration, against the measured FP64 FMA peak of this GPU;
+* cpu_baseline: the reference's own CPU path (oracle/_ref, built from the
+  reference sources) on the host's cores, bounded sample.
+
+``--impl reference`` times the reference CPU implementation alone on the same
+workload.  With torchrun (N>1) every rank runs an independent replica (the
+path needs no exchange between replicas); value = all ranks' units / max time.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "dimers+trimers/s with forces, 2048 H2O; FP32-mixed vs FP64 GPU at <=1e-6 rel E"
+CUT2, CUT3 = 9.0, 7.0
+
+
+def workload():
+    from mbx_b200 import workloads
+    ids, xyz, box = workloads.water_2048(0)
+    return ids, xyz, box
+
+
+def config(n):
+    return {"workload": "2048 H2O periodic box 39.44 A (1.0 g/cm3), cutoffs 9/7 A, seed 0",
+            "monomers": 2048, "cutoff2b": CUT2, "cutoff3b": CUT3, "l2": "flushed between steps (256 MiB write)",
+            "parallelism": "replicas" if n > 1 else "single"}
+
+
+class Clocks:
+    """Samples nvidia-smi during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 7:
+                continue
+            try:
+                sm.append(float(p[0]))
+                mx.append(float(p[1]))
+            except ValueError:
+                continue
+            for k, name in enumerate(names):
+                if p[3 + k].lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def ref_cpu(ids, xyz, box, seconds=12.0, threads=None):
+    """The reference CPU path (oracle/_ref) on this host: (units/s, cores, sample)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import mbx_oracle as mo
+    if not mo.RefSystem.available():
+        return None
+    threads = threads or os.cpu_count()
+    mo.RefSystem.set_threads(threads)
+    r = mo.RefSystem(ids, xyz, box, CUT2, CUT3)
+    nd = len(r.pair_list(2, CUT2))
+    nt = len(r.pair_list(3, CUT3))
+    r.energy(2)
+    r.energy(3)
+    t0 = time.perf_counter()
+    steps = 0
+    while True:
+        r.energy(2)
+        r.energy(3)
+        steps += 1
+        if time.perf_counter() - t0 > seconds:
+            break
+    dt = (time.perf_counter() - t0) / steps
+    return {"value": (nd + nt) / dt, "unit": "n-mers/s", "cores": threads, "kind": "reference",
+            "sample": "%d full steps (TwoBodyEnergy(true)+ThreeBodyEnergy(true), 2048 H2O), %.2f s/step, "
+                      "OMP_NUM_THREADS=%d" % (steps, dt, threads), "ms_per_step": dt * 1e3}
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return 0
+    ids, xyz, box = workload()
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import mbx_oracle as mo
+    if not mo.RefSystem.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libmbx_ref.so not built"}))
+        return 0
+    threads = os.cpu_count()
+    mo.RefSystem.set_threads(threads)
+    r = mo.RefSystem(ids, xyz, box, CUT2, CUT3)
+    units = len(r.pair_list(2, CUT2)) + len(r.pair_list(3, CUT3))
+    for _ in range(args.warmup):
+        r.energy(2)
+        r.energy(3)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        r.energy(2)
+        r.energy(3)
+        times.append(time.perf_counter() - t0)
+    dt = sum(times) / len(times)
+    v = units / dt
+    out = {"metric": METRIC, "value": v, "unit": "n-mers/s", "n_gpus": args.gpus, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config(1), "impl": "reference",
+           "cpu_baseline": {"value": v, "unit": "n-mers/s", "cores": threads, "kind": "reference",
+                            "sample": "%d steps of TwoBodyEnergy(true)+ThreeBodyEnergy(true)" % args.steps},
+           "e2e": {"value": v, "unit": "n-mers/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank)
+
+    import torch
+    from mbx_b200 import capi, system as msys
+    from mbx_b200.tables import load_fit  # noqa: F401
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    ids, xyz, box = workload()
+    stream = torch.cuda.current_stream()
+    ctx = capi.Context(local, stream.cuda_stream)
+    peaks = capi.fma_peaks(local)
+    flops = json.load(open(os.path.join(ROOT, "mbx_b200", "data", "flops.json")))
+
+    # ---------------- device-resident steps
+    sys_d = msys.from_arrays(ids, xyz, box, CUT2, CUT3, context=ctx)
+    sites = torch.tensor(sys_d.sites, dtype=torch.float64, device="cuda")
+    grad = torch.zeros_like(sites)
+    vir = np.zeros(9)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+
+    def step(mixed=False):
+        grad.zero_()
+        e2 = ctx.energy(2, sites, grad, vir, mixed=mixed)
+        ms2 = ctx.timing()
+        e3 = ctx.energy(3, sites, grad, vir, mixed=mixed)
+        ms3 = ctx.timing()
+        return e2, e3, ms2, ms3
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    listed2, eval2 = ctx.counts(2)
+    listed3, eval3 = ctx.counts(3)
+    units = listed2 + listed3
+
+    def timed(mixed):
+        times, evals, launches, energies = [], [], 0, None
+        for _ in range(args.steps):
+            flush.zero_()
+            if dist:
+                dist.barrier()
+            torch.cuda.synchronize()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            e2, e3, ms2, ms3 = step(mixed)
+            b.record(stream)
+            torch.cuda.synchronize()
+            times.append(a.elapsed_time(b))
+            evals.append(ms3[1])
+            launches += ms2[2] + ms3[2]
+            energies = (e2, e3)
+        return times, evals, launches, energies
+
+    with Clocks(local) as clk:
+        t64, ev64, launches, (e2_64, e3_64) = timed(False)
+    clocks = clk.summary()
+    for _ in range(args.warmup):
+        step(True)
+    tmx, evmx, launches_mx, (e2_mx, e3_mx) = timed(True)
+
+    ms = sum(t64) / len(t64)
+    ms_mx = sum(tmx) / len(tmx)
+    if dist:
+        tt = torch.tensor([ms, ms_mx], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms, ms_mx = tt.tolist()
+    value = world * units / (ms * 1e-3)
+
+    # ---------------- end to end through the public API (host buffers)
+    sys_h = msys.from_arrays(ids, xyz, box, CUT2, CUT3, context=ctx)
+    pinned_sites = torch.tensor(sys_h.sites, dtype=torch.float64).pin_memory()
+    pinned_grad = torch.zeros_like(pinned_sites).pin_memory()
+    sys_h.sites = pinned_sites.numpy()
+    sys_h.grad = pinned_grad.numpy()
+    for _ in range(max(args.warmup, 3)):
+        sys_h.TwoBodyEnergy(True)
+        sys_h.ThreeBodyEnergy(True)
+    e2e_t = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sys_h.TwoBodyEnergy(True)
+        g2 = sys_h.GetRealGrads()
+        sys_h.ThreeBodyEnergy(True)
+        g3 = sys_h.GetRealGrads()
+        e2e_t.append(time.perf_counter() - t0)
+    e2e_ms = 1e3 * sum(e2e_t) / len(e2e_t)
+    if dist:
+        tt = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_ms = tt.item()
+    nbytes = 8 * sys_h.sites.size
+    h2d = 2 * nbytes
+    d2h = 2 * (2 * nbytes + 8 * 8)
+
+    # ---------------- roofline of the MB-pol 3b evaluation kernel
+    kern_ms = sum(ev64) / len(ev64)
+    achieved = eval3 * flops["mbpol3b"]["flops"] / (kern_ms * 1e-3) / 1e12
+    roofline = {"bound": "fp64-fma", "kernel": "holder_kernel<mbpol3b_T, HM_GRAD_FP64>", "achieved": achieved,
+                "peak": peaks["fp64_tflops"], "unit": "TFLOP/s", "frac": achieved / peaks["fp64_tflops"],
+                "traffic": None,
+                "note": "algorithmic flops = evaluated trimers x %d (reference gradient program, "
+                        "mbx_b200/data/flops.json); peak = FP64 FMA pipe measured on this GPU by "
+                        "mbx_fma_peaks (MEASURED_PEAKS.json has no FP64 figure)" % flops["mbpol3b"]["flops"],
+                "fp32_peak": peaks["fp32_tflops"], "kernel_ms": kern_ms, "evaluated_trimers": eval3}
+
+    out = {"metric": METRIC, "value": value, "unit": "n-mers/s", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config(world),
+           "units_per_step": {"dimers": listed2, "trimers": listed3, "evaluated_dimers": eval2,
+                              "evaluated_trimers": eval3},
+           "energies": {"E2B": e2_64, "E3B": e3_64},
+           "mixed": {"value": world * units / (ms_mx * 1e-3), "ms_per_step": ms_mx, "dtype": "f32-monomial/f64-acc",
+                     "rel_err_E2B": abs(e2_mx - e2_64) / abs(e2_64), "rel_err_E3B": abs(e3_mx - e3_64) / abs(e3_64),
+                     "rel_err_E": abs((e2_mx + e3_mx) - (e2_64 + e3_64)) / abs(e2_64 + e3_64),
+                     "speedup_vs_fp64": ms / ms_mx},
+           "e2e": {"value": world * units / (e2e_ms * 1e-3), "unit": "n-mers/s", "h2d_bytes_per_step": h2d,
+                   "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms, "api": "mbx_b200.system.System"},
+           "gpu_launches": launches, "roofline": roofline, "clocks": clocks,
+           "fma_peaks_tflops": peaks}
+    if rank == 0 and not args.no_cpu_baseline:
+        cb = ref_cpu(ids, xyz, box)
+        if cb:
+            out["cpu_baseline"] = cb
+    if rank == 0:
+        print(json.dumps(out))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    ctx.close()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,125 @@
+/* mbx_b200: B200-native many-body 2-body/3-body engine -- C ABI.
+ *
+ * The drop-in boundary is the reference's bblock::System 2-body/3-body path:
+ *   double System::Get2B(bool do_grads, bool use_ghost)
+ *   double System::Get3B(bool do_grads, bool use_ghost)
+ * (bblock/system.h:1268,1279; bblock/system.cpp:2425-2725, 2769-3073), reached
+ * from TwoBodyEnergy/ThreeBodyEnergy (system.h:1088,1100, system.cpp:2403-2423,
+ * 2727-2745), plus the evaluator and generated-polynomial calling conventions
+ * below them.  Plain pointers and sizes only; every call returns 0 on success
+ * or an MBX_E* code, with a message in mbx_last_error().
+ *
+ * Coordinates follow the reference's internal layout: one array of 3 doubles
+ * per site (real atoms and electrostatic virtual sites), monomers in internal
+ * order, monomer m starting at site first_index[m].  Gradients are dE/dx
+ * (kcal/mol/A), energies kcal/mol, virial -sum r (x) dE/dr (9, row-major,
+ * symmetric).
+ */
+#ifndef MBX_B200_H
+#define MBX_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct mbx_ctx mbx_ctx;
+
+enum {
+    MBX_OK = 0,
+    MBX_EINVAL = 22,    /* bad argument, size or box */
+    MBX_ENOMEM = 12,    /* device allocation failed */
+    MBX_EDOM = 33,      /* cutoff too large for the periodic box */
+    MBX_ENOTSUP = 95,   /* unknown evaluator or monomer type */
+    MBX_ECUDA = 1000,   /* CUDA runtime error (message has details) */
+    MBX_ENODEV = 1001   /* no CUDA device */
+};
+
+/* flags */
+#define MBX_DEVICE_PTRS 1   /* array arguments are device pointers (else host) */
+#define MBX_MIXED 2         /* FP32 monomials, FP64 accumulation (else FP64) */
+#define MBX_NO_GRADS 4      /* energy only */
+
+/* Context on one device with its own stream.  Replaces the state a
+ * bblock::System keeps for the 2b/3b path (system.h:1175ff).  One context per
+ * host thread; calls on a context are serialised on its stream.  stream may be
+ * NULL (the context creates one) or a cudaStream_t to run on. */
+int mbx_create(mbx_ctx** ctx, int device, void* stream);
+int mbx_destroy(mbx_ctx* ctx);
+const char* mbx_last_error(const mbx_ctx* ctx);
+const char* mbx_version(void);
+
+/* Monomers in internal order (System::AddMonomerInfo, system.cpp:1794-1969):
+ * ids[m] ("h2o", "ch4"), first_index[m] (first site), tag[m] (tag of the
+ * monomer's first atom; n-mers are owned by the lowest tag,
+ * sys_tools.cpp:562,585), is_local[m] (NULL = all local), numsites. */
+int mbx_set_topology(mbx_ctx* ctx, int nmon, const char* const* ids, const int* first_index, const int* tag,
+                     const int* is_local, int numsites);
+
+/* cutoff2b/cutoff3b (System::Set2bCutoff/Set3bCutoff), box (9 doubles,
+ * row vectors, NULL for no periodic boundaries; System::SetPBC), and the
+ * ignored type tuples (ignore_2b_poly / ignore_3b_poly: n2 pairs in
+ * ignore2b[2*i..], n3 triples in ignore3b[3*i..]). */
+int mbx_set_config(mbx_ctx* ctx, double cutoff2b, double cutoff3b, const double* box, int n2,
+                   const char* const* ignore2b, int n3, const char* const* ignore3b);
+
+/* Get2B (nbody 2) / Get3B (nbody 3).  xyz: 3*numsites doubles, wrapped in
+ * place as System::SetPBC does (FixMonomerCoordinates, sys_tools.cpp:257).
+ * *energy receives the term; grad (3*numsites, may be NULL) and virial (9,
+ * may be NULL) are ACCUMULATED (+=) like grad_/virial_ in the reference.
+ * flags: MBX_DEVICE_PTRS, MBX_MIXED, MBX_NO_GRADS.  use_ghost as in
+ * TwoBodyEnergy(do_grads, use_ghost). */
+int mbx_energy(mbx_ctx* ctx, int nbody, double* xyz, int use_ghost, double* energy, double* grad, double* virial,
+               int flags);
+
+/* Listed n-mers of the last mbx_energy call for nbody (dimers within
+ * cutoff2b, trimers by the AddClusters rule within cutoff3b) and the number
+ * that reached an evaluator. */
+int mbx_last_counts(const mbx_ctx* ctx, int nbody, long* listed, long* evaluated);
+
+/* The n-mer list itself (System::GetPairList / AddClustersParallel,
+ * system.cpp:313, 1971): internal monomer indices, nbody per n-mer, order
+ * unspecified (canonicalise before comparing).  xyz on the host.  Writes at
+ * most cap n-mers, *count gets the total. */
+int mbx_nmers(mbx_ctx* ctx, int nbody, double cutoff, const double* xyz, int use_ghost, long* out, long cap,
+              long* count);
+
+/* Evaluator calling convention (x2b_v9x::eval(w1, w2, g1, g2, nd, virial),
+ * 2b/x2b-v9x.h:83; x3b_v2x::eval, 3b/x3b-v2x.h:85; the MB-nrg classes):
+ * n n-mers of one evaluator ("mbpol2b", "mbpol3b", "ch4h2o2b", "ch4ch42b",
+ * "ch4h2o3b"), coordinates xyz[n][nreal*3] with the monomers in evaluator
+ * order and already imaged.  grad (same layout, +=), virial (9, +=), e_per
+ * (n switched energies) may be NULL.  *energy gets the sum. */
+int mbx_evaluate(mbx_ctx* ctx, const char* evaluator, long n, const double* xyz, double* grad, double* virial,
+                 double* e_per, double* energy, int flags);
+
+/* Adjoint with respect to the linear coefficients: out[k] += sum_n w[n] *
+ * dE_n/da_k (w may be NULL for all ones), monomials recomputed from xyz. */
+int mbx_evaluate_dcoef(mbx_ctx* ctx, const char* evaluator, long n, const double* xyz, const double* w,
+                       double* out, int flags);
+
+/* Generated-polynomial calling convention (poly_2b_v6x::eval(nd, a, x, t, g),
+ * 2b/poly-2b-v6x.h:95): nd configurations, x and g variable-major
+ * (x[v*nd + i]), energies in e.  The coefficients in use are the evaluator's
+ * current ones (mbx_set_coefficients). */
+int mbx_poly(mbx_ctx* ctx, const char* evaluator, long nd, const double* x, double* g, double* e, int flags);
+
+/* Replace the linear coefficients of an evaluator (ncoef doubles; NULL
+ * restores the fitted ones).  Coefficients live in device constant memory and
+ * are shared by every context on the device. */
+int mbx_set_coefficients(mbx_ctx* ctx, const char* evaluator, const double* a, int flags);
+int mbx_evaluator_info(const char* evaluator, int* nbody, int* nreal, int* nvars, int* ncoef);
+
+/* Device-side timing of the last mbx_energy call (ms) split into n-mer build
+ * and evaluation, and the number of kernels it launched. */
+int mbx_last_timing(const mbx_ctx* ctx, double* ms_build, double* ms_eval, int* kernels);
+
+/* Measured FMA-pipe throughput of the device (results[0] FP64, results[1]
+ * FP32, TFLOP/s): the roofline denominators for the polynomial kernels. */
+int mbx_fma_peaks(int device, double* results);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,219 @@
+"""ctypes binding of the C ABI in ``include/mbx_b200.h`` (``libmbx_b200.so``).
+
+This is the Python side of the drop-in boundary: every compute call goes to
+the CUDA library.  There is no CPU fallback; loading fails loudly if the
+library has not been built or no CUDA device is present.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libmbx_b200.so")
+
+MBX_DEVICE_PTRS = 1
+MBX_MIXED = 2
+MBX_NO_GRADS = 4
+
+EVALUATORS = ("mbpol2b", "mbpol3b", "ch4h2o2b", "ch4ch42b", "ch4h2o3b")
+
+
+class MBXError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("mbx_b200 error %d: %s" % (code, msg))
+        self.code = code
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError("mbx_b200 CUDA library not built (%s); run python -m mbx_b200.build" % LIB_PATH)
+    L = ctypes.CDLL(LIB_PATH)
+    vp, dp, lp, ip = ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_long), ctypes.POINTER(ctypes.c_int)
+    cpp = ctypes.POINTER(ctypes.c_char_p)
+    L.mbx_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, vp]
+    L.mbx_destroy.argtypes = [vp]
+    L.mbx_last_error.argtypes = [vp]
+    L.mbx_last_error.restype = ctypes.c_char_p
+    L.mbx_version.restype = ctypes.c_char_p
+    L.mbx_set_topology.argtypes = [vp, ctypes.c_int, cpp, ip, ip, ip, ctypes.c_int]
+    L.mbx_set_config.argtypes = [vp, ctypes.c_double, ctypes.c_double, dp, ctypes.c_int, cpp, ctypes.c_int, cpp]
+    L.mbx_energy.argtypes = [vp, ctypes.c_int, dp, ctypes.c_int, ctypes.POINTER(ctypes.c_double), dp, dp,
+                             ctypes.c_int]
+    L.mbx_last_counts.argtypes = [vp, ctypes.c_int, lp, lp]
+    L.mbx_nmers.argtypes = [vp, ctypes.c_int, ctypes.c_double, dp, ctypes.c_int, lp, ctypes.c_long, lp]
+    L.mbx_evaluate.argtypes = [vp, ctypes.c_char_p, ctypes.c_long, dp, dp, dp, dp, ctypes.POINTER(ctypes.c_double),
+                               ctypes.c_int]
+    L.mbx_evaluate_dcoef.argtypes = [vp, ctypes.c_char_p, ctypes.c_long, dp, dp, dp, ctypes.c_int]
+    L.mbx_poly.argtypes = [vp, ctypes.c_char_p, ctypes.c_long, dp, dp, dp, ctypes.c_int]
+    L.mbx_set_coefficients.argtypes = [vp, ctypes.c_char_p, dp, ctypes.c_int]
+    L.mbx_evaluator_info.argtypes = [ctypes.c_char_p, ip, ip, ip, ip]
+    L.mbx_last_timing.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), ip]
+    L.mbx_fma_peaks.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    _lib = L
+    return L
+
+
+EXPORTED = ("mbx_create", "mbx_destroy", "mbx_last_error", "mbx_version", "mbx_set_topology", "mbx_set_config",
+            "mbx_energy", "mbx_last_counts", "mbx_nmers", "mbx_evaluate", "mbx_evaluate_dcoef", "mbx_poly",
+            "mbx_set_coefficients", "mbx_evaluator_info", "mbx_last_timing", "mbx_fma_peaks")
+
+
+def evaluator_info(name):
+    nb, nr, nv, nc = (ctypes.c_int() for _ in range(4))
+    if lib().mbx_evaluator_info(name.encode(), ctypes.byref(nb), ctypes.byref(nr), ctypes.byref(nv),
+                                ctypes.byref(nc)) != 0:
+        raise MBXError(95, "unknown evaluator %s" % name)
+    return nb.value, nr.value, nv.value, nc.value
+
+
+def fma_peaks(device=0):
+    r = (ctypes.c_double * 2)()
+    code = lib().mbx_fma_peaks(device, r)
+    if code:
+        raise MBXError(code, "fma peak benchmark failed")
+    return {"fp64_tflops": r[0], "fp32_tflops": r[1]}
+
+
+def _ptr(a):
+    """(pointer, is_device) for a numpy array or torch tensor (None -> NULL)."""
+    if a is None:
+        return None, None
+    if isinstance(a, np.ndarray):
+        if a.dtype != np.float64 or not a.flags.c_contiguous:
+            raise TypeError("arrays must be contiguous float64")
+        return a.ctypes.data, False
+    # torch tensor
+    if a.dtype.__repr__() != "torch.float64" or not a.is_contiguous():
+        raise TypeError("tensors must be contiguous float64")
+    return a.data_ptr(), a.is_cuda
+
+
+class Context:
+    """One CUDA stream and the device state of the 2b/3b path (mbx_ctx)."""
+
+    def __init__(self, device=0, stream=None):
+        L = lib()
+        h = ctypes.c_void_p()
+        code = L.mbx_create(ctypes.byref(h), device, ctypes.c_void_p(stream) if stream else None)
+        if code:
+            raise MBXError(code, "mbx_create failed (no CUDA device?)")
+        self.h = h
+        self.device = device
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().mbx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, code):
+        if code:
+            raise MBXError(code, lib().mbx_last_error(self.h).decode())
+
+    def set_topology(self, ids, first_index, tag, is_local, numsites):
+        n = len(ids)
+        arr = (ctypes.c_char_p * n)(*[s.encode() for s in ids])
+        fi = np.ascontiguousarray(first_index, np.int32)
+        tg = np.ascontiguousarray(tag, np.int32)
+        lo = None if is_local is None else np.ascontiguousarray(is_local, np.int32)
+        self._check(lib().mbx_set_topology(self.h, n, arr, fi.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                           tg.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                           None if lo is None else lo.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                           int(numsites)))
+
+    def set_config(self, cutoff2b, cutoff3b, box=None, ignore_2b=(), ignore_3b=()):
+        b = None if box is None else np.ascontiguousarray(box, np.float64).reshape(9)
+        i2 = [s.encode() for t in ignore_2b for s in t]
+        i3 = [s.encode() for t in ignore_3b for s in t]
+        a2 = (ctypes.c_char_p * max(len(i2), 1))(*i2)
+        a3 = (ctypes.c_char_p * max(len(i3), 1))(*i3)
+        self._box = b
+        self._check(lib().mbx_set_config(self.h, cutoff2b, cutoff3b, None if b is None else b.ctypes.data,
+                                         len(ignore_2b), a2, len(ignore_3b), a3))
+
+    def energy(self, nbody, xyz, grad=None, virial=None, use_ghost=False, mixed=False, grads=True):
+        """Get2B/Get3B on site coordinates xyz (numpy or CUDA tensor, wrapped in place)."""
+        px, dx = _ptr(xyz)
+        pg, dg = _ptr(grad)
+        pv, _ = _ptr(virial)
+        flags = (MBX_DEVICE_PTRS if dx else 0) | (MBX_MIXED if mixed else 0) | (0 if grads else MBX_NO_GRADS)
+        if grad is not None and bool(dg) != bool(dx):
+            raise TypeError("xyz and grad must both be host or both be device arrays")
+        if virial is not None and not isinstance(virial, np.ndarray):
+            raise TypeError("virial is a host numpy array")
+        e = ctypes.c_double()
+        self._check(lib().mbx_energy(self.h, nbody, px, int(use_ghost), ctypes.byref(e), pg, pv, flags))
+        return e.value
+
+    def counts(self, nbody):
+        a, b = ctypes.c_long(), ctypes.c_long()
+        self._check(lib().mbx_last_counts(self.h, nbody, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def timing(self):
+        a, b, k = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+        self._check(lib().mbx_last_timing(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(k)))
+        return a.value, b.value, k.value
+
+    def nmers(self, nbody, cutoff, xyz, use_ghost=False):
+        xyz = np.ascontiguousarray(xyz, np.float64)
+        cnt = ctypes.c_long()
+        self._check(lib().mbx_nmers(self.h, nbody, cutoff, xyz.ctypes.data, int(use_ghost), None, 0,
+                                    ctypes.byref(cnt)))
+        out = np.zeros(max(cnt.value, 1) * nbody, np.int64)
+        self._check(lib().mbx_nmers(self.h, nbody, cutoff, xyz.ctypes.data, int(use_ghost),
+                                    out.ctypes.data_as(ctypes.POINTER(ctypes.c_long)), cnt.value,
+                                    ctypes.byref(cnt)))
+        return out[:cnt.value * nbody].reshape(-1, nbody)
+
+    def evaluate(self, name, xyz, grad=None, virial=None, e_per=None, mixed=False, grads=True):
+        nb, nreal, nv, nc = evaluator_info(name)
+        px, dx = _ptr(xyz)
+        n = (xyz.shape[0] if xyz.ndim > 1 else xyz.size // (3 * nreal))
+        pg, _ = _ptr(grad)
+        pv, _ = _ptr(virial)
+        pe, _ = _ptr(e_per)
+        flags = (MBX_DEVICE_PTRS if dx else 0) | (MBX_MIXED if mixed else 0) | \
+                (0 if (grads and grad is not None) else MBX_NO_GRADS)
+        e = ctypes.c_double()
+        self._check(lib().mbx_evaluate(self.h, name.encode(), n, px, pg, pv, pe, ctypes.byref(e), flags))
+        return e.value
+
+    def evaluate_dcoef(self, name, xyz, w=None, out=None):
+        nb, nreal, nv, nc = evaluator_info(name)
+        px, dx = _ptr(xyz)
+        n = (xyz.shape[0] if xyz.ndim > 1 else xyz.size // (3 * nreal))
+        if out is None:
+            out = np.zeros(nc)
+        po, _ = _ptr(out)
+        pw, _ = _ptr(w)
+        self._check(lib().mbx_evaluate_dcoef(self.h, name.encode(), n, px, pw, po,
+                                             MBX_DEVICE_PTRS if dx else 0))
+        return out
+
+    def poly(self, name, x, g=None, e=None):
+        """Generated polynomial, variable-major x[nvars][nd] (poly_*::eval(nd, a, x, t, g))."""
+        nb, nreal, nv, nc = evaluator_info(name)
+        px, dx = _ptr(x)
+        nd = x.shape[-1] if x.ndim > 1 else x.size // nv
+        if e is None:
+            e = np.zeros(nd) if not dx else None
+        pg, _ = _ptr(g)
+        pe, _ = _ptr(e)
+        self._check(lib().mbx_poly(self.h, name.encode(), nd, px, pg, pe, MBX_DEVICE_PTRS if dx else 0))
+        return e
+
+    def set_coefficients(self, name, a=None):
+        pa, da = _ptr(None if a is None else a)
+        self._check(lib().mbx_set_coefficients(self.h, name.encode(), pa, MBX_DEVICE_PTRS if da else 0))

@@ -89,14 +89,16 @@ class Trie:
         return leaves, inner
 
 
-def coef_expr(coefs, conv=""):
-    """Sum of COEF(k)*c for the terms ending exactly at a node."""
+def coef_expr(coefs, fp32=False):
+    """Sum of coef[k]*c for the terms ending exactly at a node (FP32: the
+    float copy of the coefficients, coef.f(k))."""
     parts = []
     for k, c in coefs:
+        ref = ("coef.f(%d)" if fp32 else "coef[%d]") % k
         if c == 1.0:
-            parts.append("%scoef[%d]" % (conv, k))
+            parts.append(ref)
         else:
-            parts.append("%s(coef[%d] * %s)" % (conv, k, lit(c)))
+            parts.append("(%s * %s)" % (ref, lit(c) + ("f" if fp32 else "")))
     return " + ".join(parts) if parts else None
 
 
@@ -189,16 +191,19 @@ def emit_pip_mixed(trie, nvars, name, out):
         Pd = "Pd%d" % depth
         leaf_only = all(not ch["kids"] for ch in n["kids"].values())
         if pexpr_f is None:
-            w("    { const float %s = xf[%d]; const double %s = x[%d];" % (Pf, var, Pd, var))
+            w("    { const float %s = xf[%d];" % (Pf, var))
+            if not leaf_only:
+                w("      const double %s = x[%d];" % (Pd, var))
         else:
-            w("    { const float %s = %s * xf[%d]; const double %s = %s * x[%d];" %
-              (Pf, pexpr_f, var, Pd, pexpr_d, var))
+            w("    { const float %s = %s * xf[%d];" % (Pf, pexpr_f, var))
+            if not leaf_only:
+                w("      const double %s = %s * x[%d];" % (Pd, pexpr_d, var))
         if leaf_only:
             V = "Vf%d" % depth
-            ce = coef_expr(n["coef"], "(float)")
+            ce = coef_expr(n["coef"], True)
             w("      float %s = %s;" % (V, ce if ce else "0.0f"))
             for cv, ch in n["kids"].items():
-                c = coef_expr(ch["coef"], "(float)")
+                c = coef_expr(ch["coef"], True)
                 w("      %s = fmaf(%s, xf[%d], %s); gf[%d] = fmaf(%s, %s, gf[%d]);" % (V, c, cv, V, cv, c, Pf, cv))
             Vd = "(double)%s" % V
         else:
@@ -312,109 +317,226 @@ def emit_traits(spec, table, straight, out):
     w("};")
 
 
+def write_if_changed(path, text):
+    old = open(path).read() if os.path.exists(path) else None
+    if old != text:
+        with open(path, "w") as f:
+            f.write(text)
+
+
 def generate(name):
+    """Writes <name>.cuh (sizes, sites, variables, chain rule, traits) and one
+    header per polynomial variant, so that a change to one variant rebuilds
+    only the units that include it."""
     spec = SPECS[name]
     table = load_pip(name)
     trie = Trie(table)
     leaves, inner = trie.counts()
-    out = ["// Generated by mbx_b200/codegen/gen_kernels.py from mbx_b200/specs.py and",
-           "// mbx_b200/data/%s.pip -- do not edit." % name,
-           "// %d terms: %d leaves, %d inner nodes" % (table.nterms, leaves, inner),
-           "#pragma once",
-           "#define %s_NVARS %d" % (name.upper(), spec.nvars),
-           "#define %s_NCOEF %d" % (name.upper(), spec.ncoef),
-           "#define %s_NSITES %d" % (name.upper(), len(spec.sites)),
-           "#define %s_NREAL %d" % (name.upper(), spec.nreal),
-           "#define %s_NTERMS %d" % (name.upper(), table.nterms),
-           "#define %s_TRIE_LEAVES %d" % (name.upper(), leaves),
-           "#define %s_TRIE_INNER %d" % (name.upper(), inner)]
+    straight = table.nterms <= STRAIGHT_LINE_MAX_TERMS
+    head = ["// Generated by mbx_b200/codegen/gen_kernels.py from mbx_b200/specs.py and",
+            "// mbx_b200/data/%s.pip.gz -- do not edit." % name]
+    out = head + ["// %d terms: %d leaves, %d inner nodes" % (table.nterms, leaves, inner),
+                  "#pragma once",
+                  "#define %s_STRAIGHT_LINE %d" % (name.upper(), 1 if straight else 0)]
     emit_vars(spec, out)
-    if table.nterms <= STRAIGHT_LINE_MAX_TERMS:
-        out.append("#define %s_STRAIGHT_LINE 1" % name.upper())
-        emit_pip(trie, spec.nvars, name + "_pip", out)
-        emit_pip_energy(trie, spec.nvars, name + "_pip_e", out)
-        emit_pip_mixed(trie, spec.nvars, name + "_pip_mixed", out)
-        emit_dcoef(table, spec.nvars, name + "_dcoef", out)
-    else:
-        out.append("#define %s_STRAIGHT_LINE 0" % name.upper())
-    emit_traits(spec, table, table.nterms <= STRAIGHT_LINE_MAX_TERMS, out)
+    nv = spec.nvars
+    if straight:
+        out += ["template <class Coef> __device__ __forceinline__ double %s_pip(const Coef&, const double (&)[%d], "
+                "double (&)[%d]);" % (name, nv, nv),
+                "template <class Coef> __device__ __forceinline__ double %s_pip_e(const Coef&, "
+                "const double (&)[%d]);" % (name, nv),
+                "template <class Coef> __device__ __forceinline__ double %s_pip_mixed(const Coef&, const float (&)[%d],"
+                " const double (&)[%d], double (&)[%d], float (&)[%d]);" % (name, nv, nv, nv, nv),
+                "template <class Sink> __device__ __forceinline__ void %s_dcoef(const double (&)[%d], Sink&&);" %
+                (name, nv)]
+    emit_traits(spec, table, straight, out)
     os.makedirs(OUT, exist_ok=True)
-    path = os.path.join(OUT, name + ".cuh")
-    text = "\n".join(out) + "\n"
+    write_if_changed(os.path.join(OUT, name + ".cuh"), "\n".join(out) + "\n")
+    if straight:
+        for suffix, emitter, arg in (("pip", emit_pip, trie), ("pip_e", emit_pip_energy, trie),
+                                     ("pip_mixed", emit_pip_mixed, trie), ("dcoef", emit_dcoef, table)):
+            body = head + ["#pragma once", '#include "%s.cuh"' % name]
+            emitter(arg, nv, "%s_%s" % (name, suffix), body)
+            write_if_changed(os.path.join(OUT, "%s_%s.cuh" % (name, suffix)), "\n".join(body) + "\n")
+    return os.path.join(OUT, name + ".cuh"), leaves, inner
+
+
+TU_HEAD = """// Generated by mbx_b200/codegen/gen_kernels.py -- do not edit.
+// %(what)s for the %(name)s evaluator.
+#include <vector>
+#include "../holder_kernel.cuh"
+#include "%(name)s.cuh"
+%(include)s
+static __constant__ double c_%(name)s[%(ncoef)d];
+static __constant__ float cf_%(name)s[%(ncoef)d];
+struct %(name)s_CC {
+    __device__ __forceinline__ double operator[](int k) const { return c_%(name)s[k]; }
+    __device__ __forceinline__ float f(int k) const { return cf_%(name)s[k]; }
+};
+
+int mbx_set_coef_%(name)s_%(v)s(const double* a, int from_device, cudaStream_t s) {
+    cudaError_t e = cudaMemcpyToSymbolAsync(c_%(name)s, a, sizeof(double) * %(ncoef)d, 0,
+                                            from_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return (int)e;
+    // FP32 copy for the mixed-precision leaf sums (a warp-uniform FFMA operand)
+    std::vector<double> h(%(ncoef)d);
+    if (from_device) {
+        e = cudaMemcpyAsync(h.data(), a, sizeof(double) * %(ncoef)d, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return (int)e;
+    } else {
+        for (int k = 0; k < %(ncoef)d; ++k) h[k] = a[k];
+    }
+    static thread_local std::vector<float> f;
+    f.resize(%(ncoef)d);
+    for (int k = 0; k < %(ncoef)d; ++k) f[k] = (float)h[k];
+    e = cudaMemcpyToSymbolAsync(cf_%(name)s, f.data(), sizeof(float) * %(ncoef)d, 0, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    return (int)e;
+}
+"""
+
+VARIANTS = {
+    # variant: (description, body)
+    "g": ("FP64 energy + gradient kernel", """
+int mbx_launch_%(name)s_g(const HolderArgs& A, int grid, int block, cudaStream_t s) {
+    holder_kernel<%(name)s_T, %(name)s_CC, HM_GRAD_FP64, false><<<grid, block, 0, s>>>(A);
+    return (int)cudaGetLastError();
+}
+"""),
+    "e": ("FP64 energy-only kernel", """
+int mbx_launch_%(name)s_e(const HolderArgs& A, int grid, int block, cudaStream_t s) {
+    holder_kernel<%(name)s_T, %(name)s_CC, HM_ENERGY, false><<<grid, block, 0, s>>>(A);
+    return (int)cudaGetLastError();
+}
+"""),
+    "m": ("mixed-precision energy + gradient kernel", """
+int mbx_launch_%(name)s_m(const HolderArgs& A, int grid, int block, cudaStream_t s) {
+    holder_kernel<%(name)s_T, %(name)s_CC, HM_GRAD_MIXED, false><<<grid, block, 0, s>>>(A);
+    return (int)cudaGetLastError();
+}
+"""),
+    "c": ("coefficient-gradient (adjoint) kernel", """
+int mbx_launch_%(name)s_c(const HolderArgs& A, const double* w, double* out, int grid, int block, cudaStream_t s) {
+    holder_dcoef_kernel<%(name)s_T><<<grid, block, 0, s>>>(A, w, out);
+    return (int)cudaGetLastError();
+}
+"""),
+    "p": ("generated-polynomial (SoA) kernel", """
+int mbx_launch_%(name)s_p(long nd, const double* x, double* g, double* e, int grid, int block, cudaStream_t s) {
+    poly_soa_kernel<%(name)s_T, %(name)s_CC><<<grid, block, 0, s>>>(nd, x, g, e);
+    return (int)cudaGetLastError();
+}
+"""),
+    "w": ("table-driven warp kernel (energy, gradient)", """
+int mbx_launch_%(name)s_w(const HolderArgs& A, int grads, int grid, cudaStream_t s) {
+    holder_warp_kernel<%(name)s_T, 4><<<grid, 128, 0, s>>>(A, grads);
+    return (int)cudaGetLastError();
+}
+"""),
+}
+
+
+def variants_of(name):
+    return "gemcp" if load_pip(name).nterms <= STRAIGHT_LINE_MAX_TERMS else "w"
+
+
+def write_tu(path, text):
     old = open(path).read() if os.path.exists(path) else None
     if old != text:
         with open(path, "w") as f:
             f.write(text)
-    return path, leaves, inner
-
-
-KERNELS_CU = """// Generated by mbx_b200/codegen/gen_kernels.py -- do not edit.
-// Kernel instantiations and launchers for the %(name)s evaluator.
-#include "../holder_kernel.cuh"
-#include "../launch.h"
-#include "%(name)s.cuh"
-
-__constant__ double c_%(name)s[%(ncoef)d];
-struct %(name)s_CC {
-    __device__ __forceinline__ double operator[](int k) const { return c_%(name)s[k]; }
-};
-
-int mbx_set_coef_%(name)s(const double* a, int from_device, cudaStream_t s) {
-    return (int)cudaMemcpyToSymbolAsync(c_%(name)s, a, sizeof(double) * %(ncoef)d, 0,
-                                        from_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s);
-}
-
-int mbx_launch_%(name)s(const HolderArgs& A, int mode, int grid, int block, cudaStream_t s) {
-%(body)s
-    return (int)cudaGetLastError();
-}
-
-int mbx_launch_dcoef_%(name)s(const HolderArgs& A, const double* w, double* out, int grid, int block,
-                              cudaStream_t s) {
-%(dbody)s
-    return (int)cudaGetLastError();
-}
-"""
-
-STRAIGHT_BODY = """    if (A.n <= 0) return 0;
-    switch (mode) {
-        case HM_ENERGY: holder_kernel<%(name)s_T, %(name)s_CC, HM_ENERGY, false><<<grid, block, 0, s>>>(A); break;
-        case HM_GRAD_FP64: holder_kernel<%(name)s_T, %(name)s_CC, HM_GRAD_FP64, false><<<grid, block, 0, s>>>(A); break;
-        case HM_GRAD_MIXED: holder_kernel<%(name)s_T, %(name)s_CC, HM_GRAD_MIXED, false><<<grid, block, 0, s>>>(A); break;
-        default: return (int)cudaErrorInvalidValue;
-    }"""
-
-WARP_BODY = """    if (A.n <= 0) return 0;
-    if (mode != HM_ENERGY && mode != HM_GRAD_FP64 && mode != HM_GRAD_MIXED) return (int)cudaErrorInvalidValue;
-    holder_warp_kernel<%(name)s_T, 4><<<grid, 128, 0, s>>>(A, mode != HM_ENERGY);"""
-
-STRAIGHT_DBODY = """    if (A.n <= 0) return 0;
-    holder_dcoef_kernel<%(name)s_T><<<grid, block, 0, s>>>(A, w, out);"""
-
-WARP_DBODY = """    (void)A; (void)w; (void)out; (void)grid; (void)block; (void)s;
-    return (int)cudaErrorNotSupported;"""
 
 
 def write_kernels_cu(name):
     spec = SPECS[name]
-    table = load_pip(name)
-    straight = table.nterms <= STRAIGHT_LINE_MAX_TERMS
-    d = {"name": name, "ncoef": spec.ncoef}
-    d["body"] = (STRAIGHT_BODY if straight else WARP_BODY) % d
-    d["dbody"] = (STRAIGHT_DBODY if straight else WARP_DBODY) % d
-    text = KERNELS_CU % d
-    path = os.path.join(OUT, name + "_kernels.cu")
-    old = open(path).read() if os.path.exists(path) else None
-    if old != text:
-        with open(path, "w") as f:
-            f.write(text)
-    return path
+    paths = []
+    inc = {"g": "pip", "e": "pip_e", "m": "pip_mixed", "c": "dcoef", "p": "pip", "w": None}
+    for v in variants_of(name):
+        what, body = VARIANTS[v]
+        d = {"name": name, "ncoef": spec.ncoef, "v": v, "what": what,
+             "include": ('#include "%s_%s.cuh"\n' % (name, inc[v])) if inc[v] else ""}
+        path = os.path.join(OUT, "%s_%s.cu" % (name, v))
+        write_tu(path, (TU_HEAD + body) % d)
+        paths.append(path)
+    return paths
+
+
+def write_registry():
+    """Host tables: evaluator descriptions, default coefficients, term tables."""
+    from mbx_b200.tables import load_fit
+    lines = ["// Generated by mbx_b200/codegen/gen_kernels.py -- do not edit.", "#pragma once",
+             '#include "../holder_kernel.cuh"', ""]
+    for name in SPECS:
+        vs = variants_of(name)
+        for v in "gemcpw":
+            if v not in vs:
+                continue
+            if v in "gem":
+                lines.append("int mbx_launch_%s_%s(const HolderArgs& A, int grid, int block, cudaStream_t s);" %
+                             (name, v))
+            elif v == "c":
+                lines.append("int mbx_launch_%s_c(const HolderArgs& A, const double* w, double* out, int grid, "
+                             "int block, cudaStream_t s);" % name)
+            elif v == "p":
+                lines.append("int mbx_launch_%s_p(long nd, const double* x, double* g, double* e, int grid, "
+                             "int block, cudaStream_t s);" % name)
+            else:
+                lines.append("int mbx_launch_%s_w(const HolderArgs& A, int grads, int grid, cudaStream_t s);" % name)
+            lines.append("int mbx_set_coef_%s_%s(const double* a, int from_device, cudaStream_t s);" % (name, v))
+        fit = load_fit(name)
+        lines.append("static const double mbx_fit_%s[%d] = {" % (name, len(fit)))
+        for i in range(0, len(fit), 4):
+            lines.append("    " + ", ".join(repr(float(x)) for x in fit[i:i + 4]) + ",")
+        lines.append("};")
+    lines.append("")
+    lines.append("static const EvaluatorInfo mbx_evaluators[] = {")
+    for name, spec in SPECS.items():
+        vs = variants_of(name)
+        ids = list(spec.monomers) + ["", ""][:3 - len(spec.monomers)]
+        skip = {"pair_gt": 0, "two_of_three_gt": 1, "all_three_gt": 2}[spec.skip]
+
+        def fn(v, kind):
+            return ("mbx_%s_%s_%s" % (kind, name, v)) if v in vs else "nullptr"
+        lines.append('    {"%s", %d, {"%s", "%s", "%s"}, %s, %d, %d, %d, %d, mbx_fit_%s, %s, %s, %s, %s, %s, %s,' %
+                     (name, spec.nbody, ids[0], ids[1], ids[2], lit(spec.rf), skip, spec.ncoef, spec.nreal,
+                      spec.nvars, name, fn("g", "launch"), fn("e", "launch"), fn("m", "launch"), fn("c", "launch"),
+                      fn("p", "launch"), fn("w", "launch")))
+        lines.append("     {%s}}," % ", ".join(fn(v, "set_coef") for v in "gemcpw"))
+    lines.append("};")
+    lines.append("static const int mbx_num_evaluators = %d;" % len(SPECS))
+    write_tu(os.path.join(OUT, "registry.inc"), "\n".join(lines) + "\n")
+
+
+def write_term_tables():
+    """Packed term tables for the warp kernel (types without straight-line code)."""
+    lines = ["// Generated by mbx_b200/codegen/gen_kernels.py -- do not edit.", "#pragma once", ""]
+    for name in SPECS:
+        if "w" not in variants_of(name):
+            continue
+        t = load_pip(name)
+        lines.append("static const int mbx_terms_%s[%d][4] = {" % (name, t.nterms))
+        for q in range(t.nterms):
+            packed = 0
+            for i in range(4):
+                v = int(t.var[q, i]) if i < t.deg[q] else 255
+                packed |= (v & 255) << (8 * i)
+            if packed >= 1 << 31:
+                packed -= 1 << 32
+            lines.append("{%d,%d,%d,0}," % (t.k[q], packed, t.deg[q]))
+        lines.append("};")
+        lines.append("static const double mbx_tcoef_%s[%d] = {%s};" %
+                     (name, t.nterms, ",".join(repr(float(c)) for c in t.coef)))
+    write_tu(os.path.join(OUT, "terms.inc"), "\n".join(lines) + "\n")
 
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("names", nargs="*", default=list(SPECS))
     args = ap.parse_args(argv)
+    os.makedirs(OUT, exist_ok=True)
+    write_registry()
+    write_term_tables()
     for n in args.names:
         path, leaves, inner = generate(n)
         write_kernels_cu(n)

@@ -23,7 +23,9 @@
 enum { HM_ENERGY = 0, HM_GRAD_FP64 = 1, HM_GRAD_MIXED = 2, HM_ENERGY_MIXED = 3 };
 
 struct HolderArgs {
-    long n;                    // number of n-mers
+    long n;                    // number of n-mers (capacity when n_dev is set)
+    const int* n_dev;          // optional device-side count (read by the kernel, clamped to n)
+    const int* status;         // optional: a nonzero word means the n-mer build failed; do nothing
     const int4* nmers;         // system input: (m0, m1, m2, anchor slot), holder order
     const double* xyz;         // system input: site array (3 per site); AoS input: [n][NREAL*3]
     const int* first_index;    // system input: first site of every monomer
@@ -43,6 +45,7 @@ struct HolderArgs {
 struct GlobalCoef {
     const double* __restrict__ p;
     __device__ __forceinline__ double operator[](int k) const { return __ldg(p + k); }
+    __device__ __forceinline__ float f(int k) const { return (float)__ldg(p + k); }
 };
 
 __device__ __forceinline__ double ld_volatile(const double* p) {
@@ -220,11 +223,22 @@ __device__ __forceinline__ void finish_nmer(const HolderArgs& A, long t, double 
 }
 
 // One n-mer per thread, straight-line polynomial.
+__device__ __forceinline__ long nmer_count(const HolderArgs& A) {
+    if (A.status && *A.status) return 0;
+    if (!A.n_dev) return A.n;
+    const long c = *A.n_dev;
+    return c < A.n ? c : A.n;
+}
+
+#ifndef MBX_HOLDER_MINB
+#define MBX_HOLDER_MINB 1
+#endif
 template <class T, class CC, int MODE, bool CUSTOM>
-__global__ void __launch_bounds__(128) holder_kernel(const HolderArgs A) {
+__global__ void __launch_bounds__(128, MBX_HOLDER_MINB) holder_kernel(const HolderArgs A) {
     double acc[7] = {0, 0, 0, 0, 0, 0, 0};
     const bool grads = (MODE == HM_GRAD_FP64 || MODE == HM_GRAD_MIXED);
-    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < A.n; t += (long)gridDim.x * blockDim.x) {
+    const long n = nmer_count(A);
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
         double ep;
         double g[T::NVARS];
         {
@@ -244,8 +258,8 @@ __global__ void __launch_bounds__(128) holder_kernel(const HolderArgs A) {
             if constexpr (T::STRAIGHT) {
                 if constexpr (CUSTOM) {
                     const GlobalCoef coef{A.coef};
-                    if (MODE == HM_ENERGY) ep = T::pip_e(coef, x);
-                    else if (MODE == HM_GRAD_FP64) ep = T::pip(coef, x, g);
+                    if constexpr (MODE == HM_ENERGY) ep = T::pip_e(coef, x);
+                    else if constexpr (MODE == HM_GRAD_FP64) ep = T::pip(coef, x, g);
                     else {
                         float xf[T::NVARS], gf[T::NVARS];
 #pragma unroll
@@ -256,8 +270,8 @@ __global__ void __launch_bounds__(128) holder_kernel(const HolderArgs A) {
                     }
                 } else {
                     const CC coef{};
-                    if (MODE == HM_ENERGY) ep = T::pip_e(coef, x);
-                    else if (MODE == HM_GRAD_FP64) ep = T::pip(coef, x, g);
+                    if constexpr (MODE == HM_ENERGY) ep = T::pip_e(coef, x);
+                    else if constexpr (MODE == HM_GRAD_FP64) ep = T::pip(coef, x, g);
                     else {
                         float xf[T::NVARS], gf[T::NVARS];
 #pragma unroll
@@ -286,7 +300,8 @@ __global__ void __launch_bounds__(WARPS * 32) holder_warp_kernel(const HolderArg
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     double acc[7] = {0, 0, 0, 0, 0, 0, 0};
     const long stride = (long)gridDim.x * WARPS;
-    for (long t = blockIdx.x * (long)WARPS + w; t < A.n; t += stride) {
+    const long n = nmer_count(A);
+    for (long t = blockIdx.x * (long)WARPS + w; t < n; t += stride) {
         double r[T::NREAL][3];
         load_nmer<T, false>(A, t, r);
         double d[3][3], rr[3];
@@ -346,7 +361,7 @@ __global__ void __launch_bounds__(128) holder_dcoef_kernel(const HolderArgs A, c
     __shared__ double part[T::NCOEF];
     for (int k = threadIdx.x; k < T::NCOEF; k += blockDim.x) part[k] = 0.0;
     __syncthreads();
-    const long nt = A.n;
+    const long nt = nmer_count(A);
     for (long base = blockIdx.x * (long)blockDim.x; base < nt; base += (long)gridDim.x * blockDim.x) {
         const long t = base + threadIdx.x;
         double scale = 0.0;
@@ -378,4 +393,26 @@ __global__ void __launch_bounds__(128) holder_dcoef_kernel(const HolderArgs A, c
     __syncthreads();
     for (int k = threadIdx.x; k < T::NCOEF; k += blockDim.x)
         if (part[k] != 0.0) atomicAdd(out + k, part[k]);
+}
+
+// The generated-polynomial calling convention of the reference
+// (poly_2b_v6x::eval(nd, a, x, t, g), potential/2b/poly-2b-v6x.h:95): nd
+// configurations, variables and gradients stored variable-major
+// (x[v * nd + i]); energies to e[i].  One configuration per thread, so every
+// load and store is coalesced.
+template <class T, class CC>
+__global__ void __launch_bounds__(128) poly_soa_kernel(long nd, const double* __restrict__ x_soa,
+                                                       double* __restrict__ g_soa, double* __restrict__ e) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < nd; i += (long)gridDim.x * blockDim.x) {
+        double x[T::NVARS], g[T::NVARS];
+#pragma unroll
+        for (int v = 0; v < T::NVARS; ++v) { x[v] = __ldg(x_soa + v * nd + i); g[v] = 0.0; }
+        const CC coef{};
+        const double ev = T::pip(coef, x, g);
+        e[i] = ev;
+        if (g_soa) {
+#pragma unroll
+            for (int v = 0; v < T::NVARS; ++v) g_soa[v * nd + i] = g[v];
+        }
+    }
 }

@@ -1,0 +1,943 @@
+// Host runtime and C ABI of mbx_b200 (declared in include/mbx_b200.h).
+//
+// A context owns one CUDA stream and the device state the reference keeps in
+// bblock::System for the 2-body/3-body path: the topology (first_index_,
+// atom tags, local flags, monomer types), the configuration (cutoff2b_,
+// cutoff3b_, box_, box_inverse_, ignore_2b_poly_, ignore_3b_poly_) and the
+// work buffers.  mbx_energy() is System::Get2B/Get3B: FixMonomerCoordinates,
+// the n-mer enumeration, the type dispatch of e2b::get_2b_energy /
+// e3b::get_3b_energy and the evaluators, with energy, gradients and virial
+// accumulated like grad_ and virial_.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/mbx_b200.h"
+#include "holder_kernel.cuh"
+#include "nmer_build.h"
+
+typedef int (*launch_fn)(const HolderArgs&, int, int, cudaStream_t);
+typedef int (*dcoef_fn)(const HolderArgs&, const double*, double*, int, int, cudaStream_t);
+typedef int (*poly_fn)(long, const double*, double*, double*, int, int, cudaStream_t);
+typedef int (*warp_fn)(const HolderArgs&, int, int, cudaStream_t);
+typedef int (*setcoef_fn)(const double*, int, cudaStream_t);
+
+struct EvaluatorInfo {
+    const char* name;
+    int nbody;
+    const char* ids[3];
+    double rf;
+    int skip;
+    int ncoef, nreal, nvars;
+    const double* fit;
+    launch_fn g, e, m;
+    dcoef_fn c;
+    poly_fn p;
+    warp_fn w;
+    setcoef_fn set[6];
+};
+
+#include "gen/registry.inc"
+#include "gen/terms.inc"
+
+#define MBX_VERSION_STRING "mbx_b200 0.1 (sm_100a)"
+
+namespace {
+
+template <class T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    cudaError_t ensure(size_t want) {
+        if (want <= n && p) return cudaSuccess;
+        size_t m = std::max(want, n + n / 2);
+        if (m == 0) m = 1;
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+        cudaError_t e = cudaMalloc(&p, m * sizeof(T));
+        if (e == cudaSuccess) n = m;
+        return e;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+};
+
+const EvaluatorInfo* find_evaluator(const char* name) {
+    for (int i = 0; i < mbx_num_evaluators; ++i)
+        if (!strcmp(mbx_evaluators[i].name, name)) return &mbx_evaluators[i];
+    return nullptr;
+}
+
+// Slot order the reference's dispatch sorts the monomer ids into
+// (e2b::get_2b_energy, potential/2b/energy2b.cpp:240-254;
+//  e3b::get_3b_energy, potential/3b/energy3b.cpp:185-216).
+void sorted_slots(int nb, const std::string* ids, int* idx) {
+    if (nb == 2) {
+        if (ids[1] < ids[0]) { idx[0] = 1; idx[1] = 0; } else { idx[0] = 0; idx[1] = 1; }
+        return;
+    }
+    std::string m[3] = {ids[0], ids[1], ids[2]};
+    int k[3] = {0, 1, 2};
+    if (m[2] < m[0] && m[2] < m[1]) { std::swap(m[0], m[2]); std::swap(k[0], k[2]); }
+    if (m[0] > m[1] && m[0] > m[2]) {
+        std::swap(m[0], m[2]); std::swap(k[0], k[2]);
+    } else if (m[1] > m[0] && m[1] > m[2]) {
+        std::swap(m[1], m[2]); std::swap(k[1], k[2]);
+    }
+    if (m[0] > m[1]) { std::swap(m[0], m[1]); std::swap(k[0], k[1]); }
+    for (int i = 0; i < 3; ++i) idx[i] = k[i];
+}
+
+}  // namespace
+
+struct mbx_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int sm_count = 148;
+    std::string err;
+
+    // topology
+    int nmon = 0, numsites = 0, ntypes = 0;
+    std::string type_names[MBX_MAX_TYPES];
+    std::vector<int> h_first, h_nat, h_tag, h_type, h_local;
+    DevBuf<int> d_first, d_nat, d_tag, d_type;
+    DevBuf<int> d_members[2], d_query[2];
+    int nmem[2] = {0, 0}, nquery[2] = {0, 0};
+
+    // configuration
+    double cutoff[4] = {0, 0, 9.0, 7.0};  // indexed by nbody
+    BoxParams bp{};
+    std::vector<std::vector<std::string>> ignore[4];
+
+    // per-term dispatch
+    int nbucket[4] = {0, 0, 0, 0};
+    const EvaluatorInfo* bucket_eval[4][MBX_MAX_BUCKETS];
+    DimerRules drules{};
+    TrimerRules trules{};
+    long bucket_cap[4][MBX_MAX_BUCKETS];
+
+    // work buffers
+    DevBuf<double> xyz, grad, out, cloud, coef_ws;
+    DevBuf<int> cell_of, cell_count, cell_start, cell_fill, cell_items, nb_count, bucket_count, status;
+    DevBuf<NbEntry> nb;
+    DevBuf<int4> buckets, list;
+    DevBuf<unsigned long long> listed;
+    DevBuf<int4> terms;
+    DevBuf<double> tcoef, warp_coef;
+    int nb_cap = 192;
+    double* h_out = nullptr;  // pinned: [0..7] term outputs, [8..15] counters
+    cudaEvent_t ev[3];
+
+    // results of the last call
+    long last_listed[4] = {0, 0, 0, 0};
+    long last_evaluated[4] = {0, 0, 0, 0};
+    float last_ms_build = 0, last_ms_eval = 0;
+    int last_kernels = 0;
+};
+
+static int fail(mbx_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+#define CUCHK(c, expr)                                                                        \
+    do {                                                                                      \
+        cudaError_t _e = (expr);                                                              \
+        if (_e != cudaSuccess)                                                                \
+            return fail(c, MBX_ECUDA, std::string(#expr) + ": " + cudaGetErrorString(_e));    \
+    } while (0)
+
+#define RCHK(c, expr)                                                                         \
+    do {                                                                                      \
+        int _r = (expr);                                                                      \
+        if (_r != 0)                                                                          \
+            return fail(c, MBX_ECUDA, std::string(#expr) + ": " + cudaGetErrorString((cudaError_t)_r)); \
+    } while (0)
+
+extern "C" {
+
+const char* mbx_version(void) { return MBX_VERSION_STRING; }
+
+const char* mbx_last_error(const mbx_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+int mbx_create(mbx_ctx** out, int device, void* stream) {
+    if (!out) return MBX_EINVAL;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return MBX_ENODEV;
+    if (device < 0 || device >= ndev) return MBX_EINVAL;
+    mbx_ctx* c = new mbx_ctx();
+    c->device = device;
+    CUCHK(c, cudaSetDevice(device));
+    CUCHK(c, cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device));
+    if (stream) {
+        c->stream = (cudaStream_t)stream;
+    } else {
+        CUCHK(c, cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        c->own_stream = true;
+    }
+    CUCHK(c, cudaMallocHost(&c->h_out, 64 * sizeof(double)));
+    for (int i = 0; i < 3; ++i) CUCHK(c, cudaEventCreate(&c->ev[i]));
+    CUCHK(c, c->out.ensure(64));
+    CUCHK(c, c->status.ensure(4));
+    CUCHK(c, c->listed.ensure(4));
+    for (int nb = 0; nb < 4; ++nb)
+        for (int b = 0; b < MBX_MAX_BUCKETS; ++b) c->bucket_cap[nb][b] = 0;
+    // fitted coefficients into every kernel variant (constant memory, per device)
+    for (int i = 0; i < mbx_num_evaluators; ++i) {
+        const EvaluatorInfo& E = mbx_evaluators[i];
+        for (int v = 0; v < 6; ++v)
+            if (E.set[v]) RCHK(c, E.set[v](E.fit, 0, c->stream));
+    }
+    // the table-driven evaluator reads its terms and coefficients from global memory
+    {
+        const EvaluatorInfo* E = find_evaluator("ch4ch42b");
+        const long nt = sizeof(mbx_tcoef_ch4ch42b) / sizeof(double);
+        CUCHK(c, c->terms.ensure(nt));
+        CUCHK(c, c->tcoef.ensure(nt));
+        CUCHK(c, c->warp_coef.ensure(E->ncoef));
+        CUCHK(c, cudaMemcpyAsync(c->terms.p, mbx_terms_ch4ch42b, nt * sizeof(int4), cudaMemcpyHostToDevice, c->stream));
+        CUCHK(c, cudaMemcpyAsync(c->tcoef.p, mbx_tcoef_ch4ch42b, nt * sizeof(double), cudaMemcpyHostToDevice,
+                                 c->stream));
+        CUCHK(c, cudaMemcpyAsync(c->warp_coef.p, E->fit, E->ncoef * sizeof(double), cudaMemcpyHostToDevice,
+                                 c->stream));
+    }
+    CUCHK(c, cudaStreamSynchronize(c->stream));
+    *out = c;
+    return MBX_OK;
+}
+
+int mbx_destroy(mbx_ctx* c) {
+    if (!c) return MBX_OK;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    DevBuf<int>* ib[] = {&c->d_first, &c->d_nat, &c->d_tag, &c->d_type, &c->d_members[0], &c->d_members[1],
+                         &c->d_query[0], &c->d_query[1], &c->cell_of, &c->cell_count, &c->cell_start,
+                         &c->cell_fill, &c->cell_items, &c->nb_count, &c->bucket_count, &c->status};
+    for (auto* b : ib) b->release();
+    DevBuf<double>* db[] = {&c->xyz, &c->grad, &c->out, &c->cloud, &c->coef_ws, &c->tcoef, &c->warp_coef};
+    for (auto* b : db) b->release();
+    c->nb.release();
+    c->buckets.release();
+    c->list.release();
+    c->listed.release();
+    c->terms.release();
+    if (c->h_out) cudaFreeHost(c->h_out);
+    for (int i = 0; i < 3; ++i) cudaEventDestroy(c->ev[i]);
+    if (c->own_stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return MBX_OK;
+}
+
+int mbx_evaluator_info(const char* name, int* nbody, int* nreal, int* nvars, int* ncoef) {
+    const EvaluatorInfo* E = name ? find_evaluator(name) : nullptr;
+    if (!E) return MBX_ENOTSUP;
+    if (nbody) *nbody = E->nbody;
+    if (nreal) *nreal = E->nreal;
+    if (nvars) *nvars = E->nvars;
+    if (ncoef) *ncoef = E->ncoef;
+    return MBX_OK;
+}
+
+}  // extern "C"
+
+// Dispatch tables for the current topology and ignore lists.
+static int build_rules(mbx_ctx* c) {
+    for (int nb = 2; nb <= 3; ++nb) {
+        c->nbucket[nb] = 0;
+        const int T = c->ntypes;
+        const int ncode = nb == 2 ? T * T : T * T * T;
+        for (int code = 0; code < (nb == 2 ? MBX_MAX_TYPES * MBX_MAX_TYPES : MBX_MAX_TYPES * MBX_MAX_TYPES * MBX_MAX_TYPES);
+             ++code) {
+            if (nb == 2) { c->drules.bucket[code] = -1; c->drules.swap[code] = 0; }
+            else { c->trules.bucket[code] = -1; c->trules.perm[code] = 0; }
+        }
+        for (int code = 0; code < ncode; ++code) {
+            std::string ids[3];
+            // code enumerates (slot0 slowest): reconstruct the original order
+            if (nb == 2) { ids[0] = c->type_names[code / T]; ids[1] = c->type_names[code % T]; }
+            else {
+                ids[0] = c->type_names[code / (T * T)];
+                ids[1] = c->type_names[(code / T) % T];
+                ids[2] = c->type_names[code % T];
+            }
+            int so[3];
+            sorted_slots(nb, ids, so);
+            std::vector<std::string> sorted_ids;
+            for (int s = 0; s < nb; ++s) sorted_ids.push_back(ids[so[s]]);
+            // ignored tuples are skipped after the search (system.cpp:2606-2618,2940-2952)
+            bool ignored = false;
+            for (auto& ig : c->ignore[nb]) {
+                std::vector<std::string> a = ig, b = sorted_ids;
+                std::sort(a.begin(), a.end());
+                std::sort(b.begin(), b.end());
+                if (a == b) ignored = true;
+            }
+            const EvaluatorInfo* E = nullptr;
+            for (int i = 0; i < mbx_num_evaluators && !ignored; ++i) {
+                const EvaluatorInfo& X = mbx_evaluators[i];
+                if (X.nbody != nb) continue;
+                std::vector<std::string> a(X.ids, X.ids + nb), b = sorted_ids;
+                std::sort(a.begin(), a.end());
+                if (a == b) E = &X;
+            }
+            if (!E) continue;  // unknown tuples evaluate to 0 (energy2b.cpp:370, energy3b.cpp:258)
+            // evaluator slot h <- sorted slot: first unused sorted slot with the same id
+            int holder_from_orig[3];
+            bool used[3] = {false, false, false};
+            for (int h = 0; h < nb; ++h) {
+                for (int s = 0; s < nb; ++s) {
+                    if (!used[s] && sorted_ids[s] == E->ids[h]) {
+                        used[s] = true;
+                        holder_from_orig[h] = so[s];
+                        break;
+                    }
+                }
+            }
+            int b = -1;
+            for (int k = 0; k < c->nbucket[nb]; ++k)
+                if (c->bucket_eval[nb][k] == E) b = k;
+            if (b < 0) {
+                if (c->nbucket[nb] == MBX_MAX_BUCKETS) return fail(c, MBX_ENOTSUP, "too many evaluator buckets");
+                b = c->nbucket[nb]++;
+                c->bucket_eval[nb][b] = E;
+            }
+            const int dcode = nb == 2 ? (code / T) * MBX_MAX_TYPES + code % T
+                                      : ((code / (T * T)) * MBX_MAX_TYPES + (code / T) % T) * MBX_MAX_TYPES + code % T;
+            if (nb == 2) {
+                c->drules.bucket[dcode] = b;
+                c->drules.swap[dcode] = holder_from_orig[0] == 1;
+            } else {
+                c->trules.bucket[dcode] = b;
+                c->trules.perm[dcode] = holder_from_orig[0] | (holder_from_orig[1] << 2) | (holder_from_orig[2] << 4);
+            }
+        }
+        for (int b = 0; b < c->nbucket[nb]; ++b) {
+            const EvaluatorInfo* E = c->bucket_eval[nb][b];
+            const double pre = E->rf + 1e-6;
+            if (nb == 2) c->drules.pre2[b] = pre * pre;
+            else {
+                c->trules.pre2[b] = pre * pre;
+                c->trules.skip[b] = E->skip;
+            }
+        }
+    }
+    return MBX_OK;
+}
+
+extern "C" int mbx_set_topology(mbx_ctx* c, int nmon, const char* const* ids, const int* first_index, const int* tag,
+                                const int* is_local, int numsites) {
+    if (!c || nmon <= 0 || !ids || !first_index || !tag || numsites <= 0) return fail(c, MBX_EINVAL, "bad topology");
+    CUCHK(c, cudaSetDevice(c->device));
+    c->nmon = nmon;
+    c->numsites = numsites;
+    c->ntypes = 0;
+    c->h_first.assign(first_index, first_index + nmon);
+    c->h_tag.assign(tag, tag + nmon);
+    c->h_local.assign(nmon, 1);
+    if (is_local) c->h_local.assign(is_local, is_local + nmon);
+    c->h_type.resize(nmon);
+    c->h_nat.resize(nmon);
+    for (int m = 0; m < nmon; ++m) {
+        std::string id = ids[m];
+        int nat;
+        if (id == "h2o") nat = 3;
+        else if (id == "ch4") nat = 5;
+        else return fail(c, MBX_ENOTSUP, "unknown monomer id " + id);
+        c->h_nat[m] = nat;
+        int t = -1;
+        for (int k = 0; k < c->ntypes; ++k)
+            if (c->type_names[k] == id) t = k;
+        if (t < 0) {
+            if (c->ntypes == MBX_MAX_TYPES) return fail(c, MBX_ENOTSUP, "too many monomer types");
+            t = c->ntypes;
+            c->type_names[c->ntypes++] = id;
+        }
+        c->h_type[m] = t;
+        if (first_index[m] < 0 || first_index[m] + nat > numsites) return fail(c, MBX_EINVAL, "first_index out of range");
+    }
+    CUCHK(c, c->d_first.ensure(nmon));
+    CUCHK(c, c->d_nat.ensure(nmon));
+    CUCHK(c, c->d_tag.ensure(nmon));
+    CUCHK(c, c->d_type.ensure(nmon));
+    CUCHK(c, cudaMemcpyAsync(c->d_first.p, c->h_first.data(), nmon * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    CUCHK(c, cudaMemcpyAsync(c->d_nat.p, c->h_nat.data(), nmon * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    CUCHK(c, cudaMemcpyAsync(c->d_tag.p, c->h_tag.data(), nmon * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    CUCHK(c, cudaMemcpyAsync(c->d_type.p, c->h_type.data(), nmon * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    // search members and queries (AddClusters, sys_tools.cpp:502-517,535-537):
+    // use_ghost = 0: members and queries are the local monomers;
+    // use_ghost = 1: all monomers are members, the local ones query.
+    for (int g = 0; g < 2; ++g) {
+        std::vector<int> mem, qry;
+        for (int m = 0; m < nmon; ++m)
+            if (g || c->h_local[m]) mem.push_back(m);
+        for (int q = 0; q < (int)mem.size(); ++q)
+            if (c->h_local[mem[q]]) qry.push_back(q);
+        c->nmem[g] = (int)mem.size();
+        c->nquery[g] = (int)qry.size();
+        CUCHK(c, c->d_members[g].ensure(mem.size() + 1));
+        CUCHK(c, c->d_query[g].ensure(qry.size() + 1));
+        if (!mem.empty())
+            CUCHK(c, cudaMemcpyAsync(c->d_members[g].p, mem.data(), mem.size() * sizeof(int), cudaMemcpyHostToDevice,
+                                     c->stream));
+        if (!qry.empty())
+            CUCHK(c, cudaMemcpyAsync(c->d_query[g].p, qry.data(), qry.size() * sizeof(int), cudaMemcpyHostToDevice,
+                                     c->stream));
+    }
+    CUCHK(c, cudaStreamSynchronize(c->stream));
+    for (int nb = 0; nb < 4; ++nb)
+        for (int b = 0; b < MBX_MAX_BUCKETS; ++b) c->bucket_cap[nb][b] = 0;
+    return build_rules(c);
+}
+
+static int invert_box(const double* b, double* inv) {
+    // InvertUnitCell (tools/math_tools.cpp:37-64), same operation order
+    volatile double det = b[0] * (b[4] * b[8] - b[7] * b[5]) - b[1] * (b[3] * b[8] - b[5] * b[6]) +
+                          b[2] * (b[3] * b[7] - b[4] * b[6]);
+    if (std::fabs(det) < 1e-36) return 1;
+    const double di = 1 / det;
+    inv[0] = (b[4] * b[8] - b[7] * b[5]) * di;
+    inv[1] = (b[2] * b[7] - b[1] * b[8]) * di;
+    inv[2] = (b[1] * b[5] - b[2] * b[4]) * di;
+    inv[3] = (b[5] * b[6] - b[3] * b[8]) * di;
+    inv[4] = (b[0] * b[8] - b[2] * b[6]) * di;
+    inv[5] = (b[3] * b[2] - b[0] * b[5]) * di;
+    inv[6] = (b[3] * b[7] - b[6] * b[4]) * di;
+    inv[7] = (b[6] * b[1] - b[0] * b[7]) * di;
+    inv[8] = (b[0] * b[4] - b[3] * b[1]) * di;
+    return 0;
+}
+
+extern "C" int mbx_set_config(mbx_ctx* c, double cutoff2b, double cutoff3b, const double* box, int n2,
+                              const char* const* ignore2b, int n3, const char* const* ignore3b) {
+    if (!c || !(cutoff2b >= 0) || !(cutoff3b >= 0)) return fail(c, MBX_EINVAL, "bad cutoffs");
+    c->cutoff[2] = cutoff2b;
+    c->cutoff[3] = cutoff3b;
+    c->bp.use_pbc = box ? 1 : 0;
+    if (box) {
+        for (int i = 0; i < 9; ++i) c->bp.box[i] = box[i];
+        if (invert_box(box, c->bp.inv)) return fail(c, MBX_EINVAL, "Matrix has no inverse. Determinant is 0");
+        // the search finds at most one image of each monomer only while the
+        // cutoff is below half of every box height (sys_tools.cpp:553-555)
+        const double* a = box;
+        const double* bb = box + 3;
+        const double* cc = box + 6;
+        auto cross = [](const double* u, const double* v, double* w) {
+            w[0] = u[1] * v[2] - u[2] * v[1];
+            w[1] = u[2] * v[0] - u[0] * v[2];
+            w[2] = u[0] * v[1] - u[1] * v[0];
+        };
+        double bc[3], ca[3], ab[3];
+        cross(bb, cc, bc);
+        cross(cc, a, ca);
+        cross(a, bb, ab);
+        const double vol = std::fabs(a[0] * bc[0] + a[1] * bc[1] + a[2] * bc[2]);
+        const double h[3] = {vol / std::sqrt(bc[0] * bc[0] + bc[1] * bc[1] + bc[2] * bc[2]),
+                             vol / std::sqrt(ca[0] * ca[0] + ca[1] * ca[1] + ca[2] * ca[2]),
+                             vol / std::sqrt(ab[0] * ab[0] + ab[1] * ab[1] + ab[2] * ab[2])};
+        const double rc = std::max(cutoff2b, cutoff3b);
+        for (int k = 0; k < 3; ++k)
+            if (2.0 * rc >= h[k])
+                return fail(c, MBX_EDOM, "cutoff " + std::to_string(rc) + " is not below half the box height " +
+                                             std::to_string(h[k]));
+    }
+    c->ignore[2].clear();
+    c->ignore[3].clear();
+    for (int i = 0; i < n2; ++i) c->ignore[2].push_back({ignore2b[2 * i], ignore2b[2 * i + 1]});
+    for (int i = 0; i < n3; ++i) c->ignore[3].push_back({ignore3b[3 * i], ignore3b[3 * i + 1], ignore3b[3 * i + 2]});
+    if (c->nmon) return build_rules(c);
+    return MBX_OK;
+}
+
+// Cell grid for a search of radius rc.
+static CellGrid make_grid(const mbx_ctx* c, double rc, int nmem) {
+    CellGrid g{};
+    if (c->bp.use_pbc) {
+        const double* a = c->bp.box;
+        const double* b = c->bp.box + 3;
+        const double* cc = c->bp.box + 6;
+        auto cross = [](const double* u, const double* v, double* w) {
+            w[0] = u[1] * v[2] - u[2] * v[1];
+            w[1] = u[2] * v[0] - u[0] * v[2];
+            w[2] = u[0] * v[1] - u[1] * v[0];
+        };
+        double bc[3], ca[3], ab[3];
+        cross(b, cc, bc);
+        cross(cc, a, ca);
+        cross(a, b, ab);
+        const double vol = std::fabs(a[0] * bc[0] + a[1] * bc[1] + a[2] * bc[2]);
+        const double h[3] = {vol / std::sqrt(bc[0] * bc[0] + bc[1] * bc[1] + bc[2] * bc[2]),
+                             vol / std::sqrt(ca[0] * ca[0] + ca[1] * ca[1] + ca[2] * ca[2]),
+                             vol / std::sqrt(ab[0] * ab[0] + ab[1] * ab[1] + ab[2] * ab[2])};
+        for (int k = 0; k < 3; ++k) g.n[k] = std::max(1, std::min(64, (int)std::floor(h[k] / rc)));
+    } else {
+        // hashed grid: cell = floor(x / rc) mod n on every axis
+        const int n = std::max(3, std::min(32, (int)std::ceil(std::cbrt((double)nmem / 2.0))));
+        for (int k = 0; k < 3; ++k) {
+            g.n[k] = n;
+            g.lo[k] = rc;
+            g.inv_extent[k] = 1.0 / rc;
+        }
+    }
+    return g;
+}
+
+// Enumerates the n-mers of one term into the evaluator buckets (and, when
+// list_cap > 0, into c->list).  Asynchronous; status and counts on device.
+static int launch_build(mbx_ctx* c, int nbody, int use_ghost, const double* xyz, long list_cap, int* kernels) {
+    const int g = use_ghost ? 1 : 0;
+    const int nmem = c->nmem[g], nq = c->nquery[g];
+    const double rc = c->cutoff[nbody];
+    const double rc2 = rc * rc;
+    CellGrid cg = make_grid(c, rc, nmem);
+    const int ncell = cg.n[0] * cg.n[1] * cg.n[2];
+    CUCHK(c, c->cloud.ensure((size_t)std::max(nmem, 1) * 24));
+    CUCHK(c, c->cell_of.ensure(std::max(nmem, 1)));
+    CUCHK(c, c->cell_items.ensure(std::max(nmem, 1)));
+    CUCHK(c, c->cell_count.ensure(ncell + 1));
+    CUCHK(c, c->cell_start.ensure(ncell + 1));
+    CUCHK(c, c->cell_fill.ensure(ncell + 1));
+    CUCHK(c, c->nb_count.ensure(std::max(nq, 1)));
+    CUCHK(c, c->nb.ensure((size_t)std::max(nq, 1) * c->nb_cap));
+    CUCHK(c, c->bucket_count.ensure(MBX_MAX_BUCKETS));
+    // bucket capacities: grown on overflow, first guess from the query count
+    long total = 0;
+    for (int b = 0; b < c->nbucket[nbody]; ++b) {
+        if (c->bucket_cap[nbody][b] == 0) c->bucket_cap[nbody][b] = (long)std::max(nq, 1) * (nbody == 2 ? 40 : 80);
+        total += c->bucket_cap[nbody][b];
+    }
+    CUCHK(c, c->buckets.ensure(std::max(total, 1L)));
+    long off = 0;
+    for (int b = 0; b < c->nbucket[nbody]; ++b) {
+        if (nbody == 2) { c->drules.offset[b] = off; c->drules.cap[b] = (int)c->bucket_cap[2][b]; }
+        else { c->trules.offset[b] = off; c->trules.cap[b] = (int)c->bucket_cap[3][b]; }
+        off += c->bucket_cap[nbody][b];
+    }
+    if (list_cap > 0) CUCHK(c, c->list.ensure(list_cap));
+    CUCHK(c, cudaMemsetAsync(c->cell_count.p, 0, (ncell + 1) * sizeof(int), c->stream));
+    CUCHK(c, cudaMemsetAsync(c->bucket_count.p, 0, MBX_MAX_BUCKETS * sizeof(int), c->stream));
+    CUCHK(c, cudaMemsetAsync(c->listed.p, 0, 4 * sizeof(unsigned long long), c->stream));
+    CUCHK(c, cudaMemsetAsync(c->status.p, 0, 4 * sizeof(int), c->stream));
+    if (nmem < 2 || (nbody == 3 && nmem < 3) || nq == 0) return MBX_OK;
+    const int T = 128;
+    k_cloud<<<(nmem + T - 1) / T, T, 0, c->stream>>>(xyz, c->d_first.p, c->d_members[g].p, nmem, c->bp, cg,
+                                                     c->cloud.p, c->cell_of.p);
+    k_cell_count<<<(nmem + T - 1) / T, T, 0, c->stream>>>(c->cell_of.p, nmem, c->cell_count.p);
+    k_cell_scan<<<1, 1024, 0, c->stream>>>(c->cell_count.p, ncell, c->cell_start.p, c->cell_fill.p);
+    k_cell_fill<<<(nmem + T - 1) / T, T, 0, c->stream>>>(c->cell_of.p, nmem, c->cell_fill.p, c->cell_items.p);
+    k_neighbors<<<(nq * 32 + T - 1) / T, T, 0, c->stream>>>(c->cloud.p, c->cell_of.p, c->cell_start.p,
+                                                            c->cell_items.p, c->d_query[g].p, nq, cg, c->bp.use_pbc,
+                                                            rc2, c->nb_cap, c->nb_count.p, c->nb.p, c->status.p);
+    if (nbody == 2) {
+        k_dimers<<<(nq + T - 1) / T, T, 0, c->stream>>>(c->d_query[g].p, nq, c->d_members[g].p, c->d_tag.p,
+                                                        c->d_type.p, c->nb_count.p, c->nb.p, c->nb_cap, rc2, c->drules,
+                                                        c->listed.p, list_cap > 0 ? c->list.p : nullptr, list_cap,
+                                                        c->buckets.p, c->bucket_count.p, c->status.p);
+    } else {
+        const int WPB = 2;
+        const size_t smem = (size_t)WPB * c->nb_cap * sizeof(NbEntry);
+        if (smem > 48 * 1024)
+            CUCHK(c, cudaFuncSetAttribute(k_trimers, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_trimers<<<(nq + WPB - 1) / WPB, WPB * 32, smem, c->stream>>>(
+            c->d_query[g].p, nq, c->d_members[g].p, c->d_tag.p, c->d_type.p, c->cloud.p, c->nb_count.p, c->nb.p,
+            c->nb_cap, rc2, c->trules, c->listed.p, list_cap > 0 ? c->list.p : nullptr, list_cap, c->buckets.p,
+            c->bucket_count.p, c->status.p);
+    }
+    CUCHK(c, cudaGetLastError());
+    *kernels += 7;
+    return MBX_OK;
+}
+
+static HolderArgs base_args(mbx_ctx* c) {
+    HolderArgs A;
+    memset(&A, 0, sizeof(A));
+    A.bp = c->bp;
+    return A;
+}
+
+static int launch_eval(mbx_ctx* c, const EvaluatorInfo* E, HolderArgs A, int flags, int* kernels) {
+    const bool grads = !(flags & MBX_NO_GRADS);
+    const bool mixed = (flags & MBX_MIXED) != 0;
+    const int block = 128;
+    if (E->w) {
+        A.terms = c->terms.p;
+        A.tcoef = c->tcoef.p;
+        A.nterms = (long)(sizeof(mbx_tcoef_ch4ch42b) / sizeof(double));
+        if (!A.coef) A.coef = c->warp_coef.p;
+        long nw = A.n;
+        int grid = (int)std::min<long>((nw + 3) / 4, (long)c->sm_count * 8);
+        RCHK(c, E->w(A, grads ? 1 : 0, std::max(grid, 1), c->stream));
+        ++*kernels;
+        return MBX_OK;
+    }
+    launch_fn fn = !grads ? E->e : (mixed ? E->m : E->g);
+    if (!fn) return fail(c, MBX_ENOTSUP, std::string("no kernel for ") + E->name);
+    // persistent grid: a few resident blocks per SM, grid-stride over n-mers
+    const long want = (A.n + block - 1) / block;
+    const int grid = (int)std::max<long>(1, std::min<long>(want, (long)c->sm_count * 4));
+    RCHK(c, fn(A, grid, block, c->stream));
+    ++*kernels;
+    return MBX_OK;
+}
+
+extern "C" int mbx_energy(mbx_ctx* c, int nbody, double* xyz, int use_ghost, double* energy, double* grad,
+                          double* virial, int flags) {
+    if (!c || (nbody != 2 && nbody != 3) || !xyz || !energy) return fail(c, MBX_EINVAL, "bad arguments");
+    if (!c->nmon) return fail(c, MBX_EINVAL, "System has not been initialized (no topology)");
+    CUCHK(c, cudaSetDevice(c->device));
+    const bool dev = (flags & MBX_DEVICE_PTRS) != 0;
+    const bool grads = !(flags & MBX_NO_GRADS);
+    const size_t nx = 3 * (size_t)c->numsites;
+    for (int attempt = 0; attempt < 4; ++attempt) {
+        int kernels = 0;
+        double* X = xyz;
+        if (!dev) {
+            CUCHK(c, c->xyz.ensure(nx));
+            CUCHK(c, cudaMemcpyAsync(c->xyz.p, xyz, nx * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+            X = c->xyz.p;
+        }
+        CUCHK(c, cudaEventRecord(c->ev[0], c->stream));
+        // SetPBC: FixMonomerCoordinates on every call (system.cpp:741-744);
+        // device inputs are wrapped once even when the call is retried
+        if (c->bp.use_pbc && (!dev || attempt == 0)) {
+            k_fix_monomers<<<(c->nmon + 127) / 128, 128, 0, c->stream>>>(X, c->d_first.p, c->d_nat.p, c->nmon, c->bp);
+            ++kernels;
+        }
+        int r = launch_build(c, nbody, use_ghost, X, 0, &kernels);
+        if (r) return r;
+        CUCHK(c, cudaEventRecord(c->ev[1], c->stream));
+        double* G = nullptr;
+        if (grads) {
+            if (dev && grad) {
+                G = grad;  // accumulate straight into the caller's array
+            } else {
+                CUCHK(c, c->grad.ensure(nx));
+                CUCHK(c, cudaMemsetAsync(c->grad.p, 0, nx * sizeof(double), c->stream));
+                G = c->grad.p;
+            }
+        }
+        CUCHK(c, cudaMemsetAsync(c->out.p, 0, 16 * sizeof(double), c->stream));
+        long off = 0;
+        for (int b = 0; b < c->nbucket[nbody]; ++b) {
+            HolderArgs A = base_args(c);
+            A.n = c->bucket_cap[nbody][b];
+            A.n_dev = c->bucket_count.p + b;
+            A.status = c->status.p;
+            A.nmers = c->buckets.p + off;
+            A.xyz = X;
+            A.first_index = c->d_first.p;
+            A.grad = G;
+            A.out = c->out.p;
+            off += c->bucket_cap[nbody][b];
+            r = launch_eval(c, c->bucket_eval[nbody][b], A, flags, &kernels);
+            if (r) return r;
+        }
+        CUCHK(c, cudaEventRecord(c->ev[2], c->stream));
+        // results: energy + virial, counters, status
+        CUCHK(c, cudaMemcpyAsync(c->h_out, c->out.p, 8 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CUCHK(c, cudaMemcpyAsync(c->h_out + 8, c->listed.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                                 c->stream));
+        CUCHK(c, cudaMemcpyAsync(c->h_out + 9, c->bucket_count.p, MBX_MAX_BUCKETS * sizeof(int),
+                                 cudaMemcpyDeviceToHost, c->stream));
+        CUCHK(c, cudaMemcpyAsync(c->h_out + 13, c->status.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        CUCHK(c, cudaStreamSynchronize(c->stream));
+        int status[2];
+        memcpy(status, c->h_out + 13, sizeof(status));
+        int counts[MBX_MAX_BUCKETS];
+        memcpy(counts, c->h_out + 9, sizeof(counts));
+        if (status[0]) {
+            if (status[0] & MBX_STATUS_NB_OVERFLOW) c->nb_cap = std::max(c->nb_cap * 2, status[1] + 32);
+            for (int b = 0; b < c->nbucket[nbody]; ++b)
+                if (counts[b] > c->bucket_cap[nbody][b])
+                    c->bucket_cap[nbody][b] = (long)(counts[b] * 1.25) + 1024;
+            if ((status[0] & MBX_STATUS_BUCKET_OVERFLOW) && !(status[0] & MBX_STATUS_NB_OVERFLOW)) {
+                for (int b = 0; b < c->nbucket[nbody]; ++b)
+                    if (counts[b] >= c->bucket_cap[nbody][b]) c->bucket_cap[nbody][b] *= 2;
+            }
+            // the evaluators saw the status word and did nothing; rebuild
+            continue;
+        }
+        unsigned long long listed;
+        memcpy(&listed, c->h_out + 8, sizeof(listed));
+        c->last_listed[nbody] = (long)listed;
+        long ev = 0;
+        for (int b = 0; b < c->nbucket[nbody]; ++b) ev += counts[b];
+        c->last_evaluated[nbody] = ev;
+        cudaEventElapsedTime(&c->last_ms_build, c->ev[0], c->ev[1]);
+        cudaEventElapsedTime(&c->last_ms_eval, c->ev[1], c->ev[2]);
+        *energy = c->h_out[0];
+        if (virial) {
+            virial[0] += c->h_out[1];
+            virial[1] += c->h_out[2];
+            virial[2] += c->h_out[3];
+            virial[4] += c->h_out[4];
+            virial[5] += c->h_out[5];
+            virial[8] += c->h_out[6];
+            virial[3] = virial[1];
+            virial[6] = virial[2];
+            virial[7] = virial[5];
+        }
+        if (!dev) {
+            // wrapped coordinates back into the caller's array (SetPBC semantics)
+            if (c->bp.use_pbc)
+                CUCHK(c, cudaMemcpyAsync(xyz, X, nx * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+            if (grads && grad) {
+                std::vector<double> tmp(nx);
+                CUCHK(c, cudaMemcpyAsync(tmp.data(), c->grad.p, nx * sizeof(double), cudaMemcpyDeviceToHost,
+                                         c->stream));
+                CUCHK(c, cudaStreamSynchronize(c->stream));
+                for (size_t i = 0; i < nx; ++i) grad[i] += tmp[i];
+            } else {
+                CUCHK(c, cudaStreamSynchronize(c->stream));
+            }
+        } else if (grads && !grad) {
+            // nothing to return
+        }
+        c->last_kernels = kernels;
+        return MBX_OK;
+    }
+    return fail(c, MBX_ECUDA, "n-mer buffers did not converge");
+}
+
+extern "C" int mbx_last_counts(const mbx_ctx* c, int nbody, long* listed, long* evaluated) {
+    if (!c || (nbody != 2 && nbody != 3)) return MBX_EINVAL;
+    if (listed) *listed = c->last_listed[nbody];
+    if (evaluated) *evaluated = c->last_evaluated[nbody];
+    return MBX_OK;
+}
+
+extern "C" int mbx_last_timing(const mbx_ctx* c, double* ms_build, double* ms_eval, int* kernels) {
+    if (!c) return MBX_EINVAL;
+    if (ms_build) *ms_build = c->last_ms_build;
+    if (ms_eval) *ms_eval = c->last_ms_eval;
+    if (kernels) *kernels = c->last_kernels;
+    return MBX_OK;
+}
+
+extern "C" int mbx_nmers(mbx_ctx* c, int nbody, double cutoff, const double* xyz, int use_ghost, long* out, long cap,
+                         long* count) {
+    if (!c || (nbody != 2 && nbody != 3) || !xyz || !count) return fail(c, MBX_EINVAL, "bad arguments");
+    if (!c->nmon) return fail(c, MBX_EINVAL, "no topology");
+    CUCHK(c, cudaSetDevice(c->device));
+    const double saved = c->cutoff[nbody];
+    c->cutoff[nbody] = cutoff;
+    const size_t nx = 3 * (size_t)c->numsites;
+    long list_cap = std::max<long>(1024, (long)c->nquery[use_ghost ? 1 : 0] * (nbody == 2 ? 64 : 1024));
+    int rc = MBX_OK;
+    for (int attempt = 0; attempt < 6; ++attempt) {
+        int kernels = 0;
+        CUCHK(c, c->xyz.ensure(nx));
+        CUCHK(c, cudaMemcpyAsync(c->xyz.p, xyz, nx * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        rc = launch_build(c, nbody, use_ghost, c->xyz.p, list_cap, &kernels);
+        if (rc) break;
+        unsigned long long listed[2];
+        int status[2];
+        CUCHK(c, cudaMemcpyAsync(listed, c->listed.p, sizeof(listed), cudaMemcpyDeviceToHost, c->stream));
+        CUCHK(c, cudaMemcpyAsync(status, c->status.p, sizeof(status), cudaMemcpyDeviceToHost, c->stream));
+        CUCHK(c, cudaStreamSynchronize(c->stream));
+        if (status[0] & MBX_STATUS_NB_OVERFLOW) {
+            c->nb_cap = std::max(c->nb_cap * 2, status[1] + 32);
+            continue;
+        }
+        if (status[0] & MBX_STATUS_BUCKET_OVERFLOW) {
+            for (int b = 0; b < c->nbucket[nbody]; ++b) c->bucket_cap[nbody][b] *= 2;
+            continue;
+        }
+        if ((long)listed[1] > list_cap) {
+            list_cap = (long)listed[1] + 16;
+            continue;
+        }
+        *count = (long)listed[0];
+        const long n = std::min<long>(cap, (long)listed[0]);
+        if (n > 0 && out) {
+            std::vector<int4> tmp(n);
+            CUCHK(c, cudaMemcpy(tmp.data(), c->list.p, n * sizeof(int4), cudaMemcpyDeviceToHost));
+            for (long i = 0; i < n; ++i) {
+                out[nbody * i] = tmp[i].x;
+                out[nbody * i + 1] = tmp[i].y;
+                if (nbody == 3) out[nbody * i + 2] = tmp[i].z;
+            }
+        }
+        c->cutoff[nbody] = saved;
+        return MBX_OK;
+    }
+    c->cutoff[nbody] = saved;
+    return rc ? rc : fail(c, MBX_ECUDA, "n-mer list buffers did not converge");
+}
+
+// Copies an input array to the device when needed; returns the device pointer.
+static int stage_in(mbx_ctx* c, DevBuf<double>& buf, const double* src, size_t n, bool dev, const double** dst) {
+    if (dev || !src) {
+        *dst = src;
+        return MBX_OK;
+    }
+    CUCHK(c, buf.ensure(n));
+    CUCHK(c, cudaMemcpyAsync(buf.p, src, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    *dst = buf.p;
+    return MBX_OK;
+}
+
+extern "C" int mbx_evaluate(mbx_ctx* c, const char* name, long n, const double* xyz, double* grad, double* virial,
+                            double* e_per, double* energy, int flags) {
+    if (!c || !name || n < 0 || (n > 0 && !xyz)) return fail(c, MBX_EINVAL, "bad arguments");
+    const EvaluatorInfo* E = find_evaluator(name);
+    if (!E) return fail(c, MBX_ENOTSUP, std::string("unknown evaluator ") + name);
+    CUCHK(c, cudaSetDevice(c->device));
+    const bool dev = (flags & MBX_DEVICE_PTRS) != 0;
+    const size_t nx = (size_t)n * E->nreal * 3;
+    static thread_local DevBuf<double> in_buf, g_buf, e_buf;
+    const double* X;
+    int r = stage_in(c, in_buf, xyz, nx, dev, &X);
+    if (r) return r;
+    const bool grads = !(flags & MBX_NO_GRADS) && grad;
+    double* G = nullptr;
+    if (grads) {
+        if (dev) G = grad;
+        else {
+            CUCHK(c, g_buf.ensure(nx));
+            CUCHK(c, cudaMemsetAsync(g_buf.p, 0, nx * sizeof(double), c->stream));
+            G = g_buf.p;
+        }
+    }
+    double* EP = nullptr;
+    if (e_per) {
+        if (dev) EP = e_per;
+        else {
+            CUCHK(c, e_buf.ensure(std::max<long>(n, 1)));
+            EP = e_buf.p;
+        }
+    }
+    CUCHK(c, cudaMemsetAsync(c->out.p, 0, 16 * sizeof(double), c->stream));
+    HolderArgs A = base_args(c);
+    A.bp.use_pbc = 0;
+    A.n = n;
+    A.aos = 1;
+    A.xyz = X;
+    A.grad = G;
+    A.out = c->out.p;
+    A.e_per = EP;
+    int kernels = 0;
+    if (n > 0) {
+        r = launch_eval(c, E, A, grads ? (flags & MBX_MIXED) : (flags | MBX_NO_GRADS), &kernels);
+        if (r) return r;
+    }
+    CUCHK(c, cudaMemcpyAsync(c->h_out, c->out.p, 8 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    std::vector<double> gt, et;
+    if (grads && !dev) {
+        gt.resize(nx);
+        CUCHK(c, cudaMemcpyAsync(gt.data(), G, nx * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    }
+    if (e_per && !dev && n > 0) CUCHK(c, cudaMemcpyAsync(e_per, EP, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CUCHK(c, cudaStreamSynchronize(c->stream));
+    if (grads && !dev)
+        for (size_t i = 0; i < nx; ++i) grad[i] += gt[i];
+    if (energy) *energy = c->h_out[0];
+    if (virial) {
+        virial[0] += c->h_out[1];
+        virial[1] += c->h_out[2];
+        virial[2] += c->h_out[3];
+        virial[4] += c->h_out[4];
+        virial[5] += c->h_out[5];
+        virial[8] += c->h_out[6];
+        virial[3] = virial[1];
+        virial[6] = virial[2];
+        virial[7] = virial[5];
+    }
+    return MBX_OK;
+}
+
+extern "C" int mbx_evaluate_dcoef(mbx_ctx* c, const char* name, long n, const double* xyz, const double* w,
+                                  double* out, int flags) {
+    if (!c || !name || n < 0 || !out) return fail(c, MBX_EINVAL, "bad arguments");
+    const EvaluatorInfo* E = find_evaluator(name);
+    if (!E) return fail(c, MBX_ENOTSUP, std::string("unknown evaluator ") + name);
+    if (!E->c) return fail(c, MBX_ENOTSUP, std::string("no coefficient adjoint for ") + name);
+    CUCHK(c, cudaSetDevice(c->device));
+    const bool dev = (flags & MBX_DEVICE_PTRS) != 0;
+    const size_t nx = (size_t)n * E->nreal * 3;
+    static thread_local DevBuf<double> in_buf, w_buf, o_buf;
+    const double *X, *W;
+    int r = stage_in(c, in_buf, xyz, nx, dev, &X);
+    if (r) return r;
+    r = stage_in(c, w_buf, w, (size_t)n, dev, &W);
+    if (r) return r;
+    double* O = out;
+    if (!dev) {
+        CUCHK(c, o_buf.ensure(E->ncoef));
+        CUCHK(c, cudaMemsetAsync(o_buf.p, 0, E->ncoef * sizeof(double), c->stream));
+        O = o_buf.p;
+    }
+    HolderArgs A = base_args(c);
+    A.bp.use_pbc = 0;
+    A.n = n;
+    A.aos = 1;
+    A.xyz = X;
+    if (n > 0) {
+        const int grid = (int)std::max<long>(1, std::min<long>((n + 127) / 128, (long)c->sm_count * 4));
+        RCHK(c, E->c(A, W, O, grid, 128, c->stream));
+    }
+    if (!dev) {
+        std::vector<double> tmp(E->ncoef);
+        CUCHK(c, cudaMemcpyAsync(tmp.data(), O, E->ncoef * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CUCHK(c, cudaStreamSynchronize(c->stream));
+        for (int k = 0; k < E->ncoef; ++k) out[k] += tmp[k];
+    }
+    return MBX_OK;
+}
+
+extern "C" int mbx_poly(mbx_ctx* c, const char* name, long nd, const double* x, double* g, double* e, int flags) {
+    if (!c || !name || nd < 0 || (nd > 0 && (!x || !e))) return fail(c, MBX_EINVAL, "bad arguments");
+    const EvaluatorInfo* E = find_evaluator(name);
+    if (!E) return fail(c, MBX_ENOTSUP, std::string("unknown evaluator ") + name);
+    if (!E->p) return fail(c, MBX_ENOTSUP, std::string("no straight-line polynomial for ") + name);
+    CUCHK(c, cudaSetDevice(c->device));
+    const bool dev = (flags & MBX_DEVICE_PTRS) != 0;
+    const size_t nv = (size_t)nd * E->nvars;
+    static thread_local DevBuf<double> xb, gb, eb;
+    const double* X;
+    int r = stage_in(c, xb, x, nv, dev, &X);
+    if (r) return r;
+    double *G = g, *Ev = e;
+    if (!dev) {
+        CUCHK(c, gb.ensure(std::max<size_t>(nv, 1)));
+        CUCHK(c, eb.ensure(std::max<long>(nd, 1)));
+        G = g ? gb.p : nullptr;
+        Ev = eb.p;
+    }
+    if (nd > 0) {
+        const int grid = (int)std::max<long>(1, std::min<long>((nd + 127) / 128, (long)c->sm_count * 4));
+        RCHK(c, E->p(nd, X, G, Ev, grid, 128, c->stream));
+    }
+    if (!dev && nd > 0) {
+        CUCHK(c, cudaMemcpyAsync(e, Ev, nd * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        if (g) CUCHK(c, cudaMemcpyAsync(g, G, nv * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    }
+    CUCHK(c, cudaStreamSynchronize(c->stream));
+    return MBX_OK;
+}
+
+extern "C" int mbx_set_coefficients(mbx_ctx* c, const char* name, const double* a, int flags) {
+    if (!c || !name) return fail(c, MBX_EINVAL, "bad arguments");
+    const EvaluatorInfo* E = find_evaluator(name);
+    if (!E) return fail(c, MBX_ENOTSUP, std::string("unknown evaluator ") + name);
+    CUCHK(c, cudaSetDevice(c->device));
+    const bool dev = a && (flags & MBX_DEVICE_PTRS);
+    const double* src = a ? a : E->fit;
+    for (int v = 0; v < 6; ++v)
+        if (E->set[v]) RCHK(c, E->set[v](src, dev ? 1 : 0, c->stream));
+    if (E->w)
+        CUCHK(c, cudaMemcpyAsync(c->warp_coef.p, src, E->ncoef * sizeof(double),
+                                 dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, c->stream));
+    CUCHK(c, cudaStreamSynchronize(c->stream));
+    return MBX_OK;
+}

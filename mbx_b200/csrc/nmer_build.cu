@@ -1,0 +1,375 @@
+// Dimer/trimer enumeration on the GPU, reproducing the reference's lists.
+//
+// The reference (systools::AddClusters, bblock/sys_tools.cpp:472-592) builds a
+// kd-tree over the monomers' first atoms wrapped into the central cell plus
+// seven periodic copies of every point (kdutils::XyzToCloud,
+// kdtree/kdtree_utils.h:196-278), radius-searches each local monomer i with a
+// strict d^2 < cutoff^2 test (kdtree/nanoflann.hpp:166-167), and accepts
+//   dimer (i, j)    if tag_i < tag_j,
+//   trimer (i,j,k)  for every pair of i's matches (j, k distinct, neither i)
+//                   if |q_j - q_k|^2 > cutoff^2 or tag_i < min(tag_j, tag_k),
+// where q are the matched cloud points (images near i).
+//
+// Here the same cloud is built explicitly (k_cloud), monomers are binned into
+// a cell grid over fractional coordinates (k_cells*), every local monomer
+// collects its matches from the 27 surrounding cells by testing all eight
+// cloud points of each candidate (k_neighbors), and the dimer and trimer rules
+// run on those matches (k_dimers, k_trimers).  Every distance that decides
+// membership is computed with explicitly rounded operations in the
+// reference's operand order, so the sets are bit-for-bit the reference's.
+//
+// Accepted n-mers are written to per-type buckets, already in evaluator
+// (holder) order with the slot of the original first monomer, which is the
+// image anchor (GetCloseDimerImage/GetCloseTrimerImage image relative to it).
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "holder_common.cuh"
+#include "nmer_build.h"
+
+namespace {
+
+__device__ __forceinline__ double dist2_rn(double a0, double a1, double a2, double b0, double b1, double b2) {
+    const double d0 = __dsub_rn(a0, b0), d1 = __dsub_rn(a1, b1), d2 = __dsub_rn(a2, b2);
+    return __dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)), __dmul_rn(d2, d2));
+}
+
+// GetFractionalCoordinates (kdtree/kdtree_utils.h:165-190); only the signs of
+// its results matter (they choose which periodic copies exist).
+__device__ void frac_coords(const double* box, const double (&pt)[3], double (&c)[3]) {
+    const double A = box[0];
+    const double B = sqrt(box[3] * box[3] + box[4] * box[4]);
+    const double C = sqrt(box[6] * box[6] + box[7] * box[7] + box[8] * box[8]);
+    const double AdotB = box[0] * box[3], AdotC = box[0] * box[6], BdotC = box[3] * box[6] + box[4] * box[7];
+    const double gamma = acos(AdotB / A / B), beta = acos(AdotC / A / C), alpha = acos(BdotC / B / C);
+    const double ca = cos(alpha), cb = cos(beta), cg = cos(gamma), sg = sin(gamma);
+    const double omega = A * B * C * sqrt(1 - ca * ca - cb * cb - cg * cg + 2 * ca * cb * cg);
+    c[0] = 1 / A * pt[0] - cg / A / sg * pt[1] + B * C * (ca * cg - cb) / omega / sg * pt[2];
+    c[1] = 1 / B / sg * pt[1] + A * C * (cb * cg - ca) / omega / sg * pt[2];
+    c[2] = A * B * sg / omega * pt[2];
+}
+
+}  // namespace
+
+// FixMonomerCoordinates (bblock/sys_tools.cpp:257-320), in place.
+__global__ void k_fix_monomers(double* __restrict__ xyz, const int* __restrict__ first_index,
+                               const int* __restrict__ nat, int nmon, BoxParams bp) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nmon) return;
+    double* p = xyz + 3 * (size_t)first_index[i];
+    double q[3] = {p[0], p[1], p[2]}, f0[3];
+    to_frac_rn(bp.inv, q, f0);
+    f0[0] = __dsub_rn(f0[0], floor(__dadd_rn(f0[0], 0.5)));
+    f0[1] = __dsub_rn(f0[1], floor(__dadd_rn(f0[1], 0.5)));
+    f0[2] = __dsub_rn(f0[2], floor(__dadd_rn(f0[2], 0.5)));
+    to_cart_rn(bp.box, f0, q);
+    p[0] = q[0]; p[1] = q[1]; p[2] = q[2];
+    for (int j = 1; j < nat[i]; ++j) {
+        double a[3] = {p[3 * j], p[3 * j + 1], p[3 * j + 2]}, f[3];
+        to_frac_rn(bp.inv, a, f);
+        f[0] = __dsub_rn(f[0], floor(__dadd_rn(__dsub_rn(f[0], f0[0]), 0.5)));
+        f[1] = __dsub_rn(f[1], floor(__dadd_rn(__dsub_rn(f[1], f0[1]), 0.5)));
+        f[2] = __dsub_rn(f[2], floor(__dadd_rn(__dsub_rn(f[2], f0[2]), 0.5)));
+        to_cart_rn(bp.box, f, a);
+        p[3 * j] = a[0]; p[3 * j + 1] = a[1]; p[3 * j + 2] = a[2];
+    }
+}
+
+// Cloud points of every monomer in the search: slot 0 is the wrapped first
+// atom, slots 1..7 its periodic copies in the reference's shift categories
+// (m,n,l nonzero pattern: 1 = z, 2 = y, 3 = x, 4 = xyz, 5 = yz, 6 = xz, 7 = xy).
+// Also assigns the monomer's cell.
+__global__ void k_cloud(const double* __restrict__ xyz, const int* __restrict__ first_index,
+                        const int* __restrict__ members, int nmem, BoxParams bp, CellGrid cg,
+                        double* __restrict__ cloud, int* __restrict__ cell_of) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nmem) return;
+    const int i = members[q];
+    const double* p0 = xyz + 3 * (size_t)first_index[i];
+    double p[3] = {p0[0], p0[1], p0[2]};
+    double* out = cloud + (size_t)q * 24;
+    double fr[3];
+    if (bp.use_pbc) {
+        double f[3];
+        to_frac_rn(bp.inv, p, f);
+        f[0] = __dsub_rn(f[0], floor(__dadd_rn(f[0], 0.5)));
+        f[1] = __dsub_rn(f[1], floor(__dadd_rn(f[1], 0.5)));
+        f[2] = __dsub_rn(f[2], floor(__dadd_rn(f[2], 0.5)));
+        to_cart_rn(bp.box, f, p);
+        double uvw[3];
+        frac_coords(bp.box, p, uvw);
+        // per axis: the copy at -1 exists if uvw > 0, at +1 if uvw < 0; at
+        // uvw == 0 both are made and the +1 copy overwrites (loop order 0,-1,1)
+        int sgn[3];
+        for (int a = 0; a < 3; ++a) sgn[a] = (uvw[a] > 0.0) ? -1 : 1;
+        for (int cat = 1; cat < 8; ++cat) {
+            // category -> which axes are shifted
+            const int mx = (cat == 3 || cat == 4 || cat == 6 || cat == 7);
+            const int my = (cat == 2 || cat == 4 || cat == 5 || cat == 7);
+            const int mz = (cat == 1 || cat == 4 || cat == 5 || cat == 6);
+            const double m = mx ? sgn[0] : 0, n = my ? sgn[1] : 0, l = mz ? sgn[2] : 0;
+            const double sx = __dadd_rn(__dadd_rn(__dmul_rn(m, bp.box[0]), __dmul_rn(n, bp.box[3])),
+                                        __dmul_rn(l, bp.box[6]));
+            const double sy = __dadd_rn(__dadd_rn(__dmul_rn(m, bp.box[1]), __dmul_rn(n, bp.box[4])),
+                                        __dmul_rn(l, bp.box[7]));
+            const double sz = __dadd_rn(__dadd_rn(__dmul_rn(m, bp.box[2]), __dmul_rn(n, bp.box[5])),
+                                        __dmul_rn(l, bp.box[8]));
+            out[3 * cat + 0] = __dadd_rn(p[0], sx);
+            out[3 * cat + 1] = __dadd_rn(p[1], sy);
+            out[3 * cat + 2] = __dadd_rn(p[2], sz);
+        }
+        fr[0] = f[0] + 0.5; fr[1] = f[1] + 0.5; fr[2] = f[2] + 0.5;   // in [0, 1)
+    } else {
+        for (int cat = 1; cat < 8; ++cat) {
+            out[3 * cat] = out[3 * cat + 1] = out[3 * cat + 2] = 1e300;   // no copies without PBC
+        }
+        fr[0] = fr[1] = fr[2] = 0.0;
+    }
+    out[0] = p[0]; out[1] = p[1]; out[2] = p[2];
+    int c[3];
+    for (int a = 0; a < 3; ++a) {
+        if (bp.use_pbc) {
+            const int v = (int)floor(fr[a] * cg.n[a]);
+            c[a] = v < 0 ? 0 : (v >= cg.n[a] ? cg.n[a] - 1 : v);
+        } else {
+            // hashed grid: cells of edge rc, indices taken modulo n
+            const double f = floor(p[a] * cg.inv_extent[a]);
+            const long long v = (long long)fmod(f, (double)cg.n[a]);
+            c[a] = (int)((v + cg.n[a]) % cg.n[a]);
+        }
+    }
+    cell_of[q] = (c[2] * cg.n[1] + c[1]) * cg.n[0] + c[0];
+}
+
+__global__ void k_cell_count(const int* __restrict__ cell_of, int nmem, int* __restrict__ cell_count) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < nmem) atomicAdd(cell_count + cell_of[q], 1);
+}
+
+// Exclusive scan of the cell counts in one block (cell grids here are small).
+__global__ void k_cell_scan(const int* __restrict__ cell_count, int ncell, int* __restrict__ cell_start,
+                            int* __restrict__ cell_fill) {
+    __shared__ int warp_sums[32];
+    __shared__ int carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int base = 0; base < ncell; base += blockDim.x) {
+        const int i = base + threadIdx.x;
+        const int v = i < ncell ? cell_count[i] : 0;
+        int x = v;
+        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) warp_sums[w] = x;
+        __syncthreads();
+        if (w == 0) {
+            int s = lane < (int)(blockDim.x >> 5) ? warp_sums[lane] : 0;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, s, o);
+                if (lane >= o) s += y;
+            }
+            warp_sums[lane] = s;
+        }
+        __syncthreads();
+        const int excl = carry + (w ? warp_sums[w - 1] : 0) + x - v;
+        if (i < ncell) {
+            cell_start[i] = excl;
+            cell_fill[i] = excl;
+        }
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) carry = excl + v;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) cell_start[ncell] = carry;
+}
+
+__global__ void k_cell_fill(const int* __restrict__ cell_of, int nmem, int* __restrict__ cell_fill,
+                            int* __restrict__ cell_items) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < nmem) cell_items[atomicAdd(cell_fill + cell_of[q], 1)] = q;
+}
+
+// Matches of every local monomer: cloud points (member q, copy s) with
+// d^2 < rc_max^2.  One warp per query; matches are appended in candidate order.
+__global__ void k_neighbors(const double* __restrict__ cloud, const int* __restrict__ cell_of,
+                            const int* __restrict__ cell_start, const int* __restrict__ cell_items,
+                            const int* __restrict__ query, int nquery, CellGrid cg, int use_pbc, double rc2,
+                            int cap, int* __restrict__ nb_count, NbEntry* __restrict__ nb, int* __restrict__ status) {
+    const int lane = threadIdx.x & 31;
+    const int wq = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (wq >= nquery) return;
+    const int qi = query[wq];
+    const double* pi = cloud + (size_t)qi * 24;
+    const double x0 = pi[0], x1 = pi[1], x2 = pi[2];
+    const int c = cell_of[qi];
+    const int cx = c % cg.n[0], cy = (c / cg.n[0]) % cg.n[1], cz = c / (cg.n[0] * cg.n[1]);
+    int count = 0;
+    NbEntry* out = nb + (size_t)wq * cap;
+    // neighbouring cells; an axis with fewer than 3 cells is scanned once
+    const int rx = cg.n[0] >= 3 ? 1 : 0, ry = cg.n[1] >= 3 ? 1 : 0, rz = cg.n[2] >= 3 ? 1 : 0;
+    const int sx = cg.n[0] >= 3 ? 3 : cg.n[0], sy = cg.n[1] >= 3 ? 3 : cg.n[1], sz = cg.n[2] >= 3 ? 3 : cg.n[2];
+    for (int dz = 0; dz < sz; ++dz)
+        for (int dy = 0; dy < sy; ++dy)
+            for (int dx = 0; dx < sx; ++dx) {
+                // periodic in index space both with PBC and for the hashed
+                // grid without PBC (n >= 3 there, so the 27 cells are distinct)
+                int ax = rx ? cx + dx - 1 : dx, ay = ry ? cy + dy - 1 : dy, az = rz ? cz + dz - 1 : dz;
+                ax = (ax + cg.n[0]) % cg.n[0];
+                ay = (ay + cg.n[1]) % cg.n[1];
+                az = (az + cg.n[2]) % cg.n[2];
+                const int cell = (az * cg.n[1] + ay) * cg.n[0] + ax;
+                const int b = cell_start[cell], e = cell_start[cell + 1];
+                const int ncopy = use_pbc ? 8 : 1;
+                for (int base = b * ncopy; base < e * ncopy; base += 32) {
+                    const int t = base + lane;
+                    bool hit = false;
+                    NbEntry ent;
+                    if (t < e * ncopy) {
+                        const int qj = cell_items[t / ncopy];
+                        const int s = t % ncopy;
+                        const double* pj = cloud + (size_t)qj * 24 + 3 * s;
+                        const double d2 = dist2_rn(x0, x1, x2, pj[0], pj[1], pj[2]);
+                        if (d2 < rc2) {
+                            hit = true;
+                            ent.member = qj;
+                            ent.copy = s;
+                            ent.d2 = d2;
+                        }
+                    }
+                    const unsigned m = __ballot_sync(0xffffffffu, hit);
+                    if (hit) {
+                        const int pos = count + __popc(m & ((1u << lane) - 1u));
+                        if (pos < cap) out[pos] = ent;
+                    }
+                    count += __popc(m);
+                }
+            }
+    if (lane == 0) {
+        nb_count[wq] = count < cap ? count : cap;
+        if (count > cap) {
+            atomicOr(status, MBX_STATUS_NB_OVERFLOW);
+            atomicMax(status + 1, count);
+        }
+    }
+}
+
+// Dimers from the matches: (i, j) with d^2 < rc2 and tag_i < tag_j.
+__global__ void k_dimers(const int* __restrict__ query, int nquery, const int* __restrict__ members,
+                         const int* __restrict__ tag, const int* __restrict__ type, const int* __restrict__ nb_count,
+                         const NbEntry* __restrict__ nb, int cap, double rc2, DimerRules R,
+                         unsigned long long* __restrict__ listed, int4* __restrict__ list, long list_cap,
+                         int4* __restrict__ bucket_data, int* __restrict__ bucket_count,
+                         int* __restrict__ status) {
+    const int wq = blockIdx.x * blockDim.x + threadIdx.x;
+    if (wq >= nquery) return;
+    const int qi = query[wq];
+    const int mi = members[qi];
+    const int ti = tag[mi];
+    const int n = nb_count[wq];
+    const NbEntry* e = nb + (size_t)wq * cap;
+    unsigned long long mine = 0;
+    for (int a = 0; a < n; ++a) {
+        const NbEntry ea = e[a];
+        if (!(ea.d2 < rc2)) continue;
+        const int mj = members[ea.member];
+        if (!(ti < tag[mj])) continue;
+        ++mine;
+        if (list) {
+            const unsigned long long pos = atomicAdd(listed + 1, 1ull);
+            if ((long)pos < list_cap) list[pos] = make_int4(mi, mj, -1, 0);
+        }
+        const int code = type[mi] * MBX_MAX_TYPES + type[mj];
+        const int b = R.bucket[code];
+        if (b < 0) continue;
+        if (ea.d2 > R.pre2[b]) continue;     // cannot pass the evaluator's own cutoff
+        const int pos = atomicAdd(bucket_count + b, 1);
+        if (pos < R.cap[b]) {
+            const int4 rec = R.swap[code] ? make_int4(mj, mi, -1, 1) : make_int4(mi, mj, -1, 0);
+            bucket_data[R.offset[b] + pos] = rec;
+        } else {
+            atomicOr(status, MBX_STATUS_BUCKET_OVERFLOW);
+        }
+    }
+    if (mine) atomicAdd(listed, mine);
+}
+
+// Trimers: one warp per query monomer i, lanes over the pairs of its matches.
+__global__ void k_trimers(const int* __restrict__ query, int nquery, const int* __restrict__ members,
+                          const int* __restrict__ tag, const int* __restrict__ type, const double* __restrict__ cloud,
+                          const int* __restrict__ nb_count, const NbEntry* __restrict__ nb, int cap, double rc2,
+                          TrimerRules R, unsigned long long* __restrict__ listed, int4* __restrict__ list,
+                          long list_cap, int4* __restrict__ bucket_data, int* __restrict__ bucket_count,
+                          int* __restrict__ status) {
+    extern __shared__ unsigned char smem[];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int wq = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (wq >= nquery) return;
+    // compact this query's matches with d^2 < rc2 into shared memory
+    NbEntry* sh = reinterpret_cast<NbEntry*>(smem) + (size_t)w * cap;
+    const int qi = query[wq];
+    const int mi = members[qi];
+    const int ti = tag[mi];
+    const int n0 = nb_count[wq];
+    const NbEntry* e = nb + (size_t)wq * cap;
+    int n = 0;
+    for (int base = 0; base < n0; base += 32) {
+        const int a = base + lane;
+        bool keep = false;
+        NbEntry ea;
+        if (a < n0) {
+            ea = e[a];
+            keep = ea.d2 < rc2 && ea.member != qi;
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, keep);
+        if (keep) sh[n + __popc(m & ((1u << lane) - 1u))] = ea;
+        n += __popc(m);
+    }
+    __syncwarp();
+    const long npair = (long)n * (n - 1) / 2;
+    unsigned long long mine = 0;
+    for (long p = lane; p < npair; p += 32) {
+        // pair index -> (a, b), a < b
+        int a = (int)((2.0 * n - 1 - sqrt((2.0 * n - 1) * (2.0 * n - 1) - 8.0 * p)) / 2.0);
+        if (a < 0) a = 0;
+        while ((long)(a + 1) * (2 * n - a - 2) / 2 <= p) ++a;
+        while ((long)a * (2 * n - a - 1) / 2 > p) --a;
+        const int b = (int)(p - (long)a * (2 * n - a - 1) / 2) + a + 1;
+        const NbEntry ea = sh[a], eb = sh[b];
+        if (ea.member == eb.member) continue;
+        const double* pa = cloud + (size_t)ea.member * 24 + 3 * ea.copy;
+        const double* pb = cloud + (size_t)eb.member * 24 + 3 * eb.copy;
+        const double djk = dist2_rn(pa[0], pa[1], pa[2], pb[0], pb[1], pb[2]);
+        const int mj = members[ea.member], mk = members[eb.member];
+        if (!(djk > rc2 || (ti < tag[mj] && ti < tag[mk]))) continue;
+        ++mine;
+        if (list) {
+            const unsigned long long pos = atomicAdd(listed + 1, 1ull);
+            if ((long)pos < list_cap) list[pos] = make_int4(mi, mj, mk, 0);
+        }
+        const int code = (type[mi] * MBX_MAX_TYPES + type[mj]) * MBX_MAX_TYPES + type[mk];
+        const int bk = R.bucket[code];
+        if (bk < 0) continue;
+        // pre-filter with the evaluator's skip rule on the cloud distances
+        const double r2[3] = {ea.d2, eb.d2, djk};
+        const double rf2 = R.pre2[bk];
+        const int nfar = (r2[0] > rf2) + (r2[1] > rf2) + (r2[2] > rf2);
+        if (R.skip[bk] == 1 && nfar >= 2) continue;
+        if (R.skip[bk] == 2 && nfar == 3) continue;
+        const int pos = atomicAdd(bucket_count + bk, 1);
+        if (pos < R.cap[bk]) {
+            const int perm = R.perm[code];   // slot s of the holder takes original slot (perm >> 2s) & 3
+            const int orig[3] = {mi, mj, mk};
+            const int s0 = perm & 3, s1 = (perm >> 2) & 3, s2 = (perm >> 4) & 3;
+            int anchor = 0;
+            if (s1 == 0) anchor = 1;
+            if (s2 == 0) anchor = 2;
+            bucket_data[R.offset[bk] + pos] = make_int4(orig[s0], orig[s1], orig[s2], anchor);
+        } else {
+            atomicOr(status, MBX_STATUS_BUCKET_OVERFLOW);
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) mine += __shfl_xor_sync(0xffffffffu, mine, o);
+    if (lane == 0 && mine) atomicAdd(listed, mine);
+}

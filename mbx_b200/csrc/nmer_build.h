@@ -1,0 +1,62 @@
+// Shared declarations for the n-mer builder (nmer_build.cu) and its host
+// driver (mbx_capi.cu).  Internal to the library.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "holder_common.cuh"
+
+#define MBX_MAX_TYPES 4
+#define MBX_MAX_BUCKETS 8
+
+// device status word bits (status[0]); status[1] holds the largest
+// neighbour count seen when MBX_STATUS_NB_OVERFLOW is set
+#define MBX_STATUS_NB_OVERFLOW 1
+#define MBX_STATUS_BUCKET_OVERFLOW 2
+#define MBX_STATUS_LIST_OVERFLOW 4
+
+struct CellGrid {
+    int n[3];
+    double lo[3];          // unused
+    double inv_extent[3];  // no PBC: 1 / cell edge of the hashed grid
+};
+
+struct NbEntry {
+    int member;  // index into the search's member list
+    int copy;    // cloud copy 0..7
+    double d2;   // squared distance to the query, reference arithmetic
+};
+
+struct DimerRules {
+    int bucket[MBX_MAX_TYPES * MBX_MAX_TYPES];  // type pair (in n-mer order) -> bucket or -1
+    int swap[MBX_MAX_TYPES * MBX_MAX_TYPES];    // 1: evaluator order is (j, i)
+    double pre2[MBX_MAX_BUCKETS];               // (evaluator cutoff + margin)^2
+    int cap[MBX_MAX_BUCKETS];
+    long offset[MBX_MAX_BUCKETS];
+};
+
+struct TrimerRules {
+    int bucket[MBX_MAX_TYPES * MBX_MAX_TYPES * MBX_MAX_TYPES];
+    int perm[MBX_MAX_TYPES * MBX_MAX_TYPES * MBX_MAX_TYPES];  // evaluator slot s <- original slot (perm >> 2s) & 3
+    int skip[MBX_MAX_BUCKETS];                                // 1 two_of_three_gt, 2 all_three_gt
+    double pre2[MBX_MAX_BUCKETS];
+    int cap[MBX_MAX_BUCKETS];
+    long offset[MBX_MAX_BUCKETS];
+};
+
+__global__ void k_fix_monomers(double* xyz, const int* first_index, const int* nat, int nmon, BoxParams bp);
+__global__ void k_cloud(const double* xyz, const int* first_index, const int* members, int nmem, BoxParams bp,
+                        CellGrid cg, double* cloud, int* cell_of);
+__global__ void k_cell_count(const int* cell_of, int nmem, int* cell_count);
+__global__ void k_cell_scan(const int* cell_count, int ncell, int* cell_start, int* cell_fill);
+__global__ void k_cell_fill(const int* cell_of, int nmem, int* cell_fill, int* cell_items);
+__global__ void k_neighbors(const double* cloud, const int* cell_of, const int* cell_start, const int* cell_items,
+                            const int* query, int nquery, CellGrid cg, int use_pbc, double rc2, int cap,
+                            int* nb_count, NbEntry* nb, int* status);
+__global__ void k_dimers(const int* query, int nquery, const int* members, const int* tag, const int* type,
+                         const int* nb_count, const NbEntry* nb, int cap, double rc2, DimerRules R,
+                         unsigned long long* listed, int4* list, long list_cap, int4* bucket_data,
+                         int* bucket_count, int* status);
+__global__ void k_trimers(const int* query, int nquery, const int* members, const int* tag, const int* type,
+                          const double* cloud, const int* nb_count, const NbEntry* nb, int cap, double rc2,
+                          TrimerRules R, unsigned long long* listed, int4* list, long list_cap, int4* bucket_data,
+                          int* bucket_count, int* status);

@@ -259,3 +259,45 @@ def check():
         assert len(s.variables) == s.nvars, (s.name, len(s.variables))
         assert len(s.sites) == s.nreal + 2 * len(s.lp), s.name
     return True
+
+
+def sorted_slots(ids):
+    """Slot order into which the reference's dispatch sorts monomer ids
+    (potential/2b/energy2b.cpp:240-254; potential/3b/energy3b.cpp:185-216)."""
+    m = list(ids)
+    if len(m) == 2:
+        return (1, 0) if m[1] < m[0] else (0, 1)
+    k = [0, 1, 2]
+    if m[2] < m[0] and m[2] < m[1]:
+        m[0], m[2] = m[2], m[0]
+        k[0], k[2] = k[2], k[0]
+    if m[0] > m[1] and m[0] > m[2]:
+        m[0], m[2] = m[2], m[0]
+        k[0], k[2] = k[2], k[0]
+    elif m[1] > m[0] and m[1] > m[2]:
+        m[1], m[2] = m[2], m[1]
+        k[1], k[2] = k[2], k[1]
+    if m[0] > m[1]:
+        m[0], m[1] = m[1], m[0]
+        k[0], k[1] = k[1], k[0]
+    return tuple(k)
+
+
+def dispatch(ids):
+    """(evaluator name or None, evaluator slot -> original slot) for an n-mer
+    whose monomers, in n-mer order, have the given ids."""
+    so = sorted_slots(ids)
+    sorted_ids = [ids[s] for s in so]
+    table = DISPATCH_2B if len(ids) == 2 else DISPATCH_3B
+    name = table.get(tuple(sorted_ids))
+    if name is None:
+        return None, None
+    used = [False] * len(ids)
+    order = []
+    for h in SPECS[name].monomers:
+        for s in range(len(ids)):
+            if not used[s] and sorted_ids[s] == h:
+                used[s] = True
+                order.append(so[s])
+                break
+    return name, tuple(order)

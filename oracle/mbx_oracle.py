@@ -27,6 +27,7 @@ import subprocess
 import numpy as np
 
 from mbx_b200.specs import SPECS, DISPATCH_2B, DISPATCH_3B, LP_GAMMA_IN, LP_GAMMA_OUT
+from mbx_b200.specs import dispatch as dispatch_nmer
 from mbx_b200.tables import load_pip, load_fit
 from mbx_b200.topology import Topology
 
@@ -228,25 +229,24 @@ def add_clusters(nmax, cutoff, first_atoms, tag, is_local, box=None, use_ghost=F
         cap = n
 
 
-def _sorted_slots(types):
-    """Slot permutation that e2b/e3b dispatch applies to the monomer ids."""
-    if len(types) == 2:
-        return (1, 0) if types[1] < types[0] else (0, 1)
-    m = list(types)
-    idx = [0, 1, 2]
-    if m[2] < m[0] and m[2] < m[1]:
-        m[0], m[2] = m[2], m[0]
-        idx[0], idx[2] = idx[2], idx[0]
-    if m[0] > m[1] and m[0] > m[2]:
-        m[0], m[2] = m[2], m[0]
-        idx[0], idx[2] = idx[2], idx[0]
-    elif m[1] > m[0] and m[1] > m[2]:
-        m[1], m[2] = m[2], m[1]
-        idx[1], idx[2] = idx[2], idx[1]
-    if m[0] > m[1]:
-        m[0], m[1] = m[1], m[0]
-        idx[0], idx[1] = idx[1], idx[0]
-    return tuple(idx)
+def get_nb_energy(ids, xyzs, nm, do_grads=True):
+    """e2b::get_2b_energy / e3b::get_3b_energy (potential/2b/energy2b.cpp:206,
+    potential/3b/energy3b.cpp:139): nm n-mers of monomers ids, coordinates per
+    slot xyzs[s] ([nm * 3 * nat_s]), not imaged.  Returns (E, grads per slot,
+    virial); unknown tuples give 0."""
+    name, order = dispatch_nmer(list(ids))
+    blocks = [np.asarray(x, np.float64).reshape(nm, -1) for x in xyzs]
+    if name is None:
+        return 0.0, [np.zeros_like(b) for b in blocks], np.zeros(9)
+    xyz = np.concatenate([blocks[o] for o in order], axis=1)
+    e, g, vir, _ = holder_eval(name, xyz, do_grads)
+    grads = [None] * len(ids)
+    off = 0
+    for o in order:
+        w = blocks[o].shape[1]
+        grads[o] = g[:, off:off + w] if do_grads else np.zeros_like(blocks[o])
+        off += w
+    return e, grads, vir
 
 
 class OracleSystem:
@@ -294,7 +294,6 @@ class OracleSystem:
         t = self.top
         sites = self.sites.reshape(-1, 3)
         inv = invert_box(self.box) if self.box is not None else None
-        dispatch = DISPATCH_2B if nbody == 2 else DISPATCH_3B
         ignore = self.ignore_2b if nbody == 2 else self.ignore_3b
         etot = 0.0
         if len(nm) == 0:
@@ -306,8 +305,7 @@ class OracleSystem:
             types = tuple(t.type_order[c] for c in key)
             if sorted(types) in ignore:
                 continue
-            slots = _sorted_slots(types)
-            name = dispatch.get(tuple(types[s] for s in slots))
+            name, slots = dispatch_nmer(list(types))
             if name is None:
                 continue
             sel = nm[inverse == g]

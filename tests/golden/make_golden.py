@@ -1,0 +1,144 @@
+#!/usr/bin/env python3
+"""Extract the reference's golden vectors for the 2b/3b path into JSON fixtures.
+
+Reads the reference's own Catch2 unit tests and timing fixtures (from a
+reference checkout, default /root/reference) and writes ``tests/golden/*.json``:
+
+* evaluator / dispatch goldens: ``unittest-energy2b.cpp`` (h2o-h2o :48-97,
+  ch4-ch4 :314-360, ch4-h2o :361-427), ``unittest-energy3b.cpp`` (h2o x3
+  :48-145, ch4-h2o-h2o :472-571), ``unittest-poly-holder-2b.cpp``
+  (x2b_A1B2Z2_C1D4_v1x :659-706, x2b_A1B4_A1B4_v1x :935-974,
+  x2b_v9x :975-1018), ``unittest-poly-holder-3b.cpp`` (mbnrg_3b_A1B4_C1D2_C1D2
+  :337-383, x3b-v2x :910-954);
+* polynomial goldens: ``unittest-poly-2b.cpp`` (poly_2b_v6x :2537-3012,
+  poly_2b_A1B2Z2_C1D4_deg3_exp0_v1x :1581-1827, poly_2b_A1B4_A1B4_deg4_exp0_v1x
+  :1828-2326), ``unittest-poly-3b.cpp`` (poly_3b_A1B4_C1D2_C1D2_deg3_v1
+  :879-1349, poly-3b-v2x :1720-2160);
+* system fixtures: the coordinates of ``timing/256_h2o_cubic_box`` and
+  ``timing/57_ch4_513_h2o_rectangular`` with their published E2B/E3B
+  (``timing/*/output:5-6``) and configuration (``mbx.json``).
+
+Every array is copied verbatim (as numbers); nothing else of the reference is
+kept.  Run: ``python tests/golden/make_golden.py [--ref /root/reference]``.
+"""
+import argparse
+import json
+import os
+import re
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+BLOCKS = [
+    # (fixture name, file, header regex)
+    ("energy2b_h2o_h2o", "src/unittests/unittest-energy2b.cpp", r'TEST_CASE\("energy2b::get_2b_energy"\)', r'SECTION\("h2o-h2o"\)'),
+    ("energy2b_ch4_ch4", "src/unittests/unittest-energy2b.cpp", r'TEST_CASE\("energy2b::get_2b_energy"\)', r'SECTION\("ch4-ch4"\)'),
+    ("energy2b_ch4_h2o", "src/unittests/unittest-energy2b.cpp", r'TEST_CASE\("energy2b::get_2b_energy"\)', r'SECTION\("ch4-h2o"\)'),
+    ("energy3b_h2o_h2o_h2o", "src/unittests/unittest-energy3b.cpp", r'TEST_CASE', r'SECTION\("h2o-h2o-h2o"\)'),
+    ("energy3b_ch4_h2o_h2o", "src/unittests/unittest-energy3b.cpp", r'TEST_CASE', r'SECTION\("ch4-h2o-h2o"\)'),
+    ("holder2b_x2b_v9x", "src/unittests/unittest-poly-holder-2b.cpp", r'TEST_CASE\("x2b_v9x::struct"\)', None),
+    ("holder2b_ch4_h2o", "src/unittests/unittest-poly-holder-2b.cpp", r'TEST_CASE\("x2b_A1B2Z2_C1D4_v1x::struct"\)', None),
+    ("holder2b_ch4_ch4", "src/unittests/unittest-poly-holder-2b.cpp", r'TEST_CASE\("x2b_A1B4_A1B4_v1x::struct"\)', None),
+    ("holder3b_x3b_v2x", "src/unittests/unittest-poly-holder-3b.cpp", r'TEST_CASE\("x3b-v2x::class"\)', None),
+    ("holder3b_ch4_h2o_h2o", "src/unittests/unittest-poly-holder-3b.cpp", r'TEST_CASE\("mbnrg_3b_A1B4_C1D2_C1D2_deg3_v1::class"\)', None),
+    ("poly_mbpol2b", "src/unittests/unittest-poly-2b.cpp", r'TEST_CASE\(":poly_2b_v6x:struct"\)', None),
+    ("poly_ch4h2o2b", "src/unittests/unittest-poly-2b.cpp", r'TEST_CASE\(":poly_2b_A1B2Z2_C1D4_deg3_exp0_v1x:struct"\)', None),
+    ("poly_ch4ch42b", "src/unittests/unittest-poly-2b.cpp", r'TEST_CASE\("poly_2b_A1B4_A1B4_deg4_exp0_v1x:struct"\)', None),
+    ("poly_ch4h2o3b", "src/unittests/unittest-poly-3b.cpp", r'TEST_CASE\("poly_3b_A1B4_C1D2_C1D2_deg3_v1.h"\)', None),
+    ("poly_mbpol3b", "src/unittests/unittest-poly-3b.cpp", r'TEST_CASE\("poly-3b-v2x::class"\)', None),
+]
+
+SYSTEMS = [
+    ("system_256_h2o_cubic_box", "timing/256_h2o_cubic_box"),
+    ("system_57_ch4_513_h2o", "timing/57_ch4_513_h2o_rectangular"),
+]
+
+
+def strip_comments(text):
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return re.sub(r"//[^\n]*", "", text)
+
+
+def block_after(text, header, start=0):
+    m = re.compile(header).search(text, start)
+    if not m:
+        raise ValueError("header %s not found" % header)
+    i = text.index("{", m.end())
+    depth, j = 1, i + 1
+    while depth:
+        depth += (text[j] == "{") - (text[j] == "}")
+        j += 1
+    return m.start(), text[i + 1:j - 1]
+
+
+def parse_block(body):
+    out = {}
+    for m in re.finditer(r"std::vector<double>\s+(\w+)\s*=\s*\{([^}]*)\}\s*;", body):
+        out[m.group(1)] = [float(v) for v in m.group(2).replace(",", " ").split()]
+    for m in re.finditer(r"std::vector<double>\s+(\w+)\s*\(\s*([^)]*)\)\s*;", body):
+        out.setdefault(m.group(1) + "__size", m.group(2).strip())
+    for m in re.finditer(r"(?<![\w:])double\s+(\w+)\s*=\s*([-+0-9.eE]+)\s*;", body):
+        out[m.group(1)] = float(m.group(2))
+    for m in re.finditer(r"std::string\s+(\w+)\s*=\s*\"([^\"]*)\"\s*;", body):
+        out[m.group(1)] = m.group(2)
+    for m in re.finditer(r"(?:size_t|int)\s+(\w+)\s*=\s*(\d+)\s*;", body):
+        out[m.group(1)] = int(m.group(2))
+    return out
+
+
+def extract_blocks(ref):
+    for name, rel, case, section in BLOCKS:
+        text = strip_comments(open(os.path.join(ref, rel)).read())
+        pos, body = block_after(text, case)
+        if section:
+            _, body = block_after(body, section)
+        data = parse_block(body)
+        data["_source"] = rel
+        with open(os.path.join(HERE, name + ".json"), "w") as f:
+            json.dump(data, f)
+        print(name, sorted(k for k in data if not k.startswith("_")))
+
+
+def read_nrg(path):
+    ids, xyz = [], []
+    for line in open(path):
+        w = line.split()
+        if not w:
+            continue
+        if w[0].upper() == "MONOMER":
+            ids.append(w[1])
+        elif len(w) == 4 and w[0].isalpha() and w[0].upper() not in ("SYSTEM", "MOLECULE"):
+            try:
+                xyz += [float(v) for v in w[1:]]
+            except ValueError:
+                pass
+    return ids, xyz
+
+
+def extract_systems(ref):
+    for name, rel in SYSTEMS:
+        ids, xyz = read_nrg(os.path.join(ref, rel, "input.nrg"))
+        cfg = json.load(open(os.path.join(ref, rel, "mbx.json")))["MBX"]
+        out = {}
+        for line in open(os.path.join(ref, rel, "output")):
+            m = re.match(r"\s*(2B|3B)\s*=\s*([-+0-9.eE]+)", line)
+            if m:
+                out[m.group(1)] = float(m.group(2))
+        data = {"ids": ids, "xyz": xyz, "box": cfg.get("box", []), "cutoff2b": cfg["twobody_cutoff"],
+                "cutoff3b": cfg["threebody_cutoff"], "ignore_2b": cfg.get("ignore_2b_poly", []),
+                "ignore_3b": cfg.get("ignore_3b_poly", []), "E2B": out["2B"], "E3B": out["3B"],
+                "_source": rel}
+        with open(os.path.join(HERE, name + ".json"), "w") as f:
+            json.dump(data, f)
+        print(name, len(ids), "monomers", data["E2B"], data["E3B"])
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default="/root/reference")
+    a = ap.parse_args()
+    extract_blocks(a.ref)
+    extract_systems(a.ref)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,274 @@
+"""CUDA path against the oracle and the reference's golden vectors (GPU).
+
+Tolerances (north star): FP64 path energies within 1e-10 relative and
+gradients within 1e-8 kcal/mol/A of the FP64 oracle; mixed path energies
+within 1e-6 relative.  n-mer lists must be identical after canonicalisation.
+"""
+import numpy as np
+import pytest
+
+import mbx_oracle as mo
+from conftest import golden
+from mbx_b200 import system as msys, workloads
+from mbx_b200.specs import SPECS
+from mbx_b200.tables import load_fit
+
+pytestmark = pytest.mark.gpu
+
+E_REL = 1e-10
+G_ABS = 1e-8
+MIXED_REL = 1e-6
+
+
+def canon(nm):
+    nm = np.sort(np.asarray(nm, np.int64), axis=1)
+    return nm[np.lexsort(nm.T[::-1])] if len(nm) else nm
+
+
+def rel(a, b):
+    return abs(a - b) / max(abs(b), 1e-300)
+
+
+# ------------------------------------------------------------------ polynomials
+STRAIGHT = ["mbpol2b", "mbpol3b", "ch4h2o2b", "ch4h2o3b"]
+
+
+@pytest.mark.parametrize("name", STRAIGHT)
+def test_poly_random_vs_oracle(ctx, name):
+    nv = SPECS[name].nvars
+    rng = np.random.default_rng(7)
+    nd = 257
+    x = rng.uniform(0.05, 1.2, size=(nv, nd))
+    g = np.zeros((nv, nd))
+    e = ctx.poly(name, np.ascontiguousarray(x), g)
+    a = load_fit(name)
+    for i in range(0, nd, 37):
+        eo, go = mo.pip_eval(name, a, x[:, i])
+        assert rel(e[i], eo) < 1e-12 or abs(e[i] - eo) < 1e-12
+        np.testing.assert_allclose(g[:, i], go, rtol=1e-11, atol=1e-11)
+
+
+@pytest.mark.parametrize("fixture,name", [("poly_mbpol2b", "mbpol2b"), ("poly_ch4h2o2b", "ch4h2o2b"),
+                                          ("poly_ch4h2o3b", "ch4h2o3b"), ("poly_mbpol3b", "mbpol3b")])
+def test_poly_golden(ctx, fixture, name):
+    gd = golden(fixture)
+    nv = SPECS[name].nvars
+    x = np.array(gd["x"])
+    x = x.reshape(nv, -1)[:, 0] if len(x) != nv else x
+    ctx.set_coefficients(name, np.array(gd["a"]))
+    try:
+        g = np.zeros((nv, 1))
+        e = ctx.poly(name, np.ascontiguousarray(x.reshape(nv, 1)), g)
+    finally:
+        ctx.set_coefficients(name, None)
+    gexp = np.array(gd["g_expected"])
+    gexp = gexp.reshape(nv, -1)[:, 0] if len(gexp) != nv else gexp
+    e_exp = gd["e_expected"][0] if isinstance(gd["e_expected"], list) else gd["e_expected"]
+    assert abs(e[0] - e_exp) < 1e-8 * max(1, abs(e_exp))
+    np.testing.assert_allclose(g[:, 0], gexp, rtol=1e-8, atol=1e-8)
+
+
+# ------------------------------------------------------------------ evaluators
+HOLDERS = [("holder2b_x2b_v9x", "mbpol2b"), ("holder2b_ch4_h2o", "ch4h2o2b"), ("holder2b_ch4_ch4", "ch4ch42b"),
+           ("holder3b_x3b_v2x", "mbpol3b"), ("holder3b_ch4_h2o_h2o", "ch4h2o3b")]
+
+
+@pytest.mark.parametrize("fixture,name", HOLDERS)
+def test_evaluator_golden(ctx, fixture, name):
+    gd = golden(fixture)
+    s = SPECS[name]
+    n = gd.get("ndim", gd.get("ntrim"))
+    blocks = [np.array(gd["xyz%d" % (i + 1)]).reshape(n, -1) for i in range(s.nbody)]
+    xyz = np.ascontiguousarray(np.concatenate(blocks, axis=1))
+    grad = np.zeros_like(xyz)
+    vir = np.zeros(9)
+    e = ctx.evaluate(name, xyz, grad, vir)
+    eo, go, vo, _ = mo.holder_eval(name, xyz)
+    assert abs(e - gd["energy_expected"]) < 1e-6
+    assert rel(e, eo) < E_REL or abs(e - eo) < 1e-12
+    np.testing.assert_allclose(grad, go, rtol=0, atol=G_ABS)
+    np.testing.assert_allclose(vir, vo, rtol=1e-10, atol=G_ABS)
+    off = 0
+    for i in range(s.nbody):
+        w = blocks[i].shape[1]
+        np.testing.assert_allclose(grad[:, off:off + w].reshape(-1), gd["grad%d_expected" % (i + 1)], atol=1e-6)
+        off += w
+
+
+def random_nmers(name, n, seed=3):
+    """Gas-phase n-mers of the evaluator's types spanning its cutoff."""
+    s = SPECS[name]
+    rng = np.random.default_rng(seed)
+    bodies = {"h2o": workloads.water_body(), "ch4": workloads.methane_body()}
+    out = []
+    for _ in range(n):
+        parts = []
+        centre0 = np.zeros(3)
+        for k, m in enumerate(s.monomers):
+            c = centre0 if k == 0 else workloads._random_directions(rng, 1)[0] * rng.uniform(2.4, s.rf + 0.5)
+            parts.append(workloads.place(rng, bodies[m], c[None, :])[0].reshape(-1))
+        out.append(np.concatenate(parts))
+    return np.ascontiguousarray(np.array(out))
+
+
+@pytest.mark.parametrize("name", list(SPECS))
+def test_evaluator_random_vs_oracle(ctx, name):
+    n = 64 if name == "ch4ch42b" else 512
+    xyz = random_nmers(name, n)
+    grad = np.zeros_like(xyz)
+    vir = np.zeros(9)
+    eper = np.zeros(n)
+    e = ctx.evaluate(name, xyz, grad, vir, eper)
+    eo, go, vo, epo = mo.holder_eval(name, xyz, per_nmer=True)
+    assert rel(e, eo) < E_REL
+    np.testing.assert_allclose(eper, epo, rtol=1e-10, atol=1e-12)
+    np.testing.assert_allclose(grad, go, rtol=0, atol=G_ABS)
+    np.testing.assert_allclose(vir, vo, rtol=1e-9, atol=1e-8)
+
+
+@pytest.mark.parametrize("name", ["mbpol2b", "mbpol3b", "ch4h2o2b", "ch4h2o3b"])
+def test_evaluator_mixed(ctx, name):
+    xyz = random_nmers(name, 512, seed=11)
+    grad = np.zeros_like(xyz)
+    eper = np.zeros(len(xyz))
+    e = ctx.evaluate(name, xyz, grad, None, eper, mixed=True)
+    eo, go, _, epo = mo.holder_eval(name, xyz, per_nmer=True)
+    assert rel(e, eo) < MIXED_REL
+    scale = np.abs(go).max()
+    assert np.abs(grad - go).max() < 1e-5 * scale
+
+
+@pytest.mark.parametrize("name", ["mbpol2b", "mbpol3b", "ch4h2o2b", "ch4h2o3b"])
+def test_dcoef_vs_oracle(ctx, name):
+    xyz = random_nmers(name, 96, seed=5)
+    w = np.random.default_rng(1).normal(size=len(xyz))
+    out = ctx.evaluate_dcoef(name, xyz, w)
+    ref = (mo.holder_dcoef(name, xyz) * w[:, None]).sum(0)
+    np.testing.assert_allclose(out, ref, rtol=1e-9, atol=1e-9 * np.abs(ref).max())
+
+
+# ------------------------------------------------------------------ systems
+def compare_system(ids, xyz, box, c2, c3, ig2=(), ig3=(), mixed=False, lists=True):
+    o = mo.OracleSystem(ids, xyz, box, c2, c3, ig2, ig3)
+    g = msys.from_arrays(ids, xyz, box, c2, c3, ig2, ig3, precision="mixed" if mixed else "fp64")
+    for nb in (2, 3):
+        eo = o.energy(nb)
+        go = o.real_grads()
+        vo = o.virial.copy()
+        e = g.TwoBodyEnergy(True) if nb == 2 else g.ThreeBodyEnergy(True)
+        gr = g.GetRealGrads()
+        vr = g.GetVirial()
+        if mixed:
+            assert rel(e, eo) < MIXED_REL, (nb, e, eo)
+        else:
+            assert rel(e, eo) < E_REL, (nb, e, eo)
+            np.testing.assert_allclose(gr, go, rtol=0, atol=G_ABS)
+            np.testing.assert_allclose(vr, vo, rtol=1e-9, atol=1e-7)
+        if lists:
+            cut = c2 if nb == 2 else c3
+            assert np.array_equal(canon(g.GetPairList(nb, cut)), o.top.nmers_to_input(o.nmers(nb))), nb
+            listed, _ = g.NmerCounts(nb)
+            assert listed == len(o.nmers(nb))
+    return g
+
+
+def test_water_256_fp64():
+    ids, xyz, box = workloads.water_256(0)
+    compare_system(ids, xyz, box, 9.0, 7.0)
+
+
+def test_water_256_mixed():
+    ids, xyz, box = workloads.water_256(0)
+    compare_system(ids, xyz, box, 9.0, 7.0, mixed=True, lists=False)
+
+
+@pytest.mark.parametrize("fixture", ["system_256_h2o_cubic_box", "system_57_ch4_513_h2o"])
+def test_published_fixtures(fixture):
+    gd = golden(fixture)
+    g = compare_system(gd["ids"], np.array(gd["xyz"]), gd["box"] or None, gd["cutoff2b"], gd["cutoff3b"],
+                       gd["ignore_2b"], gd["ignore_3b"])
+    e2 = g.TwoBodyEnergy(False)
+    e3 = g.ThreeBodyEnergy(False)
+    assert abs(e2 - gd["E2B"]) < 1e-9 * abs(gd["E2B"]) + 1e-8
+    assert abs(e3 - gd["E3B"]) < 1e-9 * abs(gd["E3B"]) + 1e-8
+
+
+def test_methane_water_box():
+    ids, xyz, box = workloads.methane_water_box(seed=0)
+    compare_system(ids, xyz, box, 9.0, 7.0)
+
+
+def test_gas_phase_cluster():
+    ids, xyz = workloads.water_cluster(40, seed=2)
+    compare_system(ids, xyz, None, 9.0, 7.0)
+
+
+def test_edge_cases(ctx):
+    # one monomer: no n-mers, zero energy
+    ids, xyz, box = workloads.water_256(0)
+    one = msys.from_arrays(ids[:1], xyz[:9], box, 9.0, 7.0)
+    assert one.TwoBodyEnergy(True) == 0.0 and one.ThreeBodyEnergy(True) == 0.0
+    # two monomers far apart: listed but not evaluated
+    far = np.concatenate([xyz[:9], xyz[:9] + np.array([8.0, 0, 0] * 3)])
+    s = msys.from_arrays(["h2o", "h2o"], far, box, 9.0, 7.0)
+    assert s.TwoBodyEnergy(True) == 0.0
+    assert s.NmerCounts(2) == (1, 0)
+    # cutoff beyond half the box: the reference assumes it never happens; here it is an error
+    with pytest.raises(msys.CUException):
+        msys.from_arrays(ids, xyz, box, 11.0, 7.0)
+    # ignored type tuples contribute nothing
+    ig = msys.from_arrays(ids, xyz, box, 9.0, 7.0, ignore_3b=[["h2o", "h2o", "h2o"]])
+    assert ig.ThreeBodyEnergy(True) == 0.0
+    assert ig.NmerCounts(3)[0] > 0
+
+
+def test_ghost_monomers():
+    """use_ghost: ghosts join the search, only n-mers owned by a local monomer count."""
+    ids, xyz, box = workloads.water_256(0)
+    is_local = np.ones(len(ids), int)
+    is_local[::3] = 0
+    o = mo.OracleSystem(ids, xyz, box, 9.0, 7.0, is_local=is_local)
+    g = msys.System()
+    names = ["O", "H", "H"]
+    for i in range(len(ids)):
+        g.AddMonomer(xyz[9 * i:9 * i + 9], names, "h2o", int(is_local[i]))
+        g.AddMolecule([i])
+    g.Initialize()
+    g.SetUpFromJson({"MBX": {"box": list(box), "twobody_cutoff": 9.0, "threebody_cutoff": 7.0}})
+    for nb in (2, 3):
+        eo = o.energy(nb, use_ghost=True)
+        e = g.TwoBodyEnergy(True, True) if nb == 2 else g.ThreeBodyEnergy(True, True)
+        assert rel(e, eo) < E_REL
+        np.testing.assert_allclose(g.GetRealGrads(), o.real_grads(), atol=G_ABS)
+
+
+def test_water_2048_full_size():
+    """The bench workload at full size: lists equal to the oracle's, energies to the reference."""
+    ids, xyz, box = workloads.water_2048(0)
+    g = msys.from_arrays(ids, xyz, box, 9.0, 7.0)
+    o = mo.OracleSystem(ids, xyz, box, 9.0, 7.0)
+    for nb in (2, 3):
+        cut = 9.0 if nb == 2 else 7.0
+        assert np.array_equal(canon(g.GetPairList(nb, cut)), o.top.nmers_to_input(o.nmers(nb)))
+    e2 = g.TwoBodyEnergy(True)
+    g2 = g.GetRealGrads()
+    e3 = g.ThreeBodyEnergy(True)
+    g3 = g.GetRealGrads()
+    if mo.RefSystem.available():
+        r = mo.RefSystem(ids, xyz, box, 9.0, 7.0)
+        r2 = r.energy(2)
+        rg2 = r.real_grads()
+        r3 = r.energy(3)
+        rg3 = r.real_grads()
+    else:
+        r2 = o.energy(2)
+        rg2 = o.real_grads()
+        r3 = o.energy(3)
+        rg3 = o.real_grads()
+    assert rel(e2, r2) < E_REL and rel(e3, r3) < 1e-9
+    np.testing.assert_allclose(g2, rg2, atol=G_ABS)
+    np.testing.assert_allclose(g3, rg3, atol=G_ABS)
+    # mixed precision on the same box
+    m = msys.from_arrays(ids, xyz, box, 9.0, 7.0, precision="mixed")
+    assert rel(m.TwoBodyEnergy(True), r2) < MIXED_REL
+    assert rel(m.ThreeBodyEnergy(True), r3) < MIXED_REL

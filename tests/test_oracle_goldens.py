@@ -1,0 +1,106 @@
+"""The oracle restatement against the reference's own golden vectors (CPU)."""
+import numpy as np
+import pytest
+
+import mbx_oracle as mo
+from conftest import golden
+from mbx_b200.tables import load_fit, load_pip
+from mbx_b200.specs import SPECS, check
+
+# the reference's unit tests use an absolute margin of 1e-6
+# (unittest-energy2b.cpp:45, tools/testutils.h:46-54); this oracle must do better
+TOL = 1e-8
+
+
+def test_specs_consistent():
+    assert check()
+    for name, s in SPECS.items():
+        t = load_pip(name)
+        assert t.nvars == s.nvars and t.ncoef == s.ncoef
+        assert len(load_fit(name)) == s.ncoef
+
+
+POLY = [("poly_mbpol2b", "mbpol2b"), ("poly_ch4h2o2b", "ch4h2o2b"), ("poly_ch4ch42b", "ch4ch42b"),
+        ("poly_ch4h2o3b", "ch4h2o3b"), ("poly_mbpol3b", "mbpol3b")]
+
+
+@pytest.mark.parametrize("fixture,name", POLY)
+def test_poly_golden(fixture, name):
+    g = golden(fixture)
+    nv = SPECS[name].nvars
+    a = np.array(g["a"])
+    x = np.array(g["x"])
+    if name == "mbpol3b":
+        x = x.reshape(nv, -1)[:, 0] if len(x) != nv else x   # 8-lane API, lane 0
+    if name == "mbpol2b":
+        e, gr = mo.pip_eval(name, a, x)
+    else:
+        e, gr = mo.pip_eval(name, a, x[:nv])
+    e_exp = g["e_expected"][0] if isinstance(g["e_expected"], list) else g["e_expected"]
+    assert abs(e - e_exp) < TOL * max(1.0, abs(e_exp))
+    gexp = np.array(g["g_expected"])
+    if name == "mbpol3b" and len(gexp) != nv:
+        gexp = gexp.reshape(nv, -1)[:, 0]
+    np.testing.assert_allclose(gr, gexp[:nv], rtol=1e-8, atol=TOL)
+
+
+def test_poly_mbpol2b_two_configs():
+    g = golden("poly_mbpol2b")
+    a = np.array(g["a"])
+    x2 = np.array(g["x_2"]).reshape(31, 2)   # variable-major, nd = 2
+    gexp = np.array(g["g_2_expected"]).reshape(31, 2)
+    for i in range(2):
+        e, gr = mo.pip_eval("mbpol2b", a, x2[:, i])
+        assert abs(e - g["e_2_expected"][i]) < TOL * max(1.0, abs(e))
+        np.testing.assert_allclose(gr, gexp[:, i], rtol=1e-8, atol=TOL)
+
+
+DISPATCH = ["energy2b_h2o_h2o", "energy2b_ch4_ch4", "energy2b_ch4_h2o", "energy3b_h2o_h2o_h2o",
+            "energy3b_ch4_h2o_h2o"]
+
+
+@pytest.mark.parametrize("fixture", DISPATCH)
+def test_dispatch_golden(fixture):
+    g = golden(fixture)
+    nb = 3 if "xyz3" in g else 2
+    ids = [g["mon%d" % (i + 1)] for i in range(nb)]
+    xyzs = [np.array(g["xyz%d" % (i + 1)]) for i in range(nb)]
+    e, grads, vir = mo.get_nb_energy(ids, xyzs, g["nm"])
+    assert abs(e - g["energy_expected"]) < 1e-6   # the golden is printed to 11 digits
+    for i in range(nb):
+        np.testing.assert_allclose(grads[i].reshape(-1), g["grad%d_expected" % (i + 1)], rtol=1e-7, atol=1e-6)
+    np.testing.assert_allclose(vir, g["virial_expected"], rtol=1e-7, atol=1e-6)
+
+
+HOLDERS = [("holder2b_x2b_v9x", "mbpol2b"), ("holder2b_ch4_h2o", "ch4h2o2b"), ("holder2b_ch4_ch4", "ch4ch42b"),
+           ("holder3b_x3b_v2x", "mbpol3b"), ("holder3b_ch4_h2o_h2o", "ch4h2o3b")]
+
+
+@pytest.mark.parametrize("fixture,name", HOLDERS)
+def test_holder_golden(fixture, name):
+    g = golden(fixture)
+    s = SPECS[name]
+    n = g.get("ndim", g.get("ntrim"))
+    blocks = [np.array(g["xyz%d" % (i + 1)]).reshape(n, -1) for i in range(s.nbody)]
+    xyz = np.concatenate(blocks, axis=1)
+    e, grad, vir, _ = mo.holder_eval(name, xyz)
+    assert abs(e - g["energy_expected"]) < 1e-6
+    off = 0
+    for i in range(s.nbody):
+        w = blocks[i].shape[1]
+        np.testing.assert_allclose(grad[:, off:off + w].reshape(-1), g["grad%d_expected" % (i + 1)], rtol=1e-7,
+                                   atol=1e-6)
+        off += w
+    np.testing.assert_allclose(vir, g["virial_expected"], rtol=1e-7, atol=1e-6)
+
+
+@pytest.mark.parametrize("fixture", ["system_256_h2o_cubic_box", "system_57_ch4_513_h2o"])
+def test_system_published_energies(fixture):
+    """timing/*/output holds E2B and E3B to 11 significant digits."""
+    g = golden(fixture)
+    s = mo.OracleSystem(g["ids"], np.array(g["xyz"]), g["box"] or None, g["cutoff2b"], g["cutoff3b"],
+                        g["ignore_2b"], g["ignore_3b"])
+    e2 = s.energy(2, do_grads=False)
+    e3 = s.energy(3, do_grads=False)
+    assert abs(e2 - g["E2B"]) < 1e-10 * abs(g["E2B"]) + 1e-9 * 10
+    assert abs(e3 - g["E3B"]) < 1e-9 * abs(g["E3B"]) + 1e-8
