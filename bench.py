@@ -177,6 +177,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision leg")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -244,9 +245,12 @@ def main():
     with Clocks(local) as clk:
         t64, ev64, launches, (e2_64, e3_64) = timed(False)
     clocks = clk.summary()
-    for _ in range(args.warmup):
-        step(True)
-    tmx, evmx, launches_mx, (e2_mx, e3_mx) = timed(True)
+    if not args.no_mixed:
+        for _ in range(args.warmup):
+            step(True)
+        tmx, evmx, launches_mx, (e2_mx, e3_mx) = timed(True)
+    else:
+        tmx, e2_mx, e3_mx = list(t64), e2_64, e3_64
 
     ms = sum(t64) / len(t64)
     ms_mx = sum(tmx) / len(tmx)

