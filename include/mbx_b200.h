@@ -116,7 +116,8 @@ int mbx_evaluator_info(const char* evaluator, int* nbody, int* nreal, int* nvars
 int mbx_last_timing(const mbx_ctx* ctx, double* ms_build, double* ms_eval, int* kernels);
 
 /* Measured FMA-pipe throughput of the device (results[0] FP64, results[1]
- * FP32, TFLOP/s): the roofline denominators for the polynomial kernels. */
+ * FP32, results[2] FP32 issued as paired fma.rn.f32x2; TFLOP/s): the
+ * roofline denominators for the polynomial kernels.  results has 3 slots. */
 int mbx_fma_peaks(int device, double* results);
 
 #ifdef __cplusplus

@@ -73,11 +73,11 @@ def evaluator_info(name):
 
 
 def fma_peaks(device=0):
-    r = (ctypes.c_double * 2)()
+    r = (ctypes.c_double * 3)()
     code = lib().mbx_fma_peaks(device, r)
     if code:
         raise MBXError(code, "fma peak benchmark failed")
-    return {"fp64_tflops": r[0], "fp32_tflops": r[1]}
+    return {"fp64_tflops": r[0], "fp32_tflops": r[1], "fp32x2_tflops": r[2]}
 
 
 def _ptr(a):

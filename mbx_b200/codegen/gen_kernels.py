@@ -102,135 +102,192 @@ def coef_expr(coefs, fp32=False):
     return " + ".join(parts) if parts else None
 
 
-def emit_pip(trie, nvars, name, out):
-    """FP64 value + gradient: double name(const double* x, double* g)."""
-    w = out.append
-    w("// %s: polynomial and reverse-mode gradient (multivariate Horner trie)" % name)
-    w("template <class Coef>")
-    w("__device__ __forceinline__ double %s(const Coef& coef, const double (&x)[%d], double (&g)[%d]) {" %
-      (name, nvars, nvars))
-    w("    double E = 0.0;")
+def subtree_size(n):
+    return 1 + sum(subtree_size(c) for c in n["kids"].values())
 
-    def node(n, var, depth, pexpr):
-        # pexpr: expression for P(parent), None at the root's children (P = 1)
-        P = "P%d" % depth
-        V = "V%d" % depth
-        if pexpr is None:
-            w("    { const double %s = x[%d];" % (P, var))
-        else:
-            w("    { const double %s = %s * x[%d];" % (P, pexpr, var))
-        ce = coef_expr(n["coef"])
-        w("      double %s = %s;" % (V, ce if ce else "0.0"))
-        for cv, ch in n["kids"].items():
+
+def partition(trie, nparts):
+    """Top-level subtrees split into nparts groups of similar size (greedy)."""
+    kids = sorted(trie.root["kids"].items(), key=lambda kv: -subtree_size(kv[1]))
+    nparts = max(1, min(nparts, len(kids)))
+    parts = [[] for _ in range(nparts)]
+    load = [0] * nparts
+    for var, ch in kids:
+        i = load.index(min(load))
+        parts[i].append((var, ch))
+        load[i] += subtree_size(ch)
+    return [p for p in parts if p]
+
+
+def parts_for(nterms):
+    """Number of separately compiled pieces: one per ~4500 terms.  A single
+    straight-line function of 10^4-10^5 FMAs leaves the register allocator
+    with live ranges it cannot fit in 255 registers (kilobytes of spills);
+    pieces of this size compile with next to none."""
+    return max(1, (nterms + 4499) // 4500)
+
+
+def emit_split(trie, nvars, name, out, nparts, arrays, body, ret="double"):
+    """Emits name_partK as __noinline__ functions over pointers to the
+    caller's arrays and a __forceinline__ name() that calls them in turn.
+
+    arrays: [(name, ctype, role)] with role "in" (read: copied into a local
+    register array on entry) or "acc" (accumulated: zeroed locally, added to
+    the caller's array on exit).  body(w, subtrees) writes the evaluation of
+    the subtrees into the local arrays and into E."""
+    import re
+    w = out.append
+    pieces = partition(trie, nparts)
+    for i, sub in enumerate(pieces):
+        text = []
+        body(text.append, sub)
+        code = "\n".join(text)
+        params = ", ".join("%s%s* __restrict__ %sm" % ("const " if role == "in" else "", ct, a)
+                           for a, ct, role in arrays)
+        w("template <class Coef>")
+        w("__device__ __noinline__ %s %s_part%d(const Coef& coef, %s) {" % (ret, name, i, params))
+        for a, ct, role in arrays:
+            used = sorted({int(v) for v in re.findall(r"\b%s\[(\d+)\]" % a, code)})
+            w("    %s %s[%d];" % (ct, a, nvars))
+            for v in used:
+                w("    %s[%d] = %s;" % (a, v, ("%sm[%d]" % (a, v)) if role == "in" else
+                                        ("0.0f" if ct == "float" else "0.0")))
+        w("    %s E = 0.0;" % ret)
+        w(code)
+        for a, ct, role in arrays:
+            if role == "acc":
+                used = sorted({int(v) for v in re.findall(r"\b%s\[(\d+)\]" % a, code)})
+                for v in used:
+                    w("    %sm[%d] += %s[%d];" % (a, v, a, v))
+        w("    return E;")
+        w("}")
+    sig = ", ".join("%s%s (&%s)[%d]" % ("const " if role == "in" else "", ct, a, nvars) for a, ct, role in arrays)
+    w("template <class Coef>")
+    w("__device__ __forceinline__ %s %s(const Coef& coef, %s) {" % (ret, name, sig))
+    w("    %s E = 0.0;" % ret)
+    for i in range(len(pieces)):
+        w("    E += %s_part%d(coef, %s);" % (name, i, ", ".join(a for a, _, _ in arrays)))
+    w("    return E;")
+    w("}")
+
+
+def emit_pip(trie, nvars, name, out, nparts=1):
+    """FP64 value + gradient (multivariate Horner trie, reverse mode)."""
+    out.append("// %s: polynomial and reverse-mode gradient (multivariate Horner trie)" % name)
+
+    def body(w, subtrees):
+        def node(n, var, depth, pexpr):
+            # pexpr: expression for P(parent), None at the root's children (P = 1)
+            P = "P%d" % depth
+            V = "V%d" % depth
+            if pexpr is None:
+                w("    { const double %s = x[%d];" % (P, var))
+            else:
+                w("    { const double %s = %s * x[%d];" % (P, pexpr, var))
+            ce = coef_expr(n["coef"])
+            w("      double %s = %s;" % (V, ce if ce else "0.0"))
+            for cv, ch in n["kids"].items():
+                if ch["kids"]:
+                    node(ch, cv, depth + 1, P)
+                else:
+                    c = coef_expr(ch["coef"])
+                    w("      %s = fma(%s, x[%d], %s); g[%d] = fma(%s, %s, g[%d]);" % (V, c, cv, V, cv, c, P, cv))
+            if pexpr is None:
+                w("      g[%d] += %s; E = fma(x[%d], %s, E); }" % (var, V, var, V))
+            else:
+                w("      g[%d] = fma(%s, %s, g[%d]); V%d = fma(x[%d], %s, V%d); }" %
+                  (var, pexpr, V, var, depth - 1, var, V, depth - 1))
+
+        for var, ch in subtrees:
             if ch["kids"]:
-                node(ch, cv, depth + 1, P)
+                node(ch, var, 1, None)
             else:
                 c = coef_expr(ch["coef"])
-                w("      %s = fma(%s, x[%d], %s); g[%d] = fma(%s, %s, g[%d]);" % (V, c, cv, V, cv, c, P, cv))
-        if pexpr is None:
-            w("      g[%d] += %s; E = fma(x[%d], %s, E); }" % (var, V, var, V))
-        else:
-            w("      g[%d] = fma(%s, %s, g[%d]); V%d = fma(x[%d], %s, V%d); }" %
-              (var, pexpr, V, var, depth - 1, var, V, depth - 1))
+                w("    E = fma(%s, x[%d], E); g[%d] += %s;" % (c, var, var, c))
 
-    for var, ch in trie.root["kids"].items():
-        if ch["kids"]:
-            node(ch, var, 1, None)
-        else:
-            c = coef_expr(ch["coef"])
-            w("    E = fma(%s, x[%d], E); g[%d] += %s;" % (c, var, var, c))
-    w("    return E;")
-    w("}")
+    emit_split(trie, nvars, name, out, nparts, [("x", "double", "in"), ("g", "double", "acc")], body)
 
 
-def emit_pip_energy(trie, nvars, name, out):
+def emit_pip_energy(trie, nvars, name, out, nparts=1):
     """FP64 value only: plain Horner over the trie."""
-    w = out.append
-    w("template <class Coef>")
-    w("__device__ __forceinline__ double %s(const Coef& coef, const double (&x)[%d]) {" % (name, nvars))
-    w("    double E = 0.0;")
+    def body(w, subtrees):
+        def node(n, var, depth):
+            V = "V%d" % depth
+            ce = coef_expr(n["coef"])
+            w("    { double %s = %s;" % (V, ce if ce else "0.0"))
+            for cv, ch in n["kids"].items():
+                if ch["kids"]:
+                    node(ch, cv, depth + 1)
+                else:
+                    w("      %s = fma(%s, x[%d], %s);" % (V, coef_expr(ch["coef"]), cv, V))
+            tgt = "E" if depth == 1 else "V%d" % (depth - 1)
+            w("      %s = fma(x[%d], %s, %s); }" % (tgt, var, V, tgt))
 
-    def node(n, var, depth):
-        V = "V%d" % depth
-        ce = coef_expr(n["coef"])
-        w("    { double %s = %s;" % (V, ce if ce else "0.0"))
-        for cv, ch in n["kids"].items():
+        for var, ch in subtrees:
             if ch["kids"]:
-                node(ch, cv, depth + 1)
+                node(ch, var, 1)
             else:
-                w("      %s = fma(%s, x[%d], %s);" % (V, coef_expr(ch["coef"]), cv, V))
-        tgt = "E" if depth == 1 else "V%d" % (depth - 1)
-        w("      %s = fma(x[%d], %s, %s); }" % (tgt, var, V, tgt))
+                w("    E = fma(%s, x[%d], E);" % (coef_expr(ch["coef"]), var))
 
-    for var, ch in trie.root["kids"].items():
-        if ch["kids"]:
-            node(ch, var, 1)
-        else:
-            w("    E = fma(%s, x[%d], E);" % (coef_expr(ch["coef"]), var))
-    w("    return E;")
-    w("}")
+    emit_split(trie, nvars, name, out, nparts, [("x", "double", "in")], body)
 
 
-def emit_pip_mixed(trie, nvars, name, out):
+def emit_pip_mixed(trie, nvars, name, out, nparts=1):
     """Mixed precision: products and leaf-level sums in FP32, everything that
     accumulates across leaf groups (inner-node values, the energy) in FP64.
 
     Leaf gradient contributions go to FP32 accumulators gf[] (each receives one
     product per leaf); inner-node gradient contributions go to FP64 g[].  The
     caller adds gf into g at the end."""
-    w = out.append
-    w("template <class Coef>")
-    w("__device__ __forceinline__ double %s(const Coef& coef, const float (&xf)[%d], const double (&x)[%d], "
-      "double (&g)[%d], float (&gf)[%d]) {" % (name, nvars, nvars, nvars, nvars))
-    w("    double E = 0.0;")
+    def body(w, subtrees):
+        def node(n, var, depth, pexpr_f, pexpr_d):
+            Pf = "Pf%d" % depth
+            Pd = "Pd%d" % depth
+            leaf_only = all(not ch["kids"] for ch in n["kids"].values())
+            if pexpr_f is None:
+                w("    { const float %s = xf[%d];" % (Pf, var))
+                if not leaf_only:
+                    w("      const double %s = x[%d];" % (Pd, var))
+            else:
+                w("    { const float %s = %s * xf[%d];" % (Pf, pexpr_f, var))
+                if not leaf_only:
+                    w("      const double %s = %s * x[%d];" % (Pd, pexpr_d, var))
+            if leaf_only:
+                V = "Vf%d" % depth
+                ce = coef_expr(n["coef"], True)
+                w("      float %s = %s;" % (V, ce if ce else "0.0f"))
+                for cv, ch in n["kids"].items():
+                    c = coef_expr(ch["coef"], True)
+                    w("      %s = fmaf(%s, xf[%d], %s); gf[%d] = fmaf(%s, %s, gf[%d]);" %
+                      (V, c, cv, V, cv, c, Pf, cv))
+                Vd = "(double)%s" % V
+            else:
+                V = "Vd%d" % depth
+                ce = coef_expr(n["coef"])
+                w("      double %s = %s;" % (V, ce if ce else "0.0"))
+                for cv, ch in n["kids"].items():
+                    if ch["kids"]:
+                        node(ch, cv, depth + 1, Pf, Pd)
+                    else:
+                        c = coef_expr(ch["coef"])
+                        w("      %s = fma(%s, x[%d], %s); g[%d] = fma(%s, %s, g[%d]);" %
+                          (V, c, cv, V, cv, c, Pd, cv))
+                Vd = V
+            if pexpr_f is None:
+                w("      g[%d] += %s; E = fma(x[%d], %s, E); }" % (var, Vd, var, Vd))
+            else:
+                w("      g[%d] = fma(%s, %s, g[%d]); Vd%d = fma(x[%d], %s, Vd%d); }" %
+                  (var, pexpr_d, Vd, var, depth - 1, var, Vd, depth - 1))
 
-    def node(n, var, depth, pexpr_f, pexpr_d):
-        # FP32 product P and FP64 product PD along the path; inner-node values
-        # V in FP64 except the last inner level, whose leaf sums are FP32.
-        Pf = "Pf%d" % depth
-        Pd = "Pd%d" % depth
-        leaf_only = all(not ch["kids"] for ch in n["kids"].values())
-        if pexpr_f is None:
-            w("    { const float %s = xf[%d];" % (Pf, var))
-            if not leaf_only:
-                w("      const double %s = x[%d];" % (Pd, var))
-        else:
-            w("    { const float %s = %s * xf[%d];" % (Pf, pexpr_f, var))
-            if not leaf_only:
-                w("      const double %s = %s * x[%d];" % (Pd, pexpr_d, var))
-        if leaf_only:
-            V = "Vf%d" % depth
-            ce = coef_expr(n["coef"], True)
-            w("      float %s = %s;" % (V, ce if ce else "0.0f"))
-            for cv, ch in n["kids"].items():
-                c = coef_expr(ch["coef"], True)
-                w("      %s = fmaf(%s, xf[%d], %s); gf[%d] = fmaf(%s, %s, gf[%d]);" % (V, c, cv, V, cv, c, Pf, cv))
-            Vd = "(double)%s" % V
-        else:
-            V = "Vd%d" % depth
-            ce = coef_expr(n["coef"])
-            w("      double %s = %s;" % (V, ce if ce else "0.0"))
-            for cv, ch in n["kids"].items():
-                if ch["kids"]:
-                    node(ch, cv, depth + 1, Pf, Pd)
-                else:
-                    c = coef_expr(ch["coef"])
-                    w("      %s = fma(%s, x[%d], %s); g[%d] = fma(%s, %s, g[%d]);" % (V, c, cv, V, cv, c, Pd, cv))
-            Vd = V
-        if pexpr_f is None:
-            w("      g[%d] += %s; E = fma(x[%d], %s, E); }" % (var, Vd, var, Vd))
-        else:
-            w("      g[%d] = fma(%s, %s, g[%d]); Vd%d = fma(x[%d], %s, Vd%d); }" %
-              (var, pexpr_d, Vd, var, depth - 1, var, Vd, depth - 1))
+        for var, ch in subtrees:
+            if ch["kids"]:
+                node(ch, var, 1, None, None)
+            else:
+                c = coef_expr(ch["coef"])
+                w("    E = fma(%s, x[%d], E); g[%d] += %s;" % (c, var, var, c))
 
-    for var, ch in trie.root["kids"].items():
-        if ch["kids"]:
-            node(ch, var, 1, None, None)
-        else:
-            c = coef_expr(ch["coef"])
-            w("    E = fma(%s, x[%d], E); g[%d] += %s;" % (c, var, var, c))
-    w("    return E;")
-    w("}")
+    emit_split(trie, nvars, name, out, nparts,
+               [("xf", "float", "in"), ("x", "double", "in"), ("g", "double", "acc"), ("gf", "float", "acc")], body)
 
 
 def emit_dcoef(table, nvars, name, out):
@@ -298,21 +355,21 @@ def emit_traits(spec, table, straight, out):
       (1 if spec.switch == "triple" else 0, {"pair_gt": 0, "two_of_three_gt": 1, "all_three_gt": 2}[spec.skip],
        1 if straight else 0, spec.degree))
     w("    static constexpr double RI = %s, RF = %s;" % (lit(spec.ri), lit(spec.rf)))
-    w("    __device__ static void sites(const double (&r)[%d][3], double (&s)[%d][3]) { %s_sites(r, s); }" %
+    w("    __device__ __forceinline__ static void sites(const double (&r)[%d][3], double (&s)[%d][3]) { %s_sites(r, s); }" %
       (spec.nreal, ns, n))
-    w("    __device__ static void vars(const double (&s)[%d][3], double (&x)[%d]) { %s_vars(s, x); }" %
+    w("    __device__ __forceinline__ static void vars(const double (&s)[%d][3], double (&x)[%d]) { %s_vars(s, x); }" %
       (ns, spec.nvars, n))
-    w("    __device__ static void chain(const double (&s)[%d][3], const double (&g)[%d], double (&sg)[%d][3]) "
+    w("    __device__ __forceinline__ static void chain(const double (&s)[%d][3], const double (&g)[%d], double (&sg)[%d][3]) "
       "{ %s_chain(s, g, sg); }" % (ns, spec.nvars, ns, n))
     if straight:
-        w("    template <class C> __device__ static double pip(const C& c, const double (&x)[%d], double (&g)[%d]) "
+        w("    template <class C> __device__ __forceinline__ static double pip(const C& c, const double (&x)[%d], double (&g)[%d]) "
           "{ return %s_pip(c, x, g); }" % (spec.nvars, spec.nvars, n))
-        w("    template <class C> __device__ static double pip_e(const C& c, const double (&x)[%d]) "
+        w("    template <class C> __device__ __forceinline__ static double pip_e(const C& c, const double (&x)[%d]) "
           "{ return %s_pip_e(c, x); }" % (spec.nvars, n))
-        w("    template <class C> __device__ static double pip_mixed(const C& c, const float (&xf)[%d], "
+        w("    template <class C> __device__ __forceinline__ static double pip_mixed(const C& c, const float (&xf)[%d], "
           "const double (&x)[%d], double (&g)[%d], float (&gf)[%d]) { return %s_pip_mixed(c, xf, x, g, gf); }" %
           (spec.nvars, spec.nvars, spec.nvars, spec.nvars, n))
-        w("    template <class S> __device__ static void dcoef(const double (&x)[%d], S&& sink) "
+        w("    template <class S> __device__ __forceinline__ static void dcoef(const double (&x)[%d], S&& sink) "
           "{ %s_dcoef(x, sink); }" % (spec.nvars, n))
     w("};")
 
@@ -353,10 +410,14 @@ def generate(name):
     os.makedirs(OUT, exist_ok=True)
     write_if_changed(os.path.join(OUT, name + ".cuh"), "\n".join(out) + "\n")
     if straight:
+        nparts = parts_for(table.nterms)
         for suffix, emitter, arg in (("pip", emit_pip, trie), ("pip_e", emit_pip_energy, trie),
                                      ("pip_mixed", emit_pip_mixed, trie), ("dcoef", emit_dcoef, table)):
             body = head + ["#pragma once", '#include "%s.cuh"' % name]
-            emitter(arg, nv, "%s_%s" % (name, suffix), body)
+            if emitter is emit_dcoef:
+                emitter(arg, nv, "%s_%s" % (name, suffix), body)
+            else:
+                emitter(arg, nv, "%s_%s" % (name, suffix), body, nparts)
             write_if_changed(os.path.join(OUT, "%s_%s.cuh" % (name, suffix)), "\n".join(body) + "\n")
     return os.path.join(OUT, name + ".cuh"), leaves, inner
 
@@ -400,19 +461,61 @@ VARIANTS = {
     # variant: (description, body)
     "g": ("FP64 energy + gradient kernel", """
 int mbx_launch_%(name)s_g(const HolderArgs& A, int grid, int block, cudaStream_t s) {
-    holder_kernel<%(name)s_T, %(name)s_CC, HM_GRAD_FP64, false><<<grid, block, 0, s>>>(A);
+    // persistent grid: every resident block slot once (warps claim work dynamically)
+    auto kern = holder_kernel<%(name)s_T, %(name)s_CC, HM_GRAD_FP64, false>;
+    static int bps = 0, sms = 0, bps_block = 0;
+    if (!bps || bps_block != block) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, block, 0);
+        if (bps < 1) bps = 1;
+        bps_block = block;
+    }
+    const long need = (A.n + block - 1) / block;
+    grid = (int)(need < (long)sms * bps ? need : (long)sms * bps);
+    if (grid < 1) grid = 1;
+    kern<<<grid, block, 0, s>>>(A);
     return (int)cudaGetLastError();
 }
 """),
     "e": ("FP64 energy-only kernel", """
 int mbx_launch_%(name)s_e(const HolderArgs& A, int grid, int block, cudaStream_t s) {
-    holder_kernel<%(name)s_T, %(name)s_CC, HM_ENERGY, false><<<grid, block, 0, s>>>(A);
+    // persistent grid: every resident block slot once (warps claim work dynamically)
+    auto kern = holder_kernel<%(name)s_T, %(name)s_CC, HM_ENERGY, false>;
+    static int bps = 0, sms = 0, bps_block = 0;
+    if (!bps || bps_block != block) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, block, 0);
+        if (bps < 1) bps = 1;
+        bps_block = block;
+    }
+    const long need = (A.n + block - 1) / block;
+    grid = (int)(need < (long)sms * bps ? need : (long)sms * bps);
+    if (grid < 1) grid = 1;
+    kern<<<grid, block, 0, s>>>(A);
     return (int)cudaGetLastError();
 }
 """),
     "m": ("mixed-precision energy + gradient kernel", """
 int mbx_launch_%(name)s_m(const HolderArgs& A, int grid, int block, cudaStream_t s) {
-    holder_kernel<%(name)s_T, %(name)s_CC, HM_GRAD_MIXED, false><<<grid, block, 0, s>>>(A);
+    // persistent grid: every resident block slot once (warps claim work dynamically)
+    auto kern = holder_kernel<%(name)s_T, %(name)s_CC, HM_GRAD_MIXED, false>;
+    static int bps = 0, sms = 0, bps_block = 0;
+    if (!bps || bps_block != block) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, block, 0);
+        if (bps < 1) bps = 1;
+        bps_block = block;
+    }
+    const long need = (A.n + block - 1) / block;
+    grid = (int)(need < (long)sms * bps ? need : (long)sms * bps);
+    if (grid < 1) grid = 1;
+    kern<<<grid, block, 0, s>>>(A);
     return (int)cudaGetLastError();
 }
 """),

@@ -26,6 +26,7 @@ struct HolderArgs {
     long n;                    // number of n-mers (capacity when n_dev is set)
     const int* n_dev;          // optional device-side count (read by the kernel, clamped to n)
     const int* status;         // optional: a nonzero word means the n-mer build failed; do nothing
+    int* counter;              // work counter (zeroed before the launch): warps claim chunks of 32 n-mers
     const int4* nmers;         // system input: (m0, m1, m2, anchor slot), holder order
     const double* xyz;         // system input: site array (3 per site); AoS input: [n][NREAL*3]
     const int* first_index;    // system input: first site of every monomer
@@ -230,62 +231,84 @@ __device__ __forceinline__ long nmer_count(const HolderArgs& A) {
     return c < A.n ? c : A.n;
 }
 
+// Claims the next chunk of 32 n-mers for the calling warp: dynamic load
+// balance (a skipped n-mer costs nothing, an evaluated one ~10^5 flops).
+__device__ __forceinline__ long claim_chunk(const HolderArgs& A, long& static_next) {
+    const int lane = threadIdx.x & 31;
+    if (A.counter) {
+        int b = 0;
+        if (lane == 0) b = atomicAdd(A.counter, 32);
+        return (long)__shfl_sync(0xffffffffu, b, 0);
+    }
+    const long b = static_next;
+    static_next += (long)gridDim.x * blockDim.x;
+    return b;
+}
+
+// The polynomial (and its gradient) in the precision mode of the kernel.
+template <class T, int MODE, class C>
+__device__ __forceinline__ double run_pip(const C& coef, const double (&x)[T::NVARS], double (&g)[T::NVARS]) {
+    if constexpr (MODE == HM_ENERGY) {
+        return T::pip_e(coef, x);
+    } else if constexpr (MODE == HM_GRAD_FP64) {
+        return T::pip(coef, x, g);
+    } else {
+        float xf[T::NVARS], gf[T::NVARS];
+#pragma unroll
+        for (int v = 0; v < T::NVARS; ++v) { xf[v] = (float)x[v]; gf[v] = 0.0f; }
+        const double ep = T::pip_mixed(coef, xf, x, g, gf);
+#pragma unroll
+        for (int v = 0; v < T::NVARS; ++v) g[v] += (double)gf[v];
+        return ep;
+    }
+}
+
+// One n-mer: gather, skip rule, variables, polynomial, then finish_nmer.
+template <class T, class CC, int MODE, bool CUSTOM>
+__device__ __forceinline__ void eval_nmer(const HolderArgs& A, long t, double (&acc)[7]) {
+    constexpr bool grads = (MODE == HM_GRAD_FP64 || MODE == HM_GRAD_MIXED);
+    double ep;
+    double g[T::NVARS];
+    {
+        double r[T::NREAL][3];
+        load_nmer<T, false>(A, t, r);
+        double d[3][3], rr[3];
+        if (pair_dists<T>(r, d, rr)) {
+            if (A.e_per) A.e_per[t] = 0.0;
+            return;
+        }
+        double s[T::NSITES][3];
+        T::sites(r, s);
+        double x[T::NVARS];
+        T::vars(s, x);
+#pragma unroll
+        for (int v = 0; v < T::NVARS; ++v) g[v] = 0.0;
+        if constexpr (T::STRAIGHT) {
+            if constexpr (CUSTOM) ep = run_pip<T, MODE>(GlobalCoef{A.coef}, x, g);
+            else ep = run_pip<T, MODE>(CC{}, x, g);
+        } else {
+            ep = 0.0;
+        }
+    }
+    finish_nmer<T>(A, t, ep, g, grads, acc);
+}
+
 #ifndef MBX_HOLDER_MINB
 #define MBX_HOLDER_MINB 1
 #endif
+// One n-mer per thread; persistent grid, warps claim chunks of 32 n-mers
+// from a global counter.
 template <class T, class CC, int MODE, bool CUSTOM>
 __global__ void __launch_bounds__(128, MBX_HOLDER_MINB) holder_kernel(const HolderArgs A) {
     double acc[7] = {0, 0, 0, 0, 0, 0, 0};
-    const bool grads = (MODE == HM_GRAD_FP64 || MODE == HM_GRAD_MIXED);
     const long n = nmer_count(A);
-    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
-        double ep;
-        double g[T::NVARS];
-        {
-            double r[T::NREAL][3];
-            load_nmer<T, false>(A, t, r);
-            double d[3][3], rr[3];
-            if (pair_dists<T>(r, d, rr)) {
-                if (A.e_per) A.e_per[t] = 0.0;
-                continue;
-            }
-            double s[T::NSITES][3];
-            T::sites(r, s);
-            double x[T::NVARS];
-            T::vars(s, x);
-#pragma unroll
-            for (int v = 0; v < T::NVARS; ++v) g[v] = 0.0;
-            if constexpr (T::STRAIGHT) {
-                if constexpr (CUSTOM) {
-                    const GlobalCoef coef{A.coef};
-                    if constexpr (MODE == HM_ENERGY) ep = T::pip_e(coef, x);
-                    else if constexpr (MODE == HM_GRAD_FP64) ep = T::pip(coef, x, g);
-                    else {
-                        float xf[T::NVARS], gf[T::NVARS];
-#pragma unroll
-                        for (int v = 0; v < T::NVARS; ++v) { xf[v] = (float)x[v]; gf[v] = 0.0f; }
-                        ep = T::pip_mixed(coef, xf, x, g, gf);
-#pragma unroll
-                        for (int v = 0; v < T::NVARS; ++v) g[v] += (double)gf[v];
-                    }
-                } else {
-                    const CC coef{};
-                    if constexpr (MODE == HM_ENERGY) ep = T::pip_e(coef, x);
-                    else if constexpr (MODE == HM_GRAD_FP64) ep = T::pip(coef, x, g);
-                    else {
-                        float xf[T::NVARS], gf[T::NVARS];
-#pragma unroll
-                        for (int v = 0; v < T::NVARS; ++v) { xf[v] = (float)x[v]; gf[v] = 0.0f; }
-                        ep = T::pip_mixed(coef, xf, x, g, gf);
-#pragma unroll
-                        for (int v = 0; v < T::NVARS; ++v) g[v] += (double)gf[v];
-                    }
-                }
-            } else {
-                ep = 0.0;
-            }
-        }
-        finish_nmer<T>(A, t, ep, g, grads, acc);
+    const int lane = threadIdx.x & 31;
+    long static_next = blockIdx.x * (long)blockDim.x + (threadIdx.x & ~31);
+    for (;;) {
+        const long base = claim_chunk(A, static_next);
+        if (base >= n) break;
+        const long t = base + lane;
+        if (t < n) eval_nmer<T, CC, MODE, CUSTOM>(A, t, acc);
     }
     block_reduce_add<7>(acc, A.out);
 }

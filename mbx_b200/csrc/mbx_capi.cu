@@ -128,7 +128,7 @@ struct mbx_ctx {
 
     // work buffers
     DevBuf<double> xyz, grad, out, cloud, coef_ws;
-    DevBuf<int> cell_of, cell_count, cell_start, cell_fill, cell_items, nb_count, bucket_count, status;
+    DevBuf<int> cell_of, cell_count, cell_start, cell_fill, cell_items, nb_count, bucket_count, status, counters;
     DevBuf<NbEntry> nb;
     DevBuf<int4> buckets, list;
     DevBuf<unsigned long long> listed;
@@ -190,6 +190,7 @@ int mbx_create(mbx_ctx** out, int device, void* stream) {
     for (int i = 0; i < 3; ++i) CUCHK(c, cudaEventCreate(&c->ev[i]));
     CUCHK(c, c->out.ensure(64));
     CUCHK(c, c->status.ensure(4));
+    CUCHK(c, c->counters.ensure(MBX_MAX_BUCKETS));
     CUCHK(c, c->listed.ensure(4));
     for (int nb = 0; nb < 4; ++nb)
         for (int b = 0; b < MBX_MAX_BUCKETS; ++b) c->bucket_cap[nb][b] = 0;
@@ -223,7 +224,8 @@ int mbx_destroy(mbx_ctx* c) {
     cudaStreamSynchronize(c->stream);
     DevBuf<int>* ib[] = {&c->d_first, &c->d_nat, &c->d_tag, &c->d_type, &c->d_members[0], &c->d_members[1],
                          &c->d_query[0], &c->d_query[1], &c->cell_of, &c->cell_count, &c->cell_start,
-                         &c->cell_fill, &c->cell_items, &c->nb_count, &c->bucket_count, &c->status};
+                         &c->cell_fill, &c->cell_items, &c->nb_count, &c->bucket_count, &c->status,
+                         &c->counters};
     for (auto* b : ib) b->release();
     DevBuf<double>* db[] = {&c->xyz, &c->grad, &c->out, &c->cloud, &c->coef_ws, &c->tcoef, &c->warp_coef};
     for (auto* b : db) b->release();
@@ -627,9 +629,11 @@ extern "C" int mbx_energy(mbx_ctx* c, int nbody, double* xyz, int use_ghost, dou
             }
         }
         CUCHK(c, cudaMemsetAsync(c->out.p, 0, 16 * sizeof(double), c->stream));
+        CUCHK(c, cudaMemsetAsync(c->counters.p, 0, MBX_MAX_BUCKETS * sizeof(int), c->stream));
         long off = 0;
         for (int b = 0; b < c->nbucket[nbody]; ++b) {
             HolderArgs A = base_args(c);
+            A.counter = c->counters.p + b;
             A.n = c->bucket_cap[nbody][b];
             A.n_dev = c->bucket_count.p + b;
             A.status = c->status.p;
@@ -818,7 +822,9 @@ extern "C" int mbx_evaluate(mbx_ctx* c, const char* name, long n, const double* 
         }
     }
     CUCHK(c, cudaMemsetAsync(c->out.p, 0, 16 * sizeof(double), c->stream));
+    CUCHK(c, cudaMemsetAsync(c->counters.p, 0, sizeof(int), c->stream));
     HolderArgs A = base_args(c);
+    A.counter = c->counters.p;
     A.bp.use_pbc = 0;
     A.n = n;
     A.aos = 1;
