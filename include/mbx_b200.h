@@ -115,6 +115,27 @@ int mbx_evaluator_info(const char* evaluator, int* nbody, int* nreal, int* nvars
  * and evaluation, and the number of kernels it launched. */
 int mbx_last_timing(const mbx_ctx* ctx, double* ms_build, double* ms_eval, int* kernels);
 
+/* No counterpart in the reference.  Evaluator entry point that allocates no
+ * device memory, for callers that must not call cudaMalloc (allocator-free
+ * real-time loops, fixed memory pools, plugins that may not grow the
+ * process's device memory).  Same evaluator calling convention as
+ * mbx_evaluate, straight-line evaluators only ("mbpol2b", "mbpol3b",
+ * "ch4h2o2b", "ch4h2o3b"), coefficients as last set on the device; every
+ * pointer is device memory owned by the caller; runs on `stream` on the
+ * current device:
+ *   xyz[n][nreal*3] in, grad (+=, NULL for energy only) and e_per (n
+ *   switched energies, may be NULL) out, result[7] out (overwritten):
+ *   energy, then virial xx xy xz yy yz zz.
+ * The energy is summed over the n-mers in a fixed order (reproducible from
+ * call to call).  Scratch lives in one static device array shared by all
+ * calls: n must not exceed MBX_NOALLOC_MAX_NMERS (MBX_EINVAL otherwise);
+ * calls that overlap on the GPU race on it.  The first call on a device
+ * looks up the array's device address; make that call before any stream
+ * capture. */
+#define MBX_NOALLOC_MAX_NMERS 262144
+int mbx_evaluate_noalloc(const char* evaluator, long n, const double* xyz, double* grad, double* e_per,
+                         double* result, void* stream);
+
 /* Measured FMA-pipe throughput of the device (results[0] FP64, results[1]
  * FP32, results[2] FP32 issued as paired fma.rn.f32x2; TFLOP/s): the
  * roofline denominators for the polynomial kernels.  results has 3 slots. */

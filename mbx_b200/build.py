@@ -30,7 +30,7 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxe
 
 
 def sources():
-    hand = [os.path.join(CSRC, f) for f in ("mbx_capi.cu", "nmer_build.cu", "peaks.cu")]
+    hand = [os.path.join(CSRC, f) for f in ("mbx_capi.cu", "nmer_build.cu", "peaks.cu", "noalloc.cu")]
     return [s for s in hand if os.path.exists(s)] + sorted(glob.glob(os.path.join(GEN, "*.cu")))
 
 
