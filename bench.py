@@ -40,6 +40,9 @@ sys.path.insert(0, ROOT)
 
 METRIC = "dimers+trimers/s with forces, 2048 H2O; FP32-mixed vs FP64 GPU at <=1e-6 rel E"
 CUT2, CUT3 = 9.0, 7.0
+# DRAM bytes per launch of the mbpol3b gradient kernel on this workload, from one
+# ncu capture of the same command (read + write); the kernel is compute-bound
+TRAFFIC_3B = 8.02e6
 
 
 def workload():
@@ -60,7 +63,8 @@ class Clocks:
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.lines = []
+        self.lines = []          # (arrival time, csv line)
+        self.window = None       # (t0, t1) of the timed region, time.monotonic()
 
     def __enter__(self):
         q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
@@ -68,7 +72,7 @@ class Clocks:
              "clocks_event_reasons.sw_power_cap")
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -78,7 +82,13 @@ class Clocks:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.monotonic(), line.strip()))
+
+    def wait_first(self, work, limit=10.0):
+        """Runs work() until the sampler has produced a line (or limit s)."""
+        t0 = time.monotonic()
+        while self.proc and not self.lines and time.monotonic() - t0 < limit:
+            work()
 
     def __exit__(self, *a):
         if self.proc:
@@ -91,7 +101,9 @@ class Clocks:
     def summary(self):
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
+        for t, line in self.lines:
+            if self.window and not (self.window[0] <= t <= self.window[1]):
+                continue
             p = [x.strip() for x in line.split(",")]
             if len(p) < 7:
                 continue
@@ -173,7 +185,7 @@ def run_reference(args, rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -243,14 +255,17 @@ def main():
         return times, evals, launches, energies
 
     with Clocks(local) as clk:
+        clk.wait_first(step)
+        t_begin = time.monotonic()
         t64, ev64, launches, (e2_64, e3_64) = timed(False)
+        clk.window = (t_begin, time.monotonic())
     clocks = clk.summary()
     if not args.no_mixed:
         for _ in range(args.warmup):
             step(True)
         tmx, evmx, launches_mx, (e2_mx, e3_mx) = timed(True)
     else:
-        tmx, e2_mx, e3_mx = list(t64), e2_64, e3_64
+        tmx = list(t64)
 
     ms = sum(t64) / len(t64)
     ms_mx = sum(tmx) / len(tmx)
@@ -293,7 +308,8 @@ def main():
     achieved = eval3 * flops["mbpol3b"]["flops"] / (kern_ms * 1e-3) / 1e12
     roofline = {"bound": "fp64-fma", "kernel": "holder_kernel<mbpol3b_T, HM_GRAD_FP64>", "achieved": achieved,
                 "peak": peaks["fp64_tflops"], "unit": "TFLOP/s", "frac": achieved / peaks["fp64_tflops"],
-                "traffic": None,
+                "traffic": TRAFFIC_3B, "traffic_unit": "bytes per launch (ncu dram__bytes, one capture)",
+                "traffic_source": "profiles/holder_kernel_mbpol3b_grad_2048h2o.md",
                 "note": "algorithmic flops = evaluated trimers x %d (reference gradient program, "
                         "mbx_b200/data/flops.json); peak = FP64 FMA pipe measured on this GPU by "
                         "mbx_fma_peaks (MEASURED_PEAKS.json has no FP64 figure)" % flops["mbpol3b"]["flops"],
@@ -305,14 +321,16 @@ def main():
            "units_per_step": {"dimers": listed2, "trimers": listed3, "evaluated_dimers": eval2,
                               "evaluated_trimers": eval3},
            "energies": {"E2B": e2_64, "E3B": e3_64},
-           "mixed": {"value": world * units / (ms_mx * 1e-3), "ms_per_step": ms_mx, "dtype": "f32-monomial/f64-acc",
-                     "rel_err_E2B": abs(e2_mx - e2_64) / abs(e2_64), "rel_err_E3B": abs(e3_mx - e3_64) / abs(e3_64),
-                     "rel_err_E": abs((e2_mx + e3_mx) - (e2_64 + e3_64)) / abs(e2_64 + e3_64),
-                     "speedup_vs_fp64": ms / ms_mx},
            "e2e": {"value": world * units / (e2e_ms * 1e-3), "unit": "n-mers/s", "h2d_bytes_per_step": h2d,
                    "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms, "api": "mbx_b200.system.System"},
            "gpu_launches": launches, "roofline": roofline, "clocks": clocks,
            "fma_peaks_tflops": peaks}
+    if not args.no_mixed:
+        out["mixed"] = {"value": world * units / (ms_mx * 1e-3), "ms_per_step": ms_mx,
+                        "dtype": "f32-monomial/f64-acc",
+                        "rel_err_E2B": abs(e2_mx - e2_64) / abs(e2_64), "rel_err_E3B": abs(e3_mx - e3_64) / abs(e3_64),
+                        "rel_err_E": abs((e2_mx + e3_mx) - (e2_64 + e3_64)) / abs(e2_64 + e3_64),
+                        "speedup_vs_fp64": ms / ms_mx}
     if rank == 0 and not args.no_cpu_baseline:
         cb = ref_cpu(ids, xyz, box)
         if cb:
