@@ -89,6 +89,14 @@ class Trie:
         return leaves, inner
 
 
+# Code-shape options of the generated evaluators: how the trie is cut into
+# separately compiled pieces ("top": whole top-level subtrees, "terms":
+# contiguous term ranges) and into how many independent FMA chains the leaf sum
+# of a node is split (1 = one serial chain per node).
+SPLIT = "terms"
+ACC_CHAINS = 1
+
+
 def coef_expr(coefs, fp32=False):
     """Sum of coef[k]*c for the terms ending exactly at a node (FP32: the
     float copy of the coefficients, coef.f(k))."""
@@ -119,12 +127,50 @@ def partition(trie, nparts):
     return [p for p in parts if p]
 
 
-def parts_for(nterms):
-    """Number of separately compiled pieces: one per ~4500 terms.  A single
-    straight-line function of 10^4-10^5 FMAs leaves the register allocator
-    with live ranges it cannot fit in 255 registers (kilobytes of spills);
-    pieces of this size compile with next to none."""
-    return max(1, (nterms + 4499) // 4500)
+def split_terms(trie, nparts):
+    """The trie cut into nparts sub-tries of contiguous terms in depth-first
+    order, each carrying the path nodes its terms hang from.  A path node's
+    own coefficient goes with the range that holds it, so every term is in
+    exactly one sub-trie; each sub-trie evaluates to its share of the
+    polynomial (the trie value is linear in the terms)."""
+    terms = []
+
+    def walk(node, path):
+        if node is not trie.root and node["coef"]:
+            terms.append((path, node["coef"]))
+        for v, ch in node["kids"].items():
+            walk(ch, path + (v,))
+    walk(trie.root, ())
+    per = -(-len(terms) // max(1, nparts))
+    roots = []
+    for lo in range(0, len(terms), per):
+        root = {"coef": [], "kids": collections.OrderedDict()}
+        for path, coefs in terms[lo:lo + per]:
+            node = root
+            for v in path:
+                node = node["kids"].setdefault(v, {"coef": [], "kids": collections.OrderedDict()})
+            node["coef"].extend(coefs)
+        roots.append(root)
+    return [list(r["kids"].items()) for r in roots]
+
+
+def lock_threads(nvars):
+    """Threads of a lockstep evaluation block.  Up to 32 variables the
+    variables and their gradient accumulators (4 registers per variable) fit
+    under 168 registers, so a block of 384 threads (12 warps per SM) is
+    resident; wider polynomials need the full 255 registers (256 threads)."""
+    return 384 if nvars <= 32 else 256
+
+
+def parts_for(nterms, nvars=36):
+    """Number of separately compiled pieces of a trie.  A single straight-line
+    function of 10^4-10^5 FMAs leaves the register allocator live ranges it
+    cannot fit (kilobytes of spills), and the code of a piece should stay
+    small enough for the instruction cache that the warps of a lockstep block
+    share: ~400 terms per piece in 384-thread blocks, ~700 in 256-thread
+    blocks (measured on the MB-pol 2b/3b tries)."""
+    per = 400 if lock_threads(nvars) == 384 else 700
+    return max(1, (nterms + per - 1) // per)
 
 
 def emit_split(trie, nvars, name, out, nparts, arrays, body, ret="double"):
@@ -137,7 +183,7 @@ def emit_split(trie, nvars, name, out, nparts, arrays, body, ret="double"):
     the subtrees into the local arrays and into E."""
     import re
     w = out.append
-    pieces = partition(trie, nparts)
+    pieces = split_terms(trie, nparts) if SPLIT == "terms" else partition(trie, nparts)
     for i, sub in enumerate(pieces):
         text = []
         body(text.append, sub)
@@ -162,13 +208,18 @@ def emit_split(trie, nvars, name, out, nparts, arrays, body, ret="double"):
         w("    return E;")
         w("}")
     sig = ", ".join("%s%s (&%s)[%d]" % ("const " if role == "in" else "", ct, a, nvars) for a, ct, role in arrays)
-    w("template <class Coef>")
-    w("__device__ __forceinline__ %s %s(const Coef& coef, %s) {" % (ret, name, sig))
-    w("    %s E = 0.0;" % ret)
-    for i in range(len(pieces)):
-        w("    E += %s_part%d(coef, %s);" % (name, i, ", ".join(a for a, _, _ in arrays)))
-    w("    return E;")
-    w("}")
+    for lock in (False, True):
+        # name(): the pieces in turn; name_lock(): the same with a block
+        # barrier after every piece, so that all warps of a block run the same
+        # piece at the same time and share its instruction fetches
+        w("template <class Coef>")
+        w("__device__ __forceinline__ %s %s%s(const Coef& coef, %s) {" % (ret, name, "_lock" if lock else "", sig))
+        w("    %s E = 0.0;" % ret)
+        for i in range(len(pieces)):
+            w("    E += %s_part%d(coef, %s);%s" % (name, i, ", ".join(a for a, _, _ in arrays),
+                                                 " __syncthreads();" if lock else ""))
+        w("    return E;")
+        w("}")
 
 
 def emit_pip(trie, nvars, name, out, nparts=1):
@@ -186,12 +237,23 @@ def emit_pip(trie, nvars, name, out, nparts=1):
                 w("    { const double %s = %s * x[%d];" % (P, pexpr, var))
             ce = coef_expr(n["coef"])
             w("      double %s = %s;" % (V, ce if ce else "0.0"))
+            nleaf = sum(1 for ch in n["kids"].values() if not ch["kids"])
+            split = ACC_CHAINS > 1 and nleaf >= 2 * ACC_CHAINS
+            if split:
+                # leaf sums in ACC_CHAINS independent chains, joined at the end
+                for j in range(1, ACC_CHAINS):
+                    w("      double %s_%d = 0.0;" % (V, j))
+            li = 0
             for cv, ch in n["kids"].items():
                 if ch["kids"]:
                     node(ch, cv, depth + 1, P)
                 else:
                     c = coef_expr(ch["coef"])
-                    w("      %s = fma(%s, x[%d], %s); g[%d] = fma(%s, %s, g[%d]);" % (V, c, cv, V, cv, c, P, cv))
+                    acc = V if not split or li % ACC_CHAINS == 0 else "%s_%d" % (V, li % ACC_CHAINS)
+                    li += 1
+                    w("      %s = fma(%s, x[%d], %s); g[%d] = fma(%s, %s, g[%d]);" % (acc, c, cv, acc, cv, c, P, cv))
+            if split:
+                w("      %s += %s;" % (V, " + ".join("%s_%d" % (V, j) for j in range(1, ACC_CHAINS))))
             if pexpr is None:
                 w("      g[%d] += %s; E = fma(x[%d], %s, E); }" % (var, V, var, V))
             else:
@@ -355,6 +417,8 @@ def emit_traits(spec, table, straight, out):
       (1 if spec.switch == "triple" else 0, {"pair_gt": 0, "two_of_three_gt": 1, "all_three_gt": 2}[spec.skip],
        1 if straight else 0, spec.degree))
     w("    static constexpr double RI = %s, RF = %s;" % (lit(spec.ri), lit(spec.rf)))
+    w("    static constexpr int LOCK_THREADS = %d;  // threads of a lockstep evaluation block" %
+      lock_threads(spec.nvars))
     w("    __device__ __forceinline__ static void sites(const double (&r)[%d][3], double (&s)[%d][3]) { %s_sites(r, s); }" %
       (spec.nreal, ns, n))
     w("    __device__ __forceinline__ static void vars(const double (&s)[%d][3], double (&x)[%d]) { %s_vars(s, x); }" %
@@ -362,13 +426,14 @@ def emit_traits(spec, table, straight, out):
     w("    __device__ __forceinline__ static void chain(const double (&s)[%d][3], const double (&g)[%d], double (&sg)[%d][3]) "
       "{ %s_chain(s, g, sg); }" % (ns, spec.nvars, ns, n))
     if straight:
-        w("    template <class C> __device__ __forceinline__ static double pip(const C& c, const double (&x)[%d], double (&g)[%d]) "
-          "{ return %s_pip(c, x, g); }" % (spec.nvars, spec.nvars, n))
-        w("    template <class C> __device__ __forceinline__ static double pip_e(const C& c, const double (&x)[%d]) "
-          "{ return %s_pip_e(c, x); }" % (spec.nvars, n))
-        w("    template <class C> __device__ __forceinline__ static double pip_mixed(const C& c, const float (&xf)[%d], "
-          "const double (&x)[%d], double (&g)[%d], float (&gf)[%d]) { return %s_pip_mixed(c, xf, x, g, gf); }" %
-          (spec.nvars, spec.nvars, spec.nvars, spec.nvars, n))
+        for lk in ("", "_lock"):
+            w("    template <class C> __device__ __forceinline__ static double pip%s(const C& c, const double (&x)[%d], "
+              "double (&g)[%d]) { return %s_pip%s(c, x, g); }" % (lk, spec.nvars, spec.nvars, n, lk))
+            w("    template <class C> __device__ __forceinline__ static double pip_e%s(const C& c, const double (&x)[%d]) "
+              "{ return %s_pip_e%s(c, x); }" % (lk, spec.nvars, n, lk))
+            w("    template <class C> __device__ __forceinline__ static double pip_mixed%s(const C& c, "
+              "const float (&xf)[%d], const double (&x)[%d], double (&g)[%d], float (&gf)[%d]) "
+              "{ return %s_pip_mixed%s(c, xf, x, g, gf); }" % (lk, spec.nvars, spec.nvars, spec.nvars, spec.nvars, n, lk))
         w("    template <class S> __device__ __forceinline__ static void dcoef(const double (&x)[%d], S&& sink) "
           "{ %s_dcoef(x, sink); }" % (spec.nvars, n))
     w("};")
@@ -398,19 +463,21 @@ def generate(name):
     emit_vars(spec, out)
     nv = spec.nvars
     if straight:
-        out += ["template <class Coef> __device__ __forceinline__ double %s_pip(const Coef&, const double (&)[%d], "
-                "double (&)[%d]);" % (name, nv, nv),
-                "template <class Coef> __device__ __forceinline__ double %s_pip_e(const Coef&, "
-                "const double (&)[%d]);" % (name, nv),
-                "template <class Coef> __device__ __forceinline__ double %s_pip_mixed(const Coef&, const float (&)[%d],"
-                " const double (&)[%d], double (&)[%d], float (&)[%d]);" % (name, nv, nv, nv, nv),
-                "template <class Sink> __device__ __forceinline__ void %s_dcoef(const double (&)[%d], Sink&&);" %
+        for lk in ("", "_lock"):
+            out += ["template <class Coef> __device__ __forceinline__ double %s_pip%s(const Coef&, const double (&)[%d], "
+                    "double (&)[%d]);" % (name, lk, nv, nv),
+                    "template <class Coef> __device__ __forceinline__ double %s_pip_e%s(const Coef&, "
+                    "const double (&)[%d]);" % (name, lk, nv),
+                    "template <class Coef> __device__ __forceinline__ double %s_pip_mixed%s(const Coef&, "
+                    "const float (&)[%d], const double (&)[%d], double (&)[%d], float (&)[%d]);" %
+                    (name, lk, nv, nv, nv, nv)]
+        out += ["template <class Sink> __device__ __forceinline__ void %s_dcoef(const double (&)[%d], Sink&&);" %
                 (name, nv)]
     emit_traits(spec, table, straight, out)
     os.makedirs(OUT, exist_ok=True)
     write_if_changed(os.path.join(OUT, name + ".cuh"), "\n".join(out) + "\n")
     if straight:
-        nparts = parts_for(table.nterms)
+        nparts = parts_for(table.nterms, spec.nvars)
         for suffix, emitter, arg in (("pip", emit_pip, trie), ("pip_e", emit_pip_energy, trie),
                                      ("pip_mixed", emit_pip_mixed, trie), ("dcoef", emit_dcoef, table)):
             body = head + ["#pragma once", '#include "%s.cuh"' % name]
@@ -461,8 +528,10 @@ VARIANTS = {
     # variant: (description, body)
     "g": ("FP64 energy + gradient kernel", """
 int mbx_launch_%(name)s_g(const HolderArgs& A, int grid, int block, cudaStream_t s) {
-    // persistent grid: every resident block slot once (warps claim work dynamically)
-    auto kern = holder_kernel<%(name)s_T, %(name)s_CC, HM_GRAD_FP64, false>;
+    // persistent grid of lockstep blocks: every resident block slot once
+    // (blocks claim chunks of LOCK_THREADS n-mers dynamically)
+    auto kern = holder_lock_kernel<%(name)s_T, %(name)s_CC, HM_GRAD_FP64, false>;
+    block = %(name)s_T::LOCK_THREADS;
     static int bps = 0, sms = 0, bps_block = 0;
     if (!bps || bps_block != block) {
         int dev = 0;
@@ -481,8 +550,10 @@ int mbx_launch_%(name)s_g(const HolderArgs& A, int grid, int block, cudaStream_t
 """),
     "e": ("FP64 energy-only kernel", """
 int mbx_launch_%(name)s_e(const HolderArgs& A, int grid, int block, cudaStream_t s) {
-    // persistent grid: every resident block slot once (warps claim work dynamically)
-    auto kern = holder_kernel<%(name)s_T, %(name)s_CC, HM_ENERGY, false>;
+    // persistent grid of lockstep blocks: every resident block slot once
+    // (blocks claim chunks of LOCK_THREADS n-mers dynamically)
+    auto kern = holder_lock_kernel<%(name)s_T, %(name)s_CC, HM_ENERGY, false>;
+    block = %(name)s_T::LOCK_THREADS;
     static int bps = 0, sms = 0, bps_block = 0;
     if (!bps || bps_block != block) {
         int dev = 0;
@@ -501,8 +572,10 @@ int mbx_launch_%(name)s_e(const HolderArgs& A, int grid, int block, cudaStream_t
 """),
     "m": ("mixed-precision energy + gradient kernel", """
 int mbx_launch_%(name)s_m(const HolderArgs& A, int grid, int block, cudaStream_t s) {
-    // persistent grid: every resident block slot once (warps claim work dynamically)
-    auto kern = holder_kernel<%(name)s_T, %(name)s_CC, HM_GRAD_MIXED, false>;
+    // persistent grid of lockstep blocks: every resident block slot once
+    // (blocks claim chunks of LOCK_THREADS n-mers dynamically)
+    auto kern = holder_lock_kernel<%(name)s_T, %(name)s_CC, HM_GRAD_MIXED, false>;
+    block = %(name)s_T::LOCK_THREADS;
     static int bps = 0, sms = 0, bps_block = 0;
     if (!bps || bps_block != block) {
         int dev = 0;

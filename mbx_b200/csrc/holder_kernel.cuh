@@ -313,6 +313,78 @@ __global__ void __launch_bounds__(128, MBX_HOLDER_MINB) holder_kernel(const Hold
     block_reduce_add<7>(acc, A.out);
 }
 
+// The polynomial (and its gradient) in the precision mode of the kernel, with
+// a block barrier after every separately compiled piece of the trie.
+template <class T, int MODE, class C>
+__device__ __forceinline__ double run_pip_lock(const C& coef, const double (&x)[T::NVARS], double (&g)[T::NVARS]) {
+    if constexpr (MODE == HM_ENERGY) {
+        return T::pip_e_lock(coef, x);
+    } else if constexpr (MODE == HM_GRAD_FP64) {
+        return T::pip_lock(coef, x, g);
+    } else {
+        float xf[T::NVARS], gf[T::NVARS];
+#pragma unroll
+        for (int v = 0; v < T::NVARS; ++v) { xf[v] = (float)x[v]; gf[v] = 0.0f; }
+        const double ep = T::pip_mixed_lock(coef, xf, x, g, gf);
+#pragma unroll
+        for (int v = 0; v < T::NVARS; ++v) g[v] += (double)gf[v];
+        return ep;
+    }
+}
+
+// One n-mer per thread, all warps of a block in lockstep through the trie:
+// the straight-line polynomial is ~10^5 instructions, far more than the
+// instruction cache holds, so the block's warps go through it piece by piece
+// together (a barrier after each piece) and one fetch of a piece's code serves
+// all of them.  Threads without an n-mer (past the end, or beyond the
+// evaluator's cutoff) run the pieces on zero variables and discard the result.
+// Persistent grid; a block claims chunks of blockDim.x n-mers from
+// A.counter (or strides statically without it).
+template <class T, class CC, int MODE, bool CUSTOM>
+__global__ void __launch_bounds__(T::LOCK_THREADS, 1) holder_lock_kernel(const HolderArgs A) {
+    constexpr bool grads = (MODE == HM_GRAD_FP64 || MODE == HM_GRAD_MIXED);
+    __shared__ long s_base;
+    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    const long n = nmer_count(A);
+    long static_next = blockIdx.x * (long)blockDim.x;
+    for (;;) {
+        long base;
+        if (A.counter) {
+            if (threadIdx.x == 0) s_base = atomicAdd(A.counter, (int)blockDim.x);
+            __syncthreads();
+            base = s_base;
+            __syncthreads();
+        } else {
+            base = static_next;
+            static_next += (long)gridDim.x * blockDim.x;
+        }
+        if (base >= n) break;
+        const long t = base + threadIdx.x;
+        bool live = t < n;
+        double x[T::NVARS], g[T::NVARS];
+#pragma unroll
+        for (int v = 0; v < T::NVARS; ++v) { x[v] = 0.0; g[v] = 0.0; }
+        if (live) {
+            double r[T::NREAL][3];
+            load_nmer<T, false>(A, t, r);
+            double d[3][3], rr[3];
+            if (pair_dists<T>(r, d, rr)) {
+                if (A.e_per) A.e_per[t] = 0.0;
+                live = false;
+            } else {
+                double s[T::NSITES][3];
+                T::sites(r, s);
+                T::vars(s, x);
+            }
+        }
+        double ep;
+        if constexpr (CUSTOM) ep = run_pip_lock<T, MODE>(GlobalCoef{A.coef}, x, g);
+        else ep = run_pip_lock<T, MODE>(CC{}, x, g);
+        if (live) finish_nmer<T>(A, t, ep, g, grads, acc);
+    }
+    block_reduce_add<7>(acc, A.out);
+}
+
 // Warp-cooperative evaluation for polynomials too large for straight-line
 // code: lane l handles terms l, l+32, ...; variables and gradient
 // accumulators of the warp's n-mer live in shared memory.

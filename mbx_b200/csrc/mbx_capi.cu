@@ -537,11 +537,26 @@ static int launch_build(mbx_ctx* c, int nbody, int use_ghost, const double* xyz,
     k_cell_count<<<(nmem + T - 1) / T, T, 0, c->stream>>>(c->cell_of.p, nmem, c->cell_count.p);
     k_cell_scan<<<1, 1024, 0, c->stream>>>(c->cell_count.p, ncell, c->cell_start.p, c->cell_fill.p);
     k_cell_fill<<<(nmem + T - 1) / T, T, 0, c->stream>>>(c->cell_of.p, nmem, c->cell_fill.p, c->cell_items.p);
-    k_neighbors<<<(nq * 32 + T - 1) / T, T, 0, c->stream>>>(c->cloud.p, c->cell_of.p, c->cell_start.p,
-                                                            c->cell_items.p, c->d_query[g].p, nq, cg, c->bp.use_pbc,
-                                                            rc2, c->nb_cap, c->nb_count.p, c->nb.p, c->status.p);
+    // one block of 4 warps per query monomer, hits staged in shared memory;
+    // a single warp when four stages would not fit
+    const size_t stage4 = (size_t)4 * c->nb_cap * sizeof(NbEntry);
+    if (stage4 <= 160 * 1024) {
+        if (stage4 > 48 * 1024)
+            CUCHK(c, cudaFuncSetAttribute(k_neighbors4, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage4));
+        k_neighbors4<<<nq, 128, stage4, c->stream>>>(c->cloud.p, c->cell_of.p, c->cell_start.p, c->cell_items.p,
+                                                       c->d_query[g].p, nq, cg, c->bp.use_pbc, rc2, c->nb_cap,
+                                                       c->nb_count.p, c->nb.p, c->status.p);
+    } else {
+        const size_t stage1 = (size_t)c->nb_cap * sizeof(NbEntry);
+        if (stage1 > 227 * 1024) return MBX_ENOMEM;
+        if (stage1 > 48 * 1024)
+            CUCHK(c, cudaFuncSetAttribute(k_neighbors1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage1));
+        k_neighbors1<<<nq, 32, stage1, c->stream>>>(c->cloud.p, c->cell_of.p, c->cell_start.p, c->cell_items.p,
+                                                      c->d_query[g].p, nq, cg, c->bp.use_pbc, rc2, c->nb_cap,
+                                                      c->nb_count.p, c->nb.p, c->status.p);
+    }
     if (nbody == 2) {
-        k_dimers<<<(nq + T - 1) / T, T, 0, c->stream>>>(c->d_query[g].p, nq, c->d_members[g].p, c->d_tag.p,
+        k_dimers<<<(nq * 32 + T - 1) / T, T, 0, c->stream>>>(c->d_query[g].p, nq, c->d_members[g].p, c->d_tag.p,
                                                         c->d_type.p, c->nb_count.p, c->nb.p, c->nb_cap, rc2, c->drules,
                                                         c->listed.p, list_cap > 0 ? c->list.p : nullptr, list_cap,
                                                         c->buckets.p, c->bucket_count.p, c->status.p);

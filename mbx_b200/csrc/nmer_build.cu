@@ -193,76 +193,155 @@ __global__ void k_cell_fill(const int* __restrict__ cell_of, int nmem, int* __re
 
 // Matches of every local monomer: cloud points (member q, copy s) with
 // d^2 < rc_max^2.  One warp per query; matches are appended in candidate order.
-__global__ void k_neighbors(const double* __restrict__ cloud, const int* __restrict__ cell_of,
+// Matches of one query monomer: NW warps of a block split the 27 surrounding
+// cells (each warp a contiguous run of them, in the order below), stage their
+// hits in shared memory and write them out in cell order, so the list is the
+// same as a single warp scanning all cells.  A query with more than `cap`
+// matches sets MBX_STATUS_NB_OVERFLOW and its count in status[1].
+namespace {
+
+template <int NW>
+__device__ __forceinline__ void neighbors_block(const double* __restrict__ cloud, const int* __restrict__ cell_of,
                             const int* __restrict__ cell_start, const int* __restrict__ cell_items,
                             const int* __restrict__ query, int nquery, CellGrid cg, int use_pbc, double rc2,
-                            int cap, int* __restrict__ nb_count, NbEntry* __restrict__ nb, int* __restrict__ status) {
-    const int lane = threadIdx.x & 31;
-    const int wq = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+                            int cap, int* __restrict__ nb_count, NbEntry* __restrict__ nb, int* __restrict__ status,
+                            NbEntry* stage, int* wcount) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int wq = blockIdx.x;
     if (wq >= nquery) return;
     const int qi = query[wq];
     const double* pi = cloud + (size_t)qi * 24;
     const double x0 = pi[0], x1 = pi[1], x2 = pi[2];
     const int c = cell_of[qi];
     const int cx = c % cg.n[0], cy = (c / cg.n[0]) % cg.n[1], cz = c / (cg.n[0] * cg.n[1]);
-    int count = 0;
-    NbEntry* out = nb + (size_t)wq * cap;
     // neighbouring cells; an axis with fewer than 3 cells is scanned once
     const int rx = cg.n[0] >= 3 ? 1 : 0, ry = cg.n[1] >= 3 ? 1 : 0, rz = cg.n[2] >= 3 ? 1 : 0;
     const int sx = cg.n[0] >= 3 ? 3 : cg.n[0], sy = cg.n[1] >= 3 ? 3 : cg.n[1], sz = cg.n[2] >= 3 ? 3 : cg.n[2];
-    for (int dz = 0; dz < sz; ++dz)
-        for (int dy = 0; dy < sy; ++dy)
-            for (int dx = 0; dx < sx; ++dx) {
-                // periodic in index space both with PBC and for the hashed
-                // grid without PBC (n >= 3 there, so the 27 cells are distinct)
-                int ax = rx ? cx + dx - 1 : dx, ay = ry ? cy + dy - 1 : dy, az = rz ? cz + dz - 1 : dz;
-                ax = (ax + cg.n[0]) % cg.n[0];
-                ay = (ay + cg.n[1]) % cg.n[1];
-                az = (az + cg.n[2]) % cg.n[2];
-                const int cell = (az * cg.n[1] + ay) * cg.n[0] + ax;
-                const int b = cell_start[cell], e = cell_start[cell + 1];
-                const int ncopy = use_pbc ? 8 : 1;
-                for (int base = b * ncopy; base < e * ncopy; base += 32) {
-                    const int t = base + lane;
-                    bool hit = false;
-                    NbEntry ent;
-                    if (t < e * ncopy) {
-                        const int qj = cell_items[t / ncopy];
-                        const int s = t % ncopy;
-                        const double* pj = cloud + (size_t)qj * 24 + 3 * s;
-                        const double d2 = dist2_rn(x0, x1, x2, pj[0], pj[1], pj[2]);
-                        if (d2 < rc2) {
-                            hit = true;
-                            ent.member = qj;
-                            ent.copy = s;
-                            ent.d2 = d2;
-                        }
-                    }
-                    const unsigned m = __ballot_sync(0xffffffffu, hit);
-                    if (hit) {
-                        const int pos = count + __popc(m & ((1u << lane) - 1u));
-                        if (pos < cap) out[pos] = ent;
-                    }
-                    count += __popc(m);
+    const int ncell = sx * sy * sz;
+    const int k0 = w * ncell / NW, k1 = (w + 1) * ncell / NW;
+    const int ncopy = use_pbc ? 8 : 1;
+    NbEntry* mine = stage + (size_t)w * cap;
+    int count = 0;
+    for (int k = k0; k < k1; ++k) {
+        const int dx = k % sx, dy = (k / sx) % sy, dz = k / (sx * sy);
+        // periodic in index space both with PBC and for the hashed grid
+        // without PBC (n >= 3 there, so the 27 cells are distinct)
+        int ax = rx ? cx + dx - 1 : dx, ay = ry ? cy + dy - 1 : dy, az = rz ? cz + dz - 1 : dz;
+        ax = (ax + cg.n[0]) % cg.n[0];
+        ay = (ay + cg.n[1]) % cg.n[1];
+        az = (az + cg.n[2]) % cg.n[2];
+        const int cell = (az * cg.n[1] + ay) * cg.n[0] + ax;
+        const int b = cell_start[cell], e = cell_start[cell + 1];
+        for (int base = b * ncopy; base < e * ncopy; base += 32) {
+            const int t = base + lane;
+            bool hit = false;
+            NbEntry ent;
+            if (t < e * ncopy) {
+                const int qj = cell_items[t / ncopy];
+                const int s = t % ncopy;
+                const double* pj = cloud + (size_t)qj * 24 + 3 * s;
+                const double d2 = dist2_rn(x0, x1, x2, pj[0], pj[1], pj[2]);
+                if (d2 < rc2) {
+                    hit = true;
+                    ent.member = qj;
+                    ent.copy = s;
+                    ent.d2 = d2;
                 }
             }
-    if (lane == 0) {
-        nb_count[wq] = count < cap ? count : cap;
-        if (count > cap) {
+            const unsigned m = __ballot_sync(0xffffffffu, hit);
+            if (hit) {
+                const int pos = count + __popc(m & ((1u << lane) - 1u));
+                if (pos < cap) mine[pos] = ent;
+            }
+            count += __popc(m);
+        }
+    }
+    if (lane == 0) wcount[w] = count;
+    __syncthreads();
+    int off = 0, total = 0;
+    for (int j = 0; j < NW; ++j) {
+        off += j < w ? wcount[j] : 0;
+        total += wcount[j];
+    }
+    NbEntry* out = nb + (size_t)wq * cap;
+    const int lim = count < cap ? count : cap;
+    for (int i = lane; i < lim && off + i < cap; i += 32) out[off + i] = mine[i];
+    if (threadIdx.x == 0) {
+        nb_count[wq] = total < cap ? total : cap;
+        if (total > cap) {
             atomicOr(status, MBX_STATUS_NB_OVERFLOW);
-            atomicMax(status + 1, count);
+            atomicMax(status + 1, total);
         }
     }
 }
 
-// Dimers from the matches: (i, j) with d^2 < rc2 and tag_i < tag_j.
+}  // namespace
+
+__global__ void __launch_bounds__(128) k_neighbors4(const double* __restrict__ cloud, const int* __restrict__ cell_of,
+                                                    const int* __restrict__ cell_start,
+                                                    const int* __restrict__ cell_items, const int* __restrict__ query,
+                                                    int nquery, CellGrid cg, int use_pbc, double rc2, int cap,
+                                                    int* __restrict__ nb_count, NbEntry* __restrict__ nb,
+                                                    int* __restrict__ status) {
+    extern __shared__ unsigned char smem[];
+    __shared__ int wcount[4];
+    neighbors_block<4>(cloud, cell_of, cell_start, cell_items, query, nquery, cg, use_pbc, rc2, cap, nb_count, nb,
+                       status, reinterpret_cast<NbEntry*>(smem), wcount);
+}
+
+__global__ void __launch_bounds__(32) k_neighbors1(const double* __restrict__ cloud, const int* __restrict__ cell_of,
+                                                   const int* __restrict__ cell_start,
+                                                   const int* __restrict__ cell_items, const int* __restrict__ query,
+                                                   int nquery, CellGrid cg, int use_pbc, double rc2, int cap,
+                                                   int* __restrict__ nb_count, NbEntry* __restrict__ nb,
+                                                   int* __restrict__ status) {
+    extern __shared__ unsigned char smem[];
+    __shared__ int wcount[1];
+    neighbors_block<1>(cloud, cell_of, cell_start, cell_items, query, nquery, cg, use_pbc, rc2, cap, nb_count, nb,
+                       status, reinterpret_cast<NbEntry*>(smem), wcount);
+}
+
+namespace {
+
+// One slot per lane that wants one, in counters[key]: lanes with the same key
+// share one atomicAdd.  Called by all 32 lanes of the warp.
+__device__ __forceinline__ int warp_reserve(int* counters, int key, bool want) {
+    const int lane = threadIdx.x & 31;
+    const unsigned act = __ballot_sync(0xffffffffu, want);
+    int pos = -1;
+    if (want) {
+        const unsigned peers = __match_any_sync(act, key);
+        const int leader = __ffs(peers) - 1;
+        int base = 0;
+        if (lane == leader) base = atomicAdd(counters + key, __popc(peers));
+        base = __shfl_sync(peers, base, leader);
+        pos = base + __popc(peers & ((1u << lane) - 1u));
+    }
+    return pos;
+}
+
+// Same for one 64-bit counter.
+__device__ __forceinline__ long long warp_reserve_ull(unsigned long long* counter, bool want) {
+    const int lane = threadIdx.x & 31;
+    const unsigned act = __ballot_sync(0xffffffffu, want);
+    unsigned long long base = 0;
+    if (lane == 0 && act) base = atomicAdd(counter, (unsigned long long)__popc(act));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    return want ? (long long)(base + __popc(act & ((1u << lane) - 1u))) : -1;
+}
+
+}  // namespace
+
+// Dimers from the matches: (i, j) with d^2 < rc2 and tag_i < tag_j.  One warp
+// per query monomer, lanes over its matches.
 __global__ void k_dimers(const int* __restrict__ query, int nquery, const int* __restrict__ members,
                          const int* __restrict__ tag, const int* __restrict__ type, const int* __restrict__ nb_count,
                          const NbEntry* __restrict__ nb, int cap, double rc2, DimerRules R,
                          unsigned long long* __restrict__ listed, int4* __restrict__ list, long list_cap,
                          int4* __restrict__ bucket_data, int* __restrict__ bucket_count,
                          int* __restrict__ status) {
-    const int wq = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const int wq = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (wq >= nquery) return;
     const int qi = query[wq];
     const int mi = members[qi];
@@ -270,29 +349,40 @@ __global__ void k_dimers(const int* __restrict__ query, int nquery, const int* _
     const int n = nb_count[wq];
     const NbEntry* e = nb + (size_t)wq * cap;
     unsigned long long mine = 0;
-    for (int a = 0; a < n; ++a) {
-        const NbEntry ea = e[a];
-        if (!(ea.d2 < rc2)) continue;
-        const int mj = members[ea.member];
-        if (!(ti < tag[mj])) continue;
-        ++mine;
-        if (list) {
-            const unsigned long long pos = atomicAdd(listed + 1, 1ull);
-            if ((long)pos < list_cap) list[pos] = make_int4(mi, mj, -1, 0);
+    for (int base = 0; base < n; base += 32) {
+        const int a = base + lane;
+        bool keep = false;
+        int mj = 0, b = -1;
+        double d2 = 0.0;
+        if (a < n) {
+            const NbEntry ea = e[a];
+            d2 = ea.d2;
+            mj = members[ea.member];
+            keep = d2 < rc2 && ti < tag[mj];
         }
-        const int code = type[mi] * MBX_MAX_TYPES + type[mj];
-        const int b = R.bucket[code];
-        if (b < 0) continue;
-        if (ea.d2 > R.pre2[b]) continue;     // cannot pass the evaluator's own cutoff
-        const int pos = atomicAdd(bucket_count + b, 1);
-        if (pos < R.cap[b]) {
-            const int4 rec = R.swap[code] ? make_int4(mj, mi, -1, 1) : make_int4(mi, mj, -1, 0);
-            bucket_data[R.offset[b] + pos] = rec;
-        } else {
-            atomicOr(status, MBX_STATUS_BUCKET_OVERFLOW);
+        mine += keep;
+        if (list) {
+            const long long pos = warp_reserve_ull(listed + 1, keep);
+            if (keep && pos < list_cap) list[pos] = make_int4(mi, mj, -1, 0);
+        }
+        int code = 0;
+        if (keep) {
+            code = type[mi] * MBX_MAX_TYPES + type[mj];
+            b = R.bucket[code];
+            if (b >= 0 && d2 > R.pre2[b]) b = -1;   // cannot pass the evaluator's own cutoff
+        }
+        const bool ins = b >= 0;
+        const int pos = warp_reserve(bucket_count, ins ? b : 0, ins);
+        if (ins) {
+            if (pos < R.cap[b]) {
+                bucket_data[R.offset[b] + pos] = R.swap[code] ? make_int4(mj, mi, -1, 1) : make_int4(mi, mj, -1, 0);
+            } else {
+                atomicOr(status, MBX_STATUS_BUCKET_OVERFLOW);
+            }
         }
     }
-    if (mine) atomicAdd(listed, mine);
+    for (int o = 16; o > 0; o >>= 1) mine += __shfl_xor_sync(0xffffffffu, mine, o);
+    if (lane == 0 && mine) atomicAdd(listed, mine);
 }
 
 // Trimers: one warp per query monomer i, lanes over the pairs of its matches.
@@ -329,45 +419,56 @@ __global__ void k_trimers(const int* __restrict__ query, int nquery, const int* 
     __syncwarp();
     const long npair = (long)n * (n - 1) / 2;
     unsigned long long mine = 0;
-    for (long p = lane; p < npair; p += 32) {
-        // pair index -> (a, b), a < b
-        int a = (int)((2.0 * n - 1 - sqrt((2.0 * n - 1) * (2.0 * n - 1) - 8.0 * p)) / 2.0);
-        if (a < 0) a = 0;
-        while ((long)(a + 1) * (2 * n - a - 2) / 2 <= p) ++a;
-        while ((long)a * (2 * n - a - 1) / 2 > p) --a;
-        const int b = (int)(p - (long)a * (2 * n - a - 1) / 2) + a + 1;
-        const NbEntry ea = sh[a], eb = sh[b];
-        if (ea.member == eb.member) continue;
-        const double* pa = cloud + (size_t)ea.member * 24 + 3 * ea.copy;
-        const double* pb = cloud + (size_t)eb.member * 24 + 3 * eb.copy;
-        const double djk = dist2_rn(pa[0], pa[1], pa[2], pb[0], pb[1], pb[2]);
-        const int mj = members[ea.member], mk = members[eb.member];
-        if (!(djk > rc2 || (ti < tag[mj] && ti < tag[mk]))) continue;
-        ++mine;
-        if (list) {
-            const unsigned long long pos = atomicAdd(listed + 1, 1ull);
-            if ((long)pos < list_cap) list[pos] = make_int4(mi, mj, mk, 0);
+    for (long base = 0; base < npair; base += 32) {
+        const long p = base + lane;
+        bool keep = false;
+        int mj = 0, mk = 0, bk = -1, code = 0;
+        if (p < npair) {
+            // pair index -> (a, b), a < b
+            int a = (int)((2.0 * n - 1 - sqrt((2.0 * n - 1) * (2.0 * n - 1) - 8.0 * p)) / 2.0);
+            if (a < 0) a = 0;
+            while ((long)(a + 1) * (2 * n - a - 2) / 2 <= p) ++a;
+            while ((long)a * (2 * n - a - 1) / 2 > p) --a;
+            const int b = (int)(p - (long)a * (2 * n - a - 1) / 2) + a + 1;
+            const NbEntry ea = sh[a], eb = sh[b];
+            if (ea.member != eb.member) {
+                const double* pa = cloud + (size_t)ea.member * 24 + 3 * ea.copy;
+                const double* pb = cloud + (size_t)eb.member * 24 + 3 * eb.copy;
+                const double djk = dist2_rn(pa[0], pa[1], pa[2], pb[0], pb[1], pb[2]);
+                mj = members[ea.member];
+                mk = members[eb.member];
+                keep = djk > rc2 || (ti < tag[mj] && ti < tag[mk]);
+                if (keep) {
+                    code = (type[mi] * MBX_MAX_TYPES + type[mj]) * MBX_MAX_TYPES + type[mk];
+                    bk = R.bucket[code];
+                    if (bk >= 0) {
+                        // pre-filter with the evaluator's skip rule on the cloud distances
+                        const double rf2 = R.pre2[bk];
+                        const int nfar = (ea.d2 > rf2) + (eb.d2 > rf2) + (djk > rf2);
+                        if ((R.skip[bk] == 1 && nfar >= 2) || (R.skip[bk] == 2 && nfar == 3)) bk = -1;
+                    }
+                }
+            }
         }
-        const int code = (type[mi] * MBX_MAX_TYPES + type[mj]) * MBX_MAX_TYPES + type[mk];
-        const int bk = R.bucket[code];
-        if (bk < 0) continue;
-        // pre-filter with the evaluator's skip rule on the cloud distances
-        const double r2[3] = {ea.d2, eb.d2, djk};
-        const double rf2 = R.pre2[bk];
-        const int nfar = (r2[0] > rf2) + (r2[1] > rf2) + (r2[2] > rf2);
-        if (R.skip[bk] == 1 && nfar >= 2) continue;
-        if (R.skip[bk] == 2 && nfar == 3) continue;
-        const int pos = atomicAdd(bucket_count + bk, 1);
-        if (pos < R.cap[bk]) {
-            const int perm = R.perm[code];   // slot s of the holder takes original slot (perm >> 2s) & 3
-            const int orig[3] = {mi, mj, mk};
-            const int s0 = perm & 3, s1 = (perm >> 2) & 3, s2 = (perm >> 4) & 3;
-            int anchor = 0;
-            if (s1 == 0) anchor = 1;
-            if (s2 == 0) anchor = 2;
-            bucket_data[R.offset[bk] + pos] = make_int4(orig[s0], orig[s1], orig[s2], anchor);
-        } else {
-            atomicOr(status, MBX_STATUS_BUCKET_OVERFLOW);
+        mine += keep;
+        if (list) {
+            const long long pos = warp_reserve_ull(listed + 1, keep);
+            if (keep && pos < list_cap) list[pos] = make_int4(mi, mj, mk, 0);
+        }
+        const bool ins = bk >= 0;
+        const int pos = warp_reserve(bucket_count, ins ? bk : 0, ins);
+        if (ins) {
+            if (pos < R.cap[bk]) {
+                const int perm = R.perm[code];   // slot s of the holder takes original slot (perm >> 2s) & 3
+                const int orig[3] = {mi, mj, mk};
+                const int s0 = perm & 3, s1 = (perm >> 2) & 3, s2 = (perm >> 4) & 3;
+                int anchor = 0;
+                if (s1 == 0) anchor = 1;
+                if (s2 == 0) anchor = 2;
+                bucket_data[R.offset[bk] + pos] = make_int4(orig[s0], orig[s1], orig[s2], anchor);
+            } else {
+                atomicOr(status, MBX_STATUS_BUCKET_OVERFLOW);
+            }
         }
     }
     for (int o = 16; o > 0; o >>= 1) mine += __shfl_xor_sync(0xffffffffu, mine, o);

@@ -562,4 +562,51 @@ int mbxo_holder_dcoef(const mbxo_spec *s, int ncoef, long nterms, const int *tk,
     return 1;
 }
 
+/* The polynomial variables of every n-mer (the first half of holder_eval:
+ * skip rule, lone-pair sites, x_v = exp(k (d0 - r)) [/ r]); x_out[n][nvars],
+ * live[t] = 0 for an n-mer beyond the evaluator's cutoff (its x left 0). */
+long mbxo_holder_vars(const mbxo_spec *s, long n, const double *xyz, double *x_out, unsigned char *live) {
+    int first[3];
+    long nlive = 0;
+    first[0] = 0;
+    for (int m = 1; m < s->nbody; ++m) first[m] = first[m - 1] + s->nat[m - 1];
+#pragma omp parallel for schedule(static) reduction(+ : nlive)
+    for (long t = 0; t < n; ++t) {
+        const double *w = xyz + (size_t)t * s->nreal * 3;
+        double *x = x_out + (size_t)t * s->nvars;
+        double r[3];
+        int pairs[3][2] = {{0, 1}, {0, 2}, {1, 2}};
+        int npair = s->nbody == 2 ? 1 : 3;
+        for (int p = 0; p < npair; ++p) {
+            const double *a1 = w + 3 * first[pairs[p][0]], *a2 = w + 3 * first[pairs[p][1]];
+            double d0 = a1[0] - a2[0], d1 = a1[1] - a2[1], d2 = a1[2] - a2[2];
+            r[p] = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+        }
+        int skip;
+        if (s->skip == 0)
+            skip = r[0] > s->rf;
+        else if (s->skip == 1)
+            skip = (r[0] > s->rf && r[1] > s->rf) || (r[0] > s->rf && r[2] > s->rf) || (r[1] > s->rf && r[2] > s->rf);
+        else
+            skip = r[0] > s->rf && r[1] > s->rf && r[2] > s->rf;
+        for (int v = 0; v < s->nvars; ++v) x[v] = 0.0;
+        live[t] = !skip;
+        if (skip) continue;
+        ++nlive;
+        double sites[32][3], oh1[3][3], oh2[3][3];
+        for (int i = 0; i < s->nreal; ++i)
+            for (int c = 0; c < 3; ++c) sites[i][c] = w[3 * i + c];
+        for (int l = 0; l < s->nlp; ++l)
+            lp_setup(sites[s->lp[l][1]], s->gin, s->gout, sites[s->lp[l][2]], sites[s->lp[l][3]], oh1[l], oh2[l]);
+        for (int v = 0; v < s->nvars; ++v) {
+            const double *p1 = sites[s->vs1[v]], *p2 = sites[s->vs2[v]];
+            double g0 = p1[0] - p2[0], g1 = p1[1] - p2[1], g2 = p1[2] - p2[2];
+            double rr = sqrt(g0 * g0 + g1 * g1 + g2 * g2);
+            double e1 = exp(s->vk[v] * (s->vd[v] - rr));
+            x[v] = s->vkind[v] == 0 ? e1 : e1 / rr;
+        }
+    }
+    return nlive;
+}
+
 long mbxo_spec_size(void) { return (long)sizeof(mbxo_spec); }

@@ -83,6 +83,9 @@ def lib():
         L.mbxo_holder_dcoef.argtypes = [ctypes.POINTER(_Spec), ctypes.c_int, ctypes.c_long, ip, dp, ip, ip, dp, dp]
         L.mbxo_holder_dcoef.restype = ctypes.c_int
         L.mbxo_spec_size.restype = ctypes.c_long
+        L.mbxo_holder_vars.argtypes = [ctypes.POINTER(_Spec), ctypes.c_long, dp, dp,
+                                       ctypes.POINTER(ctypes.c_ubyte)]
+        L.mbxo_holder_vars.restype = ctypes.c_long
         assert L.mbxo_spec_size() == ctypes.sizeof(_Spec)
         _lib = L
     return _lib
@@ -161,6 +164,19 @@ def holder_eval(name, xyz, do_grads=True, a=None, per_nmer=False):
                                _ip(np.ascontiguousarray(t.var)), _p(a), n, _p(xyz), _p(grad),
                                _p(vir) if do_grads else None, _p(eper))
     return e, grad, vir, eper
+
+
+def holder_vars(name, xyz):
+    """Polynomial variables of every n-mer (mbxo_holder_vars): (x[n][nvars],
+    live[n]); x is 0 for n-mers beyond the evaluator's cutoff."""
+    xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+    spec = c_spec(name)
+    n = xyz.shape[0]
+    x = np.zeros((n, spec.nvars))
+    live = np.zeros(n, dtype=np.uint8)
+    lib().mbxo_holder_vars(ctypes.byref(spec), ctypes.c_long(n), _p(xyz), _p(x),
+                           live.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte)))
+    return x, live.astype(bool)
 
 
 def holder_dcoef(name, xyz):
