@@ -9,9 +9,8 @@ For each evaluator in ``mbx_b200.specs.SPECS`` this writes
 * ``<name>_pip``: the polynomial and its reverse-mode gradient, as a
   multivariate Horner trie over the expanded term table;
 * ``<name>_pip_e``: the energy-only Horner evaluation;
-* ``<name>_pip_mixed``: the same trie with the leaf level (three quarters of
-  all terms) in FP32 and the upper levels and every accumulation above the
-  leaves in FP64;
+* ``<name>_pip_s32`` (types in SHIFT_TYPES): the FP32 trie of the type's FP32
+  basis (codegen/shift.py), the mixed-precision polynomial;
 * ``<name>_dcoef``: per-coefficient monomial sums dP/da_k (for the adjoint with
   respect to the linear coefficients), recomputed from x.
 
@@ -32,6 +31,8 @@ import argparse
 import collections
 import os
 import sys
+
+import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.dirname(HERE)
@@ -95,6 +96,20 @@ class Trie:
 # of a node is split (1 = one serial chain per node).
 SPLIT = "terms"
 ACC_CHAINS = 1
+
+# Mixed precision (paired FP32 trie, the "s" kernels).  "median": the
+# polynomial is re-expanded around a symmetric reference point in the middle
+# of liquid data (codegen/shift.py); "identity": the original basis in FP32.
+# Types not listed run FP64 in the mixed mode.  MB-pol 2b is not listed: in
+# FP32 (identity basis, FP32 coefficients and leaf sums) its energy over the
+# 2048-water box is off by 1.1e-5 even with the dimers below 4.5 A in FP64
+# (the shifted basis does not condition it either).
+SHIFT_TYPES = {"mbpol3b": "median"}
+# Optional: n-mers whose first-atom distance is below this radius (A) run the
+# FP64 kernel in the mixed mode (a type of SHIFT_TYPES whose short-range
+# n-mers cancel too strongly for FP32); the builder puts them in a bucket of
+# their own.
+MIXED_FP64_RADIUS = {}
 
 
 def coef_expr(coefs, fp32=False):
@@ -190,21 +205,24 @@ def emit_split(trie, nvars, name, out, nparts, arrays, body, ret="double"):
         code = "\n".join(text)
         params = ", ".join("%s%s* __restrict__ %sm" % ("const " if role == "in" else "", ct, a)
                            for a, ct, role in arrays)
+        zero = {"float": "0.0f", "double": "0.0", "f2_t": "0ull"}
         w("template <class Coef>")
         w("__device__ __noinline__ %s %s_part%d(const Coef& coef, %s) {" % (ret, name, i, params))
         for a, ct, role in arrays:
             used = sorted({int(v) for v in re.findall(r"\b%s\[(\d+)\]" % a, code)})
             w("    %s %s[%d];" % (ct, a, nvars))
             for v in used:
-                w("    %s[%d] = %s;" % (a, v, ("%sm[%d]" % (a, v)) if role == "in" else
-                                        ("0.0f" if ct == "float" else "0.0")))
-        w("    %s E = 0.0;" % ret)
+                w("    %s[%d] = %s;" % (a, v, ("%sm[%d]" % (a, v)) if role == "in" else zero[ct]))
+        w("    %s E = %s;" % (ret, "make_double2(0.0, 0.0)" if ret == "double2" else "0.0"))
         w(code)
         for a, ct, role in arrays:
             if role == "acc":
                 used = sorted({int(v) for v in re.findall(r"\b%s\[(\d+)\]" % a, code)})
                 for v in used:
-                    w("    %sm[%d] += %s[%d];" % (a, v, a, v))
+                    if ct == "f2_t":
+                        w("    %sm[%d] = f2_add(%sm[%d], %s[%d]);" % (a, v, a, v, a, v))
+                    else:
+                        w("    %sm[%d] += %s[%d];" % (a, v, a, v))
         w("    return E;")
         w("}")
     sig = ", ".join("%s%s (&%s)[%d]" % ("const " if role == "in" else "", ct, a, nvars) for a, ct, role in arrays)
@@ -214,10 +232,14 @@ def emit_split(trie, nvars, name, out, nparts, arrays, body, ret="double"):
         # piece at the same time and share its instruction fetches
         w("template <class Coef>")
         w("__device__ __forceinline__ %s %s%s(const Coef& coef, %s) {" % (ret, name, "_lock" if lock else "", sig))
-        w("    %s E = 0.0;" % ret)
+        w("    %s E = %s;" % (ret, "make_double2(0.0, 0.0)" if ret == "double2" else "0.0"))
         for i in range(len(pieces)):
-            w("    E += %s_part%d(coef, %s);%s" % (name, i, ", ".join(a for a, _, _ in arrays),
-                                                 " __syncthreads();" if lock else ""))
+            call = "%s_part%d(coef, %s)" % (name, i, ", ".join(a for a, _, _ in arrays))
+            bar = " __syncthreads();" if lock else ""
+            if ret == "double2":
+                w("    { const double2 e = %s; E.x += e.x; E.y += e.y; }%s" % (call, bar))
+            else:
+                w("    E += %s;%s" % (call, bar))
         w("    return E;")
         w("}")
 
@@ -270,6 +292,81 @@ def emit_pip(trie, nvars, name, out, nparts=1):
     emit_split(trie, nvars, name, out, nparts, [("x", "double", "in"), ("g", "double", "acc")], body)
 
 
+def emit_pip_f32x2(trie, nvars, name, out, nparts=1):
+    """FP32 value + gradient over the trie for two n-mers at once (the low and
+    high halves of every f2_t, paired FP32 instructions): monomials,
+    coefficients and leaf sums in FP32; the top-level products are added to
+    the two energies in FP64."""
+    out.append("// %s: paired FP32 polynomial and reverse-mode gradient (multivariate Horner trie)" % name)
+
+    def cexpr(coefs):
+        if not coefs:
+            return None
+        assert all(c == 1.0 for _, c in coefs)
+        parts = ["coef.f2(%d)" % k for k, _ in coefs]
+        e = parts[0]
+        for p in parts[1:]:
+            e = "f2_add(%s, %s)" % (e, p)
+        return e
+
+    def body(w, subtrees):
+        def node(n, var, depth, pexpr):
+            P = "P%d" % depth
+            V = "V%d" % depth
+            if pexpr is None:
+                w("    { const f2_t %s = x[%d];" % (P, var))
+            else:
+                w("    { const f2_t %s = f2_mul(%s, x[%d]);" % (P, pexpr, var))
+            ce = cexpr(n["coef"])
+            w("      f2_t %s = %s;" % (V, ce if ce else "0ull"))
+            for cv, ch in n["kids"].items():
+                if ch["kids"]:
+                    node(ch, cv, depth + 1, P)
+                else:
+                    c = cexpr(ch["coef"])
+                    w("      { const f2_t c = %s; %s = f2_fma(c, x[%d], %s); g[%d] = f2_fma(c, %s, g[%d]); }" %
+                      (c, V, cv, V, cv, P, cv))
+            if pexpr is None:
+                w("      g[%d] = f2_add(g[%d], %s);" % (var, var, V))
+                w("      E.x = fma((double)f2_lo(x[%d]), (double)f2_lo(%s), E.x); "
+                  "E.y = fma((double)f2_hi(x[%d]), (double)f2_hi(%s), E.y); }" % (var, V, var, V))
+            else:
+                w("      g[%d] = f2_fma(%s, %s, g[%d]); V%d = f2_fma(x[%d], %s, V%d); }" %
+                  (var, pexpr, V, var, depth - 1, var, V, depth - 1))
+
+        for var, ch in subtrees:
+            if ch["kids"]:
+                node(ch, var, 1, None)
+            else:
+                c = cexpr(ch["coef"])
+                w("    { const f2_t c = %s; g[%d] = f2_add(g[%d], c);" % (c, var, var))
+                w("      E.x = fma((double)f2_lo(c), (double)f2_lo(x[%d]), E.x); "
+                  "E.y = fma((double)f2_hi(c), (double)f2_hi(x[%d]), E.y); }" % (var, var))
+
+    emit_split(trie, nvars, name, out, nparts, [("x", "f2_t", "in"), ("g", "f2_t", "acc")], body, ret="double2")
+
+
+def shifted_pip(name):
+    """codegen.shift.ShiftedPip of a type in SHIFT_TYPES (cached)."""
+    from mbx_b200.codegen import shift
+    if name in _SHIFTED:
+        return _SHIFTED[name]
+    spec, table = SPECS[name], load_pip(name)
+    if SHIFT_TYPES[name] == "median":
+        sp = shift.shifted(spec, table)
+    else:
+        monos = [tuple(sorted(table.var[t, :table.deg[t]].tolist())) for t in range(table.nterms)]
+        sp = shift.ShiftedPip(spec.nvars, spec.ncoef, np.zeros(spec.nvars), monos,
+                              [int(k) for k in table.k], {}, [{k: 1.0} for k in range(spec.ncoef)], [])
+        # the identity basis keeps the term multiplicities of the table
+        assert all(c == 1.0 for c in table.coef)
+    _SHIFTED[name] = sp
+    return sp
+
+
+_SHIFTED = {}
+
+
 def emit_pip_energy(trie, nvars, name, out, nparts=1):
     """FP64 value only: plain Horner over the trie."""
     def body(w, subtrees):
@@ -292,64 +389,6 @@ def emit_pip_energy(trie, nvars, name, out, nparts=1):
                 w("    E = fma(%s, x[%d], E);" % (coef_expr(ch["coef"]), var))
 
     emit_split(trie, nvars, name, out, nparts, [("x", "double", "in")], body)
-
-
-def emit_pip_mixed(trie, nvars, name, out, nparts=1):
-    """Mixed precision: products and leaf-level sums in FP32, everything that
-    accumulates across leaf groups (inner-node values, the energy) in FP64.
-
-    Leaf gradient contributions go to FP32 accumulators gf[] (each receives one
-    product per leaf); inner-node gradient contributions go to FP64 g[].  The
-    caller adds gf into g at the end."""
-    def body(w, subtrees):
-        def node(n, var, depth, pexpr_f, pexpr_d):
-            Pf = "Pf%d" % depth
-            Pd = "Pd%d" % depth
-            leaf_only = all(not ch["kids"] for ch in n["kids"].values())
-            if pexpr_f is None:
-                w("    { const float %s = xf[%d];" % (Pf, var))
-                if not leaf_only:
-                    w("      const double %s = x[%d];" % (Pd, var))
-            else:
-                w("    { const float %s = %s * xf[%d];" % (Pf, pexpr_f, var))
-                if not leaf_only:
-                    w("      const double %s = %s * x[%d];" % (Pd, pexpr_d, var))
-            if leaf_only:
-                V = "Vf%d" % depth
-                ce = coef_expr(n["coef"], True)
-                w("      float %s = %s;" % (V, ce if ce else "0.0f"))
-                for cv, ch in n["kids"].items():
-                    c = coef_expr(ch["coef"], True)
-                    w("      %s = fmaf(%s, xf[%d], %s); gf[%d] = fmaf(%s, %s, gf[%d]);" %
-                      (V, c, cv, V, cv, c, Pf, cv))
-                Vd = "(double)%s" % V
-            else:
-                V = "Vd%d" % depth
-                ce = coef_expr(n["coef"])
-                w("      double %s = %s;" % (V, ce if ce else "0.0"))
-                for cv, ch in n["kids"].items():
-                    if ch["kids"]:
-                        node(ch, cv, depth + 1, Pf, Pd)
-                    else:
-                        c = coef_expr(ch["coef"])
-                        w("      %s = fma(%s, x[%d], %s); g[%d] = fma(%s, %s, g[%d]);" %
-                          (V, c, cv, V, cv, c, Pd, cv))
-                Vd = V
-            if pexpr_f is None:
-                w("      g[%d] += %s; E = fma(x[%d], %s, E); }" % (var, Vd, var, Vd))
-            else:
-                w("      g[%d] = fma(%s, %s, g[%d]); Vd%d = fma(x[%d], %s, Vd%d); }" %
-                  (var, pexpr_d, Vd, var, depth - 1, var, Vd, depth - 1))
-
-        for var, ch in subtrees:
-            if ch["kids"]:
-                node(ch, var, 1, None, None)
-            else:
-                c = coef_expr(ch["coef"])
-                w("    E = fma(%s, x[%d], E); g[%d] += %s;" % (c, var, var, c))
-
-    emit_split(trie, nvars, name, out, nparts,
-               [("xf", "float", "in"), ("x", "double", "in"), ("g", "double", "acc"), ("gf", "float", "acc")], body)
 
 
 def emit_dcoef(table, nvars, name, out):
@@ -419,6 +458,16 @@ def emit_traits(spec, table, straight, out):
     w("    static constexpr double RI = %s, RF = %s;" % (lit(spec.ri), lit(spec.rf)))
     w("    static constexpr int LOCK_THREADS = %d;  // threads of a lockstep evaluation block" %
       lock_threads(spec.nvars))
+    shifted_type = straight and n in SHIFT_TYPES
+    w("    static constexpr int SHIFTED = %d, LOCK_THREADS_S = %d;  // paired FP32 (shifted-basis) kernel" %
+      (1 if shifted_type else 0, 256 if shifted_type else lock_threads(spec.nvars)))
+    if shifted_type:
+        w("    __device__ __forceinline__ static void shift(const double (&x)[%d], float (&xf)[%d]) "
+          "{ %s_shift(x, xf); }" % (spec.nvars, spec.nvars, n))
+        for lk in ("", "_lock"):
+            w("    template <class C> __device__ __forceinline__ static double2 pip_s32%s(const C& c, "
+              "const f2_t (&x)[%d], f2_t (&g)[%d]) { return %s_pip_s32%s(c, x, g); }" %
+              (lk, spec.nvars, spec.nvars, n, lk))
     w("    __device__ __forceinline__ static void sites(const double (&r)[%d][3], double (&s)[%d][3]) { %s_sites(r, s); }" %
       (spec.nreal, ns, n))
     w("    __device__ __forceinline__ static void vars(const double (&s)[%d][3], double (&x)[%d]) { %s_vars(s, x); }" %
@@ -431,9 +480,7 @@ def emit_traits(spec, table, straight, out):
               "double (&g)[%d]) { return %s_pip%s(c, x, g); }" % (lk, spec.nvars, spec.nvars, n, lk))
             w("    template <class C> __device__ __forceinline__ static double pip_e%s(const C& c, const double (&x)[%d]) "
               "{ return %s_pip_e%s(c, x); }" % (lk, spec.nvars, n, lk))
-            w("    template <class C> __device__ __forceinline__ static double pip_mixed%s(const C& c, "
-              "const float (&xf)[%d], const double (&x)[%d], double (&g)[%d], float (&gf)[%d]) "
-              "{ return %s_pip_mixed%s(c, xf, x, g, gf); }" % (lk, spec.nvars, spec.nvars, spec.nvars, spec.nvars, n, lk))
+
         w("    template <class S> __device__ __forceinline__ static void dcoef(const double (&x)[%d], S&& sink) "
           "{ %s_dcoef(x, sink); }" % (spec.nvars, n))
     w("};")
@@ -467,25 +514,45 @@ def generate(name):
             out += ["template <class Coef> __device__ __forceinline__ double %s_pip%s(const Coef&, const double (&)[%d], "
                     "double (&)[%d]);" % (name, lk, nv, nv),
                     "template <class Coef> __device__ __forceinline__ double %s_pip_e%s(const Coef&, "
-                    "const double (&)[%d]);" % (name, lk, nv),
-                    "template <class Coef> __device__ __forceinline__ double %s_pip_mixed%s(const Coef&, "
-                    "const float (&)[%d], const double (&)[%d], double (&)[%d], float (&)[%d]);" %
-                    (name, lk, nv, nv, nv, nv)]
+                    "const double (&)[%d]);" % (name, lk, nv)]
         out += ["template <class Sink> __device__ __forceinline__ void %s_dcoef(const double (&)[%d], Sink&&);" %
                 (name, nv)]
+        if name in SHIFT_TYPES:
+            sp = shifted_pip(name)
+            for lk in ("", "_lock"):
+                out.append("template <class Coef> __device__ __forceinline__ double2 %s_pip_s32%s(const Coef&, "
+                           "const f2_t (&)[%d], f2_t (&)[%d]);" % (name, lk, nv, nv))
+            out.append("// dx = x - x0, the reference point of the FP32 basis (%s)" % SHIFT_TYPES[name])
+            out.append("__device__ __forceinline__ void %s_shift(const double (&x)[%d], float (&xf)[%d]) {" %
+                       (name, nv, nv))
+            for v in range(nv):
+                if sp.x0[v] == 0.0:
+                    out.append("    xf[%d] = (float)x[%d];" % (v, v))
+                else:
+                    out.append("    xf[%d] = (float)(x[%d] - %s);" % (v, v, lit(float(sp.x0[v]))))
+            out.append("}")
     emit_traits(spec, table, straight, out)
     os.makedirs(OUT, exist_ok=True)
     write_if_changed(os.path.join(OUT, name + ".cuh"), "\n".join(out) + "\n")
     if straight:
         nparts = parts_for(table.nterms, spec.nvars)
         for suffix, emitter, arg in (("pip", emit_pip, trie), ("pip_e", emit_pip_energy, trie),
-                                     ("pip_mixed", emit_pip_mixed, trie), ("dcoef", emit_dcoef, table)):
+                                     ("dcoef", emit_dcoef, table)):
             body = head + ["#pragma once", '#include "%s.cuh"' % name]
             if emitter is emit_dcoef:
                 emitter(arg, nv, "%s_%s" % (name, suffix), body)
             else:
                 emitter(arg, nv, "%s_%s" % (name, suffix), body, nparts)
             write_if_changed(os.path.join(OUT, "%s_%s.cuh" % (name, suffix)), "\n".join(body) + "\n")
+        if name in SHIFT_TYPES:
+            from mbx_b200.codegen.shift import ShiftedTable
+            sp = shifted_pip(name)
+            strie = Trie(ShiftedTable(sp, name))
+            body = head + ["#pragma once", '#include "%s.cuh"' % name,
+                           "// %d monomials of the %s basis, %d coefficient orbits" %
+                           (len(sp.monos), SHIFT_TYPES[name], sp.norb)]
+            emit_pip_f32x2(strie, nv, "%s_pip_s32" % name, body, max(1, (len(sp.monos) + 699) // 700))
+            write_if_changed(os.path.join(OUT, "%s_pip_s32.cuh" % name), "\n".join(body) + "\n")
     return os.path.join(OUT, name + ".cuh"), leaves, inner
 
 
@@ -570,28 +637,6 @@ int mbx_launch_%(name)s_e(const HolderArgs& A, int grid, int block, cudaStream_t
     return (int)cudaGetLastError();
 }
 """),
-    "m": ("mixed-precision energy + gradient kernel", """
-int mbx_launch_%(name)s_m(const HolderArgs& A, int grid, int block, cudaStream_t s) {
-    // persistent grid of lockstep blocks: every resident block slot once
-    // (blocks claim chunks of LOCK_THREADS n-mers dynamically)
-    auto kern = holder_lock_kernel<%(name)s_T, %(name)s_CC, HM_GRAD_MIXED, false>;
-    block = %(name)s_T::LOCK_THREADS;
-    static int bps = 0, sms = 0, bps_block = 0;
-    if (!bps || bps_block != block) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, block, 0);
-        if (bps < 1) bps = 1;
-        bps_block = block;
-    }
-    const long need = (A.n + block - 1) / block;
-    grid = (int)(need < (long)sms * bps ? need : (long)sms * bps);
-    if (grid < 1) grid = 1;
-    kern<<<grid, block, 0, s>>>(A);
-    return (int)cudaGetLastError();
-}
-"""),
     "c": ("coefficient-gradient (adjoint) kernel", """
 int mbx_launch_%(name)s_c(const HolderArgs& A, const double* w, double* out, int grid, int block, cudaStream_t s) {
     holder_dcoef_kernel<%(name)s_T><<<grid, block, 0, s>>>(A, w, out);
@@ -614,7 +659,103 @@ int mbx_launch_%(name)s_w(const HolderArgs& A, int grads, int grid, cudaStream_t
 
 
 def variants_of(name):
-    return "gemcp" if load_pip(name).nterms <= STRAIGHT_LINE_MAX_TERMS else "w"
+    if load_pip(name).nterms > STRAIGHT_LINE_MAX_TERMS:
+        return "w"
+    return "gecp" + ("s" if name in SHIFT_TYPES else "")
+
+
+SHIFT_TU = """// Generated by mbx_b200/codegen/gen_kernels.py -- do not edit.
+// Paired FP32 (%(basis)s basis) energy + gradient kernel for the %(name)s evaluator.
+#include <cstring>
+#include <vector>
+#include "../holder_kernel.cuh"
+#include "%(name)s.cuh"
+#include "%(name)s_pip_s32.cuh"
+
+// one coefficient per monomial orbit of the basis, as an FP32 pair (c, c)
+// for the paired instructions
+static __constant__ f2_t cs_%(name)s[%(norb)d];
+static __constant__ double cs0_%(name)s[1];        // constant term (FP64)
+struct %(name)s_CS {
+    __device__ __forceinline__ f2_t f2(int k) const { return cs_%(name)s[k]; }
+    __device__ __forceinline__ double b0() const { return cs0_%(name)s[0]; }
+};
+
+// b = F a: the basis coefficients are linear in the fitted ones.  Row j of F
+// (entries sF_row[j] .. sF_row[j+1]) lists (k, factor); sF0 is the constant.
+static const int sF_row_%(name)s[%(norb1)d] = {%(rows)s};
+static const int sF_k_%(name)s[%(nnz)d] = {%(ks)s};
+static const double sF_f_%(name)s[%(nnz)d] = {%(fs)s};
+static const int sF0_k_%(name)s[%(nnz0)d] = {%(k0)s};
+static const double sF0_f_%(name)s[%(nnz0)d] = {%(f0)s};
+
+int mbx_set_coef_%(name)s_s(const double* a, int from_device, cudaStream_t s) {
+    std::vector<double> h(%(ncoef)d);
+    cudaError_t e = cudaSuccess;
+    if (from_device) {
+        e = cudaMemcpyAsync(h.data(), a, sizeof(double) * %(ncoef)d, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return (int)e;
+    } else {
+        for (int k = 0; k < %(ncoef)d; ++k) h[k] = a[k];
+    }
+    std::vector<unsigned long long> b(%(norb)d);
+    for (int j = 0; j < %(norb)d; ++j) {
+        double acc = 0.0;
+        for (int q = sF_row_%(name)s[j]; q < sF_row_%(name)s[j + 1]; ++q) acc += sF_f_%(name)s[q] * h[sF_k_%(name)s[q]];
+        const float f = (float)acc;
+        unsigned int u;
+        memcpy(&u, &f, sizeof(u));
+        b[j] = (unsigned long long)u | ((unsigned long long)u << 32);
+    }
+    double b0 = 0.0;
+    for (int q = 0; q < %(nnz0)d; ++q) b0 += sF0_f_%(name)s[q] * h[sF0_k_%(name)s[q]];
+    e = cudaMemcpyToSymbolAsync(cs_%(name)s, b.data(), sizeof(unsigned long long) * %(norb)d, 0,
+                                cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyToSymbolAsync(cs0_%(name)s, &b0, sizeof(double), 0, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    return (int)e;
+}
+
+int mbx_launch_%(name)s_s(const HolderArgs& A, int grid, int block, cudaStream_t s) {
+    // persistent grid of lockstep blocks (two n-mers per thread): every
+    // resident block slot once
+    auto kern = holder_pair_kernel<%(name)s_T, %(name)s_CS>;
+    block = %(name)s_T::LOCK_THREADS_S;
+    static int bps = 0, sms = 0;
+    if (!bps) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, block, 0);
+        if (bps < 1) bps = 1;
+    }
+    const long need = (A.n + 2 * block - 1) / (2 * block);
+    grid = (int)(need < (long)sms * bps ? need : (long)sms * bps);
+    if (grid < 1) grid = 1;
+    kern<<<grid, block, 0, s>>>(A);
+    return (int)cudaGetLastError();
+}
+"""
+
+
+def write_shift_tu(name, path):
+    sp = shifted_pip(name)
+    rows, ks, fs = [0], [], []
+    for row in sp.F:
+        for k, f in sorted(row.items()):
+            ks.append(k)
+            fs.append(f)
+        rows.append(len(ks))
+    k0 = sorted(sp.const_F)
+    d = {"name": name, "basis": SHIFT_TYPES[name], "norb": sp.norb, "norb1": sp.norb + 1,
+         "ncoef": SPECS[name].ncoef, "nnz": len(ks), "nnz0": max(1, len(k0)),
+         "rows": ",".join(map(str, rows)), "ks": ",".join(map(str, ks)),
+         "fs": ",".join(repr(float(f)) for f in fs),
+         "k0": ",".join(map(str, k0)) if k0 else "0",
+         "f0": ",".join(repr(float(sp.const_F[k])) for k in k0) if k0 else "0.0"}
+    write_tu(path, SHIFT_TU % d)
 
 
 def write_tu(path, text):
@@ -627,8 +768,13 @@ def write_tu(path, text):
 def write_kernels_cu(name):
     spec = SPECS[name]
     paths = []
-    inc = {"g": "pip", "e": "pip_e", "m": "pip_mixed", "c": "dcoef", "p": "pip", "w": None}
+    inc = {"g": "pip", "e": "pip_e", "c": "dcoef", "p": "pip", "w": None}
     for v in variants_of(name):
+        if v == "s":
+            path = os.path.join(OUT, "%s_s.cu" % name)
+            write_shift_tu(name, path)
+            paths.append(path)
+            continue
         what, body = VARIANTS[v]
         d = {"name": name, "ncoef": spec.ncoef, "v": v, "what": what,
              "include": ('#include "%s_%s.cuh"\n' % (name, inc[v])) if inc[v] else ""}
@@ -645,10 +791,10 @@ def write_registry():
              '#include "../holder_kernel.cuh"', ""]
     for name in SPECS:
         vs = variants_of(name)
-        for v in "gemcpw":
+        for v in "gecpws":
             if v not in vs:
                 continue
-            if v in "gem":
+            if v in "ges":
                 lines.append("int mbx_launch_%s_%s(const HolderArgs& A, int grid, int block, cudaStream_t s);" %
                              (name, v))
             elif v == "c":
@@ -674,11 +820,12 @@ def write_registry():
 
         def fn(v, kind):
             return ("mbx_%s_%s_%s" % (kind, name, v)) if v in vs else "nullptr"
-        lines.append('    {"%s", %d, {"%s", "%s", "%s"}, %s, %d, %d, %d, %d, mbx_fit_%s, %s, %s, %s, %s, %s, %s,' %
+        lines.append('    {"%s", %d, {"%s", "%s", "%s"}, %s, %d, %d, %d, %d, mbx_fit_%s, %s, %s, %s, %s, %s, %s, %s,' %
                      (name, spec.nbody, ids[0], ids[1], ids[2], lit(spec.rf), skip, spec.ncoef, spec.nreal,
-                      spec.nvars, name, fn("g", "launch"), fn("e", "launch"), fn("m", "launch"), fn("c", "launch"),
-                      fn("p", "launch"), fn("w", "launch")))
-        lines.append("     {%s}}," % ", ".join(fn(v, "set_coef") for v in "gemcpw"))
+                      spec.nvars, name, fn("g", "launch"), fn("e", "launch"), fn("c", "launch"),
+                      fn("p", "launch"), fn("w", "launch"), fn("s", "launch"),
+                      lit(MIXED_FP64_RADIUS.get(name, 0.0))))
+        lines.append("     {%s, nullptr}}," % ", ".join(fn(v, "set_coef") for v in "gecpws"))
     lines.append("};")
     lines.append("static const int mbx_num_evaluators = %d;" % len(SPECS))
     write_tu(os.path.join(OUT, "registry.inc"), "\n".join(lines) + "\n")

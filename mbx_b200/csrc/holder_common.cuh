@@ -14,6 +14,30 @@
 #include <cuda_runtime.h>
 #include <math.h>
 
+// Two FP32 lanes in one 64-bit register (low half: first value), operated on
+// by the paired FP32 instructions of sm_100 (one instruction, two results).
+typedef unsigned long long f2_t;
+__device__ __forceinline__ f2_t f2_fma(f2_t a, f2_t b, f2_t c) {
+    f2_t d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+__device__ __forceinline__ f2_t f2_mul(f2_t a, f2_t b) {
+    f2_t d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f2_t f2_add(f2_t a, f2_t b) {
+    f2_t d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f2_t f2_pack(float lo, float hi) {
+    return (f2_t)__float_as_uint(lo) | ((f2_t)__float_as_uint(hi) << 32);
+}
+__device__ __forceinline__ float f2_lo(f2_t a) { return __uint_as_float((unsigned)a); }
+__device__ __forceinline__ float f2_hi(f2_t a) { return __uint_as_float((unsigned)(a >> 32)); }
+
 #define MBX_LP_GAMMA_IN (-9.721486914088159e-02)
 #define MBX_LP_GAMMA_OUT (9.859272078406150e-02)
 

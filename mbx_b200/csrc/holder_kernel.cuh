@@ -20,7 +20,7 @@
 #include "holder_common.cuh"
 
 // Precision / output modes.
-enum { HM_ENERGY = 0, HM_GRAD_FP64 = 1, HM_GRAD_MIXED = 2, HM_ENERGY_MIXED = 3 };
+enum { HM_ENERGY = 0, HM_GRAD_FP64 = 1 };
 
 struct HolderArgs {
     long n;                    // number of n-mers (capacity when n_dev is set)
@@ -223,94 +223,12 @@ __device__ __forceinline__ void finish_nmer(const HolderArgs& A, long t, double 
     }
 }
 
-// One n-mer per thread, straight-line polynomial.
+// Number of n-mers to evaluate (0 when the n-mer build reported a failure).
 __device__ __forceinline__ long nmer_count(const HolderArgs& A) {
     if (A.status && *A.status) return 0;
     if (!A.n_dev) return A.n;
     const long c = *A.n_dev;
     return c < A.n ? c : A.n;
-}
-
-// Claims the next chunk of 32 n-mers for the calling warp: dynamic load
-// balance (a skipped n-mer costs nothing, an evaluated one ~10^5 flops).
-__device__ __forceinline__ long claim_chunk(const HolderArgs& A, long& static_next) {
-    const int lane = threadIdx.x & 31;
-    if (A.counter) {
-        int b = 0;
-        if (lane == 0) b = atomicAdd(A.counter, 32);
-        return (long)__shfl_sync(0xffffffffu, b, 0);
-    }
-    const long b = static_next;
-    static_next += (long)gridDim.x * blockDim.x;
-    return b;
-}
-
-// The polynomial (and its gradient) in the precision mode of the kernel.
-template <class T, int MODE, class C>
-__device__ __forceinline__ double run_pip(const C& coef, const double (&x)[T::NVARS], double (&g)[T::NVARS]) {
-    if constexpr (MODE == HM_ENERGY) {
-        return T::pip_e(coef, x);
-    } else if constexpr (MODE == HM_GRAD_FP64) {
-        return T::pip(coef, x, g);
-    } else {
-        float xf[T::NVARS], gf[T::NVARS];
-#pragma unroll
-        for (int v = 0; v < T::NVARS; ++v) { xf[v] = (float)x[v]; gf[v] = 0.0f; }
-        const double ep = T::pip_mixed(coef, xf, x, g, gf);
-#pragma unroll
-        for (int v = 0; v < T::NVARS; ++v) g[v] += (double)gf[v];
-        return ep;
-    }
-}
-
-// One n-mer: gather, skip rule, variables, polynomial, then finish_nmer.
-template <class T, class CC, int MODE, bool CUSTOM>
-__device__ __forceinline__ void eval_nmer(const HolderArgs& A, long t, double (&acc)[7]) {
-    constexpr bool grads = (MODE == HM_GRAD_FP64 || MODE == HM_GRAD_MIXED);
-    double ep;
-    double g[T::NVARS];
-    {
-        double r[T::NREAL][3];
-        load_nmer<T, false>(A, t, r);
-        double d[3][3], rr[3];
-        if (pair_dists<T>(r, d, rr)) {
-            if (A.e_per) A.e_per[t] = 0.0;
-            return;
-        }
-        double s[T::NSITES][3];
-        T::sites(r, s);
-        double x[T::NVARS];
-        T::vars(s, x);
-#pragma unroll
-        for (int v = 0; v < T::NVARS; ++v) g[v] = 0.0;
-        if constexpr (T::STRAIGHT) {
-            if constexpr (CUSTOM) ep = run_pip<T, MODE>(GlobalCoef{A.coef}, x, g);
-            else ep = run_pip<T, MODE>(CC{}, x, g);
-        } else {
-            ep = 0.0;
-        }
-    }
-    finish_nmer<T>(A, t, ep, g, grads, acc);
-}
-
-#ifndef MBX_HOLDER_MINB
-#define MBX_HOLDER_MINB 1
-#endif
-// One n-mer per thread; persistent grid, warps claim chunks of 32 n-mers
-// from a global counter.
-template <class T, class CC, int MODE, bool CUSTOM>
-__global__ void __launch_bounds__(128, MBX_HOLDER_MINB) holder_kernel(const HolderArgs A) {
-    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
-    const long n = nmer_count(A);
-    const int lane = threadIdx.x & 31;
-    long static_next = blockIdx.x * (long)blockDim.x + (threadIdx.x & ~31);
-    for (;;) {
-        const long base = claim_chunk(A, static_next);
-        if (base >= n) break;
-        const long t = base + lane;
-        if (t < n) eval_nmer<T, CC, MODE, CUSTOM>(A, t, acc);
-    }
-    block_reduce_add<7>(acc, A.out);
 }
 
 // The polynomial (and its gradient) in the precision mode of the kernel, with
@@ -322,13 +240,8 @@ __device__ __forceinline__ double run_pip_lock(const C& coef, const double (&x)[
     } else if constexpr (MODE == HM_GRAD_FP64) {
         return T::pip_lock(coef, x, g);
     } else {
-        float xf[T::NVARS], gf[T::NVARS];
-#pragma unroll
-        for (int v = 0; v < T::NVARS; ++v) { xf[v] = (float)x[v]; gf[v] = 0.0f; }
-        const double ep = T::pip_mixed_lock(coef, xf, x, g, gf);
-#pragma unroll
-        for (int v = 0; v < T::NVARS; ++v) g[v] += (double)gf[v];
-        return ep;
+        static_assert(MODE == HM_GRAD_FP64, "unknown mode");
+        return 0.0;
     }
 }
 
@@ -342,7 +255,7 @@ __device__ __forceinline__ double run_pip_lock(const C& coef, const double (&x)[
 // A.counter (or strides statically without it).
 template <class T, class CC, int MODE, bool CUSTOM>
 __global__ void __launch_bounds__(T::LOCK_THREADS, 1) holder_lock_kernel(const HolderArgs A) {
-    constexpr bool grads = (MODE == HM_GRAD_FP64 || MODE == HM_GRAD_MIXED);
+    constexpr bool grads = (MODE == HM_GRAD_FP64);
     __shared__ long s_base;
     double acc[7] = {0, 0, 0, 0, 0, 0, 0};
     const long n = nmer_count(A);
@@ -381,6 +294,85 @@ __global__ void __launch_bounds__(T::LOCK_THREADS, 1) holder_lock_kernel(const H
         if constexpr (CUSTOM) ep = run_pip_lock<T, MODE>(GlobalCoef{A.coef}, x, g);
         else ep = run_pip_lock<T, MODE>(CC{}, x, g);
         if (live) finish_nmer<T>(A, t, ep, g, grads, acc);
+    }
+    block_reduce_add<7>(acc, A.out);
+}
+
+// Variables of n-mer t shifted to the type's FP32 basis, dx = x - x0 rounded
+// to FP32 (x itself is built in FP64).  Returns false, with x = 0, for t >= n
+// or an n-mer beyond the evaluator's cutoff.
+template <class T>
+__device__ __forceinline__ bool nmer_vars_f32(const HolderArgs& A, long t, long n, float (&xf)[T::NVARS]) {
+    double x[T::NVARS];
+#pragma unroll
+    for (int v = 0; v < T::NVARS; ++v) x[v] = 0.0;
+    bool live = t < n;
+    if (live) {
+        double r[T::NREAL][3];
+        load_nmer<T, false>(A, t, r);
+        double d[3][3], rr[3];
+        if (pair_dists<T>(r, d, rr)) {
+            if (A.e_per) A.e_per[t] = 0.0;
+            live = false;
+        } else {
+            double s[T::NSITES][3];
+            T::sites(r, s);
+            T::vars(s, x);
+        }
+    }
+    T::shift(x, xf);
+    return live;
+}
+
+// Mixed-precision evaluation: two n-mers per thread, one in each half of the
+// paired FP32 registers, through the type's FP32-basis trie (T::SHIFTED) in
+// lockstep blocks.  Variables, switch, chain rule, virial and all sums stay
+// FP64.  A block claims chunks of 2 x blockDim.x n-mers.
+template <class T, class CC>
+__global__ void __launch_bounds__(T::LOCK_THREADS_S, 1) holder_pair_kernel(const HolderArgs A) {
+    __shared__ long s_base;
+    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    const long n = nmer_count(A);
+    const long chunk = 2L * blockDim.x;
+    long static_next = blockIdx.x * chunk;
+    const CC coef{};
+    for (;;) {
+        long base;
+        if (A.counter) {
+            if (threadIdx.x == 0) s_base = atomicAdd(A.counter, (int)chunk);
+            __syncthreads();
+            base = s_base;
+            __syncthreads();
+        } else {
+            base = static_next;
+            static_next += (long)gridDim.x * chunk;
+        }
+        if (base >= n) break;
+        const long t0 = base + threadIdx.x, t1 = t0 + blockDim.x;
+        f2_t x2[T::NVARS], g2[T::NVARS];
+        bool live0, live1;
+        {
+            float lo[T::NVARS], hi[T::NVARS];
+            live0 = nmer_vars_f32<T>(A, t0, n, lo);
+            live1 = nmer_vars_f32<T>(A, t1, n, hi);
+#pragma unroll
+            for (int v = 0; v < T::NVARS; ++v) {
+                x2[v] = f2_pack(lo[v], hi[v]);
+                g2[v] = 0ull;
+            }
+        }
+        const double2 ep = T::pip_s32_lock(coef, x2, g2);
+        double g[T::NVARS];
+        if (live0) {
+#pragma unroll
+            for (int v = 0; v < T::NVARS; ++v) g[v] = (double)f2_lo(g2[v]);
+            finish_nmer<T>(A, t0, coef.b0() + ep.x, g, true, acc);
+        }
+        if (live1) {
+#pragma unroll
+            for (int v = 0; v < T::NVARS; ++v) g[v] = (double)f2_hi(g2[v]);
+            finish_nmer<T>(A, t1, coef.b0() + ep.y, g, true, acc);
+        }
     }
     block_reduce_add<7>(acc, A.out);
 }

@@ -35,11 +35,13 @@ struct EvaluatorInfo {
     int skip;
     int ncoef, nreal, nvars;
     const double* fit;
-    launch_fn g, e, m;
+    launch_fn g, e;
     dcoef_fn c;
     poly_fn p;
     warp_fn w;
-    setcoef_fn set[6];
+    launch_fn s;      // FP32 kernel of the mixed mode (FP32 basis), or null
+    double split_r;   // mixed mode: n-mers with first-atom distance below this run in FP64 (0: none)
+    setcoef_fn set[7];
 };
 
 #include "gen/registry.inc"
@@ -122,6 +124,7 @@ struct mbx_ctx {
     // per-term dispatch
     int nbucket[4] = {0, 0, 0, 0};
     const EvaluatorInfo* bucket_eval[4][MBX_MAX_BUCKETS];
+    bool bucket_near[4][MBX_MAX_BUCKETS];   // the FP64 short-range share of a split evaluator
     DimerRules drules{};
     TrimerRules trules{};
     long bucket_cap[4][MBX_MAX_BUCKETS];
@@ -197,7 +200,7 @@ int mbx_create(mbx_ctx** out, int device, void* stream) {
     // fitted coefficients into every kernel variant (constant memory, per device)
     for (int i = 0; i < mbx_num_evaluators; ++i) {
         const EvaluatorInfo& E = mbx_evaluators[i];
-        for (int v = 0; v < 6; ++v)
+        for (int v = 0; v < 7; ++v)
             if (E.set[v]) RCHK(c, E.set[v](E.fit, 0, c->stream));
     }
     // the table-driven evaluator reads its terms and coefficients from global memory
@@ -257,6 +260,7 @@ int mbx_evaluator_info(const char* name, int* nbody, int* nreal, int* nvars, int
 static int build_rules(mbx_ctx* c) {
     for (int nb = 2; nb <= 3; ++nb) {
         c->nbucket[nb] = 0;
+        for (int b = 0; b < MBX_MAX_BUCKETS; ++b) c->bucket_near[nb][b] = false;
         const int T = c->ntypes;
         const int ncode = nb == 2 ? T * T : T * T * T;
         for (int code = 0; code < (nb == 2 ? MBX_MAX_TYPES * MBX_MAX_TYPES : MBX_MAX_TYPES * MBX_MAX_TYPES * MBX_MAX_TYPES);
@@ -331,6 +335,26 @@ static int build_rules(mbx_ctx* c) {
             else {
                 c->trules.pre2[b] = pre * pre;
                 c->trules.skip[b] = E->skip;
+            }
+        }
+        if (nb == 2) {
+            // mixed mode: a second bucket per split evaluator takes the dimers
+            // closer than split_r (evaluated in FP64); unused otherwise
+            const int nmain = c->nbucket[2];
+            for (int b = 0; b < MBX_MAX_BUCKETS; ++b) {
+                c->drules.near[b] = -1;
+                c->drules.split2[b] = 0.0;
+            }
+            for (int b = 0; b < nmain; ++b) {
+                const EvaluatorInfo* E = c->bucket_eval[2][b];
+                if (!(E->split_r > 0) || !E->s) continue;
+                if (c->nbucket[2] == MBX_MAX_BUCKETS) return fail(c, MBX_ENOTSUP, "too many evaluator buckets");
+                const int nbk = c->nbucket[2]++;
+                c->bucket_eval[2][nbk] = E;
+                c->bucket_near[2][nbk] = true;
+                c->drules.pre2[nbk] = c->drules.pre2[b];
+                c->drules.near[b] = nbk;
+                c->drules.split2[b] = E->split_r * E->split_r;
             }
         }
     }
@@ -496,7 +520,8 @@ static CellGrid make_grid(const mbx_ctx* c, double rc, int nmem) {
 
 // Enumerates the n-mers of one term into the evaluator buckets (and, when
 // list_cap > 0, into c->list).  Asynchronous; status and counts on device.
-static int launch_build(mbx_ctx* c, int nbody, int use_ghost, const double* xyz, long list_cap, int* kernels) {
+static int launch_build(mbx_ctx* c, int nbody, int use_ghost, const double* xyz, long list_cap, int* kernels,
+                        bool mixed = false) {
     const int g = use_ghost ? 1 : 0;
     const int nmem = c->nmem[g], nq = c->nquery[g];
     const double rc = c->cutoff[nbody];
@@ -556,8 +581,11 @@ static int launch_build(mbx_ctx* c, int nbody, int use_ghost, const double* xyz,
                                                       c->nb_count.p, c->nb.p, c->status.p);
     }
     if (nbody == 2) {
+        DimerRules R = c->drules;
+        if (!mixed)
+            for (int b = 0; b < MBX_MAX_BUCKETS; ++b) R.split2[b] = 0.0;   // no short-range split
         k_dimers<<<(nq * 32 + T - 1) / T, T, 0, c->stream>>>(c->d_query[g].p, nq, c->d_members[g].p, c->d_tag.p,
-                                                        c->d_type.p, c->nb_count.p, c->nb.p, c->nb_cap, rc2, c->drules,
+                                                        c->d_type.p, c->nb_count.p, c->nb.p, c->nb_cap, rc2, R,
                                                         c->listed.p, list_cap > 0 ? c->list.p : nullptr, list_cap,
                                                         c->buckets.p, c->bucket_count.p, c->status.p);
     } else {
@@ -582,7 +610,8 @@ static HolderArgs base_args(mbx_ctx* c) {
     return A;
 }
 
-static int launch_eval(mbx_ctx* c, const EvaluatorInfo* E, HolderArgs A, int flags, int* kernels) {
+static int launch_eval(mbx_ctx* c, const EvaluatorInfo* E, HolderArgs A, int flags, int* kernels,
+                       bool near = false) {
     const bool grads = !(flags & MBX_NO_GRADS);
     const bool mixed = (flags & MBX_MIXED) != 0;
     const int block = 128;
@@ -597,7 +626,11 @@ static int launch_eval(mbx_ctx* c, const EvaluatorInfo* E, HolderArgs A, int fla
         ++*kernels;
         return MBX_OK;
     }
-    launch_fn fn = !grads ? E->e : (mixed ? E->m : E->g);
+    // mixed mode: the FP32-basis kernel where the type has one; FP64 for the
+    // short-range bucket of a split type, for a split type's AoS input (no
+    // builder to separate the short-range n-mers) and for types without one
+    const bool fp32 = mixed && !near && E->s && !(A.aos && E->split_r > 0);
+    launch_fn fn = !grads ? E->e : fp32 ? E->s : E->g;
     if (!fn) return fail(c, MBX_ENOTSUP, std::string("no kernel for ") + E->name);
     // persistent grid: a few resident blocks per SM, grid-stride over n-mers
     const long want = (A.n + block - 1) / block;
@@ -630,7 +663,8 @@ extern "C" int mbx_energy(mbx_ctx* c, int nbody, double* xyz, int use_ghost, dou
             k_fix_monomers<<<(c->nmon + 127) / 128, 128, 0, c->stream>>>(X, c->d_first.p, c->d_nat.p, c->nmon, c->bp);
             ++kernels;
         }
-        int r = launch_build(c, nbody, use_ghost, X, 0, &kernels);
+        const bool mixed = (flags & MBX_MIXED) && grads;
+        int r = launch_build(c, nbody, use_ghost, X, 0, &kernels, mixed);
         if (r) return r;
         CUCHK(c, cudaEventRecord(c->ev[1], c->stream));
         double* G = nullptr;
@@ -658,7 +692,8 @@ extern "C" int mbx_energy(mbx_ctx* c, int nbody, double* xyz, int use_ghost, dou
             A.grad = G;
             A.out = c->out.p;
             off += c->bucket_cap[nbody][b];
-            r = launch_eval(c, c->bucket_eval[nbody][b], A, flags, &kernels);
+            if (c->bucket_near[nbody][b] && !mixed) continue;   // empty without the split
+            r = launch_eval(c, c->bucket_eval[nbody][b], A, flags, &kernels, c->bucket_near[nbody][b]);
             if (r) return r;
         }
         CUCHK(c, cudaEventRecord(c->ev[2], c->stream));
@@ -954,7 +989,7 @@ extern "C" int mbx_set_coefficients(mbx_ctx* c, const char* name, const double* 
     CUCHK(c, cudaSetDevice(c->device));
     const bool dev = a && (flags & MBX_DEVICE_PTRS);
     const double* src = a ? a : E->fit;
-    for (int v = 0; v < 6; ++v)
+    for (int v = 0; v < 7; ++v)
         if (E->set[v]) RCHK(c, E->set[v](src, dev ? 1 : 0, c->stream));
     if (E->w)
         CUCHK(c, cudaMemcpyAsync(c->warp_coef.p, src, E->ncoef * sizeof(double),

@@ -370,6 +370,7 @@ __global__ void k_dimers(const int* __restrict__ query, int nquery, const int* _
             code = type[mi] * MBX_MAX_TYPES + type[mj];
             b = R.bucket[code];
             if (b >= 0 && d2 > R.pre2[b]) b = -1;   // cannot pass the evaluator's own cutoff
+            if (b >= 0 && d2 < R.split2[b]) b = R.near[b];   // mixed mode: short-range share
         }
         const bool ins = b >= 0;
         const int pos = warp_reserve(bucket_count, ins ? b : 0, ins);

@@ -32,6 +32,8 @@ struct DimerRules {
     double pre2[MBX_MAX_BUCKETS];               // (evaluator cutoff + margin)^2
     int cap[MBX_MAX_BUCKETS];
     long offset[MBX_MAX_BUCKETS];
+    int near[MBX_MAX_BUCKETS];                  // bucket for dimers with d^2 < split2 (-1: none)
+    double split2[MBX_MAX_BUCKETS];             // 0: no split
 };
 
 struct TrimerRules {

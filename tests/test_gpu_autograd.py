@@ -76,9 +76,19 @@ def test_coefficient_gradient_refit_loss(name, maker):
 
 
 def test_mixed_refit_forward():
+    """Mixed forward of the refitting workload (gas-phase trimers, off the FP32
+    basis' liquid reference point: 1e-5 of the summed energy), and the
+    coefficient gradient through it (the shifted coefficients follow a)."""
     from mbx_b200 import torch_ops
     xyz_np = workloads.gas_trimers(500, seed=1)
     coef = torch_ops.fitted_coefficients("mbpol3b")
     e64 = torch_ops.nmer_energies("mbpol3b", torch.tensor(xyz_np, device="cuda"), coef)
     e32 = torch_ops.nmer_energies("mbpol3b", torch.tensor(xyz_np, device="cuda"), coef, mixed=True)
-    assert abs(float(e32.sum() - e64.sum())) / abs(float(e64.sum())) < 1e-6
+    assert abs(float(e32.sum() - e64.sum())) / float(e64.abs().sum()) < 1e-5
+    # custom coefficients reach the FP32 basis (b = F a recomputed)
+    c2 = (coef * 1.01).detach()
+    e64b = torch_ops.nmer_energies("mbpol3b", torch.tensor(xyz_np, device="cuda"), c2)
+    e32b = torch_ops.nmer_energies("mbpol3b", torch.tensor(xyz_np, device="cuda"), c2, mixed=True)
+    assert abs(float(e32b.sum() - e64b.sum())) / float(e64b.abs().sum()) < 1e-5
+    assert abs(float(e64b.sum()) - 1.01 * float(e64.sum())) < 1e-9 * float(e64.abs().sum())
+    torch_ops.context().set_coefficients("mbpol3b", None)
