@@ -337,8 +337,8 @@ def main():
     if not args.no_mixed:
         g3_64, g3_mx = g64 - g2_64, gmx - g2_mx
         out["mixed"] = {"value": world * units / (ms_mx * 1e-3), "ms_per_step": ms_mx,
-                        "dtype": "f32 trie (3b: shifted basis; 2b: O-O >= 4.5 A) / f64 variables, "
-                                 "switch, chain rule, sums",
+                        "dtype": "3b: paired f32 trie over a shifted basis, f64 variables, switch, chain rule "
+                                 "and sums; 2b: f64",
                         "error_vs": "FP64 path of the same run (within 1e-10 of the reference)",
                         "rel_err_E2B": abs(e2_mx - e2_64) / abs(e2_64), "rel_err_E3B": abs(e3_mx - e3_64) / abs(e3_64),
                         "rel_err_E": abs((e2_mx + e3_mx) - (e2_64 + e3_64)) / abs(e2_64 + e3_64),

@@ -182,10 +182,18 @@ def parts_for(nterms, nvars=36):
     function of 10^4-10^5 FMAs leaves the register allocator live ranges it
     cannot fit (kilobytes of spills), and the code of a piece should stay
     small enough for the instruction cache that the warps of a lockstep block
-    share: ~400 terms per piece in 384-thread blocks, ~700 in 256-thread
-    blocks (measured on the MB-pol 2b/3b tries)."""
-    per = 400 if lock_threads(nvars) == 384 else 700
+    share: ~400 terms per piece in 384-thread blocks, ~450 in 256-thread
+    blocks (measured on the MB-pol 2b/3b tries: 350-450 terms is the
+    plateau)."""
+    per = 400 if lock_threads(nvars) == 384 else 450
     return max(1, (nterms + per - 1) // per)
+
+
+# FP64 kernels whose coefficients are copied to shared memory per block (the
+# trie reads them from there instead of the constant bank): measured on the
+# 2048-water trimers, MB-pol 3b 1.37 ms (shared, 450-term pieces) vs 1.58 ms
+# (constant); MB-pol 2b is faster from the constant bank (0.18 vs 0.25 ms).
+SMEM_COEF_TYPES = {"mbpol3b"}
 
 
 def emit_split(trie, nvars, name, out, nparts, arrays, body, ret="double"):
@@ -226,6 +234,17 @@ def emit_split(trie, nvars, name, out, nparts, arrays, body, ret="double"):
         w("    return E;")
         w("}")
     sig = ", ".join("%s%s (&%s)[%d]" % ("const " if role == "in" else "", ct, a, nvars) for a, ct, role in arrays)
+    # name_piece(k, ...): piece k alone (the code warm-up launch runs each
+    # piece once so that its instructions are in L2 before the evaluation)
+    w("#define %s_NPIECES %d" % (name.upper(), len(pieces)))
+    w("template <class Coef>")
+    w("__device__ __forceinline__ %s %s_piece(int k, const Coef& coef, %s) {" % (ret, name, sig))
+    w("    switch (k) {")
+    for i in range(len(pieces)):
+        w("    case %d: return %s_part%d(coef, %s);" % (i, name, i, ", ".join(a for a, _, _ in arrays)))
+    w("    default: return %s;" % ("make_double2(0.0, 0.0)" if ret == "double2" else "0.0"))
+    w("    }")
+    w("}")
     for lock in (False, True):
         # name(): the pieces in turn; name_lock(): the same with a block
         # barrier after every piece, so that all warps of a block run the same
@@ -461,6 +480,16 @@ def emit_traits(spec, table, straight, out):
     shifted_type = straight and n in SHIFT_TYPES
     w("    static constexpr int SHIFTED = %d, LOCK_THREADS_S = %d;  // paired FP32 (shifted-basis) kernel" %
       (1 if shifted_type else 0, 256 if shifted_type else lock_threads(spec.nvars)))
+    w("    static constexpr int NORB = %d;  // coefficients of the FP32 basis" %
+      (shifted_pip(n).norb if shifted_type else 1))
+    w("    static constexpr int SMEM_COEF = %d;  // FP64 kernel reads its coefficients from shared memory" %
+      (1 if n in SMEM_COEF_TYPES else 0))
+    if straight:
+        w("    template <class C> __device__ __forceinline__ static double pip_piece(int k, const C& c, "
+          "const double (&x)[%d], double (&g)[%d]) { return %s_pip_piece(k, c, x, g); }" % (spec.nvars, spec.nvars, n))
+    if shifted_type:
+        w("    template <class C> __device__ __forceinline__ static double2 pip_s32_piece(int k, const C& c, "
+          "const f2_t (&x)[%d], f2_t (&g)[%d]) { return %s_pip_s32_piece(k, c, x, g); }" % (spec.nvars, spec.nvars, n))
     if shifted_type:
         w("    __device__ __forceinline__ static void shift(const double (&x)[%d], float (&xf)[%d]) "
           "{ %s_shift(x, xf); }" % (spec.nvars, spec.nvars, n))
@@ -510,6 +539,8 @@ def generate(name):
     emit_vars(spec, out)
     nv = spec.nvars
     if straight:
+        out.append("template <class Coef> __device__ __forceinline__ double %s_pip_piece(int, const Coef&, "
+                   "const double (&)[%d], double (&)[%d]);" % (name, nv, nv))
         for lk in ("", "_lock"):
             out += ["template <class Coef> __device__ __forceinline__ double %s_pip%s(const Coef&, const double (&)[%d], "
                     "double (&)[%d]);" % (name, lk, nv, nv),
@@ -519,6 +550,8 @@ def generate(name):
                 (name, nv)]
         if name in SHIFT_TYPES:
             sp = shifted_pip(name)
+            out.append("template <class Coef> __device__ __forceinline__ double2 %s_pip_s32_piece(int, const Coef&, "
+                       "const f2_t (&)[%d], f2_t (&)[%d]);" % (name, nv, nv))
             for lk in ("", "_lock"):
                 out.append("template <class Coef> __device__ __forceinline__ double2 %s_pip_s32%s(const Coef&, "
                            "const f2_t (&)[%d], f2_t (&)[%d]);" % (name, lk, nv, nv))
@@ -551,7 +584,10 @@ def generate(name):
             body = head + ["#pragma once", '#include "%s.cuh"' % name,
                            "// %d monomials of the %s basis, %d coefficient orbits" %
                            (len(sp.monos), SHIFT_TYPES[name], sp.norb)]
-            emit_pip_f32x2(strie, nv, "%s_pip_s32" % name, body, max(1, (len(sp.monos) + 699) // 700))
+            # ~330 terms per piece: larger pieces spill in the paired form
+            # (measured: 300-350 terms 0.79-0.81 ms, 450 terms 1.29 ms for the
+            # 2048-water trimers)
+            emit_pip_f32x2(strie, nv, "%s_pip_s32" % name, body, max(1, (len(sp.monos) + 329) // 330))
             write_if_changed(os.path.join(OUT, "%s_pip_s32.cuh" % name), "\n".join(body) + "\n")
     return os.path.join(OUT, name + ".cuh"), leaves, inner
 
@@ -612,6 +648,12 @@ int mbx_launch_%(name)s_g(const HolderArgs& A, int grid, int block, cudaStream_t
     grid = (int)(need < (long)sms * bps ? need : (long)sms * bps);
     if (grid < 1) grid = 1;
     kern<<<grid, block, 0, s>>>(A);
+    return (int)cudaGetLastError();
+}
+
+int mbx_warm_%(name)s_g(double* sink, cudaStream_t s) {
+    // one warp per trie piece: brings the evaluation kernel's code into L2
+    holder_warm_kernel<%(name)s_T, %(name)s_CC, HM_GRAD_FP64><<<%(NAME)s_PIP_NPIECES, 32, 0, s>>>(sink);
     return (int)cudaGetLastError();
 }
 """),
@@ -718,6 +760,12 @@ int mbx_set_coef_%(name)s_s(const double* a, int from_device, cudaStream_t s) {
     return (int)e;
 }
 
+int mbx_warm_%(name)s_s(double* sink, cudaStream_t s) {
+    // one warp per trie piece: brings the evaluation kernel's code into L2
+    holder_warm_kernel<%(name)s_T, %(name)s_CS, HM_GRAD_SHIFT32><<<%(NAME)s_PIP_S32_NPIECES, 32, 0, s>>>(sink);
+    return (int)cudaGetLastError();
+}
+
 int mbx_launch_%(name)s_s(const HolderArgs& A, int grid, int block, cudaStream_t s) {
     // persistent grid of lockstep blocks (two n-mers per thread): every
     // resident block slot once
@@ -749,7 +797,7 @@ def write_shift_tu(name, path):
             fs.append(f)
         rows.append(len(ks))
     k0 = sorted(sp.const_F)
-    d = {"name": name, "basis": SHIFT_TYPES[name], "norb": sp.norb, "norb1": sp.norb + 1,
+    d = {"name": name, "NAME": name.upper(), "basis": SHIFT_TYPES[name], "norb": sp.norb, "norb1": sp.norb + 1,
          "ncoef": SPECS[name].ncoef, "nnz": len(ks), "nnz0": max(1, len(k0)),
          "rows": ",".join(map(str, rows)), "ks": ",".join(map(str, ks)),
          "fs": ",".join(repr(float(f)) for f in fs),
@@ -776,7 +824,7 @@ def write_kernels_cu(name):
             paths.append(path)
             continue
         what, body = VARIANTS[v]
-        d = {"name": name, "ncoef": spec.ncoef, "v": v, "what": what,
+        d = {"name": name, "NAME": name.upper(), "ncoef": spec.ncoef, "v": v, "what": what,
              "include": ('#include "%s_%s.cuh"\n' % (name, inc[v])) if inc[v] else ""}
         path = os.path.join(OUT, "%s_%s.cu" % (name, v))
         write_tu(path, (TU_HEAD + body) % d)
@@ -797,6 +845,8 @@ def write_registry():
             if v in "ges":
                 lines.append("int mbx_launch_%s_%s(const HolderArgs& A, int grid, int block, cudaStream_t s);" %
                              (name, v))
+            if v in "gs":
+                lines.append("int mbx_warm_%s_%s(double* sink, cudaStream_t s);" % (name, v))
             elif v == "c":
                 lines.append("int mbx_launch_%s_c(const HolderArgs& A, const double* w, double* out, int grid, "
                              "int block, cudaStream_t s);" % name)
@@ -825,6 +875,7 @@ def write_registry():
                       spec.nvars, name, fn("g", "launch"), fn("e", "launch"), fn("c", "launch"),
                       fn("p", "launch"), fn("w", "launch"), fn("s", "launch"),
                       lit(MIXED_FP64_RADIUS.get(name, 0.0))))
+        lines.append("     %s, %s," % (fn("g", "warm"), fn("s", "warm")))
         lines.append("     {%s, nullptr}}," % ", ".join(fn(v, "set_coef") for v in "gecpws"))
     lines.append("};")
     lines.append("static const int mbx_num_evaluators = %d;" % len(SPECS))

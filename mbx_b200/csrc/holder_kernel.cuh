@@ -20,7 +20,9 @@
 #include "holder_common.cuh"
 
 // Precision / output modes.
-enum { HM_ENERGY = 0, HM_GRAD_FP64 = 1 };
+// HM_GRAD_SHIFT32 names the paired FP32 kernel (holder_pair_kernel) where a
+// template needs to tell the two gradient kernels apart.
+enum { HM_ENERGY = 0, HM_GRAD_FP64 = 1, HM_GRAD_SHIFT32 = 4 };
 
 struct HolderArgs {
     long n;                    // number of n-mers (capacity when n_dev is set)
@@ -245,6 +247,14 @@ __device__ __forceinline__ double run_pip_lock(const C& coef, const double (&x)[
     }
 }
 
+// FP64 coefficients copied from constant to shared memory once per block
+// (types with T::SMEM_COEF).
+template <class CC>
+struct SharedCoef {
+    const double* p;
+    __device__ __forceinline__ double operator[](int k) const { return p[k]; }
+};
+
 // One n-mer per thread, all warps of a block in lockstep through the trie:
 // the straight-line polynomial is ~10^5 instructions, far more than the
 // instruction cache holds, so the block's warps go through it piece by piece
@@ -257,6 +267,11 @@ template <class T, class CC, int MODE, bool CUSTOM>
 __global__ void __launch_bounds__(T::LOCK_THREADS, 1) holder_lock_kernel(const HolderArgs A) {
     constexpr bool grads = (MODE == HM_GRAD_FP64);
     __shared__ long s_base;
+    __shared__ double s_coef[T::SMEM_COEF ? T::NCOEF : 1];
+    if constexpr (T::SMEM_COEF && !CUSTOM) {
+        for (int k = threadIdx.x; k < T::NCOEF; k += blockDim.x) s_coef[k] = CC{}[k];
+        __syncthreads();
+    }
     double acc[7] = {0, 0, 0, 0, 0, 0, 0};
     const long n = nmer_count(A);
     long static_next = blockIdx.x * (long)blockDim.x;
@@ -292,6 +307,7 @@ __global__ void __launch_bounds__(T::LOCK_THREADS, 1) holder_lock_kernel(const H
         }
         double ep;
         if constexpr (CUSTOM) ep = run_pip_lock<T, MODE>(GlobalCoef{A.coef}, x, g);
+        else if constexpr (T::SMEM_COEF) ep = run_pip_lock<T, MODE>(SharedCoef<CC>{s_coef}, x, g);
         else ep = run_pip_lock<T, MODE>(CC{}, x, g);
         if (live) finish_nmer<T>(A, t, ep, g, grads, acc);
     }
@@ -328,14 +344,27 @@ __device__ __forceinline__ bool nmer_vars_f32(const HolderArgs& A, long t, long 
 // paired FP32 registers, through the type's FP32-basis trie (T::SHIFTED) in
 // lockstep blocks.  Variables, switch, chain rule, virial and all sums stay
 // FP64.  A block claims chunks of 2 x blockDim.x n-mers.
+// Coefficient pairs of the FP32 basis copied from constant to shared memory
+// once per block (a shared-memory operand costs fewer instructions per leaf
+// than a constant-bank one in the paired form).
+template <class CC>
+struct SharedPairs {
+    const f2_t* p;
+    __device__ __forceinline__ f2_t f2(int k) const { return p[k]; }
+    __device__ __forceinline__ double b0() const { return CC{}.b0(); }
+};
+
 template <class T, class CC>
 __global__ void __launch_bounds__(T::LOCK_THREADS_S, 1) holder_pair_kernel(const HolderArgs A) {
     __shared__ long s_base;
+    __shared__ f2_t s_coef[T::NORB];
+    for (int k = threadIdx.x; k < T::NORB; k += blockDim.x) s_coef[k] = CC{}.f2(k);
+    __syncthreads();
     double acc[7] = {0, 0, 0, 0, 0, 0, 0};
     const long n = nmer_count(A);
     const long chunk = 2L * blockDim.x;
     long static_next = blockIdx.x * chunk;
-    const CC coef{};
+    const SharedPairs<CC> coef{s_coef};
     for (;;) {
         long base;
         if (A.counter) {
@@ -375,6 +404,40 @@ __global__ void __launch_bounds__(T::LOCK_THREADS_S, 1) holder_pair_kernel(const
         }
     }
     block_reduce_add<7>(acc, A.out);
+}
+
+// Code warm-up: block k (one warp) runs piece k of the trie once on zero
+// variables, with the same coefficient view as the evaluation kernel, so that
+// the piece's instructions are in L2 when the evaluation reaches it.  Launched
+// beside the n-mer builder.  The result never meets the sink's condition; the
+// store keeps the calls from being removed.
+template <class T, class CC, int MODE>
+__global__ void __launch_bounds__(32) holder_warm_kernel(double* sink) {
+    const int k = blockIdx.x;
+    double e;
+    if constexpr (MODE == HM_GRAD_SHIFT32) {
+        __shared__ f2_t s_pairs[T::NORB];
+        for (int j = threadIdx.x; j < T::NORB; j += blockDim.x) s_pairs[j] = CC{}.f2(j);
+        __syncwarp();
+        f2_t x[T::NVARS], g[T::NVARS];
+#pragma unroll
+        for (int v = 0; v < T::NVARS; ++v) { x[v] = 0ull; g[v] = 0ull; }
+        const double2 r = T::pip_s32_piece(k, SharedPairs<CC>{s_pairs}, x, g);
+        e = r.x + r.y + (double)f2_lo(g[0]);
+    } else {
+        double x[T::NVARS], g[T::NVARS];
+#pragma unroll
+        for (int v = 0; v < T::NVARS; ++v) { x[v] = 0.0; g[v] = 0.0; }
+        if constexpr (T::SMEM_COEF) {
+            __shared__ double s_c[T::NCOEF];
+            for (int j = threadIdx.x; j < T::NCOEF; j += blockDim.x) s_c[j] = CC{}[j];
+            __syncwarp();
+            e = T::pip_piece(k, SharedCoef<CC>{s_c}, x, g) + g[0];
+        } else {
+            e = T::pip_piece(k, CC{}, x, g) + g[0];
+        }
+    }
+    if (e == 1.0e300 && threadIdx.x == 0) sink[0] = e;
 }
 
 // Warp-cooperative evaluation for polynomials too large for straight-line

@@ -22,6 +22,7 @@
 #include "nmer_build.h"
 
 typedef int (*launch_fn)(const HolderArgs&, int, int, cudaStream_t);
+typedef int (*warm_fn)(double* sink, cudaStream_t s);
 typedef int (*dcoef_fn)(const HolderArgs&, const double*, double*, int, int, cudaStream_t);
 typedef int (*poly_fn)(long, const double*, double*, double*, int, int, cudaStream_t);
 typedef int (*warp_fn)(const HolderArgs&, int, int, cudaStream_t);
@@ -41,6 +42,7 @@ struct EvaluatorInfo {
     warp_fn w;
     launch_fn s;      // FP32 kernel of the mixed mode (FP32 basis), or null
     double split_r;   // mixed mode: n-mers with first-atom distance below this run in FP64 (0: none)
+    warm_fn warm_g, warm_s;   // code warm-up launches of the g and s kernels
     setcoef_fn set[7];
 };
 
@@ -140,6 +142,10 @@ struct mbx_ctx {
     int nb_cap = 192;
     double* h_out = nullptr;  // pinned: [0..7] term outputs, [8..15] counters
     cudaEvent_t ev[3];
+    // code warm-up of the evaluation kernels, beside the n-mer build
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    DevBuf<double> warm_sink;
 
     // results of the last call
     long last_listed[4] = {0, 0, 0, 0};
@@ -191,6 +197,10 @@ int mbx_create(mbx_ctx** out, int device, void* stream) {
     }
     CUCHK(c, cudaMallocHost(&c->h_out, 64 * sizeof(double)));
     for (int i = 0; i < 3; ++i) CUCHK(c, cudaEventCreate(&c->ev[i]));
+    CUCHK(c, cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
+    CUCHK(c, cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
+    CUCHK(c, cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
+    CUCHK(c, c->warm_sink.ensure(1));
     CUCHK(c, c->out.ensure(64));
     CUCHK(c, c->status.ensure(4));
     CUCHK(c, c->counters.ensure(MBX_MAX_BUCKETS));
@@ -239,6 +249,9 @@ int mbx_destroy(mbx_ctx* c) {
     c->terms.release();
     if (c->h_out) cudaFreeHost(c->h_out);
     for (int i = 0; i < 3; ++i) cudaEventDestroy(c->ev[i]);
+    if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+    if (c->ev_join) cudaEventDestroy(c->ev_join);
+    if (c->side) cudaStreamDestroy(c->side);
     if (c->own_stream) cudaStreamDestroy(c->stream);
     delete c;
     return MBX_OK;
@@ -589,11 +602,12 @@ static int launch_build(mbx_ctx* c, int nbody, int use_ghost, const double* xyz,
                                                         c->listed.p, list_cap > 0 ? c->list.p : nullptr, list_cap,
                                                         c->buckets.p, c->bucket_count.p, c->status.p);
     } else {
-        const int WPB = 2;
-        const size_t smem = (size_t)WPB * c->nb_cap * sizeof(NbEntry);
+        // one block of 4 warps per query; its matches staged in shared memory
+        const size_t smem = (size_t)c->nb_cap * MBX_TRIMATCH_BYTES;
+        if (smem > 227 * 1024) return fail(c, MBX_ENOMEM, "trimer staging exceeds shared memory");
         if (smem > 48 * 1024)
             CUCHK(c, cudaFuncSetAttribute(k_trimers, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_trimers<<<(nq + WPB - 1) / WPB, WPB * 32, smem, c->stream>>>(
+        k_trimers<<<nq, 128, smem, c->stream>>>(
             c->d_query[g].p, nq, c->d_members[g].p, c->d_tag.p, c->d_type.p, c->cloud.p, c->nb_count.p, c->nb.p,
             c->nb_cap, rc2, c->trules, c->listed.p, list_cap > 0 ? c->list.p : nullptr, list_cap, c->buckets.p,
             c->bucket_count.p, c->status.p);
@@ -664,8 +678,32 @@ extern "C" int mbx_energy(mbx_ctx* c, int nbody, double* xyz, int use_ghost, dou
             ++kernels;
         }
         const bool mixed = (flags & MBX_MIXED) && grads;
+        // warm the evaluation kernels' code into L2 on the side stream while
+        // the n-mers are built (one warp per trie piece)
+        bool warmed = false;
+        if (grads) {
+            CUCHK(c, cudaEventRecord(c->ev_fork, c->stream));
+            CUCHK(c, cudaStreamWaitEvent(c->side, c->ev_fork, 0));
+            warm_fn done[2 * MBX_MAX_BUCKETS];
+            int ndone = 0;
+            for (int b = 0; b < c->nbucket[nbody]; ++b) {
+                const EvaluatorInfo* E = c->bucket_eval[nbody][b];
+                if (c->bucket_near[nbody][b] && !mixed) continue;
+                const bool fp32 = mixed && !c->bucket_near[nbody][b] && E->s;
+                warm_fn fn = fp32 ? E->warm_s : E->warm_g;
+                bool seen = false;
+                for (int i = 0; i < ndone; ++i) seen = seen || done[i] == fn;
+                if (!fn || seen) continue;
+                done[ndone++] = fn;
+                RCHK(c, fn(c->warm_sink.p, c->side));
+                ++kernels;
+            }
+            CUCHK(c, cudaEventRecord(c->ev_join, c->side));
+            warmed = true;
+        }
         int r = launch_build(c, nbody, use_ghost, X, 0, &kernels, mixed);
         if (r) return r;
+        if (warmed) CUCHK(c, cudaStreamWaitEvent(c->stream, c->ev_join, 0));
         CUCHK(c, cudaEventRecord(c->ev[1], c->stream));
         double* G = nullptr;
         if (grads) {

@@ -232,28 +232,45 @@ __device__ __forceinline__ void neighbors_block(const double* __restrict__ cloud
         az = (az + cg.n[2]) % cg.n[2];
         const int cell = (az * cg.n[1] + ay) * cg.n[0] + ax;
         const int b = cell_start[cell], e = cell_start[cell + 1];
-        for (int base = b * ncopy; base < e * ncopy; base += 32) {
-            const int t = base + lane;
-            bool hit = false;
-            NbEntry ent;
-            if (t < e * ncopy) {
-                const int qj = cell_items[t / ncopy];
-                const int s = t % ncopy;
-                const double* pj = cloud + (size_t)qj * 24 + 3 * s;
-                const double d2 = dist2_rn(x0, x1, x2, pj[0], pj[1], pj[2]);
-                if (d2 < rc2) {
-                    hit = true;
-                    ent.member = qj;
-                    ent.copy = s;
-                    ent.d2 = d2;
+        // the cell's items in chunks of 32 (one load per lane, then shuffled);
+        // its (item, copy) points in item-major order, lanes over consecutive
+        // points (coalesced cloud loads), two independent 32-point blocks at a time
+        for (int c0 = b; c0 < e; c0 += 32) {
+            const int nit = e - c0 < 32 ? e - c0 : 32;
+            const int my_item = lane < nit ? cell_items[c0 + lane] : 0;
+            const int total = nit * ncopy;
+            for (int base = 0; base < total; base += 64) {
+                bool hit[2];
+                NbEntry ent[2];
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int t = base + 32 * h + lane;
+                    const bool ok = t < total;
+                    const int it = ok ? t / ncopy : 0;
+                    const int qj = __shfl_sync(0xffffffffu, my_item, it);
+                    hit[h] = false;
+                    if (ok) {
+                        const int s = t - it * ncopy;
+                        const double* pj = cloud + (size_t)qj * 24 + 3 * s;
+                        const double d2 = dist2_rn(x0, x1, x2, pj[0], pj[1], pj[2]);
+                        if (d2 < rc2) {
+                            hit[h] = true;
+                            ent[h].member = qj;
+                            ent[h].copy = s;
+                            ent[h].d2 = d2;
+                        }
+                    }
+                }
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const unsigned m = __ballot_sync(0xffffffffu, hit[h]);
+                    if (hit[h]) {
+                        const int pos = count + __popc(m & ((1u << lane) - 1u));
+                        if (pos < cap) mine[pos] = ent[h];
+                    }
+                    count += __popc(m);
                 }
             }
-            const unsigned m = __ballot_sync(0xffffffffu, hit);
-            if (hit) {
-                const int pos = count + __popc(m & ((1u << lane) - 1u));
-                if (pos < cap) mine[pos] = ent;
-            }
-            count += __popc(m);
         }
     }
     if (lane == 0) wcount[w] = count;
@@ -302,6 +319,15 @@ __global__ void __launch_bounds__(32) k_neighbors1(const double* __restrict__ cl
 }
 
 namespace {
+
+// A match of a trimer query staged in shared memory: its cloud point, the
+// squared distance to the query, the member index and its monomer, tag, type.
+struct TriMatch {
+    double p[3];
+    double d2;
+    int member, m, tag, type;
+};
+static_assert(sizeof(TriMatch) == MBX_TRIMATCH_BYTES, "TriMatch layout");
 
 // One slot per lane that wants one, in counters[key]: lanes with the same key
 // share one atomicAdd.  Called by all 32 lanes of the warp.
@@ -386,41 +412,61 @@ __global__ void k_dimers(const int* __restrict__ query, int nquery, const int* _
     if (lane == 0 && mine) atomicAdd(listed, mine);
 }
 
-// Trimers: one warp per query monomer i, lanes over the pairs of its matches.
-__global__ void k_trimers(const int* __restrict__ query, int nquery, const int* __restrict__ members,
+// Trimers: a block of warps per query monomer i.  Its matches within rc are
+// staged in shared memory with everything the rules read (cloud point,
+// member, tag, type), then the block's lanes run over the pairs of matches.
+__global__ void __launch_bounds__(128) k_trimers(const int* __restrict__ query, int nquery,
+                          const int* __restrict__ members,
                           const int* __restrict__ tag, const int* __restrict__ type, const double* __restrict__ cloud,
                           const int* __restrict__ nb_count, const NbEntry* __restrict__ nb, int cap, double rc2,
                           TrimerRules R, unsigned long long* __restrict__ listed, int4* __restrict__ list,
                           long list_cap, int4* __restrict__ bucket_data, int* __restrict__ bucket_count,
                           int* __restrict__ status) {
     extern __shared__ unsigned char smem[];
+    TriMatch* sh = reinterpret_cast<TriMatch*>(smem);
+    __shared__ int s_n;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int wq = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int wq = blockIdx.x;
     if (wq >= nquery) return;
-    // compact this query's matches with d^2 < rc2 into shared memory
-    NbEntry* sh = reinterpret_cast<NbEntry*>(smem) + (size_t)w * cap;
     const int qi = query[wq];
     const int mi = members[qi];
     const int ti = tag[mi];
-    const int n0 = nb_count[wq];
-    const NbEntry* e = nb + (size_t)wq * cap;
-    int n = 0;
-    for (int base = 0; base < n0; base += 32) {
-        const int a = base + lane;
-        bool keep = false;
-        NbEntry ea;
-        if (a < n0) {
-            ea = e[a];
-            keep = ea.d2 < rc2 && ea.member != qi;
+    if (w == 0) {
+        // compact this query's matches with d^2 < rc2 (other monomers only)
+        const int n0 = nb_count[wq];
+        const NbEntry* e = nb + (size_t)wq * cap;
+        int n = 0;
+        for (int base = 0; base < n0; base += 32) {
+            const int a = base + lane;
+            bool keep = false;
+            NbEntry ea;
+            if (a < n0) {
+                ea = e[a];
+                keep = ea.d2 < rc2 && ea.member != qi;
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, keep);
+            if (keep) {
+                TriMatch t;
+                const double* p = cloud + (size_t)ea.member * 24 + 3 * ea.copy;
+                t.p[0] = p[0];
+                t.p[1] = p[1];
+                t.p[2] = p[2];
+                t.d2 = ea.d2;
+                t.member = ea.member;
+                t.m = members[ea.member];
+                t.tag = tag[t.m];
+                t.type = type[t.m];
+                sh[n + __popc(m & ((1u << lane) - 1u))] = t;
+            }
+            n += __popc(m);
         }
-        const unsigned m = __ballot_sync(0xffffffffu, keep);
-        if (keep) sh[n + __popc(m & ((1u << lane) - 1u))] = ea;
-        n += __popc(m);
+        if (lane == 0) s_n = n;
     }
-    __syncwarp();
+    __syncthreads();
+    const int n = s_n;
     const long npair = (long)n * (n - 1) / 2;
     unsigned long long mine = 0;
-    for (long base = 0; base < npair; base += 32) {
+    for (long base = 32L * w; base < npair; base += blockDim.x) {
         const long p = base + lane;
         bool keep = false;
         int mj = 0, mk = 0, bk = -1, code = 0;
@@ -431,16 +477,15 @@ __global__ void k_trimers(const int* __restrict__ query, int nquery, const int* 
             while ((long)(a + 1) * (2 * n - a - 2) / 2 <= p) ++a;
             while ((long)a * (2 * n - a - 1) / 2 > p) --a;
             const int b = (int)(p - (long)a * (2 * n - a - 1) / 2) + a + 1;
-            const NbEntry ea = sh[a], eb = sh[b];
+            const TriMatch& ea = sh[a];
+            const TriMatch& eb = sh[b];
             if (ea.member != eb.member) {
-                const double* pa = cloud + (size_t)ea.member * 24 + 3 * ea.copy;
-                const double* pb = cloud + (size_t)eb.member * 24 + 3 * eb.copy;
-                const double djk = dist2_rn(pa[0], pa[1], pa[2], pb[0], pb[1], pb[2]);
-                mj = members[ea.member];
-                mk = members[eb.member];
-                keep = djk > rc2 || (ti < tag[mj] && ti < tag[mk]);
+                const double djk = dist2_rn(ea.p[0], ea.p[1], ea.p[2], eb.p[0], eb.p[1], eb.p[2]);
+                mj = ea.m;
+                mk = eb.m;
+                keep = djk > rc2 || (ti < ea.tag && ti < eb.tag);
                 if (keep) {
-                    code = (type[mi] * MBX_MAX_TYPES + type[mj]) * MBX_MAX_TYPES + type[mk];
+                    code = (type[mi] * MBX_MAX_TYPES + ea.type) * MBX_MAX_TYPES + eb.type;
                     bk = R.bucket[code];
                     if (bk >= 0) {
                         // pre-filter with the evaluator's skip rule on the cloud distances

@@ -14,6 +14,9 @@
 #define MBX_STATUS_BUCKET_OVERFLOW 2
 #define MBX_STATUS_LIST_OVERFLOW 4
 
+// shared-memory bytes per staged match of k_trimers (3 + 1 doubles, 4 ints)
+#define MBX_TRIMATCH_BYTES 48
+
 struct CellGrid {
     int n[3];
     double lo[3];          // unused
