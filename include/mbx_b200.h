@@ -40,6 +40,7 @@ enum {
 #define MBX_DEVICE_PTRS 1   /* array arguments are device pointers (else host) */
 #define MBX_MIXED 2         /* FP32 monomials, FP64 accumulation (else FP64) */
 #define MBX_NO_GRADS 4      /* energy only */
+#define MBX_GRAPH 8         /* mbx_batch_energy: capture the sequence in a CUDA graph, replay it */
 
 /* Context on one device with its own stream.  Replaces the state a
  * bblock::System keeps for the 2b/3b path (system.h:1175ff).  One context per
@@ -114,6 +115,42 @@ int mbx_evaluator_info(const char* evaluator, int* nbody, int* nreal, int* nvars
 /* Device-side timing of the last mbx_energy call (ms) split into n-mer build
  * and evaluation, and the number of kernels it launched. */
 int mbx_last_timing(const mbx_ctx* ctx, double* ms_build, double* ms_eval, int* kernels);
+
+/* Batched configurations.  No counterpart in the reference (MBX evaluates
+ * one bblock::System per call); for path-integral beads, cluster sets and
+ * other independent configurations evaluated together.  The topology given
+ * to mbx_set_topology is the concatenation of nconf configurations, all
+ * monomers local: configuration k owns monomers conf_mon[k] .. conf_mon[k+1]-1
+ * (conf_mon[0] = 0, conf_mon[nconf] = nmon) and has the box boxes[9k..9k+8]
+ * when has_box[k] (boxes NULL: no configuration has one; has_box NULL: all
+ * have).  Each box must satisfy the cutoff rule of mbx_set_config. */
+int mbx_set_batch(mbx_ctx* ctx, int nconf, const int* conf_mon, const double* boxes, const int* has_box);
+
+/* One term (nbody 2 or 3) of every configuration of the batch: the n-mers of
+ * each configuration are built inside it (its box, its monomers only), then
+ * every evaluator runs once over all configurations' n-mers.  xyz: device
+ * site array of the whole batch (wrapped in place per box like mbx_energy);
+ * grad: device, += (NULL: energy only); energies[nconf] (host) receive each
+ * configuration's term energy, virials[9 nconf] (host, may be NULL) are +=.
+ * flags: MBX_DEVICE_PTRS (required), MBX_MIXED, MBX_NO_GRADS, MBX_GRAPH: the
+ * device sequence is captured into a CUDA graph after the call and replayed
+ * by later calls with the same xyz, grad and flags (re-captured whenever a
+ * buffer has to grow). */
+int mbx_batch_energy(mbx_ctx* ctx, int nbody, double* xyz, double* grad, double* energies, double* virials,
+                     int flags);
+
+/* Autotuner of the n-mer builder's launch shapes for one term (no
+ * counterpart in the reference): times the term on the current batch (or the
+ * whole system when no batch is set) with device arrays xyz/grad and flags as
+ * in mbx_batch_energy / mbx_energy, and keeps, axis by axis, the fastest
+ * warps per neighbour query (1, 4), unroll depth of the neighbour loop
+ * (1, 2, 4), threads per trimer block (64, 128, 256) or per dimer block, and
+ * whether the evaluation code is warmed into L2 beside the build.  out[5]
+ * (may be NULL): nb_warps, nb_unroll, tri_threads, dim_threads, warm;
+ * best_ms (may be NULL): the time of the chosen shape. */
+int mbx_tune(mbx_ctx* ctx, int nbody, double* xyz, double* grad, int flags, int* out, double* best_ms);
+/* The launch shapes in use for a term (out[5] as for mbx_tune). */
+int mbx_get_knobs(const mbx_ctx* ctx, int nbody, int* out);
 
 /* No counterpart in the reference.  Evaluator entry point that allocates no
  * device memory, for callers that must not call cudaMalloc (allocator-free

@@ -14,6 +14,7 @@ LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libmbx_b200
 MBX_DEVICE_PTRS = 1
 MBX_MIXED = 2
 MBX_NO_GRADS = 4
+MBX_GRAPH = 8
 
 EVALUATORS = ("mbpol2b", "mbpol3b", "ch4h2o2b", "ch4ch42b", "ch4h2o3b")
 
@@ -55,13 +56,21 @@ def lib():
     L.mbx_evaluator_info.argtypes = [ctypes.c_char_p, ip, ip, ip, ip]
     L.mbx_last_timing.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), ip]
     L.mbx_fma_peaks.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    L.mbx_set_batch.argtypes = [vp, ctypes.c_int, ip, dp, ip]
+    L.mbx_batch_energy.argtypes = [vp, ctypes.c_int, dp, dp, ctypes.POINTER(ctypes.c_double),
+                                   ctypes.POINTER(ctypes.c_double), ctypes.c_int]
+    L.mbx_tune.argtypes = [vp, ctypes.c_int, dp, dp, ctypes.c_int, ip, ctypes.POINTER(ctypes.c_double)]
+    L.mbx_get_knobs.argtypes = [vp, ctypes.c_int, ip]
     _lib = L
     return L
 
 
 EXPORTED = ("mbx_create", "mbx_destroy", "mbx_last_error", "mbx_version", "mbx_set_topology", "mbx_set_config",
             "mbx_energy", "mbx_last_counts", "mbx_nmers", "mbx_evaluate", "mbx_evaluate_dcoef", "mbx_poly",
-            "mbx_set_coefficients", "mbx_evaluator_info", "mbx_last_timing", "mbx_fma_peaks")
+            "mbx_set_coefficients", "mbx_evaluator_info", "mbx_last_timing", "mbx_fma_peaks", "mbx_set_batch",
+            "mbx_batch_energy", "mbx_tune", "mbx_get_knobs")
+
+KNOBS = ("nb_warps", "nb_unroll", "tri_threads", "dim_threads", "warm")
 
 
 def evaluator_info(name):
@@ -217,3 +226,51 @@ class Context:
     def set_coefficients(self, name, a=None):
         pa, da = _ptr(None if a is None else a)
         self._check(lib().mbx_set_coefficients(self.h, name.encode(), pa, MBX_DEVICE_PTRS if da else 0))
+
+    # ------------------------------------------------------------ batches
+    def set_batch(self, conf_mon, boxes=None, has_box=None):
+        """Configuration k owns monomers conf_mon[k] .. conf_mon[k+1]-1 of the
+        topology; boxes[k] (9) where has_box[k]."""
+        cm = np.ascontiguousarray(conf_mon, np.int32)
+        nconf = len(cm) - 1
+        b = None if boxes is None else np.ascontiguousarray(boxes, np.float64).reshape(nconf, 9)
+        hb = None if has_box is None else np.ascontiguousarray(has_box, np.int32)
+        ipp = ctypes.POINTER(ctypes.c_int)
+        self._check(lib().mbx_set_batch(self.h, nconf, cm.ctypes.data_as(ipp), None if b is None else b.ctypes.data,
+                                        None if hb is None else hb.ctypes.data_as(ipp)))
+        self._nconf = nconf
+        self._keep = (cm, b, hb)
+
+    def batch_energy(self, nbody, xyz, grad=None, mixed=False, graph=False, virials=False):
+        """One term of every configuration (device xyz, device grad +=).
+        Returns energies[nconf] (and virials[nconf, 9] when asked)."""
+        px, dx = _ptr(xyz)
+        pg, dg = _ptr(grad)
+        if not dx or (grad is not None and not dg):
+            raise TypeError("batches take CUDA tensors")
+        flags = MBX_DEVICE_PTRS | (MBX_MIXED if mixed else 0) | (MBX_GRAPH if graph else 0) | \
+            (0 if grad is not None else MBX_NO_GRADS)
+        e = np.zeros(self._nconf)
+        v = np.zeros((self._nconf, 9)) if virials else None
+        dpp = ctypes.POINTER(ctypes.c_double)
+        self._check(lib().mbx_batch_energy(self.h, nbody, px, pg, e.ctypes.data_as(dpp),
+                                           None if v is None else v.ctypes.data_as(dpp), flags))
+        return (e, v) if virials else e
+
+    def tune(self, nbody, xyz, grad=None, mixed=False):
+        """Autotunes the builder's launch shapes of a term on the current batch
+        (or system); returns (knobs dict, best ms)."""
+        px, dx = _ptr(xyz)
+        pg, _ = _ptr(grad)
+        if not dx:
+            raise TypeError("tuning takes CUDA tensors")
+        flags = MBX_DEVICE_PTRS | (MBX_MIXED if mixed else 0) | (0 if grad is not None else MBX_NO_GRADS)
+        out = (ctypes.c_int * 5)()
+        ms = ctypes.c_double()
+        self._check(lib().mbx_tune(self.h, nbody, px, pg, flags, out, ctypes.byref(ms)))
+        return dict(zip(KNOBS, list(out))), ms.value
+
+    def knobs(self, nbody):
+        out = (ctypes.c_int * 5)()
+        self._check(lib().mbx_get_knobs(self.h, nbody, out))
+        return dict(zip(KNOBS, list(out)))

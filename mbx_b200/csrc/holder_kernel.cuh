@@ -38,6 +38,11 @@ struct HolderArgs {
     double* e_per;             // optional: switched energy of every n-mer
     const double* coef;        // custom linear coefficients (global) or null
     int aos;                   // 1: AoS per-n-mer input (already imaged, no gather)
+    // batched configurations (system input): per-configuration boxes and
+    // energy + virial sums (8 doubles each), the configuration of every monomer
+    const BoxParams* conf_bp;  // null: one configuration in bp
+    const int* mon_conf;
+    double* conf_out;
     // table-driven polynomial (warp kernel)
     const int4* terms;         // (k, v0 | v1<<8 | v2<<16 | v3<<24 (255 = none), deg, unused)
     const double* tcoef;       // term multiplicities
@@ -55,6 +60,37 @@ __device__ __forceinline__ double ld_volatile(const double* p) {
     double v;
     asm volatile("ld.global.nc.f64 %0, [%1];" : "=d"(v) : "l"(p));
     return v;
+}
+
+// GetCloseDimerImage / GetCloseTrimerImage: every monomer but the anchor slot
+// moved to the image next to the anchor's first atom.
+template <class T>
+__device__ __forceinline__ void image_nmer(const BoxParams& bp, int anchor, double (&r)[T::NREAL][3]) {
+    const int nat[3] = {T::NAT0, T::NAT1, T::NAT2};
+    const int first[3] = {T::FIRST0, T::FIRST1, T::FIRST2};
+    {
+        double p0[3];
+#pragma unroll
+        for (int s = 0; s < T::NBODY; ++s)
+            if (s == anchor) { p0[0] = r[first[s]][0]; p0[1] = r[first[s]][1]; p0[2] = r[first[s]][2]; }
+#pragma unroll
+        for (int s = 0; s < T::NBODY; ++s) {
+            if (s == anchor) continue;
+            double q0[3] = {r[first[s]][0], r[first[s]][1], r[first[s]][2]};
+            double d[3];
+            image_shift(bp, p0, q0, d);
+#pragma unroll
+            for (int a = 0; a < 5; ++a) {
+                if (a < nat[s]) {
+                    double q[3] = {r[first[s] + a][0], r[first[s] + a][1], r[first[s] + a][2]};
+                    apply_shift(bp, d, q);
+                    r[first[s] + a][0] = q[0];
+                    r[first[s] + a][1] = q[1];
+                    r[first[s] + a][2] = q[2];
+                }
+            }
+        }
+    }
 }
 
 template <class T, bool VOL>
@@ -79,29 +115,11 @@ __device__ __forceinline__ void load_nmer(const HolderArgs& A, long t, double (&
             if (a < 3 * nat[s]) r[first[s] + a / 3][a % 3] = VOL ? ld_volatile(p + a) : __ldg(p + a);
         }
     }
-    if (A.bp.use_pbc) {
-        const int anchor = nm.w;
-        double p0[3];
-#pragma unroll
-        for (int s = 0; s < T::NBODY; ++s)
-            if (s == anchor) { p0[0] = r[first[s]][0]; p0[1] = r[first[s]][1]; p0[2] = r[first[s]][2]; }
-#pragma unroll
-        for (int s = 0; s < T::NBODY; ++s) {
-            if (s == anchor) continue;
-            double q0[3] = {r[first[s]][0], r[first[s]][1], r[first[s]][2]};
-            double d[3];
-            image_shift(A.bp, p0, q0, d);
-#pragma unroll
-            for (int a = 0; a < 5; ++a) {
-                if (a < nat[s]) {
-                    double q[3] = {r[first[s] + a][0], r[first[s] + a][1], r[first[s] + a][2]};
-                    apply_shift(A.bp, d, q);
-                    r[first[s] + a][0] = q[0];
-                    r[first[s] + a][1] = q[1];
-                    r[first[s] + a][2] = q[2];
-                }
-            }
-        }
+    if (A.conf_bp) {
+        const BoxParams& bp = A.conf_bp[__ldg(A.mon_conf + nm.x)];
+        if (bp.use_pbc) image_nmer<T>(bp, nm.w, r);
+    } else if (A.bp.use_pbc) {
+        image_nmer<T>(A.bp, nm.w, r);
     }
 }
 
@@ -163,6 +181,21 @@ __device__ __forceinline__ double apply_switch(const double (&d)[3][3], const do
     return s0 * s1 + s0 * s2 + s1 * s2;
 }
 
+// Adds v[0..7) into dst[0..7) (one configuration's energy and virial), one
+// atomic per value for all lanes of the warp that are here with the same dst.
+__device__ __forceinline__ void conf_accumulate(double* dst, const double (&v)[7]) {
+    const int lane = threadIdx.x & 31;
+    const unsigned act = __activemask();
+    const unsigned peers = __match_any_sync(act, (unsigned long long)dst);
+    const int leader = __ffs(peers) - 1;
+#pragma unroll
+    for (int i = 0; i < 7; ++i) {
+        double sum = 0.0;
+        for (unsigned m = peers; m; m &= m - 1) sum += __shfl_sync(peers, v[i], __ffs(m) - 1);
+        if (lane == leader && sum != 0.0) atomicAdd(dst + i, sum);
+    }
+}
+
 // Everything after the polynomial: chain rule, switch, virial, scatter.
 template <class T>
 __device__ __forceinline__ void finish_nmer(const HolderArgs& A, long t, double ep, const double (&g)[T::NVARS],
@@ -190,18 +223,26 @@ __device__ __forceinline__ void finish_nmer(const HolderArgs& A, long t, double 
         apply_switch<T>(d, rr, ep, tg, true);
     }
     const double es = sw * ep;
-    acc[0] += es;
     if (A.e_per) A.e_per[t] = es;
-    if (!grads) return;
+    double v[7] = {es, 0, 0, 0, 0, 0, 0};
+    if (grads) {
 #pragma unroll
-    for (int i = 0; i < T::NREAL; ++i) {
-        acc[1] -= r[i][0] * tg[i][0];
-        acc[2] -= r[i][0] * tg[i][1];
-        acc[3] -= r[i][0] * tg[i][2];
-        acc[4] -= r[i][1] * tg[i][1];
-        acc[5] -= r[i][1] * tg[i][2];
-        acc[6] -= r[i][2] * tg[i][2];
+        for (int i = 0; i < T::NREAL; ++i) {
+            v[1] -= r[i][0] * tg[i][0];
+            v[2] -= r[i][0] * tg[i][1];
+            v[3] -= r[i][0] * tg[i][2];
+            v[4] -= r[i][1] * tg[i][1];
+            v[5] -= r[i][1] * tg[i][2];
+            v[6] -= r[i][2] * tg[i][2];
+        }
     }
+    if (A.conf_out) {
+        conf_accumulate(A.conf_out + 8 * __ldg(A.mon_conf + __ldg(A.nmers + t).x), v);
+    } else {
+#pragma unroll
+        for (int i = 0; i < 7; ++i) acc[i] += v[i];
+    }
+    if (!grads) return;
     if (A.aos) {
         double* p = A.grad + (size_t)t * (T::NREAL * 3);
 #pragma unroll

@@ -10,6 +10,8 @@
 // accumulated like grad_ and virial_.
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -53,6 +55,10 @@ struct EvaluatorInfo {
 
 namespace {
 
+// Incremented whenever a device buffer is reallocated: a captured graph holds
+// the old addresses and is re-captured when this has moved on.
+std::atomic<unsigned long> g_realloc_gen{0};
+
 template <class T>
 struct DevBuf {
     T* p = nullptr;
@@ -61,6 +67,7 @@ struct DevBuf {
         if (want <= n && p) return cudaSuccess;
         size_t m = std::max(want, n + n / 2);
         if (m == 0) m = 1;
+        g_realloc_gen.fetch_add(1);
         if (p) cudaFree(p);
         p = nullptr;
         n = 0;
@@ -140,12 +147,35 @@ struct mbx_ctx {
     DevBuf<int4> terms;
     DevBuf<double> tcoef, warp_coef;
     int nb_cap = 192;
+    // runtime launch shapes of the builder (set by mbx_tune)
+    struct Knobs {
+        int nb_warps = 4, nb_unroll = 2, tri_threads = 128, dim_threads = 128;
+        int warm = 1;   // code warm-up launch beside the build
+    } knobs[4];         // per term (indexed by nbody)
     double* h_out = nullptr;  // pinned: [0..7] term outputs, [8..15] counters
     cudaEvent_t ev[3];
     // code warm-up of the evaluation kernels, beside the n-mer build
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     DevBuf<double> warm_sink;
+
+    // batched configurations: configuration k owns monomers conf_mon[k] ..
+    // conf_mon[k+1]-1 and has box conf_bp[k]
+    int nconf = 0;
+    std::vector<int> conf_mon;
+    std::vector<BoxParams> conf_bp;
+    DevBuf<BoxParams> d_conf_bp;
+    DevBuf<int> d_mon_conf;
+    DevBuf<double> conf_out;
+    double* h_conf = nullptr;   // pinned, 8 per configuration
+    // captured batch sequences (per term), replayed while the key matches
+    struct Graph {
+        cudaGraphExec_t exec = nullptr;
+        const double* xyz = nullptr;
+        const double* grad = nullptr;
+        int flags = 0;
+        unsigned long gen = 0;
+    } graph[4];
 
     // results of the last call
     long last_listed[4] = {0, 0, 0, 0};
@@ -247,11 +277,17 @@ int mbx_destroy(mbx_ctx* c) {
     c->list.release();
     c->listed.release();
     c->terms.release();
+    c->d_conf_bp.release();
+    c->d_mon_conf.release();
+    c->conf_out.release();
     if (c->h_out) cudaFreeHost(c->h_out);
     for (int i = 0; i < 3; ++i) cudaEventDestroy(c->ev[i]);
     if (c->ev_fork) cudaEventDestroy(c->ev_fork);
     if (c->ev_join) cudaEventDestroy(c->ev_join);
     if (c->side) cudaStreamDestroy(c->side);
+    for (auto& gr : c->graph)
+        if (gr.exec) cudaGraphExecDestroy(gr.exec);
+    if (c->h_conf) cudaFreeHost(c->h_conf);
     if (c->own_stream) cudaStreamDestroy(c->stream);
     delete c;
     return MBX_OK;
@@ -457,39 +493,45 @@ static int invert_box(const double* b, double* inv) {
     return 0;
 }
 
+// BoxParams of a box (NULL: no periodic boundaries).  The search finds at
+// most one image of each monomer only while the cutoff rc is below half of
+// every box height (sys_tools.cpp:553-555): MBX_EDOM otherwise.
+static int make_box(mbx_ctx* c, const double* box, double rc, BoxParams* out) {
+    memset(out, 0, sizeof(*out));
+    out->use_pbc = box ? 1 : 0;
+    if (!box) return MBX_OK;
+    for (int i = 0; i < 9; ++i) out->box[i] = box[i];
+    if (invert_box(box, out->inv)) return fail(c, MBX_EINVAL, "Matrix has no inverse. Determinant is 0");
+    const double* a = box;
+    const double* bb = box + 3;
+    const double* cc = box + 6;
+    auto cross = [](const double* u, const double* v, double* w) {
+        w[0] = u[1] * v[2] - u[2] * v[1];
+        w[1] = u[2] * v[0] - u[0] * v[2];
+        w[2] = u[0] * v[1] - u[1] * v[0];
+    };
+    double bc[3], ca[3], ab[3];
+    cross(bb, cc, bc);
+    cross(cc, a, ca);
+    cross(a, bb, ab);
+    const double vol = std::fabs(a[0] * bc[0] + a[1] * bc[1] + a[2] * bc[2]);
+    const double h[3] = {vol / std::sqrt(bc[0] * bc[0] + bc[1] * bc[1] + bc[2] * bc[2]),
+                         vol / std::sqrt(ca[0] * ca[0] + ca[1] * ca[1] + ca[2] * ca[2]),
+                         vol / std::sqrt(ab[0] * ab[0] + ab[1] * ab[1] + ab[2] * ab[2])};
+    for (int k = 0; k < 3; ++k)
+        if (2.0 * rc >= h[k])
+            return fail(c, MBX_EDOM, "cutoff " + std::to_string(rc) + " is not below half the box height " +
+                                         std::to_string(h[k]));
+    return MBX_OK;
+}
+
 extern "C" int mbx_set_config(mbx_ctx* c, double cutoff2b, double cutoff3b, const double* box, int n2,
                               const char* const* ignore2b, int n3, const char* const* ignore3b) {
     if (!c || !(cutoff2b >= 0) || !(cutoff3b >= 0)) return fail(c, MBX_EINVAL, "bad cutoffs");
     c->cutoff[2] = cutoff2b;
     c->cutoff[3] = cutoff3b;
-    c->bp.use_pbc = box ? 1 : 0;
-    if (box) {
-        for (int i = 0; i < 9; ++i) c->bp.box[i] = box[i];
-        if (invert_box(box, c->bp.inv)) return fail(c, MBX_EINVAL, "Matrix has no inverse. Determinant is 0");
-        // the search finds at most one image of each monomer only while the
-        // cutoff is below half of every box height (sys_tools.cpp:553-555)
-        const double* a = box;
-        const double* bb = box + 3;
-        const double* cc = box + 6;
-        auto cross = [](const double* u, const double* v, double* w) {
-            w[0] = u[1] * v[2] - u[2] * v[1];
-            w[1] = u[2] * v[0] - u[0] * v[2];
-            w[2] = u[0] * v[1] - u[1] * v[0];
-        };
-        double bc[3], ca[3], ab[3];
-        cross(bb, cc, bc);
-        cross(cc, a, ca);
-        cross(a, bb, ab);
-        const double vol = std::fabs(a[0] * bc[0] + a[1] * bc[1] + a[2] * bc[2]);
-        const double h[3] = {vol / std::sqrt(bc[0] * bc[0] + bc[1] * bc[1] + bc[2] * bc[2]),
-                             vol / std::sqrt(ca[0] * ca[0] + ca[1] * ca[1] + ca[2] * ca[2]),
-                             vol / std::sqrt(ab[0] * ab[0] + ab[1] * ab[1] + ab[2] * ab[2])};
-        const double rc = std::max(cutoff2b, cutoff3b);
-        for (int k = 0; k < 3; ++k)
-            if (2.0 * rc >= h[k])
-                return fail(c, MBX_EDOM, "cutoff " + std::to_string(rc) + " is not below half the box height " +
-                                             std::to_string(h[k]));
-    }
+    int r = make_box(c, box, std::max(cutoff2b, cutoff3b), &c->bp);
+    if (r) return r;
     c->ignore[2].clear();
     c->ignore[3].clear();
     for (int i = 0; i < n2; ++i) c->ignore[2].push_back({ignore2b[2 * i], ignore2b[2 * i + 1]});
@@ -498,13 +540,13 @@ extern "C" int mbx_set_config(mbx_ctx* c, double cutoff2b, double cutoff3b, cons
     return MBX_OK;
 }
 
-// Cell grid for a search of radius rc.
-static CellGrid make_grid(const mbx_ctx* c, double rc, int nmem) {
+// Cell grid for a search of radius rc in box bp.
+static CellGrid make_grid(const BoxParams& bp, double rc, int nmem) {
     CellGrid g{};
-    if (c->bp.use_pbc) {
-        const double* a = c->bp.box;
-        const double* b = c->bp.box + 3;
-        const double* cc = c->bp.box + 6;
+    if (bp.use_pbc) {
+        const double* a = bp.box;
+        const double* b = bp.box + 3;
+        const double* cc = bp.box + 6;
         auto cross = [](const double* u, const double* v, double* w) {
             w[0] = u[1] * v[2] - u[2] * v[1];
             w[1] = u[2] * v[0] - u[0] * v[2];
@@ -531,29 +573,13 @@ static CellGrid make_grid(const mbx_ctx* c, double rc, int nmem) {
     return g;
 }
 
-// Enumerates the n-mers of one term into the evaluator buckets (and, when
-// list_cap > 0, into c->list).  Asynchronous; status and counts on device.
-static int launch_build(mbx_ctx* c, int nbody, int use_ghost, const double* xyz, long list_cap, int* kernels,
-                        bool mixed = false) {
-    const int g = use_ghost ? 1 : 0;
-    const int nmem = c->nmem[g], nq = c->nquery[g];
-    const double rc = c->cutoff[nbody];
-    const double rc2 = rc * rc;
-    CellGrid cg = make_grid(c, rc, nmem);
-    const int ncell = cg.n[0] * cg.n[1] * cg.n[2];
-    CUCHK(c, c->cloud.ensure((size_t)std::max(nmem, 1) * 24));
-    CUCHK(c, c->cell_of.ensure(std::max(nmem, 1)));
-    CUCHK(c, c->cell_items.ensure(std::max(nmem, 1)));
-    CUCHK(c, c->cell_count.ensure(ncell + 1));
-    CUCHK(c, c->cell_start.ensure(ncell + 1));
-    CUCHK(c, c->cell_fill.ensure(ncell + 1));
-    CUCHK(c, c->nb_count.ensure(std::max(nq, 1)));
-    CUCHK(c, c->nb.ensure((size_t)std::max(nq, 1) * c->nb_cap));
+// Bucket capacities (grown on overflow; first guess from the query count)
+// and offsets of one term; zeroes the bucket counters and the status word.
+static int prepare_buckets(mbx_ctx* c, int nbody, long nq_guess, long list_cap) {
     CUCHK(c, c->bucket_count.ensure(MBX_MAX_BUCKETS));
-    // bucket capacities: grown on overflow, first guess from the query count
     long total = 0;
     for (int b = 0; b < c->nbucket[nbody]; ++b) {
-        if (c->bucket_cap[nbody][b] == 0) c->bucket_cap[nbody][b] = (long)std::max(nq, 1) * (nbody == 2 ? 40 : 80);
+        if (c->bucket_cap[nbody][b] == 0) c->bucket_cap[nbody][b] = std::max(nq_guess, 1L) * (nbody == 2 ? 40 : 80);
         total += c->bucket_cap[nbody][b];
     }
     CUCHK(c, c->buckets.ensure(std::max(total, 1L)));
@@ -564,57 +590,89 @@ static int launch_build(mbx_ctx* c, int nbody, int use_ghost, const double* xyz,
         off += c->bucket_cap[nbody][b];
     }
     if (list_cap > 0) CUCHK(c, c->list.ensure(list_cap));
-    CUCHK(c, cudaMemsetAsync(c->cell_count.p, 0, (ncell + 1) * sizeof(int), c->stream));
     CUCHK(c, cudaMemsetAsync(c->bucket_count.p, 0, MBX_MAX_BUCKETS * sizeof(int), c->stream));
     CUCHK(c, cudaMemsetAsync(c->listed.p, 0, 4 * sizeof(unsigned long long), c->stream));
     CUCHK(c, cudaMemsetAsync(c->status.p, 0, 4 * sizeof(int), c->stream));
+    return MBX_OK;
+}
+
+// One search: the monomers members[0..nmem) (global ids) searched around
+// the queries query[0..nq) (positions in members), in box bp.
+struct BuildScope {
+    const int* members;
+    int nmem;
+    const int* query;
+    int nq;
+    BoxParams bp;
+};
+
+// Enumerates the n-mers of one scope into the evaluator buckets (appending:
+// the counters are zeroed by prepare_buckets) and, when list_cap > 0, into
+// c->list.  Asynchronous; status and counts on device.
+static int launch_build_scope(mbx_ctx* c, int nbody, const BuildScope& S, const double* xyz, long list_cap,
+                              int* kernels, bool mixed) {
+    const int nmem = S.nmem, nq = S.nq;
     if (nmem < 2 || (nbody == 3 && nmem < 3) || nq == 0) return MBX_OK;
+    const double rc = c->cutoff[nbody];
+    const double rc2 = rc * rc;
+    CellGrid cg = make_grid(S.bp, rc, nmem);
+    const int ncell = cg.n[0] * cg.n[1] * cg.n[2];
+    CUCHK(c, c->cloud.ensure((size_t)std::max(nmem, 1) * 24));
+    CUCHK(c, c->cell_of.ensure(std::max(nmem, 1)));
+    CUCHK(c, c->cell_items.ensure(std::max(nmem, 1)));
+    CUCHK(c, c->cell_count.ensure(ncell + 1));
+    CUCHK(c, c->cell_start.ensure(ncell + 1));
+    CUCHK(c, c->cell_fill.ensure(ncell + 1));
+    CUCHK(c, c->nb_count.ensure(std::max(nq, 1)));
+    CUCHK(c, c->nb.ensure((size_t)std::max(nq, 1) * c->nb_cap));
+    CUCHK(c, cudaMemsetAsync(c->cell_count.p, 0, (ncell + 1) * sizeof(int), c->stream));
     const int T = 128;
-    k_cloud<<<(nmem + T - 1) / T, T, 0, c->stream>>>(xyz, c->d_first.p, c->d_members[g].p, nmem, c->bp, cg,
-                                                     c->cloud.p, c->cell_of.p);
+    k_cloud<<<(nmem + T - 1) / T, T, 0, c->stream>>>(xyz, c->d_first.p, S.members, nmem, S.bp, cg, c->cloud.p,
+                                                     c->cell_of.p);
     k_cell_count<<<(nmem + T - 1) / T, T, 0, c->stream>>>(c->cell_of.p, nmem, c->cell_count.p);
     k_cell_scan<<<1, 1024, 0, c->stream>>>(c->cell_count.p, ncell, c->cell_start.p, c->cell_fill.p);
     k_cell_fill<<<(nmem + T - 1) / T, T, 0, c->stream>>>(c->cell_of.p, nmem, c->cell_fill.p, c->cell_items.p);
-    // one block of 4 warps per query monomer, hits staged in shared memory;
-    // a single warp when four stages would not fit
-    const size_t stage4 = (size_t)4 * c->nb_cap * sizeof(NbEntry);
-    if (stage4 <= 160 * 1024) {
-        if (stage4 > 48 * 1024)
-            CUCHK(c, cudaFuncSetAttribute(k_neighbors4, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage4));
-        k_neighbors4<<<nq, 128, stage4, c->stream>>>(c->cloud.p, c->cell_of.p, c->cell_start.p, c->cell_items.p,
-                                                       c->d_query[g].p, nq, cg, c->bp.use_pbc, rc2, c->nb_cap,
-                                                       c->nb_count.p, c->nb.p, c->status.p);
-    } else {
-        const size_t stage1 = (size_t)c->nb_cap * sizeof(NbEntry);
-        if (stage1 > 227 * 1024) return MBX_ENOMEM;
-        if (stage1 > 48 * 1024)
-            CUCHK(c, cudaFuncSetAttribute(k_neighbors1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage1));
-        k_neighbors1<<<nq, 32, stage1, c->stream>>>(c->cloud.p, c->cell_of.p, c->cell_start.p, c->cell_items.p,
-                                                      c->d_query[g].p, nq, cg, c->bp.use_pbc, rc2, c->nb_cap,
-                                                      c->nb_count.p, c->nb.p, c->status.p);
-    }
+    k_cell_sort<<<(ncell + T - 1) / T, T, 0, c->stream>>>(c->cell_start.p, ncell, c->cell_items.p);
+    // neighbour search: warps per query and unroll depth are tunable; one
+    // warp when four staging areas would not fit in shared memory
+    const auto& K = c->knobs[nbody];
+    const int nbw = (size_t)4 * c->nb_cap * sizeof(NbEntry) <= 160 * 1024 ? K.nb_warps : 1;
+    if ((size_t)c->nb_cap * sizeof(NbEntry) > 227 * 1024) return fail(c, MBX_ENOMEM, "neighbour staging");
+    RCHK(c, launch_neighbors(nbw, K.nb_unroll, c->cloud.p, c->cell_of.p, c->cell_start.p, c->cell_items.p,
+                             S.query, nq, cg, S.bp.use_pbc, rc2, c->nb_cap, c->nb_count.p, c->nb.p, c->status.p,
+                             c->stream));
     if (nbody == 2) {
         DimerRules R = c->drules;
         if (!mixed)
             for (int b = 0; b < MBX_MAX_BUCKETS; ++b) R.split2[b] = 0.0;   // no short-range split
-        k_dimers<<<(nq * 32 + T - 1) / T, T, 0, c->stream>>>(c->d_query[g].p, nq, c->d_members[g].p, c->d_tag.p,
-                                                        c->d_type.p, c->nb_count.p, c->nb.p, c->nb_cap, rc2, R,
-                                                        c->listed.p, list_cap > 0 ? c->list.p : nullptr, list_cap,
-                                                        c->buckets.p, c->bucket_count.p, c->status.p);
+        const int DT = K.dim_threads;
+        k_dimers<<<(int)(((long)nq * 32 + DT - 1) / DT), DT, 0, c->stream>>>(
+            S.query, nq, S.members, c->d_tag.p, c->d_type.p, c->nb_count.p, c->nb.p, c->nb_cap, rc2, R, c->listed.p,
+            list_cap > 0 ? c->list.p : nullptr, list_cap, c->buckets.p, c->bucket_count.p, c->status.p);
     } else {
-        // one block of 4 warps per query; its matches staged in shared memory
+        // a block per query (tunable threads); its matches staged in shared memory
         const size_t smem = (size_t)c->nb_cap * MBX_TRIMATCH_BYTES;
         if (smem > 227 * 1024) return fail(c, MBX_ENOMEM, "trimer staging exceeds shared memory");
         if (smem > 48 * 1024)
             CUCHK(c, cudaFuncSetAttribute(k_trimers, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_trimers<<<nq, 128, smem, c->stream>>>(
-            c->d_query[g].p, nq, c->d_members[g].p, c->d_tag.p, c->d_type.p, c->cloud.p, c->nb_count.p, c->nb.p,
-            c->nb_cap, rc2, c->trules, c->listed.p, list_cap > 0 ? c->list.p : nullptr, list_cap, c->buckets.p,
-            c->bucket_count.p, c->status.p);
+        k_trimers<<<nq, K.tri_threads, smem, c->stream>>>(
+            S.query, nq, S.members, c->d_tag.p, c->d_type.p, c->cloud.p, c->nb_count.p, c->nb.p, c->nb_cap, rc2,
+            c->trules, c->listed.p, list_cap > 0 ? c->list.p : nullptr, list_cap, c->buckets.p, c->bucket_count.p,
+            c->status.p);
     }
     CUCHK(c, cudaGetLastError());
-    *kernels += 7;
+    *kernels += 8;
     return MBX_OK;
+}
+
+// The whole system as one search (members/queries of the ghost mode).
+static int launch_build(mbx_ctx* c, int nbody, int use_ghost, const double* xyz, long list_cap, int* kernels,
+                        bool mixed = false) {
+    const int g = use_ghost ? 1 : 0;
+    int r = prepare_buckets(c, nbody, c->nquery[g], list_cap);
+    if (r) return r;
+    BuildScope S{c->d_members[g].p, c->nmem[g], c->d_query[g].p, c->nquery[g], c->bp};
+    return launch_build_scope(c, nbody, S, xyz, list_cap, kernels, mixed);
 }
 
 static HolderArgs base_args(mbx_ctx* c) {
@@ -681,7 +739,7 @@ extern "C" int mbx_energy(mbx_ctx* c, int nbody, double* xyz, int use_ghost, dou
         // warm the evaluation kernels' code into L2 on the side stream while
         // the n-mers are built (one warp per trie piece)
         bool warmed = false;
-        if (grads) {
+        if (grads && c->knobs[nbody].warm) {
             CUCHK(c, cudaEventRecord(c->ev_fork, c->stream));
             CUCHK(c, cudaStreamWaitEvent(c->side, c->ev_fork, 0));
             warm_fn done[2 * MBX_MAX_BUCKETS];
@@ -1033,5 +1091,315 @@ extern "C" int mbx_set_coefficients(mbx_ctx* c, const char* name, const double* 
         CUCHK(c, cudaMemcpyAsync(c->warp_coef.p, src, E->ncoef * sizeof(double),
                                  dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, c->stream));
     CUCHK(c, cudaStreamSynchronize(c->stream));
+    return MBX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Batched configurations (no counterpart in the reference, which evaluates
+// one System per call): the topology is the concatenation of nconf
+// configurations, each with its own box; one n-mer build per configuration
+// into shared buckets, then one evaluation launch per evaluator over all of
+// them, energies and virials summed per configuration.
+
+static void drop_graphs(mbx_ctx* c) {
+    for (auto& gr : c->graph) {
+        if (gr.exec) cudaGraphExecDestroy(gr.exec);
+        gr = mbx_ctx::Graph{};
+    }
+}
+
+extern "C" int mbx_set_batch(mbx_ctx* c, int nconf, const int* conf_mon, const double* boxes, const int* has_box) {
+    if (!c || nconf <= 0 || !conf_mon) return fail(c, MBX_EINVAL, "bad batch");
+    if (!c->nmon) return fail(c, MBX_EINVAL, "no topology");
+    if (conf_mon[0] != 0 || conf_mon[nconf] != c->nmon) return fail(c, MBX_EINVAL, "batch does not cover the topology");
+    for (int k = 0; k < nconf; ++k)
+        if (conf_mon[k + 1] < conf_mon[k]) return fail(c, MBX_EINVAL, "configuration ranges out of order");
+    for (int m = 0; m < c->nmon; ++m)
+        if (!c->h_local[m]) return fail(c, MBX_EINVAL, "batches take local monomers only");
+    CUCHK(c, cudaSetDevice(c->device));
+    const double rc = std::max(c->cutoff[2], c->cutoff[3]);
+    std::vector<BoxParams> bp(nconf);
+    for (int k = 0; k < nconf; ++k) {
+        const bool pbc = boxes && (!has_box || has_box[k]);
+        int r = make_box(c, pbc ? boxes + 9 * k : nullptr, rc, &bp[k]);
+        if (r) return r;
+    }
+    std::vector<int> mon_conf(c->nmon);
+    for (int k = 0; k < nconf; ++k)
+        for (int m = conf_mon[k]; m < conf_mon[k + 1]; ++m) mon_conf[m] = k;
+    drop_graphs(c);
+    c->nconf = nconf;
+    c->conf_mon.assign(conf_mon, conf_mon + nconf + 1);
+    c->conf_bp = bp;
+    CUCHK(c, c->d_conf_bp.ensure(nconf));
+    CUCHK(c, c->d_mon_conf.ensure(c->nmon));
+    CUCHK(c, c->conf_out.ensure(8 * (size_t)nconf));
+    if (c->h_conf) CUCHK(c, cudaFreeHost(c->h_conf));
+    c->h_conf = nullptr;
+    CUCHK(c, cudaMallocHost(&c->h_conf, 8 * (size_t)nconf * sizeof(double)));
+    CUCHK(c, cudaMemcpyAsync(c->d_conf_bp.p, bp.data(), nconf * sizeof(BoxParams), cudaMemcpyHostToDevice, c->stream));
+    CUCHK(c, cudaMemcpyAsync(c->d_mon_conf.p, mon_conf.data(), c->nmon * sizeof(int), cudaMemcpyHostToDevice,
+                             c->stream));
+    CUCHK(c, cudaStreamSynchronize(c->stream));
+    return MBX_OK;
+}
+
+// Everything one batched term does on the device, without a host
+// synchronisation (so that it can be captured into a graph): wrap every
+// configuration, warm the evaluation code, build every configuration's
+// n-mers, evaluate every bucket once, copy the per-configuration sums and the
+// status back to pinned memory.
+static int batch_sequence(mbx_ctx* c, int nbody, double* X, double* G, bool grads, bool mixed, int* kernels) {
+    for (int k = 0; k < c->nconf; ++k) {
+        const int b = c->conf_mon[k], n = c->conf_mon[k + 1] - b;
+        if (n > 0 && c->conf_bp[k].use_pbc) {
+            k_fix_monomers<<<(n + 127) / 128, 128, 0, c->stream>>>(X, c->d_first.p + b, c->d_nat.p + b, n,
+                                                                   c->conf_bp[k]);
+            ++*kernels;
+        }
+    }
+    bool warmed = false;
+    if (grads && c->knobs[nbody].warm) {
+        CUCHK(c, cudaEventRecord(c->ev_fork, c->stream));
+        CUCHK(c, cudaStreamWaitEvent(c->side, c->ev_fork, 0));
+        warm_fn done[MBX_MAX_BUCKETS];
+        int ndone = 0;
+        for (int b = 0; b < c->nbucket[nbody]; ++b) {
+            const EvaluatorInfo* E = c->bucket_eval[nbody][b];
+            if (c->bucket_near[nbody][b] && !mixed) continue;
+            warm_fn fn = (mixed && !c->bucket_near[nbody][b] && E->s) ? E->warm_s : E->warm_g;
+            bool seen = false;
+            for (int i = 0; i < ndone; ++i) seen = seen || done[i] == fn;
+            if (!fn || seen) continue;
+            done[ndone++] = fn;
+            RCHK(c, fn(c->warm_sink.p, c->side));
+            ++*kernels;
+        }
+        CUCHK(c, cudaEventRecord(c->ev_join, c->side));
+        warmed = true;
+    }
+    int r = prepare_buckets(c, nbody, c->nmon, 0);
+    if (r) return r;
+    for (int k = 0; k < c->nconf; ++k) {
+        const int b = c->conf_mon[k], n = c->conf_mon[k + 1] - b;
+        // members: global ids b..b+n-1 (the identity list of the all-local
+        // topology, offset); queries: positions 0..n-1 in it
+        BuildScope S{c->d_members[0].p + b, n, c->d_members[0].p, n, c->conf_bp[k]};
+        r = launch_build_scope(c, nbody, S, X, 0, kernels, mixed);
+        if (r) return r;
+    }
+    if (warmed) CUCHK(c, cudaStreamWaitEvent(c->stream, c->ev_join, 0));
+    CUCHK(c, cudaMemsetAsync(c->conf_out.p, 0, 8 * (size_t)c->nconf * sizeof(double), c->stream));
+    CUCHK(c, cudaMemsetAsync(c->out.p, 0, 16 * sizeof(double), c->stream));
+    CUCHK(c, cudaMemsetAsync(c->counters.p, 0, MBX_MAX_BUCKETS * sizeof(int), c->stream));
+    long off = 0;
+    for (int b = 0; b < c->nbucket[nbody]; ++b) {
+        HolderArgs A = base_args(c);
+        A.counter = c->counters.p + b;
+        A.n = c->bucket_cap[nbody][b];
+        A.n_dev = c->bucket_count.p + b;
+        A.status = c->status.p;
+        A.nmers = c->buckets.p + off;
+        A.xyz = X;
+        A.first_index = c->d_first.p;
+        A.grad = G;
+        A.out = c->out.p;
+        A.conf_bp = c->d_conf_bp.p;
+        A.mon_conf = c->d_mon_conf.p;
+        A.conf_out = c->conf_out.p;
+        off += c->bucket_cap[nbody][b];
+        if (c->bucket_near[nbody][b] && !mixed) continue;
+        r = launch_eval(c, c->bucket_eval[nbody][b], A, (mixed ? MBX_MIXED : 0) | (grads ? 0 : MBX_NO_GRADS),
+                        kernels, c->bucket_near[nbody][b]);
+        if (r) return r;
+    }
+    CUCHK(c, cudaMemcpyAsync(c->h_conf, c->conf_out.p, 8 * (size_t)c->nconf * sizeof(double), cudaMemcpyDeviceToHost,
+                             c->stream));
+    CUCHK(c, cudaMemcpyAsync(c->h_out + 8, c->listed.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                             c->stream));
+    CUCHK(c, cudaMemcpyAsync(c->h_out + 9, c->bucket_count.p, MBX_MAX_BUCKETS * sizeof(int), cudaMemcpyDeviceToHost,
+                             c->stream));
+    CUCHK(c, cudaMemcpyAsync(c->h_out + 13, c->status.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    return MBX_OK;
+}
+
+// After a sequence: 0 when the build fit its buffers (counts recorded), else
+// the capacities are grown and 1 is returned (run it again).
+static int batch_check(mbx_ctx* c, int nbody) {
+    int status[2];
+    memcpy(status, c->h_out + 13, sizeof(status));
+    int counts[MBX_MAX_BUCKETS];
+    memcpy(counts, c->h_out + 9, sizeof(counts));
+    if (status[0]) {
+        if (status[0] & MBX_STATUS_NB_OVERFLOW) c->nb_cap = std::max(c->nb_cap * 2, status[1] + 32);
+        for (int b = 0; b < c->nbucket[nbody]; ++b) {
+            if (counts[b] > c->bucket_cap[nbody][b]) c->bucket_cap[nbody][b] = (long)(counts[b] * 1.25) + 1024;
+            else if ((status[0] & MBX_STATUS_BUCKET_OVERFLOW) && counts[b] >= c->bucket_cap[nbody][b])
+                c->bucket_cap[nbody][b] *= 2;
+        }
+        return 1;
+    }
+    unsigned long long listed;
+    memcpy(&listed, c->h_out + 8, sizeof(listed));
+    c->last_listed[nbody] = (long)listed;
+    long ev = 0;
+    for (int b = 0; b < c->nbucket[nbody]; ++b) ev += counts[b];
+    c->last_evaluated[nbody] = ev;
+    return 0;
+}
+
+extern "C" int mbx_batch_energy(mbx_ctx* c, int nbody, double* xyz, double* grad, double* energies, double* virials,
+                                int flags) {
+    if (!c || (nbody != 2 && nbody != 3) || !xyz || !energies) return fail(c, MBX_EINVAL, "bad arguments");
+    if (!c->nconf) return fail(c, MBX_EINVAL, "no batch (mbx_set_batch)");
+    if (!(flags & MBX_DEVICE_PTRS)) return fail(c, MBX_EINVAL, "batches take device arrays (MBX_DEVICE_PTRS)");
+    CUCHK(c, cudaSetDevice(c->device));
+    const bool grads = !(flags & MBX_NO_GRADS) && grad;
+    const bool mixed = (flags & MBX_MIXED) && grads;
+    const int key = flags & (MBX_MIXED | MBX_NO_GRADS);
+    auto& gr = c->graph[nbody];
+    int kernels = 0;
+    bool done = false;
+    CUCHK(c, cudaEventRecord(c->ev[0], c->stream));
+    if ((flags & MBX_GRAPH) && gr.exec && gr.xyz == xyz && gr.grad == grad && gr.flags == key &&
+        gr.gen == g_realloc_gen.load()) {
+        CUCHK(c, cudaGraphLaunch(gr.exec, c->stream));
+        CUCHK(c, cudaEventRecord(c->ev[2], c->stream));
+        CUCHK(c, cudaStreamSynchronize(c->stream));
+        if (batch_check(c, nbody) == 0) {
+            done = true;
+            kernels = 1;
+        } else {
+            drop_graphs(c);   // buffers grow: capture again after a plain run
+        }
+    }
+    if (!done) {
+        for (int attempt = 0;; ++attempt) {
+            if (attempt == 4) return fail(c, MBX_ENOMEM, "batch buffers kept overflowing");
+            kernels = 0;
+            CUCHK(c, cudaEventRecord(c->ev[0], c->stream));
+            int r = batch_sequence(c, nbody, xyz, grads ? grad : nullptr, grads, mixed, &kernels);
+            if (r) return r;
+            CUCHK(c, cudaEventRecord(c->ev[2], c->stream));
+            CUCHK(c, cudaStreamSynchronize(c->stream));
+            if (batch_check(c, nbody) == 0) break;
+            // the failed pass added nothing (the evaluators saw the status
+            // word), so it can simply run again with the larger buffers
+        }
+        if (flags & MBX_GRAPH) {
+            // capture the same sequence for the next calls
+            if (gr.exec) cudaGraphExecDestroy(gr.exec);
+            gr = mbx_ctx::Graph{};
+            cudaGraph_t g = nullptr;
+            int dummy = 0;
+            CUCHK(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed));
+            const unsigned long gen = g_realloc_gen.load();
+            int r = batch_sequence(c, nbody, xyz, grads ? grad : nullptr, grads, mixed, &dummy);
+            cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+            if (r) {
+                if (g) cudaGraphDestroy(g);
+                return r;
+            }
+            if (e != cudaSuccess) return fail(c, MBX_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+            if (gen != g_realloc_gen.load()) {
+                cudaGraphDestroy(g);   // a buffer moved while capturing: next call captures again
+            } else {
+                e = cudaGraphInstantiate(&gr.exec, g, 0);
+                cudaGraphDestroy(g);
+                if (e != cudaSuccess) return fail(c, MBX_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+                gr.xyz = xyz;
+                gr.grad = grad;
+                gr.flags = key;
+                gr.gen = gen;
+            }
+        }
+    }
+    for (int k = 0; k < c->nconf; ++k) {
+        const double* o = c->h_conf + 8 * k;
+        energies[k] = o[0];
+        if (virials) {
+            double* v = virials + 9 * k;
+            v[0] += o[1]; v[1] += o[2]; v[2] += o[3];
+            v[3] += o[2]; v[4] += o[4]; v[5] += o[5];
+            v[6] += o[3]; v[7] += o[5]; v[8] += o[6];
+        }
+    }
+    c->last_ms_build = 0;
+    cudaEventElapsedTime(&c->last_ms_eval, c->ev[0], c->ev[2]);
+    c->last_kernels = kernels;
+    return MBX_OK;
+}
+
+// Launch shapes of the builder for one term, chosen by timing the term on the
+// caller's batch (or the whole system when no batch is set): coordinate
+// descent over the warps per neighbour query and its unroll depth, the
+// threads of the trimer pair loop ("trimers per block") and of the dimer
+// rules, and the code warm-up.  out[5] (optional) receives the choice:
+// nb_warps, nb_unroll, tri_threads, dim_threads, warm; *best_ms the time.
+extern "C" int mbx_tune(mbx_ctx* c, int nbody, double* xyz, double* grad, int flags, int* out, double* best_ms) {
+    if (!c || (nbody != 2 && nbody != 3) || !xyz) return fail(c, MBX_EINVAL, "bad arguments");
+    if (!(flags & MBX_DEVICE_PTRS)) return fail(c, MBX_EINVAL, "tuning takes device arrays (MBX_DEVICE_PTRS)");
+    const int reps = 3;
+    auto time_once = [&](double* ms) -> int {
+        double e0 = 0.0;
+        std::vector<double> e(std::max(c->nconf, 1));
+        float best = 1e30f;
+        for (int r = 0; r <= reps; ++r) {   // first pass untimed (sizes buffers, loads code)
+            int rc = c->nconf ? mbx_batch_energy(c, nbody, xyz, grad, e.data(), nullptr, flags & ~MBX_GRAPH)
+                              : mbx_energy(c, nbody, xyz, 0, &e0, grad, nullptr, flags);
+            if (rc) return rc;
+            const float t = c->nconf ? c->last_ms_eval : c->last_ms_build + c->last_ms_eval;
+            if (r > 0) best = std::min(best, t);
+        }
+        *ms = best;
+        return MBX_OK;
+    };
+    auto& K = c->knobs[nbody];
+    double cur;
+    int rc = time_once(&cur);
+    if (rc) return rc;
+    struct Axis { int* field; std::vector<int> values; };
+    std::vector<Axis> axes = {{&K.nb_warps, {4, 1}}, {&K.nb_unroll, {1, 2, 4}}, {&K.warm, {1, 0}}};
+    if (nbody == 3) axes.push_back({&K.tri_threads, {64, 128, 256}});
+    else axes.push_back({&K.dim_threads, {64, 128, 256}});
+    for (auto& ax : axes) {
+        const int keep = *ax.field;
+        int best_v = keep;
+        for (int v : ax.values) {
+            if (v == keep) continue;
+            *ax.field = v;
+            double t;
+            rc = time_once(&t);
+            if (rc) {
+                *ax.field = keep;
+                return rc;
+            }
+            if (t < cur * 0.98) {   // a clear gain only
+                cur = t;
+                best_v = v;
+            }
+        }
+        *ax.field = best_v;
+    }
+    drop_graphs(c);
+    if (out) {
+        out[0] = K.nb_warps;
+        out[1] = K.nb_unroll;
+        out[2] = K.tri_threads;
+        out[3] = K.dim_threads;
+        out[4] = K.warm;
+    }
+    if (best_ms) *best_ms = cur;
+    return MBX_OK;
+}
+
+extern "C" int mbx_get_knobs(const mbx_ctx* c, int nbody, int* out) {
+    if (!c || (nbody != 2 && nbody != 3) || !out) return MBX_EINVAL;
+    const auto& K = c->knobs[nbody];
+    out[0] = K.nb_warps;
+    out[1] = K.nb_unroll;
+    out[2] = K.tri_threads;
+    out[3] = K.dim_threads;
+    out[4] = K.warm;
     return MBX_OK;
 }

@@ -191,6 +191,25 @@ __global__ void k_cell_fill(const int* __restrict__ cell_of, int nmem, int* __re
     if (q < nmem) cell_items[atomicAdd(cell_fill + cell_of[q], 1)] = q;
 }
 
+// The items of every cell in ascending order (k_cell_fill places them in
+// atomic order): the neighbour lists, and with them the slot order of every
+// n-mer, are then the same from run to run.  One thread per cell, insertion
+// sort (a few dozen items per cell).
+__global__ void k_cell_sort(const int* __restrict__ cell_start, int ncell, int* __restrict__ cell_items) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncell) return;
+    const int b = cell_start[c], e = cell_start[c + 1];
+    for (int i = b + 1; i < e; ++i) {
+        const int v = cell_items[i];
+        int j = i - 1;
+        while (j >= b && cell_items[j] > v) {
+            cell_items[j + 1] = cell_items[j];
+            --j;
+        }
+        cell_items[j + 1] = v;
+    }
+}
+
 // Matches of every local monomer: cloud points (member q, copy s) with
 // d^2 < rc_max^2.  One warp per query; matches are appended in candidate order.
 // Matches of one query monomer: NW warps of a block split the 27 surrounding
@@ -200,7 +219,7 @@ __global__ void k_cell_fill(const int* __restrict__ cell_of, int nmem, int* __re
 // matches sets MBX_STATUS_NB_OVERFLOW and its count in status[1].
 namespace {
 
-template <int NW>
+template <int NW, int U>
 __device__ __forceinline__ void neighbors_block(const double* __restrict__ cloud, const int* __restrict__ cell_of,
                             const int* __restrict__ cell_start, const int* __restrict__ cell_items,
                             const int* __restrict__ query, int nquery, CellGrid cg, int use_pbc, double rc2,
@@ -234,16 +253,16 @@ __device__ __forceinline__ void neighbors_block(const double* __restrict__ cloud
         const int b = cell_start[cell], e = cell_start[cell + 1];
         // the cell's items in chunks of 32 (one load per lane, then shuffled);
         // its (item, copy) points in item-major order, lanes over consecutive
-        // points (coalesced cloud loads), two independent 32-point blocks at a time
+        // points (coalesced cloud loads), U independent 32-point blocks at a time
         for (int c0 = b; c0 < e; c0 += 32) {
             const int nit = e - c0 < 32 ? e - c0 : 32;
             const int my_item = lane < nit ? cell_items[c0 + lane] : 0;
             const int total = nit * ncopy;
-            for (int base = 0; base < total; base += 64) {
-                bool hit[2];
-                NbEntry ent[2];
+            for (int base = 0; base < total; base += 32 * U) {
+                bool hit[U];
+                NbEntry ent[U];
 #pragma unroll
-                for (int h = 0; h < 2; ++h) {
+                for (int h = 0; h < U; ++h) {
                     const int t = base + 32 * h + lane;
                     const bool ok = t < total;
                     const int it = ok ? t / ncopy : 0;
@@ -262,7 +281,7 @@ __device__ __forceinline__ void neighbors_block(const double* __restrict__ cloud
                     }
                 }
 #pragma unroll
-                for (int h = 0; h < 2; ++h) {
+                for (int h = 0; h < U; ++h) {
                     const unsigned m = __ballot_sync(0xffffffffu, hit[h]);
                     if (hit[h]) {
                         const int pos = count + __popc(m & ((1u << lane) - 1u));
@@ -294,28 +313,48 @@ __device__ __forceinline__ void neighbors_block(const double* __restrict__ cloud
 
 }  // namespace
 
-__global__ void __launch_bounds__(128) k_neighbors4(const double* __restrict__ cloud, const int* __restrict__ cell_of,
-                                                    const int* __restrict__ cell_start,
-                                                    const int* __restrict__ cell_items, const int* __restrict__ query,
-                                                    int nquery, CellGrid cg, int use_pbc, double rc2, int cap,
-                                                    int* __restrict__ nb_count, NbEntry* __restrict__ nb,
-                                                    int* __restrict__ status) {
+template <int NW, int U>
+__global__ void __launch_bounds__(NW * 32) k_neighbors(const double* __restrict__ cloud,
+                                                       const int* __restrict__ cell_of,
+                                                       const int* __restrict__ cell_start,
+                                                       const int* __restrict__ cell_items,
+                                                       const int* __restrict__ query, int nquery, CellGrid cg,
+                                                       int use_pbc, double rc2, int cap, int* __restrict__ nb_count,
+                                                       NbEntry* __restrict__ nb, int* __restrict__ status) {
     extern __shared__ unsigned char smem[];
-    __shared__ int wcount[4];
-    neighbors_block<4>(cloud, cell_of, cell_start, cell_items, query, nquery, cg, use_pbc, rc2, cap, nb_count, nb,
-                       status, reinterpret_cast<NbEntry*>(smem), wcount);
+    __shared__ int wcount[NW];
+    neighbors_block<NW, U>(cloud, cell_of, cell_start, cell_items, query, nquery, cg, use_pbc, rc2, cap, nb_count,
+                           nb, status, reinterpret_cast<NbEntry*>(smem), wcount);
 }
 
-__global__ void __launch_bounds__(32) k_neighbors1(const double* __restrict__ cloud, const int* __restrict__ cell_of,
-                                                   const int* __restrict__ cell_start,
-                                                   const int* __restrict__ cell_items, const int* __restrict__ query,
-                                                   int nquery, CellGrid cg, int use_pbc, double rc2, int cap,
-                                                   int* __restrict__ nb_count, NbEntry* __restrict__ nb,
-                                                   int* __restrict__ status) {
-    extern __shared__ unsigned char smem[];
-    __shared__ int wcount[1];
-    neighbors_block<1>(cloud, cell_of, cell_start, cell_items, query, nquery, cg, use_pbc, rc2, cap, nb_count, nb,
-                       status, reinterpret_cast<NbEntry*>(smem), wcount);
+// Host side: one block of `warps` warps per query (1 or 4), U = `unroll`
+// independent 32-point blocks per iteration (1, 2 or 4); the hits of each
+// warp are staged in warps x cap NbEntry of dynamic shared memory.
+int launch_neighbors(int warps, int unroll, const double* cloud, const int* cell_of, const int* cell_start,
+                     const int* cell_items, const int* query, int nquery, CellGrid cg, int use_pbc, double rc2,
+                     int cap, int* nb_count, NbEntry* nb, int* status, cudaStream_t s) {
+    if (nquery <= 0) return 0;
+    const size_t smem = (size_t)warps * cap * sizeof(NbEntry);
+    if (smem > 227 * 1024) return (int)cudaErrorInvalidValue;
+#define MBX_NB_CASE(NW, UU)                                                                                      \
+    if (warps == NW && unroll == UU) {                                                                           \
+        if (smem > 48 * 1024) {                                                                                  \
+            cudaError_t e = cudaFuncSetAttribute(k_neighbors<NW, UU>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                                 (int)smem);                                                    \
+            if (e != cudaSuccess) return (int)e;                                                                 \
+        }                                                                                                        \
+        k_neighbors<NW, UU><<<nquery, NW * 32, smem, s>>>(cloud, cell_of, cell_start, cell_items, query, nquery, \
+                                                           cg, use_pbc, rc2, cap, nb_count, nb, status);          \
+        return (int)cudaGetLastError();                                                                          \
+    }
+    MBX_NB_CASE(4, 1)
+    MBX_NB_CASE(4, 2)
+    MBX_NB_CASE(4, 4)
+    MBX_NB_CASE(1, 1)
+    MBX_NB_CASE(1, 2)
+    MBX_NB_CASE(1, 4)
+#undef MBX_NB_CASE
+    return (int)cudaErrorInvalidValue;
 }
 
 namespace {
@@ -415,7 +454,7 @@ __global__ void k_dimers(const int* __restrict__ query, int nquery, const int* _
 // Trimers: a block of warps per query monomer i.  Its matches within rc are
 // staged in shared memory with everything the rules read (cloud point,
 // member, tag, type), then the block's lanes run over the pairs of matches.
-__global__ void __launch_bounds__(128) k_trimers(const int* __restrict__ query, int nquery,
+__global__ void __launch_bounds__(256) k_trimers(const int* __restrict__ query, int nquery,
                           const int* __restrict__ members,
                           const int* __restrict__ tag, const int* __restrict__ type, const double* __restrict__ cloud,
                           const int* __restrict__ nb_count, const NbEntry* __restrict__ nb, int cap, double rc2,

@@ -54,14 +54,12 @@ __global__ void k_cloud(const double* xyz, const int* first_index, const int* me
 __global__ void k_cell_count(const int* cell_of, int nmem, int* cell_count);
 __global__ void k_cell_scan(const int* cell_count, int ncell, int* cell_start, int* cell_fill);
 __global__ void k_cell_fill(const int* cell_of, int nmem, int* cell_fill, int* cell_items);
-// one block of 4 warps (k_neighbors4) or of 1 warp (k_neighbors1) per query;
-// dynamic shared memory: warps x cap NbEntry
-__global__ void k_neighbors4(const double* cloud, const int* cell_of, const int* cell_start, const int* cell_items,
-                             const int* query, int nquery, CellGrid cg, int use_pbc, double rc2, int cap,
-                             int* nb_count, NbEntry* nb, int* status);
-__global__ void k_neighbors1(const double* cloud, const int* cell_of, const int* cell_start, const int* cell_items,
-                             const int* query, int nquery, CellGrid cg, int use_pbc, double rc2, int cap,
-                             int* nb_count, NbEntry* nb, int* status);
+__global__ void k_cell_sort(const int* cell_start, int ncell, int* cell_items);
+// Matches of every query monomer (k_neighbors): `warps` warps per query (1 or
+// 4), `unroll` independent 32-point blocks per iteration (1, 2 or 4).
+int launch_neighbors(int warps, int unroll, const double* cloud, const int* cell_of, const int* cell_start,
+                     const int* cell_items, const int* query, int nquery, CellGrid cg, int use_pbc, double rc2,
+                     int cap, int* nb_count, NbEntry* nb, int* status, cudaStream_t s);
 __global__ void k_dimers(const int* query, int nquery, const int* members, const int* tag, const int* type,
                          const int* nb_count, const NbEntry* nb, int cap, double rc2, DimerRules R,
                          unsigned long long* listed, int4* list, long list_cap, int4* bucket_data,

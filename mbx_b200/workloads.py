@@ -148,3 +148,19 @@ def methane_water_box(n_ch4=57, n_h2o=513, box=(24.6, 24.6, 31.0), seed=0, dmin=
     ids = ["ch4"] * n_ch4 + ["h2o"] * n_h2o
     xyz = np.concatenate([ch4.reshape(-1), h2o.reshape(-1)])
     return ids, xyz, np.array([L[0], 0, 0, 0, L[1], 0, 0, 0, L[2]], float)
+
+
+def batch_beads_clusters(n_beads=32, n_clusters=64, sigma=0.05, nmin=8, nmax=512, seed=0):
+    """The batched workload: n_beads path-integral beads of the 2048-water box
+    (every atom displaced by independent Gaussian noise of width sigma A per
+    bead) plus n_clusters gas-phase water clusters of sizes drawn uniformly
+    from nmin..nmax molecules at liquid density in a sphere.  Returns
+    [(ids, input-order xyz, box or None)]."""
+    ids, xyz, box = water_2048(seed)
+    out = [(ids, b, box) for b in beads(xyz, n_beads, sigma, seed + 1)]
+    rng = np.random.default_rng(seed + 2)
+    sizes = rng.integers(nmin, nmax + 1, size=n_clusters)
+    for k, n in enumerate(sizes):
+        cid, cxyz = water_cluster(int(n), seed=seed + 1000 + k)
+        out.append((cid, cxyz, None))
+    return out
