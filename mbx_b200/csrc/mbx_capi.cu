@@ -140,7 +140,8 @@ struct mbx_ctx {
 
     // work buffers
     DevBuf<double> xyz, grad, out, cloud, coef_ws;
-    DevBuf<int> cell_of, cell_count, cell_start, cell_fill, cell_items, nb_count, bucket_count, status, counters;
+    DevBuf<int> cell_of, cell_count, cell_start, cell_fill, cell_items, cell_sorted, nb_count, bucket_count, status,
+        counters;
     DevBuf<NbEntry> nb;
     DevBuf<int4> buckets, list;
     DevBuf<unsigned long long> listed;
@@ -267,8 +268,8 @@ int mbx_destroy(mbx_ctx* c) {
     cudaStreamSynchronize(c->stream);
     DevBuf<int>* ib[] = {&c->d_first, &c->d_nat, &c->d_tag, &c->d_type, &c->d_members[0], &c->d_members[1],
                          &c->d_query[0], &c->d_query[1], &c->cell_of, &c->cell_count, &c->cell_start,
-                         &c->cell_fill, &c->cell_items, &c->nb_count, &c->bucket_count, &c->status,
-                         &c->counters};
+                         &c->cell_fill, &c->cell_items, &c->cell_sorted, &c->nb_count, &c->bucket_count,
+                         &c->status, &c->counters};
     for (auto* b : ib) b->release();
     DevBuf<double>* db[] = {&c->xyz, &c->grad, &c->out, &c->cloud, &c->coef_ws, &c->tcoef, &c->warp_coef};
     for (auto* b : db) b->release();
@@ -620,6 +621,7 @@ static int launch_build_scope(mbx_ctx* c, int nbody, const BuildScope& S, const 
     CUCHK(c, c->cloud.ensure((size_t)std::max(nmem, 1) * 24));
     CUCHK(c, c->cell_of.ensure(std::max(nmem, 1)));
     CUCHK(c, c->cell_items.ensure(std::max(nmem, 1)));
+    CUCHK(c, c->cell_sorted.ensure(std::max(nmem, 1)));
     CUCHK(c, c->cell_count.ensure(ncell + 1));
     CUCHK(c, c->cell_start.ensure(ncell + 1));
     CUCHK(c, c->cell_fill.ensure(ncell + 1));
@@ -632,13 +634,14 @@ static int launch_build_scope(mbx_ctx* c, int nbody, const BuildScope& S, const 
     k_cell_count<<<(nmem + T - 1) / T, T, 0, c->stream>>>(c->cell_of.p, nmem, c->cell_count.p);
     k_cell_scan<<<1, 1024, 0, c->stream>>>(c->cell_count.p, ncell, c->cell_start.p, c->cell_fill.p);
     k_cell_fill<<<(nmem + T - 1) / T, T, 0, c->stream>>>(c->cell_of.p, nmem, c->cell_fill.p, c->cell_items.p);
-    k_cell_sort<<<(ncell + T - 1) / T, T, 0, c->stream>>>(c->cell_start.p, ncell, c->cell_items.p);
+    k_cell_sort<<<(ncell * 32 + T - 1) / T, T, 0, c->stream>>>(c->cell_start.p, ncell, c->cell_items.p,
+                                                                c->cell_sorted.p);
     // neighbour search: warps per query and unroll depth are tunable; one
     // warp when four staging areas would not fit in shared memory
     const auto& K = c->knobs[nbody];
     const int nbw = (size_t)4 * c->nb_cap * sizeof(NbEntry) <= 160 * 1024 ? K.nb_warps : 1;
     if ((size_t)c->nb_cap * sizeof(NbEntry) > 227 * 1024) return fail(c, MBX_ENOMEM, "neighbour staging");
-    RCHK(c, launch_neighbors(nbw, K.nb_unroll, c->cloud.p, c->cell_of.p, c->cell_start.p, c->cell_items.p,
+    RCHK(c, launch_neighbors(nbw, K.nb_unroll, c->cloud.p, c->cell_of.p, c->cell_start.p, c->cell_sorted.p,
                              S.query, nq, cg, S.bp.use_pbc, rc2, c->nb_cap, c->nb_count.p, c->nb.p, c->status.p,
                              c->stream));
     if (nbody == 2) {

@@ -193,25 +193,23 @@ __global__ void k_cell_fill(const int* __restrict__ cell_of, int nmem, int* __re
 
 // The items of every cell in ascending order (k_cell_fill places them in
 // atomic order): the neighbour lists, and with them the slot order of every
-// n-mer, are then the same from run to run.  One thread per cell, insertion
-// sort (a few dozen items per cell).
-__global__ void k_cell_sort(const int* __restrict__ cell_start, int ncell, int* __restrict__ cell_items) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+// n-mer, are then the same from run to run.  One warp per cell; an item's
+// place is the number of smaller items of its cell (all items differ).
+__global__ void k_cell_sort(const int* __restrict__ cell_start, int ncell, const int* __restrict__ items,
+                            int* __restrict__ sorted) {
+    const int lane = threadIdx.x & 31;
+    const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (c >= ncell) return;
-    const int b = cell_start[c], e = cell_start[c + 1];
-    for (int i = b + 1; i < e; ++i) {
-        const int v = cell_items[i];
-        int j = i - 1;
-        while (j >= b && cell_items[j] > v) {
-            cell_items[j + 1] = cell_items[j];
-            --j;
-        }
-        cell_items[j + 1] = v;
+    const int b = cell_start[c], n = cell_start[c + 1] - b;
+    for (int i0 = 0; i0 < n; i0 += 32) {
+        const int i = i0 + lane;
+        const int v = i < n ? items[b + i] : 0;
+        int rank = 0;
+        for (int j = 0; j < n; ++j) rank += items[b + j] < v;
+        if (i < n) sorted[b + rank] = v;
     }
 }
 
-// Matches of every local monomer: cloud points (member q, copy s) with
-// d^2 < rc_max^2.  One warp per query; matches are appended in candidate order.
 // Matches of one query monomer: NW warps of a block split the 27 surrounding
 // cells (each warp a contiguous run of them, in the order below), stage their
 // hits in shared memory and write them out in cell order, so the list is the

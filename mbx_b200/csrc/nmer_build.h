@@ -54,7 +54,7 @@ __global__ void k_cloud(const double* xyz, const int* first_index, const int* me
 __global__ void k_cell_count(const int* cell_of, int nmem, int* cell_count);
 __global__ void k_cell_scan(const int* cell_count, int ncell, int* cell_start, int* cell_fill);
 __global__ void k_cell_fill(const int* cell_of, int nmem, int* cell_fill, int* cell_items);
-__global__ void k_cell_sort(const int* cell_start, int ncell, int* cell_items);
+__global__ void k_cell_sort(const int* cell_start, int ncell, const int* items, int* sorted);
 // Matches of every query monomer (k_neighbors): `warps` warps per query (1 or
 // 4), `unroll` independent 32-point blocks per iteration (1, 2 or 4).
 int launch_neighbors(int warps, int unroll, const double* cloud, const int* cell_of, const int* cell_start,
