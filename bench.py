@@ -42,7 +42,7 @@ METRIC = "dimers+trimers/s with forces, 2048 H2O; FP32-mixed vs FP64 GPU at <=1e
 CUT2, CUT3 = 9.0, 7.0
 # DRAM bytes per launch of the mbpol3b gradient kernel on this workload, from one
 # ncu capture of the same command (read + write); the kernel is compute-bound
-TRAFFIC_3B = 6.22e6
+TRAFFIC_3B = 5.75e6
 
 
 def workload():

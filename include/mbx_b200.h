@@ -144,13 +144,14 @@ int mbx_batch_energy(mbx_ctx* ctx, int nbody, double* xyz, double* grad, double*
  * whole system when no batch is set) with device arrays xyz/grad and flags as
  * in mbx_batch_energy / mbx_energy, and keeps, axis by axis, the fastest
  * warps per neighbour query (1, 4), unroll depth of the neighbour loop
- * (1, 2, 4), threads per trimer block (64, 128, 256) or per dimer block, and
- * whether the evaluation code is warmed into L2 beside the build.  out[5]
- * (may be NULL): nb_warps, nb_unroll, tri_threads, dim_threads, warm;
+ * (1, 2, 4) and threads per trimer block (64, 128, 256) or per dimer block.
+ * out[4] (may be NULL): nb_warps, nb_unroll, tri_threads, dim_threads;
  * best_ms (may be NULL): the time of the chosen shape. */
 int mbx_tune(mbx_ctx* ctx, int nbody, double* xyz, double* grad, int flags, int* out, double* best_ms);
-/* The launch shapes in use for a term (out[5] as for mbx_tune). */
+/* The launch shapes in use for a term (out[4] as for mbx_tune), and setting
+ * them (e.g. a shape tuned in an earlier run; MBX_EINVAL out of range). */
 int mbx_get_knobs(const mbx_ctx* ctx, int nbody, int* out);
+int mbx_set_knobs(mbx_ctx* ctx, int nbody, const int* in);
 
 /* No counterpart in the reference.  Evaluator entry point that allocates no
  * device memory, for callers that must not call cudaMalloc (allocator-free

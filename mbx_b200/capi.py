@@ -61,6 +61,7 @@ def lib():
                                    ctypes.POINTER(ctypes.c_double), ctypes.c_int]
     L.mbx_tune.argtypes = [vp, ctypes.c_int, dp, dp, ctypes.c_int, ip, ctypes.POINTER(ctypes.c_double)]
     L.mbx_get_knobs.argtypes = [vp, ctypes.c_int, ip]
+    L.mbx_set_knobs.argtypes = [vp, ctypes.c_int, ip]
     _lib = L
     return L
 
@@ -68,9 +69,9 @@ def lib():
 EXPORTED = ("mbx_create", "mbx_destroy", "mbx_last_error", "mbx_version", "mbx_set_topology", "mbx_set_config",
             "mbx_energy", "mbx_last_counts", "mbx_nmers", "mbx_evaluate", "mbx_evaluate_dcoef", "mbx_poly",
             "mbx_set_coefficients", "mbx_evaluator_info", "mbx_last_timing", "mbx_fma_peaks", "mbx_set_batch",
-            "mbx_batch_energy", "mbx_tune", "mbx_get_knobs")
+            "mbx_batch_energy", "mbx_tune", "mbx_get_knobs", "mbx_set_knobs")
 
-KNOBS = ("nb_warps", "nb_unroll", "tri_threads", "dim_threads", "warm")
+KNOBS = ("nb_warps", "nb_unroll", "tri_threads", "dim_threads")
 
 
 def evaluator_info(name):
@@ -265,12 +266,19 @@ class Context:
         if not dx:
             raise TypeError("tuning takes CUDA tensors")
         flags = MBX_DEVICE_PTRS | (MBX_MIXED if mixed else 0) | (0 if grad is not None else MBX_NO_GRADS)
-        out = (ctypes.c_int * 5)()
+        out = (ctypes.c_int * 4)()
         ms = ctypes.c_double()
         self._check(lib().mbx_tune(self.h, nbody, px, pg, flags, out, ctypes.byref(ms)))
         return dict(zip(KNOBS, list(out))), ms.value
 
     def knobs(self, nbody):
-        out = (ctypes.c_int * 5)()
+        out = (ctypes.c_int * 4)()
         self._check(lib().mbx_get_knobs(self.h, nbody, out))
         return dict(zip(KNOBS, list(out)))
+
+    def set_knobs(self, nbody, **kw):
+        """Sets launch shapes of a term (keys of KNOBS; the others kept)."""
+        k = self.knobs(nbody)
+        k.update(kw)
+        arr = (ctypes.c_int * 4)(*[int(k[n]) for n in KNOBS])
+        self._check(lib().mbx_set_knobs(self.h, nbody, arr))

@@ -197,70 +197,75 @@ SMEM_COEF_TYPES = {"mbpol3b"}
 
 
 def emit_split(trie, nvars, name, out, nparts, arrays, body, ret="double"):
-    """Emits name_partK as __noinline__ functions over pointers to the
-    caller's arrays and a __forceinline__ name() that calls them in turn.
+    """Emits name_partK as __noinline__ functions over strided pointers to the
+    caller's arrays, and the wrappers that call them in turn.
 
     arrays: [(name, ctype, role)] with role "in" (read: copied into a local
     register array on entry) or "acc" (accumulated: zeroed locally, added to
-    the caller's array on exit).  body(w, subtrees) writes the evaluation of
-    the subtrees into the local arrays and into E."""
+    the caller's array on exit).  A piece reads element v of an array at
+    pointer[v * S], S a template parameter: S = 1 for a thread's own local
+    array, S = block size for a shared-memory array laid out [v][thread] (the
+    lockstep kernels keep x and g there: shared memory instead of the
+    thread's stack for the values every piece loads and stores).  body(w,
+    subtrees) writes the evaluation of the subtrees into the local arrays and
+    into E."""
     import re
     w = out.append
+    zero = {"float": "0.0f", "double": "0.0", "f2_t": "0ull"}
+    e0 = "make_double2(0.0, 0.0)" if ret == "double2" else "0.0"
     pieces = split_terms(trie, nparts) if SPLIT == "terms" else partition(trie, nparts)
+    params = ", ".join("%s%s* __restrict__ %sm" % ("const " if role == "in" else "", ct, a) for a, ct, role in arrays)
     for i, sub in enumerate(pieces):
         text = []
         body(text.append, sub)
         code = "\n".join(text)
-        params = ", ".join("%s%s* __restrict__ %sm" % ("const " if role == "in" else "", ct, a)
-                           for a, ct, role in arrays)
-        zero = {"float": "0.0f", "double": "0.0", "f2_t": "0ull"}
-        w("template <class Coef>")
+        w("template <class Coef, int S>")
         w("__device__ __noinline__ %s %s_part%d(const Coef& coef, %s) {" % (ret, name, i, params))
         for a, ct, role in arrays:
             used = sorted({int(v) for v in re.findall(r"\b%s\[(\d+)\]" % a, code)})
             w("    %s %s[%d];" % (ct, a, nvars))
             for v in used:
-                w("    %s[%d] = %s;" % (a, v, ("%sm[%d]" % (a, v)) if role == "in" else zero[ct]))
-        w("    %s E = %s;" % (ret, "make_double2(0.0, 0.0)" if ret == "double2" else "0.0"))
+                w("    %s[%d] = %s;" % (a, v, ("%sm[%d * S]" % (a, v)) if role == "in" else zero[ct]))
+        w("    %s E = %s;" % (ret, e0))
         w(code)
         for a, ct, role in arrays:
             if role == "acc":
                 used = sorted({int(v) for v in re.findall(r"\b%s\[(\d+)\]" % a, code)})
                 for v in used:
                     if ct == "f2_t":
-                        w("    %sm[%d] = f2_add(%sm[%d], %s[%d]);" % (a, v, a, v, a, v))
+                        w("    %sm[%d * S] = f2_add(%sm[%d * S], %s[%d]);" % (a, v, a, v, a, v))
                     else:
-                        w("    %sm[%d] += %s[%d];" % (a, v, a, v))
+                        w("    %sm[%d * S] += %s[%d];" % (a, v, a, v))
         w("    return E;")
         w("}")
-    sig = ", ".join("%s%s (&%s)[%d]" % ("const " if role == "in" else "", ct, a, nvars) for a, ct, role in arrays)
-    # name_piece(k, ...): piece k alone (the code warm-up launch runs each
-    # piece once so that its instructions are in L2 before the evaluation)
-    w("#define %s_NPIECES %d" % (name.upper(), len(pieces)))
-    w("template <class Coef>")
-    w("__device__ __forceinline__ %s %s_piece(int k, const Coef& coef, %s) {" % (ret, name, sig))
-    w("    switch (k) {")
-    for i in range(len(pieces)):
-        w("    case %d: return %s_part%d(coef, %s);" % (i, name, i, ", ".join(a for a, _, _ in arrays)))
-    w("    default: return %s;" % ("make_double2(0.0, 0.0)" if ret == "double2" else "0.0"))
-    w("    }")
-    w("}")
-    for lock in (False, True):
-        # name(): the pieces in turn; name_lock(): the same with a block
-        # barrier after every piece, so that all warps of a block run the same
-        # piece at the same time and share its instruction fetches
-        w("template <class Coef>")
-        w("__device__ __forceinline__ %s %s%s(const Coef& coef, %s) {" % (ret, name, "_lock" if lock else "", sig))
-        w("    %s E = %s;" % (ret, "make_double2(0.0, 0.0)" if ret == "double2" else "0.0"))
+
+    def calls(lock, targs, args):
         for i in range(len(pieces)):
-            call = "%s_part%d(coef, %s)" % (name, i, ", ".join(a for a, _, _ in arrays))
+            call = "%s_part%d<%s>(coef, %s)" % (name, i, targs, args)
             bar = " __syncthreads();" if lock else ""
             if ret == "double2":
                 w("    { const double2 e = %s; E.x += e.x; E.y += e.y; }%s" % (call, bar))
             else:
                 w("    E += %s;%s" % (call, bar))
-        w("    return E;")
-        w("}")
+
+    # name(coef, x[], g[]): the pieces in turn over the thread's own arrays
+    sig = ", ".join("%s%s (&%s)[%d]" % ("const " if role == "in" else "", ct, a, nvars) for a, ct, role in arrays)
+    w("template <class Coef>")
+    w("__device__ __forceinline__ %s %s(const Coef& coef, %s) {" % (ret, name, sig))
+    w("    %s E = %s;" % (ret, e0))
+    calls(False, "Coef, 1", ", ".join(a for a, _, _ in arrays))
+    w("    return E;")
+    w("}")
+    # name_lock<S>(coef, xm, gm): over shared arrays [v][S] (pointers at the
+    # thread's column), a block barrier after every piece so that all warps
+    # of a block run the same piece at the same time and share its
+    # instruction fetches
+    w("template <int S, class Coef>")
+    w("__device__ __forceinline__ %s %s_lock(const Coef& coef, %s) {" % (ret, name, params))
+    w("    %s E = %s;" % (ret, e0))
+    calls(True, "Coef, S", ", ".join("%sm" % a for a, _, _ in arrays))
+    w("    return E;")
+    w("}")
 
 
 def emit_pip(trie, nvars, name, out, nparts=1):
@@ -484,19 +489,12 @@ def emit_traits(spec, table, straight, out):
       (shifted_pip(n).norb if shifted_type else 1))
     w("    static constexpr int SMEM_COEF = %d;  // FP64 kernel reads its coefficients from shared memory" %
       (1 if n in SMEM_COEF_TYPES else 0))
-    if straight:
-        w("    template <class C> __device__ __forceinline__ static double pip_piece(int k, const C& c, "
-          "const double (&x)[%d], double (&g)[%d]) { return %s_pip_piece(k, c, x, g); }" % (spec.nvars, spec.nvars, n))
-    if shifted_type:
-        w("    template <class C> __device__ __forceinline__ static double2 pip_s32_piece(int k, const C& c, "
-          "const f2_t (&x)[%d], f2_t (&g)[%d]) { return %s_pip_s32_piece(k, c, x, g); }" % (spec.nvars, spec.nvars, n))
+
     if shifted_type:
         w("    __device__ __forceinline__ static void shift(const double (&x)[%d], float (&xf)[%d]) "
           "{ %s_shift(x, xf); }" % (spec.nvars, spec.nvars, n))
-        for lk in ("", "_lock"):
-            w("    template <class C> __device__ __forceinline__ static double2 pip_s32%s(const C& c, "
-              "const f2_t (&x)[%d], f2_t (&g)[%d]) { return %s_pip_s32%s(c, x, g); }" %
-              (lk, spec.nvars, spec.nvars, n, lk))
+        w("    template <int S, class C> __device__ __forceinline__ static double2 pip_s32_lock(const C& c, "
+          "const f2_t* __restrict__ x, f2_t* __restrict__ g) { return %s_pip_s32_lock<S>(c, x, g); }" % n)
     w("    __device__ __forceinline__ static void sites(const double (&r)[%d][3], double (&s)[%d][3]) { %s_sites(r, s); }" %
       (spec.nreal, ns, n))
     w("    __device__ __forceinline__ static void vars(const double (&s)[%d][3], double (&x)[%d]) { %s_vars(s, x); }" %
@@ -504,11 +502,14 @@ def emit_traits(spec, table, straight, out):
     w("    __device__ __forceinline__ static void chain(const double (&s)[%d][3], const double (&g)[%d], double (&sg)[%d][3]) "
       "{ %s_chain(s, g, sg); }" % (ns, spec.nvars, ns, n))
     if straight:
-        for lk in ("", "_lock"):
-            w("    template <class C> __device__ __forceinline__ static double pip%s(const C& c, const double (&x)[%d], "
-              "double (&g)[%d]) { return %s_pip%s(c, x, g); }" % (lk, spec.nvars, spec.nvars, n, lk))
-            w("    template <class C> __device__ __forceinline__ static double pip_e%s(const C& c, const double (&x)[%d]) "
-              "{ return %s_pip_e%s(c, x); }" % (lk, spec.nvars, n, lk))
+        w("    template <class C> __device__ __forceinline__ static double pip(const C& c, const double (&x)[%d], "
+          "double (&g)[%d]) { return %s_pip(c, x, g); }" % (spec.nvars, spec.nvars, n))
+        w("    template <class C> __device__ __forceinline__ static double pip_e(const C& c, const double (&x)[%d]) "
+          "{ return %s_pip_e(c, x); }" % (spec.nvars, n))
+        w("    template <int S, class C> __device__ __forceinline__ static double pip_lock(const C& c, "
+          "const double* __restrict__ x, double* __restrict__ g) { return %s_pip_lock<S>(c, x, g); }" % n)
+        w("    template <int S, class C> __device__ __forceinline__ static double pip_e_lock(const C& c, "
+          "const double* __restrict__ x) { return %s_pip_e_lock<S>(c, x); }" % n)
 
         w("    template <class S> __device__ __forceinline__ static void dcoef(const double (&x)[%d], S&& sink) "
           "{ %s_dcoef(x, sink); }" % (spec.nvars, n))
@@ -539,22 +540,20 @@ def generate(name):
     emit_vars(spec, out)
     nv = spec.nvars
     if straight:
-        out.append("template <class Coef> __device__ __forceinline__ double %s_pip_piece(int, const Coef&, "
-                   "const double (&)[%d], double (&)[%d]);" % (name, nv, nv))
-        for lk in ("", "_lock"):
-            out += ["template <class Coef> __device__ __forceinline__ double %s_pip%s(const Coef&, const double (&)[%d], "
-                    "double (&)[%d]);" % (name, lk, nv, nv),
-                    "template <class Coef> __device__ __forceinline__ double %s_pip_e%s(const Coef&, "
-                    "const double (&)[%d]);" % (name, lk, nv)]
+        out += ["template <class Coef> __device__ __forceinline__ double %s_pip(const Coef&, const double (&)[%d], "
+                "double (&)[%d]);" % (name, nv, nv),
+                "template <class Coef> __device__ __forceinline__ double %s_pip_e(const Coef&, "
+                "const double (&)[%d]);" % (name, nv),
+                "template <int S, class Coef> __device__ __forceinline__ double %s_pip_lock(const Coef&, "
+                "const double* __restrict__, double* __restrict__);" % name,
+                "template <int S, class Coef> __device__ __forceinline__ double %s_pip_e_lock(const Coef&, "
+                "const double* __restrict__);" % name]
         out += ["template <class Sink> __device__ __forceinline__ void %s_dcoef(const double (&)[%d], Sink&&);" %
                 (name, nv)]
         if name in SHIFT_TYPES:
             sp = shifted_pip(name)
-            out.append("template <class Coef> __device__ __forceinline__ double2 %s_pip_s32_piece(int, const Coef&, "
-                       "const f2_t (&)[%d], f2_t (&)[%d]);" % (name, nv, nv))
-            for lk in ("", "_lock"):
-                out.append("template <class Coef> __device__ __forceinline__ double2 %s_pip_s32%s(const Coef&, "
-                           "const f2_t (&)[%d], f2_t (&)[%d]);" % (name, lk, nv, nv))
+            out.append("template <int S, class Coef> __device__ __forceinline__ double2 %s_pip_s32_lock(const Coef&, "
+                       "const f2_t* __restrict__, f2_t* __restrict__);" % name)
             out.append("// dx = x - x0, the reference point of the FP32 basis (%s)" % SHIFT_TYPES[name])
             out.append("__device__ __forceinline__ void %s_shift(const double (&x)[%d], float (&xf)[%d]) {" %
                        (name, nv, nv))
@@ -632,50 +631,48 @@ VARIANTS = {
     "g": ("FP64 energy + gradient kernel", """
 int mbx_launch_%(name)s_g(const HolderArgs& A, int grid, int block, cudaStream_t s) {
     // persistent grid of lockstep blocks: every resident block slot once
-    // (blocks claim chunks of LOCK_THREADS n-mers dynamically)
+    // (blocks claim chunks of LOCK_THREADS n-mers dynamically); the
+    // variables and their gradient accumulators of the block's n-mers in dynamic shared memory
     auto kern = holder_lock_kernel<%(name)s_T, %(name)s_CC, HM_GRAD_FP64, false>;
     block = %(name)s_T::LOCK_THREADS;
-    static int bps = 0, sms = 0, bps_block = 0;
-    if (!bps || bps_block != block) {
+    const int smem = 2 * %(name)s_T::NVARS * %(name)s_T::LOCK_THREADS * (int)sizeof(double);
+    static int bps = 0, sms = 0;
+    if (!bps) {
         int dev = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, block, 0);
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, block, smem);
         if (bps < 1) bps = 1;
-        bps_block = block;
     }
     const long need = (A.n + block - 1) / block;
     grid = (int)(need < (long)sms * bps ? need : (long)sms * bps);
     if (grid < 1) grid = 1;
-    kern<<<grid, block, 0, s>>>(A);
-    return (int)cudaGetLastError();
-}
-
-int mbx_warm_%(name)s_g(double* sink, cudaStream_t s) {
-    // one warp per trie piece: brings the evaluation kernel's code into L2
-    holder_warm_kernel<%(name)s_T, %(name)s_CC, HM_GRAD_FP64><<<%(NAME)s_PIP_NPIECES, 32, 0, s>>>(sink);
+    kern<<<grid, block, smem, s>>>(A);
     return (int)cudaGetLastError();
 }
 """),
     "e": ("FP64 energy-only kernel", """
 int mbx_launch_%(name)s_e(const HolderArgs& A, int grid, int block, cudaStream_t s) {
     // persistent grid of lockstep blocks: every resident block slot once
-    // (blocks claim chunks of LOCK_THREADS n-mers dynamically)
+    // (blocks claim chunks of LOCK_THREADS n-mers dynamically); the
+    // variables of the block's n-mers in dynamic shared memory
     auto kern = holder_lock_kernel<%(name)s_T, %(name)s_CC, HM_ENERGY, false>;
     block = %(name)s_T::LOCK_THREADS;
-    static int bps = 0, sms = 0, bps_block = 0;
-    if (!bps || bps_block != block) {
+    const int smem = 1 * %(name)s_T::NVARS * %(name)s_T::LOCK_THREADS * (int)sizeof(double);
+    static int bps = 0, sms = 0;
+    if (!bps) {
         int dev = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, block, 0);
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, block, smem);
         if (bps < 1) bps = 1;
-        bps_block = block;
     }
     const long need = (A.n + block - 1) / block;
     grid = (int)(need < (long)sms * bps ? need : (long)sms * bps);
     if (grid < 1) grid = 1;
-    kern<<<grid, block, 0, s>>>(A);
+    kern<<<grid, block, smem, s>>>(A);
     return (int)cudaGetLastError();
 }
 """),
@@ -760,29 +757,26 @@ int mbx_set_coef_%(name)s_s(const double* a, int from_device, cudaStream_t s) {
     return (int)e;
 }
 
-int mbx_warm_%(name)s_s(double* sink, cudaStream_t s) {
-    // one warp per trie piece: brings the evaluation kernel's code into L2
-    holder_warm_kernel<%(name)s_T, %(name)s_CS, HM_GRAD_SHIFT32><<<%(NAME)s_PIP_S32_NPIECES, 32, 0, s>>>(sink);
-    return (int)cudaGetLastError();
-}
-
 int mbx_launch_%(name)s_s(const HolderArgs& A, int grid, int block, cudaStream_t s) {
     // persistent grid of lockstep blocks (two n-mers per thread): every
-    // resident block slot once
+    // resident block slot once; the paired variables and gradient
+    // accumulators of the block in dynamic shared memory
     auto kern = holder_pair_kernel<%(name)s_T, %(name)s_CS>;
     block = %(name)s_T::LOCK_THREADS_S;
+    const int smem = 2 * %(name)s_T::NVARS * %(name)s_T::LOCK_THREADS_S * (int)sizeof(f2_t);
     static int bps = 0, sms = 0;
     if (!bps) {
         int dev = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, block, 0);
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, block, smem);
         if (bps < 1) bps = 1;
     }
     const long need = (A.n + 2 * block - 1) / (2 * block);
     grid = (int)(need < (long)sms * bps ? need : (long)sms * bps);
     if (grid < 1) grid = 1;
-    kern<<<grid, block, 0, s>>>(A);
+    kern<<<grid, block, smem, s>>>(A);
     return (int)cudaGetLastError();
 }
 """
@@ -845,8 +839,6 @@ def write_registry():
             if v in "ges":
                 lines.append("int mbx_launch_%s_%s(const HolderArgs& A, int grid, int block, cudaStream_t s);" %
                              (name, v))
-            if v in "gs":
-                lines.append("int mbx_warm_%s_%s(double* sink, cudaStream_t s);" % (name, v))
             elif v == "c":
                 lines.append("int mbx_launch_%s_c(const HolderArgs& A, const double* w, double* out, int grid, "
                              "int block, cudaStream_t s);" % name)
@@ -875,7 +867,6 @@ def write_registry():
                       spec.nvars, name, fn("g", "launch"), fn("e", "launch"), fn("c", "launch"),
                       fn("p", "launch"), fn("w", "launch"), fn("s", "launch"),
                       lit(MIXED_FP64_RADIUS.get(name, 0.0))))
-        lines.append("     %s, %s," % (fn("g", "warm"), fn("s", "warm")))
         lines.append("     {%s, nullptr}}," % ", ".join(fn(v, "set_coef") for v in "gecpws"))
     lines.append("};")
     lines.append("static const int mbx_num_evaluators = %d;" % len(SPECS))

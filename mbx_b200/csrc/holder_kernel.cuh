@@ -275,18 +275,21 @@ __device__ __forceinline__ long nmer_count(const HolderArgs& A) {
 }
 
 // The polynomial (and its gradient) in the precision mode of the kernel, with
-// a block barrier after every separately compiled piece of the trie.
+// a block barrier after every separately compiled piece of the trie; x and
+// the gradient accumulators in shared memory, [v][thread], at the thread's
+// column (xs, gs).
 template <class T, int MODE, class C>
-__device__ __forceinline__ double run_pip_lock(const C& coef, const double (&x)[T::NVARS], double (&g)[T::NVARS]) {
+__device__ __forceinline__ double run_pip_lock(const C& coef, const double* xs, double* gs) {
     if constexpr (MODE == HM_ENERGY) {
-        return T::pip_e_lock(coef, x);
-    } else if constexpr (MODE == HM_GRAD_FP64) {
-        return T::pip_lock(coef, x, g);
+        return T::template pip_e_lock<T::LOCK_THREADS>(coef, xs);
     } else {
         static_assert(MODE == HM_GRAD_FP64, "unknown mode");
-        return 0.0;
+        return T::template pip_lock<T::LOCK_THREADS>(coef, xs, gs);
     }
 }
+
+// Dynamic shared memory of the lockstep kernels (their x/g columns).
+extern __shared__ __align__(16) unsigned char mbx_dyn_smem[];
 
 // FP64 coefficients copied from constant to shared memory once per block
 // (types with T::SMEM_COEF).
@@ -307,6 +310,9 @@ struct SharedCoef {
 template <class T, class CC, int MODE, bool CUSTOM>
 __global__ void __launch_bounds__(T::LOCK_THREADS, 1) holder_lock_kernel(const HolderArgs A) {
     constexpr bool grads = (MODE == HM_GRAD_FP64);
+    constexpr int L = T::LOCK_THREADS;   // == blockDim.x
+    double* xs = reinterpret_cast<double*>(mbx_dyn_smem) + threadIdx.x;
+    double* gs = xs + T::NVARS * L;      // used in gradient mode only
     __shared__ long s_base;
     __shared__ double s_coef[T::SMEM_COEF ? T::NCOEF : 1];
     if constexpr (T::SMEM_COEF && !CUSTOM) {
@@ -330,27 +336,39 @@ __global__ void __launch_bounds__(T::LOCK_THREADS, 1) holder_lock_kernel(const H
         if (base >= n) break;
         const long t = base + threadIdx.x;
         bool live = t < n;
-        double x[T::NVARS], g[T::NVARS];
+        {
+            double x[T::NVARS];
 #pragma unroll
-        for (int v = 0; v < T::NVARS; ++v) { x[v] = 0.0; g[v] = 0.0; }
-        if (live) {
-            double r[T::NREAL][3];
-            load_nmer<T, false>(A, t, r);
-            double d[3][3], rr[3];
-            if (pair_dists<T>(r, d, rr)) {
-                if (A.e_per) A.e_per[t] = 0.0;
-                live = false;
-            } else {
-                double s[T::NSITES][3];
-                T::sites(r, s);
-                T::vars(s, x);
+            for (int v = 0; v < T::NVARS; ++v) x[v] = 0.0;
+            if (live) {
+                double r[T::NREAL][3];
+                load_nmer<T, false>(A, t, r);
+                double d[3][3], rr[3];
+                if (pair_dists<T>(r, d, rr)) {
+                    if (A.e_per) A.e_per[t] = 0.0;
+                    live = false;
+                } else {
+                    double s[T::NSITES][3];
+                    T::sites(r, s);
+                    T::vars(s, x);
+                }
+            }
+#pragma unroll
+            for (int v = 0; v < T::NVARS; ++v) {
+                xs[v * L] = x[v];
+                if (grads) gs[v * L] = 0.0;
             }
         }
         double ep;
-        if constexpr (CUSTOM) ep = run_pip_lock<T, MODE>(GlobalCoef{A.coef}, x, g);
-        else if constexpr (T::SMEM_COEF) ep = run_pip_lock<T, MODE>(SharedCoef<CC>{s_coef}, x, g);
-        else ep = run_pip_lock<T, MODE>(CC{}, x, g);
-        if (live) finish_nmer<T>(A, t, ep, g, grads, acc);
+        if constexpr (CUSTOM) ep = run_pip_lock<T, MODE>(GlobalCoef{A.coef}, xs, gs);
+        else if constexpr (T::SMEM_COEF) ep = run_pip_lock<T, MODE>(SharedCoef<CC>{s_coef}, xs, gs);
+        else ep = run_pip_lock<T, MODE>(CC{}, xs, gs);
+        if (live) {
+            double g[T::NVARS];
+#pragma unroll
+            for (int v = 0; v < T::NVARS; ++v) g[v] = grads ? gs[v * L] : 0.0;
+            finish_nmer<T>(A, t, ep, g, grads, acc);
+        }
     }
     block_reduce_add<7>(acc, A.out);
 }
@@ -397,6 +415,9 @@ struct SharedPairs {
 
 template <class T, class CC>
 __global__ void __launch_bounds__(T::LOCK_THREADS_S, 1) holder_pair_kernel(const HolderArgs A) {
+    constexpr int L = T::LOCK_THREADS_S;   // == blockDim.x
+    f2_t* xs = reinterpret_cast<f2_t*>(mbx_dyn_smem) + threadIdx.x;
+    f2_t* gs = xs + T::NVARS * L;
     __shared__ long s_base;
     __shared__ f2_t s_coef[T::NORB];
     for (int k = threadIdx.x; k < T::NORB; k += blockDim.x) s_coef[k] = CC{}.f2(k);
@@ -419,7 +440,6 @@ __global__ void __launch_bounds__(T::LOCK_THREADS_S, 1) holder_pair_kernel(const
         }
         if (base >= n) break;
         const long t0 = base + threadIdx.x, t1 = t0 + blockDim.x;
-        f2_t x2[T::NVARS], g2[T::NVARS];
         bool live0, live1;
         {
             float lo[T::NVARS], hi[T::NVARS];
@@ -427,58 +447,24 @@ __global__ void __launch_bounds__(T::LOCK_THREADS_S, 1) holder_pair_kernel(const
             live1 = nmer_vars_f32<T>(A, t1, n, hi);
 #pragma unroll
             for (int v = 0; v < T::NVARS; ++v) {
-                x2[v] = f2_pack(lo[v], hi[v]);
-                g2[v] = 0ull;
+                xs[v * L] = f2_pack(lo[v], hi[v]);
+                gs[v * L] = 0ull;
             }
         }
-        const double2 ep = T::pip_s32_lock(coef, x2, g2);
+        const double2 ep = T::template pip_s32_lock<L>(coef, xs, gs);
         double g[T::NVARS];
         if (live0) {
 #pragma unroll
-            for (int v = 0; v < T::NVARS; ++v) g[v] = (double)f2_lo(g2[v]);
+            for (int v = 0; v < T::NVARS; ++v) g[v] = (double)f2_lo(gs[v * L]);
             finish_nmer<T>(A, t0, coef.b0() + ep.x, g, true, acc);
         }
         if (live1) {
 #pragma unroll
-            for (int v = 0; v < T::NVARS; ++v) g[v] = (double)f2_hi(g2[v]);
+            for (int v = 0; v < T::NVARS; ++v) g[v] = (double)f2_hi(gs[v * L]);
             finish_nmer<T>(A, t1, coef.b0() + ep.y, g, true, acc);
         }
     }
     block_reduce_add<7>(acc, A.out);
-}
-
-// Code warm-up: block k (one warp) runs piece k of the trie once on zero
-// variables, with the same coefficient view as the evaluation kernel, so that
-// the piece's instructions are in L2 when the evaluation reaches it.  Launched
-// beside the n-mer builder.  The result never meets the sink's condition; the
-// store keeps the calls from being removed.
-template <class T, class CC, int MODE>
-__global__ void __launch_bounds__(32) holder_warm_kernel(double* sink) {
-    const int k = blockIdx.x;
-    double e;
-    if constexpr (MODE == HM_GRAD_SHIFT32) {
-        __shared__ f2_t s_pairs[T::NORB];
-        for (int j = threadIdx.x; j < T::NORB; j += blockDim.x) s_pairs[j] = CC{}.f2(j);
-        __syncwarp();
-        f2_t x[T::NVARS], g[T::NVARS];
-#pragma unroll
-        for (int v = 0; v < T::NVARS; ++v) { x[v] = 0ull; g[v] = 0ull; }
-        const double2 r = T::pip_s32_piece(k, SharedPairs<CC>{s_pairs}, x, g);
-        e = r.x + r.y + (double)f2_lo(g[0]);
-    } else {
-        double x[T::NVARS], g[T::NVARS];
-#pragma unroll
-        for (int v = 0; v < T::NVARS; ++v) { x[v] = 0.0; g[v] = 0.0; }
-        if constexpr (T::SMEM_COEF) {
-            __shared__ double s_c[T::NCOEF];
-            for (int j = threadIdx.x; j < T::NCOEF; j += blockDim.x) s_c[j] = CC{}[j];
-            __syncwarp();
-            e = T::pip_piece(k, SharedCoef<CC>{s_c}, x, g) + g[0];
-        } else {
-            e = T::pip_piece(k, CC{}, x, g) + g[0];
-        }
-    }
-    if (e == 1.0e300 && threadIdx.x == 0) sink[0] = e;
 }
 
 // Warp-cooperative evaluation for polynomials too large for straight-line

@@ -24,7 +24,6 @@
 #include "nmer_build.h"
 
 typedef int (*launch_fn)(const HolderArgs&, int, int, cudaStream_t);
-typedef int (*warm_fn)(double* sink, cudaStream_t s);
 typedef int (*dcoef_fn)(const HolderArgs&, const double*, double*, int, int, cudaStream_t);
 typedef int (*poly_fn)(long, const double*, double*, double*, int, int, cudaStream_t);
 typedef int (*warp_fn)(const HolderArgs&, int, int, cudaStream_t);
@@ -44,7 +43,6 @@ struct EvaluatorInfo {
     warp_fn w;
     launch_fn s;      // FP32 kernel of the mixed mode (FP32 basis), or null
     double split_r;   // mixed mode: n-mers with first-atom distance below this run in FP64 (0: none)
-    warm_fn warm_g, warm_s;   // code warm-up launches of the g and s kernels
     setcoef_fn set[7];
 };
 
@@ -151,14 +149,10 @@ struct mbx_ctx {
     // runtime launch shapes of the builder (set by mbx_tune)
     struct Knobs {
         int nb_warps = 4, nb_unroll = 2, tri_threads = 128, dim_threads = 128;
-        int warm = 1;   // code warm-up launch beside the build
     } knobs[4];         // per term (indexed by nbody)
     double* h_out = nullptr;  // pinned: [0..7] term outputs, [8..15] counters
     cudaEvent_t ev[3];
-    // code warm-up of the evaluation kernels, beside the n-mer build
-    cudaStream_t side = nullptr;
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
-    DevBuf<double> warm_sink;
+
 
     // batched configurations: configuration k owns monomers conf_mon[k] ..
     // conf_mon[k+1]-1 and has box conf_bp[k]
@@ -228,10 +222,7 @@ int mbx_create(mbx_ctx** out, int device, void* stream) {
     }
     CUCHK(c, cudaMallocHost(&c->h_out, 64 * sizeof(double)));
     for (int i = 0; i < 3; ++i) CUCHK(c, cudaEventCreate(&c->ev[i]));
-    CUCHK(c, cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
-    CUCHK(c, cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
-    CUCHK(c, cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
-    CUCHK(c, c->warm_sink.ensure(1));
+
     CUCHK(c, c->out.ensure(64));
     CUCHK(c, c->status.ensure(4));
     CUCHK(c, c->counters.ensure(MBX_MAX_BUCKETS));
@@ -283,9 +274,6 @@ int mbx_destroy(mbx_ctx* c) {
     c->conf_out.release();
     if (c->h_out) cudaFreeHost(c->h_out);
     for (int i = 0; i < 3; ++i) cudaEventDestroy(c->ev[i]);
-    if (c->ev_fork) cudaEventDestroy(c->ev_fork);
-    if (c->ev_join) cudaEventDestroy(c->ev_join);
-    if (c->side) cudaStreamDestroy(c->side);
     for (auto& gr : c->graph)
         if (gr.exec) cudaGraphExecDestroy(gr.exec);
     if (c->h_conf) cudaFreeHost(c->h_conf);
@@ -739,32 +727,8 @@ extern "C" int mbx_energy(mbx_ctx* c, int nbody, double* xyz, int use_ghost, dou
             ++kernels;
         }
         const bool mixed = (flags & MBX_MIXED) && grads;
-        // warm the evaluation kernels' code into L2 on the side stream while
-        // the n-mers are built (one warp per trie piece)
-        bool warmed = false;
-        if (grads && c->knobs[nbody].warm) {
-            CUCHK(c, cudaEventRecord(c->ev_fork, c->stream));
-            CUCHK(c, cudaStreamWaitEvent(c->side, c->ev_fork, 0));
-            warm_fn done[2 * MBX_MAX_BUCKETS];
-            int ndone = 0;
-            for (int b = 0; b < c->nbucket[nbody]; ++b) {
-                const EvaluatorInfo* E = c->bucket_eval[nbody][b];
-                if (c->bucket_near[nbody][b] && !mixed) continue;
-                const bool fp32 = mixed && !c->bucket_near[nbody][b] && E->s;
-                warm_fn fn = fp32 ? E->warm_s : E->warm_g;
-                bool seen = false;
-                for (int i = 0; i < ndone; ++i) seen = seen || done[i] == fn;
-                if (!fn || seen) continue;
-                done[ndone++] = fn;
-                RCHK(c, fn(c->warm_sink.p, c->side));
-                ++kernels;
-            }
-            CUCHK(c, cudaEventRecord(c->ev_join, c->side));
-            warmed = true;
-        }
         int r = launch_build(c, nbody, use_ghost, X, 0, &kernels, mixed);
         if (r) return r;
-        if (warmed) CUCHK(c, cudaStreamWaitEvent(c->stream, c->ev_join, 0));
         CUCHK(c, cudaEventRecord(c->ev[1], c->stream));
         double* G = nullptr;
         if (grads) {
@@ -982,10 +946,12 @@ extern "C" int mbx_evaluate(mbx_ctx* c, const char* name, long n, const double* 
     A.out = c->out.p;
     A.e_per = EP;
     int kernels = 0;
+    CUCHK(c, cudaEventRecord(c->ev[1], c->stream));
     if (n > 0) {
         r = launch_eval(c, E, A, grads ? (flags & MBX_MIXED) : (flags | MBX_NO_GRADS), &kernels);
         if (r) return r;
     }
+    CUCHK(c, cudaEventRecord(c->ev[2], c->stream));
     CUCHK(c, cudaMemcpyAsync(c->h_out, c->out.p, 8 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     std::vector<double> gt, et;
     if (grads && !dev) {
@@ -996,6 +962,9 @@ extern "C" int mbx_evaluate(mbx_ctx* c, const char* name, long n, const double* 
     CUCHK(c, cudaStreamSynchronize(c->stream));
     if (grads && !dev)
         for (size_t i = 0; i < nx; ++i) grad[i] += gt[i];
+    c->last_ms_build = 0;
+    cudaEventElapsedTime(&c->last_ms_eval, c->ev[1], c->ev[2]);
+    c->last_kernels = kernels;
     if (energy) *energy = c->h_out[0];
     if (virial) {
         virial[0] += c->h_out[1];
@@ -1149,9 +1118,8 @@ extern "C" int mbx_set_batch(mbx_ctx* c, int nconf, const int* conf_mon, const d
 
 // Everything one batched term does on the device, without a host
 // synchronisation (so that it can be captured into a graph): wrap every
-// configuration, warm the evaluation code, build every configuration's
-// n-mers, evaluate every bucket once, copy the per-configuration sums and the
-// status back to pinned memory.
+// configuration, build every configuration's n-mers, evaluate every bucket
+// once, copy the per-configuration sums and the status back to pinned memory.
 static int batch_sequence(mbx_ctx* c, int nbody, double* X, double* G, bool grads, bool mixed, int* kernels) {
     for (int k = 0; k < c->nconf; ++k) {
         const int b = c->conf_mon[k], n = c->conf_mon[k + 1] - b;
@@ -1160,26 +1128,6 @@ static int batch_sequence(mbx_ctx* c, int nbody, double* X, double* G, bool grad
                                                                    c->conf_bp[k]);
             ++*kernels;
         }
-    }
-    bool warmed = false;
-    if (grads && c->knobs[nbody].warm) {
-        CUCHK(c, cudaEventRecord(c->ev_fork, c->stream));
-        CUCHK(c, cudaStreamWaitEvent(c->side, c->ev_fork, 0));
-        warm_fn done[MBX_MAX_BUCKETS];
-        int ndone = 0;
-        for (int b = 0; b < c->nbucket[nbody]; ++b) {
-            const EvaluatorInfo* E = c->bucket_eval[nbody][b];
-            if (c->bucket_near[nbody][b] && !mixed) continue;
-            warm_fn fn = (mixed && !c->bucket_near[nbody][b] && E->s) ? E->warm_s : E->warm_g;
-            bool seen = false;
-            for (int i = 0; i < ndone; ++i) seen = seen || done[i] == fn;
-            if (!fn || seen) continue;
-            done[ndone++] = fn;
-            RCHK(c, fn(c->warm_sink.p, c->side));
-            ++*kernels;
-        }
-        CUCHK(c, cudaEventRecord(c->ev_join, c->side));
-        warmed = true;
     }
     int r = prepare_buckets(c, nbody, c->nmon, 0);
     if (r) return r;
@@ -1191,7 +1139,6 @@ static int batch_sequence(mbx_ctx* c, int nbody, double* X, double* G, bool grad
         r = launch_build_scope(c, nbody, S, X, 0, kernels, mixed);
         if (r) return r;
     }
-    if (warmed) CUCHK(c, cudaStreamWaitEvent(c->stream, c->ev_join, 0));
     CUCHK(c, cudaMemsetAsync(c->conf_out.p, 0, 8 * (size_t)c->nconf * sizeof(double), c->stream));
     CUCHK(c, cudaMemsetAsync(c->out.p, 0, 16 * sizeof(double), c->stream));
     CUCHK(c, cudaMemsetAsync(c->counters.p, 0, MBX_MAX_BUCKETS * sizeof(int), c->stream));
@@ -1337,8 +1284,8 @@ extern "C" int mbx_batch_energy(mbx_ctx* c, int nbody, double* xyz, double* grad
 // caller's batch (or the whole system when no batch is set): coordinate
 // descent over the warps per neighbour query and its unroll depth, the
 // threads of the trimer pair loop ("trimers per block") and of the dimer
-// rules, and the code warm-up.  out[5] (optional) receives the choice:
-// nb_warps, nb_unroll, tri_threads, dim_threads, warm; *best_ms the time.
+// rules.  out[4] (optional) receives the choice: nb_warps, nb_unroll,
+// tri_threads, dim_threads; *best_ms the time.
 extern "C" int mbx_tune(mbx_ctx* c, int nbody, double* xyz, double* grad, int flags, int* out, double* best_ms) {
     if (!c || (nbody != 2 && nbody != 3) || !xyz) return fail(c, MBX_EINVAL, "bad arguments");
     if (!(flags & MBX_DEVICE_PTRS)) return fail(c, MBX_EINVAL, "tuning takes device arrays (MBX_DEVICE_PTRS)");
@@ -1362,7 +1309,7 @@ extern "C" int mbx_tune(mbx_ctx* c, int nbody, double* xyz, double* grad, int fl
     int rc = time_once(&cur);
     if (rc) return rc;
     struct Axis { int* field; std::vector<int> values; };
-    std::vector<Axis> axes = {{&K.nb_warps, {4, 1}}, {&K.nb_unroll, {1, 2, 4}}, {&K.warm, {1, 0}}};
+    std::vector<Axis> axes = {{&K.nb_warps, {4, 1}}, {&K.nb_unroll, {1, 2, 4}}};
     if (nbody == 3) axes.push_back({&K.tri_threads, {64, 128, 256}});
     else axes.push_back({&K.dim_threads, {64, 128, 256}});
     for (auto& ax : axes) {
@@ -1390,7 +1337,6 @@ extern "C" int mbx_tune(mbx_ctx* c, int nbody, double* xyz, double* grad, int fl
         out[1] = K.nb_unroll;
         out[2] = K.tri_threads;
         out[3] = K.dim_threads;
-        out[4] = K.warm;
     }
     if (best_ms) *best_ms = cur;
     return MBX_OK;
@@ -1403,6 +1349,19 @@ extern "C" int mbx_get_knobs(const mbx_ctx* c, int nbody, int* out) {
     out[1] = K.nb_unroll;
     out[2] = K.tri_threads;
     out[3] = K.dim_threads;
-    out[4] = K.warm;
+    return MBX_OK;
+}
+
+extern "C" int mbx_set_knobs(mbx_ctx* c, int nbody, const int* in) {
+    if (!c || (nbody != 2 && nbody != 3) || !in) return fail(c, MBX_EINVAL, "bad arguments");
+    const bool ok = (in[0] == 1 || in[0] == 4) && (in[1] == 1 || in[1] == 2 || in[1] == 4) &&
+                    (in[2] == 64 || in[2] == 128 || in[2] == 256) && (in[3] == 64 || in[3] == 128 || in[3] == 256);
+    if (!ok) return fail(c, MBX_EINVAL, "launch shape out of range");
+    auto& K = c->knobs[nbody];
+    K.nb_warps = in[0];
+    K.nb_unroll = in[1];
+    K.tri_threads = in[2];
+    K.dim_threads = in[3];
+    drop_graphs(c);
     return MBX_OK;
 }
