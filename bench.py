@@ -182,7 +182,7 @@ def run_reference(args, rank):
     return 0
 
 
-def batched_leg(args, local, flush, fp64_value):
+def batched_leg(args, local, flush, fp64_value, dist=None, world=1):
     """32 beads of the 2048-water box (sigma 0.05 A) + 64 gas-phase clusters of
     8-512 molecules: mixed precision, builder shapes autotuned, the whole 2b+3b
     device sequence replayed from CUDA graphs; errors against the FP64
@@ -227,13 +227,14 @@ def batched_leg(args, local, flush, fp64_value):
         torch.cuda.synchronize()
         times.append(ms2 + ms3)
         emx = t0 + t1
-    ms = sum(times) / len(times)
+    from mbx_b200 import replicas
+    ms, = replicas.max_over_ranks([sum(times) / len(times)], dist, "cuda")
     units = listed2 + listed3
     rel = np.abs(emx - e64) / np.abs(e64)
     return {"workload": "32 beads of the 2048-H2O box (Gaussian sigma 0.05 A per atom) + 64 gas-phase water "
                         "clusters of 8-512 molecules at 0.0334 /A^3, seed 0; cutoffs 9/7 A",
             "configurations": len(cfgs), "molecules": int(sum(len(c[0]) for c in cfgs)),
-            "value": units / (ms * 1e-3), "unit": "n-mers/s", "ms_per_step": ms,
+            "value": replicas.throughput(units, ms, world), "unit": "n-mers/s", "ms_per_step": ms,
             "units_per_step": {"dimers": listed2, "trimers": listed3, "evaluated_dimers": eval2,
                                "evaluated_trimers": eval3},
             "dtype": "mixed (3b paired f32 over a shifted basis; 2b f64)", "cuda_graph": True,
@@ -241,7 +242,7 @@ def batched_leg(args, local, flush, fp64_value):
                       "L2 flushed before each step",
             "autotuned": tuned,
             "max_rel_err_E_per_configuration": float(rel.max()),
-            "speedup_vs_fp64_plain": (units / (ms * 1e-3)) / fp64_value}
+            "speedup_vs_fp64_plain": replicas.throughput(units, ms, world) / fp64_value}
 
 
 def main():
@@ -261,7 +262,7 @@ def main():
         return run_reference(args, rank)
 
     import torch
-    from mbx_b200 import capi, system as msys
+    from mbx_b200 import capi, replicas, system as msys
     from mbx_b200.tables import load_fit  # noqa: F401
 
     torch.cuda.set_device(local)
@@ -341,11 +342,8 @@ def main():
 
     ms = sum(t64) / len(t64)
     ms_mx = sum(tmx) / len(tmx)
-    if dist:
-        tt = torch.tensor([ms, ms_mx], dtype=torch.float64, device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms, ms_mx = tt.tolist()
-    value = world * units / (ms * 1e-3)
+    ms, ms_mx = replicas.max_over_ranks([ms, ms_mx], dist, "cuda")
+    value = replicas.throughput(units, ms, world)
 
     # ---------------- end to end through the public API (host buffers)
     sys_h = msys.from_arrays(ids, xyz, box, CUT2, CUT3, context=ctx)
@@ -367,10 +365,7 @@ def main():
         g3 = sys_h.GetRealGrads()
         e2e_t.append(time.perf_counter() - t0)
     e2e_ms = 1e3 * sum(e2e_t) / len(e2e_t)
-    if dist:
-        tt = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_ms = tt.item()
+    e2e_ms, = replicas.max_over_ranks([e2e_ms], dist, "cuda")
     nbytes = 8 * sys_h.sites.size
     h2d = 2 * nbytes
     d2h = 2 * (2 * nbytes + 8 * 8)
@@ -418,7 +413,7 @@ def main():
                                        "peak": peaks["fp32_tflops"], "frac": amx / peaks["fp32_tflops"],
                                        "bound": "fp32-fma"}
     if not args.no_batch:
-        out["batched"] = batched_leg(args, local, flush, value)
+        out["batched"] = batched_leg(args, local, flush, value, dist, world)
     if rank == 0 and not args.no_cpu_baseline:
         cb = ref_cpu(ids, xyz, box)
         if cb:
