@@ -108,6 +108,27 @@ void sorted_slots(int nb, const std::string* ids, int* idx) {
 
 }  // namespace
 
+// Scratch of one n-mer search (cloud, cell list, matches).  A context owns
+// several, so that the searches of a batch's configurations can run side by
+// side on their own streams.
+struct BuildScratch {
+    DevBuf<double> cloud;
+    DevBuf<int> cell_of, cell_count, cell_start, cell_fill, cell_items, cell_sorted, nb_count;
+    DevBuf<NbEntry> nb;
+    void release() {
+        cloud.release();
+        cell_of.release();
+        cell_count.release();
+        cell_start.release();
+        cell_fill.release();
+        cell_items.release();
+        cell_sorted.release();
+        nb_count.release();
+        nb.release();
+    }
+};
+#define MBX_BUILD_LANES 4   // concurrent searches of a batch (streams + scratch sets)
+
 struct mbx_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -137,10 +158,11 @@ struct mbx_ctx {
     long bucket_cap[4][MBX_MAX_BUCKETS];
 
     // work buffers
-    DevBuf<double> xyz, grad, out, cloud, coef_ws;
-    DevBuf<int> cell_of, cell_count, cell_start, cell_fill, cell_items, cell_sorted, nb_count, bucket_count, status,
-        counters;
-    DevBuf<NbEntry> nb;
+    DevBuf<double> xyz, grad, out, coef_ws;
+    DevBuf<int> bucket_count, status, counters;
+    BuildScratch scratch[MBX_BUILD_LANES];   // [0]: every single-system search
+    cudaStream_t lane_stream[MBX_BUILD_LANES] = {nullptr};   // [0] unused (the context stream)
+    cudaEvent_t lane_fork = nullptr, lane_join[MBX_BUILD_LANES] = {nullptr};
     DevBuf<int4> buckets, list;
     DevBuf<unsigned long long> listed;
     DevBuf<int4> terms;
@@ -222,6 +244,11 @@ int mbx_create(mbx_ctx** out, int device, void* stream) {
     }
     CUCHK(c, cudaMallocHost(&c->h_out, 64 * sizeof(double)));
     for (int i = 0; i < 3; ++i) CUCHK(c, cudaEventCreate(&c->ev[i]));
+    CUCHK(c, cudaEventCreateWithFlags(&c->lane_fork, cudaEventDisableTiming));
+    for (int i = 1; i < MBX_BUILD_LANES; ++i) {
+        CUCHK(c, cudaStreamCreateWithFlags(&c->lane_stream[i], cudaStreamNonBlocking));
+        CUCHK(c, cudaEventCreateWithFlags(&c->lane_join[i], cudaEventDisableTiming));
+    }
 
     CUCHK(c, c->out.ensure(64));
     CUCHK(c, c->status.ensure(4));
@@ -258,13 +285,16 @@ int mbx_destroy(mbx_ctx* c) {
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
     DevBuf<int>* ib[] = {&c->d_first, &c->d_nat, &c->d_tag, &c->d_type, &c->d_members[0], &c->d_members[1],
-                         &c->d_query[0], &c->d_query[1], &c->cell_of, &c->cell_count, &c->cell_start,
-                         &c->cell_fill, &c->cell_items, &c->cell_sorted, &c->nb_count, &c->bucket_count,
-                         &c->status, &c->counters};
+                         &c->d_query[0], &c->d_query[1], &c->bucket_count, &c->status, &c->counters};
     for (auto* b : ib) b->release();
-    DevBuf<double>* db[] = {&c->xyz, &c->grad, &c->out, &c->cloud, &c->coef_ws, &c->tcoef, &c->warp_coef};
+    DevBuf<double>* db[] = {&c->xyz, &c->grad, &c->out, &c->coef_ws, &c->tcoef, &c->warp_coef};
     for (auto* b : db) b->release();
-    c->nb.release();
+    for (auto& sc : c->scratch) sc.release();
+    for (int i = 1; i < MBX_BUILD_LANES; ++i) {
+        if (c->lane_stream[i]) cudaStreamDestroy(c->lane_stream[i]);
+        if (c->lane_join[i]) cudaEventDestroy(c->lane_join[i]);
+    }
+    if (c->lane_fork) cudaEventDestroy(c->lane_fork);
     c->buckets.release();
     c->list.release();
     c->listed.release();
@@ -599,46 +629,48 @@ struct BuildScope {
 // the counters are zeroed by prepare_buckets) and, when list_cap > 0, into
 // c->list.  Asynchronous; status and counts on device.
 static int launch_build_scope(mbx_ctx* c, int nbody, const BuildScope& S, const double* xyz, long list_cap,
-                              int* kernels, bool mixed) {
+                              int* kernels, bool mixed, int lane = 0) {
+    BuildScratch& B = c->scratch[lane];
+    cudaStream_t st = lane ? c->lane_stream[lane] : c->stream;
     const int nmem = S.nmem, nq = S.nq;
     if (nmem < 2 || (nbody == 3 && nmem < 3) || nq == 0) return MBX_OK;
     const double rc = c->cutoff[nbody];
     const double rc2 = rc * rc;
     CellGrid cg = make_grid(S.bp, rc, nmem);
     const int ncell = cg.n[0] * cg.n[1] * cg.n[2];
-    CUCHK(c, c->cloud.ensure((size_t)std::max(nmem, 1) * 24));
-    CUCHK(c, c->cell_of.ensure(std::max(nmem, 1)));
-    CUCHK(c, c->cell_items.ensure(std::max(nmem, 1)));
-    CUCHK(c, c->cell_sorted.ensure(std::max(nmem, 1)));
-    CUCHK(c, c->cell_count.ensure(ncell + 1));
-    CUCHK(c, c->cell_start.ensure(ncell + 1));
-    CUCHK(c, c->cell_fill.ensure(ncell + 1));
-    CUCHK(c, c->nb_count.ensure(std::max(nq, 1)));
-    CUCHK(c, c->nb.ensure((size_t)std::max(nq, 1) * c->nb_cap));
-    CUCHK(c, cudaMemsetAsync(c->cell_count.p, 0, (ncell + 1) * sizeof(int), c->stream));
+    CUCHK(c, B.cloud.ensure((size_t)std::max(nmem, 1) * 24));
+    CUCHK(c, B.cell_of.ensure(std::max(nmem, 1)));
+    CUCHK(c, B.cell_items.ensure(std::max(nmem, 1)));
+    CUCHK(c, B.cell_sorted.ensure(std::max(nmem, 1)));
+    CUCHK(c, B.cell_count.ensure(ncell + 1));
+    CUCHK(c, B.cell_start.ensure(ncell + 1));
+    CUCHK(c, B.cell_fill.ensure(ncell + 1));
+    CUCHK(c, B.nb_count.ensure(std::max(nq, 1)));
+    CUCHK(c, B.nb.ensure((size_t)std::max(nq, 1) * c->nb_cap));
+    CUCHK(c, cudaMemsetAsync(B.cell_count.p, 0, (ncell + 1) * sizeof(int), st));
     const int T = 128;
-    k_cloud<<<(nmem + T - 1) / T, T, 0, c->stream>>>(xyz, c->d_first.p, S.members, nmem, S.bp, cg, c->cloud.p,
-                                                     c->cell_of.p);
-    k_cell_count<<<(nmem + T - 1) / T, T, 0, c->stream>>>(c->cell_of.p, nmem, c->cell_count.p);
-    k_cell_scan<<<1, 1024, 0, c->stream>>>(c->cell_count.p, ncell, c->cell_start.p, c->cell_fill.p);
-    k_cell_fill<<<(nmem + T - 1) / T, T, 0, c->stream>>>(c->cell_of.p, nmem, c->cell_fill.p, c->cell_items.p);
-    k_cell_sort<<<(ncell * 32 + T - 1) / T, T, 0, c->stream>>>(c->cell_start.p, ncell, c->cell_items.p,
-                                                                c->cell_sorted.p);
+    k_cloud<<<(nmem + T - 1) / T, T, 0, st>>>(xyz, c->d_first.p, S.members, nmem, S.bp, cg, B.cloud.p,
+                                                     B.cell_of.p);
+    k_cell_count<<<(nmem + T - 1) / T, T, 0, st>>>(B.cell_of.p, nmem, B.cell_count.p);
+    k_cell_scan<<<1, 1024, 0, st>>>(B.cell_count.p, ncell, B.cell_start.p, B.cell_fill.p);
+    k_cell_fill<<<(nmem + T - 1) / T, T, 0, st>>>(B.cell_of.p, nmem, B.cell_fill.p, B.cell_items.p);
+    k_cell_sort<<<(ncell * 32 + T - 1) / T, T, 0, st>>>(B.cell_start.p, ncell, B.cell_items.p,
+                                                                B.cell_sorted.p);
     // neighbour search: warps per query and unroll depth are tunable; one
     // warp when four staging areas would not fit in shared memory
     const auto& K = c->knobs[nbody];
     const int nbw = (size_t)4 * c->nb_cap * sizeof(NbEntry) <= 160 * 1024 ? K.nb_warps : 1;
     if ((size_t)c->nb_cap * sizeof(NbEntry) > 227 * 1024) return fail(c, MBX_ENOMEM, "neighbour staging");
-    RCHK(c, launch_neighbors(nbw, K.nb_unroll, c->cloud.p, c->cell_of.p, c->cell_start.p, c->cell_sorted.p,
-                             S.query, nq, cg, S.bp.use_pbc, rc2, c->nb_cap, c->nb_count.p, c->nb.p, c->status.p,
-                             c->stream));
+    RCHK(c, launch_neighbors(nbw, K.nb_unroll, B.cloud.p, B.cell_of.p, B.cell_start.p, B.cell_sorted.p,
+                             S.query, nq, cg, S.bp.use_pbc, rc2, c->nb_cap, B.nb_count.p, B.nb.p, c->status.p,
+                             st));
     if (nbody == 2) {
         DimerRules R = c->drules;
         if (!mixed)
             for (int b = 0; b < MBX_MAX_BUCKETS; ++b) R.split2[b] = 0.0;   // no short-range split
         const int DT = K.dim_threads;
-        k_dimers<<<(int)(((long)nq * 32 + DT - 1) / DT), DT, 0, c->stream>>>(
-            S.query, nq, S.members, c->d_tag.p, c->d_type.p, c->nb_count.p, c->nb.p, c->nb_cap, rc2, R, c->listed.p,
+        k_dimers<<<(int)(((long)nq * 32 + DT - 1) / DT), DT, 0, st>>>(
+            S.query, nq, S.members, c->d_tag.p, c->d_type.p, B.nb_count.p, B.nb.p, c->nb_cap, rc2, R, c->listed.p,
             list_cap > 0 ? c->list.p : nullptr, list_cap, c->buckets.p, c->bucket_count.p, c->status.p);
     } else {
         // a block per query (tunable threads); its matches staged in shared memory
@@ -646,8 +678,8 @@ static int launch_build_scope(mbx_ctx* c, int nbody, const BuildScope& S, const 
         if (smem > 227 * 1024) return fail(c, MBX_ENOMEM, "trimer staging exceeds shared memory");
         if (smem > 48 * 1024)
             CUCHK(c, cudaFuncSetAttribute(k_trimers, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_trimers<<<nq, K.tri_threads, smem, c->stream>>>(
-            S.query, nq, S.members, c->d_tag.p, c->d_type.p, c->cloud.p, c->nb_count.p, c->nb.p, c->nb_cap, rc2,
+        k_trimers<<<nq, K.tri_threads, smem, st>>>(
+            S.query, nq, S.members, c->d_tag.p, c->d_type.p, B.cloud.p, B.nb_count.p, B.nb.p, c->nb_cap, rc2,
             c->trules, c->listed.p, list_cap > 0 ? c->list.p : nullptr, list_cap, c->buckets.p, c->bucket_count.p,
             c->status.p);
     }
@@ -1131,13 +1163,23 @@ static int batch_sequence(mbx_ctx* c, int nbody, double* X, double* G, bool grad
     }
     int r = prepare_buckets(c, nbody, c->nmon, 0);
     if (r) return r;
+    // the configurations' searches on MBX_BUILD_LANES streams (each with its
+    // own scratch; configuration k on lane k mod lanes), joined before the
+    // evaluation; they append to the same buckets through atomics
+    const int lanes = std::min(MBX_BUILD_LANES, c->nconf);
+    CUCHK(c, cudaEventRecord(c->lane_fork, c->stream));
+    for (int l = 1; l < lanes; ++l) CUCHK(c, cudaStreamWaitEvent(c->lane_stream[l], c->lane_fork, 0));
     for (int k = 0; k < c->nconf; ++k) {
         const int b = c->conf_mon[k], n = c->conf_mon[k + 1] - b;
         // members: global ids b..b+n-1 (the identity list of the all-local
         // topology, offset); queries: positions 0..n-1 in it
         BuildScope S{c->d_members[0].p + b, n, c->d_members[0].p, n, c->conf_bp[k]};
-        r = launch_build_scope(c, nbody, S, X, 0, kernels, mixed);
+        r = launch_build_scope(c, nbody, S, X, 0, kernels, mixed, k % lanes);
         if (r) return r;
+    }
+    for (int l = 1; l < lanes; ++l) {
+        CUCHK(c, cudaEventRecord(c->lane_join[l], c->lane_stream[l]));
+        CUCHK(c, cudaStreamWaitEvent(c->stream, c->lane_join[l], 0));
     }
     CUCHK(c, cudaMemsetAsync(c->conf_out.p, 0, 8 * (size_t)c->nconf * sizeof(double), c->stream));
     CUCHK(c, cudaMemsetAsync(c->out.p, 0, 16 * sizeof(double), c->stream));
