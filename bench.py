@@ -1,22 +1,25 @@
 #!/usr/bin/env python3
 """Throughput of the 2-body + 3-body path: dimers+trimers/s with forces, 2048 H2O.
 
-One step = one TwoBodyEnergy + one ThreeBodyEnergy (System::Get2B + Get3B) of
-the 2048-water box (cubic 39.44 A, 2b cutoff 9 A, 3b cutoff 7 A, seed 0):
-FixMonomerCoordinates, the n-mer search, every evaluator with energies,
-gradients and virial.  Units = listed n-mers (dimers within 9 A + trimers by
-the reference's AddClusters rule within 7 A), the reference's unit of work.
+One step = one Get2B + one Get3B of the 2048-water box (cubic 39.44 A, 2b
+cutoff 9 A, 3b cutoff 7 A, seed 0): FixMonomerCoordinates, the n-mer search,
+every evaluator with energies, gradients and virial, both terms in one call
+(mbx_energy_2b3b: the two terms side by side on the GPU).  Units = listed
+n-mers (dimers within 9 A + trimers by the reference's AddClusters rule within
+7 A), the reference's unit of work.
 
 * value: device-resident (coordinates and gradients in HBM), CUDA events on
   the library's stream, L2 flushed between steps (inputs are far smaller than
   the 126 MB L2), FP64 path;
-* e2e: the same through the public API (mbx_b200.system.System) with pinned
-  host buffers, host<->device copies inside, wall clock per step;
+* e2e: the same through the public API (mbx_b200.system.System,
+  TwoAndThreeBodyEnergy) with pinned host buffers, host<->device copies
+  inside, wall clock per step;
 * mixed: the FP32-monomial / FP64-accumulate path, its throughput and its
   energy error against the FP64 path;
-* roofline: the MB-pol 3b evaluation kernel, algorithmic flops counted from
-  the reference's gradient program (mbx_b200/data/flops.json) over its
-  CUDA-event duration, against the measured FP64 FMA peak of this GPU;
+* roofline: the MB-pol 3b evaluation kernel launched alone (3b-only calls,
+  L2 flushed), algorithmic flops counted from the reference's gradient
+  program (mbx_b200/data/flops.json) over its CUDA-event duration, against
+  the measured FP64 FMA peak of this GPU;
 * cpu_baseline: the reference's own CPU path (oracle/_ref, built from the
   reference sources) on the host's cores, bounded sample.
 
@@ -286,12 +289,10 @@ def main():
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
 
     def step(mixed=False):
+        # Get2B + Get3B: both terms in one call, side by side on the GPU
         grad.zero_()
-        e2 = ctx.energy(2, sites, grad, vir, mixed=mixed)
-        ms2 = ctx.timing()
-        e3 = ctx.energy(3, sites, grad, vir, mixed=mixed)
-        ms3 = ctx.timing()
-        return e2, e3, ms2, ms3
+        e2, e3 = ctx.energy_2b3b(sites, grad, vir, mixed=mixed)
+        return e2, e3, ctx.timing()
 
     for _ in range(max(args.warmup, 3)):
         step()
@@ -300,7 +301,7 @@ def main():
     units = listed2 + listed3
 
     def timed(mixed):
-        times, evals, launches, energies = [], [], 0, None
+        times, launches, energies = [], 0, None
         for _ in range(args.steps):
             flush.zero_()
             if dist:
@@ -309,27 +310,42 @@ def main():
             a = torch.cuda.Event(enable_timing=True)
             b = torch.cuda.Event(enable_timing=True)
             a.record(stream)
-            e2, e3, ms2, ms3 = step(mixed)
+            e2, e3, tm = step(mixed)
             b.record(stream)
             torch.cuda.synchronize()
             times.append(a.elapsed_time(b))
-            evals.append(ms3[1])
-            launches += ms2[2] + ms3[2]
+            launches += tm[2]
             energies = (e2, e3)
-        return times, evals, launches, energies
+        return times, launches, energies
+
+    def kernel_3b(mixed, steps):
+        """Duration of the 3b evaluation kernel launched alone (CUDA events
+        on the library's stream), L2 flushed before each call."""
+        evs = []
+        for _ in range(steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            grad.zero_()
+            ctx.energy(3, sites, grad, vir, mixed=mixed)
+            evs.append(ctx.timing()[1])
+        return evs
 
     with Clocks(local) as clk:
         clk.wait_first(step)
         t_begin = time.monotonic()
-        t64, ev64, launches, (e2_64, e3_64) = timed(False)
+        t64, launches, (e2_64, e3_64) = timed(False)
         clk.window = (t_begin, time.monotonic())
     clocks = clk.summary()
     g64 = grad.cpu().numpy()
+    ev64 = kernel_3b(False, max(3, min(args.steps, 20)))
     if not args.no_mixed:
         for _ in range(max(args.warmup, 3)):
             step(True)
-        tmx, evmx, launches_mx, (e2_mx, e3_mx) = timed(True)
+        tmx, launches_mx, (e2_mx, e3_mx) = timed(True)
+        grad.zero_()
+        ctx.energy_2b3b(sites, grad, vir, mixed=True)
         gmx = grad.cpu().numpy()
+        evmx = kernel_3b(True, max(3, min(args.steps, 20)))
         # per-term forces of the two paths (2b and 3b gradients separately)
         grad.zero_()
         ctx.energy(2, sites, grad, vir)
@@ -352,23 +368,20 @@ def main():
     sys_h.sites = pinned_sites.numpy()
     sys_h.grad = pinned_grad.numpy()
     for _ in range(max(args.warmup, 3)):
-        sys_h.TwoBodyEnergy(True)
-        sys_h.ThreeBodyEnergy(True)
+        sys_h.TwoAndThreeBodyEnergy(True)
     e2e_t = []
     for _ in range(args.steps):
         flush.zero_()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        sys_h.TwoBodyEnergy(True)
-        g2 = sys_h.GetRealGrads()
-        sys_h.ThreeBodyEnergy(True)
-        g3 = sys_h.GetRealGrads()
+        sys_h.TwoAndThreeBodyEnergy(True)
+        g23 = sys_h.GetRealGrads()
         e2e_t.append(time.perf_counter() - t0)
     e2e_ms = 1e3 * sum(e2e_t) / len(e2e_t)
     e2e_ms, = replicas.max_over_ranks([e2e_ms], dist, "cuda")
     nbytes = 8 * sys_h.sites.size
-    h2d = 2 * nbytes
-    d2h = 2 * (2 * nbytes + 8 * 8)
+    h2d = nbytes                     # the coordinates, once per step
+    d2h = 2 * nbytes + 2 * 8 * 8     # wrapped coordinates + gradient; both terms' results
 
     # ---------------- roofline of the MB-pol 3b evaluation kernel
     kern_ms = sum(ev64) / len(ev64)
@@ -390,7 +403,8 @@ def main():
                               "evaluated_trimers": eval3},
            "energies": {"E2B": e2_64, "E3B": e3_64},
            "e2e": {"value": world * units / (e2e_ms * 1e-3), "unit": "n-mers/s", "h2d_bytes_per_step": h2d,
-                   "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms, "api": "mbx_b200.system.System"},
+                   "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
+                   "api": "mbx_b200.system.System.TwoAndThreeBodyEnergy (mbx_energy_2b3b, host arrays)"},
            "gpu_launches": launches, "roofline": roofline, "clocks": clocks,
            "fma_peaks_tflops": peaks}
     if not args.no_mixed:

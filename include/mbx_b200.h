@@ -116,6 +116,17 @@ int mbx_evaluator_info(const char* evaluator, int* nbody, int* nreal, int* nvars
  * and evaluation, and the number of kernels it launched. */
 int mbx_last_timing(const mbx_ctx* ctx, double* ms_build, double* ms_eval, int* kernels);
 
+/* Both terms in one call (no counterpart in the reference, whose
+ * System::Energy calls Get2B and Get3B one after the other): the coordinates
+ * are wrapped once, then the 2b and the 3b term run side by side on two
+ * streams (the 2b term on a child context with its own buffers), so that
+ * each fills the SMs the other leaves idle.  Arguments as for mbx_energy;
+ * *e2 and *e3 receive the term energies, grad and virial the sum of both
+ * terms (+=).  mbx_last_counts gives both terms' counts afterwards;
+ * mbx_last_timing the 3b term's. */
+int mbx_energy_2b3b(mbx_ctx* ctx, double* xyz, int use_ghost, double* e2, double* e3, double* grad, double* virial,
+                    int flags);
+
 /* Batched configurations.  No counterpart in the reference (MBX evaluates
  * one bblock::System per call); for path-integral beads, cluster sets and
  * other independent configurations evaluated together.  The topology given

@@ -47,6 +47,8 @@ def lib():
     L.mbx_energy.argtypes = [vp, ctypes.c_int, dp, ctypes.c_int, ctypes.POINTER(ctypes.c_double), dp, dp,
                              ctypes.c_int]
     L.mbx_last_counts.argtypes = [vp, ctypes.c_int, lp, lp]
+    L.mbx_energy_2b3b.argtypes = [vp, dp, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                  ctypes.POINTER(ctypes.c_double), dp, dp, ctypes.c_int]
     L.mbx_nmers.argtypes = [vp, ctypes.c_int, ctypes.c_double, dp, ctypes.c_int, lp, ctypes.c_long, lp]
     L.mbx_evaluate.argtypes = [vp, ctypes.c_char_p, ctypes.c_long, dp, dp, dp, dp, ctypes.POINTER(ctypes.c_double),
                                ctypes.c_int]
@@ -69,7 +71,7 @@ def lib():
 EXPORTED = ("mbx_create", "mbx_destroy", "mbx_last_error", "mbx_version", "mbx_set_topology", "mbx_set_config",
             "mbx_energy", "mbx_last_counts", "mbx_nmers", "mbx_evaluate", "mbx_evaluate_dcoef", "mbx_poly",
             "mbx_set_coefficients", "mbx_evaluator_info", "mbx_last_timing", "mbx_fma_peaks", "mbx_set_batch",
-            "mbx_batch_energy", "mbx_tune", "mbx_get_knobs", "mbx_set_knobs")
+            "mbx_batch_energy", "mbx_tune", "mbx_get_knobs", "mbx_set_knobs", "mbx_energy_2b3b")
 
 KNOBS = ("nb_warps", "nb_unroll", "tri_threads", "dim_threads")
 
@@ -165,6 +167,21 @@ class Context:
         e = ctypes.c_double()
         self._check(lib().mbx_energy(self.h, nbody, px, int(use_ghost), ctypes.byref(e), pg, pv, flags))
         return e.value
+
+    def energy_2b3b(self, xyz, grad=None, virial=None, use_ghost=False, mixed=False, grads=True):
+        """Get2B and Get3B side by side on the GPU; returns (E2B, E3B)."""
+        px, dx = _ptr(xyz)
+        pg, dg = _ptr(grad)
+        pv, _ = _ptr(virial)
+        flags = (MBX_DEVICE_PTRS if dx else 0) | (MBX_MIXED if mixed else 0) | (0 if grads else MBX_NO_GRADS)
+        if grad is not None and bool(dg) != bool(dx):
+            raise TypeError("xyz and grad must both be host or both be device arrays")
+        if virial is not None and not isinstance(virial, np.ndarray):
+            raise TypeError("virial is a host numpy array")
+        e2, e3 = ctypes.c_double(), ctypes.c_double()
+        self._check(lib().mbx_energy_2b3b(self.h, px, int(use_ghost), ctypes.byref(e2), ctypes.byref(e3), pg, pv,
+                                          flags))
+        return e2.value, e3.value
 
     def counts(self, nbody):
         a, b = ctypes.c_long(), ctypes.c_long()

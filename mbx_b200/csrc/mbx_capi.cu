@@ -163,6 +163,11 @@ struct mbx_ctx {
     BuildScratch scratch[MBX_BUILD_LANES];   // [0]: every single-system search
     cudaStream_t lane_stream[MBX_BUILD_LANES] = {nullptr};   // [0] unused (the context stream)
     cudaEvent_t lane_fork = nullptr, lane_join[MBX_BUILD_LANES] = {nullptr};
+    // mbx_energy_2b3b: the 2b term on a child context, kept in step with this
+    // one (gen counts topology/configuration changes)
+    mbx_ctx* child = nullptr;
+    unsigned long gen = 0, child_gen = ~0ul;
+    cudaEvent_t ev_fork = nullptr;
     DevBuf<int4> buckets, list;
     DevBuf<unsigned long long> listed;
     DevBuf<int4> terms;
@@ -245,6 +250,7 @@ int mbx_create(mbx_ctx** out, int device, void* stream) {
     CUCHK(c, cudaMallocHost(&c->h_out, 64 * sizeof(double)));
     for (int i = 0; i < 3; ++i) CUCHK(c, cudaEventCreate(&c->ev[i]));
     CUCHK(c, cudaEventCreateWithFlags(&c->lane_fork, cudaEventDisableTiming));
+    CUCHK(c, cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
     for (int i = 1; i < MBX_BUILD_LANES; ++i) {
         CUCHK(c, cudaStreamCreateWithFlags(&c->lane_stream[i], cudaStreamNonBlocking));
         CUCHK(c, cudaEventCreateWithFlags(&c->lane_join[i], cudaEventDisableTiming));
@@ -295,6 +301,8 @@ int mbx_destroy(mbx_ctx* c) {
         if (c->lane_join[i]) cudaEventDestroy(c->lane_join[i]);
     }
     if (c->lane_fork) cudaEventDestroy(c->lane_fork);
+    if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+    if (c->child) mbx_destroy(c->child);
     c->buckets.release();
     c->list.release();
     c->listed.release();
@@ -491,6 +499,7 @@ extern "C" int mbx_set_topology(mbx_ctx* c, int nmon, const char* const* ids, co
     CUCHK(c, cudaStreamSynchronize(c->stream));
     for (int nb = 0; nb < 4; ++nb)
         for (int b = 0; b < MBX_MAX_BUCKETS; ++b) c->bucket_cap[nb][b] = 0;
+    ++c->gen;
     return build_rules(c);
 }
 
@@ -551,6 +560,7 @@ extern "C" int mbx_set_config(mbx_ctx* c, double cutoff2b, double cutoff3b, cons
     c->cutoff[3] = cutoff3b;
     int r = make_box(c, box, std::max(cutoff2b, cutoff3b), &c->bp);
     if (r) return r;
+    ++c->gen;
     c->ignore[2].clear();
     c->ignore[3].clear();
     for (int i = 0; i < n2; ++i) c->ignore[2].push_back({ignore2b[2 * i], ignore2b[2 * i + 1]});
@@ -735,127 +745,236 @@ static int launch_eval(mbx_ctx* c, const EvaluatorInfo* E, HolderArgs A, int fla
     return MBX_OK;
 }
 
+// Enqueues one term on the context's stream (n-mer build, evaluation, the
+// results copied to pinned memory), on device coordinates X (already
+// wrapped) accumulating into the device gradient G (NULL: energy only).
+static int term_enqueue(mbx_ctx* c, int nbody, int use_ghost, double* X, double* G, int flags, int* kernels) {
+    const bool grads = !(flags & MBX_NO_GRADS);
+    const bool mixed = (flags & MBX_MIXED) && grads;
+    CUCHK(c, cudaEventRecord(c->ev[0], c->stream));
+    int r = launch_build(c, nbody, use_ghost, X, 0, kernels, mixed);
+    if (r) return r;
+    CUCHK(c, cudaEventRecord(c->ev[1], c->stream));
+    CUCHK(c, cudaMemsetAsync(c->out.p, 0, 16 * sizeof(double), c->stream));
+    CUCHK(c, cudaMemsetAsync(c->counters.p, 0, MBX_MAX_BUCKETS * sizeof(int), c->stream));
+    long off = 0;
+    for (int b = 0; b < c->nbucket[nbody]; ++b) {
+        HolderArgs A = base_args(c);
+        A.counter = c->counters.p + b;
+        A.n = c->bucket_cap[nbody][b];
+        A.n_dev = c->bucket_count.p + b;
+        A.status = c->status.p;
+        A.nmers = c->buckets.p + off;
+        A.xyz = X;
+        A.first_index = c->d_first.p;
+        A.grad = grads ? G : nullptr;
+        A.out = c->out.p;
+        off += c->bucket_cap[nbody][b];
+        if (c->bucket_near[nbody][b] && !mixed) continue;   // empty without the split
+        r = launch_eval(c, c->bucket_eval[nbody][b], A, flags, kernels, c->bucket_near[nbody][b]);
+        if (r) return r;
+    }
+    CUCHK(c, cudaEventRecord(c->ev[2], c->stream));
+    // results: energy + virial, counters, status
+    CUCHK(c, cudaMemcpyAsync(c->h_out, c->out.p, 8 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CUCHK(c, cudaMemcpyAsync(c->h_out + 8, c->listed.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                             c->stream));
+    CUCHK(c, cudaMemcpyAsync(c->h_out + 9, c->bucket_count.p, MBX_MAX_BUCKETS * sizeof(int), cudaMemcpyDeviceToHost,
+                             c->stream));
+    CUCHK(c, cudaMemcpyAsync(c->h_out + 13, c->status.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    return MBX_OK;
+}
+
+// After the stream of a term_enqueue has completed: 1 when the build did not
+// fit its buffers (capacities grown; the evaluators saw the status word and
+// added nothing: enqueue again), else 0 with the energy, the virial (+=),
+// the counts and the timing recorded.
+static int term_finish(mbx_ctx* c, int nbody, double* energy, double* virial, int kernels) {
+    int status[2];
+    memcpy(status, c->h_out + 13, sizeof(status));
+    int counts[MBX_MAX_BUCKETS];
+    memcpy(counts, c->h_out + 9, sizeof(counts));
+    if (status[0]) {
+        if (status[0] & MBX_STATUS_NB_OVERFLOW) c->nb_cap = std::max(c->nb_cap * 2, status[1] + 32);
+        for (int b = 0; b < c->nbucket[nbody]; ++b)
+            if (counts[b] > c->bucket_cap[nbody][b]) c->bucket_cap[nbody][b] = (long)(counts[b] * 1.25) + 1024;
+        if ((status[0] & MBX_STATUS_BUCKET_OVERFLOW) && !(status[0] & MBX_STATUS_NB_OVERFLOW)) {
+            for (int b = 0; b < c->nbucket[nbody]; ++b)
+                if (counts[b] >= c->bucket_cap[nbody][b]) c->bucket_cap[nbody][b] *= 2;
+        }
+        return 1;
+    }
+    unsigned long long listed;
+    memcpy(&listed, c->h_out + 8, sizeof(listed));
+    c->last_listed[nbody] = (long)listed;
+    long ev = 0;
+    for (int b = 0; b < c->nbucket[nbody]; ++b) ev += counts[b];
+    c->last_evaluated[nbody] = ev;
+    cudaEventElapsedTime(&c->last_ms_build, c->ev[0], c->ev[1]);
+    cudaEventElapsedTime(&c->last_ms_eval, c->ev[1], c->ev[2]);
+    c->last_kernels = kernels;
+    *energy = c->h_out[0];
+    if (virial) {
+        virial[0] += c->h_out[1];
+        virial[1] += c->h_out[2];
+        virial[2] += c->h_out[3];
+        virial[4] += c->h_out[4];
+        virial[5] += c->h_out[5];
+        virial[8] += c->h_out[6];
+        virial[3] = virial[1];
+        virial[6] = virial[2];
+        virial[7] = virial[5];
+    }
+    return 0;
+}
+
+// Coordinates on the device (staged from the host when needed) and wrapped
+// (SetPBC: FixMonomerCoordinates on every call, system.cpp:741-744); the
+// gradient accumulator on the device (the caller's when it is device memory).
+static int stage_term_io(mbx_ctx* c, double* xyz, double* grad, int flags, double** X, double** G, int* kernels) {
+    const bool dev = (flags & MBX_DEVICE_PTRS) != 0;
+    const bool grads = !(flags & MBX_NO_GRADS);
+    const size_t nx = 3 * (size_t)c->numsites;
+    *X = xyz;
+    if (!dev) {
+        CUCHK(c, c->xyz.ensure(nx));
+        CUCHK(c, cudaMemcpyAsync(c->xyz.p, xyz, nx * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        *X = c->xyz.p;
+    }
+    if (c->bp.use_pbc) {
+        k_fix_monomers<<<(c->nmon + 127) / 128, 128, 0, c->stream>>>(*X, c->d_first.p, c->d_nat.p, c->nmon, c->bp);
+        ++*kernels;
+    }
+    *G = nullptr;
+    if (grads) {
+        if (dev && grad) {
+            *G = grad;  // accumulate straight into the caller's array
+        } else {
+            CUCHK(c, c->grad.ensure(nx));
+            CUCHK(c, cudaMemsetAsync(c->grad.p, 0, nx * sizeof(double), c->stream));
+            *G = c->grad.p;
+        }
+    }
+    return MBX_OK;
+}
+
+// Host outputs of a call with host arrays: the wrapped coordinates and the
+// gradient (+=) back into the caller's arrays.
+static int unstage_term_io(mbx_ctx* c, double* xyz, double* grad, int flags, double* X, double* G) {
+    const bool dev = (flags & MBX_DEVICE_PTRS) != 0;
+    const bool grads = !(flags & MBX_NO_GRADS);
+    const size_t nx = 3 * (size_t)c->numsites;
+    if (dev) return MBX_OK;
+    if (c->bp.use_pbc) CUCHK(c, cudaMemcpyAsync(xyz, X, nx * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (grads && grad) {
+        std::vector<double> tmp(nx);
+        CUCHK(c, cudaMemcpyAsync(tmp.data(), G, nx * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CUCHK(c, cudaStreamSynchronize(c->stream));
+        for (size_t i = 0; i < nx; ++i) grad[i] += tmp[i];
+    } else {
+        CUCHK(c, cudaStreamSynchronize(c->stream));
+    }
+    return MBX_OK;
+}
+
 extern "C" int mbx_energy(mbx_ctx* c, int nbody, double* xyz, int use_ghost, double* energy, double* grad,
                           double* virial, int flags) {
     if (!c || (nbody != 2 && nbody != 3) || !xyz || !energy) return fail(c, MBX_EINVAL, "bad arguments");
     if (!c->nmon) return fail(c, MBX_EINVAL, "System has not been initialized (no topology)");
     CUCHK(c, cudaSetDevice(c->device));
-    const bool dev = (flags & MBX_DEVICE_PTRS) != 0;
-    const bool grads = !(flags & MBX_NO_GRADS);
-    const size_t nx = 3 * (size_t)c->numsites;
+    int kernels = 0;
+    double *X, *G;
+    int r = stage_term_io(c, xyz, grad, flags, &X, &G, &kernels);
+    if (r) return r;
     for (int attempt = 0; attempt < 4; ++attempt) {
-        int kernels = 0;
-        double* X = xyz;
-        if (!dev) {
-            CUCHK(c, c->xyz.ensure(nx));
-            CUCHK(c, cudaMemcpyAsync(c->xyz.p, xyz, nx * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-            X = c->xyz.p;
-        }
-        CUCHK(c, cudaEventRecord(c->ev[0], c->stream));
-        // SetPBC: FixMonomerCoordinates on every call (system.cpp:741-744);
-        // device inputs are wrapped once even when the call is retried
-        if (c->bp.use_pbc && (!dev || attempt == 0)) {
-            k_fix_monomers<<<(c->nmon + 127) / 128, 128, 0, c->stream>>>(X, c->d_first.p, c->d_nat.p, c->nmon, c->bp);
-            ++kernels;
-        }
-        const bool mixed = (flags & MBX_MIXED) && grads;
-        int r = launch_build(c, nbody, use_ghost, X, 0, &kernels, mixed);
+        r = term_enqueue(c, nbody, use_ghost, X, G, flags, &kernels);
         if (r) return r;
-        CUCHK(c, cudaEventRecord(c->ev[1], c->stream));
-        double* G = nullptr;
-        if (grads) {
-            if (dev && grad) {
-                G = grad;  // accumulate straight into the caller's array
-            } else {
-                CUCHK(c, c->grad.ensure(nx));
-                CUCHK(c, cudaMemsetAsync(c->grad.p, 0, nx * sizeof(double), c->stream));
-                G = c->grad.p;
-            }
-        }
-        CUCHK(c, cudaMemsetAsync(c->out.p, 0, 16 * sizeof(double), c->stream));
-        CUCHK(c, cudaMemsetAsync(c->counters.p, 0, MBX_MAX_BUCKETS * sizeof(int), c->stream));
-        long off = 0;
-        for (int b = 0; b < c->nbucket[nbody]; ++b) {
-            HolderArgs A = base_args(c);
-            A.counter = c->counters.p + b;
-            A.n = c->bucket_cap[nbody][b];
-            A.n_dev = c->bucket_count.p + b;
-            A.status = c->status.p;
-            A.nmers = c->buckets.p + off;
-            A.xyz = X;
-            A.first_index = c->d_first.p;
-            A.grad = G;
-            A.out = c->out.p;
-            off += c->bucket_cap[nbody][b];
-            if (c->bucket_near[nbody][b] && !mixed) continue;   // empty without the split
-            r = launch_eval(c, c->bucket_eval[nbody][b], A, flags, &kernels, c->bucket_near[nbody][b]);
-            if (r) return r;
-        }
-        CUCHK(c, cudaEventRecord(c->ev[2], c->stream));
-        // results: energy + virial, counters, status
-        CUCHK(c, cudaMemcpyAsync(c->h_out, c->out.p, 8 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-        CUCHK(c, cudaMemcpyAsync(c->h_out + 8, c->listed.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
-                                 c->stream));
-        CUCHK(c, cudaMemcpyAsync(c->h_out + 9, c->bucket_count.p, MBX_MAX_BUCKETS * sizeof(int),
-                                 cudaMemcpyDeviceToHost, c->stream));
-        CUCHK(c, cudaMemcpyAsync(c->h_out + 13, c->status.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
         CUCHK(c, cudaStreamSynchronize(c->stream));
-        int status[2];
-        memcpy(status, c->h_out + 13, sizeof(status));
-        int counts[MBX_MAX_BUCKETS];
-        memcpy(counts, c->h_out + 9, sizeof(counts));
-        if (status[0]) {
-            if (status[0] & MBX_STATUS_NB_OVERFLOW) c->nb_cap = std::max(c->nb_cap * 2, status[1] + 32);
-            for (int b = 0; b < c->nbucket[nbody]; ++b)
-                if (counts[b] > c->bucket_cap[nbody][b])
-                    c->bucket_cap[nbody][b] = (long)(counts[b] * 1.25) + 1024;
-            if ((status[0] & MBX_STATUS_BUCKET_OVERFLOW) && !(status[0] & MBX_STATUS_NB_OVERFLOW)) {
-                for (int b = 0; b < c->nbucket[nbody]; ++b)
-                    if (counts[b] >= c->bucket_cap[nbody][b]) c->bucket_cap[nbody][b] *= 2;
-            }
-            // the evaluators saw the status word and did nothing; rebuild
-            continue;
-        }
-        unsigned long long listed;
-        memcpy(&listed, c->h_out + 8, sizeof(listed));
-        c->last_listed[nbody] = (long)listed;
-        long ev = 0;
-        for (int b = 0; b < c->nbucket[nbody]; ++b) ev += counts[b];
-        c->last_evaluated[nbody] = ev;
-        cudaEventElapsedTime(&c->last_ms_build, c->ev[0], c->ev[1]);
-        cudaEventElapsedTime(&c->last_ms_eval, c->ev[1], c->ev[2]);
-        *energy = c->h_out[0];
-        if (virial) {
-            virial[0] += c->h_out[1];
-            virial[1] += c->h_out[2];
-            virial[2] += c->h_out[3];
-            virial[4] += c->h_out[4];
-            virial[5] += c->h_out[5];
-            virial[8] += c->h_out[6];
-            virial[3] = virial[1];
-            virial[6] = virial[2];
-            virial[7] = virial[5];
-        }
-        if (!dev) {
-            // wrapped coordinates back into the caller's array (SetPBC semantics)
-            if (c->bp.use_pbc)
-                CUCHK(c, cudaMemcpyAsync(xyz, X, nx * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-            if (grads && grad) {
-                std::vector<double> tmp(nx);
-                CUCHK(c, cudaMemcpyAsync(tmp.data(), c->grad.p, nx * sizeof(double), cudaMemcpyDeviceToHost,
-                                         c->stream));
-                CUCHK(c, cudaStreamSynchronize(c->stream));
-                for (size_t i = 0; i < nx; ++i) grad[i] += tmp[i];
-            } else {
-                CUCHK(c, cudaStreamSynchronize(c->stream));
-            }
-        } else if (grads && !grad) {
-            // nothing to return
-        }
-        c->last_kernels = kernels;
-        return MBX_OK;
+        if (term_finish(c, nbody, energy, virial, kernels) == 0) return unstage_term_io(c, xyz, grad, flags, X, G);
+        kernels = 0;
     }
     return fail(c, MBX_ECUDA, "n-mer buffers did not converge");
+}
+
+// The child context of mbx_energy_2b3b: the 2b term on its own stream and
+// buffers, same topology, configuration, launch shapes and CH4-CH4
+// coefficients as the parent.
+static int sync_child(mbx_ctx* c) {
+    if (c->child && c->child_gen == c->gen) return MBX_OK;
+    if (!c->child) {
+        int r = mbx_create(&c->child, c->device, nullptr);
+        if (r) return fail(c, r, "child context");
+    }
+    mbx_ctx* k = c->child;
+    std::vector<const char*> ids(c->nmon);
+    for (int m = 0; m < c->nmon; ++m) ids[m] = c->type_names[c->h_type[m]].c_str();
+    int r = mbx_set_topology(k, c->nmon, ids.data(), c->h_first.data(), c->h_tag.data(), c->h_local.data(),
+                             c->numsites);
+    if (r) return fail(c, r, std::string("child topology: ") + k->err);
+    std::vector<const char*> i2, i3;
+    for (auto& t : c->ignore[2]) for (auto& x : t) i2.push_back(x.c_str());
+    for (auto& t : c->ignore[3]) for (auto& x : t) i3.push_back(x.c_str());
+    r = mbx_set_config(k, c->cutoff[2], c->cutoff[3], c->bp.use_pbc ? c->bp.box : nullptr, (int)c->ignore[2].size(),
+                       i2.data(), (int)c->ignore[3].size(), i3.data());
+    if (r) return fail(c, r, std::string("child configuration: ") + k->err);
+    for (int nb = 0; nb < 4; ++nb) k->knobs[nb] = c->knobs[nb];
+    if (c->warp_coef.p && k->warp_coef.p)
+        CUCHK(c, cudaMemcpy(k->warp_coef.p, c->warp_coef.p, std::min(c->warp_coef.n, k->warp_coef.n) * sizeof(double),
+                            cudaMemcpyDeviceToDevice));
+    c->child_gen = c->gen;
+    return MBX_OK;
+}
+
+extern "C" int mbx_energy_2b3b(mbx_ctx* c, double* xyz, int use_ghost, double* e2, double* e3, double* grad,
+                               double* virial, int flags) {
+    if (!c || !xyz || !e2 || !e3) return fail(c, MBX_EINVAL, "bad arguments");
+    if (!c->nmon) return fail(c, MBX_EINVAL, "System has not been initialized (no topology)");
+    CUCHK(c, cudaSetDevice(c->device));
+    int r = sync_child(c);
+    if (r) return r;
+    mbx_ctx* k = c->child;
+    int kernels = 0, kk = 0;
+    double *X, *G;
+    r = stage_term_io(c, xyz, grad, flags, &X, &G, &kernels);
+    if (r) return r;
+    // the 2b term on the child's stream once the coordinates are wrapped
+    CUCHK(c, cudaEventRecord(c->ev_fork, c->stream));
+    CUCHK(c, cudaStreamWaitEvent(k->stream, c->ev_fork, 0));
+    r = term_enqueue(c, 3, use_ghost, X, G, flags, &kernels);
+    if (r) return r;
+    r = term_enqueue(k, 2, use_ghost, X, G, flags, &kk);
+    if (r) return fail(c, r, std::string("2b term: ") + k->err);
+    CUCHK(c, cudaStreamSynchronize(k->stream));
+    CUCHK(c, cudaStreamSynchronize(c->stream));
+    int again3 = term_finish(c, 3, e3, virial, kernels);
+    int again2 = term_finish(k, 2, e2, virial, kk);
+    // a term whose n-mers did not fit its buffers added nothing: run it again
+    for (int attempt = 0; (again2 || again3) && attempt < 4; ++attempt) {
+        if (again3) {
+            kernels = 0;
+            r = term_enqueue(c, 3, use_ghost, X, G, flags, &kernels);
+            if (r) return r;
+        }
+        if (again2) {
+            CUCHK(c, cudaEventRecord(c->ev_fork, c->stream));
+            CUCHK(c, cudaStreamWaitEvent(k->stream, c->ev_fork, 0));
+            kk = 0;
+            r = term_enqueue(k, 2, use_ghost, X, G, flags, &kk);
+            if (r) return fail(c, r, std::string("2b term: ") + k->err);
+        }
+        CUCHK(c, cudaStreamSynchronize(k->stream));
+        CUCHK(c, cudaStreamSynchronize(c->stream));
+        if (again3) again3 = term_finish(c, 3, e3, virial, kernels);
+        if (again2) again2 = term_finish(k, 2, e2, virial, kk);
+    }
+    if (again2 || again3) return fail(c, MBX_ECUDA, "n-mer buffers did not converge");
+    c->last_listed[2] = k->last_listed[2];
+    c->last_evaluated[2] = k->last_evaluated[2];
+    c->last_kernels = kernels + kk;
+    // the 2b term also waited for the wrap: make the caller's stream see its work
+    CUCHK(c, cudaEventRecord(k->ev[2], k->stream));
+    CUCHK(c, cudaStreamWaitEvent(c->stream, k->ev[2], 0));
+    return unstage_term_io(c, xyz, grad, flags, X, G);
 }
 
 extern "C" int mbx_last_counts(const mbx_ctx* c, int nbody, long* listed, long* evaluated) {
@@ -1091,9 +1210,11 @@ extern "C" int mbx_set_coefficients(mbx_ctx* c, const char* name, const double* 
     const double* src = a ? a : E->fit;
     for (int v = 0; v < 7; ++v)
         if (E->set[v]) RCHK(c, E->set[v](src, dev ? 1 : 0, c->stream));
-    if (E->w)
+    if (E->w) {
         CUCHK(c, cudaMemcpyAsync(c->warp_coef.p, src, E->ncoef * sizeof(double),
                                  dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, c->stream));
+        ++c->gen;   // the child context copies them again
+    }
     CUCHK(c, cudaStreamSynchronize(c->stream));
     return MBX_OK;
 }
@@ -1374,6 +1495,7 @@ extern "C" int mbx_tune(mbx_ctx* c, int nbody, double* xyz, double* grad, int fl
         *ax.field = best_v;
     }
     drop_graphs(c);
+    ++c->gen;
     if (out) {
         out[0] = K.nb_warps;
         out[1] = K.nb_unroll;
@@ -1405,5 +1527,6 @@ extern "C" int mbx_set_knobs(mbx_ctx* c, int nbody, const int* in) {
     K.tri_threads = in[2];
     K.dim_threads = in[3];
     drop_graphs(c);
+    ++c->gen;
     return MBX_OK;
 }

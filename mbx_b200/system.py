@@ -136,6 +136,20 @@ class System:
     def ThreeBodyEnergy(self, do_grads, use_ghost=False):
         return self._term(3, do_grads, use_ghost)
 
+    def TwoAndThreeBodyEnergy(self, do_grads, use_ghost=False):
+        """Both terms in one call (no counterpart in the reference, whose
+        Energy() runs Get2B and Get3B one after the other): the 2b and 3b
+        terms run side by side on the GPU.  Returns (E2B, E3B); the gradient
+        and virial hold their sum."""
+        if not self.initialized:
+            raise CUException("System has not been initialized. 2B/3B Energy calculation not possible.")
+        self.grad[:] = 0.0
+        self.virial[:] = 0.0
+        e2, e3 = self._ctx.energy_2b3b(self.sites, self.grad if do_grads else None, self.virial,
+                                       use_ghost=use_ghost, mixed=self.precision == "mixed", grads=do_grads)
+        self.energy = e2 + e3
+        return e2, e3
+
     # ------------------------------------------------------------ getters
     def GetRealGrads(self):
         return self.top.input_from_sites(self.grad)

@@ -328,3 +328,35 @@ def test_water_2048_mixed():
     e3 = m.ThreeBodyEnergy(True)
     assert rel(e2, r2) < MIXED_REL_TERM and rel(e3, r3) < MIXED_REL_TERM
     assert rel(e2 + e3, r2 + r3) < MIXED_REL
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_energy_2b3b_matches_separate_terms(mixed):
+    """mbx_energy_2b3b (both terms side by side) against the separate calls,
+    host arrays through the System mirror and device arrays through the C ABI."""
+    torch = pytest.importorskip("torch")
+    from mbx_b200 import capi
+    ids, xyz, box = workloads.water_256(0)
+    prec = "mixed" if mixed else "fp64"
+    a = msys.from_arrays(ids, xyz, box, 9.0, 7.0, precision=prec)
+    e2 = a.TwoBodyEnergy(True)
+    g2 = np.asarray(a.GetRealGrads())
+    v2 = a.GetVirial()
+    e3 = a.ThreeBodyEnergy(True)
+    g3 = np.asarray(a.GetRealGrads())
+    v3 = a.GetVirial()
+    b = msys.from_arrays(ids, xyz, box, 9.0, 7.0, precision=prec)
+    f2, f3 = b.TwoAndThreeBodyEnergy(True)
+    tol = 1e-12 if not mixed else 1e-9
+    assert abs(f2 - e2) <= tol * abs(e2) + 1e-10 and abs(f3 - e3) <= tol * abs(e3) + 1e-10
+    np.testing.assert_allclose(b.GetRealGrads(), g2 + g3, rtol=0, atol=1e-9)
+    np.testing.assert_allclose(b.GetVirial(), v2 + v3, rtol=1e-10, atol=1e-8)
+    assert b.NmerCounts(2) == a.NmerCounts(2) and b.NmerCounts(3) == a.NmerCounts(3)
+    # device arrays, twice in a row (the child context is reused)
+    ctx = capi.Context(0)
+    c = msys.from_arrays(ids, xyz, box, 9.0, 7.0, context=ctx)
+    sites = torch.tensor(c.sites, device="cuda")
+    for _ in range(2):
+        g = torch.zeros_like(sites)
+        d2, d3 = ctx.energy_2b3b(sites, g, np.zeros(9), mixed=mixed)
+        assert abs(d2 - e2) <= tol * abs(e2) + 1e-10 and abs(d3 - e3) <= tol * abs(e3) + 1e-10
