@@ -150,6 +150,14 @@ int mbx_set_batch(mbx_ctx* ctx, int nconf, const int* conf_mon, const double* bo
 int mbx_batch_energy(mbx_ctx* ctx, int nbody, double* xyz, double* grad, double* energies, double* virials,
                      int flags);
 
+/* Both terms of every configuration of the batch in one call, side by side
+ * on two streams (the 2b term on a child context mirroring the batch);
+ * arguments as for mbx_batch_energy, e2[nconf] and e3[nconf] the term
+ * energies, virials the sum of both (+=).  MBX_GRAPH captures both streams'
+ * work into one graph. */
+int mbx_batch_energy_2b3b(mbx_ctx* ctx, double* xyz, double* grad, double* e2, double* e3, double* virials,
+                          int flags);
+
 /* Autotuner of the n-mer builder's launch shapes for one term (no
  * counterpart in the reference): times the term on the current batch (or the
  * whole system when no batch is set) with device arrays xyz/grad and flags as

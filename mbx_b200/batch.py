@@ -50,6 +50,11 @@ class Batch:
         return self.ctx.batch_energy(nbody, self.sites, self.grad if grads else None, mixed=mixed, graph=graph,
                                      virials=virials)
 
+    def energy_2b3b(self, grads=True, mixed=False, graph=True, virials=False):
+        """Both terms of every configuration side by side: (e2[], e3[])."""
+        return self.ctx.batch_energy_2b3b(self.sites, self.grad if grads else None, mixed=mixed, graph=graph,
+                                          virials=virials)
+
     def tune(self, nbody, mixed=False):
         return self.ctx.tune(nbody, self.sites, self.grad, mixed=mixed)
 

@@ -62,6 +62,8 @@ def lib():
     L.mbx_batch_energy.argtypes = [vp, ctypes.c_int, dp, dp, ctypes.POINTER(ctypes.c_double),
                                    ctypes.POINTER(ctypes.c_double), ctypes.c_int]
     L.mbx_tune.argtypes = [vp, ctypes.c_int, dp, dp, ctypes.c_int, ip, ctypes.POINTER(ctypes.c_double)]
+    L.mbx_batch_energy_2b3b.argtypes = [vp, dp, dp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                                        ctypes.POINTER(ctypes.c_double), ctypes.c_int]
     L.mbx_get_knobs.argtypes = [vp, ctypes.c_int, ip]
     L.mbx_set_knobs.argtypes = [vp, ctypes.c_int, ip]
     _lib = L
@@ -71,7 +73,8 @@ def lib():
 EXPORTED = ("mbx_create", "mbx_destroy", "mbx_last_error", "mbx_version", "mbx_set_topology", "mbx_set_config",
             "mbx_energy", "mbx_last_counts", "mbx_nmers", "mbx_evaluate", "mbx_evaluate_dcoef", "mbx_poly",
             "mbx_set_coefficients", "mbx_evaluator_info", "mbx_last_timing", "mbx_fma_peaks", "mbx_set_batch",
-            "mbx_batch_energy", "mbx_tune", "mbx_get_knobs", "mbx_set_knobs", "mbx_energy_2b3b")
+            "mbx_batch_energy", "mbx_tune", "mbx_get_knobs", "mbx_set_knobs", "mbx_energy_2b3b",
+            "mbx_batch_energy_2b3b")
 
 KNOBS = ("nb_warps", "nb_unroll", "tri_threads", "dim_threads")
 
@@ -274,6 +277,23 @@ class Context:
         self._check(lib().mbx_batch_energy(self.h, nbody, px, pg, e.ctypes.data_as(dpp),
                                            None if v is None else v.ctypes.data_as(dpp), flags))
         return (e, v) if virials else e
+
+    def batch_energy_2b3b(self, xyz, grad=None, mixed=False, graph=False, virials=False):
+        """Both terms of every configuration, side by side on the GPU.
+        Returns (e2[nconf], e3[nconf]) (and virials[nconf, 9], summed)."""
+        px, dx = _ptr(xyz)
+        pg, dg = _ptr(grad)
+        if not dx or (grad is not None and not dg):
+            raise TypeError("batches take CUDA tensors")
+        flags = MBX_DEVICE_PTRS | (MBX_MIXED if mixed else 0) | (MBX_GRAPH if graph else 0) | \
+            (0 if grad is not None else MBX_NO_GRADS)
+        e2 = np.zeros(self._nconf)
+        e3 = np.zeros(self._nconf)
+        v = np.zeros((self._nconf, 9)) if virials else None
+        dpp = ctypes.POINTER(ctypes.c_double)
+        self._check(lib().mbx_batch_energy_2b3b(self.h, px, pg, e2.ctypes.data_as(dpp), e3.ctypes.data_as(dpp),
+                                                None if v is None else v.ctypes.data_as(dpp), flags))
+        return (e2, e3, v) if virials else (e2, e3)
 
     def tune(self, nbody, xyz, grad=None, mixed=False):
         """Autotunes the builder's launch shapes of a term on the current batch

@@ -918,6 +918,16 @@ static int sync_child(mbx_ctx* c) {
                        i2.data(), (int)c->ignore[3].size(), i3.data());
     if (r) return fail(c, r, std::string("child configuration: ") + k->err);
     for (int nb = 0; nb < 4; ++nb) k->knobs[nb] = c->knobs[nb];
+    if (c->nconf) {
+        std::vector<double> boxes(9 * (size_t)c->nconf);
+        std::vector<int> has(c->nconf);
+        for (int q = 0; q < c->nconf; ++q) {
+            for (int i = 0; i < 9; ++i) boxes[9 * q + i] = c->conf_bp[q].box[i];
+            has[q] = c->conf_bp[q].use_pbc;
+        }
+        r = mbx_set_batch(k, c->nconf, c->conf_mon.data(), boxes.data(), has.data());
+        if (r) return fail(c, r, std::string("child batch: ") + k->err);
+    }
     if (c->warp_coef.p && k->warp_coef.p)
         CUCHK(c, cudaMemcpy(k->warp_coef.p, c->warp_coef.p, std::min(c->warp_coef.n, k->warp_coef.n) * sizeof(double),
                             cudaMemcpyDeviceToDevice));
@@ -1253,6 +1263,7 @@ extern "C" int mbx_set_batch(mbx_ctx* c, int nconf, const int* conf_mon, const d
     for (int k = 0; k < nconf; ++k)
         for (int m = conf_mon[k]; m < conf_mon[k + 1]; ++m) mon_conf[m] = k;
     drop_graphs(c);
+    ++c->gen;
     c->nconf = nconf;
     c->conf_mon.assign(conf_mon, conf_mon + nconf + 1);
     c->conf_bp = bp;
@@ -1273,7 +1284,7 @@ extern "C" int mbx_set_batch(mbx_ctx* c, int nconf, const int* conf_mon, const d
 // synchronisation (so that it can be captured into a graph): wrap every
 // configuration, build every configuration's n-mers, evaluate every bucket
 // once, copy the per-configuration sums and the status back to pinned memory.
-static int batch_sequence(mbx_ctx* c, int nbody, double* X, double* G, bool grads, bool mixed, int* kernels) {
+static int batch_wrap(mbx_ctx* c, double* X, int* kernels) {
     for (int k = 0; k < c->nconf; ++k) {
         const int b = c->conf_mon[k], n = c->conf_mon[k + 1] - b;
         if (n > 0 && c->conf_bp[k].use_pbc) {
@@ -1281,6 +1292,16 @@ static int batch_sequence(mbx_ctx* c, int nbody, double* X, double* G, bool grad
                                                                    c->conf_bp[k]);
             ++*kernels;
         }
+    }
+    CUCHK(c, cudaGetLastError());
+    return MBX_OK;
+}
+
+static int batch_sequence(mbx_ctx* c, int nbody, double* X, double* G, bool grads, bool mixed, int* kernels,
+                          bool wrap = true) {
+    if (wrap) {
+        int rw = batch_wrap(c, X, kernels);
+        if (rw) return rw;
     }
     int r = prepare_buckets(c, nbody, c->nmon, 0);
     if (r) return r;
@@ -1528,5 +1549,119 @@ extern "C" int mbx_set_knobs(mbx_ctx* c, int nbody, const int* in) {
     K.dim_threads = in[3];
     drop_graphs(c);
     ++c->gen;
+    return MBX_OK;
+}
+
+// Both terms of every configuration of the batch, side by side: the 3b term
+// on this context's stream, the 2b term on the child's (a mirror of the
+// batch), the coordinates wrapped once before they fork.  With MBX_GRAPH the
+// two streams' work is captured into one graph.
+static int batch_enqueue_2b3b(mbx_ctx* c, double* X, double* G, bool grads, bool mixed, bool run3, bool run2,
+                              int* kernels) {
+    mbx_ctx* k = c->child;
+    int r = batch_wrap(c, X, kernels);
+    if (r) return r;
+    if (run2) {
+        CUCHK(c, cudaEventRecord(c->ev_fork, c->stream));
+        CUCHK(c, cudaStreamWaitEvent(k->stream, c->ev_fork, 0));
+    }
+    if (run3) {
+        r = batch_sequence(c, 3, X, G, grads, mixed, kernels, false);
+        if (r) return r;
+    }
+    if (run2) {
+        r = batch_sequence(k, 2, X, G, grads, mixed, kernels, false);
+        if (r) return fail(c, r, std::string("2b term: ") + k->err);
+        CUCHK(c, cudaEventRecord(k->ev_fork, k->stream));
+        CUCHK(c, cudaStreamWaitEvent(c->stream, k->ev_fork, 0));
+    }
+    return MBX_OK;
+}
+
+extern "C" int mbx_batch_energy_2b3b(mbx_ctx* c, double* xyz, double* grad, double* e2, double* e3,
+                                     double* virials, int flags) {
+    if (!c || !xyz || !e2 || !e3) return fail(c, MBX_EINVAL, "bad arguments");
+    if (!c->nconf) return fail(c, MBX_EINVAL, "no batch (mbx_set_batch)");
+    if (!(flags & MBX_DEVICE_PTRS)) return fail(c, MBX_EINVAL, "batches take device arrays (MBX_DEVICE_PTRS)");
+    CUCHK(c, cudaSetDevice(c->device));
+    int r = sync_child(c);
+    if (r) return r;
+    mbx_ctx* k = c->child;
+    const bool grads = !(flags & MBX_NO_GRADS) && grad;
+    const bool mixed = (flags & MBX_MIXED) && grads;
+    double* G = grads ? grad : nullptr;
+    const int key = (flags & (MBX_MIXED | MBX_NO_GRADS)) | 0x100;
+    auto& gr = c->graph[0];
+    int kernels = 0;
+    bool need3 = true, need2 = true;
+    CUCHK(c, cudaEventRecord(c->ev[0], c->stream));
+    if ((flags & MBX_GRAPH) && gr.exec && gr.xyz == xyz && gr.grad == grad && gr.flags == key &&
+        gr.gen == g_realloc_gen.load()) {
+        CUCHK(c, cudaGraphLaunch(gr.exec, c->stream));
+        CUCHK(c, cudaEventRecord(c->ev[2], c->stream));
+        CUCHK(c, cudaStreamSynchronize(c->stream));
+        kernels = 1;
+        need3 = batch_check(c, 3) != 0;
+        need2 = batch_check(k, 2) != 0;
+        if (need3 || need2) drop_graphs(c);   // buffers grow: capture again after a plain run
+    }
+    if (need3 || need2) {
+        // a term whose n-mers did not fit added nothing: (re)run only such terms
+        for (int attempt = 0; need3 || need2; ++attempt) {
+            if (attempt == 4) return fail(c, MBX_ENOMEM, "batch buffers kept overflowing");
+            CUCHK(c, cudaEventRecord(c->ev[0], c->stream));
+            r = batch_enqueue_2b3b(c, xyz, G, grads, mixed, need3, need2, &kernels);
+            if (r) return r;
+            CUCHK(c, cudaEventRecord(c->ev[2], c->stream));
+            CUCHK(c, cudaStreamSynchronize(c->stream));
+            if (need3) need3 = batch_check(c, 3) != 0;
+            if (need2) need2 = batch_check(k, 2) != 0;
+        }
+        if (flags & MBX_GRAPH) {
+            if (gr.exec) cudaGraphExecDestroy(gr.exec);
+            gr = mbx_ctx::Graph{};
+            cudaGraph_t g = nullptr;
+            int dummy = 0;
+            CUCHK(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed));
+            const unsigned long gen = g_realloc_gen.load();
+            r = batch_enqueue_2b3b(c, xyz, G, grads, mixed, true, true, &dummy);
+            cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+            if (r) {
+                if (g) cudaGraphDestroy(g);
+                return r;
+            }
+            if (e != cudaSuccess) return fail(c, MBX_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+            if (gen != g_realloc_gen.load()) {
+                cudaGraphDestroy(g);
+            } else {
+                e = cudaGraphInstantiate(&gr.exec, g, 0);
+                cudaGraphDestroy(g);
+                if (e != cudaSuccess) return fail(c, MBX_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+                gr.xyz = xyz;
+                gr.grad = grad;
+                gr.flags = key;
+                gr.gen = gen;
+            }
+        }
+    }
+    for (int q = 0; q < c->nconf; ++q) {
+        const double* o3 = c->h_conf + 8 * q;
+        const double* o2 = k->h_conf + 8 * q;
+        e3[q] = o3[0];
+        e2[q] = o2[0];
+        if (virials) {
+            double* v = virials + 9 * q;
+            const double s1 = o2[1] + o3[1], s2 = o2[2] + o3[2], s3 = o2[3] + o3[3];
+            const double s4 = o2[4] + o3[4], s5 = o2[5] + o3[5], s6 = o2[6] + o3[6];
+            v[0] += s1; v[1] += s2; v[2] += s3;
+            v[3] += s2; v[4] += s4; v[5] += s5;
+            v[6] += s3; v[7] += s5; v[8] += s6;
+        }
+    }
+    c->last_listed[2] = k->last_listed[2];
+    c->last_evaluated[2] = k->last_evaluated[2];
+    c->last_ms_build = 0;
+    cudaEventElapsedTime(&c->last_ms_eval, c->ev[0], c->ev[2]);
+    c->last_kernels = kernels;
     return MBX_OK;
 }

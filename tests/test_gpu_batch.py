@@ -115,3 +115,23 @@ def test_tune_keeps_results():
     knobs2, _ = b.tune(2)
     assert knobs2["dim_threads"] in (64, 128, 256)
     assert b.ctx.knobs(3) == knobs
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_batch_2b3b_matches_separate_terms(mixed):
+    """Both terms side by side (child context mirroring the batch) against the
+    separate term calls; plain run, graph capture and replays."""
+    cfgs = small_batch()
+    b = Batch(cfgs)
+    b.energy(2, mixed=mixed, graph=False)          # wraps the coordinates
+    b.grad.zero_()
+    e2, v2 = b.energy(2, mixed=mixed, graph=False, virials=True)
+    e3, v3 = b.energy(3, mixed=mixed, graph=False, virials=True)
+    g_sep = b.grad.clone()
+    for graph in (False, True, True, True):
+        b.grad.zero_()
+        f2, f3, v = b.energy_2b3b(mixed=mixed, graph=graph, virials=True)
+        np.testing.assert_allclose(f2, e2, rtol=1e-12, atol=1e-10)
+        np.testing.assert_allclose(f3, e3, rtol=1e-12, atol=1e-10)
+        np.testing.assert_allclose(v, v2 + v3, rtol=1e-10, atol=1e-8)
+        torch.testing.assert_close(b.grad, g_sep, rtol=0, atol=1e-9)
