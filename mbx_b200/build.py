@@ -40,7 +40,7 @@ def deps(src):
     if os.path.dirname(src) == GEN:
         name, v = base[:-3].rsplit("_", 1)
         common.append(os.path.join(GEN, name + ".cuh"))
-        variant = {"g": "pip", "e": "pip_e", "m": "pip_mixed", "c": "dcoef", "p": "pip"}.get(v)
+        variant = {"g": "pip", "e": "pip_e", "c": "dcoef", "p": "pip", "s": "pip_s32"}.get(v)
         if variant:
             common.append(os.path.join(GEN, "%s_%s.cuh" % (name, variant)))
     else:

@@ -182,10 +182,11 @@ def parts_for(nterms, nvars=36):
     function of 10^4-10^5 FMAs leaves the register allocator live ranges it
     cannot fit (kilobytes of spills), and the code of a piece should stay
     small enough for the instruction cache that the warps of a lockstep block
-    share: ~400 terms per piece in 384-thread blocks, ~450 in 256-thread
-    blocks (measured on the MB-pol 2b/3b tries: 350-450 terms is the
-    plateau)."""
-    per = 400 if lock_threads(nvars) == 384 else 450
+    share: ~400 terms per piece in 384-thread blocks, ~600 in 256-thread
+    blocks with shared-memory x/g columns (MB-pol 3b gradient kernel on the
+    2048-water trimers: 1.42/1.39/1.35/1.32/1.47 ms at 300/375/450/600/700
+    terms per piece, and 2.1 ms at 800-900, past the instruction cache)."""
+    per = 400 if lock_threads(nvars) == 384 else 600
     return max(1, (nterms + per - 1) // per)
 
 
@@ -265,6 +266,19 @@ def emit_split(trie, nvars, name, out, nparts, arrays, body, ret="double"):
     w("    %s E = %s;" % (ret, e0))
     calls(True, "Coef, S", ", ".join("%sm" % a for a, _, _ in arrays))
     w("    return E;")
+    w("}")
+    # name_piece<S>(k, coef, xm, gm): piece k alone, the same instantiation
+    # as name_lock<S> calls (holder_prime_kernel runs one piece per block to
+    # bring the code of all pieces into L2 in parallel)
+    w("static constexpr int %s_NPIECES = %d;" % (name, len(pieces)))
+    w("template <int S, class Coef>")
+    w("__device__ __forceinline__ %s %s_piece(int k, const Coef& coef, %s) {" % (ret, name, params))
+    w("    switch (k) {")
+    args = ", ".join("%sm" % a for a, _, _ in arrays)
+    for i in range(len(pieces)):
+        w("    case %d: return %s_part%d<Coef, S>(coef, %s);" % (i, name, i, args))
+    w("    default: return %s;" % e0)
+    w("    }")
     w("}")
 
 
@@ -495,6 +509,8 @@ def emit_traits(spec, table, straight, out):
           "{ %s_shift(x, xf); }" % (spec.nvars, spec.nvars, n))
         w("    template <int S, class C> __device__ __forceinline__ static double2 pip_s32_lock(const C& c, "
           "const f2_t* __restrict__ x, f2_t* __restrict__ g) { return %s_pip_s32_lock<S>(c, x, g); }" % n)
+        w("    template <int S, class C> __device__ __forceinline__ static double2 pip_s32_piece(int k, const C& c, "
+          "const f2_t* __restrict__ x, f2_t* __restrict__ g) { return %s_pip_s32_piece<S>(k, c, x, g); }" % n)
     w("    __device__ __forceinline__ static void sites(const double (&r)[%d][3], double (&s)[%d][3]) { %s_sites(r, s); }" %
       (spec.nreal, ns, n))
     w("    __device__ __forceinline__ static void vars(const double (&s)[%d][3], double (&x)[%d]) { %s_vars(s, x); }" %
@@ -510,6 +526,10 @@ def emit_traits(spec, table, straight, out):
           "const double* __restrict__ x, double* __restrict__ g) { return %s_pip_lock<S>(c, x, g); }" % n)
         w("    template <int S, class C> __device__ __forceinline__ static double pip_e_lock(const C& c, "
           "const double* __restrict__ x) { return %s_pip_e_lock<S>(c, x); }" % n)
+        w("    template <int S, class C> __device__ __forceinline__ static double pip_piece(int k, const C& c, "
+          "const double* __restrict__ x, double* __restrict__ g) { return %s_pip_piece<S>(k, c, x, g); }" % n)
+        w("    template <int S, class C> __device__ __forceinline__ static double pip_e_piece(int k, const C& c, "
+          "const double* __restrict__ x) { return %s_pip_e_piece<S>(k, c, x); }" % n)
 
         w("    template <class S> __device__ __forceinline__ static void dcoef(const double (&x)[%d], S&& sink) "
           "{ %s_dcoef(x, sink); }" % (spec.nvars, n))
@@ -547,6 +567,10 @@ def generate(name):
                 "template <int S, class Coef> __device__ __forceinline__ double %s_pip_lock(const Coef&, "
                 "const double* __restrict__, double* __restrict__);" % name,
                 "template <int S, class Coef> __device__ __forceinline__ double %s_pip_e_lock(const Coef&, "
+                "const double* __restrict__);" % name,
+                "template <int S, class Coef> __device__ __forceinline__ double %s_pip_piece(int, const Coef&, "
+                "const double* __restrict__, double* __restrict__);" % name,
+                "template <int S, class Coef> __device__ __forceinline__ double %s_pip_e_piece(int, const Coef&, "
                 "const double* __restrict__);" % name]
         out += ["template <class Sink> __device__ __forceinline__ void %s_dcoef(const double (&)[%d], Sink&&);" %
                 (name, nv)]
@@ -554,6 +578,8 @@ def generate(name):
             sp = shifted_pip(name)
             out.append("template <int S, class Coef> __device__ __forceinline__ double2 %s_pip_s32_lock(const Coef&, "
                        "const f2_t* __restrict__, f2_t* __restrict__);" % name)
+            out.append("template <int S, class Coef> __device__ __forceinline__ double2 %s_pip_s32_piece(int, "
+                       "const Coef&, const f2_t* __restrict__, f2_t* __restrict__);" % name)
             out.append("// dx = x - x0, the reference point of the FP32 basis (%s)" % SHIFT_TYPES[name])
             out.append("__device__ __forceinline__ void %s_shift(const double (&x)[%d], float (&xf)[%d]) {" %
                        (name, nv, nv))
@@ -583,16 +609,17 @@ def generate(name):
             body = head + ["#pragma once", '#include "%s.cuh"' % name,
                            "// %d monomials of the %s basis, %d coefficient orbits" %
                            (len(sp.monos), SHIFT_TYPES[name], sp.norb)]
-            # ~330 terms per piece: larger pieces spill in the paired form
-            # (measured: 300-350 terms 0.79-0.81 ms, 450 terms 1.29 ms for the
-            # 2048-water trimers)
-            emit_pip_f32x2(strie, nv, "%s_pip_s32" % name, body, max(1, (len(sp.monos) + 329) // 330))
+            # ~400 terms per piece: larger pieces spill in the paired form
+            # (2048-water trimers, x/g in shared memory: 0.833/0.818/0.910 ms
+            # at 330/400/480 terms per piece)
+            emit_pip_f32x2(strie, nv, "%s_pip_s32" % name, body, max(1, (len(sp.monos) + 399) // 400))
             write_if_changed(os.path.join(OUT, "%s_pip_s32.cuh" % name), "\n".join(body) + "\n")
     return os.path.join(OUT, name + ".cuh"), leaves, inner
 
 
 TU_HEAD = """// Generated by mbx_b200/codegen/gen_kernels.py -- do not edit.
 // %(what)s for the %(name)s evaluator.
+#include <cstring>
 #include <vector>
 #include "../holder_kernel.cuh"
 #include "%(name)s.cuh"
@@ -651,6 +678,28 @@ int mbx_launch_%(name)s_g(const HolderArgs& A, int grid, int block, cudaStream_t
     kern<<<grid, block, smem, s>>>(A);
     return (int)cudaGetLastError();
 }
+
+int mbx_prime_%(name)s_g(cudaStream_t s) {
+    // code prefetch of the FP64 gradient trie: a launch of the evaluation kernel itself in its
+    // prefetch mode (prime_pieces), one warp per SM, every piece run by at
+    // least four of them
+    auto kern = holder_lock_kernel<%(name)s_T, %(name)s_CC, HM_GRAD_FP64, false>;
+    const int smem_full = 2 * %(name)s_T::NVARS * %(name)s_T::LOCK_THREADS * (int)sizeof(double);
+    const int smem = %(name)s_T::NVARS * %(name)s_T::LOCK_THREADS * (int)sizeof(double);
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_full);
+    }
+    HolderArgs A;
+    memset(&A, 0, sizeof(A));
+    A.prime_npieces = %(name)s_pip_NPIECES;
+    A.prime_passes = (4 * A.prime_npieces + sms - 1) / sms;
+    kern<<<sms, 32, smem, s>>>(A);
+    return (int)cudaGetLastError();
+}
 """),
     "e": ("FP64 energy-only kernel", """
 int mbx_launch_%(name)s_e(const HolderArgs& A, int grid, int block, cudaStream_t s) {
@@ -673,6 +722,28 @@ int mbx_launch_%(name)s_e(const HolderArgs& A, int grid, int block, cudaStream_t
     grid = (int)(need < (long)sms * bps ? need : (long)sms * bps);
     if (grid < 1) grid = 1;
     kern<<<grid, block, smem, s>>>(A);
+    return (int)cudaGetLastError();
+}
+
+int mbx_prime_%(name)s_e(cudaStream_t s) {
+    // code prefetch of the FP64 energy trie: a launch of the evaluation kernel itself in its
+    // prefetch mode (prime_pieces), one warp per SM, every piece run by at
+    // least four of them
+    auto kern = holder_lock_kernel<%(name)s_T, %(name)s_CC, HM_ENERGY, false>;
+    const int smem_full = 1 * %(name)s_T::NVARS * %(name)s_T::LOCK_THREADS * (int)sizeof(double);
+    const int smem = %(name)s_T::NVARS * %(name)s_T::LOCK_THREADS * (int)sizeof(double);
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_full);
+    }
+    HolderArgs A;
+    memset(&A, 0, sizeof(A));
+    A.prime_npieces = %(name)s_pip_e_NPIECES;
+    A.prime_passes = (4 * A.prime_npieces + sms - 1) / sms;
+    kern<<<sms, 32, smem, s>>>(A);
     return (int)cudaGetLastError();
 }
 """),
@@ -779,6 +850,28 @@ int mbx_launch_%(name)s_s(const HolderArgs& A, int grid, int block, cudaStream_t
     kern<<<grid, block, smem, s>>>(A);
     return (int)cudaGetLastError();
 }
+
+int mbx_prime_%(name)s_s(cudaStream_t s) {
+    // code prefetch of the paired FP32 trie: a launch of the evaluation kernel itself in its
+    // prefetch mode (prime_pieces), one warp per SM, every piece run by at
+    // least four of them
+    auto kern = holder_pair_kernel<%(name)s_T, %(name)s_CS>;
+    const int smem_full = 2 * %(name)s_T::NVARS * %(name)s_T::LOCK_THREADS_S * (int)sizeof(f2_t);
+    const int smem = %(name)s_T::NVARS * %(name)s_T::LOCK_THREADS_S * (int)sizeof(f2_t);
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_full);
+    }
+    HolderArgs A;
+    memset(&A, 0, sizeof(A));
+    A.prime_npieces = %(name)s_pip_s32_NPIECES;
+    A.prime_passes = (4 * A.prime_npieces + sms - 1) / sms;
+    kern<<<sms, 32, smem, s>>>(A);
+    return (int)cudaGetLastError();
+}
 """
 
 
@@ -839,6 +932,7 @@ def write_registry():
             if v in "ges":
                 lines.append("int mbx_launch_%s_%s(const HolderArgs& A, int grid, int block, cudaStream_t s);" %
                              (name, v))
+                lines.append("int mbx_prime_%s_%s(cudaStream_t s);" % (name, v))
             elif v == "c":
                 lines.append("int mbx_launch_%s_c(const HolderArgs& A, const double* w, double* out, int grid, "
                              "int block, cudaStream_t s);" % name)
@@ -867,6 +961,7 @@ def write_registry():
                       spec.nvars, name, fn("g", "launch"), fn("e", "launch"), fn("c", "launch"),
                       fn("p", "launch"), fn("w", "launch"), fn("s", "launch"),
                       lit(MIXED_FP64_RADIUS.get(name, 0.0))))
+        lines.append("     %s, %s, %s," % (fn("g", "prime"), fn("e", "prime"), fn("s", "prime")))
         lines.append("     {%s, nullptr}}," % ", ".join(fn(v, "set_coef") for v in "gecpws"))
     lines.append("};")
     lines.append("static const int mbx_num_evaluators = %d;" % len(SPECS))

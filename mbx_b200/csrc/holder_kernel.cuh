@@ -47,6 +47,9 @@ struct HolderArgs {
     const int4* terms;         // (k, v0 | v1<<8 | v2<<16 | v3<<24 (255 = none), deg, unused)
     const double* tcoef;       // term multiplicities
     long nterms;
+    // code prefetch launch of a lockstep kernel (prime_passes > 0; see
+    // prime_pieces): of the rest only out (null) is read
+    int prime_passes, prime_npieces;
 };
 
 // Coefficient source: a global pointer, read through the read-only path.
@@ -299,6 +302,42 @@ struct SharedCoef {
     __device__ __forceinline__ double operator[](int k) const { return p[k]; }
 };
 
+// Code prefetch mode of the lockstep kernels.  Their trie is ~10^5
+// instructions of straight-line code.  Once other work has evicted it from
+// L2 (the rest of an MD step between two force calls), the first pass of
+// each SM through it waits on DRAM for every instruction fetch: ~0.4 ms of a
+// 1.3 ms FP64 evaluation of the 2048-water trimers, ~0.5 ms of the 0.8 ms
+// paired FP32 one.  An SM only gains from code that SMs of its own half of
+// the chip have fetched (one block through the whole trie beforehand
+// recovers half; a block on every SM, all of it).  A prefetch launch of the
+// same kernel (ptxas compiles a __noinline__ piece separately for every
+// kernel that calls it, so only the kernel's own launch fetches the code the
+// evaluation runs) has one warp per block run piece (block + j * grid) mod
+// npieces in pass j: every piece fetched by several SMs spread over the chip,
+// all pieces at once.  It is launched beside the n-mer search, ahead of the
+// evaluation.  The lanes' x and g columns share one [v][L] array (x at
+// columns 0-31, g at 32-63) of zeros; the results are discarded.
+template <int L, class V, class Piece>
+__device__ __forceinline__ void prime_pieces(const HolderArgs& A, int nvars, Piece&& piece) {
+    static_assert(L >= 64, "x and g columns of the prefetch overlap");
+    V* xs = reinterpret_cast<V*>(mbx_dyn_smem) + threadIdx.x;
+    V* gs = xs + 32;
+#pragma unroll 1
+    for (int v = 0; v < nvars; ++v) {
+        xs[v * L] = V(0);
+        gs[v * L] = V(0);
+    }
+    __syncwarp();
+    double sum = 0.0;
+#pragma unroll 1
+    for (int j = 0; j < A.prime_passes; ++j) {
+        const int k = (int)(((long)blockIdx.x + (long)j * gridDim.x) % A.prime_npieces);
+        sum += piece(k, xs, gs);
+        __syncwarp();
+    }
+    if (A.out) A.out[threadIdx.x] = sum;   // null in a prefetch launch; keeps the calls
+}
+
 // One n-mer per thread, all warps of a block in lockstep through the trie:
 // the straight-line polynomial is ~10^5 instructions, far more than the
 // instruction cache holds, so the block's warps go through it piece by piece
@@ -318,6 +357,20 @@ __global__ void __launch_bounds__(T::LOCK_THREADS, 1) holder_lock_kernel(const H
     if constexpr (T::SMEM_COEF && !CUSTOM) {
         for (int k = threadIdx.x; k < T::NCOEF; k += blockDim.x) s_coef[k] = CC{}[k];
         __syncthreads();
+    }
+    if constexpr (!CUSTOM) {
+        if (A.prime_passes > 0) {
+            prime_pieces<L, double>(A, T::NVARS, [&](int k, const double* x, double* g) -> double {
+                if constexpr (MODE == HM_ENERGY) {
+                    if constexpr (T::SMEM_COEF) return T::template pip_e_piece<L>(k, SharedCoef<CC>{s_coef}, x);
+                    else return T::template pip_e_piece<L>(k, CC{}, x);
+                } else {
+                    if constexpr (T::SMEM_COEF) return T::template pip_piece<L>(k, SharedCoef<CC>{s_coef}, x, g);
+                    else return T::template pip_piece<L>(k, CC{}, x, g);
+                }
+            });
+            return;
+        }
     }
     double acc[7] = {0, 0, 0, 0, 0, 0, 0};
     const long n = nmer_count(A);
@@ -422,11 +475,18 @@ __global__ void __launch_bounds__(T::LOCK_THREADS_S, 1) holder_pair_kernel(const
     __shared__ f2_t s_coef[T::NORB];
     for (int k = threadIdx.x; k < T::NORB; k += blockDim.x) s_coef[k] = CC{}.f2(k);
     __syncthreads();
+    const SharedPairs<CC> coef{s_coef};
+    if (A.prime_passes > 0) {
+        prime_pieces<L, f2_t>(A, T::NVARS, [&](int k, const f2_t* x, f2_t* g) -> double {
+            const double2 e = T::template pip_s32_piece<L>(k, coef, x, g);
+            return e.x + e.y;
+        });
+        return;
+    }
     double acc[7] = {0, 0, 0, 0, 0, 0, 0};
     const long n = nmer_count(A);
     const long chunk = 2L * blockDim.x;
     long static_next = blockIdx.x * chunk;
-    const SharedPairs<CC> coef{s_coef};
     for (;;) {
         long base;
         if (A.counter) {

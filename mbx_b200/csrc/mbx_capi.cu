@@ -26,6 +26,7 @@
 typedef int (*launch_fn)(const HolderArgs&, int, int, cudaStream_t);
 typedef int (*dcoef_fn)(const HolderArgs&, const double*, double*, int, int, cudaStream_t);
 typedef int (*poly_fn)(long, const double*, double*, double*, int, int, cudaStream_t);
+typedef int (*prime_fn)(cudaStream_t);
 typedef int (*warp_fn)(const HolderArgs&, int, int, cudaStream_t);
 typedef int (*setcoef_fn)(const double*, int, cudaStream_t);
 
@@ -43,6 +44,7 @@ struct EvaluatorInfo {
     warp_fn w;
     launch_fn s;      // FP32 kernel of the mixed mode (FP32 basis), or null
     double split_r;   // mixed mode: n-mers with first-atom distance below this run in FP64 (0: none)
+    prime_fn pg, pe, ps;   // code prefetch of the g, e and s kernels (holder_prime_kernel), or null
     setcoef_fn set[7];
 };
 
@@ -163,6 +165,9 @@ struct mbx_ctx {
     BuildScratch scratch[MBX_BUILD_LANES];   // [0]: every single-system search
     cudaStream_t lane_stream[MBX_BUILD_LANES] = {nullptr};   // [0] unused (the context stream)
     cudaEvent_t lane_fork = nullptr, lane_join[MBX_BUILD_LANES] = {nullptr};
+    // code prefetch of a term's evaluation kernels, beside its n-mer search
+    cudaStream_t prime_stream = nullptr;
+    cudaEvent_t prime_fork = nullptr, prime_join = nullptr;
     // mbx_energy_2b3b: the 2b term on a child context, kept in step with this
     // one (gen counts topology/configuration changes)
     mbx_ctx* child = nullptr;
@@ -251,6 +256,9 @@ int mbx_create(mbx_ctx** out, int device, void* stream) {
     for (int i = 0; i < 3; ++i) CUCHK(c, cudaEventCreate(&c->ev[i]));
     CUCHK(c, cudaEventCreateWithFlags(&c->lane_fork, cudaEventDisableTiming));
     CUCHK(c, cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
+    CUCHK(c, cudaStreamCreateWithFlags(&c->prime_stream, cudaStreamNonBlocking));
+    CUCHK(c, cudaEventCreateWithFlags(&c->prime_fork, cudaEventDisableTiming));
+    CUCHK(c, cudaEventCreateWithFlags(&c->prime_join, cudaEventDisableTiming));
     for (int i = 1; i < MBX_BUILD_LANES; ++i) {
         CUCHK(c, cudaStreamCreateWithFlags(&c->lane_stream[i], cudaStreamNonBlocking));
         CUCHK(c, cudaEventCreateWithFlags(&c->lane_join[i], cudaEventDisableTiming));
@@ -302,6 +310,12 @@ int mbx_destroy(mbx_ctx* c) {
     }
     if (c->lane_fork) cudaEventDestroy(c->lane_fork);
     if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+    if (c->prime_stream) {
+        cudaStreamSynchronize(c->prime_stream);
+        cudaStreamDestroy(c->prime_stream);
+    }
+    if (c->prime_fork) cudaEventDestroy(c->prime_fork);
+    if (c->prime_join) cudaEventDestroy(c->prime_join);
     if (c->child) mbx_destroy(c->child);
     c->buckets.release();
     c->list.release();
@@ -745,6 +759,33 @@ static int launch_eval(mbx_ctx* c, const EvaluatorInfo* E, HolderArgs A, int fla
     return MBX_OK;
 }
 
+// Code prefetch (holder_prime_kernel) of the evaluation kernels that a term's
+// buckets will launch, forked from the context stream onto the prime stream
+// so that it runs beside the n-mer search; prime_join marks its end and the
+// first evaluation waits for it.  Same kernel choice as launch_eval.
+static int launch_prime(mbx_ctx* c, int nbody, int flags, int* kernels) {
+    const bool grads = !(flags & MBX_NO_GRADS);
+    const bool mixed = (flags & MBX_MIXED) != 0;
+    prime_fn done[MBX_MAX_BUCKETS];
+    int ndone = 0;
+    CUCHK(c, cudaEventRecord(c->prime_fork, c->stream));
+    CUCHK(c, cudaStreamWaitEvent(c->prime_stream, c->prime_fork, 0));
+    for (int b = 0; b < c->nbucket[nbody]; ++b) {
+        const bool near = c->bucket_near[nbody][b];
+        if (near && !mixed) continue;
+        const EvaluatorInfo* E = c->bucket_eval[nbody][b];
+        if (E->w) continue;
+        const bool fp32 = mixed && !near && E->s;
+        const prime_fn fn = !grads ? E->pe : fp32 ? E->ps : E->pg;
+        if (!fn || std::find(done, done + ndone, fn) != done + ndone) continue;
+        done[ndone++] = fn;
+        RCHK(c, fn(c->prime_stream));
+        ++*kernels;
+    }
+    CUCHK(c, cudaEventRecord(c->prime_join, c->prime_stream));
+    return MBX_OK;
+}
+
 // Enqueues one term on the context's stream (n-mer build, evaluation, the
 // results copied to pinned memory), on device coordinates X (already
 // wrapped) accumulating into the device gradient G (NULL: energy only).
@@ -752,8 +793,11 @@ static int term_enqueue(mbx_ctx* c, int nbody, int use_ghost, double* X, double*
     const bool grads = !(flags & MBX_NO_GRADS);
     const bool mixed = (flags & MBX_MIXED) && grads;
     CUCHK(c, cudaEventRecord(c->ev[0], c->stream));
-    int r = launch_build(c, nbody, use_ghost, X, 0, kernels, mixed);
+    int r = launch_prime(c, nbody, flags, kernels);
     if (r) return r;
+    r = launch_build(c, nbody, use_ghost, X, 0, kernels, mixed);
+    if (r) return r;
+    CUCHK(c, cudaStreamWaitEvent(c->stream, c->prime_join, 0));
     CUCHK(c, cudaEventRecord(c->ev[1], c->stream));
     CUCHK(c, cudaMemsetAsync(c->out.p, 0, 16 * sizeof(double), c->stream));
     CUCHK(c, cudaMemsetAsync(c->counters.p, 0, MBX_MAX_BUCKETS * sizeof(int), c->stream));
@@ -1305,6 +1349,8 @@ static int batch_sequence(mbx_ctx* c, int nbody, double* X, double* G, bool grad
     }
     int r = prepare_buckets(c, nbody, c->nmon, 0);
     if (r) return r;
+    r = launch_prime(c, nbody, (mixed ? MBX_MIXED : 0) | (grads ? 0 : MBX_NO_GRADS), kernels);
+    if (r) return r;
     // the configurations' searches on MBX_BUILD_LANES streams (each with its
     // own scratch; configuration k on lane k mod lanes), joined before the
     // evaluation; they append to the same buckets through atomics
@@ -1323,6 +1369,7 @@ static int batch_sequence(mbx_ctx* c, int nbody, double* X, double* G, bool grad
         CUCHK(c, cudaEventRecord(c->lane_join[l], c->lane_stream[l]));
         CUCHK(c, cudaStreamWaitEvent(c->stream, c->lane_join[l], 0));
     }
+    CUCHK(c, cudaStreamWaitEvent(c->stream, c->prime_join, 0));
     CUCHK(c, cudaMemsetAsync(c->conf_out.p, 0, 8 * (size_t)c->nconf * sizeof(double), c->stream));
     CUCHK(c, cudaMemsetAsync(c->out.p, 0, 16 * sizeof(double), c->stream));
     CUCHK(c, cudaMemsetAsync(c->counters.p, 0, MBX_MAX_BUCKETS * sizeof(int), c->stream));
