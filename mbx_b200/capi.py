@@ -16,7 +16,8 @@ MBX_MIXED = 2
 MBX_NO_GRADS = 4
 MBX_GRAPH = 8
 
-EVALUATORS = ("mbpol2b", "mbpol3b", "ch4h2o2b", "ch4ch42b", "ch4h2o3b")
+EVALUATORS = ("mbpol2b", "mbpol3b", "ch4h2o2b", "ch4ch42b", "ch4h2o3b",
+              "h2oli2b", "h2ona2b", "h2ok2b", "h2orb2b", "h2ocs2b")
 
 
 class MBXError(RuntimeError):

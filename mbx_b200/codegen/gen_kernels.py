@@ -965,6 +965,12 @@ def write_registry():
         lines.append("     {%s, nullptr}}," % ", ".join(fn(v, "set_coef") for v in "gecpws"))
     lines.append("};")
     lines.append("static const int mbx_num_evaluators = %d;" % len(SPECS))
+    # real atoms per monomer id (SetUpMonomers, bblock/sys_tools.cpp:133-254)
+    from mbx_b200.specs import MONOMER_ATOMS
+    lines.append("struct MonomerInfo { const char* id; int nat; };")
+    lines.append("static const MonomerInfo mbx_monomers[] = {%s};" %
+                 ", ".join('{"%s", %d}' % (m, n) for m, n in MONOMER_ATOMS.items()))
+    lines.append("static const int mbx_num_monomers = %d;" % len(MONOMER_ATOMS))
     write_tu(os.path.join(OUT, "registry.inc"), "\n".join(lines) + "\n")
 
 

@@ -25,6 +25,7 @@ mbpol3b  potential/3b/poly-3b-v2x-nogrd.cpp:38 (eval(a, x))              36   11
 ch4h2o2b potential/2b/poly_2b_A1B2Z2_C1D4_deg3_exp0_v1.cpp:38             38   603
 ch4ch42b potential/2b/poly_2b_A1B4_A1B4_deg4_exp0_v1.cpp:44982 (+fmg1-15) 45   1345
 ch4h2o3b potential/3b/poly_3b_A1B4_C1D2_C1D2_deg3_nograd_v1.cpp:39        55   1254
+h2oion2b potential/2b/poly-2b-A1B2Z2_C-v1.cpp:38 (eval(nd, a, x))        8    429
 ======== ================================================================ ==== ====
 
 It also extracts the fitted linear coefficients (the model parameters) from
@@ -35,10 +36,14 @@ the evaluator classes:
 * ch4h2o2b: ``coefficients`` in potential/2b/x2b_A1B2Z2_C1D4_deg3_exp0_v1x.cpp:175
 * ch4ch42b: ``coefficients`` in potential/2b/x2b_A1B4_A1B4_deg4_exp0_v1x.cpp
 * ch4h2o3b: ``coefficients`` in potential/3b/mbnrg_3b_A1B4_C1D2_C1D2_deg3_v1.cpp
+* h2oli2b, h2ona2b, h2ok2b, h2orb2b, h2ocs2b (table h2oion2b): ``twobodyfit``
+  of the ion's constructor block in potential/2b/x2b-A1B2Z2_C-v1x.cpp:181
+  (li+), :628 (na+), :1075 (k+), :1522 (rb+), :1969 (cs+)
 
-Output (``mbx_b200/data/``): ``<name>.pip.gz`` (term table, gzip) and ``<name>.fit``
-(coefficients, one per line, printed with ``repr`` so they round-trip
-bit-exactly).
+Output (``mbx_b200/data/``): ``<table>.pip.gz`` (term table, gzip) and
+``<evaluator>.fit`` (coefficients, one per line, printed with ``repr`` so they
+round-trip bit-exactly); an evaluator's table is named after it unless
+several evaluators share one polynomial.
 
 Usage: ``python -m mbx_b200.codegen.pip_extract [--ref /root/reference]``
 """
@@ -58,6 +63,7 @@ PROGRAMS = {
     "ch4h2o2b": ("potential/2b/poly_2b_A1B2Z2_C1D4_deg3_exp0_v1.cpp", 38, 603, 3),
     "ch4ch42b": ("potential/2b/poly_2b_A1B4_A1B4_deg4_exp0_v1.cpp", 45, 1345, 4),
     "ch4h2o3b": ("potential/3b/poly_3b_A1B4_C1D2_C1D2_deg3_nograd_v1.cpp", 55, 1254, 3),
+    "h2oion2b": ("potential/2b/poly-2b-A1B2Z2_C-v1.cpp", 8, 429, 5),
 }
 
 FITS = {
@@ -67,6 +73,13 @@ FITS = {
     "ch4ch42b": ("potential/2b/x2b_A1B4_A1B4_deg4_exp0_v1x.cpp", r"coefficients\s*=\s*std::vector<double>\s*\{"),
     "ch4h2o3b": ("potential/3b/mbnrg_3b_A1B4_C1D2_C1D2_deg3_v1.cpp", r"coefficients\s*=\s*std::vector<double>\s*\{"),
 }
+_ION2B = "potential/2b/x2b-A1B2Z2_C-v1x.cpp"
+for _ion, _name in (("li", "h2oli2b"), ("na", "h2ona2b"), ("k", "h2ok2b"), ("rb", "h2orb2b"), ("cs", "h2ocs2b")):
+    FITS[_name] = (_ION2B, r'if \(mon1 == "h2o" && mon2 == "%s\+"\) \{\s*twobodyfit\s*=\s*std::vector<double>\s*\{' % _ion)
+
+# evaluator -> the program (table) its coefficients belong to
+TABLE_OF = {name: name for name in PROGRAMS if name in FITS}
+TABLE_OF.update({n: "h2oion2b" for n in ("h2oli2b", "h2ona2b", "h2ok2b", "h2orb2b", "h2ocs2b")})
 
 TOKEN = re.compile(
     r"\s*(?:(?P<num>\d+\.\d*(?:[eE][-+]?\d+)?|\d+(?:[eE][-+]?\d+)?)"
@@ -251,7 +264,7 @@ def extract_program(ref, name):
         bodies = function_bodies(text, ["fmg%d" % i for i in range(1, 16)])
         main = re.search(r"::eval\(const double a\[1345\], const double x\[45\]\)\s*\{(.*?)\n\}", text, re.S).group(1)
         bodies.append(main)
-    elif name == "mbpol2b":
+    elif name in ("mbpol2b", "h2oion2b"):
         m = re.search(r"for \(size_t nv = 0; nv < nd; nv\+\+\) \{(.*?)\n    \}\n    return energy;", text, re.S)
         bodies = [m.group(1)]
     else:
@@ -299,7 +312,7 @@ def extract_fit(ref, name, ncoef):
     return vals
 
 
-def write_tables(name, terms, fit, nvars, ncoef, degree):
+def write_table(name, terms, nvars, ncoef, degree):
     os.makedirs(DATA, exist_ok=True)
     with gzip.GzipFile(os.path.join(DATA, name + ".pip.gz"), "wb", mtime=0) as gz, \
             __import__("io").TextIOWrapper(gz) as f:
@@ -309,6 +322,10 @@ def write_tables(name, terms, fit, nvars, ncoef, degree):
             ci = int(c)
             cs = str(ci) if ci == c else repr(c)
             f.write("%d %s %d %s\n" % (k, cs, len(mono), " ".join(map(str, mono))))
+
+
+def write_fit(name, fit):
+    os.makedirs(DATA, exist_ok=True)
     with open(os.path.join(DATA, name + ".fit"), "w") as f:
         for v in fit:
             f.write(repr(v) + "\n")
@@ -323,11 +340,13 @@ def main(argv=None):
         t0 = time.time()
         rel, nvars, ncoef, degree = PROGRAMS[name]
         terms = extract_program(args.ref, name)
-        fit = extract_fit(args.ref, name, ncoef)
         used = sorted({t[0] for t in terms})
-        write_tables(name, terms, fit, nvars, ncoef, degree)
-        print("%-9s %6d terms, %4d/%d coefficients used, %.1fs" % (name, len(terms), len(used), ncoef,
-                                                                   time.time() - t0))
+        write_table(name, terms, nvars, ncoef, degree)
+        fits = [e for e, t in TABLE_OF.items() if t == name]
+        for e in fits:
+            write_fit(e, extract_fit(args.ref, e, ncoef))
+        print("%-9s %6d terms, %4d/%d coefficients used, fits %s, %.1fs" %
+              (name, len(terms), len(used), ncoef, ",".join(fits), time.time() - t0))
     return 0
 
 

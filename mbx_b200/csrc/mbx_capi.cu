@@ -466,10 +466,10 @@ extern "C" int mbx_set_topology(mbx_ctx* c, int nmon, const char* const* ids, co
     c->h_nat.resize(nmon);
     for (int m = 0; m < nmon; ++m) {
         std::string id = ids[m];
-        int nat;
-        if (id == "h2o") nat = 3;
-        else if (id == "ch4") nat = 5;
-        else return fail(c, MBX_ENOTSUP, "unknown monomer id " + id);
+        int nat = 0;
+        for (int k = 0; k < mbx_num_monomers; ++k)
+            if (id == mbx_monomers[k].id) nat = mbx_monomers[k].nat;
+        if (!nat) return fail(c, MBX_ENOTSUP, "unknown monomer id " + id);
         c->h_nat[m] = nat;
         int t = -1;
         for (int k = 0; k < c->ntypes; ++k)

@@ -64,6 +64,11 @@ class Spec:
     ncoef: int
     degree: int
     ref: str                   # reference evaluator (file:line)
+    table: str = ""            # PIP table in mbx_b200/data when shared by several evaluators ("": name)
+
+    @property
+    def pip_table(self):
+        return self.table or self.name
 
     @property
     def nbody(self):
@@ -239,19 +244,78 @@ CH4H2O3B = Spec(
     nvars=55, ncoef=1254, degree=3, ref="potential/3b/mbnrg_3b_A1B4_C1D2_C1D2_deg3_v1.cpp:1481",
 )
 
-SPECS = {s.name: s for s in (MBPOL2B, MBPOL3B, CH4H2O2B, CH4CH42B, CH4H2O3B)}
+# ---------------------------------------------------------------------------
+# Alkali-metal ion - water 2b: h2o_ion::x2b_h2o_ion_v2x(mon1 = "h2o", ion),
+# water first, potential/2b/x2b-A1B2Z2_C-v1x.cpp:2604-2770 (variables
+# :2637-2649; lone pairs from monomer::setup :121-135 with the MB-pol gammas;
+# switch f_switch :2418-2430 on the O-ion distance, dimers beyond r2f
+# skipped :2600).  One polynomial (poly_2b_h2o_ion_v1x, 8 variables, degree
+# 5, 429 coefficients) for all five ions; the non-linear constants, the
+# switch radii and the coefficients are per ion (constructor blocks
+# :181-625 li+, :628-1072 na+, :1075-1519 k+, :1522-1966 rb+, :1969-2413
+# cs+).
+# ---------------------------------------------------------------------------
+_S = ("O", "H1", "H2", "X", "Xp", "Xm")
+_ION2B = {
+    # ion: (k_HH_intra, k_OH_intra, k_XH_coul, k_XO_coul, k_xlp_main,
+    #       d_HH_intra, d_OH_intra, d_XH_coul, d_XO_coul, d_xlp_main, r2i, r2f)
+    "li+": (2.841179733353343e-01, 1.999999982813816e+00, 1.221694270779757e-01, 8.277382286185307e-01,
+            1.168420032277624e+00, 1.999965084185145e+00, 1.138547391709435e+00, 4.576629521685452e+00,
+            3.210235763647789e+00, 3.611985038328086e+00, 5.0, 6.0),
+    "na+": (7.823878977486063e-01, 1.999999957825146e+00, 7.950431747693237e-02, 6.680682051951390e-01,
+            8.311885364375440e-01, 1.999918468032695e+00, 5.269425988634360e-01, 6.287228652758436e+00,
+            6.242799339695940e+00, 3.872159916140287e+00, 5.5, 6.5),
+    "k+": (3.377427362895352e-01, 1.999994321311263e+00, 1.986401977927494e-01, 1.373943653398614e+00,
+           7.815071238402381e-01, 5.669440892013204e-01, 7.466617529933223e-01, 4.662999403661182e+00,
+           3.646598993078812e+00, 3.748049151082972e+00, 6.0, 7.0),
+    "rb+": (3.195475762417059e-01, 6.446164826239851e-01, 5.104027836124081e-01, 1.273907587244391e+00,
+            7.482531727951891e-01, 1.431386688762102e+00, 1.999530480711730e+00, 4.312600876869783e+00,
+            4.872074227770685e+00, 3.821777646259915e+00, 6.0, 7.0),
+    "cs+": (3.418356162428376e-01, 3.760948616075574e-01, 4.355574735817115e-01, 9.970388969117101e-01,
+            6.771893256000681e-01, 1.998465969152339e+00, 1.999745711872710e+00, 6.331169164351936e+00,
+            6.050756912670806e+00, 4.309622503190793e+00, 6.0, 7.0),
+}
+
+
+def _ion2b(ion, name):
+    kHH, kOH, kXH, kXO, kXL, dHH, dOH, dXH, dXO, dXL, ri, rf = _ION2B[ion]
+    tab = [("exp", "H1", "H2", kHH, dHH),
+           ("exp", "O", "H1", kOH, dOH), ("exp", "O", "H2", kOH, dOH),
+           ("coul", "X", "H1", kXH, dXH), ("coul", "X", "H2", kXH, dXH),
+           ("coul", "X", "O", kXO, dXO),
+           ("exp", "X", "Xp", kXL, dXL), ("exp", "X", "Xm", kXL, dXL)]
+    return Spec(name=name, monomers=("h2o", ion), nat=(3, 1), sites=_S, lp=((0, 0, 4, 5),),
+                variables=_vars(_S, tab), switch="pair", ri=ri, rf=rf, skip="pair_gt",
+                nvars=8, ncoef=429, degree=5, ref="potential/2b/x2b-A1B2Z2_C-v1x.cpp:2604", table="h2oion2b")
+
+
+H2OLI2B = _ion2b("li+", "h2oli2b")
+H2ONA2B = _ion2b("na+", "h2ona2b")
+H2OK2B = _ion2b("k+", "h2ok2b")
+H2ORB2B = _ion2b("rb+", "h2orb2b")
+H2OCS2B = _ion2b("cs+", "h2ocs2b")
+ALKALI = ("li+", "na+", "k+", "rb+", "cs+")
+
+SPECS = {s.name: s for s in (MBPOL2B, MBPOL3B, CH4H2O2B, CH4CH42B, CH4H2O3B,
+                             H2OLI2B, H2ONA2B, H2OK2B, H2ORB2B, H2OCS2B)}
 
 # Dispatch by sorted monomer ids (e2b::get_2b_energy, potential/2b/energy2b.cpp:
 # 240-254,258,282,323; e3b::get_3b_energy, potential/3b/energy3b.cpp:185-216,
 # 220,243).  Any other tuple evaluates to 0, as in the reference's else branch.
-DISPATCH_2B = {("h2o", "h2o"): "mbpol2b", ("ch4", "h2o"): "ch4h2o2b", ("ch4", "ch4"): "ch4ch42b"}
+DISPATCH_2B = {("h2o", "h2o"): "mbpol2b", ("ch4", "h2o"): "ch4h2o2b", ("ch4", "ch4"): "ch4ch42b",
+               ("h2o", "li+"): "h2oli2b", ("h2o", "na+"): "h2ona2b", ("h2o", "k+"): "h2ok2b",
+               ("h2o", "rb+"): "h2orb2b", ("cs+", "h2o"): "h2ocs2b"}
 DISPATCH_3B = {("h2o", "h2o", "h2o"): "mbpol3b", ("ch4", "h2o", "h2o"): "ch4h2o3b"}
 
 # Real atoms and total sites (real + electrostatic virtual sites) per monomer
 # type, as the reference's monomer table sets them (bblock/sys_tools.cpp
-# SetUpMonomers:133-254: h2o has 3 atoms + the M site, ch4 5 atoms).
-MONOMER_ATOMS = {"h2o": 3, "ch4": 5}
-MONOMER_SITES = {"h2o": 4, "ch4": 5}
+# SetUpMonomers:133-254: h2o has 3 atoms + the M site, ch4 5 atoms, the
+# alkali-metal ions one atom, :222-225).
+MONOMER_ATOMS = {"h2o": 3, "ch4": 5, "li+": 1, "na+": 1, "k+": 1, "rb+": 1, "cs+": 1}
+MONOMER_SITES = {"h2o": 4, "ch4": 5, "li+": 1, "na+": 1, "k+": 1, "rb+": 1, "cs+": 1}
+# atom names a caller passes to AddMonomer for each id (input order)
+MONOMER_ATOM_NAMES = {"h2o": ("O", "H", "H"), "ch4": ("C", "H", "H", "H", "H"), "li+": ("Li",), "na+": ("Na",),
+                      "k+": ("K",), "rb+": ("Rb",), "cs+": ("Cs",)}
 
 
 def check():

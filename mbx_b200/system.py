@@ -17,7 +17,7 @@ import json
 import numpy as np
 
 from . import capi
-from .specs import MONOMER_ATOMS
+from .specs import MONOMER_ATOM_NAMES, MONOMER_ATOMS
 from .topology import Topology
 
 
@@ -182,7 +182,7 @@ def from_arrays(ids, xyz, box=None, cutoff2b=9.0, cutoff3b=7.0, ignore_2b=(), ig
                 precision="fp64", context=None):
     """Builds an initialised System from monomer ids and input-order coordinates."""
     from .specs import MONOMER_ATOMS as NAT
-    names = {"h2o": ["O", "H", "H"], "ch4": ["C", "H", "H", "H", "H"]}
+    names = {m: list(v) for m, v in MONOMER_ATOM_NAMES.items()}
     s = System(device, context)
     xyz = np.asarray(xyz, np.float64).reshape(-1)
     off = 0

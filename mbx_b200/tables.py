@@ -32,6 +32,12 @@ class PipTable:
 
 @functools.lru_cache(maxsize=None)
 def load_pip(name):
+    """Term table of an evaluator (its shared table where it has one) or of a
+    table name.  var[t, :deg[t]] are the variables of term t; the array is
+    max(4, degree) wide."""
+    from .specs import SPECS
+    if name in SPECS:
+        name = SPECS[name].pip_table
     path = os.path.join(DATA, name + ".pip.gz")
     with gzip.open(path, "rt") as f:
         f.readline()
@@ -39,7 +45,7 @@ def load_pip(name):
         k = np.empty(nterms, np.int32)
         coef = np.empty(nterms, np.float64)
         deg = np.empty(nterms, np.int32)
-        var = np.full((nterms, 4), -1, np.int32)
+        var = np.full((nterms, max(4, degree)), -1, np.int32)
         for t, line in enumerate(f):
             p = line.split()
             k[t] = int(p[0])

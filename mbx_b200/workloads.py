@@ -68,6 +68,23 @@ def water_box(n_side=14, n_mol=2048, L=39.44, seed=0, jitter=0.3):
     return ["h2o"] * n_mol, xyz.reshape(-1), box
 
 
+def ion_water_box(ions, n_side=7, n_mol=256, L=19.72, seed=0, jitter=0.3):
+    """Water box of the water_box recipe in which the first len(ions) of the
+    picked lattice sites hold the given monomer ids (one-atom ions at the
+    site centre) instead of waters.  Input order: the ions, then the waters."""
+    rng = np.random.default_rng(seed)
+    s = L / n_side
+    g = (np.arange(n_side) + 0.5) * s - L / 2
+    lattice = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+    pick = rng.choice(len(lattice), size=n_mol, replace=False)
+    centres = lattice[pick] + rng.uniform(-jitter, jitter, size=(n_mol, 3))
+    ni = len(ions)
+    xyz = place(rng, water_body(), centres[ni:])
+    out = np.concatenate([centres[:ni].reshape(-1), xyz.reshape(-1)])
+    box = np.array([L, 0, 0, 0, L, 0, 0, 0, L], float)
+    return list(ions) + ["h2o"] * (n_mol - ni), out, box
+
+
 def water_256(seed=0):
     return water_box(7, 256, 19.72, seed)
 

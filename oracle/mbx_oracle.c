@@ -286,14 +286,14 @@ done:
 /* ---------------------------------------------------------------- the PIP */
 
 /* P(a, x) = sum_t a[k_t] * c_t * prod_{i < deg_t} x[v_t,i]; g (optional) gets
- * dP/dx (overwritten). */
+ * dP/dx (overwritten).  tv: tw variable slots per term (tw >= the degree). */
 double mbxo_pip_eval(int nvars, long nterms, const int *tk, const double *tc, const int *tdeg, const int *tv,
-                     const double *a, const double *x, double *g) {
+                     int tw, const double *a, const double *x, double *g) {
     double e = 0.0;
     if (g)
         for (int j = 0; j < nvars; ++j) g[j] = 0.0;
     for (long t = 0; t < nterms; ++t) {
-        const int *v = tv + 4 * t;
+        const int *v = tv + (long)tw * t;
         int deg = tdeg[t];
         double c = a[tk[t]] * tc[t];
         double m = c;
@@ -380,8 +380,8 @@ static void lp_grads(const double *g1, const double *g2, double gin, double gout
  * 9): accumulated; e_out (optional, n): switched energy per n-mer.
  * Returns the summed switched energy. */
 double mbxo_holder_eval(const mbxo_spec *s, long nterms, const int *tk, const double *tc, const int *tdeg,
-                        const int *tv, const double *a, long n, const double *xyz, double *grad, double *virial,
-                        double *e_out) {
+                        const int *tv, int tw, const double *a, long n, const double *xyz, double *grad,
+                        double *virial, double *e_out) {
     double etot = 0.0;
     double vir[6] = {0, 0, 0, 0, 0, 0};
     int first[3];
@@ -434,7 +434,7 @@ double mbxo_holder_eval(const mbxo_spec *s, long nterms, const int *tk, const do
             dv[v][1] = g1 * gg;
             dv[v][2] = g2 * gg;
         }
-        double ep = mbxo_pip_eval(s->nvars, nterms, tk, tc, tdeg, tv, a, x, grad ? gx : NULL);
+        double ep = mbxo_pip_eval(s->nvars, nterms, tk, tc, tdeg, tv, tw, a, x, grad ? gx : NULL);
         double sw, gsw[3];
         double sp[3], gp[3];
         if (!s->sw_triple) {
@@ -512,7 +512,7 @@ double mbxo_holder_eval(const mbxo_spec *s, long nterms, const int *tk, const do
  * the switched energy with respect to the linear coefficients).  out: ncoef
  * doubles (overwritten).  Returns 0 when the n-mer is skipped (row zero). */
 int mbxo_holder_dcoef(const mbxo_spec *s, int ncoef, long nterms, const int *tk, const double *tc, const int *tdeg,
-                      const int *tv, const double *xyz, double *out) {
+                      const int *tv, int tw, const double *xyz, double *out) {
     for (int k = 0; k < ncoef; ++k) out[k] = 0.0;
     int first[3];
     first[0] = 0;
@@ -555,7 +555,7 @@ int mbxo_holder_dcoef(const mbxo_spec *s, int ncoef, long nterms, const int *tk,
     }
     for (long t = 0; t < nterms; ++t) {
         double m = tc[t];
-        for (int i = 0; i < tdeg[t]; ++i) m *= x[tv[4 * t + i]];
+        for (int i = 0; i < tdeg[t]; ++i) m *= x[tv[(long)tw * t + i]];
         out[tk[t]] += m;
     }
     for (int k = 0; k < ncoef; ++k) out[k] *= sw;

@@ -63,7 +63,8 @@ _lib = None
 def lib():
     global _lib
     if _lib is None:
-        if not os.path.exists(LIB):
+        src = os.path.join(HERE, "mbx_oracle.c")
+        if not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(src):
             build()
         L = ctypes.CDLL(LIB)
         dp = ctypes.POINTER(ctypes.c_double)
@@ -75,12 +76,13 @@ def lib():
         L.mbxo_add_clusters.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int, dp, dp, dp, lp,
                                         ip, ctypes.c_int, lp, ctypes.c_long]
         L.mbxo_add_clusters.restype = ctypes.c_long
-        L.mbxo_pip_eval.argtypes = [ctypes.c_int, ctypes.c_long, ip, dp, ip, ip, dp, dp, dp]
+        L.mbxo_pip_eval.argtypes = [ctypes.c_int, ctypes.c_long, ip, dp, ip, ip, ctypes.c_int, dp, dp, dp]
         L.mbxo_pip_eval.restype = ctypes.c_double
-        L.mbxo_holder_eval.argtypes = [ctypes.POINTER(_Spec), ctypes.c_long, ip, dp, ip, ip, dp, ctypes.c_long, dp,
-                                       dp, dp, dp]
+        L.mbxo_holder_eval.argtypes = [ctypes.POINTER(_Spec), ctypes.c_long, ip, dp, ip, ip, ctypes.c_int, dp,
+                                       ctypes.c_long, dp, dp, dp, dp]
         L.mbxo_holder_eval.restype = ctypes.c_double
-        L.mbxo_holder_dcoef.argtypes = [ctypes.POINTER(_Spec), ctypes.c_int, ctypes.c_long, ip, dp, ip, ip, dp, dp]
+        L.mbxo_holder_dcoef.argtypes = [ctypes.POINTER(_Spec), ctypes.c_int, ctypes.c_long, ip, dp, ip, ip, ctypes.c_int,
+                                        dp, dp]
         L.mbxo_holder_dcoef.restype = ctypes.c_int
         L.mbxo_spec_size.restype = ctypes.c_long
         L.mbxo_holder_vars.argtypes = [ctypes.POINTER(_Spec), ctypes.c_long, dp, dp,
@@ -144,7 +146,7 @@ def pip_eval(name, a, x, want_grad=True):
     a = np.ascontiguousarray(a, np.float64)
     g = np.zeros(t.nvars) if want_grad else None
     e = lib().mbxo_pip_eval(t.nvars, t.nterms, _ip(t.k), _p(t.coef), _ip(t.deg), _ip(np.ascontiguousarray(t.var)),
-                            _p(a), _p(x), _p(g))
+                            t.var.shape[1], _p(a), _p(x), _p(g))
     return (e, g) if want_grad else e
 
 
@@ -161,7 +163,7 @@ def holder_eval(name, xyz, do_grads=True, a=None, per_nmer=False):
     vir = np.zeros(9)
     eper = np.zeros(n) if per_nmer else None
     e = lib().mbxo_holder_eval(ctypes.byref(c_spec(name)), t.nterms, _ip(t.k), _p(t.coef), _ip(t.deg),
-                               _ip(np.ascontiguousarray(t.var)), _p(a), n, _p(xyz), _p(grad),
+                               _ip(np.ascontiguousarray(t.var)), t.var.shape[1], _p(a), n, _p(xyz), _p(grad),
                                _p(vir) if do_grads else None, _p(eper))
     return e, grad, vir, eper
 
@@ -187,7 +189,7 @@ def holder_dcoef(name, xyz):
     out = np.zeros((len(xyz), s.ncoef))
     for i in range(len(xyz)):
         lib().mbxo_holder_dcoef(ctypes.byref(c_spec(name)), s.ncoef, t.nterms, _ip(t.k), _p(t.coef), _ip(t.deg),
-                                _ip(np.ascontiguousarray(t.var)), _p(xyz[i]), _p(out[i]))
+                                _ip(np.ascontiguousarray(t.var)), t.var.shape[1], _p(xyz[i]), _p(out[i]))
     return out
 
 

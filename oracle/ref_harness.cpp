@@ -34,6 +34,7 @@
 #include "potential/2b/poly_2b_A1B2Z2_C1D4_deg3_exp0_v1x.h"
 #include "potential/2b/poly_2b_A1B4_A1B4_deg4_exp0_v1x.h"
 #include "potential/3b/poly_3b_A1B4_C1D2_C1D2_deg3_v1.h"
+#include "potential/2b/poly-2b-A1B2Z2_C-v1x.h"
 
 namespace {
 
@@ -50,6 +51,11 @@ std::vector<std::string> split_ids(const char* ids) {
 std::vector<std::string> atom_names(const std::string& id) {
     if (id == "h2o") return {"O", "H", "H"};
     if (id == "ch4") return {"C", "H", "H", "H", "H"};
+    if (id == "li+") return {"Li"};
+    if (id == "na+") return {"Na"};
+    if (id == "k+") return {"K"};
+    if (id == "rb+") return {"Rb"};
+    if (id == "cs+") return {"Cs"};
     throw std::runtime_error("harness knows no atom names for monomer id " + id);
 }
 
@@ -178,7 +184,8 @@ double mbxref_get_3b(const char* m1, const char* m2, const char* m3, long nm, co
 }
 
 // Raw generated polynomials.  kind: 0 MB-pol 2b (31 vars), 1 MB-pol 3b (36),
-// 2 CH4-H2O 2b (38), 3 CH4-CH4 2b (45), 4 CH4-H2O-H2O 3b (55).
+// 2 CH4-H2O 2b (38), 3 CH4-CH4 2b (45), 4 CH4-H2O-H2O 3b (55), 5 alkali-ion -
+// water 2b (8).
 // One configuration per call; g may be NULL for energy only.
 double mbxref_poly(int kind, const double* a, const double* x, double* g) {
     switch (kind) {
@@ -208,6 +215,11 @@ double mbxref_poly(int kind, const double* a, const double* x, double* g) {
         case 4: {
             mbnrg_A1B4_C1D2_C1D2_deg3::poly_A1B4_C1D2_C1D2_deg3_v1 p;
             return g ? p.eval(x, a, g) : p.eval(x, a);
+        }
+        case 5: {
+            if (!g) return h2o_ion::poly_2b_h2o_ion_v1x::eval(1, a, x)[0];
+            for (int j = 0; j < 8; ++j) g[j] = 0.0;
+            return h2o_ion::poly_2b_h2o_ion_v1x::eval(1, a, x, g)[0];
         }
     }
     return 0.0;

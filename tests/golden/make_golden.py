@@ -10,6 +10,10 @@ reference checkout, default /root/reference) and writes ``tests/golden/*.json``:
   (x2b_A1B2Z2_C1D4_v1x :659-706, x2b_A1B4_A1B4_v1x :935-974,
   x2b_v9x :975-1018), ``unittest-poly-holder-3b.cpp`` (mbnrg_3b_A1B4_C1D2_C1D2
   :337-383, x3b-v2x :910-954);
+* alkali-ion - water 2b: ``unittest-energy2b.cpp`` (cs-h2o :166-236, li-h2o
+  :237-313), ``unittest-poly-holder-2b.cpp`` (x2b_h2o_ion_v2x :707-934, one
+  fixture per ion), ``unittest-poly-2b.cpp`` (poly_2b_A1B2Z2_C_deg5_v1x
+  :2327-2536);
 * polynomial goldens: ``unittest-poly-2b.cpp`` (poly_2b_v6x :2537-3012,
   poly_2b_A1B2Z2_C1D4_deg3_exp0_v1x :1581-1827, poly_2b_A1B4_A1B4_deg4_exp0_v1x
   :1828-2326), ``unittest-poly-3b.cpp`` (poly_3b_A1B4_C1D2_C1D2_deg3_v1
@@ -45,7 +49,12 @@ BLOCKS = [
     ("poly_ch4ch42b", "src/unittests/unittest-poly-2b.cpp", r'TEST_CASE\("poly_2b_A1B4_A1B4_deg4_exp0_v1x:struct"\)', None),
     ("poly_ch4h2o3b", "src/unittests/unittest-poly-3b.cpp", r'TEST_CASE\("poly_3b_A1B4_C1D2_C1D2_deg3_v1.h"\)', None),
     ("poly_mbpol3b", "src/unittests/unittest-poly-3b.cpp", r'TEST_CASE\("poly-3b-v2x::class"\)', None),
-]
+    # alkali-metal ion - water 2b
+    ("energy2b_cs_h2o", "src/unittests/unittest-energy2b.cpp", r'TEST_CASE\("energy2b::get_2b_energy"\)', r'SECTION\("cs-h2o"\)'),
+    ("energy2b_li_h2o", "src/unittests/unittest-energy2b.cpp", r'TEST_CASE\("energy2b::get_2b_energy"\)', r'SECTION\("li-h2o"\)'),
+    ("poly_h2oion2b", "src/unittests/unittest-poly-2b.cpp", r'TEST_CASE\(":poly_2b_A1B2Z2_C_deg5_v1x:struct"\)', None),
+] + [("holder2b_h2o_%s" % ion, "src/unittests/unittest-poly-holder-2b.cpp", r'TEST_CASE\("x2b_h2o_ion_v2x::struct"\)',
+      r'SECTION\("h2o-%s"\)' % ion) for ion in ("li", "na", "k", "rb", "cs")]
 
 SYSTEMS = [
     ("system_256_h2o_cubic_box", "timing/256_h2o_cubic_box"),

@@ -13,7 +13,7 @@ import pytest
 import mbx_oracle as mo
 from conftest import golden
 from mbx_b200 import system as msys, workloads
-from mbx_b200.specs import SPECS
+from mbx_b200.specs import ALKALI, SPECS
 from mbx_b200.tables import load_fit
 
 pytestmark = pytest.mark.gpu
@@ -42,7 +42,7 @@ def rel(a, b):
 
 
 # ------------------------------------------------------------------ polynomials
-STRAIGHT = ["mbpol2b", "mbpol3b", "ch4h2o2b", "ch4h2o3b"]
+STRAIGHT = ["mbpol2b", "mbpol3b", "ch4h2o2b", "ch4h2o3b", "h2oli2b", "h2ocs2b"]
 
 
 @pytest.mark.parametrize("name", STRAIGHT)
@@ -61,7 +61,8 @@ def test_poly_random_vs_oracle(ctx, name):
 
 
 @pytest.mark.parametrize("fixture,name", [("poly_mbpol2b", "mbpol2b"), ("poly_ch4h2o2b", "ch4h2o2b"),
-                                          ("poly_ch4h2o3b", "ch4h2o3b"), ("poly_mbpol3b", "mbpol3b")])
+                                          ("poly_ch4h2o3b", "ch4h2o3b"), ("poly_mbpol3b", "mbpol3b"),
+                                          ("poly_h2oion2b", "h2oli2b")])
 def test_poly_golden(ctx, fixture, name):
     gd = golden(fixture)
     nv = SPECS[name].nvars
@@ -83,6 +84,7 @@ def test_poly_golden(ctx, fixture, name):
 # ------------------------------------------------------------------ evaluators
 HOLDERS = [("holder2b_x2b_v9x", "mbpol2b"), ("holder2b_ch4_h2o", "ch4h2o2b"), ("holder2b_ch4_ch4", "ch4ch42b"),
            ("holder3b_x3b_v2x", "mbpol3b"), ("holder3b_ch4_h2o_h2o", "ch4h2o3b")]
+HOLDERS += [("holder2b_h2o_%s" % ion, "h2o%s2b" % ion) for ion in ("li", "na", "k", "rb", "cs")]
 
 
 @pytest.mark.parametrize("fixture,name", HOLDERS)
@@ -112,6 +114,8 @@ def random_nmers(name, n, seed=3):
     s = SPECS[name]
     rng = np.random.default_rng(seed)
     bodies = {"h2o": workloads.water_body(), "ch4": workloads.methane_body()}
+    for ion in ALKALI:
+        bodies[ion] = np.zeros((1, 3))
     out = []
     for _ in range(n):
         parts = []
@@ -244,6 +248,20 @@ def test_methane_water_box_mixed():
     """Mixed MB-nrg system (57 CH4 + 513 H2O): the water trimers go through the
     paired FP32 kernel, every CH4 type stays FP64."""
     ids, xyz, box = workloads.methane_water_box(seed=0)
+    compare_system(ids, xyz, box, 9.0, 7.0, mixed=True, lists=False)
+
+
+@pytest.mark.parametrize("ion", ALKALI)
+def test_ion_water_box(ion):
+    """256-site box with three alkali ions: the ion-water dimers through the
+    h2o-ion 2b kernels (FP64 in both modes), lists, energies, gradients and
+    virial against the oracle."""
+    ids, xyz, box = workloads.ion_water_box([ion] * 3, seed=1)
+    compare_system(ids, xyz, box, 9.0, 7.0)
+
+
+def test_ion_water_box_mixed():
+    ids, xyz, box = workloads.ion_water_box(["na+", "k+", "cs+"], seed=2)
     compare_system(ids, xyz, box, 9.0, 7.0, mixed=True, lists=False)
 
 

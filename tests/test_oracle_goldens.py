@@ -5,7 +5,8 @@ import pytest
 import mbx_oracle as mo
 from conftest import golden
 from mbx_b200.tables import load_fit, load_pip
-from mbx_b200.specs import SPECS, check
+from mbx_b200 import workloads
+from mbx_b200.specs import ALKALI, SPECS, check
 
 # the reference's unit tests use an absolute margin of 1e-6
 # (unittest-energy2b.cpp:45, tools/testutils.h:46-54); this oracle must do better
@@ -21,7 +22,7 @@ def test_specs_consistent():
 
 
 POLY = [("poly_mbpol2b", "mbpol2b"), ("poly_ch4h2o2b", "ch4h2o2b"), ("poly_ch4ch42b", "ch4ch42b"),
-        ("poly_ch4h2o3b", "ch4h2o3b"), ("poly_mbpol3b", "mbpol3b")]
+        ("poly_ch4h2o3b", "ch4h2o3b"), ("poly_mbpol3b", "mbpol3b"), ("poly_h2oion2b", "h2oli2b")]
 
 
 @pytest.mark.parametrize("fixture,name", POLY)
@@ -44,6 +45,17 @@ def test_poly_golden(fixture, name):
     np.testing.assert_allclose(gr, gexp[:nv], rtol=1e-8, atol=TOL)
 
 
+def test_poly_h2oion2b_six_configs():
+    g = golden("poly_h2oion2b")
+    a = np.array(g["a"])
+    x6 = np.array(g["x_6"]).reshape(8, 6)   # variable-major, nd = 6
+    gexp = np.array(g["g_6_expected"]).reshape(8, 6)
+    for i in range(6):
+        e, gr = mo.pip_eval("h2oli2b", a, x6[:, i])
+        assert abs(e - g["e_6_expected"][i]) < TOL * max(1.0, abs(e))
+        np.testing.assert_allclose(gr, gexp[:, i], rtol=1e-8, atol=TOL)
+
+
 def test_poly_mbpol2b_two_configs():
     g = golden("poly_mbpol2b")
     a = np.array(g["a"])
@@ -56,7 +68,7 @@ def test_poly_mbpol2b_two_configs():
 
 
 DISPATCH = ["energy2b_h2o_h2o", "energy2b_ch4_ch4", "energy2b_ch4_h2o", "energy3b_h2o_h2o_h2o",
-            "energy3b_ch4_h2o_h2o"]
+            "energy3b_ch4_h2o_h2o", "energy2b_cs_h2o", "energy2b_li_h2o"]
 
 
 @pytest.mark.parametrize("fixture", DISPATCH)
@@ -74,6 +86,7 @@ def test_dispatch_golden(fixture):
 
 HOLDERS = [("holder2b_x2b_v9x", "mbpol2b"), ("holder2b_ch4_h2o", "ch4h2o2b"), ("holder2b_ch4_ch4", "ch4ch42b"),
            ("holder3b_x3b_v2x", "mbpol3b"), ("holder3b_ch4_h2o_h2o", "ch4h2o3b")]
+HOLDERS += [("holder2b_h2o_%s" % ion, "h2o%s2b" % ion) for ion in ("li", "na", "k", "rb", "cs")]
 
 
 @pytest.mark.parametrize("fixture,name", HOLDERS)
@@ -104,3 +117,18 @@ def test_system_published_energies(fixture):
     e3 = s.energy(3, do_grads=False)
     assert abs(e2 - g["E2B"]) < 1e-10 * abs(g["E2B"]) + 1e-9 * 10
     assert abs(e3 - g["E3B"]) < 1e-9 * abs(g["E3B"]) + 1e-8
+
+
+@pytest.mark.parametrize("ion", ALKALI)
+def test_ion_water_2b_vs_reference(ion):
+    """Get2B of a 256-site box holding three alkali ions: the oracle against
+    the compiled reference (oracle/_ref), all pair types of the box."""
+    if not mo.RefSystem.available():
+        pytest.skip("reference library not built here")
+    ids, xyz, box = workloads.ion_water_box([ion] * (1 if ion == "na+" else 3), seed=1)
+    o = mo.OracleSystem(ids, xyz, box, 9.0, 7.0)
+    r = mo.RefSystem(ids, xyz, box, 9.0, 7.0)
+    e_o, e_r = o.energy(2), r.energy(2)
+    assert abs(e_o - e_r) < 1e-10 * abs(e_r)
+    np.testing.assert_allclose(o.real_grads(), r.real_grads(), rtol=0, atol=1e-8)
+    np.testing.assert_allclose(o.virial, r.virial(), rtol=1e-9, atol=1e-7)
