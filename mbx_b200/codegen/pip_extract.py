@@ -26,7 +26,12 @@ ch4h2o2b potential/2b/poly_2b_A1B2Z2_C1D4_deg3_exp0_v1.cpp:38             38   6
 ch4ch42b potential/2b/poly_2b_A1B4_A1B4_deg4_exp0_v1.cpp:44982 (+fmg1-15) 45   1345
 ch4h2o3b potential/3b/poly_3b_A1B4_C1D2_C1D2_deg3_nograd_v1.cpp:39        55   1254
 h2oion2b potential/2b/poly-2b-A1B2Z2_C-v1.cpp:38 (eval(nd, a, x))        8    429
+h2oion3b potential/3b/poly-3b-h2o-ion-v1x_deg4_filtered.cpp:39 (*)       21   1016
 ======== ================================================================ ==== ====
+
+(*) the only program of this polynomial computes value and gradient; the
+value is its ``double e = tN;``, and only the assignments tN depends on are
+expanded.
 
 It also extracts the fitted linear coefficients (the model parameters) from
 the evaluator classes:
@@ -39,6 +44,10 @@ the evaluator classes:
 * h2oli2b, h2ona2b, h2ok2b, h2orb2b, h2ocs2b (table h2oion2b): ``twobodyfit``
   of the ion's constructor block in potential/2b/x2b-A1B2Z2_C-v1x.cpp:181
   (li+), :628 (na+), :1075 (k+), :1522 (rb+), :1969 (cs+)
+* h2oli3b, h2ona3b, h2ok3b, h2orb3b, h2ocs3b (table h2oion3b): ``the_poly`` of
+  the ion's constructor block in
+  potential/3b/x3b-h2o-ion-v1x-deg4-filtered.cpp:485 (li+), :1522 (na+),
+  :2561 (k+), :3602 (rb+), :4639 (cs+)
 
 Output (``mbx_b200/data/``): ``<table>.pip.gz`` (term table, gzip) and
 ``<evaluator>.fit`` (coefficients, one per line, printed with ``repr`` so they
@@ -64,7 +73,10 @@ PROGRAMS = {
     "ch4ch42b": ("potential/2b/poly_2b_A1B4_A1B4_deg4_exp0_v1.cpp", 45, 1345, 4),
     "ch4h2o3b": ("potential/3b/poly_3b_A1B4_C1D2_C1D2_deg3_nograd_v1.cpp", 55, 1254, 3),
     "h2oion2b": ("potential/2b/poly-2b-A1B2Z2_C-v1.cpp", 8, 429, 5),
+    "h2oion3b": ("potential/3b/poly-3b-h2o-ion-v1x_deg4_filtered.cpp", 21, 1016, 4),
 }
+# programs whose value is a named temporary (value + gradient programs)
+RESULT_VAR = {"h2oion3b": r"double e = (t\d+)\s*;"}
 
 FITS = {
     "mbpol2b": ("potential/2b/x2b-v9x.cpp", r"const double thefit\[\]\s*=\s*\{"),
@@ -80,6 +92,10 @@ for _ion, _name in (("li", "h2oli2b"), ("na", "h2ona2b"), ("k", "h2ok2b"), ("rb"
 # evaluator -> the program (table) its coefficients belong to
 TABLE_OF = {name: name for name in PROGRAMS if name in FITS}
 TABLE_OF.update({n: "h2oion2b" for n in ("h2oli2b", "h2ona2b", "h2ok2b", "h2orb2b", "h2ocs2b")})
+_ION3B = "potential/3b/x3b-h2o-ion-v1x-deg4-filtered.cpp"
+for _ion in ("li", "na", "k", "rb", "cs"):
+    FITS["h2o%s3b" % _ion] = (_ION3B, r'\(m3 == "%s\+"\) \{\s*const double the_poly\[\]\s*=\s*\{' % _ion)
+    TABLE_OF["h2o%s3b" % _ion] = "h2oion3b"
 
 TOKEN = re.compile(
     r"\s*(?:(?P<num>\d+\.\d*(?:[eE][-+]?\d+)?|\d+(?:[eE][-+]?\d+)?)"
@@ -260,6 +276,7 @@ def extract_program(ref, name):
     rel, nvars, ncoef, degree = PROGRAMS[name]
     path = os.path.join(ref, "src", rel)
     text = strip_comments(open(path).read())
+    text = re.sub(r"#ifdef DEBUG.*?#endif", "", text, flags=re.S)
     if name == "ch4ch42b":
         bodies = function_bodies(text, ["fmg%d" % i for i in range(1, 16)])
         main = re.search(r"::eval\(const double a\[1345\], const double x\[45\]\)\s*\{(.*?)\n\}", text, re.S).group(1)
@@ -275,6 +292,8 @@ def extract_program(ref, name):
     env = {}
     parser = Parser(env, xindex_factory(rel))
     result = None
+    if name in RESULT_VAR:
+        return _terms(extract_result_var(bodies[0], RESULT_VAR[name], parser, env), rel, nvars, ncoef, degree)
     for body in bodies:
         for target, expr in statements(body):
             if target in ("fmg%d" % i for i in range(1, 16)):
@@ -288,6 +307,33 @@ def extract_program(ref, name):
                 env[target] = v
     if result is None:
         raise ValueError("no result expression found in %s" % rel)
+    return _terms(result, rel, nvars, ncoef, degree)
+
+
+def extract_result_var(body, pattern, parser, env):
+    """The polynomial a value + gradient program returns as ``double e = tN``:
+    the assignments tN depends on (transitively), expanded in program order."""
+    exprs = {}
+    order = []
+    for target, expr in statements(body):
+        if target != "<result>":
+            exprs[target] = expr
+            order.append(target)
+    root = re.search(pattern, body).group(1)
+    need, stack = set(), [root]
+    while stack:
+        t = stack.pop()
+        if t in need:
+            continue
+        need.add(t)
+        stack += [d.replace("[", "").replace("]", "") for d in re.findall(r"\bt\[?\d+\]?", exprs[t])]
+    for t in order:
+        if t in need:
+            env[t] = parser.parse(exprs[t])
+    return env[root]
+
+
+def _terms(result, rel, nvars, ncoef, degree):
     terms = []
     for (k, mono), c in result.items():
         if k < 0:

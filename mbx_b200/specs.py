@@ -296,16 +296,78 @@ H2ORB2B = _ion2b("rb+", "h2orb2b")
 H2OCS2B = _ion2b("cs+", "h2ocs2b")
 ALKALI = ("li+", "na+", "k+", "rb+", "cs+")
 
+# ---------------------------------------------------------------------------
+# Alkali-metal ion - water - water 3b: x3b_h2o_ion_v1x_deg4_filtered(ion),
+# waters first, potential/3b/x3b-h2o-ion-v1x-deg4-filtered.cpp:206-480
+# (variables :309-337, all exp(-k (r - r0)) = ``exp`` with d0 = r0;
+# f_switch :98-111 on the three first-atom distances, trimers with two of
+# them beyond r3f skipped :296).  One polynomial
+# (poly_3b_h2o_ion_v1x_deg4_filtered, 21 variables, degree 4, 1016
+# coefficients); constants and coefficients per ion (constructor blocks
+# :485-1521 li+, :1522-2560 na+, :2561-3601 k+, :3602-4638 rb+,
+# :4639-5677 cs+).
+# ---------------------------------------------------------------------------
+_S = ("Oa", "Ha1", "Ha2", "Ob", "Hb1", "Hb2", "X")
+_ION3B = {
+    # ion: (kOH_intra, dOH_intra, kHH_intra, dHH_intra, kHH, dHH, kOH, dOH,
+    #       kOO, dOO, kXH, dXH, kXO, dXO, r3i, r3f)
+    "li+": (3.699637401847997e-01, 1.068868829761452e+01, 1.679876695401232e-01, 1.975171570009532e+00,
+            1.684254969412778e-01, 1.129172172428989e+00, 9.935182415951276e-01, 4.802676630871010e+00,
+            8.505367453684953e-01, 9.078259767894229e+00, 4.576806684033723e-02, 3.739394864987378e+00,
+            1.919355248053607e-01, 6.346405495344363e+00, 0.0, 4.5),
+    "na+": (1.079285891981862e+00, 2.493557848672918e+00, -2.009859067711048e-01, 4.331575675326020e+00,
+            4.884318738475223e-01, 1.003637515624313e+01, 6.109404006641794e-01, 7.677682294461052e+00,
+            6.521263121174117e-01, 4.789256072989140e+00, 4.772422237444002e-02, 6.916712361001890e+00,
+            1.252130248577817e-01, 9.920052988243551e+00, 0.0, 4.5),
+    "k+": (5.465082839032473e-01, 3.154303998006160e+00, 1.505534948596776e+00, 9.488236920987529e+00,
+           5.669173309079441e-01, 1.023524681458323e+01, 7.149221098880705e-01, 5.287618686287184e+00,
+           5.877602499345129e-01, 4.432532991705378e+00, 4.399022736050681e-02, 1.561826519728719e+00,
+           4.772570648100866e-01, 3.541346877424266e+00, 0.0, 4.5),
+    "rb+": (2.571848425019958e-01, 7.619101258901348e-01, 4.935811847841025e+00, 2.117837104002506e+00,
+            6.641539139948633e-01, 1.127561151275100e+01, 8.262323078009421e-01, 6.835848274082730e+00,
+            4.657013878889721e-01, 7.037153931329832e+00, 1.973569678997551e-02, 6.299823660916497e-01,
+            3.504015211699528e-01, 1.112494982897995e+01, 0.0, 4.5),
+    "cs+": (8.068929184027878e-01, 2.035944886211303e-04, 2.343614900390014e-01, 5.101199357764126e-01,
+            2.580358900220996e-01, 7.186210165587381e+00, 7.063990540733522e-01, 1.142220902170943e+01,
+            2.374997393974423e-02, 3.021128948742693e+00, 4.022139878389860e-01, 8.914038895157681e+00,
+            5.995683887693093e-02, 2.398846003968965e+00, 0.0, 4.5),
+}
+
+
+def _ion3b(ion, name):
+    kOHi, dOHi, kHHi, dHHi, kHH, dHH, kOH, dOH, kOO, dOO, kXH, dXH, kXO, dXO, ri, rf = _ION3B[ion]
+    tab = [("Oa", "Ha1", kOHi, dOHi), ("Oa", "Ha2", kOHi, dOHi), ("Ha1", "Ha2", kHHi, dHHi),
+           ("Ob", "Hb1", kOHi, dOHi), ("Ob", "Hb2", kOHi, dOHi), ("Hb1", "Hb2", kHHi, dHHi),
+           ("Ha1", "Hb1", kHH, dHH), ("Ha1", "Hb2", kHH, dHH), ("Ha2", "Hb1", kHH, dHH), ("Ha2", "Hb2", kHH, dHH),
+           ("Oa", "Hb1", kOH, dOH), ("Oa", "Hb2", kOH, dOH), ("Ob", "Ha1", kOH, dOH), ("Ob", "Ha2", kOH, dOH),
+           ("Oa", "Ob", kOO, dOO),
+           ("Ha1", "X", kXH, dXH), ("Ha2", "X", kXH, dXH), ("Hb1", "X", kXH, dXH), ("Hb2", "X", kXH, dXH),
+           ("Oa", "X", kXO, dXO), ("Ob", "X", kXO, dXO)]
+    return Spec(name=name, monomers=("h2o", "h2o", ion), nat=(3, 3, 1), sites=_S, lp=(),
+                variables=_vars(_S, [("exp", a, b, k, d) for a, b, k, d in tab]),
+                switch="triple", ri=ri, rf=rf, skip="two_of_three_gt", nvars=21, ncoef=1016, degree=4,
+                ref="potential/3b/x3b-h2o-ion-v1x-deg4-filtered.cpp:206", table="h2oion3b")
+
+
+H2OLI3B = _ion3b("li+", "h2oli3b")
+H2ONA3B = _ion3b("na+", "h2ona3b")
+H2OK3B = _ion3b("k+", "h2ok3b")
+H2ORB3B = _ion3b("rb+", "h2orb3b")
+H2OCS3B = _ion3b("cs+", "h2ocs3b")
+
 SPECS = {s.name: s for s in (MBPOL2B, MBPOL3B, CH4H2O2B, CH4CH42B, CH4H2O3B,
-                             H2OLI2B, H2ONA2B, H2OK2B, H2ORB2B, H2OCS2B)}
+                             H2OLI2B, H2ONA2B, H2OK2B, H2ORB2B, H2OCS2B,
+                             H2OLI3B, H2ONA3B, H2OK3B, H2ORB3B, H2OCS3B)}
 
 # Dispatch by sorted monomer ids (e2b::get_2b_energy, potential/2b/energy2b.cpp:
-# 240-254,258,282,323; e3b::get_3b_energy, potential/3b/energy3b.cpp:185-216,
-# 220,243).  Any other tuple evaluates to 0, as in the reference's else branch.
+# 240-254,258-281,282,323; e3b::get_3b_energy, potential/3b/energy3b.cpp:185-216,
+# 220-228,243).  Any other tuple evaluates to 0, as in the reference's else branch.
 DISPATCH_2B = {("h2o", "h2o"): "mbpol2b", ("ch4", "h2o"): "ch4h2o2b", ("ch4", "ch4"): "ch4ch42b",
                ("h2o", "li+"): "h2oli2b", ("h2o", "na+"): "h2ona2b", ("h2o", "k+"): "h2ok2b",
                ("h2o", "rb+"): "h2orb2b", ("cs+", "h2o"): "h2ocs2b"}
-DISPATCH_3B = {("h2o", "h2o", "h2o"): "mbpol3b", ("ch4", "h2o", "h2o"): "ch4h2o3b"}
+DISPATCH_3B = {("h2o", "h2o", "h2o"): "mbpol3b", ("ch4", "h2o", "h2o"): "ch4h2o3b",
+               ("h2o", "h2o", "li+"): "h2oli3b", ("h2o", "h2o", "na+"): "h2ona3b", ("h2o", "h2o", "k+"): "h2ok3b",
+               ("h2o", "h2o", "rb+"): "h2orb3b", ("cs+", "h2o", "h2o"): "h2ocs3b"}
 
 # Real atoms and total sites (real + electrostatic virtual sites) per monomer
 # type, as the reference's monomer table sets them (bblock/sys_tools.cpp

@@ -35,6 +35,7 @@
 #include "potential/2b/poly_2b_A1B4_A1B4_deg4_exp0_v1x.h"
 #include "potential/3b/poly_3b_A1B4_C1D2_C1D2_deg3_v1.h"
 #include "potential/2b/poly-2b-A1B2Z2_C-v1x.h"
+#include "potential/3b/poly-3b-h2o-ion-v1x_deg4_filtered.h"
 
 namespace {
 
@@ -185,7 +186,7 @@ double mbxref_get_3b(const char* m1, const char* m2, const char* m3, long nm, co
 
 // Raw generated polynomials.  kind: 0 MB-pol 2b (31 vars), 1 MB-pol 3b (36),
 // 2 CH4-H2O 2b (38), 3 CH4-CH4 2b (45), 4 CH4-H2O-H2O 3b (55), 5 alkali-ion -
-// water 2b (8).
+// water 2b (8), 6 water - water - alkali-ion 3b (21).
 // One configuration per call; g may be NULL for energy only.
 double mbxref_poly(int kind, const double* a, const double* x, double* g) {
     switch (kind) {
@@ -220,6 +221,10 @@ double mbxref_poly(int kind, const double* a, const double* x, double* g) {
             if (!g) return h2o_ion::poly_2b_h2o_ion_v1x::eval(1, a, x)[0];
             for (int j = 0; j < 8; ++j) g[j] = 0.0;
             return h2o_ion::poly_2b_h2o_ion_v1x::eval(1, a, x, g)[0];
+        }
+        case 6: {
+            double gs[21];
+            return h2o_ion::poly_3b_h2o_ion_v1x_deg4_filtered::eval(a, x, g ? g : gs);
         }
     }
     return 0.0;

@@ -14,6 +14,10 @@ reference checkout, default /root/reference) and writes ``tests/golden/*.json``:
   :237-313), ``unittest-poly-holder-2b.cpp`` (x2b_h2o_ion_v2x :707-934, one
   fixture per ion), ``unittest-poly-2b.cpp`` (poly_2b_A1B2Z2_C_deg5_v1x
   :2327-2536);
+* water - water - alkali-ion 3b: ``unittest-energy3b.cpp`` (li-h2o-h2o
+  :146-357, cs-h2o-h2o :358-471), ``unittest-poly-holder-3b.cpp``
+  (x3b_h2o_ion_v1x_deg4_filtered :384-909, one fixture per ion),
+  ``unittest-poly-3b.cpp`` (poly_3b_h2o_ion_v1x_deg4_filtered :1350-1719);
 * polynomial goldens: ``unittest-poly-2b.cpp`` (poly_2b_v6x :2537-3012,
   poly_2b_A1B2Z2_C1D4_deg3_exp0_v1x :1581-1827, poly_2b_A1B4_A1B4_deg4_exp0_v1x
   :1828-2326), ``unittest-poly-3b.cpp`` (poly_3b_A1B4_C1D2_C1D2_deg3_v1
@@ -55,6 +59,15 @@ BLOCKS = [
     ("poly_h2oion2b", "src/unittests/unittest-poly-2b.cpp", r'TEST_CASE\(":poly_2b_A1B2Z2_C_deg5_v1x:struct"\)', None),
 ] + [("holder2b_h2o_%s" % ion, "src/unittests/unittest-poly-holder-2b.cpp", r'TEST_CASE\("x2b_h2o_ion_v2x::struct"\)',
       r'SECTION\("h2o-%s"\)' % ion) for ion in ("li", "na", "k", "rb", "cs")]
+# water - water - alkali-ion 3b
+BLOCKS += [
+    ("energy3b_li_h2o_h2o", "src/unittests/unittest-energy3b.cpp", r'TEST_CASE', r'SECTION\("li-h2o-h2o"\)'),
+    ("energy3b_cs_h2o_h2o", "src/unittests/unittest-energy3b.cpp", r'TEST_CASE', r'SECTION\("cs-h2o-h2o"\)'),
+    ("poly_h2oion3b", "src/unittests/unittest-poly-3b.cpp", r'TEST_CASE\("poly-3b-h2o-ion-v1x_deg4_filtered::class"\)',
+     None),
+] + [("holder3b_h2o_h2o_%s" % ion, "src/unittests/unittest-poly-holder-3b.cpp",
+      r'TEST_CASE\("x3b-3b-h2o-ion-v1x_deg4_filtered::class"\)', r'SECTION\("h2o-h2o-%s"\)' % ion)
+     for ion in ("li", "na", "k", "rb", "cs")]
 
 SYSTEMS = [
     ("system_256_h2o_cubic_box", "timing/256_h2o_cubic_box"),

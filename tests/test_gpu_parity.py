@@ -42,7 +42,7 @@ def rel(a, b):
 
 
 # ------------------------------------------------------------------ polynomials
-STRAIGHT = ["mbpol2b", "mbpol3b", "ch4h2o2b", "ch4h2o3b", "h2oli2b", "h2ocs2b"]
+STRAIGHT = ["mbpol2b", "mbpol3b", "ch4h2o2b", "ch4h2o3b", "h2oli2b", "h2ocs2b", "h2ona3b"]
 
 
 @pytest.mark.parametrize("name", STRAIGHT)
@@ -62,7 +62,7 @@ def test_poly_random_vs_oracle(ctx, name):
 
 @pytest.mark.parametrize("fixture,name", [("poly_mbpol2b", "mbpol2b"), ("poly_ch4h2o2b", "ch4h2o2b"),
                                           ("poly_ch4h2o3b", "ch4h2o3b"), ("poly_mbpol3b", "mbpol3b"),
-                                          ("poly_h2oion2b", "h2oli2b")])
+                                          ("poly_h2oion2b", "h2oli2b"), ("poly_h2oion3b", "h2oli3b")])
 def test_poly_golden(ctx, fixture, name):
     gd = golden(fixture)
     nv = SPECS[name].nvars
@@ -85,6 +85,7 @@ def test_poly_golden(ctx, fixture, name):
 HOLDERS = [("holder2b_x2b_v9x", "mbpol2b"), ("holder2b_ch4_h2o", "ch4h2o2b"), ("holder2b_ch4_ch4", "ch4ch42b"),
            ("holder3b_x3b_v2x", "mbpol3b"), ("holder3b_ch4_h2o_h2o", "ch4h2o3b")]
 HOLDERS += [("holder2b_h2o_%s" % ion, "h2o%s2b" % ion) for ion in ("li", "na", "k", "rb", "cs")]
+HOLDERS += [("holder3b_h2o_h2o_%s" % ion, "h2o%s3b" % ion) for ion in ("li", "na", "k", "rb", "cs")]
 
 
 @pytest.mark.parametrize("fixture,name", HOLDERS)
@@ -253,9 +254,9 @@ def test_methane_water_box_mixed():
 
 @pytest.mark.parametrize("ion", ALKALI)
 def test_ion_water_box(ion):
-    """256-site box with three alkali ions: the ion-water dimers through the
-    h2o-ion 2b kernels (FP64 in both modes), lists, energies, gradients and
-    virial against the oracle."""
+    """256-site box with three alkali ions: the ion-water dimers and the
+    water-water-ion trimers through the ion kernels (FP64 in both modes),
+    lists, energies, gradients and virial against the oracle."""
     ids, xyz, box = workloads.ion_water_box([ion] * 3, seed=1)
     compare_system(ids, xyz, box, 9.0, 7.0)
 

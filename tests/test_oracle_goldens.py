@@ -22,7 +22,8 @@ def test_specs_consistent():
 
 
 POLY = [("poly_mbpol2b", "mbpol2b"), ("poly_ch4h2o2b", "ch4h2o2b"), ("poly_ch4ch42b", "ch4ch42b"),
-        ("poly_ch4h2o3b", "ch4h2o3b"), ("poly_mbpol3b", "mbpol3b"), ("poly_h2oion2b", "h2oli2b")]
+        ("poly_ch4h2o3b", "ch4h2o3b"), ("poly_mbpol3b", "mbpol3b"), ("poly_h2oion2b", "h2oli2b"),
+        ("poly_h2oion3b", "h2oli3b")]
 
 
 @pytest.mark.parametrize("fixture,name", POLY)
@@ -68,7 +69,8 @@ def test_poly_mbpol2b_two_configs():
 
 
 DISPATCH = ["energy2b_h2o_h2o", "energy2b_ch4_ch4", "energy2b_ch4_h2o", "energy3b_h2o_h2o_h2o",
-            "energy3b_ch4_h2o_h2o", "energy2b_cs_h2o", "energy2b_li_h2o"]
+            "energy3b_ch4_h2o_h2o", "energy2b_cs_h2o", "energy2b_li_h2o", "energy3b_li_h2o_h2o",
+            "energy3b_cs_h2o_h2o"]
 
 
 @pytest.mark.parametrize("fixture", DISPATCH)
@@ -87,6 +89,7 @@ def test_dispatch_golden(fixture):
 HOLDERS = [("holder2b_x2b_v9x", "mbpol2b"), ("holder2b_ch4_h2o", "ch4h2o2b"), ("holder2b_ch4_ch4", "ch4ch42b"),
            ("holder3b_x3b_v2x", "mbpol3b"), ("holder3b_ch4_h2o_h2o", "ch4h2o3b")]
 HOLDERS += [("holder2b_h2o_%s" % ion, "h2o%s2b" % ion) for ion in ("li", "na", "k", "rb", "cs")]
+HOLDERS += [("holder3b_h2o_h2o_%s" % ion, "h2o%s3b" % ion) for ion in ("li", "na", "k", "rb", "cs")]
 
 
 @pytest.mark.parametrize("fixture,name", HOLDERS)
@@ -120,15 +123,18 @@ def test_system_published_energies(fixture):
 
 
 @pytest.mark.parametrize("ion", ALKALI)
-def test_ion_water_2b_vs_reference(ion):
-    """Get2B of a 256-site box holding three alkali ions: the oracle against
-    the compiled reference (oracle/_ref), all pair types of the box."""
+@pytest.mark.parametrize("nb", [2, 3])
+def test_ion_water_vs_reference(ion, nb):
+    """Get2B / Get3B of a 256-site box holding alkali ions: the oracle against
+    the compiled reference (oracle/_ref), every n-mer type of the box (one
+    Na+, whose Na+-Na+ pairs have a polynomial in the reference that is not
+    on this path; three of the others)."""
     if not mo.RefSystem.available():
         pytest.skip("reference library not built here")
     ids, xyz, box = workloads.ion_water_box([ion] * (1 if ion == "na+" else 3), seed=1)
     o = mo.OracleSystem(ids, xyz, box, 9.0, 7.0)
     r = mo.RefSystem(ids, xyz, box, 9.0, 7.0)
-    e_o, e_r = o.energy(2), r.energy(2)
+    e_o, e_r = o.energy(nb), r.energy(nb)
     assert abs(e_o - e_r) < 1e-10 * abs(e_r)
     np.testing.assert_allclose(o.real_grads(), r.real_grads(), rtol=0, atol=1e-8)
     np.testing.assert_allclose(o.virial, r.virial(), rtol=1e-9, atol=1e-7)
