@@ -491,7 +491,7 @@ def emit_traits(spec, table, straight, out):
     w("    static constexpr int NAT0 = %d, NAT1 = %d, NAT2 = %d;" % tuple(nat))
     w("    static constexpr int FIRST0 = %d, FIRST1 = %d, FIRST2 = %d;" % tuple(first))
     w("    static constexpr int SWITCH_TRIPLE = %d, SKIP = %d, STRAIGHT = %d, DEGREE = %d;" %
-      (1 if spec.switch == "triple" else 0, {"pair_gt": 0, "two_of_three_gt": 1, "all_three_gt": 2}[spec.skip],
+      ({"pair": 0, "triple": 1, "triple2": 2}[spec.switch], {"pair_gt": 0, "two_of_three_gt": 1, "all_three_gt": 2}[spec.skip],
        1 if straight else 0, spec.degree))
     w("    static constexpr double RI = %s, RF = %s;" % (lit(spec.ri), lit(spec.rf)))
     w("    static constexpr int LOCK_THREADS = %d;  // threads of a lockstep evaluation block" %

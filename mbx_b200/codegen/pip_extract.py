@@ -12,8 +12,9 @@ and writes the polynomial in the explicit form
 as a term table (one line per (k, m) pair).  The build's own CUDA generator
 (``gen_kernels.py``) and the oracle restatement (``oracle/mbx_oracle.c``)
 both work from these tables; neither contains any of the reference programs.
-The table is checked against the compiled reference polynomial in
-``tests/test_pip_tables.py``.
+Every table is checked against the compiled reference polynomial (value
+and gradient at random variables) in ``tests/test_oracle_goldens.py``
+(``test_table_vs_reference_program``).
 
 Programs parsed (file:line of the energy-only evaluator in the reference):
 
@@ -27,6 +28,8 @@ ch4ch42b potential/2b/poly_2b_A1B4_A1B4_deg4_exp0_v1.cpp:44982 (+fmg1-15) 45   1
 ch4h2o3b potential/3b/poly_3b_A1B4_C1D2_C1D2_deg3_nograd_v1.cpp:39        55   1254
 h2oion2b potential/2b/poly-2b-A1B2Z2_C-v1.cpp:38 (eval(nd, a, x))        8    429
 h2oion3b potential/3b/poly-3b-h2o-ion-v1x_deg4_filtered.cpp:39 (*)       21   1016
+halh2o2b potential/2b/poly_2b_A1_B1C2X2_deg6_nograd_v1.cpp:50             8    906
+halh2o3b potential/3b/poly_3b_A1_B1C2X2_B1C2X2_deg4_nograd_v1.cpp:50      41   3173
 ======== ================================================================ ==== ====
 
 (*) the only program of this polynomial computes value and gradient; the
@@ -48,6 +51,13 @@ the evaluator classes:
   the ion's constructor block in
   potential/3b/x3b-h2o-ion-v1x-deg4-filtered.cpp:485 (li+), :1522 (na+),
   :2561 (k+), :3602 (rb+), :4639 (cs+)
+* fh2o2b, clh2o2b, brh2o2b, ih2o2b (table halh2o2b): ``coefficients`` of the
+  halide's constructor block in potential/2b/mbnrg_2b_A1_B1C2X2_deg6_v1.cpp:12
+  (f-), :929 (cl-), :1846 (br-), :2763 (i-)
+* fh2o3b, clh2o3b, brh2o3b, ih2o3b (table halh2o3b): ``coefficients`` of the
+  halide's constructor block in
+  potential/3b/mbnrg_3b_A1_B1C2X2_B1C2X2_deg4_v1.cpp:13 (f-), :3204 (cl-),
+  :6395 (br-), :9586 (i-)
 
 Output (``mbx_b200/data/``): ``<table>.pip.gz`` (term table, gzip) and
 ``<evaluator>.fit`` (coefficients, one per line, printed with ``repr`` so they
@@ -74,6 +84,8 @@ PROGRAMS = {
     "ch4h2o3b": ("potential/3b/poly_3b_A1B4_C1D2_C1D2_deg3_nograd_v1.cpp", 55, 1254, 3),
     "h2oion2b": ("potential/2b/poly-2b-A1B2Z2_C-v1.cpp", 8, 429, 5),
     "h2oion3b": ("potential/3b/poly-3b-h2o-ion-v1x_deg4_filtered.cpp", 21, 1016, 4),
+    "halh2o2b": ("potential/2b/poly_2b_A1_B1C2X2_deg6_nograd_v1.cpp", 8, 906, 6),
+    "halh2o3b": ("potential/3b/poly_3b_A1_B1C2X2_B1C2X2_deg4_nograd_v1.cpp", 41, 3173, 4),
 }
 # programs whose value is a named temporary (value + gradient programs)
 RESULT_VAR = {"h2oion3b": r"double e = (t\d+)\s*;"}
@@ -96,6 +108,15 @@ _ION3B = "potential/3b/x3b-h2o-ion-v1x-deg4-filtered.cpp"
 for _ion in ("li", "na", "k", "rb", "cs"):
     FITS["h2o%s3b" % _ion] = (_ION3B, r'\(m3 == "%s\+"\) \{\s*const double the_poly\[\]\s*=\s*\{' % _ion)
     TABLE_OF["h2o%s3b" % _ion] = "h2oion3b"
+for _hal in ("f", "cl", "br", "i"):
+    FITS["%sh2o2b" % _hal] = ("potential/2b/mbnrg_2b_A1_B1C2X2_deg6_v1.cpp",
+                              r'if \(mon1 == "%s-" and mon2 == "h2o"\) \{\s*coefficients\s*=\s*std::vector<double>\s*\{'
+                              % _hal)
+    FITS["%sh2o3b" % _hal] = ("potential/3b/mbnrg_3b_A1_B1C2X2_B1C2X2_deg4_v1.cpp",
+                              r'if \(mon1 == "%s-" and mon2 == "h2o" and mon3 == "h2o"\) \{\s*coefficients\s*=\s*'
+                              r'std::vector<double>\s*\{' % _hal)
+    TABLE_OF["%sh2o2b" % _hal] = "halh2o2b"
+    TABLE_OF["%sh2o3b" % _hal] = "halh2o3b"
 
 TOKEN = re.compile(
     r"\s*(?:(?P<num>\d+\.\d*(?:[eE][-+]?\d+)?|\d+(?:[eE][-+]?\d+)?)"
@@ -236,17 +257,17 @@ ASSIGN = re.compile(r"(?:const\s+double\s+)?(t\d+|t\[\d+\])\s*=\s*([^;]*);", re.
 def statements(body):
     """Yield (target, expr) for assignments and ('<result>', expr) for the result."""
     for stmt in body.split(";"):
-        s = " ".join(stmt.split())
+        s = " ".join(stmt.split()).replace(" [", "[")
         if not s:
             continue
         m = re.fullmatch(r"(?:const double )?(t\d+|t\[\d+\]) = (.*)", s)
         if m:
             yield m.group(1).replace("[", "").replace("]", ""), m.group(2)
             continue
-        m = re.fullmatch(r"(?:return \(?|energy\[nv\] = )(.*)", s)
+        m = re.fullmatch(r"(?:return ?\(?|energy\[nv\] = )(.*)", s)
         if m and ("t" in m.group(1)):
             expr = m.group(1)
-            if s.startswith("return (") and expr.endswith(")") and expr.count("(") < expr.count(")"):
+            if re.match(r"return ?\(", s) and expr.endswith(")") and expr.count("(") < expr.count(")"):
                 expr = expr[:-1]
             yield "<result>", expr
 

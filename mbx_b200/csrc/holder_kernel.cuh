@@ -166,14 +166,16 @@ __device__ __forceinline__ double apply_switch(const double (&d)[3][3], const do
         }
         return sw;
     }
+    // SWITCH_TRIPLE 1: s0 s1 + s0 s2 + s1 s2; 2: the same minus 2 s0 s1 s2
     double g0, g1, g2;
     const double s0 = f_switch(rr[0], T::RI, T::RF, g0);
     const double s1 = f_switch(rr[1], T::RI, T::RF, g1);
     const double s2 = f_switch(rr[2], T::RI, T::RF, g2);
+    const double c = T::SWITCH_TRIPLE == 2 ? 2.0 : 0.0;
     if (grads) {
-        const double f0 = g0 * (s1 + s2) * ep / rr[0];
-        const double f1 = g1 * (s0 + s2) * ep / rr[1];
-        const double f2 = g2 * (s0 + s1) * ep / rr[2];
+        const double f0 = g0 * (s1 + s2 - c * s1 * s2) * ep / rr[0];
+        const double f1 = g1 * (s0 + s2 - c * s0 * s2) * ep / rr[1];
+        const double f2 = g2 * (s0 + s1 - c * s0 * s1) * ep / rr[2];
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
             tg[first[0]][c] += f0 * d[0][c] + f1 * d[1][c];
@@ -181,7 +183,7 @@ __device__ __forceinline__ double apply_switch(const double (&d)[3][3], const do
             tg[first[2]][c] -= f1 * d[1][c] + f2 * d[2][c];
         }
     }
-    return s0 * s1 + s0 * s2 + s1 * s2;
+    return s0 * s1 + s0 * s2 + s1 * s2 - c * s0 * s1 * s2;
 }
 
 // Adds v[0..7) into dst[0..7) (one configuration's energy and virial), one

@@ -34,6 +34,8 @@ Switches (cosine, ``f_switch``):
   x2b_A1B4_A1B4_deg4_exp0_v1x.cpp:1453-1466)
 * ``triple``: s12 s13 + s12 s23 + s13 s23 on the three first-atom distances
   (x3b-v2x.cpp:1275-1288,1690; mbnrg_3b_A1B4_C1D2_C1D2_deg3_v1.cpp:1318-1333)
+* ``triple2``: s12 s13 + s12 s23 + s13 s23 - 2 s12 s13 s23
+  (mbnrg_3b_A1_B1C2X2_B1C2X2_deg4_v1.cpp:12927,13127,13181-13183)
 
 Skip rules (n-mers not evaluated; their energy and gradient are exactly 0):
 * ``pair_gt``: r12 > rf  (x2b-v9x.cpp:1563)
@@ -56,7 +58,7 @@ class Spec:
     sites: Tuple[str, ...]     # real atoms in holder order, then virtual sites
     lp: Tuple[Tuple[int, int, int, int], ...]  # (monomer, first real site, X+ site, X- site)
     variables: Tuple[Tuple[str, int, int, float, float], ...]  # (kind, site1, site2, k, d0)
-    switch: str                # "pair" or "triple"
+    switch: str                # "pair", "triple" or "triple2"
     ri: float
     rf: float
     skip: str                  # "pair_gt", "two_of_three_gt", "all_three_gt"
@@ -355,29 +357,131 @@ H2OK3B = _ion3b("k+", "h2ok3b")
 H2ORB3B = _ion3b("rb+", "h2orb3b")
 H2OCS3B = _ion3b("cs+", "h2ocs3b")
 
+# ---------------------------------------------------------------------------
+# Halide - water 2b: mbnrg_A1_B1C2X2_deg6_v1(halide, "h2o"), halide first,
+# potential/2b/mbnrg_2b_A1_B1C2X2_deg6_v1.cpp:3789-3980 (variables
+# :3865-3872, tools/variable.cpp v_exp/v_coul with d0 = 0; MB-pol lone pairs
+# :3853-3856; f_switch :3685-3699 on the halide-O distance, dimers beyond ro
+# skipped :3810).  One polynomial (poly_A1_B1C2X2_deg6_v1, 8 variables,
+# degree 6, 906 coefficients); constants and coefficients per halide
+# (constructor blocks :12-927 f-, :929-1844 cl-, :1846-2761 br-,
+# :2763-3678 i-).
+# ---------------------------------------------------------------------------
+_S = ("A", "B", "C1", "C2", "X1", "X2")
+_HAL2B = {
+    # halide: (k_AB (coul), k_AC (coul), k_AX, k_BC intra, k_CC intra, ri, ro)
+    "f-": (6.235116852837913e-08, 3.545923893694392e-01, 3.507638336966289e-01, 4.131876960255009e-01,
+           3.616986527314591e-01, 5.3, 7.3),
+    "cl-": (4.434101301397339e-07, 3.581531291002636e-08, 3.220935488191130e-01, 2.809297687850453e-01,
+            3.015683487617984e-01, 5.8, 7.8),
+    "br-": (4.363632730909749e-06, 6.538608932949625e-07, 2.834802070784692e-01, 1.238561725021965e-01,
+            3.140346943732611e-01, 5.9, 7.9),
+    "i-": (7.590595972237534e-07, 3.470400079944597e-06, 2.480149059099078e-01, 3.002335368068454e-01,
+           2.183115173238724e-01, 6.2, 8.2),
+}
+
+
+def _hal2b(ion, name):
+    kAB, kAC, kAX, kBC, kCC, ri, ro = _HAL2B[ion]
+    tab = [("coul", "A", "B", kAB, 0.0), ("coul", "A", "C1", kAC, 0.0), ("coul", "A", "C2", kAC, 0.0),
+           ("exp", "A", "X1", kAX, 0.0), ("exp", "A", "X2", kAX, 0.0),
+           ("exp", "B", "C1", kBC, 0.0), ("exp", "B", "C2", kBC, 0.0), ("exp", "C1", "C2", kCC, 0.0)]
+    return Spec(name=name, monomers=(ion, "h2o"), nat=(1, 3), sites=_S, lp=((1, 1, 4, 5),),
+                variables=_vars(_S, tab), switch="pair", ri=ri, rf=ro, skip="pair_gt",
+                nvars=8, ncoef=906, degree=6, ref="potential/2b/mbnrg_2b_A1_B1C2X2_deg6_v1.cpp:3789",
+                table="halh2o2b")
+
+
+FH2O2B = _hal2b("f-", "fh2o2b")
+CLH2O2B = _hal2b("cl-", "clh2o2b")
+BRH2O2B = _hal2b("br-", "brh2o2b")
+IH2O2B = _hal2b("i-", "ih2o2b")
+HALIDES = ("f-", "cl-", "br-", "i-")
+
+# ---------------------------------------------------------------------------
+# Halide - water - water 3b: mbnrg_A1_B1C2X2_B1C2X2_deg4_v1(halide, "h2o",
+# "h2o"), halide first, potential/3b/mbnrg_3b_A1_B1C2X2_B1C2X2_deg4_v1.cpp:
+# 12956-13282 (variables :13072-13112, d0 = 0; MB-pol lone pairs on both
+# waters; switch ``triple2`` :13127; trimers with all three first-atom
+# distances beyond ro skipped :12990).  One polynomial
+# (poly_A1_B1C2X2_B1C2X2_deg4_v1, 41 variables, degree 4, 3173 coefficients);
+# constants and coefficients per halide (constructor blocks :13-3202 f-,
+# :3204-6393 cl-, :6395-9584 br-, :9586-12775 i-).
+# ---------------------------------------------------------------------------
+_S = ("A", "B1", "C1", "C2", "B2", "C3", "C4", "X1", "X2", "X3", "X4")
+_HAL3B = {
+    # halide: (kAB c, kAC c, kAX, kBB c, kBC intra, kBC c, kBX, kCC intra, kCC c, kCX, kXX, ri, ro)
+    "f-": (1.683174003900960e-02, 1.462488339952361e-01, 1.495490093533567e-01, 3.398373799669774e+00,
+           8.390335120106681e-01, 3.159841858407245e-09, 4.996257547423549e-01, 2.635206665339118e+00,
+           4.004058684253884e-02, 2.561129825500117e-01, 3.703274677292788e-01, 0.0, 5.8),
+    "cl-": (3.050780499728952e+00, 2.317377443605641e-02, 2.360729625543786e-01, 3.864106971541486e+00,
+            1.994298755795063e-01, 9.464531078609996e-02, 4.009804221983941e+00, 1.933213969741414e+00,
+            1.271399144654976e-01, 2.092270464467735e-01, 5.164915204892290e-01, 0.0, 5.8),
+    "br-": (4.934350368264340e-09, 8.053864705533755e-05, 1.767787145924113e-01, 4.808245301601014e+00,
+            3.132138118081313e-01, 1.315368607065956e+00, 6.791698758407823e-01, 6.865835071774395e+00,
+            6.324551383433107e-02, 2.549642769697353e-01, 2.245436992967047e+00, 0.0, 5.9),
+    "i-": (5.157227102182063e-09, 1.983825013735218e-06, 3.818504443080583e-01, 9.683345246557618e-02,
+           1.267839872255443e-01, 2.540217377512282e-01, 1.570538875818527e+00, 1.652271352978735e+00,
+           2.456950872841040e-02, 2.124956943635082e-01, 1.036383352473932e+00, 0.0, 6.0),
+}
+
+
+def _hal3b(ion, name):
+    kAB, kAC, kAX, kBB, kBCi, kBC, kBX, kCCi, kCC, kCX, kXX, ri, ro = _HAL3B[ion]
+    c, e = "coul", "exp"
+    tab = [(c, "A", "B1", kAB), (c, "A", "B2", kAB),
+           (c, "A", "C1", kAC), (c, "A", "C2", kAC), (c, "A", "C3", kAC), (c, "A", "C4", kAC),
+           (e, "A", "X1", kAX), (e, "A", "X2", kAX), (e, "A", "X3", kAX), (e, "A", "X4", kAX),
+           (c, "B1", "B2", kBB), (e, "B1", "C1", kBCi), (e, "B1", "C2", kBCi),
+           (c, "B1", "C3", kBC), (c, "B1", "C4", kBC), (e, "B1", "X3", kBX), (e, "B1", "X4", kBX),
+           (c, "B2", "C1", kBC), (c, "B2", "C2", kBC), (e, "B2", "C3", kBCi), (e, "B2", "C4", kBCi),
+           (e, "B2", "X1", kBX), (e, "B2", "X2", kBX),
+           (e, "C1", "C2", kCCi), (c, "C1", "C3", kCC), (c, "C1", "C4", kCC),
+           (e, "C1", "X3", kCX), (e, "C1", "X4", kCX),
+           (c, "C2", "C3", kCC), (c, "C2", "C4", kCC), (e, "C2", "X3", kCX), (e, "C2", "X4", kCX),
+           (e, "C3", "C4", kCCi), (e, "C3", "X1", kCX), (e, "C3", "X2", kCX), (e, "C4", "X1", kCX),
+           (e, "C4", "X2", kCX),
+           (e, "X1", "X3", kXX), (e, "X1", "X4", kXX), (e, "X2", "X3", kXX), (e, "X2", "X4", kXX)]
+    return Spec(name=name, monomers=(ion, "h2o", "h2o"), nat=(1, 3, 3), sites=_S, lp=((1, 1, 7, 8), (2, 4, 9, 10)),
+                variables=_vars(_S, [(kind, a, b, k, 0.0) for kind, a, b, k in tab]), switch="triple2",
+                ri=ri, rf=ro, skip="all_three_gt", nvars=41, ncoef=3173, degree=4,
+                ref="potential/3b/mbnrg_3b_A1_B1C2X2_B1C2X2_deg4_v1.cpp:12956", table="halh2o3b")
+
+
+FH2O3B = _hal3b("f-", "fh2o3b")
+CLH2O3B = _hal3b("cl-", "clh2o3b")
+BRH2O3B = _hal3b("br-", "brh2o3b")
+IH2O3B = _hal3b("i-", "ih2o3b")
+
 SPECS = {s.name: s for s in (MBPOL2B, MBPOL3B, CH4H2O2B, CH4CH42B, CH4H2O3B,
                              H2OLI2B, H2ONA2B, H2OK2B, H2ORB2B, H2OCS2B,
-                             H2OLI3B, H2ONA3B, H2OK3B, H2ORB3B, H2OCS3B)}
+                             H2OLI3B, H2ONA3B, H2OK3B, H2ORB3B, H2OCS3B,
+                             FH2O2B, CLH2O2B, BRH2O2B, IH2O2B, FH2O3B, CLH2O3B, BRH2O3B, IH2O3B)}
 
 # Dispatch by sorted monomer ids (e2b::get_2b_energy, potential/2b/energy2b.cpp:
 # 240-254,258-281,282,323; e3b::get_3b_energy, potential/3b/energy3b.cpp:185-216,
 # 220-228,243).  Any other tuple evaluates to 0, as in the reference's else branch.
 DISPATCH_2B = {("h2o", "h2o"): "mbpol2b", ("ch4", "h2o"): "ch4h2o2b", ("ch4", "ch4"): "ch4ch42b",
                ("h2o", "li+"): "h2oli2b", ("h2o", "na+"): "h2ona2b", ("h2o", "k+"): "h2ok2b",
-               ("h2o", "rb+"): "h2orb2b", ("cs+", "h2o"): "h2ocs2b"}
+               ("h2o", "rb+"): "h2orb2b", ("cs+", "h2o"): "h2ocs2b",
+               ("f-", "h2o"): "fh2o2b", ("cl-", "h2o"): "clh2o2b", ("br-", "h2o"): "brh2o2b", ("h2o", "i-"): "ih2o2b"}
 DISPATCH_3B = {("h2o", "h2o", "h2o"): "mbpol3b", ("ch4", "h2o", "h2o"): "ch4h2o3b",
                ("h2o", "h2o", "li+"): "h2oli3b", ("h2o", "h2o", "na+"): "h2ona3b", ("h2o", "h2o", "k+"): "h2ok3b",
-               ("h2o", "h2o", "rb+"): "h2orb3b", ("cs+", "h2o", "h2o"): "h2ocs3b"}
+               ("h2o", "h2o", "rb+"): "h2orb3b", ("cs+", "h2o", "h2o"): "h2ocs3b",
+               ("f-", "h2o", "h2o"): "fh2o3b", ("cl-", "h2o", "h2o"): "clh2o3b", ("br-", "h2o", "h2o"): "brh2o3b",
+               ("h2o", "h2o", "i-"): "ih2o3b"}
 
 # Real atoms and total sites (real + electrostatic virtual sites) per monomer
 # type, as the reference's monomer table sets them (bblock/sys_tools.cpp
 # SetUpMonomers:133-254: h2o has 3 atoms + the M site, ch4 5 atoms, the
-# alkali-metal ions one atom, :222-225).
-MONOMER_ATOMS = {"h2o": 3, "ch4": 5, "li+": 1, "na+": 1, "k+": 1, "rb+": 1, "cs+": 1}
-MONOMER_SITES = {"h2o": 4, "ch4": 5, "li+": 1, "na+": 1, "k+": 1, "rb+": 1, "cs+": 1}
+# alkali-metal and halide ions one atom, :221-225).
+MONOMER_ATOMS = {"h2o": 3, "ch4": 5, "li+": 1, "na+": 1, "k+": 1, "rb+": 1, "cs+": 1,
+                 "f-": 1, "cl-": 1, "br-": 1, "i-": 1}
+MONOMER_SITES = dict(MONOMER_ATOMS, h2o=4)
 # atom names a caller passes to AddMonomer for each id (input order)
 MONOMER_ATOM_NAMES = {"h2o": ("O", "H", "H"), "ch4": ("C", "H", "H", "H", "H"), "li+": ("Li",), "na+": ("Na",),
-                      "k+": ("K",), "rb+": ("Rb",), "cs+": ("Cs",)}
+                      "k+": ("K",), "rb+": ("Rb",), "cs+": ("Cs",), "f-": ("F",), "cl-": ("Cl",), "br-": ("Br",),
+                      "i-": ("I",)}
 
 
 def check():

@@ -324,7 +324,7 @@ typedef struct {
     int vkind[64];  /* 0 exp, 1 coul */
     int vs1[64], vs2[64];
     double vk[64], vd[64];
-    int sw_triple;  /* 0 pair, 1 triple */
+    int sw_triple;  /* 0 pair, 1 triple, 2 triple minus 2 s0 s1 s2 */
     double ri, rf;
     int skip;       /* 0 pair_gt, 1 two_of_three_gt, 2 all_three_gt */
     double gin, gout;
@@ -443,6 +443,7 @@ double mbxo_holder_eval(const mbxo_spec *s, long nterms, const int *tk, const do
         } else {
             for (int p = 0; p < 3; ++p) sp[p] = f_switch(r[p], s->ri, s->rf, &gp[p]);
             sw = sp[0] * sp[1] + sp[0] * sp[2] + sp[1] * sp[2];
+            if (s->sw_triple == 2) sw -= 2.0 * sp[0] * sp[1] * sp[2];
         }
         double es = sw * ep;
         etot += es;
@@ -471,9 +472,10 @@ double mbxo_holder_eval(const mbxo_spec *s, long nterms, const int *tk, const do
                 tg[first[1]][c] -= dd;
             }
         } else {
-            gsw[0] = gp[0] * (sp[1] + sp[2]) * ep / r[0];
-            gsw[1] = gp[1] * (sp[0] + sp[2]) * ep / r[1];
-            gsw[2] = gp[2] * (sp[0] + sp[1]) * ep / r[2];
+            double c2 = s->sw_triple == 2 ? 2.0 : 0.0;
+            gsw[0] = gp[0] * (sp[1] + sp[2] - c2 * sp[1] * sp[2]) * ep / r[0];
+            gsw[1] = gp[1] * (sp[0] + sp[2] - c2 * sp[0] * sp[2]) * ep / r[1];
+            gsw[2] = gp[2] * (sp[0] + sp[1] - c2 * sp[0] * sp[1]) * ep / r[2];
             for (int c = 0; c < 3; ++c) {
                 tg[first[0]][c] += gsw[0] * d[0][c] + gsw[1] * d[1][c];
                 tg[first[1]][c] += gsw[2] * d[2][c] - gsw[0] * d[0][c];
@@ -552,6 +554,7 @@ int mbxo_holder_dcoef(const mbxo_spec *s, int ncoef, long nterms, const int *tk,
     } else {
         for (int p = 0; p < 3; ++p) sp[p] = f_switch(r[p], s->ri, s->rf, &gp[p]);
         sw = sp[0] * sp[1] + sp[0] * sp[2] + sp[1] * sp[2];
+        if (s->sw_triple == 2) sw -= 2.0 * sp[0] * sp[1] * sp[2];
     }
     for (long t = 0; t < nterms; ++t) {
         double m = tc[t];

@@ -129,7 +129,7 @@ def c_spec(name):
         cs.vs2[v] = b
         cs.vk[v] = k
         cs.vd[v] = d0
-    cs.sw_triple = 1 if s.switch == "triple" else 0
+    cs.sw_triple = {"pair": 0, "triple": 1, "triple2": 2}[s.switch]
     cs.ri = s.ri
     cs.rf = s.rf
     cs.skip = {"pair_gt": 0, "two_of_three_gt": 1, "all_three_gt": 2}[s.skip]

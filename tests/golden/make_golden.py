@@ -14,6 +14,11 @@ reference checkout, default /root/reference) and writes ``tests/golden/*.json``:
   :237-313), ``unittest-poly-holder-2b.cpp`` (x2b_h2o_ion_v2x :707-934, one
   fixture per ion), ``unittest-poly-2b.cpp`` (poly_2b_A1B2Z2_C_deg5_v1x
   :2327-2536);
+* halide - water 2b / halide - water - water 3b: ``unittest-energy2b.cpp``
+  (f--h2o :1322, cl-h2o :1380, br-h2o :1438, i-h2o :1498),
+  ``unittest-energy3b.cpp`` (f-h2o-h2o :1010, cl- :1104, br- :1198, i- :1292),
+  ``unittest-poly-holder-2b.cpp`` (mbnrg_A1_B1C2X2_deg6_v1 sections :64-219),
+  ``unittest-poly-holder-3b.cpp`` (mbnrg_A1_B1C2X2_B1C2X2_deg4_v1 :174-336);
 * water - water - alkali-ion 3b: ``unittest-energy3b.cpp`` (li-h2o-h2o
   :146-357, cs-h2o-h2o :358-471), ``unittest-poly-holder-3b.cpp``
   (x3b_h2o_ion_v1x_deg4_filtered :384-909, one fixture per ion),
@@ -68,6 +73,18 @@ BLOCKS += [
 ] + [("holder3b_h2o_h2o_%s" % ion, "src/unittests/unittest-poly-holder-3b.cpp",
       r'TEST_CASE\("x3b-3b-h2o-ion-v1x_deg4_filtered::class"\)', r'SECTION\("h2o-h2o-%s"\)' % ion)
      for ion in ("li", "na", "k", "rb", "cs")]
+# halide - water 2b and halide - water - water 3b
+_HAL = (("f", "f--h2o", "f-h2o-h2o"), ("cl", "cl-h2o", "cl-h2o-h2o"), ("br", "br-h2o", "br-h2o-h2o"),
+        ("i", "i-h2o", "i-h2o-h2o"))
+BLOCKS += [("energy2b_%s_h2o" % h, "src/unittests/unittest-energy2b.cpp", r'TEST_CASE\("energy2b::get_2b_energy"\)',
+            r'SECTION\("%s"\)' % s2) for h, s2, _ in _HAL]
+BLOCKS += [("energy3b_%s_h2o_h2o" % h, "src/unittests/unittest-energy3b.cpp", r'TEST_CASE', r'SECTION\("%s"\)' % s3)
+           for h, _, s3 in _HAL]
+BLOCKS += [("holder2b_%s_h2o" % h, "src/unittests/unittest-poly-holder-2b.cpp",
+            r'TEST_CASE\("mbnrg_A1_B1C2X2_deg5_v1::struct"\)', r'SECTION\("%s--h2o"\)' % h) for h, _, _ in _HAL]
+BLOCKS += [("holder3b_%s_h2o_h2o" % h, "src/unittests/unittest-poly-holder-3b.cpp",
+            r'TEST_CASE\("mbnrg_A1_B1C2X2_B1C2X2_deg4_v1::struct"\)', r'SECTION\("%s--h2o-h2o"\)' % h)
+           for h, _, _ in _HAL]
 
 SYSTEMS = [
     ("system_256_h2o_cubic_box", "timing/256_h2o_cubic_box"),

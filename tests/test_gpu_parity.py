@@ -13,7 +13,7 @@ import pytest
 import mbx_oracle as mo
 from conftest import golden
 from mbx_b200 import system as msys, workloads
-from mbx_b200.specs import ALKALI, SPECS
+from mbx_b200.specs import ALKALI, HALIDES, SPECS
 from mbx_b200.tables import load_fit
 
 pytestmark = pytest.mark.gpu
@@ -86,6 +86,8 @@ HOLDERS = [("holder2b_x2b_v9x", "mbpol2b"), ("holder2b_ch4_h2o", "ch4h2o2b"), ("
            ("holder3b_x3b_v2x", "mbpol3b"), ("holder3b_ch4_h2o_h2o", "ch4h2o3b")]
 HOLDERS += [("holder2b_h2o_%s" % ion, "h2o%s2b" % ion) for ion in ("li", "na", "k", "rb", "cs")]
 HOLDERS += [("holder3b_h2o_h2o_%s" % ion, "h2o%s3b" % ion) for ion in ("li", "na", "k", "rb", "cs")]
+HOLDERS += [("holder2b_%s_h2o" % h, "%sh2o2b" % h) for h in ("f", "cl", "br", "i")]
+HOLDERS += [("holder3b_%s_h2o_h2o" % h, "%sh2o3b" % h) for h in ("f", "cl", "br", "i")]
 
 
 @pytest.mark.parametrize("fixture,name", HOLDERS)
@@ -115,7 +117,7 @@ def random_nmers(name, n, seed=3):
     s = SPECS[name]
     rng = np.random.default_rng(seed)
     bodies = {"h2o": workloads.water_body(), "ch4": workloads.methane_body()}
-    for ion in ALKALI:
+    for ion in ALKALI + HALIDES:
         bodies[ion] = np.zeros((1, 3))
     out = []
     for _ in range(n):
@@ -252,7 +254,7 @@ def test_methane_water_box_mixed():
     compare_system(ids, xyz, box, 9.0, 7.0, mixed=True, lists=False)
 
 
-@pytest.mark.parametrize("ion", ALKALI)
+@pytest.mark.parametrize("ion", ALKALI + HALIDES)
 def test_ion_water_box(ion):
     """256-site box with three alkali ions: the ion-water dimers and the
     water-water-ion trimers through the ion kernels (FP64 in both modes),
@@ -262,7 +264,7 @@ def test_ion_water_box(ion):
 
 
 def test_ion_water_box_mixed():
-    ids, xyz, box = workloads.ion_water_box(["na+", "k+", "cs+"], seed=2)
+    ids, xyz, box = workloads.ion_water_box(["na+", "cl-", "k+"], seed=2)
     compare_system(ids, xyz, box, 9.0, 7.0, mixed=True, lists=False)
 
 

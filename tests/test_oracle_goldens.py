@@ -6,7 +6,7 @@ import mbx_oracle as mo
 from conftest import golden
 from mbx_b200.tables import load_fit, load_pip
 from mbx_b200 import workloads
-from mbx_b200.specs import ALKALI, SPECS, check
+from mbx_b200.specs import ALKALI, HALIDES, SPECS, check
 
 # the reference's unit tests use an absolute margin of 1e-6
 # (unittest-energy2b.cpp:45, tools/testutils.h:46-54); this oracle must do better
@@ -71,6 +71,8 @@ def test_poly_mbpol2b_two_configs():
 DISPATCH = ["energy2b_h2o_h2o", "energy2b_ch4_ch4", "energy2b_ch4_h2o", "energy3b_h2o_h2o_h2o",
             "energy3b_ch4_h2o_h2o", "energy2b_cs_h2o", "energy2b_li_h2o", "energy3b_li_h2o_h2o",
             "energy3b_cs_h2o_h2o"]
+DISPATCH += ["energy2b_%s_h2o" % h for h in ("f", "cl", "br", "i")]
+DISPATCH += ["energy3b_%s_h2o_h2o" % h for h in ("f", "cl", "br", "i")]
 
 
 @pytest.mark.parametrize("fixture", DISPATCH)
@@ -90,6 +92,8 @@ HOLDERS = [("holder2b_x2b_v9x", "mbpol2b"), ("holder2b_ch4_h2o", "ch4h2o2b"), ("
            ("holder3b_x3b_v2x", "mbpol3b"), ("holder3b_ch4_h2o_h2o", "ch4h2o3b")]
 HOLDERS += [("holder2b_h2o_%s" % ion, "h2o%s2b" % ion) for ion in ("li", "na", "k", "rb", "cs")]
 HOLDERS += [("holder3b_h2o_h2o_%s" % ion, "h2o%s3b" % ion) for ion in ("li", "na", "k", "rb", "cs")]
+HOLDERS += [("holder2b_%s_h2o" % h, "%sh2o2b" % h) for h in ("f", "cl", "br", "i")]
+HOLDERS += [("holder3b_%s_h2o_h2o" % h, "%sh2o3b" % h) for h in ("f", "cl", "br", "i")]
 
 
 @pytest.mark.parametrize("fixture,name", HOLDERS)
@@ -122,16 +126,45 @@ def test_system_published_energies(fixture):
     assert abs(e3 - g["E3B"]) < 1e-9 * abs(g["E3B"]) + 1e-8
 
 
-@pytest.mark.parametrize("ion", ALKALI)
+# the reference's generated program for each extracted table (harness kind)
+REF_PROGRAM = {"mbpol2b": 0, "mbpol3b": 1, "ch4h2o2b": 2, "ch4ch42b": 3, "ch4h2o3b": 4, "h2oli2b": 5, "h2oli3b": 6,
+               "fh2o2b": 7, "fh2o3b": 8}
+
+
+@pytest.mark.parametrize("name", list(REF_PROGRAM))
+def test_table_vs_reference_program(name):
+    """The extracted term table (through the oracle's evaluation) against the
+    compiled reference program it came from, value and gradient at random
+    variables with the type's fitted coefficients (CH4-CH4: value only, the
+    reference ships no gradient program for it)."""
+    if not mo.RefSystem.available():
+        pytest.skip("reference library not built here")
+    nv = SPECS[name].nvars
+    a = load_fit(name)
+    rng = np.random.default_rng(11)
+    grad = name != "ch4ch42b"
+    for _ in range(4):
+        x = rng.uniform(0.05, 1.2, size=nv)
+        if grad:
+            e_r, g_r = mo.RefSystem.poly(REF_PROGRAM[name], a, x)
+            e_o, g_o = mo.pip_eval(name, a, x)
+            np.testing.assert_allclose(g_o, g_r, rtol=1e-9, atol=1e-9 * max(1.0, np.abs(g_r).max()))
+        else:
+            e_r = mo.RefSystem.poly(REF_PROGRAM[name], a, x, want_grad=False)
+            e_o = mo.pip_eval(name, a, x, want_grad=False)
+        assert abs(e_o - e_r) < 1e-9 * max(1.0, abs(e_r))
+
+
+@pytest.mark.parametrize("ion", ALKALI + HALIDES)
 @pytest.mark.parametrize("nb", [2, 3])
 def test_ion_water_vs_reference(ion, nb):
-    """Get2B / Get3B of a 256-site box holding alkali ions: the oracle against
-    the compiled reference (oracle/_ref), every n-mer type of the box (one
-    Na+, whose Na+-Na+ pairs have a polynomial in the reference that is not
+    """Get2B / Get3B of a 256-site box holding ions: the oracle against the
+    compiled reference (oracle/_ref), every n-mer type of the box (one Na+ or
+    Cl-, whose like-ion pairs have a polynomial in the reference that is not
     on this path; three of the others)."""
     if not mo.RefSystem.available():
         pytest.skip("reference library not built here")
-    ids, xyz, box = workloads.ion_water_box([ion] * (1 if ion == "na+" else 3), seed=1)
+    ids, xyz, box = workloads.ion_water_box([ion] * (1 if ion in ("na+", "cl-") else 3), seed=1)
     o = mo.OracleSystem(ids, xyz, box, 9.0, 7.0)
     r = mo.RefSystem(ids, xyz, box, 9.0, 7.0)
     e_o, e_r = o.energy(nb), r.energy(nb)
