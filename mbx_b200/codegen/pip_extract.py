@@ -30,6 +30,9 @@ h2oion2b potential/2b/poly-2b-A1B2Z2_C-v1.cpp:38 (eval(nd, a, x))        8    42
 h2oion3b potential/3b/poly-3b-h2o-ion-v1x_deg4_filtered.cpp:39 (*)       21   1016
 halh2o2b potential/2b/poly_2b_A1_B1C2X2_deg6_nograd_v1.cpp:50             8    906
 halh2o3b potential/3b/poly_3b_A1_B1C2X2_B1C2X2_deg4_nograd_v1.cpp:50      41   3173
+a1a12b   potential/2b/poly_2b_A1_A1_deg9_nograd_v1.cpp:50                 1    9
+a1b12b   potential/2b/poly_2b_A1_B1_deg9_nograd_v1.cpp:50                 1    9
+arh2o2b  potential/2b/poly_2b_A1_B1C2X2_deg5_nograd_v1.cpp:50             8    496
 ======== ================================================================ ==== ====
 
 (*) the only program of this polynomial computes value and gradient; the
@@ -58,6 +61,10 @@ the evaluator classes:
   halide's constructor block in
   potential/3b/mbnrg_3b_A1_B1C2X2_B1C2X2_deg4_v1.cpp:13 (f-), :3204 (cl-),
   :6395 (br-), :9586 (i-)
+* nana2b, clcl2b, arar2b (table a1a12b), nacl2b, csar2b (table a1b12b):
+  ``coefficients`` of the pair's block in potential/2b/mbnrg_2b_A1_A1_deg9_v1.cpp
+  :11 (na+ na+), :27 (cl- cl-), :43 (ar ar) and mbnrg_2b_A1_B1_deg9_v1.cpp :11
+  (na+ cl-), :27 (cs+ ar); arh2o2b: mbnrg_2b_A1_B1C2X2_deg5_v1.cpp:11
 
 Output (``mbx_b200/data/``): ``<table>.pip.gz`` (term table, gzip) and
 ``<evaluator>.fit`` (coefficients, one per line, printed with ``repr`` so they
@@ -86,6 +93,9 @@ PROGRAMS = {
     "h2oion3b": ("potential/3b/poly-3b-h2o-ion-v1x_deg4_filtered.cpp", 21, 1016, 4),
     "halh2o2b": ("potential/2b/poly_2b_A1_B1C2X2_deg6_nograd_v1.cpp", 8, 906, 6),
     "halh2o3b": ("potential/3b/poly_3b_A1_B1C2X2_B1C2X2_deg4_nograd_v1.cpp", 41, 3173, 4),
+    "a1a12b": ("potential/2b/poly_2b_A1_A1_deg9_nograd_v1.cpp", 1, 9, 9),
+    "a1b12b": ("potential/2b/poly_2b_A1_B1_deg9_nograd_v1.cpp", 1, 9, 9),
+    "arh2o2b": ("potential/2b/poly_2b_A1_B1C2X2_deg5_nograd_v1.cpp", 8, 496, 5),
 }
 # programs whose value is a named temporary (value + gradient programs)
 RESULT_VAR = {"h2oion3b": r"double e = (t\d+)\s*;"}
@@ -117,6 +127,16 @@ for _hal in ("f", "cl", "br", "i"):
                               r'std::vector<double>\s*\{' % _hal)
     TABLE_OF["%sh2o2b" % _hal] = "halh2o2b"
     TABLE_OF["%sh2o3b" % _hal] = "halh2o3b"
+for _m1, _m2, _name, _table, _file in (
+        ("na\\+", "na\\+", "nana2b", "a1a12b", "mbnrg_2b_A1_A1_deg9_v1.cpp"),
+        ("cl-", "cl-", "clcl2b", "a1a12b", "mbnrg_2b_A1_A1_deg9_v1.cpp"),
+        ("ar", "ar", "arar2b", "a1a12b", "mbnrg_2b_A1_A1_deg9_v1.cpp"),
+        ("na\\+", "cl-", "nacl2b", "a1b12b", "mbnrg_2b_A1_B1_deg9_v1.cpp"),
+        ("cs\\+", "ar", "csar2b", "a1b12b", "mbnrg_2b_A1_B1_deg9_v1.cpp"),
+        ("ar", "h2o", "arh2o2b", "arh2o2b", "mbnrg_2b_A1_B1C2X2_deg5_v1.cpp")):
+    FITS[_name] = ("potential/2b/" + _file, r'if \(mon1 == "%s" and mon2 == "%s"\) \{\s*coefficients\s*=\s*'
+                   r'std::vector<double>\s*\{' % (_m1, _m2))
+    TABLE_OF[_name] = _table
 
 TOKEN = re.compile(
     r"\s*(?:(?P<num>\d+\.\d*(?:[eE][-+]?\d+)?|\d+(?:[eE][-+]?\d+)?)"

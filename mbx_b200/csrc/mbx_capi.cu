@@ -130,6 +130,11 @@ struct BuildScratch {
     }
 };
 #define MBX_BUILD_LANES 4   // concurrent searches of a batch (streams + scratch sets)
+// pinned result block (h_out, 64 doubles): [0..7) term energy + virial, [8]
+// listed n-mers, then the bucket counts (ints) and the status words (2 ints)
+#define MBX_H_COUNTS 9
+#define MBX_H_STATUS (MBX_H_COUNTS + (MBX_MAX_BUCKETS + 1) / 2)
+static_assert(MBX_H_STATUS + 1 <= 64, "pinned result block too small");
 
 struct mbx_ctx {
     int device = 0;
@@ -823,9 +828,9 @@ static int term_enqueue(mbx_ctx* c, int nbody, int use_ghost, double* X, double*
     CUCHK(c, cudaMemcpyAsync(c->h_out, c->out.p, 8 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     CUCHK(c, cudaMemcpyAsync(c->h_out + 8, c->listed.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                              c->stream));
-    CUCHK(c, cudaMemcpyAsync(c->h_out + 9, c->bucket_count.p, MBX_MAX_BUCKETS * sizeof(int), cudaMemcpyDeviceToHost,
+    CUCHK(c, cudaMemcpyAsync(c->h_out + MBX_H_COUNTS, c->bucket_count.p, MBX_MAX_BUCKETS * sizeof(int), cudaMemcpyDeviceToHost,
                              c->stream));
-    CUCHK(c, cudaMemcpyAsync(c->h_out + 13, c->status.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CUCHK(c, cudaMemcpyAsync(c->h_out + MBX_H_STATUS, c->status.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     return MBX_OK;
 }
 
@@ -835,9 +840,9 @@ static int term_enqueue(mbx_ctx* c, int nbody, int use_ghost, double* X, double*
 // the counts and the timing recorded.
 static int term_finish(mbx_ctx* c, int nbody, double* energy, double* virial, int kernels) {
     int status[2];
-    memcpy(status, c->h_out + 13, sizeof(status));
+    memcpy(status, c->h_out + MBX_H_STATUS, sizeof(status));
     int counts[MBX_MAX_BUCKETS];
-    memcpy(counts, c->h_out + 9, sizeof(counts));
+    memcpy(counts, c->h_out + MBX_H_COUNTS, sizeof(counts));
     if (status[0]) {
         if (status[0] & MBX_STATUS_NB_OVERFLOW) c->nb_cap = std::max(c->nb_cap * 2, status[1] + 32);
         for (int b = 0; b < c->nbucket[nbody]; ++b)
@@ -1398,9 +1403,9 @@ static int batch_sequence(mbx_ctx* c, int nbody, double* X, double* G, bool grad
                              c->stream));
     CUCHK(c, cudaMemcpyAsync(c->h_out + 8, c->listed.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                              c->stream));
-    CUCHK(c, cudaMemcpyAsync(c->h_out + 9, c->bucket_count.p, MBX_MAX_BUCKETS * sizeof(int), cudaMemcpyDeviceToHost,
+    CUCHK(c, cudaMemcpyAsync(c->h_out + MBX_H_COUNTS, c->bucket_count.p, MBX_MAX_BUCKETS * sizeof(int), cudaMemcpyDeviceToHost,
                              c->stream));
-    CUCHK(c, cudaMemcpyAsync(c->h_out + 13, c->status.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CUCHK(c, cudaMemcpyAsync(c->h_out + MBX_H_STATUS, c->status.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     return MBX_OK;
 }
 
@@ -1408,9 +1413,9 @@ static int batch_sequence(mbx_ctx* c, int nbody, double* X, double* G, bool grad
 // the capacities are grown and 1 is returned (run it again).
 static int batch_check(mbx_ctx* c, int nbody) {
     int status[2];
-    memcpy(status, c->h_out + 13, sizeof(status));
+    memcpy(status, c->h_out + MBX_H_STATUS, sizeof(status));
     int counts[MBX_MAX_BUCKETS];
-    memcpy(counts, c->h_out + 9, sizeof(counts));
+    memcpy(counts, c->h_out + MBX_H_COUNTS, sizeof(counts));
     if (status[0]) {
         if (status[0] & MBX_STATUS_NB_OVERFLOW) c->nb_cap = std::max(c->nb_cap * 2, status[1] + 32);
         for (int b = 0; b < c->nbucket[nbody]; ++b) {

@@ -5,8 +5,8 @@
 
 #include "holder_common.cuh"
 
-#define MBX_MAX_TYPES 4
-#define MBX_MAX_BUCKETS 8
+#define MBX_MAX_TYPES 8     // monomer types of one topology
+#define MBX_MAX_BUCKETS 16  // evaluators (buckets) of one term
 
 // device status word bits (status[0]); status[1] holds the largest
 // neighbour count seen when MBX_STATUS_NB_OVERFLOW is set

@@ -257,7 +257,7 @@ CH4H2O3B = Spec(
 # :181-625 li+, :628-1072 na+, :1075-1519 k+, :1522-1966 rb+, :1969-2413
 # cs+).
 # ---------------------------------------------------------------------------
-_S = ("O", "H1", "H2", "X", "Xp", "Xm")
+_S_ION2B = ("O", "H1", "H2", "X", "Xp", "Xm")
 _ION2B = {
     # ion: (k_HH_intra, k_OH_intra, k_XH_coul, k_XO_coul, k_xlp_main,
     #       d_HH_intra, d_OH_intra, d_XH_coul, d_XO_coul, d_xlp_main, r2i, r2f)
@@ -286,8 +286,8 @@ def _ion2b(ion, name):
            ("coul", "X", "H1", kXH, dXH), ("coul", "X", "H2", kXH, dXH),
            ("coul", "X", "O", kXO, dXO),
            ("exp", "X", "Xp", kXL, dXL), ("exp", "X", "Xm", kXL, dXL)]
-    return Spec(name=name, monomers=("h2o", ion), nat=(3, 1), sites=_S, lp=((0, 0, 4, 5),),
-                variables=_vars(_S, tab), switch="pair", ri=ri, rf=rf, skip="pair_gt",
+    return Spec(name=name, monomers=("h2o", ion), nat=(3, 1), sites=_S_ION2B, lp=((0, 0, 4, 5),),
+                variables=_vars(_S_ION2B, tab), switch="pair", ri=ri, rf=rf, skip="pair_gt",
                 nvars=8, ncoef=429, degree=5, ref="potential/2b/x2b-A1B2Z2_C-v1x.cpp:2604", table="h2oion2b")
 
 
@@ -309,7 +309,7 @@ ALKALI = ("li+", "na+", "k+", "rb+", "cs+")
 # :485-1521 li+, :1522-2560 na+, :2561-3601 k+, :3602-4638 rb+,
 # :4639-5677 cs+).
 # ---------------------------------------------------------------------------
-_S = ("Oa", "Ha1", "Ha2", "Ob", "Hb1", "Hb2", "X")
+_S_ION3B = ("Oa", "Ha1", "Ha2", "Ob", "Hb1", "Hb2", "X")
 _ION3B = {
     # ion: (kOH_intra, dOH_intra, kHH_intra, dHH_intra, kHH, dHH, kOH, dOH,
     #       kOO, dOO, kXH, dXH, kXO, dXO, r3i, r3f)
@@ -345,8 +345,8 @@ def _ion3b(ion, name):
            ("Oa", "Ob", kOO, dOO),
            ("Ha1", "X", kXH, dXH), ("Ha2", "X", kXH, dXH), ("Hb1", "X", kXH, dXH), ("Hb2", "X", kXH, dXH),
            ("Oa", "X", kXO, dXO), ("Ob", "X", kXO, dXO)]
-    return Spec(name=name, monomers=("h2o", "h2o", ion), nat=(3, 3, 1), sites=_S, lp=(),
-                variables=_vars(_S, [("exp", a, b, k, d) for a, b, k, d in tab]),
+    return Spec(name=name, monomers=("h2o", "h2o", ion), nat=(3, 3, 1), sites=_S_ION3B, lp=(),
+                variables=_vars(_S_ION3B, [("exp", a, b, k, d) for a, b, k, d in tab]),
                 switch="triple", ri=ri, rf=rf, skip="two_of_three_gt", nvars=21, ncoef=1016, degree=4,
                 ref="potential/3b/x3b-h2o-ion-v1x-deg4-filtered.cpp:206", table="h2oion3b")
 
@@ -367,7 +367,7 @@ H2OCS3B = _ion3b("cs+", "h2ocs3b")
 # (constructor blocks :12-927 f-, :929-1844 cl-, :1846-2761 br-,
 # :2763-3678 i-).
 # ---------------------------------------------------------------------------
-_S = ("A", "B", "C1", "C2", "X1", "X2")
+_S_HAL2B = ("A", "B", "C1", "C2", "X1", "X2")
 _HAL2B = {
     # halide: (k_AB (coul), k_AC (coul), k_AX, k_BC intra, k_CC intra, ri, ro)
     "f-": (6.235116852837913e-08, 3.545923893694392e-01, 3.507638336966289e-01, 4.131876960255009e-01,
@@ -386,8 +386,8 @@ def _hal2b(ion, name):
     tab = [("coul", "A", "B", kAB, 0.0), ("coul", "A", "C1", kAC, 0.0), ("coul", "A", "C2", kAC, 0.0),
            ("exp", "A", "X1", kAX, 0.0), ("exp", "A", "X2", kAX, 0.0),
            ("exp", "B", "C1", kBC, 0.0), ("exp", "B", "C2", kBC, 0.0), ("exp", "C1", "C2", kCC, 0.0)]
-    return Spec(name=name, monomers=(ion, "h2o"), nat=(1, 3), sites=_S, lp=((1, 1, 4, 5),),
-                variables=_vars(_S, tab), switch="pair", ri=ri, rf=ro, skip="pair_gt",
+    return Spec(name=name, monomers=(ion, "h2o"), nat=(1, 3), sites=_S_HAL2B, lp=((1, 1, 4, 5),),
+                variables=_vars(_S_HAL2B, tab), switch="pair", ri=ri, rf=ro, skip="pair_gt",
                 nvars=8, ncoef=906, degree=6, ref="potential/2b/mbnrg_2b_A1_B1C2X2_deg6_v1.cpp:3789",
                 table="halh2o2b")
 
@@ -408,7 +408,7 @@ HALIDES = ("f-", "cl-", "br-", "i-")
 # constants and coefficients per halide (constructor blocks :13-3202 f-,
 # :3204-6393 cl-, :6395-9584 br-, :9586-12775 i-).
 # ---------------------------------------------------------------------------
-_S = ("A", "B1", "C1", "C2", "B2", "C3", "C4", "X1", "X2", "X3", "X4")
+_S_HAL3B = ("A", "B1", "C1", "C2", "B2", "C3", "C4", "X1", "X2", "X3", "X4")
 _HAL3B = {
     # halide: (kAB c, kAC c, kAX, kBB c, kBC intra, kBC c, kBX, kCC intra, kCC c, kCX, kXX, ri, ro)
     "f-": (1.683174003900960e-02, 1.462488339952361e-01, 1.495490093533567e-01, 3.398373799669774e+00,
@@ -442,11 +442,56 @@ def _hal3b(ion, name):
            (e, "C3", "C4", kCCi), (e, "C3", "X1", kCX), (e, "C3", "X2", kCX), (e, "C4", "X1", kCX),
            (e, "C4", "X2", kCX),
            (e, "X1", "X3", kXX), (e, "X1", "X4", kXX), (e, "X2", "X3", kXX), (e, "X2", "X4", kXX)]
-    return Spec(name=name, monomers=(ion, "h2o", "h2o"), nat=(1, 3, 3), sites=_S, lp=((1, 1, 7, 8), (2, 4, 9, 10)),
-                variables=_vars(_S, [(kind, a, b, k, 0.0) for kind, a, b, k in tab]), switch="triple2",
+    return Spec(name=name, monomers=(ion, "h2o", "h2o"), nat=(1, 3, 3), sites=_S_HAL3B,
+                lp=((1, 1, 7, 8), (2, 4, 9, 10)),
+                variables=_vars(_S_HAL3B, [(kind, a, b, k, 0.0) for kind, a, b, k in tab]), switch="triple2",
                 ri=ri, rf=ro, skip="all_three_gt", nvars=41, ncoef=3173, degree=4,
                 ref="potential/3b/mbnrg_3b_A1_B1C2X2_B1C2X2_deg4_v1.cpp:12956", table="halh2o3b")
 
+
+# ---------------------------------------------------------------------------
+# Atom - atom 2b (like ions, argon): mbnrg_A1_A1_deg9_v1(m, m) and
+# mbnrg_A1_B1_deg9_v1(a, b): one variable exp(k (d0 - r)) (variable::v_exp0,
+# tools/variable.cpp:49), a degree-9 polynomial, cosine switch 7 -> 9 A
+# (potential/2b/mbnrg_2b_A1_A1_deg9_v1.cpp:138-235, constructor blocks :11-25
+# na+, :27-41 cl-, :43-57 ar; potential/2b/mbnrg_2b_A1_B1_deg9_v1.cpp:121-220,
+# blocks :11-25 (na+, cl-), :27-41 (cs+, ar)).
+# ---------------------------------------------------------------------------
+_ATOM2B = {
+    # (first, second): (k, d0, ri, ro, name, table)
+    ("na+", "na+"): (4.380148617370266e-01, 7.568203895545039e+00, 7.0, 9.0, "nana2b", "a1a12b"),
+    ("cl-", "cl-"): (3.397551018612796e-01, 1.015131833802185e+01, 7.0, 9.0, "clcl2b", "a1a12b"),
+    ("ar", "ar"): (6.511296783204924e-01, 5.457946966470896e+00, 7.0, 9.0, "arar2b", "a1a12b"),
+    ("na+", "cl-"): (7.325513873941363e-01, 5.045021050700971e+00, 7.0, 9.0, "nacl2b", "a1b12b"),
+    ("cs+", "ar"): (7.020794887920050e-01, 5.319522241193717e+00, 7.0, 9.0, "csar2b", "a1b12b"),
+}
+
+
+def _atom2b(pair):
+    k, d0, ri, ro, name, table = _ATOM2B[pair]
+    src = "potential/2b/mbnrg_2b_A1_A1_deg9_v1.cpp:138" if table == "a1a12b" else \
+        "potential/2b/mbnrg_2b_A1_B1_deg9_v1.cpp:121"
+    return Spec(name=name, monomers=pair, nat=(1, 1), sites=("A", "B"), lp=(),
+                variables=_vars(("A", "B"), [("exp", "A", "B", k, d0)]), switch="pair", ri=ri, rf=ro,
+                skip="pair_gt", nvars=1, ncoef=9, degree=9, ref=src, table=table)
+
+
+ATOM2B = tuple(_atom2b(p) for p in _ATOM2B)
+
+# Argon - water 2b: mbnrg_A1_B1C2X2_deg5_v1("ar", "h2o"), argon first; the
+# halide-water template at degree 5 (potential/2b/mbnrg_2b_A1_B1C2X2_deg5_v1.cpp
+# :616-760, variables :684-691, switch 6 -> 8 A, constructor block :11-516).
+_k = (2.024685536820054e-07, 1.081497729997992e-01, 5.088638473248670e-01, 5.831588251891519e-01,
+      1.961512707948666e-01)
+ARH2O2B = Spec(
+    name="arh2o2b", monomers=("ar", "h2o"), nat=(1, 3), sites=_S_HAL2B, lp=((1, 1, 4, 5),),
+    variables=_vars(_S_HAL2B, [("coul", "A", "B", _k[0], 0.0), ("coul", "A", "C1", _k[1], 0.0),
+                         ("coul", "A", "C2", _k[1], 0.0), ("exp", "A", "X1", _k[2], 0.0),
+                         ("exp", "A", "X2", _k[2], 0.0), ("exp", "B", "C1", _k[3], 0.0),
+                         ("exp", "B", "C2", _k[3], 0.0), ("exp", "C1", "C2", _k[4], 0.0)]),
+    switch="pair", ri=6.0, rf=8.0, skip="pair_gt", nvars=8, ncoef=496, degree=5,
+    ref="potential/2b/mbnrg_2b_A1_B1C2X2_deg5_v1.cpp:616",
+)
 
 FH2O3B = _hal3b("f-", "fh2o3b")
 CLH2O3B = _hal3b("cl-", "clh2o3b")
@@ -456,7 +501,8 @@ IH2O3B = _hal3b("i-", "ih2o3b")
 SPECS = {s.name: s for s in (MBPOL2B, MBPOL3B, CH4H2O2B, CH4CH42B, CH4H2O3B,
                              H2OLI2B, H2ONA2B, H2OK2B, H2ORB2B, H2OCS2B,
                              H2OLI3B, H2ONA3B, H2OK3B, H2ORB3B, H2OCS3B,
-                             FH2O2B, CLH2O2B, BRH2O2B, IH2O2B, FH2O3B, CLH2O3B, BRH2O3B, IH2O3B)}
+                             FH2O2B, CLH2O2B, BRH2O2B, IH2O2B, FH2O3B, CLH2O3B, BRH2O3B, IH2O3B,
+                             ARH2O2B) + ATOM2B}
 
 # Dispatch by sorted monomer ids (e2b::get_2b_energy, potential/2b/energy2b.cpp:
 # 240-254,258-281,282,323; e3b::get_3b_energy, potential/3b/energy3b.cpp:185-216,
@@ -464,7 +510,9 @@ SPECS = {s.name: s for s in (MBPOL2B, MBPOL3B, CH4H2O2B, CH4CH42B, CH4H2O3B,
 DISPATCH_2B = {("h2o", "h2o"): "mbpol2b", ("ch4", "h2o"): "ch4h2o2b", ("ch4", "ch4"): "ch4ch42b",
                ("h2o", "li+"): "h2oli2b", ("h2o", "na+"): "h2ona2b", ("h2o", "k+"): "h2ok2b",
                ("h2o", "rb+"): "h2orb2b", ("cs+", "h2o"): "h2ocs2b",
-               ("f-", "h2o"): "fh2o2b", ("cl-", "h2o"): "clh2o2b", ("br-", "h2o"): "brh2o2b", ("h2o", "i-"): "ih2o2b"}
+               ("f-", "h2o"): "fh2o2b", ("cl-", "h2o"): "clh2o2b", ("br-", "h2o"): "brh2o2b", ("h2o", "i-"): "ih2o2b",
+               ("na+", "na+"): "nana2b", ("cl-", "cl-"): "clcl2b", ("ar", "ar"): "arar2b", ("cl-", "na+"): "nacl2b",
+               ("ar", "cs+"): "csar2b", ("ar", "h2o"): "arh2o2b"}
 DISPATCH_3B = {("h2o", "h2o", "h2o"): "mbpol3b", ("ch4", "h2o", "h2o"): "ch4h2o3b",
                ("h2o", "h2o", "li+"): "h2oli3b", ("h2o", "h2o", "na+"): "h2ona3b", ("h2o", "h2o", "k+"): "h2ok3b",
                ("h2o", "h2o", "rb+"): "h2orb3b", ("cs+", "h2o", "h2o"): "h2ocs3b",
@@ -474,14 +522,14 @@ DISPATCH_3B = {("h2o", "h2o", "h2o"): "mbpol3b", ("ch4", "h2o", "h2o"): "ch4h2o3
 # Real atoms and total sites (real + electrostatic virtual sites) per monomer
 # type, as the reference's monomer table sets them (bblock/sys_tools.cpp
 # SetUpMonomers:133-254: h2o has 3 atoms + the M site, ch4 5 atoms, the
-# alkali-metal and halide ions one atom, :221-225).
+# alkali-metal and halide ions and argon one atom, :210-225).
 MONOMER_ATOMS = {"h2o": 3, "ch4": 5, "li+": 1, "na+": 1, "k+": 1, "rb+": 1, "cs+": 1,
-                 "f-": 1, "cl-": 1, "br-": 1, "i-": 1}
+                 "f-": 1, "cl-": 1, "br-": 1, "i-": 1, "ar": 1}
 MONOMER_SITES = dict(MONOMER_ATOMS, h2o=4)
 # atom names a caller passes to AddMonomer for each id (input order)
 MONOMER_ATOM_NAMES = {"h2o": ("O", "H", "H"), "ch4": ("C", "H", "H", "H", "H"), "li+": ("Li",), "na+": ("Na",),
                       "k+": ("K",), "rb+": ("Rb",), "cs+": ("Cs",), "f-": ("F",), "cl-": ("Cl",), "br-": ("Br",),
-                      "i-": ("I",)}
+                      "i-": ("I",), "ar": ("Ar",)}
 
 
 def check():

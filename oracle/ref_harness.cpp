@@ -38,6 +38,9 @@
 #include "potential/3b/poly-3b-h2o-ion-v1x_deg4_filtered.h"
 #include "potential/2b/poly_2b_A1_B1C2X2_deg6_v1.h"
 #include "potential/3b/poly_3b_A1_B1C2X2_B1C2X2_deg4_v1.h"
+#include "potential/2b/poly_2b_A1_A1_deg9_v1.h"
+#include "potential/2b/poly_2b_A1_B1_deg9_v1.h"
+#include "potential/2b/poly_2b_A1_B1C2X2_deg5_v1.h"
 
 namespace {
 
@@ -63,6 +66,7 @@ std::vector<std::string> atom_names(const std::string& id) {
     if (id == "cl-") return {"Cl"};
     if (id == "br-") return {"Br"};
     if (id == "i-") return {"I"};
+    if (id == "ar") return {"Ar"};
     throw std::runtime_error("harness knows no atom names for monomer id " + id);
 }
 
@@ -193,7 +197,8 @@ double mbxref_get_3b(const char* m1, const char* m2, const char* m3, long nm, co
 // Raw generated polynomials.  kind: 0 MB-pol 2b (31 vars), 1 MB-pol 3b (36),
 // 2 CH4-H2O 2b (38), 3 CH4-CH4 2b (45), 4 CH4-H2O-H2O 3b (55), 5 alkali-ion -
 // water 2b (8), 6 water - water - alkali-ion 3b (21), 7 halide - water 2b (8),
-// 8 halide - water - water 3b (41).
+// 8 halide - water - water 3b (41), 9 like atoms 2b (1), 10 unlike atoms 2b (1),
+// 11 argon - water 2b (8).
 // One configuration per call; g may be NULL for energy only.
 double mbxref_poly(int kind, const double* a, const double* x, double* g) {
     switch (kind) {
@@ -243,6 +248,24 @@ double mbxref_poly(int kind, const double* a, const double* x, double* g) {
             mbnrg_A1_B1C2X2_B1C2X2_deg4::poly_A1_B1C2X2_B1C2X2_deg4_v1 p;
             if (!g) return p.eval(x, a);
             for (int j = 0; j < 41; ++j) g[j] = 0.0;
+            return p.eval(x, a, g);
+        }
+        case 9: {
+            mbnrg_A1_A1_deg9::poly_A1_A1_deg9_v1 p;
+            if (!g) return p.eval(x, a);
+            g[0] = 0.0;
+            return p.eval(x, a, g);
+        }
+        case 10: {
+            mbnrg_A1_B1_deg9::poly_A1_B1_deg9_v1 p;
+            if (!g) return p.eval(x, a);
+            g[0] = 0.0;
+            return p.eval(x, a, g);
+        }
+        case 11: {
+            mbnrg_A1_B1C2X2_deg5::poly_A1_B1C2X2_deg5_v1 p;
+            if (!g) return p.eval(x, a);
+            for (int j = 0; j < 8; ++j) g[j] = 0.0;
             return p.eval(x, a, g);
         }
     }

@@ -19,6 +19,11 @@ reference checkout, default /root/reference) and writes ``tests/golden/*.json``:
   ``unittest-energy3b.cpp`` (f-h2o-h2o :1010, cl- :1104, br- :1198, i- :1292),
   ``unittest-poly-holder-2b.cpp`` (mbnrg_A1_B1C2X2_deg6_v1 sections :64-219),
   ``unittest-poly-holder-3b.cpp`` (mbnrg_A1_B1C2X2_B1C2X2_deg4_v1 :174-336);
+* atom - atom 2b and argon - water 2b: ``unittest-energy2b.cpp`` (ar-ar :820,
+  cl-cl :867, na-na :914, ar-cs :965, na-cl :1012, ar-h2o :1063),
+  ``unittest-poly-holder-2b.cpp`` (mbnrg_A1_A1_deg9_v1 :1229-1312,
+  mbnrg_A1_B1_deg9_v1 :1313-1370, mbnrg_A1_B1C2X2_deg5_v1 ar-h2o :220),
+  ``unittest-poly-2b.cpp`` (poly_2b_A1_B1C2X2_deg5_v1 :53-204);
 * water - water - alkali-ion 3b: ``unittest-energy3b.cpp`` (li-h2o-h2o
   :146-357, cs-h2o-h2o :358-471), ``unittest-poly-holder-3b.cpp``
   (x3b_h2o_ion_v1x_deg4_filtered :384-909, one fixture per ion),
@@ -85,6 +90,17 @@ BLOCKS += [("holder2b_%s_h2o" % h, "src/unittests/unittest-poly-holder-2b.cpp",
 BLOCKS += [("holder3b_%s_h2o_h2o" % h, "src/unittests/unittest-poly-holder-3b.cpp",
             r'TEST_CASE\("mbnrg_A1_B1C2X2_B1C2X2_deg4_v1::struct"\)', r'SECTION\("%s--h2o-h2o"\)' % h)
            for h, _, _ in _HAL]
+# atom - atom 2b and argon - water 2b
+BLOCKS += [("energy2b_%s" % f, "src/unittests/unittest-energy2b.cpp", r'TEST_CASE\("energy2b::get_2b_energy"\)',
+            r'SECTION\("%s"\)' % sec) for f, sec in (("ar_ar", "ar-ar"), ("cl_cl", "cl-cl"), ("na_na", "na-na"),
+                                                      ("ar_cs", "ar-cs"), ("na_cl", "na-cl"), ("ar_h2o", "ar-h2o"))]
+BLOCKS += [("holder2b_%s" % f, "src/unittests/unittest-poly-holder-2b.cpp", r'TEST_CASE\("%s"\)' % tc,
+            r'SECTION\("%s"\)' % sec) for f, tc, sec in (
+    ("ar_ar", "mbnrg_A1_A1_deg9_v1::struct", "ar-ar"), ("cl_cl", "mbnrg_A1_A1_deg9_v1::struct", "cl-cl"),
+    ("na_na", "mbnrg_A1_A1_deg9_v1::struct", "na-na"), ("na_cl", "mbnrg_A1_B1_deg9_v1::struct", "na-cl"),
+    ("ar_cs", "mbnrg_A1_B1_deg9_v1::struct", "ar-cs"), ("ar_h2o", "mbnrg_A1_B1C2X2_deg5_v1::struct", "ar-h2o"))]
+BLOCKS += [("poly_arh2o2b", "src/unittests/unittest-poly-2b.cpp", r'TEST_CASE\(":poly_2b_A1_B1C2X2_deg5_v1:struct"\)',
+            None)]
 
 SYSTEMS = [
     ("system_256_h2o_cubic_box", "timing/256_h2o_cubic_box"),

@@ -88,6 +88,8 @@ HOLDERS += [("holder2b_h2o_%s" % ion, "h2o%s2b" % ion) for ion in ("li", "na", "
 HOLDERS += [("holder3b_h2o_h2o_%s" % ion, "h2o%s3b" % ion) for ion in ("li", "na", "k", "rb", "cs")]
 HOLDERS += [("holder2b_%s_h2o" % h, "%sh2o2b" % h) for h in ("f", "cl", "br", "i")]
 HOLDERS += [("holder3b_%s_h2o_h2o" % h, "%sh2o3b" % h) for h in ("f", "cl", "br", "i")]
+HOLDERS += [("holder2b_ar_ar", "arar2b"), ("holder2b_cl_cl", "clcl2b"), ("holder2b_na_na", "nana2b"),
+            ("holder2b_na_cl", "nacl2b"), ("holder2b_ar_cs", "csar2b"), ("holder2b_ar_h2o", "arh2o2b")]
 
 
 @pytest.mark.parametrize("fixture,name", HOLDERS)
@@ -117,7 +119,7 @@ def random_nmers(name, n, seed=3):
     s = SPECS[name]
     rng = np.random.default_rng(seed)
     bodies = {"h2o": workloads.water_body(), "ch4": workloads.methane_body()}
-    for ion in ALKALI + HALIDES:
+    for ion in ALKALI + HALIDES + ("ar",):
         bodies[ion] = np.zeros((1, 3))
     out = []
     for _ in range(n):
@@ -260,6 +262,16 @@ def test_ion_water_box(ion):
     water-water-ion trimers through the ion kernels (FP64 in both modes),
     lists, energies, gradients and virial against the oracle."""
     ids, xyz, box = workloads.ion_water_box([ion] * 3, seed=1)
+    compare_system(ids, xyz, box, 9.0, 7.0)
+
+
+@pytest.mark.parametrize("ions", [("na+", "cl-", "na+", "cl-", "na+", "cl-"), ("ar", "ar", "ar"),
+                                  ("cs+", "ar", "cs+", "ar"), ("li+", "f-", "k+", "br-")])
+def test_solution_box(ions):
+    """Salt solutions and argon in water: every pair type of the box (ion-ion
+    and atom-atom included) and the ion trimers on the GPU against the
+    oracle; five monomer types in the last one."""
+    ids, xyz, box = workloads.ion_water_box(list(ions), seed=4)
     compare_system(ids, xyz, box, 9.0, 7.0)
 
 

@@ -23,7 +23,7 @@ def test_specs_consistent():
 
 POLY = [("poly_mbpol2b", "mbpol2b"), ("poly_ch4h2o2b", "ch4h2o2b"), ("poly_ch4ch42b", "ch4ch42b"),
         ("poly_ch4h2o3b", "ch4h2o3b"), ("poly_mbpol3b", "mbpol3b"), ("poly_h2oion2b", "h2oli2b"),
-        ("poly_h2oion3b", "h2oli3b")]
+        ("poly_h2oion3b", "h2oli3b"), ("poly_arh2o2b", "arh2o2b")]
 
 
 @pytest.mark.parametrize("fixture,name", POLY)
@@ -73,6 +73,7 @@ DISPATCH = ["energy2b_h2o_h2o", "energy2b_ch4_ch4", "energy2b_ch4_h2o", "energy3
             "energy3b_cs_h2o_h2o"]
 DISPATCH += ["energy2b_%s_h2o" % h for h in ("f", "cl", "br", "i")]
 DISPATCH += ["energy3b_%s_h2o_h2o" % h for h in ("f", "cl", "br", "i")]
+DISPATCH += ["energy2b_%s" % p for p in ("ar_ar", "cl_cl", "na_na", "ar_cs", "na_cl", "ar_h2o")]
 
 
 @pytest.mark.parametrize("fixture", DISPATCH)
@@ -94,6 +95,8 @@ HOLDERS += [("holder2b_h2o_%s" % ion, "h2o%s2b" % ion) for ion in ("li", "na", "
 HOLDERS += [("holder3b_h2o_h2o_%s" % ion, "h2o%s3b" % ion) for ion in ("li", "na", "k", "rb", "cs")]
 HOLDERS += [("holder2b_%s_h2o" % h, "%sh2o2b" % h) for h in ("f", "cl", "br", "i")]
 HOLDERS += [("holder3b_%s_h2o_h2o" % h, "%sh2o3b" % h) for h in ("f", "cl", "br", "i")]
+HOLDERS += [("holder2b_ar_ar", "arar2b"), ("holder2b_cl_cl", "clcl2b"), ("holder2b_na_na", "nana2b"),
+            ("holder2b_na_cl", "nacl2b"), ("holder2b_ar_cs", "csar2b"), ("holder2b_ar_h2o", "arh2o2b")]
 
 
 @pytest.mark.parametrize("fixture,name", HOLDERS)
@@ -128,7 +131,7 @@ def test_system_published_energies(fixture):
 
 # the reference's generated program for each extracted table (harness kind)
 REF_PROGRAM = {"mbpol2b": 0, "mbpol3b": 1, "ch4h2o2b": 2, "ch4ch42b": 3, "ch4h2o3b": 4, "h2oli2b": 5, "h2oli3b": 6,
-               "fh2o2b": 7, "fh2o3b": 8}
+               "fh2o2b": 7, "fh2o3b": 8, "nana2b": 9, "nacl2b": 10, "arh2o2b": 11}
 
 
 @pytest.mark.parametrize("name", list(REF_PROGRAM))
@@ -165,6 +168,24 @@ def test_ion_water_vs_reference(ion, nb):
     if not mo.RefSystem.available():
         pytest.skip("reference library not built here")
     ids, xyz, box = workloads.ion_water_box([ion] * (1 if ion in ("na+", "cl-") else 3), seed=1)
+    o = mo.OracleSystem(ids, xyz, box, 9.0, 7.0)
+    r = mo.RefSystem(ids, xyz, box, 9.0, 7.0)
+    e_o, e_r = o.energy(nb), r.energy(nb)
+    assert abs(e_o - e_r) < 1e-10 * abs(e_r)
+    np.testing.assert_allclose(o.real_grads(), r.real_grads(), rtol=0, atol=1e-8)
+    np.testing.assert_allclose(o.virial, r.virial(), rtol=1e-9, atol=1e-7)
+
+
+@pytest.mark.parametrize("ions", [("na+", "cl-", "na+", "cl-", "na+", "cl-"), ("ar", "ar", "ar"),
+                                  ("cs+", "ar", "cs+", "ar"), ("li+", "f-", "k+", "br-")])
+@pytest.mark.parametrize("nb", [2, 3])
+def test_solution_vs_reference(ions, nb):
+    """Salt solutions and argon in water (every pair type of the box has an
+    evaluator here, ion-ion and atom-atom included): the oracle against the
+    compiled reference."""
+    if not mo.RefSystem.available():
+        pytest.skip("reference library not built here")
+    ids, xyz, box = workloads.ion_water_box(list(ions), seed=4)
     o = mo.OracleSystem(ids, xyz, box, 9.0, 7.0)
     r = mo.RefSystem(ids, xyz, box, 9.0, 7.0)
     e_o, e_r = o.energy(nb), r.energy(nb)
