@@ -768,9 +768,19 @@ int mbx_launch_%(name)s_w(const HolderArgs& A, int grads, int grid, cudaStream_t
 }
 
 
+# Large template MB-nrg types built with the energy + gradient and the
+# energy-only kernels only: every further kernel of a ~3e4-term trie adds
+# ~10 MB of code (ptxas compiles the trie's pieces once per calling kernel),
+# so their raw-polynomial (mbx_poly) and coefficient-adjoint
+# (mbx_evaluate_dcoef) entries answer MBX_ENOTSUP.
+LEAN_TYPES = {"nh3nh32b", "nh3pbe2b", "ch4co22b", "mbpbe2b", "co23b", "mbpbe3b"}
+
+
 def variants_of(name):
     if load_pip(name).nterms > STRAIGHT_LINE_MAX_TERMS:
         return "w"
+    if name in LEAN_TYPES:
+        return "ge"
     return "gecp" + ("s" if name in SHIFT_TYPES else "")
 
 

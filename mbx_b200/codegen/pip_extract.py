@@ -111,8 +111,24 @@ _ION2B = "potential/2b/x2b-A1B2Z2_C-v1x.cpp"
 for _ion, _name in (("li", "h2oli2b"), ("na", "h2ona2b"), ("k", "h2ok2b"), ("rb", "h2orb2b"), ("cs", "h2ocs2b")):
     FITS[_name] = (_ION2B, r'if \(mon1 == "h2o" && mon2 == "%s\+"\) \{\s*twobodyfit\s*=\s*std::vector<double>\s*\{' % _ion)
 
+# the template-generated MB-nrg evaluators whose specs codegen/mbnrg_spec.py
+# extracts: their energy-only programs and constructor blocks
+def _mbnrg_programs():
+    from mbx_b200.codegen import mbnrg_spec as ms
+    progs, fits, tables = {}, {}, {}
+    for name, (source, mons, table, header) in ms.SOURCES.items():
+        progs[table] = (ms.PROGRAMS[table], header)
+        fits[name] = (source, ms.fit_pattern(mons))
+        tables[name] = table
+    return progs, fits, tables
+
+
+MBNRG_PROGRAMS, _fits, _tables = _mbnrg_programs()
+FITS.update(_fits)
+
 # evaluator -> the program (table) its coefficients belong to
 TABLE_OF = {name: name for name in PROGRAMS if name in FITS}
+TABLE_OF.update(_tables)
 TABLE_OF.update({n: "h2oion2b" for n in ("h2oli2b", "h2ona2b", "h2ok2b", "h2orb2b", "h2ocs2b")})
 _ION3B = "potential/3b/x3b-h2o-ion-v1x-deg4-filtered.cpp"
 for _ion in ("li", "na", "k", "rb", "cs"):
@@ -314,7 +330,7 @@ def strip_comments(text):
 
 
 def extract_program(ref, name):
-    rel, nvars, ncoef, degree = PROGRAMS[name]
+    rel, nvars, ncoef, degree = program(ref, name)
     path = os.path.join(ref, "src", rel)
     text = strip_comments(open(path).read())
     text = re.sub(r"#ifdef DEBUG.*?#endif", "", text, flags=re.S)
@@ -386,6 +402,15 @@ def _terms(result, rel, nvars, ncoef, degree):
     return terms
 
 
+def program(ref, name):
+    """(source, nvars, ncoef, degree) of a table's energy-only program."""
+    if name in PROGRAMS:
+        return PROGRAMS[name]
+    from mbx_b200.codegen.mbnrg_spec import poly_size
+    rel, header = MBNRG_PROGRAMS[name]
+    return (rel,) + poly_size(ref, header)
+
+
 def extract_fit(ref, name, ncoef):
     rel, pattern = FITS[name]
     text = strip_comments(open(os.path.join(ref, "src", rel)).read())
@@ -421,11 +446,11 @@ def write_fit(name, fit):
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
-    ap.add_argument("names", nargs="*", default=list(PROGRAMS))
+    ap.add_argument("names", nargs="*", default=list(PROGRAMS) + list(MBNRG_PROGRAMS))
     args = ap.parse_args(argv)
     for name in args.names:
         t0 = time.time()
-        rel, nvars, ncoef, degree = PROGRAMS[name]
+        rel, nvars, ncoef, degree = program(args.ref, name)
         terms = extract_program(args.ref, name)
         used = sorted({t[0] for t in terms})
         write_table(name, terms, nvars, ncoef, degree)

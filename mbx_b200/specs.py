@@ -493,6 +493,28 @@ ARH2O2B = Spec(
     ref="potential/2b/mbnrg_2b_A1_B1C2X2_deg5_v1.cpp:616",
 )
 
+# ---------------------------------------------------------------------------
+# Template-generated MB-nrg evaluators (H2, NH3, CH4-CO2, MB-pbe water, CO2
+# 3b): their specs are read from the reference's sources by
+# codegen/mbnrg_spec.py into data/<name>.spec.json (same fields as above).
+# ---------------------------------------------------------------------------
+EXTRACTED = ("h2h22b", "h2oh22b", "csh22b", "nh3nh32b", "nh3pbe2b", "ch4co22b", "mbpbe2b", "co23b", "mbpbe3b")
+
+
+def _load_extracted(name):
+    import json
+    import os
+    with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", name + ".spec.json")) as f:
+        d = json.load(f)
+    return Spec(name=d["name"], monomers=tuple(d["monomers"]), nat=tuple(d["nat"]), sites=tuple(d["sites"]),
+                lp=tuple(tuple(x) for x in d["lp"]),
+                variables=tuple((v[0], int(v[1]), int(v[2]), float(v[3]), float(v[4])) for v in d["variables"]),
+                switch=d["switch"], ri=float(d["ri"]), rf=float(d["rf"]), skip=d["skip"], nvars=int(d["nvars"]),
+                ncoef=int(d["ncoef"]), degree=int(d["degree"]), ref=d["ref"], table=d["table"])
+
+
+TEMPLATE_SPECS = tuple(_load_extracted(n) for n in EXTRACTED)
+
 FH2O3B = _hal3b("f-", "fh2o3b")
 CLH2O3B = _hal3b("cl-", "clh2o3b")
 BRH2O3B = _hal3b("br-", "brh2o3b")
@@ -502,7 +524,7 @@ SPECS = {s.name: s for s in (MBPOL2B, MBPOL3B, CH4H2O2B, CH4CH42B, CH4H2O3B,
                              H2OLI2B, H2ONA2B, H2OK2B, H2ORB2B, H2OCS2B,
                              H2OLI3B, H2ONA3B, H2OK3B, H2ORB3B, H2OCS3B,
                              FH2O2B, CLH2O2B, BRH2O2B, IH2O2B, FH2O3B, CLH2O3B, BRH2O3B, IH2O3B,
-                             ARH2O2B) + ATOM2B}
+                             ARH2O2B) + ATOM2B + TEMPLATE_SPECS}
 
 # Dispatch by sorted monomer ids (e2b::get_2b_energy, potential/2b/energy2b.cpp:
 # 240-254,258-281,282,323; e3b::get_3b_energy, potential/3b/energy3b.cpp:185-216,
@@ -512,24 +534,29 @@ DISPATCH_2B = {("h2o", "h2o"): "mbpol2b", ("ch4", "h2o"): "ch4h2o2b", ("ch4", "c
                ("h2o", "rb+"): "h2orb2b", ("cs+", "h2o"): "h2ocs2b",
                ("f-", "h2o"): "fh2o2b", ("cl-", "h2o"): "clh2o2b", ("br-", "h2o"): "brh2o2b", ("h2o", "i-"): "ih2o2b",
                ("na+", "na+"): "nana2b", ("cl-", "cl-"): "clcl2b", ("ar", "ar"): "arar2b", ("cl-", "na+"): "nacl2b",
-               ("ar", "cs+"): "csar2b", ("ar", "h2o"): "arh2o2b"}
+               ("ar", "cs+"): "csar2b", ("ar", "h2o"): "arh2o2b",
+               ("h2", "h2"): "h2h22b", ("h2", "h2o"): "h2oh22b", ("cs+", "h2"): "csh22b", ("nh3", "nh3"): "nh3nh32b",
+               ("nh3pbe0d3bj", "nh3pbe0d3bj"): "nh3pbe2b", ("ch4", "co2"): "ch4co22b", ("mbpbe", "mbpbe"): "mbpbe2b"}
 DISPATCH_3B = {("h2o", "h2o", "h2o"): "mbpol3b", ("ch4", "h2o", "h2o"): "ch4h2o3b",
                ("h2o", "h2o", "li+"): "h2oli3b", ("h2o", "h2o", "na+"): "h2ona3b", ("h2o", "h2o", "k+"): "h2ok3b",
                ("h2o", "h2o", "rb+"): "h2orb3b", ("cs+", "h2o", "h2o"): "h2ocs3b",
                ("f-", "h2o", "h2o"): "fh2o3b", ("cl-", "h2o", "h2o"): "clh2o3b", ("br-", "h2o", "h2o"): "brh2o3b",
-               ("h2o", "h2o", "i-"): "ih2o3b"}
+               ("h2o", "h2o", "i-"): "ih2o3b", ("co2", "co2", "co2"): "co23b", ("mbpbe", "mbpbe", "mbpbe"): "mbpbe3b"}
 
 # Real atoms and total sites (real + electrostatic virtual sites) per monomer
 # type, as the reference's monomer table sets them (bblock/sys_tools.cpp
 # SetUpMonomers:133-254: h2o has 3 atoms + the M site, ch4 5 atoms, the
-# alkali-metal and halide ions and argon one atom, :210-225).
+# alkali-metal and halide ions and argon one atom, :210-225, h2 two, nh3
+# four, co2 three, mbpbe like h2o three atoms and four sites, :191-233).
 MONOMER_ATOMS = {"h2o": 3, "ch4": 5, "li+": 1, "na+": 1, "k+": 1, "rb+": 1, "cs+": 1,
-                 "f-": 1, "cl-": 1, "br-": 1, "i-": 1, "ar": 1}
-MONOMER_SITES = dict(MONOMER_ATOMS, h2o=4)
+                 "f-": 1, "cl-": 1, "br-": 1, "i-": 1, "ar": 1, "h2": 2, "nh3": 4, "nh3pbe0d3bj": 4, "co2": 3,
+                 "mbpbe": 3}
+MONOMER_SITES = dict(MONOMER_ATOMS, h2o=4, mbpbe=4)
 # atom names a caller passes to AddMonomer for each id (input order)
 MONOMER_ATOM_NAMES = {"h2o": ("O", "H", "H"), "ch4": ("C", "H", "H", "H", "H"), "li+": ("Li",), "na+": ("Na",),
                       "k+": ("K",), "rb+": ("Rb",), "cs+": ("Cs",), "f-": ("F",), "cl-": ("Cl",), "br-": ("Br",),
-                      "i-": ("I",), "ar": ("Ar",)}
+                      "i-": ("I",), "ar": ("Ar",), "h2": ("H", "H"), "nh3": ("N", "H", "H", "H"),
+                      "nh3pbe0d3bj": ("N", "H", "H", "H"), "co2": ("C", "O", "O"), "mbpbe": ("O", "H", "H")}
 
 
 def check():

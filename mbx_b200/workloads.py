@@ -51,6 +51,46 @@ def methane_body():
     return np.array([[0, 0, 0], [t, t, t], [t, -t, -t], [-t, t, -t], [-t, -t, t]], float)
 
 
+def ammonia_body(r_nh=1.012, theta=106.7):
+    """N first, three H on a cone (H-N-H angle theta degrees)."""
+    t = np.radians(theta)
+    # half-angle of the cone from the H-N-H angle: cos t = 1 - 1.5 sin^2 a
+    a = np.arcsin(np.sqrt((1.0 - np.cos(t)) / 1.5))
+    phis = np.radians([0.0, 120.0, 240.0])
+    h = [[r_nh * np.sin(a) * np.cos(f), r_nh * np.sin(a) * np.sin(f), r_nh * np.cos(a)] for f in phis]
+    return np.array([[0.0, 0.0, 0.0]] + h)
+
+
+def co2_body(r_co=1.16):
+    return np.array([[0.0, 0.0, 0.0], [0.0, 0.0, r_co], [0.0, 0.0, -r_co]])
+
+
+def h2_body(r_hh=0.741):
+    return np.array([[0.0, 0.0, 0.0], [0.0, 0.0, r_hh]])
+
+
+BODIES = {"h2o": water_body, "mbpbe": water_body, "ch4": methane_body, "nh3": ammonia_body,
+          "nh3pbe0d3bj": ammonia_body, "co2": co2_body, "h2": h2_body}
+
+
+def molecule_box(ids, n_side=7, L=19.72, seed=0, jitter=0.3):
+    """Molecules (ids in input order; one-atom ions and argon too) on the
+    sites of an n_side^3 lattice in a cubic box of edge L, picked and
+    jittered like water_box, each rigid body randomly rotated."""
+    rng = np.random.default_rng(seed)
+    s = L / n_side
+    g = (np.arange(n_side) + 0.5) * s - L / 2
+    lattice = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+    pick = rng.choice(len(lattice), size=len(ids), replace=False)
+    centres = lattice[pick] + rng.uniform(-jitter, jitter, size=(len(ids), 3))
+    parts = []
+    for m, c in zip(ids, centres):
+        body = BODIES[m]() if m in BODIES else np.zeros((1, 3))
+        parts.append(place(rng, body, c[None, :])[0].reshape(-1))
+    box = np.array([L, 0, 0, 0, L, 0, 0, 0, L], float)
+    return list(ids), np.concatenate(parts), box
+
+
 def place(rng, body, centres):
     rot = random_rotations(rng, len(centres))
     return centres[:, None, :] + np.einsum("nij,aj->nai", rot, body)

@@ -41,6 +41,14 @@
 #include "potential/2b/poly_2b_A1_A1_deg9_v1.h"
 #include "potential/2b/poly_2b_A1_B1_deg9_v1.h"
 #include "potential/2b/poly_2b_A1_B1C2X2_deg5_v1.h"
+#include "potential/2b/poly_2b_A2_A2_deg6_v1.h"
+#include "potential/2b/poly_2b_A1B2Z2_C2_deg5_v1.h"
+#include "potential/2b/poly_2b_A1_B2_deg7_v1.h"
+#include "potential/2b/poly_2b_A1B3_A1B3_deg4_v1.h"
+#include "potential/2b/poly_2b_A1B4_C1D2_deg4_v1.h"
+#include "potential/2b/poly_2b_A1B2Z2_A1B2Z2_deg4_vmbpbe.h"
+#include "potential/3b/poly_3b_A1B2_A1B2_A1B2_deg4_v1.h"
+#include "potential/3b/poly_3b_A1B2_A1B2_A1B2_deg4_vmbpbe.h"
 
 namespace {
 
@@ -67,6 +75,10 @@ std::vector<std::string> atom_names(const std::string& id) {
     if (id == "br-") return {"Br"};
     if (id == "i-") return {"I"};
     if (id == "ar") return {"Ar"};
+    if (id == "h2") return {"H", "H"};
+    if (id == "nh3" || id == "nh3pbe0d3bj") return {"N", "H", "H", "H"};
+    if (id == "co2") return {"C", "O", "O"};
+    if (id == "mbpbe") return {"O", "H", "H"};
     throw std::runtime_error("harness knows no atom names for monomer id " + id);
 }
 
@@ -198,7 +210,8 @@ double mbxref_get_3b(const char* m1, const char* m2, const char* m3, long nm, co
 // 2 CH4-H2O 2b (38), 3 CH4-CH4 2b (45), 4 CH4-H2O-H2O 3b (55), 5 alkali-ion -
 // water 2b (8), 6 water - water - alkali-ion 3b (21), 7 halide - water 2b (8),
 // 8 halide - water - water 3b (41), 9 like atoms 2b (1), 10 unlike atoms 2b (1),
-// 11 argon - water 2b (8).
+// 11 argon - water 2b (8); 12-19 the template MB-nrg tables h2h22b, h2oh22b,
+// csh22b, nh3nh32b, ch4co22b, mbpbe2b, co23b, mbpbe3b.
 // One configuration per call; g may be NULL for energy only.
 double mbxref_poly(int kind, const double* a, const double* x, double* g) {
     switch (kind) {
@@ -266,6 +279,54 @@ double mbxref_poly(int kind, const double* a, const double* x, double* g) {
             mbnrg_A1_B1C2X2_deg5::poly_A1_B1C2X2_deg5_v1 p;
             if (!g) return p.eval(x, a);
             for (int j = 0; j < 8; ++j) g[j] = 0.0;
+            return p.eval(x, a, g);
+        }
+        case 12: {
+            mbnrg_A2_A2_deg6::poly_A2_A2_deg6_v1 p;
+            if (!g) return p.eval(x, a);
+            for (int j = 0; j < 6; ++j) g[j] = 0.0;
+            return p.eval(x, a, g);
+        }
+        case 13: {
+            mbnrg_A1B2Z2_C2_deg5::poly_A1B2Z2_C2_deg5_v1 p;
+            if (!g) return p.eval(x, a);
+            for (int j = 0; j < 14; ++j) g[j] = 0.0;
+            return p.eval(x, a, g);
+        }
+        case 14: {
+            mbnrg_A1_B2_deg7::poly_A1_B2_deg7_v1 p;
+            if (!g) return p.eval(x, a);
+            for (int j = 0; j < 3; ++j) g[j] = 0.0;
+            return p.eval(x, a, g);
+        }
+        case 15: {
+            mbnrg_A1B3_A1B3_deg4::poly_A1B3_A1B3_deg4_v1 p;
+            if (!g) return p.eval(x, a);
+            for (int j = 0; j < 28; ++j) g[j] = 0.0;
+            return p.eval(x, a, g);
+        }
+        case 16: {
+            mbnrg_A1B4_C1D2_deg4::poly_A1B4_C1D2_deg4_v1 p;
+            if (!g) return p.eval(x, a);
+            for (int j = 0; j < 28; ++j) g[j] = 0.0;
+            return p.eval(x, a, g);
+        }
+        case 17: {
+            mbnrg_A1B2Z2_A1B2Z2_deg4::poly_A1B2Z2_A1B2Z2_deg4_vmbpbe p;
+            if (!g) return p.eval(x, a);
+            for (int j = 0; j < 31; ++j) g[j] = 0.0;
+            return p.eval(x, a, g);
+        }
+        case 18: {
+            mbnrg_A1B2_A1B2_A1B2_deg4::poly_A1B2_A1B2_A1B2_deg4_v1 p;
+            if (!g) return p.eval(x, a);
+            for (int j = 0; j < 27; ++j) g[j] = 0.0;
+            return p.eval(x, a, g);
+        }
+        case 19: {
+            mbnrg_A1B2_A1B2_A1B2_deg4::poly_A1B2_A1B2_A1B2_deg4_vmbpbe p;
+            if (!g) return p.eval(x, a);
+            for (int j = 0; j < 36; ++j) g[j] = 0.0;
             return p.eval(x, a, g);
         }
     }

@@ -24,6 +24,11 @@ reference checkout, default /root/reference) and writes ``tests/golden/*.json``:
   ``unittest-poly-holder-2b.cpp`` (mbnrg_A1_A1_deg9_v1 :1229-1312,
   mbnrg_A1_B1_deg9_v1 :1313-1370, mbnrg_A1_B1C2X2_deg5_v1 ar-h2o :220),
   ``unittest-poly-2b.cpp`` (poly_2b_A1_B1C2X2_deg5_v1 :53-204);
+* template MB-nrg types: ``unittest-energy2b.cpp`` (h2-h2 :544, h2-h2o :607,
+  nh3-nh3 :674, nh3pbe0d3bj :741, h2-cs :1126, mbpbe-mbpbe :1250, ch4-co2
+  :1943), ``unittest-energy3b.cpp`` (mbpbe x3 :911, co2 x3 :1386),
+  ``unittest-poly-holder-2b.cpp`` (:1019-1546), ``unittest-poly-holder-3b.cpp``
+  (:84-173);
 * water - water - alkali-ion 3b: ``unittest-energy3b.cpp`` (li-h2o-h2o
   :146-357, cs-h2o-h2o :358-471), ``unittest-poly-holder-3b.cpp``
   (x3b_h2o_ion_v1x_deg4_filtered :384-909, one fixture per ion),
@@ -101,6 +106,25 @@ BLOCKS += [("holder2b_%s" % f, "src/unittests/unittest-poly-holder-2b.cpp", r'TE
     ("ar_cs", "mbnrg_A1_B1_deg9_v1::struct", "ar-cs"), ("ar_h2o", "mbnrg_A1_B1C2X2_deg5_v1::struct", "ar-h2o"))]
 BLOCKS += [("poly_arh2o2b", "src/unittests/unittest-poly-2b.cpp", r'TEST_CASE\(":poly_2b_A1_B1C2X2_deg5_v1:struct"\)',
             None)]
+# template MB-nrg evaluators (H2, NH3, CH4-CO2, MB-pbe, CO2 3b)
+BLOCKS += [("energy2b_%s" % f, "src/unittests/unittest-energy2b.cpp", r'TEST_CASE\("energy2b::get_2b_energy"\)',
+            r'SECTION\("%s"\)' % sec) for f, sec in (
+    ("h2_h2", "h2-h2"), ("h2_h2o", "h2-h2o"), ("nh3_nh3", "nh3-nh3"), ("nh3pbe_nh3pbe", "nh3pbe0d3bj-nh3pbe0d3bj"),
+    ("h2_cs", "h2-cs"), ("mbpbe_mbpbe", "mbpbe-mbpbe"), ("ch4_co2", "ch4-co2"))]
+BLOCKS += [("energy3b_%s" % f, "src/unittests/unittest-energy3b.cpp", r'TEST_CASE', r'SECTION\("%s"\)' % sec)
+           for f, sec in (("mbpbe_mbpbe_mbpbe", "mbpbe-mbpbe-mbpbe"), ("co2_co2_co2", "co2-co2-co2"))]
+BLOCKS += [("holder2b_%s" % f, "src/unittests/unittest-poly-holder-2b.cpp", r'TEST_CASE\("%s"\)' % tc,
+            r'SECTION\("%s"\)' % sec) for f, tc, sec in (
+    ("h2_h2", "mbnrg_A2_A2_deg6_v1::struct", "h2-h2"), ("h2_h2o", "mbnrg_2b_A1B2Z2_C2_deg5_v1::struct", "h2-h2o"),
+    ("nh3_nh3", "mbnrg_A1B3_A1B3_deg4_v1::struct", "nh3-nh3"),
+    ("nh3pbe_nh3pbe", "mbnrg_A1B3_A1B3_deg4_v1::struct", "nh3pbe0d3bj-nh3pbe0d3bj"),
+    ("cs_h2", "mbnrg_A1_B2_deg7_v1::struct", "cs-h2"), ("mbpbe_mbpbe", "mbnrg_A1B2Z2_A1B2Z2_deg4_vmbpbe::struct",
+                                                       "mbpbe-mbpbe"),
+    ("ch4_co2", "mbnrg_A1B4_C1D2_deg4_v1::struct", "ch4-co2"))]
+BLOCKS += [("holder3b_%s" % f, "src/unittests/unittest-poly-holder-3b.cpp", r'TEST_CASE\("%s"\)' % tc,
+            r'SECTION\("%s"\)' % sec) for f, tc, sec in (
+    ("mbpbe_mbpbe_mbpbe", "mbnrg_A1B2_A1B2_A1B2_deg4_vmbpbe::struct", "mbpbe-mbpbe-mbpbe"),
+    ("co2_co2_co2", "mbnrg_A1B2_A1B2_A1B2_deg4_v1::struct", "co2-co2-co2"))]
 
 SYSTEMS = [
     ("system_256_h2o_cubic_box", "timing/256_h2o_cubic_box"),

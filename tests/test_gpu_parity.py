@@ -90,6 +90,10 @@ HOLDERS += [("holder2b_%s_h2o" % h, "%sh2o2b" % h) for h in ("f", "cl", "br", "i
 HOLDERS += [("holder3b_%s_h2o_h2o" % h, "%sh2o3b" % h) for h in ("f", "cl", "br", "i")]
 HOLDERS += [("holder2b_ar_ar", "arar2b"), ("holder2b_cl_cl", "clcl2b"), ("holder2b_na_na", "nana2b"),
             ("holder2b_na_cl", "nacl2b"), ("holder2b_ar_cs", "csar2b"), ("holder2b_ar_h2o", "arh2o2b")]
+HOLDERS += [("holder2b_h2_h2", "h2h22b"), ("holder2b_h2_h2o", "h2oh22b"), ("holder2b_nh3_nh3", "nh3nh32b"),
+            ("holder2b_nh3pbe_nh3pbe", "nh3pbe2b"), ("holder2b_cs_h2", "csh22b"), ("holder2b_mbpbe_mbpbe", "mbpbe2b"),
+            ("holder2b_ch4_co2", "ch4co22b"), ("holder3b_mbpbe_mbpbe_mbpbe", "mbpbe3b"),
+            ("holder3b_co2_co2_co2", "co23b")]
 
 
 @pytest.mark.parametrize("fixture,name", HOLDERS)
@@ -97,7 +101,8 @@ def test_evaluator_golden(ctx, fixture, name):
     gd = golden(fixture)
     s = SPECS[name]
     n = gd.get("ndim", gd.get("ntrim"))
-    blocks = [np.array(gd["xyz%d" % (i + 1)]).reshape(n, -1) for i in range(s.nbody)]
+    order = {"holder2b_h2_h2o": (1, 0)}.get(fixture, range(s.nbody))   # holder slot i <- xyz(order[i] + 1)
+    blocks = [np.array(gd["xyz%d" % (k + 1)]).reshape(n, -1) for k in order]
     xyz = np.ascontiguousarray(np.concatenate(blocks, axis=1))
     grad = np.zeros_like(xyz)
     vir = np.zeros(9)
@@ -108,9 +113,9 @@ def test_evaluator_golden(ctx, fixture, name):
     np.testing.assert_allclose(grad, go, rtol=0, atol=G_ABS)
     np.testing.assert_allclose(vir, vo, rtol=1e-10, atol=G_ABS)
     off = 0
-    for i in range(s.nbody):
+    for i, k in enumerate(order):
         w = blocks[i].shape[1]
-        np.testing.assert_allclose(grad[:, off:off + w].reshape(-1), gd["grad%d_expected" % (i + 1)], atol=1e-6)
+        np.testing.assert_allclose(grad[:, off:off + w].reshape(-1), gd["grad%d_expected" % (k + 1)], atol=1e-6)
         off += w
 
 
@@ -118,7 +123,7 @@ def random_nmers(name, n, seed=3):
     """Gas-phase n-mers of the evaluator's types spanning its cutoff."""
     s = SPECS[name]
     rng = np.random.default_rng(seed)
-    bodies = {"h2o": workloads.water_body(), "ch4": workloads.methane_body()}
+    bodies = {m: f() for m, f in workloads.BODIES.items()}
     for ion in ALKALI + HALIDES + ("ar",):
         bodies[ion] = np.zeros((1, 3))
     out = []
@@ -272,6 +277,16 @@ def test_solution_box(ions):
     and atom-atom included) and the ion trimers on the GPU against the
     oracle; five monomer types in the last one."""
     ids, xyz, box = workloads.ion_water_box(list(ions), seed=4)
+    compare_system(ids, xyz, box, 9.0, 7.0)
+
+
+@pytest.mark.parametrize("ids", [["nh3"] * 200, ["nh3pbe0d3bj"] * 200, ["h2"] * 60 + ["h2o"] * 150 + ["cs+"] * 2,
+                                 ["mbpbe"] * 220, ["ch4"] + ["h2o"] * 180 + ["na+", "cl-"]])
+def test_molecule_box(ids):
+    """Liquids and mixtures of the template MB-nrg types on the GPU against
+    the oracle (the same boxes the oracle is checked on against the
+    compiled reference)."""
+    ids, xyz, box = workloads.molecule_box(ids, seed=3)
     compare_system(ids, xyz, box, 9.0, 7.0)
 
 
