@@ -52,7 +52,9 @@ const char* mbx_last_error(const mbx_ctx* ctx);
 const char* mbx_version(void);
 
 /* Monomers in internal order (System::AddMonomerInfo, system.cpp:1794-1969):
- * ids[m] ("h2o", "ch4"), first_index[m] (first site), tag[m] (tag of the
+ * ids[m] (the reference's monomer ids of this path: "h2o", "ch4", "li+",
+ * "na+", "k+", "rb+", "cs+", "f-", "cl-", "br-", "i-", "ar", "h2", "nh3",
+ * "nh3pbe0d3bj", "co2", "mbpbe"), first_index[m] (first site), tag[m] (tag of the
  * monomer's first atom; n-mers are owned by the lowest tag,
  * sys_tools.cpp:562,585), is_local[m] (NULL = all local), numsites. */
 int mbx_set_topology(mbx_ctx* ctx, int nmon, const char* const* ids, const int* first_index, const int* tag,
@@ -89,7 +91,9 @@ int mbx_nmers(mbx_ctx* ctx, int nbody, double cutoff, const double* xyz, int use
 /* Evaluator calling convention (x2b_v9x::eval(w1, w2, g1, g2, nd, virial),
  * 2b/x2b-v9x.h:83; x3b_v2x::eval, 3b/x3b-v2x.h:85; the MB-nrg classes):
  * n n-mers of one evaluator ("mbpol2b", "mbpol3b", "ch4h2o2b", "ch4ch42b",
- * "ch4h2o3b"), coordinates xyz[n][nreal*3] with the monomers in evaluator
+ * "ch4h2o3b", the ion types "h2o<ion>2b" / "h2o<ion>3b" / "<halide>h2o2b" /
+ * "<halide>h2o3b", ...; mbx_evaluator_info answers for any name), coordinates
+ * xyz[n][nreal*3] with the monomers in evaluator
  * order and already imaged.  grad (same layout, +=), virial (9, +=), e_per
  * (n switched energies) may be NULL.  *energy gets the sum. */
 int mbx_evaluate(mbx_ctx* ctx, const char* evaluator, long n, const double* xyz, double* grad, double* virial,
