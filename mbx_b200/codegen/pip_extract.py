@@ -30,6 +30,7 @@ h2oion2b potential/2b/poly-2b-A1B2Z2_C-v1.cpp:38 (eval(nd, a, x))        8    42
 h2oion3b potential/3b/poly-3b-h2o-ion-v1x_deg4_filtered.cpp:39 (*)       21   1016
 halh2o2b potential/2b/poly_2b_A1_B1C2X2_deg6_nograd_v1.cpp:50             8    906
 halh2o3b potential/3b/poly_3b_A1_B1C2X2_B1C2X2_deg4_nograd_v1.cpp:50      41   3173
+co2co22btab potential/2b/poly_2b_A1B2_A1B2_v1.cpp:39 (**)               15   2269
 a1a12b   potential/2b/poly_2b_A1_A1_deg9_nograd_v1.cpp:50                 1    9
 a1b12b   potential/2b/poly_2b_A1_B1_deg9_nograd_v1.cpp:50                 1    9
 arh2o2b  potential/2b/poly_2b_A1_B1C2X2_deg5_nograd_v1.cpp:50             8    496
@@ -37,7 +38,8 @@ arh2o2b  potential/2b/poly_2b_A1_B1C2X2_deg5_nograd_v1.cpp:50             8    4
 
 (*) the only program of this polynomial computes value and gradient; the
 value is its ``double e = tN;``, and only the assignments tN depends on are
-expanded.
+expanded.  (**) the value is the expression assigned to ``double e`` before
+``return e;``.
 
 It also extracts the fitted linear coefficients (the model parameters) from
 the evaluator classes:
@@ -65,6 +67,8 @@ the evaluator classes:
   ``coefficients`` of the pair's block in potential/2b/mbnrg_2b_A1_A1_deg9_v1.cpp
   :11 (na+ na+), :27 (cl- cl-), :43 (ar ar) and mbnrg_2b_A1_B1_deg9_v1.cpp :11
   (na+ cl-), :27 (cs+ ar); arh2o2b: mbnrg_2b_A1_B1C2X2_deg5_v1.cpp:11
+* co2a2b, co2co22b (table co2co22btab): ``coefficients`` of the model's block
+  in potential/2b/x2b_A1B2_A1B2_v1x.cpp :88 (co2_archive), :2373 (co2)
 
 Output (``mbx_b200/data/``): ``<table>.pip.gz`` (term table, gzip) and
 ``<evaluator>.fit`` (coefficients, one per line, printed with ``repr`` so they
@@ -96,7 +100,10 @@ PROGRAMS = {
     "a1a12b": ("potential/2b/poly_2b_A1_A1_deg9_nograd_v1.cpp", 1, 9, 9),
     "a1b12b": ("potential/2b/poly_2b_A1_B1_deg9_nograd_v1.cpp", 1, 9, 9),
     "arh2o2b": ("potential/2b/poly_2b_A1_B1C2X2_deg5_nograd_v1.cpp", 8, 496, 5),
+    "co2co22btab": ("potential/2b/poly_2b_A1B2_A1B2_v1.cpp", 15, 2269, 5),
 }
+# programs whose value is assigned to ``double e`` and then returned
+E_ASSIGN = {"co2co22btab"}
 # programs whose value is a named temporary (value + gradient programs)
 RESULT_VAR = {"h2oion3b": r"double e = (t\d+)\s*;"}
 
@@ -153,6 +160,10 @@ for _m1, _m2, _name, _table, _file in (
     FITS[_name] = ("potential/2b/" + _file, r'if \(mon1 == "%s" and mon2 == "%s"\) \{\s*coefficients\s*=\s*'
                    r'std::vector<double>\s*\{' % (_m1, _m2))
     TABLE_OF[_name] = _table
+for _m, _name in (("co2_archive", "co2a2b"), ("co2", "co2co22b")):
+    FITS[_name] = ("potential/2b/x2b_A1B2_A1B2_v1x.cpp", r'if \(mon1 == "%s" && mon2 == "%s"\) \{\s*coefficients\s*=\s*'
+                   r'std::vector<double>\s*\{' % (_m, _m))
+    TABLE_OF[_name] = "co2co22btab"
 
 TOKEN = re.compile(
     r"\s*(?:(?P<num>\d+\.\d*(?:[eE][-+]?\d+)?|\d+(?:[eE][-+]?\d+)?)"
@@ -334,6 +345,8 @@ def extract_program(ref, name):
     path = os.path.join(ref, "src", rel)
     text = strip_comments(open(path).read())
     text = re.sub(r"#ifdef DEBUG.*?#endif", "", text, flags=re.S)
+    if name in E_ASSIGN:
+        text = re.sub(r"\bdouble e\s*=", "return", text).replace("return e;", "")
     if name == "ch4ch42b":
         bodies = function_bodies(text, ["fmg%d" % i for i in range(1, 16)])
         main = re.search(r"::eval\(const double a\[1345\], const double x\[45\]\)\s*\{(.*?)\n\}", text, re.S).group(1)

@@ -515,6 +515,65 @@ def _load_extracted(name):
 
 TEMPLATE_SPECS = tuple(_load_extracted(n) for n in EXTRACTED)
 
+# ---------------------------------------------------------------------------
+# CO2 - CO2 2b: x2b_A1B2_A1B2_v1x(m, m) for the CO2 models co2_archive, co2
+# and co2cm5100 .. co2cm580, potential/2b/x2b_A1B2_A1B2_v1x.cpp:18485-18700
+# (variables :18562-18580, local variable::v_exp(r0, k) = exp(k (r0 - r))
+# :62-77; f_switch :18373-18386 on the C-C distance, dimers beyond r2f
+# skipped :18541).  One polynomial (poly_2b_A1B2_A1B2_v1x, 15 variables,
+# degree 5, 2269 coefficients); constants and coefficients per model
+# (constructor blocks at the lines given below).
+# ---------------------------------------------------------------------------
+_S_CO22B = ("Aa", "B1a", "B2a", "Ab", "B1b", "B2b")
+_CO22B = {
+    # model: (evaluator, d_intra_AB, k_intra_AB, d_intra_BB, k_intra_BB, d_AA, k_AA, d_AB, k_AB, d_BB, k_BB, r2i,
+    #         r2f), constructor block line
+    "co2_archive": ("co2a2b", 2.533470783111825e+00, 1.772445777810116e+00, 1.299246633223584e+00,
+                    1.546435354569379e+00, 4.042621705776338e+00, 1.375890559471216e+00, 4.893559114105628e+00,
+                    7.248440685272545e-01, 2.785825083032128e+00, 2.691866638221668e+00, 8.0, 9.0),  # :88
+    "co2": ("co2co22b", 3.098180719521002e+00, 1.267379326287500e+00, 2.152649569148020e+00, 6.904623477544016e-01,
+            4.195717132005157e+00, 6.959794865790364e-02, 6.633057823695092e+00, 9.311550654726656e-01,
+            5.614642310195038e+00, 1.053234040860423e+00, 7.0, 9.0),  # :2373
+    "co2cm5100": ("cm5100co22b", 3.098180719521002e+00, 1.267379326287500e+00, 2.152649569148020e+00,
+                  6.904623477544016e-01, 4.195717132005157e+00, 6.959794865790364e-02, 6.633057823695092e+00,
+                  9.311550654726656e-01, 5.614642310195038e+00, 1.053234040860423e+00, 7.0, 9.0),  # :4657
+    "co2cm595": ("cm595co22b", 4.903036747511356e+00, 9.019913232531600e-01, 2.703937855283358e+00,
+                 1.004834209745757e+00, 4.537101521312326e+00, 9.163852883742113e-02, 6.300498483648834e+00,
+                 9.021417601624032e-01, 5.827456239776177e+00, 1.089701616045492e+00, 7.0, 9.0),  # :6941
+    "co2cm590": ("cm590co22b", 2.329138487337566e+00, 1.434391663074755e+00, 3.229816367099317e+00,
+                 9.702035861774958e-01, 4.006166160264772e+00, 1.117857009888089e-01, 5.789451971684920e+00,
+                 8.757387756335298e-01, 5.798891302817732e+00, 1.133531479542603e+00, 7.0, 9.0),  # :9226
+    "co2cm585": ("cm585co22b", 2.165524277685071e+00, 2.061892967817994e+00, 2.835603377312035e+00,
+                 3.459793262493814e+00, 4.235604053709159e+00, 1.141488887995241e-01, 4.667583436073858e+00,
+                 8.691887001880019e-01, 5.473818228420447e+00, 1.157204319628839e+00, 7.0, 9.0),  # :11513
+    "co2cm5875": ("cm5875co22b", 3.134332315833306e+00, 1.282904902772805e+00, 4.434199799497058e+00,
+                  8.407363065419096e-01, 1.800437262469989e+00, 1.216397961826567e-01, 6.926666442517130e+00,
+                  8.810761305307210e-01, 4.127797348559158e+00, 1.148765431751049e+00, 7.0, 9.0),  # :13798
+    "co2cm580": ("cm580co22b", 4.158829702809511e+00, 8.744952741703924e-01, 9.999985981119849e+00,
+                 4.486543492998215e-01, 3.899891165573160e+00, 1.074038746629509e+00, 4.292889407717251e+00,
+                 6.400679425638476e-01, 4.386671648943636e+00, 1.326376079648352e+00, 7.0, 9.0),  # :16083
+}
+# On this path: co2 and co2_archive.  The six co2cm* models share the
+# polynomial with their own constants; each would be another ~10 MB of
+# kernel code, and they are left out (their dimers evaluate to 0 here).
+CO2_MODELS = ("co2", "co2_archive")
+
+
+def _co22b(model):
+    name, dAB_i, kAB_i, dBB_i, kBB_i, dAA, kAA, dAB, kAB, dBB, kBB, ri, rf = _CO22B[model]
+    tab = [("Aa", "B1a", kAB_i, dAB_i), ("Aa", "B2a", kAB_i, dAB_i), ("B1a", "B2a", kBB_i, dBB_i),
+           ("Ab", "B1b", kAB_i, dAB_i), ("Ab", "B2b", kAB_i, dAB_i), ("B1b", "B2b", kBB_i, dBB_i),
+           ("Aa", "Ab", kAA, dAA), ("Aa", "B1b", kAB, dAB), ("Aa", "B2b", kAB, dAB),
+           ("B1a", "Ab", kAB, dAB), ("B1a", "B1b", kBB, dBB), ("B1a", "B2b", kBB, dBB),
+           ("B2a", "Ab", kAB, dAB), ("B2a", "B1b", kBB, dBB), ("B2a", "B2b", kBB, dBB)]
+    return Spec(name=name, monomers=(model, model), nat=(3, 3), sites=_S_CO22B, lp=(),
+                variables=_vars(_S_CO22B, [("exp", a, b, k, d) for a, b, k, d in tab]), switch="pair", ri=ri,
+                rf=rf, skip="pair_gt", nvars=15, ncoef=2269, degree=5,
+                ref="potential/2b/x2b_A1B2_A1B2_v1x.cpp:18485", table="co2co22btab")
+
+
+CO22B = tuple(_co22b(m) for m in CO2_MODELS)
+
 FH2O3B = _hal3b("f-", "fh2o3b")
 CLH2O3B = _hal3b("cl-", "clh2o3b")
 BRH2O3B = _hal3b("br-", "brh2o3b")
@@ -524,7 +583,7 @@ SPECS = {s.name: s for s in (MBPOL2B, MBPOL3B, CH4H2O2B, CH4CH42B, CH4H2O3B,
                              H2OLI2B, H2ONA2B, H2OK2B, H2ORB2B, H2OCS2B,
                              H2OLI3B, H2ONA3B, H2OK3B, H2ORB3B, H2OCS3B,
                              FH2O2B, CLH2O2B, BRH2O2B, IH2O2B, FH2O3B, CLH2O3B, BRH2O3B, IH2O3B,
-                             ARH2O2B) + ATOM2B + TEMPLATE_SPECS}
+                             ARH2O2B) + ATOM2B + TEMPLATE_SPECS + CO22B}
 
 # Dispatch by sorted monomer ids (e2b::get_2b_energy, potential/2b/energy2b.cpp:
 # 240-254,258-281,282,323; e3b::get_3b_energy, potential/3b/energy3b.cpp:185-216,
@@ -537,6 +596,7 @@ DISPATCH_2B = {("h2o", "h2o"): "mbpol2b", ("ch4", "h2o"): "ch4h2o2b", ("ch4", "c
                ("ar", "cs+"): "csar2b", ("ar", "h2o"): "arh2o2b",
                ("h2", "h2"): "h2h22b", ("h2", "h2o"): "h2oh22b", ("cs+", "h2"): "csh22b", ("nh3", "nh3"): "nh3nh32b",
                ("nh3pbe0d3bj", "nh3pbe0d3bj"): "nh3pbe2b", ("ch4", "co2"): "ch4co22b", ("mbpbe", "mbpbe"): "mbpbe2b"}
+DISPATCH_2B.update({(m, m): _CO22B[m][0] for m in CO2_MODELS})
 DISPATCH_3B = {("h2o", "h2o", "h2o"): "mbpol3b", ("ch4", "h2o", "h2o"): "ch4h2o3b",
                ("h2o", "h2o", "li+"): "h2oli3b", ("h2o", "h2o", "na+"): "h2ona3b", ("h2o", "h2o", "k+"): "h2ok3b",
                ("h2o", "h2o", "rb+"): "h2orb3b", ("cs+", "h2o", "h2o"): "h2ocs3b",
@@ -550,13 +610,16 @@ DISPATCH_3B = {("h2o", "h2o", "h2o"): "mbpol3b", ("ch4", "h2o", "h2o"): "ch4h2o3
 # four, co2 three, mbpbe like h2o three atoms and four sites, :191-233).
 MONOMER_ATOMS = {"h2o": 3, "ch4": 5, "li+": 1, "na+": 1, "k+": 1, "rb+": 1, "cs+": 1,
                  "f-": 1, "cl-": 1, "br-": 1, "i-": 1, "ar": 1, "h2": 2, "nh3": 4, "nh3pbe0d3bj": 4, "co2": 3,
-                 "mbpbe": 3}
+                 "mbpbe": 3, "co2_archive": 3, "co2cm5100": 3, "co2cm595": 3, "co2cm590": 3, "co2cm585": 3,
+                 "co2cm5875": 3, "co2cm580": 3}
 MONOMER_SITES = dict(MONOMER_ATOMS, h2o=4, mbpbe=4)
 # atom names a caller passes to AddMonomer for each id (input order)
 MONOMER_ATOM_NAMES = {"h2o": ("O", "H", "H"), "ch4": ("C", "H", "H", "H", "H"), "li+": ("Li",), "na+": ("Na",),
                       "k+": ("K",), "rb+": ("Rb",), "cs+": ("Cs",), "f-": ("F",), "cl-": ("Cl",), "br-": ("Br",),
                       "i-": ("I",), "ar": ("Ar",), "h2": ("H", "H"), "nh3": ("N", "H", "H", "H"),
                       "nh3pbe0d3bj": ("N", "H", "H", "H"), "co2": ("C", "O", "O"), "mbpbe": ("O", "H", "H")}
+MONOMER_ATOM_NAMES.update({m: ("C", "O", "O") for m in ("co2_archive", "co2cm5100", "co2cm595", "co2cm590",
+                                                         "co2cm585", "co2cm5875", "co2cm580")})
 
 
 def check():

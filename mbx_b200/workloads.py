@@ -70,7 +70,7 @@ def h2_body(r_hh=0.741):
 
 
 BODIES = {"h2o": water_body, "mbpbe": water_body, "ch4": methane_body, "nh3": ammonia_body,
-          "nh3pbe0d3bj": ammonia_body, "co2": co2_body, "h2": h2_body}
+          "nh3pbe0d3bj": ammonia_body, "co2": co2_body, "co2_archive": co2_body, "h2": h2_body}
 
 
 def molecule_box(ids, n_side=7, L=19.72, seed=0, jitter=0.3):

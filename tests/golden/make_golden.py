@@ -29,6 +29,9 @@ reference checkout, default /root/reference) and writes ``tests/golden/*.json``:
   :1943), ``unittest-energy3b.cpp`` (mbpbe x3 :911, co2 x3 :1386),
   ``unittest-poly-holder-2b.cpp`` (:1019-1546), ``unittest-poly-holder-3b.cpp``
   (:84-173);
+* CO2 - CO2 2b: ``unittest-energy2b.cpp`` (co2_archive :99, co2 :1558),
+  ``unittest-poly-holder-2b.cpp`` (x2b_A1B2_A1B2_v1x :263-560),
+  ``unittest-poly-2b.cpp`` (poly_2b_A1B2_A1B2_v1x :205-993);
 * water - water - alkali-ion 3b: ``unittest-energy3b.cpp`` (li-h2o-h2o
   :146-357, cs-h2o-h2o :358-471), ``unittest-poly-holder-3b.cpp``
   (x3b_h2o_ion_v1x_deg4_filtered :384-909, one fixture per ion),
@@ -125,6 +128,18 @@ BLOCKS += [("holder3b_%s" % f, "src/unittests/unittest-poly-holder-3b.cpp", r'TE
             r'SECTION\("%s"\)' % sec) for f, tc, sec in (
     ("mbpbe_mbpbe_mbpbe", "mbnrg_A1B2_A1B2_A1B2_deg4_vmbpbe::struct", "mbpbe-mbpbe-mbpbe"),
     ("co2_co2_co2", "mbnrg_A1B2_A1B2_A1B2_deg4_v1::struct", "co2-co2-co2"))]
+# CO2 - CO2 2b (co2_archive and co2 models)
+BLOCKS += [
+    ("energy2b_co2a_co2a", "src/unittests/unittest-energy2b.cpp", r'TEST_CASE\("energy2b::get_2b_energy"\)',
+     r'SECTION\("co2-co2"\)'),
+    ("energy2b_co2_co2", "src/unittests/unittest-energy2b.cpp", r'TEST_CASE\("energy2b::get_2b_energy"\)',
+     (r'SECTION\("co2-co2"\)', 1)),
+    ("holder2b_co2a_co2a", "src/unittests/unittest-poly-holder-2b.cpp", r'TEST_CASE\("x2b_A1B2_A1B2_v1x::struct"\)',
+     r'SECTION\("co2_archive-co2_archive"\)'),
+    ("holder2b_co2_co2", "src/unittests/unittest-poly-holder-2b.cpp", r'TEST_CASE\("x2b_A1B2_A1B2_v1x::struct"\)',
+     r'SECTION\("co2-co2"\)'),
+    ("poly_co2co22b", "src/unittests/unittest-poly-2b.cpp", r'TEST_CASE\(":poly_2b_A1B2_A1B2_v1x:struct"\)', None),
+]
 
 SYSTEMS = [
     ("system_256_h2o_cubic_box", "timing/256_h2o_cubic_box"),
@@ -169,7 +184,12 @@ def extract_blocks(ref):
         text = strip_comments(open(os.path.join(ref, rel)).read())
         pos, body = block_after(text, case)
         if section:
-            _, body = block_after(body, section)
+            # (regex, n): the n-th section with that header (0 = the first)
+            sec, nth = section if isinstance(section, tuple) else (section, 0)
+            start = 0
+            for _ in range(nth):
+                start = re.compile(sec).search(body, start).end()
+            _, body = block_after(body, sec, start)
         data = parse_block(body)
         data["_source"] = rel
         with open(os.path.join(HERE, name + ".json"), "w") as f:
