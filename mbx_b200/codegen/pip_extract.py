@@ -31,6 +31,7 @@ h2oion3b potential/3b/poly-3b-h2o-ion-v1x_deg4_filtered.cpp:39 (*)       21   10
 halh2o2b potential/2b/poly_2b_A1_B1C2X2_deg6_nograd_v1.cpp:50             8    906
 halh2o3b potential/3b/poly_3b_A1_B1C2X2_B1C2X2_deg4_nograd_v1.cpp:50      41   3173
 co2co22btab potential/2b/poly_2b_A1B2_A1B2_v1.cpp:39 (**)               15   2269
+h2oco22b potential/2b/poly_2b_A1B2Z2_C1D2_v1.cpp:39                      21   1653
 a1a12b   potential/2b/poly_2b_A1_A1_deg9_nograd_v1.cpp:50                 1    9
 a1b12b   potential/2b/poly_2b_A1_B1_deg9_nograd_v1.cpp:50                 1    9
 arh2o2b  potential/2b/poly_2b_A1_B1C2X2_deg5_nograd_v1.cpp:50             8    496
@@ -101,6 +102,7 @@ PROGRAMS = {
     "a1b12b": ("potential/2b/poly_2b_A1_B1_deg9_nograd_v1.cpp", 1, 9, 9),
     "arh2o2b": ("potential/2b/poly_2b_A1_B1C2X2_deg5_nograd_v1.cpp", 8, 496, 5),
     "co2co22btab": ("potential/2b/poly_2b_A1B2_A1B2_v1.cpp", 15, 2269, 5),
+    "h2oco22b": ("potential/2b/poly_2b_A1B2Z2_C1D2_v1.cpp", 21, 1653, 4),
 }
 # programs whose value is assigned to ``double e`` and then returned
 E_ASSIGN = {"co2co22btab"}
@@ -164,6 +166,9 @@ for _m, _name in (("co2_archive", "co2a2b"), ("co2", "co2co22b")):
     FITS[_name] = ("potential/2b/x2b_A1B2_A1B2_v1x.cpp", r'if \(mon1 == "%s" && mon2 == "%s"\) \{\s*coefficients\s*=\s*'
                    r'std::vector<double>\s*\{' % (_m, _m))
     TABLE_OF[_name] = "co2co22btab"
+FITS["h2oco22b"] = ("potential/2b/x2b_A1B2Z2_C1D2_v1x.cpp",
+                    r'if \(mon1 == "h2o" && mon2 == "co2"\) \{\s*coefficients\s*=\s*std::vector<double>\s*\{')
+TABLE_OF["h2oco22b"] = "h2oco22b"
 
 TOKEN = re.compile(
     r"\s*(?:(?P<num>\d+\.\d*(?:[eE][-+]?\d+)?|\d+(?:[eE][-+]?\d+)?)"

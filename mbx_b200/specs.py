@@ -574,6 +574,32 @@ def _co22b(model):
 
 CO22B = tuple(_co22b(m) for m in CO2_MODELS)
 
+# ---------------------------------------------------------------------------
+# H2O - CO2 2b: x2b_A1B2Z2_C1D2_v1x("h2o", "co2"), water first,
+# potential/2b/x2b_A1B2Z2_C1D2_v1x.cpp:3635-3891 (variables :3685-3711,
+# local variable::v_exp(r0, k) = exp(k (r0 - r)) :63-77; MB-pol lone pairs
+# :3683; f_switch :3503-3516 on the O-C distance, dimers beyond r2f skipped
+# :3690; constructor block :1821-3498).  The reference evaluates every CO2
+# model against water with these constants (energy2b.cpp:318-321); its
+# co2_archive block sets no switch radii and is not on this path.
+# ---------------------------------------------------------------------------
+_S_H2OCO2 = ("A", "B1", "B2", "C", "D1", "D2", "Z1", "Z2")
+_hc = dict(iAB=(4.592278064081765e-01, 4.092695741312179e-01), iBB=(1.797813612275968e+00, 2.515176186264408e+00),
+           iCD=(1.231347340156158e+00, 1.752314332686619e+00), iDD=(1.094966061053114e+00, 2.988285212499331e+00),
+           AC=(2.896045802044917e+00, 3.685742424189701e+00), AD=(1.353339012220006e+00, 3.527920970445803e+00),
+           BC=(9.715865977702702e-01, 2.782062426936132e+00), BD=(7.363939494330982e-01, 8.005028705768890e-01),
+           CZ=(8.336695227449923e-01, 5.744059557046924e+00), DZ=(1.053500025566689e+00, 3.961598744247630e+00))
+_tab = [("A", "B1", "iAB"), ("A", "B2", "iAB"), ("B1", "B2", "iBB"), ("C", "D1", "iCD"), ("C", "D2", "iCD"),
+        ("D1", "D2", "iDD"), ("A", "C", "AC"), ("A", "D1", "AD"), ("A", "D2", "AD"), ("B1", "C", "BC"),
+        ("B1", "D1", "BD"), ("B1", "D2", "BD"), ("B2", "C", "BC"), ("B2", "D1", "BD"), ("B2", "D2", "BD"),
+        ("Z1", "C", "CZ"), ("Z1", "D1", "DZ"), ("Z1", "D2", "DZ"), ("Z2", "C", "CZ"), ("Z2", "D1", "DZ"),
+        ("Z2", "D2", "DZ")]
+H2OCO22B = Spec(
+    name="h2oco22b", monomers=("h2o", "co2"), nat=(3, 3), sites=_S_H2OCO2, lp=((0, 0, 6, 7),),
+    variables=_vars(_S_H2OCO2, [("exp", a, b) + _hc[key] for a, b, key in _tab]), switch="pair", ri=8.0, rf=9.0,
+    skip="pair_gt", nvars=21, ncoef=1653, degree=4, ref="potential/2b/x2b_A1B2Z2_C1D2_v1x.cpp:3635",
+)
+
 FH2O3B = _hal3b("f-", "fh2o3b")
 CLH2O3B = _hal3b("cl-", "clh2o3b")
 BRH2O3B = _hal3b("br-", "brh2o3b")
@@ -583,7 +609,7 @@ SPECS = {s.name: s for s in (MBPOL2B, MBPOL3B, CH4H2O2B, CH4CH42B, CH4H2O3B,
                              H2OLI2B, H2ONA2B, H2OK2B, H2ORB2B, H2OCS2B,
                              H2OLI3B, H2ONA3B, H2OK3B, H2ORB3B, H2OCS3B,
                              FH2O2B, CLH2O2B, BRH2O2B, IH2O2B, FH2O3B, CLH2O3B, BRH2O3B, IH2O3B,
-                             ARH2O2B) + ATOM2B + TEMPLATE_SPECS + CO22B}
+                             ARH2O2B, H2OCO22B) + ATOM2B + TEMPLATE_SPECS + CO22B}
 
 # Dispatch by sorted monomer ids (e2b::get_2b_energy, potential/2b/energy2b.cpp:
 # 240-254,258-281,282,323; e3b::get_3b_energy, potential/3b/energy3b.cpp:185-216,
@@ -597,6 +623,7 @@ DISPATCH_2B = {("h2o", "h2o"): "mbpol2b", ("ch4", "h2o"): "ch4h2o2b", ("ch4", "c
                ("h2", "h2"): "h2h22b", ("h2", "h2o"): "h2oh22b", ("cs+", "h2"): "csh22b", ("nh3", "nh3"): "nh3nh32b",
                ("nh3pbe0d3bj", "nh3pbe0d3bj"): "nh3pbe2b", ("ch4", "co2"): "ch4co22b", ("mbpbe", "mbpbe"): "mbpbe2b"}
 DISPATCH_2B.update({(m, m): _CO22B[m][0] for m in CO2_MODELS})
+DISPATCH_2B[("co2", "h2o")] = "h2oco22b"
 DISPATCH_3B = {("h2o", "h2o", "h2o"): "mbpol3b", ("ch4", "h2o", "h2o"): "ch4h2o3b",
                ("h2o", "h2o", "li+"): "h2oli3b", ("h2o", "h2o", "na+"): "h2ona3b", ("h2o", "h2o", "k+"): "h2ok3b",
                ("h2o", "h2o", "rb+"): "h2orb3b", ("cs+", "h2o", "h2o"): "h2ocs3b",

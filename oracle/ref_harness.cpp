@@ -42,6 +42,7 @@
 #include "potential/2b/poly_2b_A1_B1_deg9_v1.h"
 #include "potential/2b/poly_2b_A1_B1C2X2_deg5_v1.h"
 #include "potential/2b/poly_2b_A1B2_A1B2_v1x.h"
+#include "potential/2b/poly_2b_A1B2Z2_C1D2_v1x.h"
 #include "potential/2b/poly_2b_A2_A2_deg6_v1.h"
 #include "potential/2b/poly_2b_A1B2Z2_C2_deg5_v1.h"
 #include "potential/2b/poly_2b_A1_B2_deg7_v1.h"
@@ -212,7 +213,8 @@ double mbxref_get_3b(const char* m1, const char* m2, const char* m3, long nm, co
 // water 2b (8), 6 water - water - alkali-ion 3b (21), 7 halide - water 2b (8),
 // 8 halide - water - water 3b (41), 9 like atoms 2b (1), 10 unlike atoms 2b (1),
 // 11 argon - water 2b (8); 12-19 the template MB-nrg tables h2h22b, h2oh22b,
-// csh22b, nh3nh32b, ch4co22b, mbpbe2b, co23b, mbpbe3b; 20 CO2 - CO2 2b (15).
+// csh22b, nh3nh32b, ch4co22b, mbpbe2b, co23b, mbpbe3b; 20 CO2 - CO2 2b (15),
+// 21 H2O - CO2 2b (21).
 // One configuration per call; g may be NULL for energy only.
 double mbxref_poly(int kind, const double* a, const double* x, double* g) {
     switch (kind) {
@@ -335,6 +337,11 @@ double mbxref_poly(int kind, const double* a, const double* x, double* g) {
         if (!g) return x2b_A1B2_A1B2_deg5::poly_2b_A1B2_A1B2_deg5_v1x::eval(a, x);
         for (int j = 0; j < 15; ++j) g[j] = 0.0;
         return x2b_A1B2_A1B2_deg5::poly_2b_A1B2_A1B2_deg5_v1x::eval(a, x, g);
+    }
+    if (kind == 21) {
+        if (!g) return x2b_A1B2Z2_C1D2_deg4::poly_2b_A1B2Z2_C1D2_deg4_v1x::eval(a, x);
+        for (int j = 0; j < 21; ++j) g[j] = 0.0;
+        return x2b_A1B2Z2_C1D2_deg4::poly_2b_A1B2Z2_C1D2_deg4_v1x::eval(a, x, g);
     }
     return 0.0;
 }

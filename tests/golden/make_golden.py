@@ -32,6 +32,9 @@ reference checkout, default /root/reference) and writes ``tests/golden/*.json``:
 * CO2 - CO2 2b: ``unittest-energy2b.cpp`` (co2_archive :99, co2 :1558),
   ``unittest-poly-holder-2b.cpp`` (x2b_A1B2_A1B2_v1x :263-560),
   ``unittest-poly-2b.cpp`` (poly_2b_A1B2_A1B2_v1x :205-993);
+* H2O - CO2 2b: ``unittest-energy2b.cpp`` (h2o-co2 :2000),
+  ``unittest-poly-holder-2b.cpp`` (x2b_A1B2Z2_C1D2_v1x h2o-co2 :562),
+  ``unittest-poly-2b.cpp`` (poly_2b_A1B2Z2_C1D2_v1x :994-1580);
 * water - water - alkali-ion 3b: ``unittest-energy3b.cpp`` (li-h2o-h2o
   :146-357, cs-h2o-h2o :358-471), ``unittest-poly-holder-3b.cpp``
   (x3b_h2o_ion_v1x_deg4_filtered :384-909, one fixture per ion),
@@ -139,6 +142,12 @@ BLOCKS += [
     ("holder2b_co2_co2", "src/unittests/unittest-poly-holder-2b.cpp", r'TEST_CASE\("x2b_A1B2_A1B2_v1x::struct"\)',
      r'SECTION\("co2-co2"\)'),
     ("poly_co2co22b", "src/unittests/unittest-poly-2b.cpp", r'TEST_CASE\(":poly_2b_A1B2_A1B2_v1x:struct"\)', None),
+    # H2O - CO2 2b (co2 model)
+    ("energy2b_h2o_co2", "src/unittests/unittest-energy2b.cpp", r'TEST_CASE\("energy2b::get_2b_energy"\)',
+     r'SECTION\("h2o-co2"\)'),
+    ("holder2b_h2o_co2", "src/unittests/unittest-poly-holder-2b.cpp", r'TEST_CASE\("x2b_A1B2Z2_C1D2_v1x::struct"\)',
+     r'SECTION\("h2o-co2"\)'),
+    ("poly_h2oco22b", "src/unittests/unittest-poly-2b.cpp", r'TEST_CASE\(":poly_2b_A1B2Z2_C1D2_v1x:struct"\)', None),
 ]
 
 SYSTEMS = [

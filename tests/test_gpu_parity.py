@@ -93,7 +93,8 @@ HOLDERS += [("holder2b_ar_ar", "arar2b"), ("holder2b_cl_cl", "clcl2b"), ("holder
 HOLDERS += [("holder2b_h2_h2", "h2h22b"), ("holder2b_h2_h2o", "h2oh22b"), ("holder2b_nh3_nh3", "nh3nh32b"),
             ("holder2b_nh3pbe_nh3pbe", "nh3pbe2b"), ("holder2b_cs_h2", "csh22b"), ("holder2b_mbpbe_mbpbe", "mbpbe2b"),
             ("holder2b_ch4_co2", "ch4co22b"), ("holder3b_mbpbe_mbpbe_mbpbe", "mbpbe3b"),
-            ("holder3b_co2_co2_co2", "co23b"), ("holder2b_co2a_co2a", "co2a2b"), ("holder2b_co2_co2", "co2co22b")]
+            ("holder3b_co2_co2_co2", "co23b"), ("holder2b_co2a_co2a", "co2a2b"), ("holder2b_co2_co2", "co2co22b"),
+            ("holder2b_h2o_co2", "h2oco22b")]
 
 
 @pytest.mark.parametrize("fixture,name", HOLDERS)
@@ -285,7 +286,7 @@ def test_solution_box(ions):
 @pytest.mark.parametrize("ids,L", [(["nh3"] * 200, 19.72), (["nh3pbe0d3bj"] * 200, 19.72),
                                    (["h2"] * 60 + ["h2o"] * 150 + ["cs+"] * 2, 19.72), (["mbpbe"] * 220, 19.72),
                                    (["ch4"] + ["h2o"] * 180 + ["na+", "cl-"], 19.72), (["co2"] * 200, 26.0),
-                                   (["co2_archive"] * 200, 26.0)])
+                                   (["co2_archive"] * 200, 26.0), (["co2"] * 30 + ["h2o"] * 250, 22.0)])
 def test_molecule_box(ids, L):
     """Liquids and mixtures of the MB-nrg types beyond water and ions on the
     GPU against the oracle (the boxes the oracle is checked on against the

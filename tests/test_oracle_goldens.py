@@ -23,7 +23,8 @@ def test_specs_consistent():
 
 POLY = [("poly_mbpol2b", "mbpol2b"), ("poly_ch4h2o2b", "ch4h2o2b"), ("poly_ch4ch42b", "ch4ch42b"),
         ("poly_ch4h2o3b", "ch4h2o3b"), ("poly_mbpol3b", "mbpol3b"), ("poly_h2oion2b", "h2oli2b"),
-        ("poly_h2oion3b", "h2oli3b"), ("poly_arh2o2b", "arh2o2b"), ("poly_co2co22b", "co2co22b")]
+        ("poly_h2oion3b", "h2oli3b"), ("poly_arh2o2b", "arh2o2b"), ("poly_co2co22b", "co2co22b"),
+        ("poly_h2oco22b", "h2oco22b")]
 
 
 @pytest.mark.parametrize("fixture,name", POLY)
@@ -76,7 +77,8 @@ DISPATCH += ["energy3b_%s_h2o_h2o" % h for h in ("f", "cl", "br", "i")]
 DISPATCH += ["energy2b_%s" % p for p in ("ar_ar", "cl_cl", "na_na", "ar_cs", "na_cl", "ar_h2o")]
 DISPATCH += ["energy2b_%s" % p for p in ("h2_h2", "h2_h2o", "nh3_nh3", "nh3pbe_nh3pbe", "h2_cs", "mbpbe_mbpbe",
                                          "ch4_co2")]
-DISPATCH += ["energy3b_mbpbe_mbpbe_mbpbe", "energy3b_co2_co2_co2", "energy2b_co2a_co2a", "energy2b_co2_co2"]
+DISPATCH += ["energy3b_mbpbe_mbpbe_mbpbe", "energy3b_co2_co2_co2", "energy2b_co2a_co2a", "energy2b_co2_co2",
+             "energy2b_h2o_co2"]
 
 
 @pytest.mark.parametrize("fixture", DISPATCH)
@@ -103,7 +105,8 @@ HOLDERS += [("holder2b_ar_ar", "arar2b"), ("holder2b_cl_cl", "clcl2b"), ("holder
 HOLDERS += [("holder2b_h2_h2", "h2h22b"), ("holder2b_h2_h2o", "h2oh22b"), ("holder2b_nh3_nh3", "nh3nh32b"),
             ("holder2b_nh3pbe_nh3pbe", "nh3pbe2b"), ("holder2b_cs_h2", "csh22b"), ("holder2b_mbpbe_mbpbe", "mbpbe2b"),
             ("holder2b_ch4_co2", "ch4co22b"), ("holder3b_mbpbe_mbpbe_mbpbe", "mbpbe3b"),
-            ("holder3b_co2_co2_co2", "co23b"), ("holder2b_co2a_co2a", "co2a2b"), ("holder2b_co2_co2", "co2co22b")]
+            ("holder3b_co2_co2_co2", "co23b"), ("holder2b_co2a_co2a", "co2a2b"), ("holder2b_co2_co2", "co2co22b"),
+            ("holder2b_h2o_co2", "h2oco22b")]
 
 
 # fixtures whose test passes the monomers to the holder in another order
@@ -146,7 +149,7 @@ def test_system_published_energies(fixture):
 REF_PROGRAM = {"mbpol2b": 0, "mbpol3b": 1, "ch4h2o2b": 2, "ch4ch42b": 3, "ch4h2o3b": 4, "h2oli2b": 5, "h2oli3b": 6,
                "fh2o2b": 7, "fh2o3b": 8, "nana2b": 9, "nacl2b": 10, "arh2o2b": 11, "h2h22b": 12, "h2oh22b": 13,
                "csh22b": 14, "nh3nh32b": 15, "ch4co22b": 16, "mbpbe2b": 17, "co23b": 18, "mbpbe3b": 19,
-               "co2co22b": 20}
+               "co2co22b": 20, "h2oco22b": 21}
 
 
 @pytest.mark.parametrize("name", list(REF_PROGRAM))
@@ -221,6 +224,8 @@ MOLECULE_BOXES = [
     # overlaps the 2.3 A long molecules)
     (["co2"] * 200, (2, 3), 26.0),
     (["co2_archive"] * 200, (2,), 26.0),
+    # CO2 in water
+    (["co2"] * 30 + ["h2o"] * 250, (2, 3), 22.0),
 ]
 
 
