@@ -124,7 +124,7 @@ class Clocks:
                 "samples": len(sm)}
 
 
-def ref_cpu(ids, xyz, box, seconds=12.0, threads=None):
+def ref_cpu(ids, xyz, box, seconds=12.0, threads=None, label="2048 H2O"):
     """The reference CPU path (oracle/_ref) on this host: (units/s, cores, sample)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import mbx_oracle as mo
@@ -135,8 +135,8 @@ def ref_cpu(ids, xyz, box, seconds=12.0, threads=None):
     r = mo.RefSystem(ids, xyz, box, CUT2, CUT3)
     nd = len(r.pair_list(2, CUT2))
     nt = len(r.pair_list(3, CUT3))
-    r.energy(2)
-    r.energy(3)
+    e2 = r.energy(2)
+    e3 = r.energy(3)
     t0 = time.perf_counter()
     steps = 0
     while True:
@@ -147,8 +147,9 @@ def ref_cpu(ids, xyz, box, seconds=12.0, threads=None):
             break
     dt = (time.perf_counter() - t0) / steps
     return {"value": (nd + nt) / dt, "unit": "n-mers/s", "cores": threads, "kind": "reference",
-            "sample": "%d full steps (TwoBodyEnergy(true)+ThreeBodyEnergy(true), 2048 H2O), %.2f s/step, "
-                      "OMP_NUM_THREADS=%d" % (steps, dt, threads), "ms_per_step": dt * 1e3}
+            "sample": "%d full steps (TwoBodyEnergy(true)+ThreeBodyEnergy(true), %s), %.2f s/step, "
+                      "OMP_NUM_THREADS=%d" % (steps, label, dt, threads), "ms_per_step": dt * 1e3,
+            "energies": {"E2B": e2, "E3B": e3}}
 
 
 def run_reference(args, rank):
@@ -240,6 +241,56 @@ def batched_leg(args, local, flush, fp64_value, dist=None, world=1):
             "speedup_vs_fp64_plain": replicas.throughput(units, ms, world) / fp64_value}
 
 
+def salt_leg(args, local, flush, cpu=True):
+    """A 1 M NaCl solution at the headline size: the 2048-site lattice box with
+    32 Na+ and 32 Cl- in place of waters, FP64 through mbx_energy_2b3b
+    (MB-pol water, the Na+/Cl- - water 2b and 3b, Na+-Na+, Cl--Cl-, Na+-Cl-
+    2b); energies against the compiled reference on the same box."""
+    import torch
+    from mbx_b200 import capi, system as msys, workloads
+    ids, xyz, box = workloads.ion_water_box(["na+", "cl-"] * 32, n_side=14, n_mol=2048, L=39.44, seed=0)
+    stream = torch.cuda.current_stream()
+    ctx = capi.Context(local, stream.cuda_stream)
+    s = msys.from_arrays(ids, xyz, box, CUT2, CUT3, context=ctx)
+    sites = torch.tensor(s.sites, dtype=torch.float64, device="cuda")
+    grad = torch.zeros_like(sites)
+    vir = np.zeros(9)
+    for _ in range(max(args.warmup, 3)):
+        grad.zero_()
+        e2, e3 = ctx.energy_2b3b(sites, grad, vir)
+    listed2, eval2 = ctx.counts(2)
+    listed3, eval3 = ctx.counts(3)
+    times = []
+    for _ in range(max(3, min(args.steps, 50))):
+        flush.zero_()
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        grad.zero_()
+        e2, e3 = ctx.energy_2b3b(sites, grad, vir)
+        b.record(stream)
+        torch.cuda.synchronize()
+        times.append(a.elapsed_time(b))
+    ctx.close()
+    ms = sum(times) / len(times)
+    units = listed2 + listed3
+    out = {"workload": "1 M NaCl: 1984 H2O + 32 Na+ + 32 Cl- on the 2048-site lattice box 39.44 A, seed 0; "
+                       "cutoffs 9/7 A",
+           "value": units / (ms * 1e-3), "unit": "n-mers/s", "ms_per_step": ms, "dtype": "f64",
+           "units_per_step": {"dimers": listed2, "trimers": listed3, "evaluated_dimers": eval2,
+                              "evaluated_trimers": eval3},
+           "energies": {"E2B": e2, "E3B": e3}}
+    if cpu:
+        cb = ref_cpu(ids, xyz, box, seconds=8.0, label="1 M NaCl, 2048 sites")
+        if cb:
+            out["cpu_reference"] = {k: cb[k] for k in ("value", "unit", "cores", "sample", "ms_per_step")}
+            out["rel_err_E2B_vs_reference"] = abs(e2 - cb["energies"]["E2B"]) / abs(cb["energies"]["E2B"])
+            out["rel_err_E3B_vs_reference"] = abs(e3 - cb["energies"]["E3B"]) / abs(cb["energies"]["E3B"])
+            out["speedup_vs_reference_cpu"] = cb["ms_per_step"] / ms
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -249,6 +300,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-configurations leg")
+    ap.add_argument("--no-salt", action="store_true", help="skip the NaCl-solution leg")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -420,6 +472,8 @@ def main():
                                        "bound": "fp32-fma"}
     if not args.no_batch:
         out["batched"] = batched_leg(args, local, flush, value, dist, world)
+    if not args.no_salt and rank == 0 and world == 1:
+        out["salt"] = salt_leg(args, local, flush, cpu=not args.no_cpu_baseline)
     if rank == 0 and not args.no_cpu_baseline:
         cb = ref_cpu(ids, xyz, box)
         if cb:
