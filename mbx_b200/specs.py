@@ -600,6 +600,33 @@ H2OCO22B = Spec(
     skip="pair_gt", nvars=21, ncoef=1653, degree=4, ref="potential/2b/x2b_A1B2Z2_C1D2_v1x.cpp:3635",
 )
 
+# ---------------------------------------------------------------------------
+# Helium: He - He 2b x2b_A1_A1_v1x (potential/2b/x2b_A1_A1_deg23_v1x.cpp:398,
+# one variable exp(k (d0 - r)) :441, degree-23 polynomial, switch 7 -> 8 A on
+# the He-He distance, block :283-316) and H2O - He 2b x2b_A1B2Z2_C1_v1x
+# (potential/2b/x2b_A1B2Z2_C1_deg5_v1x.cpp:896, water first, MB-pol lone
+# pairs :948, local v_exp / v_coul with d0 = 0 :76-122, variables :953-960,
+# switch 9.5 -> 10.5 A on the O-He distance, block :283-291).
+# ---------------------------------------------------------------------------
+HEHE2B = Spec(
+    name="hehe2b", monomers=("he", "he"), nat=(1, 1), sites=("A", "B"), lp=(),
+    variables=_vars(("A", "B"), [("exp", "A", "B", 3.224372466704150e-01, 5.731623745108086e+00)]),
+    switch="pair", ri=7.0, rf=8.0, skip="pair_gt", nvars=1, ncoef=23, degree=23,
+    ref="potential/2b/x2b_A1_A1_deg23_v1x.cpp:398",
+)
+_S_H2OHE = ("A", "B1", "B2", "C", "Z1", "Z2")
+_kAB, _kBB, _kAC, _kBC, _kCZ = (3.508775028719293e-03, 2.754491059307637e-02, 2.291365738385344e-01,
+                                7.249481919751055e-01, 1.496283150810939e-01)
+H2OHE2B = Spec(
+    name="h2ohe2b", monomers=("h2o", "he"), nat=(3, 1), sites=_S_H2OHE, lp=((0, 0, 4, 5),),
+    variables=_vars(_S_H2OHE, [("exp", "A", "B1", _kAB, 0.0), ("exp", "A", "B2", _kAB, 0.0),
+                               ("exp", "B1", "B2", _kBB, 0.0), ("exp", "A", "C", _kAC, 0.0),
+                               ("exp", "B1", "C", _kBC, 0.0), ("exp", "B2", "C", _kBC, 0.0),
+                               ("coul", "Z1", "C", _kCZ, 0.0), ("coul", "Z2", "C", _kCZ, 0.0)]),
+    switch="pair", ri=9.5, rf=10.5, skip="pair_gt", nvars=8, ncoef=496, degree=5,
+    ref="potential/2b/x2b_A1B2Z2_C1_deg5_v1x.cpp:896",
+)
+
 FH2O3B = _hal3b("f-", "fh2o3b")
 CLH2O3B = _hal3b("cl-", "clh2o3b")
 BRH2O3B = _hal3b("br-", "brh2o3b")
@@ -609,7 +636,7 @@ SPECS = {s.name: s for s in (MBPOL2B, MBPOL3B, CH4H2O2B, CH4CH42B, CH4H2O3B,
                              H2OLI2B, H2ONA2B, H2OK2B, H2ORB2B, H2OCS2B,
                              H2OLI3B, H2ONA3B, H2OK3B, H2ORB3B, H2OCS3B,
                              FH2O2B, CLH2O2B, BRH2O2B, IH2O2B, FH2O3B, CLH2O3B, BRH2O3B, IH2O3B,
-                             ARH2O2B, H2OCO22B) + ATOM2B + TEMPLATE_SPECS + CO22B}
+                             ARH2O2B, H2OCO22B, HEHE2B, H2OHE2B) + ATOM2B + TEMPLATE_SPECS + CO22B}
 
 # Dispatch by sorted monomer ids (e2b::get_2b_energy, potential/2b/energy2b.cpp:
 # 240-254,258-281,282,323; e3b::get_3b_energy, potential/3b/energy3b.cpp:185-216,
@@ -624,6 +651,8 @@ DISPATCH_2B = {("h2o", "h2o"): "mbpol2b", ("ch4", "h2o"): "ch4h2o2b", ("ch4", "c
                ("nh3pbe0d3bj", "nh3pbe0d3bj"): "nh3pbe2b", ("ch4", "co2"): "ch4co22b", ("mbpbe", "mbpbe"): "mbpbe2b"}
 DISPATCH_2B.update({(m, m): _CO22B[m][0] for m in CO2_MODELS})
 DISPATCH_2B[("co2", "h2o")] = "h2oco22b"
+DISPATCH_2B[("he", "he")] = "hehe2b"
+DISPATCH_2B[("h2o", "he")] = "h2ohe2b"
 DISPATCH_3B = {("h2o", "h2o", "h2o"): "mbpol3b", ("ch4", "h2o", "h2o"): "ch4h2o3b",
                ("h2o", "h2o", "li+"): "h2oli3b", ("h2o", "h2o", "na+"): "h2ona3b", ("h2o", "h2o", "k+"): "h2ok3b",
                ("h2o", "h2o", "rb+"): "h2orb3b", ("cs+", "h2o", "h2o"): "h2ocs3b",
@@ -638,13 +667,14 @@ DISPATCH_3B = {("h2o", "h2o", "h2o"): "mbpol3b", ("ch4", "h2o", "h2o"): "ch4h2o3
 MONOMER_ATOMS = {"h2o": 3, "ch4": 5, "li+": 1, "na+": 1, "k+": 1, "rb+": 1, "cs+": 1,
                  "f-": 1, "cl-": 1, "br-": 1, "i-": 1, "ar": 1, "h2": 2, "nh3": 4, "nh3pbe0d3bj": 4, "co2": 3,
                  "mbpbe": 3, "co2_archive": 3, "co2cm5100": 3, "co2cm595": 3, "co2cm590": 3, "co2cm585": 3,
-                 "co2cm5875": 3, "co2cm580": 3}
+                 "co2cm5875": 3, "co2cm580": 3, "he": 1}
 MONOMER_SITES = dict(MONOMER_ATOMS, h2o=4, mbpbe=4)
 # atom names a caller passes to AddMonomer for each id (input order)
 MONOMER_ATOM_NAMES = {"h2o": ("O", "H", "H"), "ch4": ("C", "H", "H", "H", "H"), "li+": ("Li",), "na+": ("Na",),
                       "k+": ("K",), "rb+": ("Rb",), "cs+": ("Cs",), "f-": ("F",), "cl-": ("Cl",), "br-": ("Br",),
                       "i-": ("I",), "ar": ("Ar",), "h2": ("H", "H"), "nh3": ("N", "H", "H", "H"),
                       "nh3pbe0d3bj": ("N", "H", "H", "H"), "co2": ("C", "O", "O"), "mbpbe": ("O", "H", "H")}
+MONOMER_ATOM_NAMES["he"] = ("He",)
 MONOMER_ATOM_NAMES.update({m: ("C", "O", "O") for m in ("co2_archive", "co2cm5100", "co2cm595", "co2cm590",
                                                          "co2cm585", "co2cm5875", "co2cm580")})
 

@@ -91,6 +91,21 @@ def molecule_box(ids, n_side=7, L=19.72, seed=0, jitter=0.3):
     return list(ids), np.concatenate(parts), box
 
 
+def dilute_box(solute, n_solute, n_water=220, dmin=6.5, n_side=7, L=19.72, seed=0):
+    """molecule_box of n_solute one-atom solutes in water whose solute-solute
+    distances (minimum image) are all at least dmin: the first seed from
+    `seed` on that gives such a box."""
+    for s in range(seed, seed + 1000):
+        ids, xyz, box = molecule_box([solute] * n_solute + ["h2o"] * n_water, n_side, L, s)
+        p = xyz[:3 * n_solute].reshape(-1, 3)
+        d = p[:, None, :] - p[None, :, :]
+        d -= L * np.round(d / L)
+        r = np.linalg.norm(d, axis=2) + np.eye(n_solute) * 1e9
+        if r.min() >= dmin:
+            return ids, xyz, box
+    raise ValueError("no dilute box found")
+
+
 def place(rng, body, centres):
     rot = random_rotations(rng, len(centres))
     return centres[:, None, :] + np.einsum("nij,aj->nai", rot, body)

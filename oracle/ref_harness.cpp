@@ -43,6 +43,8 @@
 #include "potential/2b/poly_2b_A1_B1C2X2_deg5_v1.h"
 #include "potential/2b/poly_2b_A1B2_A1B2_v1x.h"
 #include "potential/2b/poly_2b_A1B2Z2_C1D2_v1x.h"
+#include "potential/2b/poly_2b_A1_A1_deg23_v1x.h"
+#include "potential/2b/poly_2b_A1B2Z2_C1_deg5_v1x.h"
 #include "potential/2b/poly_2b_A2_A2_deg6_v1.h"
 #include "potential/2b/poly_2b_A1B2Z2_C2_deg5_v1.h"
 #include "potential/2b/poly_2b_A1_B2_deg7_v1.h"
@@ -81,6 +83,7 @@ std::vector<std::string> atom_names(const std::string& id) {
     if (id == "nh3" || id == "nh3pbe0d3bj") return {"N", "H", "H", "H"};
     if (id == "co2" || id == "co2_archive") return {"C", "O", "O"};
     if (id == "mbpbe") return {"O", "H", "H"};
+    if (id == "he") return {"He"};
     throw std::runtime_error("harness knows no atom names for monomer id " + id);
 }
 
@@ -214,7 +217,7 @@ double mbxref_get_3b(const char* m1, const char* m2, const char* m3, long nm, co
 // 8 halide - water - water 3b (41), 9 like atoms 2b (1), 10 unlike atoms 2b (1),
 // 11 argon - water 2b (8); 12-19 the template MB-nrg tables h2h22b, h2oh22b,
 // csh22b, nh3nh32b, ch4co22b, mbpbe2b, co23b, mbpbe3b; 20 CO2 - CO2 2b (15),
-// 21 H2O - CO2 2b (21).
+// 21 H2O - CO2 2b (21), 22 He - He 2b (1), 23 H2O - He 2b (8).
 // One configuration per call; g may be NULL for energy only.
 double mbxref_poly(int kind, const double* a, const double* x, double* g) {
     switch (kind) {
@@ -337,6 +340,15 @@ double mbxref_poly(int kind, const double* a, const double* x, double* g) {
         if (!g) return x2b_A1B2_A1B2_deg5::poly_2b_A1B2_A1B2_deg5_v1x::eval(a, x);
         for (int j = 0; j < 15; ++j) g[j] = 0.0;
         return x2b_A1B2_A1B2_deg5::poly_2b_A1B2_A1B2_deg5_v1x::eval(a, x, g);
+    }
+    if (kind == 22 || kind == 23) {
+        const int nv = kind == 22 ? 1 : 8;
+        if (g)
+            for (int j = 0; j < nv; ++j) g[j] = 0.0;
+        if (kind == 22) return g ? x2b_A1_A1_deg23::poly_2b_A1_A1_deg23_v1x::eval(a, x, g)
+                                 : x2b_A1_A1_deg23::poly_2b_A1_A1_deg23_v1x::eval(a, x);
+        return g ? x2b_A1B2Z2_C1_deg5::poly_2b_A1B2Z2_C1_deg5_v1x::eval(a, x, g)
+                 : x2b_A1B2Z2_C1_deg5::poly_2b_A1B2Z2_C1_deg5_v1x::eval(a, x);
     }
     if (kind == 21) {
         if (!g) return x2b_A1B2Z2_C1D2_deg4::poly_2b_A1B2Z2_C1D2_deg4_v1x::eval(a, x);

@@ -125,7 +125,7 @@ def random_nmers(name, n, seed=3):
     s = SPECS[name]
     rng = np.random.default_rng(seed)
     bodies = {m: f() for m, f in workloads.BODIES.items()}
-    for ion in ALKALI + HALIDES + ("ar",):
+    for ion in ALKALI + HALIDES + ("ar", "he"):
         bodies[ion] = np.zeros((1, 3))
     out = []
     for _ in range(n):
@@ -133,7 +133,8 @@ def random_nmers(name, n, seed=3):
         centre0 = np.zeros(3)
         for k, m in enumerate(s.monomers):
             # first-atom separations from contact (3.2 A for the 2.3 A long CO2) to beyond the cutoff
-            rmin = 3.2 if any(m.startswith("co2") for m in s.monomers) else 2.4
+            # He-He from 6 A: its degree-23 polynomial is ill-conditioned closer in
+            rmin = 3.2 if any(m.startswith("co2") for m in s.monomers) else 6.0 if name == "hehe2b" else 2.4
             c = centre0 if k == 0 else workloads._random_directions(rng, 1)[0] * rng.uniform(rmin, s.rf + 0.5)
             parts.append(workloads.place(rng, bodies[m], c[None, :])[0].reshape(-1))
         out.append(np.concatenate(parts))
@@ -286,7 +287,8 @@ def test_solution_box(ions):
 @pytest.mark.parametrize("ids,L", [(["nh3"] * 200, 19.72), (["nh3pbe0d3bj"] * 200, 19.72),
                                    (["h2"] * 60 + ["h2o"] * 150 + ["cs+"] * 2, 19.72), (["mbpbe"] * 220, 19.72),
                                    (["ch4"] + ["h2o"] * 180 + ["na+", "cl-"], 19.72), (["co2"] * 200, 26.0),
-                                   (["co2_archive"] * 200, 26.0), (["co2"] * 30 + ["h2o"] * 250, 22.0)])
+                                   (["co2_archive"] * 200, 26.0), (["co2"] * 30 + ["h2o"] * 250, 22.0),
+                                   (["he"] + ["h2o"] * 220, 19.72)])
 def test_molecule_box(ids, L):
     """Liquids and mixtures of the MB-nrg types beyond water and ions on the
     GPU against the oracle (the boxes the oracle is checked on against the
@@ -296,6 +298,13 @@ def test_molecule_box(ids, L):
     plus 1e-10 relative."""
     ids, xyz, box = workloads.molecule_box(ids, L=L, seed=3)
     compare_system(ids, xyz, box, 9.0, 7.0, g_rtol=1e-10)
+
+
+def test_helium_dilute():
+    """He in water with He-He pairs at 6.5 A and more (the He-He polynomial
+    is ill-conditioned at shorter range)."""
+    ids, xyz, box = workloads.dilute_box("he", 10, seed=1)
+    compare_system(ids, xyz, box, 9.0, 7.0)
 
 
 def test_ion_water_box_mixed():
