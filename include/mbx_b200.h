@@ -54,7 +54,9 @@ const char* mbx_version(void);
 /* Monomers in internal order (System::AddMonomerInfo, system.cpp:1794-1969):
  * ids[m] (the reference's monomer ids of this path: "h2o", "ch4", "li+",
  * "na+", "k+", "rb+", "cs+", "f-", "cl-", "br-", "i-", "ar", "h2", "nh3",
- * "nh3pbe0d3bj", "co2", "mbpbe"), first_index[m] (first site), tag[m] (tag of the
+ * "nh3pbe0d3bj", "co2", "co2_archive", "mbpbe", "he", "n2o5"; the co2cm*
+ * models are known monomers whose n-mers have no evaluator here),
+ * first_index[m] (first site), tag[m] (tag of the
  * monomer's first atom; n-mers are owned by the lowest tag,
  * sys_tools.cpp:562,585), is_local[m] (NULL = all local), numsites. */
 int mbx_set_topology(mbx_ctx* ctx, int nmon, const char* const* ids, const int* first_index, const int* tag,
@@ -92,7 +94,8 @@ int mbx_nmers(mbx_ctx* ctx, int nbody, double cutoff, const double* xyz, int use
  * 2b/x2b-v9x.h:83; x3b_v2x::eval, 3b/x3b-v2x.h:85; the MB-nrg classes):
  * n n-mers of one evaluator ("mbpol2b", "mbpol3b", "ch4h2o2b", "ch4ch42b",
  * "ch4h2o3b", the ion types "h2o<ion>2b" / "h2o<ion>3b" / "<halide>h2o2b" /
- * "<halide>h2o3b", ...; mbx_evaluator_info answers for any name), coordinates
+ * "<halide>h2o3b", "n2o5h2o2b", "n2o5h2o3b", ...; mbx_evaluator_info
+ * answers for any name), coordinates
  * xyz[n][nreal*3] with the monomers in evaluator
  * order and already imaged.  grad (same layout, +=), virial (9, +=), e_per
  * (n switched energies) may be NULL.  *energy gets the sum. */

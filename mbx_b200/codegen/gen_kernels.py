@@ -176,6 +176,9 @@ def lock_threads(nvars):
     variables and their gradient accumulators (4 registers per variable) fit
     under 168 registers, so a block of 384 threads (12 warps per SM) is
     resident; wider polynomials need the full 255 registers (256 threads)."""
+    if nvars > 56:
+        # x and g columns of 256 threads would exceed the 227 KB of shared memory
+        return 128
     return 384 if nvars <= 32 else 256
 
 
@@ -189,6 +192,10 @@ def parts_for(nterms, nvars=36):
     2048-water trimers: 1.42/1.39/1.35/1.32/1.47 ms at 300/375/450/600/700
     terms per piece, and 2.1 ms at 800-900, past the instruction cache)."""
     per = 400 if lock_threads(nvars) == 384 else 600
+    if nvars > 56:
+        # a piece loads every variable it uses into registers: fewer terms per
+        # piece for the widest polynomials
+        per = 200
     return max(1, (nterms + per - 1) // per)
 
 
@@ -493,9 +500,11 @@ def emit_traits(spec, table, straight, out):
     w("    static constexpr int NAT0 = %d, NAT1 = %d, NAT2 = %d;" % tuple(nat))
     w("    static constexpr int FIRST0 = %d, FIRST1 = %d, FIRST2 = %d;" % tuple(first))
     w("    static constexpr int SWITCH_TRIPLE = %d, SKIP = %d, STRAIGHT = %d, DEGREE = %d;" %
-      ({"pair": 0, "triple": 1, "triple2": 2}[spec.switch], {"pair_gt": 0, "two_of_three_gt": 1, "all_three_gt": 2}[spec.skip],
+      ({"pair": 0, "triple": 1, "triple2": 2, "cos2": 3}[spec.switch], {"pair_gt": 0, "two_of_three_gt": 1, "all_three_gt": 2}[spec.skip],
        1 if straight else 0, spec.degree))
     w("    static constexpr double RI = %s, RF = %s;" % (lit(spec.ri), lit(spec.rf)))
+    w("    static constexpr int VIRIAL_RAW = %d;  // virial of the unswitched polynomial gradient" %
+      (1 if spec.virial == "raw" else 0))
     w("    static constexpr int LOCK_THREADS = %d;  // threads of a lockstep evaluation block" %
       lock_threads(spec.nvars))
     shifted_type = straight and n in SHIFT_TYPES
@@ -775,7 +784,8 @@ int mbx_launch_%(name)s_w(const HolderArgs& A, int grads, int grid, cudaStream_t
 # ~10 MB of code (ptxas compiles the trie's pieces once per calling kernel),
 # so their raw-polynomial (mbx_poly) and coefficient-adjoint
 # (mbx_evaluate_dcoef) entries answer MBX_ENOTSUP.
-LEAN_TYPES = {"nh3nh32b", "nh3pbe2b", "ch4co22b", "mbpbe2b", "co23b", "mbpbe3b", "co2co22b", "co2a2b"}
+LEAN_TYPES = {"nh3nh32b", "nh3pbe2b", "ch4co22b", "mbpbe2b", "co23b", "mbpbe3b", "co2co22b", "co2a2b",
+              "n2o5h2o3b"}
 
 
 def variants_of(name):

@@ -56,10 +56,10 @@ SOURCES = {
               "potential/3b/poly_3b_A1B2_A1B2_A1B2_deg4_v1.h"),
     "mbpbe3b": ("potential/3b/mbnrg_3b_A1B2_A1B2_A1B2_deg4_vmbpbe.cpp", ("mbpbe", "mbpbe", "mbpbe"), "mbpbe3b",
                 "potential/3b/poly_3b_A1B2_A1B2_A1B2_deg4_vmbpbe.h"),
+    # switches with 1 - cos^2((s12 + s13 + s23 - 1) pi / 2) (the "cos2" form)
+    "n2o5h2o3b": ("potential/3b/mbnrg_3b_A1B2C4_D1E2_D1E2_deg3_v1.cpp", ("n2o5", "h2o", "h2o"), "n2o5h2o3b",
+                  "potential/3b/poly_3b_A1B2C4_D1E2_D1E2_deg3_v1.h"),
 }
-# Not in the template: mbnrg_3b_A1B2C4_D1E2_D1E2_deg3_v1 (n2o5-h2o-h2o) switches
-# with 1 - cos^2((s12 + s13 + s23 - 1) pi / 2), potential/3b/
-# mbnrg_3b_A1B2C4_D1E2_D1E2_deg3_v1.cpp:2464-2471.
 
 # the energy-only program of each table (pip_extract)
 PROGRAMS = {
@@ -71,6 +71,7 @@ PROGRAMS = {
     "mbpbe2b": "potential/2b/poly_2b_A1B2Z2_A1B2Z2_deg4_nograd_vmbpbe.cpp",
     "co23b": "potential/3b/poly_3b_A1B2_A1B2_A1B2_deg4_nograd_v1.cpp",
     "mbpbe3b": "potential/3b/poly_3b_A1B2_A1B2_A1B2_deg4_nograd_vmbpbe.cpp",
+    "n2o5h2o3b": "potential/3b/poly_3b_A1B2C4_D1E2_D1E2_deg3_nograd_v1.cpp",
 }
 
 
@@ -184,9 +185,19 @@ def extract(ref, name, source, mons, table, header):
         p, q = p.replace("coords_", ""), q.replace("coords_", "")
         variables.append(("exp" if kind.startswith("v_exp") else "coul", sites.index(p), sites.index(q), k, d0))
     # switch and skip
-    sw = _ws(re.search(r"\bsw\s*=\s*(sw[^;]*);", body).group(1))
     forms = {"sw12": "pair", "sw12*sw13+sw12*sw23+sw13*sw23": "triple",
              "sw12*sw13+sw12*sw23+sw13*sw23-2*sw12*sw23*sw13": "triple2"}
+    cos2 = ("if((sw12+sw13+sw23)<1.0){sw=0.0;}elseif((sw12+sw13+sw23)>2.0){sw=1.0;}"
+            "else{sw=std::cos((sw12+sw13+sw23-1.0)*M_PI/2.0);sw=1.0-sw*sw;}")
+    cos2_grad = ("if((sw12+sw13+sw23)>1.0&&(sw12+sw13+sw23)<2.0){"
+                 "gsw12*=-(M_PI/2.0)*sin(M_PI*(sw12+sw13+sw23))*energies[j]/d12r;")
+    if cos2 in _ws(body):
+        if cos2_grad not in _ws(body):
+            raise ValueError("%s: cos2 switch without its gradient" % source)
+        sw = "cos2"
+        forms[sw] = "cos2"
+    else:
+        sw = _ws(re.search(r"\bsw\s*=\s*(sw[^;]*);", body).group(1))
     if sw not in forms:
         raise ValueError("%s: switch %s is not supported" % (source, sw))
     skip_expr = _ws(re.search(r"if\s*\(\s*true\s*&&\s*([^{]*)\)\s*\{\s*continue\s*;", body).group(1))

@@ -34,6 +34,7 @@ co2co22btab potential/2b/poly_2b_A1B2_A1B2_v1.cpp:39 (**)               15   226
 h2oco22b potential/2b/poly_2b_A1B2Z2_C1D2_v1.cpp:39                      21   1653
 hehe2b   potential/2b/poly_2b_A1_A1_deg23_v1.cpp:5                        1    23
 h2ohe2b  potential/2b/poly_2b_A1B2Z2_C1_deg5_v1.cpp:5                     8    496
+n2o5h2o2b potential/2b/poly_2b_A1B2C4_D1E2_deg3_v1.cpp:5                 45   983
 a1a12b   potential/2b/poly_2b_A1_A1_deg9_nograd_v1.cpp:50                 1    9
 a1b12b   potential/2b/poly_2b_A1_B1_deg9_nograd_v1.cpp:50                 1    9
 arh2o2b  potential/2b/poly_2b_A1_B1C2X2_deg5_nograd_v1.cpp:50             8    496
@@ -107,6 +108,7 @@ PROGRAMS = {
     "h2oco22b": ("potential/2b/poly_2b_A1B2Z2_C1D2_v1.cpp", 21, 1653, 4),
     "hehe2b": ("potential/2b/poly_2b_A1_A1_deg23_v1.cpp", 1, 23, 23),
     "h2ohe2b": ("potential/2b/poly_2b_A1B2Z2_C1_deg5_v1.cpp", 8, 496, 5),
+    "n2o5h2o2b": ("potential/2b/poly_2b_A1B2C4_D1E2_deg3_v1.cpp", 45, 983, 3),
 }
 # programs whose value is assigned to ``double e`` and then returned
 E_ASSIGN = {"co2co22btab"}
@@ -173,6 +175,9 @@ for _m, _name in (("co2_archive", "co2a2b"), ("co2", "co2co22b")):
 FITS["h2oco22b"] = ("potential/2b/x2b_A1B2Z2_C1D2_v1x.cpp",
                     r'if \(mon1 == "h2o" && mon2 == "co2"\) \{\s*coefficients\s*=\s*std::vector<double>\s*\{')
 TABLE_OF["h2oco22b"] = "h2oco22b"
+FITS["n2o5h2o2b"] = ("potential/2b/x2b_A1B2C4_D1E2_deg3_v1x.cpp",
+                     r'if \(mon1 == "h2o" && mon2 == "n2o5"\) \{\s*coefficients\s*=\s*std::vector<double>\s*\{')
+TABLE_OF["n2o5h2o2b"] = "n2o5h2o2b"
 FITS["hehe2b"] = ("potential/2b/x2b_A1_A1_deg23_v1x.cpp",
                   r'if \( mon1 == "he" && mon2 == "he" \) \{\s*coefficients\s*=\s*std::vector<double>\s*\{')
 FITS["h2ohe2b"] = ("potential/2b/x2b_A1B2Z2_C1_deg5_v1x.cpp",

@@ -166,11 +166,31 @@ __device__ __forceinline__ double apply_switch(const double (&d)[3][3], const do
         }
         return sw;
     }
-    // SWITCH_TRIPLE 1: s0 s1 + s0 s2 + s1 s2; 2: the same minus 2 s0 s1 s2
+    // SWITCH_TRIPLE 1: s0 s1 + s0 s2 + s1 s2; 2: the same minus 2 s0 s1 s2;
+    // 3: 1 - cos^2((S - 1) pi / 2) on S = s0 + s1 + s2, 0 below S = 1 and 1
+    // above S = 2 (mbnrg_3b_A1B2C4_D1E2_D1E2_deg3_v1.cpp:2464-2471, gradient
+    // -(pi / 2) sin(pi S) strictly inside (1, 2), :2563-2570)
     double g0, g1, g2;
     const double s0 = f_switch(rr[0], T::RI, T::RF, g0);
     const double s1 = f_switch(rr[1], T::RI, T::RF, g1);
     const double s2 = f_switch(rr[2], T::RI, T::RF, g2);
+    if (T::SWITCH_TRIPLE == 3) {
+        const double S = s0 + s1 + s2;
+        if (grads && S > 1.0 && S < 2.0) {
+            const double dS = -(M_PI / 2.0) * sin(M_PI * S) * ep;
+            const double f0 = g0 * dS / rr[0], f1 = g1 * dS / rr[1], f2 = g2 * dS / rr[2];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                tg[first[0]][c] += f0 * d[0][c] + f1 * d[1][c];
+                tg[first[1]][c] += f2 * d[2][c] - f0 * d[0][c];
+                tg[first[2]][c] -= f1 * d[1][c] + f2 * d[2][c];
+            }
+        }
+        if (S < 1.0) return 0.0;
+        if (S > 2.0) return 1.0;
+        const double cs = cos((S - 1.0) * M_PI / 2.0);
+        return 1.0 - cs * cs;
+    }
     const double c = T::SWITCH_TRIPLE == 2 ? 2.0 : 0.0;
     if (grads) {
         const double f0 = g0 * (s1 + s2 - c * s1 * s2) * ep / rr[0];
@@ -220,17 +240,8 @@ __device__ __forceinline__ void finish_nmer(const HolderArgs& A, long t, double 
             for (int c = 0; c < 3; ++c) tg[i][c] = sg[i][c];
     }
     const double sw = apply_switch<T>(d, rr, ep, tg, false);
-    if (grads) {
-#pragma unroll
-        for (int i = 0; i < T::NREAL; ++i)
-#pragma unroll
-            for (int c = 0; c < 3; ++c) tg[i][c] *= sw;
-        apply_switch<T>(d, rr, ep, tg, true);
-    }
-    const double es = sw * ep;
-    if (A.e_per) A.e_per[t] = es;
-    double v[7] = {es, 0, 0, 0, 0, 0, 0};
-    if (grads) {
+    double v[7] = {0, 0, 0, 0, 0, 0, 0};
+    auto virial = [&]() {
 #pragma unroll
         for (int i = 0; i < T::NREAL; ++i) {
             v[1] -= r[i][0] * tg[i][0];
@@ -240,7 +251,21 @@ __device__ __forceinline__ void finish_nmer(const HolderArgs& A, long t, double 
             v[5] -= r[i][1] * tg[i][2];
             v[6] -= r[i][2] * tg[i][2];
         }
+    };
+    if (grads) {
+        // VIRIAL_RAW: the evaluator's virial is that of the polynomial
+        // gradient alone, before the switch (x2b_A1B2C4_D1E2_deg3_v1x.cpp:1353-1391)
+        if (T::VIRIAL_RAW) virial();
+#pragma unroll
+        for (int i = 0; i < T::NREAL; ++i)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) tg[i][c] *= sw;
+        apply_switch<T>(d, rr, ep, tg, true);
+        if (!T::VIRIAL_RAW) virial();
     }
+    const double es = sw * ep;
+    if (A.e_per) A.e_per[t] = es;
+    v[0] = es;
     if (A.conf_out) {
         conf_accumulate(A.conf_out + 8 * __ldg(A.mon_conf + __ldg(A.nmers + t).x), v);
     } else {

@@ -58,7 +58,7 @@ class Spec:
     sites: Tuple[str, ...]     # real atoms in holder order, then virtual sites
     lp: Tuple[Tuple[int, int, int, int], ...]  # (monomer, first real site, X+ site, X- site)
     variables: Tuple[Tuple[str, int, int, float, float], ...]  # (kind, site1, site2, k, d0)
-    switch: str                # "pair", "triple" or "triple2"
+    switch: str                # "pair", "triple", "triple2" or "cos2"
     ri: float
     rf: float
     skip: str                  # "pair_gt", "two_of_three_gt", "all_three_gt"
@@ -67,6 +67,10 @@ class Spec:
     degree: int
     ref: str                   # reference evaluator (file:line)
     table: str = ""            # PIP table in mbx_b200/data when shared by several evaluators ("": name)
+    # "raw": the evaluator's virial sums -r . g over the polynomial gradient
+    # alone (no switch factor, no switch gradient), as the reference's
+    # x2b_A1B2C4_D1E2_v1x does; "": over the switched gradient
+    virial: str = ""
 
     @property
     def pip_table(self):
@@ -498,7 +502,8 @@ ARH2O2B = Spec(
 # 3b): their specs are read from the reference's sources by
 # codegen/mbnrg_spec.py into data/<name>.spec.json (same fields as above).
 # ---------------------------------------------------------------------------
-EXTRACTED = ("h2h22b", "h2oh22b", "csh22b", "nh3nh32b", "nh3pbe2b", "ch4co22b", "mbpbe2b", "co23b", "mbpbe3b")
+EXTRACTED = ("h2h22b", "h2oh22b", "csh22b", "nh3nh32b", "nh3pbe2b", "ch4co22b", "mbpbe2b", "co23b", "mbpbe3b",
+             "n2o5h2o3b")
 
 
 def _load_extracted(name):
@@ -627,6 +632,38 @@ H2OHE2B = Spec(
     ref="potential/2b/x2b_A1B2Z2_C1_deg5_v1x.cpp:896",
 )
 
+# ---------------------------------------------------------------------------
+# N2O5 - H2O 2b: x2b_A1B2C4_D1E2_v1x("h2o", "n2o5"), N2O5 first (sites A =
+# bridging O, B = N, C = terminal O; water D = O, E = H),
+# potential/2b/x2b_A1B2C4_D1E2_deg3_v1x.cpp:1183 (variables exp(-k r) with the
+# local variable::v_exp :19-34, listed :1226-1270; switch 8 -> 9 A on the
+# bridging-O - water-O distance, dimers beyond r2f skipped :1200; constructor
+# block :59-1060).  Its virial sums -r . g over the polynomial's own gradient,
+# before the switch factor and without the switch gradient (:1353-1391), so
+# it differs from -r . (total gradient) for dimers between 8 and 9 A.
+# N2O5 - H2O - H2O 3b is the template evaluator
+# mbnrg_3b_A1B2C4_D1E2_D1E2_deg3_v1 with the cos2 switch (extracted spec).
+# ---------------------------------------------------------------------------
+_S_N2O5H2O = ("A", "B1", "B2", "C1", "C2", "C3", "C4", "D", "E1", "E2")
+_kn = dict(AD=7.286306346099436e-01, AE=7.828602981218888e-01, BD=3.351348473713356e-01, BE=3.639320594943890e-01,
+           CD=6.858079184494418e-01, CE=6.808310453124187e-01, BB=6.196445062175264e-01, CC=3.302260758676124e-01,
+           AB=8.129813213030901e-01, AC=4.872207055177465e-01, BC=9.817144022006012e-01, EE=1.532053819248005e-01,
+           DE=1.268361659534204e+00)
+_C4 = ("C1", "C2", "C3", "C4")
+_tab = ([("B1", "B2", "BB")] + [(a, b, "CC") for i, a in enumerate(_C4) for b in _C4[i + 1:]] +
+        [("A", b, "AB") for b in ("B1", "B2")] + [("A", c, "AC") for c in _C4] +
+        [(b, c, "BC") for b in ("B1", "B2") for c in _C4] + [("E1", "E2", "EE"), ("D", "E1", "DE"), ("D", "E2", "DE"),
+                                                             ("A", "D", "AD"), ("A", "E1", "AE"), ("A", "E2", "AE"),
+                                                             ("B1", "D", "BD"), ("B2", "D", "BD")] +
+        [(b, e, "BE") for b in ("B1", "B2") for e in ("E1", "E2")] + [(c, "D", "CD") for c in _C4] +
+        [(c, e, "CE") for c in _C4 for e in ("E1", "E2")])
+N2O5H2O2B = Spec(
+    name="n2o5h2o2b", monomers=("n2o5", "h2o"), nat=(7, 3), sites=_S_N2O5H2O, lp=(),
+    variables=_vars(_S_N2O5H2O, [("exp", a, b, _kn[key], 0.0) for a, b, key in _tab]), switch="pair", ri=8.0,
+    rf=9.0, skip="pair_gt", nvars=45, ncoef=983, degree=3, ref="potential/2b/x2b_A1B2C4_D1E2_deg3_v1x.cpp:1183",
+    virial="raw",
+)
+
 FH2O3B = _hal3b("f-", "fh2o3b")
 CLH2O3B = _hal3b("cl-", "clh2o3b")
 BRH2O3B = _hal3b("br-", "brh2o3b")
@@ -636,7 +673,7 @@ SPECS = {s.name: s for s in (MBPOL2B, MBPOL3B, CH4H2O2B, CH4CH42B, CH4H2O3B,
                              H2OLI2B, H2ONA2B, H2OK2B, H2ORB2B, H2OCS2B,
                              H2OLI3B, H2ONA3B, H2OK3B, H2ORB3B, H2OCS3B,
                              FH2O2B, CLH2O2B, BRH2O2B, IH2O2B, FH2O3B, CLH2O3B, BRH2O3B, IH2O3B,
-                             ARH2O2B, H2OCO22B, HEHE2B, H2OHE2B) + ATOM2B + TEMPLATE_SPECS + CO22B}
+                             ARH2O2B, H2OCO22B, HEHE2B, H2OHE2B, N2O5H2O2B) + ATOM2B + TEMPLATE_SPECS + CO22B}
 
 # Dispatch by sorted monomer ids (e2b::get_2b_energy, potential/2b/energy2b.cpp:
 # 240-254,258-281,282,323; e3b::get_3b_energy, potential/3b/energy3b.cpp:185-216,
@@ -653,11 +690,13 @@ DISPATCH_2B.update({(m, m): _CO22B[m][0] for m in CO2_MODELS})
 DISPATCH_2B[("co2", "h2o")] = "h2oco22b"
 DISPATCH_2B[("he", "he")] = "hehe2b"
 DISPATCH_2B[("h2o", "he")] = "h2ohe2b"
+DISPATCH_2B[("h2o", "n2o5")] = "n2o5h2o2b"
 DISPATCH_3B = {("h2o", "h2o", "h2o"): "mbpol3b", ("ch4", "h2o", "h2o"): "ch4h2o3b",
                ("h2o", "h2o", "li+"): "h2oli3b", ("h2o", "h2o", "na+"): "h2ona3b", ("h2o", "h2o", "k+"): "h2ok3b",
                ("h2o", "h2o", "rb+"): "h2orb3b", ("cs+", "h2o", "h2o"): "h2ocs3b",
                ("f-", "h2o", "h2o"): "fh2o3b", ("cl-", "h2o", "h2o"): "clh2o3b", ("br-", "h2o", "h2o"): "brh2o3b",
-               ("h2o", "h2o", "i-"): "ih2o3b", ("co2", "co2", "co2"): "co23b", ("mbpbe", "mbpbe", "mbpbe"): "mbpbe3b"}
+               ("h2o", "h2o", "i-"): "ih2o3b", ("co2", "co2", "co2"): "co23b", ("mbpbe", "mbpbe", "mbpbe"): "mbpbe3b",
+               ("h2o", "h2o", "n2o5"): "n2o5h2o3b"}
 
 # Real atoms and total sites (real + electrostatic virtual sites) per monomer
 # type, as the reference's monomer table sets them (bblock/sys_tools.cpp
@@ -667,7 +706,7 @@ DISPATCH_3B = {("h2o", "h2o", "h2o"): "mbpol3b", ("ch4", "h2o", "h2o"): "ch4h2o3
 MONOMER_ATOMS = {"h2o": 3, "ch4": 5, "li+": 1, "na+": 1, "k+": 1, "rb+": 1, "cs+": 1,
                  "f-": 1, "cl-": 1, "br-": 1, "i-": 1, "ar": 1, "h2": 2, "nh3": 4, "nh3pbe0d3bj": 4, "co2": 3,
                  "mbpbe": 3, "co2_archive": 3, "co2cm5100": 3, "co2cm595": 3, "co2cm590": 3, "co2cm585": 3,
-                 "co2cm5875": 3, "co2cm580": 3, "he": 1}
+                 "co2cm5875": 3, "co2cm580": 3, "he": 1, "n2o5": 7}
 MONOMER_SITES = dict(MONOMER_ATOMS, h2o=4, mbpbe=4)
 # atom names a caller passes to AddMonomer for each id (input order)
 MONOMER_ATOM_NAMES = {"h2o": ("O", "H", "H"), "ch4": ("C", "H", "H", "H", "H"), "li+": ("Li",), "na+": ("Na",),
@@ -675,6 +714,9 @@ MONOMER_ATOM_NAMES = {"h2o": ("O", "H", "H"), "ch4": ("C", "H", "H", "H", "H"), 
                       "i-": ("I",), "ar": ("Ar",), "h2": ("H", "H"), "nh3": ("N", "H", "H", "H"),
                       "nh3pbe0d3bj": ("N", "H", "H", "H"), "co2": ("C", "O", "O"), "mbpbe": ("O", "H", "H")}
 MONOMER_ATOM_NAMES["he"] = ("He",)
+# n2o5: bridging O, the two N, then the four terminal O (bonds 0-1, 0-2, 1-3,
+# 1-4, 2-5, 2-6, bblock/sys_tools.cpp:725-733)
+MONOMER_ATOM_NAMES["n2o5"] = ("O", "N", "N", "O", "O", "O", "O")
 MONOMER_ATOM_NAMES.update({m: ("C", "O", "O") for m in ("co2_archive", "co2cm5100", "co2cm595", "co2cm590",
                                                          "co2cm585", "co2cm5875", "co2cm580")})
 

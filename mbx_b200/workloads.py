@@ -69,8 +69,26 @@ def h2_body(r_hh=0.741):
     return np.array([[0.0, 0.0, 0.0], [0.0, 0.0, r_hh]])
 
 
+def n2o5_body(r_on=1.50, r_no=1.19, a_non=112.0, a_ono=134.0):
+    """O2N-O-NO2: the bridging O first, the two N (N-O-N angle a_non), then
+    each N's two terminal O (O-N-O angle a_ono) above and below the N-O-N
+    plane, the bridging O - N bond bisecting them."""
+    h = np.radians(a_non) / 2.0
+    t = np.radians(a_ono) / 2.0
+    atoms = [[0.0, 0.0, 0.0]]
+    ns = []
+    for sgn in (1.0, -1.0):
+        u = np.array([sgn * np.sin(h), -np.cos(h), 0.0])
+        ns.append((r_on * u, u))
+        atoms.append(r_on * u)
+    for n, u in ns:
+        for z in (1.0, -1.0):
+            atoms.append(n + r_no * (np.cos(t) * u + z * np.sin(t) * np.array([0.0, 0.0, 1.0])))
+    return np.array(atoms)
+
+
 BODIES = {"h2o": water_body, "mbpbe": water_body, "ch4": methane_body, "nh3": ammonia_body,
-          "nh3pbe0d3bj": ammonia_body, "co2": co2_body, "co2_archive": co2_body, "h2": h2_body}
+          "nh3pbe0d3bj": ammonia_body, "co2": co2_body, "co2_archive": co2_body, "h2": h2_body, "n2o5": n2o5_body}
 
 
 def molecule_box(ids, n_side=7, L=19.72, seed=0, jitter=0.3):

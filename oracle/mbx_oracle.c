@@ -313,6 +313,20 @@ double mbxo_pip_eval(int nvars, long nterms, const int *tk, const double *tc, co
 
 /* ------------------------------------------------------------ evaluators */
 
+/* Switch of the N2O5 - H2O - H2O 3b on S = s12 + s13 + s23
+ * (mbnrg_3b_A1B2C4_D1E2_D1E2_deg3_v1.cpp:2464-2471, gradient :2563-2570):
+ * 0 for S < 1, 1 for S > 2, 1 - cos^2((S - 1) pi / 2) between; *dS (optional)
+ * gets dsw/dS = -(pi / 2) sin(pi S) strictly inside (1, 2), else 0. */
+static double switch_cos2(double S, double *dS) {
+    if (dS) *dS = (S > 1.0 && S < 2.0) ? -(M_PI / 2.0) * sin(M_PI * S) : 0.0;
+    if (S < 1.0) return 0.0;
+    if (S > 2.0) return 1.0;
+    double c = cos((S - 1.0) * M_PI / 2.0);
+    return 1.0 - c * c;
+}
+
+#define MBXO_MAXV 128  /* polynomial variables of one evaluator, at most */
+
 typedef struct {
     int nbody;
     int nreal;      /* real atoms across the n-mer, holder order */
@@ -321,13 +335,15 @@ typedef struct {
     int nlp;        /* lone-pair pairs */
     int lp[3][4];   /* (monomer, first real site, X+ site, X- site) */
     int nvars;
-    int vkind[64];  /* 0 exp, 1 coul */
-    int vs1[64], vs2[64];
-    double vk[64], vd[64];
-    int sw_triple;  /* 0 pair, 1 triple, 2 triple minus 2 s0 s1 s2 */
+    int vkind[MBXO_MAXV];  /* 0 exp, 1 coul */
+    int vs1[MBXO_MAXV], vs2[MBXO_MAXV];
+    double vk[MBXO_MAXV], vd[MBXO_MAXV];
+    int sw_triple;  /* 0 pair, 1 triple, 2 triple minus 2 s0 s1 s2, 3 1 - cos^2((S - 1) pi / 2), S = s0+s1+s2 */
     double ri, rf;
     int skip;       /* 0 pair_gt, 1 two_of_three_gt, 2 all_three_gt */
     double gin, gout;
+    int virial_raw; /* 1: virial over the unswitched polynomial gradient
+                       (x2b_A1B2C4_D1E2_deg3_v1x.cpp:1353-1391) */
 } mbxo_spec;
 
 static double f_switch(double r, double ri, double rf, double *g) {
@@ -415,7 +431,7 @@ double mbxo_holder_eval(const mbxo_spec *s, long nterms, const int *tk, const do
             for (int c = 0; c < 3; ++c) sites[i][c] = w[3 * i + c];
         for (int l = 0; l < s->nlp; ++l)
             lp_setup(sites[s->lp[l][1]], s->gin, s->gout, sites[s->lp[l][2]], sites[s->lp[l][3]], oh1[l], oh2[l]);
-        double x[64], gx[64], dv[64][3];
+        double x[MBXO_MAXV], gx[MBXO_MAXV], dv[MBXO_MAXV][3];
         for (int v = 0; v < s->nvars; ++v) {
             const double *p1 = sites[s->vs1[v]], *p2 = sites[s->vs2[v]];
             double g0 = p1[0] - p2[0], g1 = p1[1] - p2[1], g2 = p1[2] - p2[2];
@@ -444,6 +460,7 @@ double mbxo_holder_eval(const mbxo_spec *s, long nterms, const int *tk, const do
             for (int p = 0; p < 3; ++p) sp[p] = f_switch(r[p], s->ri, s->rf, &gp[p]);
             sw = sp[0] * sp[1] + sp[0] * sp[2] + sp[1] * sp[2];
             if (s->sw_triple == 2) sw -= 2.0 * sp[0] * sp[1] * sp[2];
+            if (s->sw_triple == 3) sw = switch_cos2(sp[0] + sp[1] + sp[2], NULL);
         }
         double es = sw * ep;
         etot += es;
@@ -473,9 +490,15 @@ double mbxo_holder_eval(const mbxo_spec *s, long nterms, const int *tk, const do
             }
         } else {
             double c2 = s->sw_triple == 2 ? 2.0 : 0.0;
-            gsw[0] = gp[0] * (sp[1] + sp[2] - c2 * sp[1] * sp[2]) * ep / r[0];
-            gsw[1] = gp[1] * (sp[0] + sp[2] - c2 * sp[0] * sp[2]) * ep / r[1];
-            gsw[2] = gp[2] * (sp[0] + sp[1] - c2 * sp[0] * sp[1]) * ep / r[2];
+            if (s->sw_triple == 3) {
+                double dS;
+                switch_cos2(sp[0] + sp[1] + sp[2], &dS);
+                for (int p = 0; p < 3; ++p) gsw[p] = gp[p] * dS * ep / r[p];
+            } else {
+                gsw[0] = gp[0] * (sp[1] + sp[2] - c2 * sp[1] * sp[2]) * ep / r[0];
+                gsw[1] = gp[1] * (sp[0] + sp[2] - c2 * sp[0] * sp[2]) * ep / r[1];
+                gsw[2] = gp[2] * (sp[0] + sp[1] - c2 * sp[0] * sp[1]) * ep / r[2];
+            }
             for (int c = 0; c < 3; ++c) {
                 tg[first[0]][c] += gsw[0] * d[0][c] + gsw[1] * d[1][c];
                 tg[first[1]][c] += gsw[2] * d[2][c] - gsw[0] * d[0][c];
@@ -486,12 +509,13 @@ double mbxo_holder_eval(const mbxo_spec *s, long nterms, const int *tk, const do
             for (int c = 0; c < 3; ++c) gout[3 * i + c] += tg[i][c];
         for (int i = 0; i < s->nreal; ++i) {
             const double *q = w + 3 * i;
-            vir[0] -= q[0] * tg[i][0];
-            vir[1] -= q[0] * tg[i][1];
-            vir[2] -= q[0] * tg[i][2];
-            vir[3] -= q[1] * tg[i][1];
-            vir[4] -= q[1] * tg[i][2];
-            vir[5] -= q[2] * tg[i][2];
+            const double *vg = s->virial_raw ? sg[i] : tg[i];
+            vir[0] -= q[0] * vg[0];
+            vir[1] -= q[0] * vg[1];
+            vir[2] -= q[0] * vg[2];
+            vir[3] -= q[1] * vg[1];
+            vir[4] -= q[1] * vg[2];
+            vir[5] -= q[2] * vg[2];
         }
     }
     /* the reference fills the lower triangle from the upper one
@@ -536,7 +560,7 @@ int mbxo_holder_dcoef(const mbxo_spec *s, int ncoef, long nterms, const int *tk,
     else
         skip = r[0] > s->rf && r[1] > s->rf && r[2] > s->rf;
     if (skip) return 0;
-    double sites[32][3], oh1[3][3], oh2[3][3], x[64];
+    double sites[32][3], oh1[3][3], oh2[3][3], x[MBXO_MAXV];
     for (int i = 0; i < s->nreal; ++i)
         for (int c = 0; c < 3; ++c) sites[i][c] = w[3 * i + c];
     for (int l = 0; l < s->nlp; ++l)
@@ -555,6 +579,7 @@ int mbxo_holder_dcoef(const mbxo_spec *s, int ncoef, long nterms, const int *tk,
         for (int p = 0; p < 3; ++p) sp[p] = f_switch(r[p], s->ri, s->rf, &gp[p]);
         sw = sp[0] * sp[1] + sp[0] * sp[2] + sp[1] * sp[2];
         if (s->sw_triple == 2) sw -= 2.0 * sp[0] * sp[1] * sp[2];
+        if (s->sw_triple == 3) sw = switch_cos2(sp[0] + sp[1] + sp[2], NULL);
     }
     for (long t = 0; t < nterms; ++t) {
         double m = tc[t];

@@ -50,10 +50,10 @@ class _Spec(ctypes.Structure):
     _fields_ = [
         ("nbody", ctypes.c_int), ("nreal", ctypes.c_int), ("nsites", ctypes.c_int), ("nat", ctypes.c_int * 3),
         ("nlp", ctypes.c_int), ("lp", (ctypes.c_int * 4) * 3), ("nvars", ctypes.c_int),
-        ("vkind", ctypes.c_int * 64), ("vs1", ctypes.c_int * 64), ("vs2", ctypes.c_int * 64),
-        ("vk", ctypes.c_double * 64), ("vd", ctypes.c_double * 64), ("sw_triple", ctypes.c_int),
+        ("vkind", ctypes.c_int * 128), ("vs1", ctypes.c_int * 128), ("vs2", ctypes.c_int * 128),
+        ("vk", ctypes.c_double * 128), ("vd", ctypes.c_double * 128), ("sw_triple", ctypes.c_int),
         ("ri", ctypes.c_double), ("rf", ctypes.c_double), ("skip", ctypes.c_int),
-        ("gin", ctypes.c_double), ("gout", ctypes.c_double),
+        ("gin", ctypes.c_double), ("gout", ctypes.c_double), ("virial_raw", ctypes.c_int),
     ]
 
 
@@ -129,10 +129,11 @@ def c_spec(name):
         cs.vs2[v] = b
         cs.vk[v] = k
         cs.vd[v] = d0
-    cs.sw_triple = {"pair": 0, "triple": 1, "triple2": 2}[s.switch]
+    cs.sw_triple = {"pair": 0, "triple": 1, "triple2": 2, "cos2": 3}[s.switch]
     cs.ri = s.ri
     cs.rf = s.rf
     cs.skip = {"pair_gt": 0, "two_of_three_gt": 1, "all_three_gt": 2}[s.skip]
+    cs.virial_raw = 1 if s.virial == "raw" else 0
     cs.gin = LP_GAMMA_IN
     cs.gout = LP_GAMMA_OUT
     _spec_cache[name] = cs

@@ -53,6 +53,8 @@
 #include "potential/2b/poly_2b_A1B2Z2_A1B2Z2_deg4_vmbpbe.h"
 #include "potential/3b/poly_3b_A1B2_A1B2_A1B2_deg4_v1.h"
 #include "potential/3b/poly_3b_A1B2_A1B2_A1B2_deg4_vmbpbe.h"
+#include "potential/2b/poly_2b_A1B2C4_D1E2_deg3_v1x.h"
+#include "potential/3b/poly_3b_A1B2C4_D1E2_D1E2_deg3_v1.h"
 
 namespace {
 
@@ -84,6 +86,7 @@ std::vector<std::string> atom_names(const std::string& id) {
     if (id == "co2" || id == "co2_archive") return {"C", "O", "O"};
     if (id == "mbpbe") return {"O", "H", "H"};
     if (id == "he") return {"He"};
+    if (id == "n2o5") return {"O", "N", "N", "O", "O", "O", "O"};
     throw std::runtime_error("harness knows no atom names for monomer id " + id);
 }
 
@@ -217,7 +220,8 @@ double mbxref_get_3b(const char* m1, const char* m2, const char* m3, long nm, co
 // 8 halide - water - water 3b (41), 9 like atoms 2b (1), 10 unlike atoms 2b (1),
 // 11 argon - water 2b (8); 12-19 the template MB-nrg tables h2h22b, h2oh22b,
 // csh22b, nh3nh32b, ch4co22b, mbpbe2b, co23b, mbpbe3b; 20 CO2 - CO2 2b (15),
-// 21 H2O - CO2 2b (21), 22 He - He 2b (1), 23 H2O - He 2b (8).
+// 21 H2O - CO2 2b (21), 22 He - He 2b (1), 23 H2O - He 2b (8), 24 N2O5 - H2O
+// 2b (45), 25 N2O5 - H2O - H2O 3b (78).
 // One configuration per call; g may be NULL for energy only.
 double mbxref_poly(int kind, const double* a, const double* x, double* g) {
     switch (kind) {
@@ -349,6 +353,17 @@ double mbxref_poly(int kind, const double* a, const double* x, double* g) {
                                  : x2b_A1_A1_deg23::poly_2b_A1_A1_deg23_v1x::eval(a, x);
         return g ? x2b_A1B2Z2_C1_deg5::poly_2b_A1B2Z2_C1_deg5_v1x::eval(a, x, g)
                  : x2b_A1B2Z2_C1_deg5::poly_2b_A1B2Z2_C1_deg5_v1x::eval(a, x);
+    }
+    if (kind == 24) {
+        if (!g) return x2b_A1B2C4_D1E2_deg3::poly_2b_A1B2C4_D1E2_deg3_v1x::eval(a, x);
+        for (int j = 0; j < 45; ++j) g[j] = 0.0;
+        return x2b_A1B2C4_D1E2_deg3::poly_2b_A1B2C4_D1E2_deg3_v1x::eval(a, x, g);
+    }
+    if (kind == 25) {
+        mbnrg_A1B2C4_D1E2_D1E2_deg3::poly_A1B2C4_D1E2_D1E2_deg3_v1 p;
+        if (!g) return p.eval(x, a);
+        for (int j = 0; j < 78; ++j) g[j] = 0.0;
+        return p.eval(x, a, g);
     }
     if (kind == 21) {
         if (!g) return x2b_A1B2Z2_C1D2_deg4::poly_2b_A1B2Z2_C1D2_deg4_v1x::eval(a, x);

@@ -35,6 +35,10 @@ reference checkout, default /root/reference) and writes ``tests/golden/*.json``:
 * H2O - CO2 2b: ``unittest-energy2b.cpp`` (h2o-co2 :2000),
   ``unittest-poly-holder-2b.cpp`` (x2b_A1B2Z2_C1D2_v1x h2o-co2 :562),
   ``unittest-poly-2b.cpp`` (poly_2b_A1B2Z2_C1D2_v1x :994-1580);
+* N2O5 - water 2b and 3b: ``unittest-energy2b.cpp`` (n2o5-h2o :1180),
+  ``unittest-poly-holder-2b.cpp`` (x2b_A1B2C4_D1E2_v1x h2o-n2o5 :1407),
+  ``unittest-energy3b.cpp`` (n2o5-h2o-h2o :808), ``unittest-poly-holder-3b.cpp``
+  (mbnrg_A1B2C4_D1E2_D1E2_deg3_v1 :956);
 * water - water - alkali-ion 3b: ``unittest-energy3b.cpp`` (li-h2o-h2o
   :146-357, cs-h2o-h2o :358-471), ``unittest-poly-holder-3b.cpp``
   (x3b_h2o_ion_v1x_deg4_filtered :384-909, one fixture per ion),
@@ -148,6 +152,16 @@ BLOCKS += [
     ("holder2b_h2o_co2", "src/unittests/unittest-poly-holder-2b.cpp", r'TEST_CASE\("x2b_A1B2Z2_C1D2_v1x::struct"\)',
      r'SECTION\("h2o-co2"\)'),
     ("poly_h2oco22b", "src/unittests/unittest-poly-2b.cpp", r'TEST_CASE\(":poly_2b_A1B2Z2_C1D2_v1x:struct"\)', None),
+]
+# N2O5 - H2O 2b and N2O5 - H2O - H2O 3b
+BLOCKS += [
+    ("energy2b_n2o5_h2o", "src/unittests/unittest-energy2b.cpp", r'TEST_CASE\("energy2b::get_2b_energy"\)',
+     r'SECTION\("n2o5-h2o"\)'),
+    ("holder2b_h2o_n2o5", "src/unittests/unittest-poly-holder-2b.cpp", r'TEST_CASE\("x2b_A1B2C4_D1E2_v1x::struct"\)',
+     r'SECTION\("h2o-n2o5"\)'),
+    ("energy3b_n2o5_h2o_h2o", "src/unittests/unittest-energy3b.cpp", r'TEST_CASE', r'SECTION\("n2o5-h2o-h2o"\)'),
+    ("holder3b_n2o5_h2o_h2o", "src/unittests/unittest-poly-holder-3b.cpp", r'TEST_CASE\("::struct"\)',
+     r'SECTION\("n2o5-h2o-h2o"\)'),
 ]
 
 SYSTEMS = [

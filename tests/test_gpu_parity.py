@@ -95,6 +95,10 @@ HOLDERS += [("holder2b_h2_h2", "h2h22b"), ("holder2b_h2_h2o", "h2oh22b"), ("hold
             ("holder2b_ch4_co2", "ch4co22b"), ("holder3b_mbpbe_mbpbe_mbpbe", "mbpbe3b"),
             ("holder3b_co2_co2_co2", "co23b"), ("holder2b_co2a_co2a", "co2a2b"), ("holder2b_co2_co2", "co2co22b"),
             ("holder2b_h2o_co2", "h2oco22b")]
+HOLDERS += [("holder2b_h2o_n2o5", "n2o5h2o2b"), ("holder3b_n2o5_h2o_h2o", "n2o5h2o3b")]
+# fixtures whose test passes the monomers to the holder in another order
+# (holder slot i <- xyz(order[i] + 1))
+HOLDER_ORDER = {"holder2b_h2_h2o": (1, 0), "holder2b_h2o_n2o5": (1, 0)}
 
 
 @pytest.mark.parametrize("fixture,name", HOLDERS)
@@ -102,7 +106,7 @@ def test_evaluator_golden(ctx, fixture, name):
     gd = golden(fixture)
     s = SPECS[name]
     n = gd.get("ndim", gd.get("ntrim"))
-    order = {"holder2b_h2_h2o": (1, 0)}.get(fixture, range(s.nbody))   # holder slot i <- xyz(order[i] + 1)
+    order = HOLDER_ORDER.get(fixture, range(s.nbody))
     blocks = [np.array(gd["xyz%d" % (k + 1)]).reshape(n, -1) for k in order]
     xyz = np.ascontiguousarray(np.concatenate(blocks, axis=1))
     grad = np.zeros_like(xyz)
@@ -133,8 +137,10 @@ def random_nmers(name, n, seed=3):
         centre0 = np.zeros(3)
         for k, m in enumerate(s.monomers):
             # first-atom separations from contact (3.2 A for the 2.3 A long CO2) to beyond the cutoff
-            # He-He from 6 A: its degree-23 polynomial is ill-conditioned closer in
-            rmin = 3.2 if any(m.startswith("co2") for m in s.monomers) else 6.0 if name == "hehe2b" else 2.4
+            # He-He from 6 A: its degree-23 polynomial is ill-conditioned closer in; N2O5 (terminal O
+            # 2.25 A from the bridging O) from 3 A
+            rmin = (3.2 if any(m.startswith("co2") for m in s.monomers) else 6.0 if name == "hehe2b" else
+                    3.0 if "n2o5" in s.monomers else 2.4)
             c = centre0 if k == 0 else workloads._random_directions(rng, 1)[0] * rng.uniform(rmin, s.rf + 0.5)
             parts.append(workloads.place(rng, bodies[m], c[None, :])[0].reshape(-1))
         out.append(np.concatenate(parts))
@@ -288,7 +294,7 @@ def test_solution_box(ions):
                                    (["h2"] * 60 + ["h2o"] * 150 + ["cs+"] * 2, 19.72), (["mbpbe"] * 220, 19.72),
                                    (["ch4"] + ["h2o"] * 180 + ["na+", "cl-"], 19.72), (["co2"] * 200, 26.0),
                                    (["co2_archive"] * 200, 26.0), (["co2"] * 30 + ["h2o"] * 250, 22.0),
-                                   (["he"] + ["h2o"] * 220, 19.72)])
+                                   (["he"] + ["h2o"] * 220, 19.72), (["n2o5"] * 10 + ["h2o"] * 250, 26.0)])
 def test_molecule_box(ids, L):
     """Liquids and mixtures of the MB-nrg types beyond water and ions on the
     GPU against the oracle (the boxes the oracle is checked on against the

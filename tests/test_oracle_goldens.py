@@ -79,6 +79,7 @@ DISPATCH += ["energy2b_%s" % p for p in ("h2_h2", "h2_h2o", "nh3_nh3", "nh3pbe_n
                                          "ch4_co2")]
 DISPATCH += ["energy3b_mbpbe_mbpbe_mbpbe", "energy3b_co2_co2_co2", "energy2b_co2a_co2a", "energy2b_co2_co2",
              "energy2b_h2o_co2"]
+DISPATCH += ["energy2b_n2o5_h2o", "energy3b_n2o5_h2o_h2o"]
 
 
 @pytest.mark.parametrize("fixture", DISPATCH)
@@ -107,11 +108,12 @@ HOLDERS += [("holder2b_h2_h2", "h2h22b"), ("holder2b_h2_h2o", "h2oh22b"), ("hold
             ("holder2b_ch4_co2", "ch4co22b"), ("holder3b_mbpbe_mbpbe_mbpbe", "mbpbe3b"),
             ("holder3b_co2_co2_co2", "co23b"), ("holder2b_co2a_co2a", "co2a2b"), ("holder2b_co2_co2", "co2co22b"),
             ("holder2b_h2o_co2", "h2oco22b")]
+HOLDERS += [("holder2b_h2o_n2o5", "n2o5h2o2b"), ("holder3b_n2o5_h2o_h2o", "n2o5h2o3b")]
 
 
 # fixtures whose test passes the monomers to the holder in another order
 # (unittest-poly-holder-2b.cpp:1098: eval(xyz2, xyz1, ...)): holder slot i <- xyz(order[i] + 1)
-HOLDER_ORDER = {"holder2b_h2_h2o": (1, 0)}
+HOLDER_ORDER = {"holder2b_h2_h2o": (1, 0), "holder2b_h2o_n2o5": (1, 0)}
 
 
 @pytest.mark.parametrize("fixture,name", HOLDERS)
@@ -149,7 +151,7 @@ def test_system_published_energies(fixture):
 REF_PROGRAM = {"mbpol2b": 0, "mbpol3b": 1, "ch4h2o2b": 2, "ch4ch42b": 3, "ch4h2o3b": 4, "h2oli2b": 5, "h2oli3b": 6,
                "fh2o2b": 7, "fh2o3b": 8, "nana2b": 9, "nacl2b": 10, "arh2o2b": 11, "h2h22b": 12, "h2oh22b": 13,
                "csh22b": 14, "nh3nh32b": 15, "ch4co22b": 16, "mbpbe2b": 17, "co23b": 18, "mbpbe3b": 19,
-               "co2co22b": 20, "h2oco22b": 21, "hehe2b": 22, "h2ohe2b": 23}
+               "co2co22b": 20, "h2oco22b": 21, "hehe2b": 22, "h2ohe2b": 23, "n2o5h2o2b": 24, "n2o5h2o3b": 25}
 
 
 @pytest.mark.parametrize("name", list(REF_PROGRAM))
@@ -228,6 +230,8 @@ MOLECULE_BOXES = [
     (["co2"] * 30 + ["h2o"] * 250, (2, 3), 22.0),
     # helium: water with a single He (He-He pairs in test_helium_dilute_vs_reference)
     (["he"] + ["h2o"] * 220, (2, 3)),
+    # N2O5 in water (a 26 A box: the molecule spans 4.5 A)
+    (["n2o5"] * 10 + ["h2o"] * 250, (2, 3), 26.0),
 ]
 
 
