@@ -54,8 +54,8 @@ const char* mbx_version(void);
 /* Monomers in internal order (System::AddMonomerInfo, system.cpp:1794-1969):
  * ids[m] (the reference's monomer ids of this path: "h2o", "ch4", "li+",
  * "na+", "k+", "rb+", "cs+", "f-", "cl-", "br-", "i-", "ar", "h2", "nh3",
- * "nh3pbe0d3bj", "co2", "co2_archive", "mbpbe", "he", "n2o5"; the co2cm*
- * models are known monomers whose n-mers have no evaluator here),
+ * "nh3pbe0d3bj", "co2", "co2_archive", "co2cm5100", "co2cm595", "co2cm590",
+ * "co2cm585", "co2cm5875", "co2cm580", "mbpbe", "he", "n2o5"),
  * first_index[m] (first site), tag[m] (tag of the
  * monomer's first atom; n-mers are owned by the lowest tag,
  * sys_tools.cpp:562,585), is_local[m] (NULL = all local), numsites. */

@@ -22,7 +22,10 @@ EVALUATORS = ("mbpol2b", "mbpol3b", "ch4h2o2b", "ch4ch42b", "ch4h2o3b",
               "fh2o2b", "clh2o2b", "brh2o2b", "ih2o2b", "fh2o3b", "clh2o3b", "brh2o3b", "ih2o3b",
               "nana2b", "clcl2b", "arar2b", "nacl2b", "csar2b", "arh2o2b",
               "h2h22b", "h2oh22b", "csh22b", "nh3nh32b", "nh3pbe2b", "ch4co22b", "mbpbe2b", "co23b", "mbpbe3b",
-              "co2co22b", "co2a2b", "h2oco22b", "hehe2b", "h2ohe2b", "n2o5h2o2b", "n2o5h2o3b")
+              "co2co22b", "co2a2b", "h2oco22b", "hehe2b", "h2ohe2b", "n2o5h2o2b", "n2o5h2o3b",
+              "cm5100co22b", "cm595co22b", "cm590co22b", "cm585co22b", "cm5875co22b", "cm580co22b",
+              "h2ocm5100co22b", "h2ocm595co22b", "h2ocm590co22b", "h2ocm585co22b", "h2ocm5875co22b",
+              "h2ocm580co22b")
 
 
 class MBXError(RuntimeError):

@@ -785,10 +785,12 @@ int mbx_launch_%(name)s_w(const HolderArgs& A, int grads, int grid, cudaStream_t
 # so their raw-polynomial (mbx_poly) and coefficient-adjoint
 # (mbx_evaluate_dcoef) entries answer MBX_ENOTSUP.
 LEAN_TYPES = {"nh3nh32b", "nh3pbe2b", "ch4co22b", "mbpbe2b", "co23b", "mbpbe3b", "co2co22b", "co2a2b",
-              "n2o5h2o3b"}
+              "n2o5h2o3b", "cm595co22b", "cm590co22b", "cm585co22b", "cm5875co22b", "cm580co22b"}
 
 
 def variants_of(name):
+    from mbx_b200.specs import KERNEL_ALIASES
+    name = KERNEL_ALIASES.get(name, name)
     if load_pip(name).nterms > STRAIGHT_LINE_MAX_TERMS:
         return "w"
     if name in LEAN_TYPES:
@@ -944,10 +946,13 @@ def write_kernels_cu(name):
 def write_registry():
     """Host tables: evaluator descriptions, default coefficients, term tables."""
     from mbx_b200.tables import load_fit
+    from mbx_b200.specs import KERNEL_ALIASES
     lines = ["// Generated by mbx_b200/codegen/gen_kernels.py -- do not edit.", "#pragma once",
              '#include "../holder_kernel.cuh"', ""]
     for name in SPECS:
         vs = variants_of(name)
+        if name in KERNEL_ALIASES:
+            vs = ""   # runs the kernels of KERNEL_ALIASES[name], declared there
         for v in "gecpws":
             if v not in vs:
                 continue
@@ -973,11 +978,12 @@ def write_registry():
     lines.append("static const EvaluatorInfo mbx_evaluators[] = {")
     for name, spec in SPECS.items():
         vs = variants_of(name)
+        kern = KERNEL_ALIASES.get(name, name)
         ids = list(spec.monomers) + ["", ""][:3 - len(spec.monomers)]
         skip = {"pair_gt": 0, "two_of_three_gt": 1, "all_three_gt": 2}[spec.skip]
 
         def fn(v, kind):
-            return ("mbx_%s_%s_%s" % (kind, name, v)) if v in vs else "nullptr"
+            return ("mbx_%s_%s_%s" % (kind, kern, v)) if v in vs else "nullptr"
         lines.append('    {"%s", %d, {"%s", "%s", "%s"}, %s, %d, %d, %d, %d, mbx_fit_%s, %s, %s, %s, %s, %s, %s, %s,' %
                      (name, spec.nbody, ids[0], ids[1], ids[2], lit(spec.rf), skip, spec.ncoef, spec.nreal,
                       spec.nvars, name, fn("g", "launch"), fn("e", "launch"), fn("c", "launch"),
@@ -1025,7 +1031,10 @@ def main(argv=None):
     os.makedirs(OUT, exist_ok=True)
     write_registry()
     write_term_tables()
+    from mbx_b200.specs import KERNEL_ALIASES
     for n in args.names:
+        if n in KERNEL_ALIASES:
+            continue
         path, leaves, inner = generate(n)
         write_kernels_cu(n)
         print("%s: %d leaves, %d inner -> %s" % (n, leaves, inner, path))

@@ -168,7 +168,9 @@ for _m1, _m2, _name, _table, _file in (
     FITS[_name] = ("potential/2b/" + _file, r'if \(mon1 == "%s" and mon2 == "%s"\) \{\s*coefficients\s*=\s*'
                    r'std::vector<double>\s*\{' % (_m1, _m2))
     TABLE_OF[_name] = _table
-for _m, _name in (("co2_archive", "co2a2b"), ("co2", "co2co22b")):
+for _m, _name in (("co2_archive", "co2a2b"), ("co2", "co2co22b"), ("co2cm5100", "cm5100co22b"),
+                  ("co2cm595", "cm595co22b"), ("co2cm590", "cm590co22b"), ("co2cm585", "cm585co22b"),
+                  ("co2cm5875", "cm5875co22b"), ("co2cm580", "cm580co22b")):
     FITS[_name] = ("potential/2b/x2b_A1B2_A1B2_v1x.cpp", r'if \(mon1 == "%s" && mon2 == "%s"\) \{\s*coefficients\s*=\s*'
                    r'std::vector<double>\s*\{' % (_m, _m))
     TABLE_OF[_name] = "co2co22btab"

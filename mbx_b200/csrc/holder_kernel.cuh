@@ -65,6 +65,12 @@ __device__ __forceinline__ double ld_volatile(const double* p) {
     return v;
 }
 
+// Real atoms of the evaluator's largest monomer (loop bound over one monomer's atoms).
+template <class T>
+__host__ __device__ constexpr int max_nat() {
+    return T::NAT0 > T::NAT1 ? (T::NAT0 > T::NAT2 ? T::NAT0 : T::NAT2) : (T::NAT1 > T::NAT2 ? T::NAT1 : T::NAT2);
+}
+
 // GetCloseDimerImage / GetCloseTrimerImage: every monomer but the anchor slot
 // moved to the image next to the anchor's first atom.
 template <class T>
@@ -83,7 +89,7 @@ __device__ __forceinline__ void image_nmer(const BoxParams& bp, int anchor, doub
             double d[3];
             image_shift(bp, p0, q0, d);
 #pragma unroll
-            for (int a = 0; a < 5; ++a) {
+            for (int a = 0; a < max_nat<T>(); ++a) {
                 if (a < nat[s]) {
                     double q[3] = {r[first[s] + a][0], r[first[s] + a][1], r[first[s] + a][2]};
                     apply_shift(bp, d, q);
@@ -98,6 +104,7 @@ __device__ __forceinline__ void image_nmer(const BoxParams& bp, int anchor, doub
 
 template <class T, bool VOL>
 __device__ __forceinline__ void load_nmer(const HolderArgs& A, long t, double (&r)[T::NREAL][3]) {
+    constexpr int MAXNAT = max_nat<T>();
     if (A.aos) {
         const double* p = A.xyz + (size_t)t * (T::NREAL * 3);
 #pragma unroll
@@ -114,7 +121,7 @@ __device__ __forceinline__ void load_nmer(const HolderArgs& A, long t, double (&
     for (int s = 0; s < T::NBODY; ++s) {
         const double* p = A.xyz + 3 * (size_t)__ldg(A.first_index + mon[s]);
 #pragma unroll
-        for (int a = 0; a < 3 * 5; ++a) {
+        for (int a = 0; a < 3 * MAXNAT; ++a) {
             if (a < 3 * nat[s]) r[first[s] + a / 3][a % 3] = VOL ? ld_volatile(p + a) : __ldg(p + a);
         }
     }
@@ -289,7 +296,7 @@ __device__ __forceinline__ void finish_nmer(const HolderArgs& A, long t, double 
     for (int s = 0; s < T::NBODY; ++s) {
         double* p = A.grad + 3 * (size_t)__ldg(A.first_index + mon[s]);
 #pragma unroll
-        for (int a = 0; a < 5; ++a)
+        for (int a = 0; a < max_nat<T>(); ++a)
             if (a < nat[s])
 #pragma unroll
                 for (int c = 0; c < 3; ++c) atomicAdd(p + 3 * a + c, tg[first[s] + a][c]);

@@ -43,7 +43,7 @@ Skip rules (n-mers not evaluated; their energy and gradient are exactly 0):
 * ``all_three_gt``: all of r12, r13, r23 > rf
   (mbnrg_3b_A1B4_C1D2_C1D2_deg3_v1.cpp:1561)
 """
-from dataclasses import dataclass, field
+from dataclasses import dataclass, field, replace
 from typing import List, Tuple
 
 LP_GAMMA_IN = -9.721486914088159e-02
@@ -561,7 +561,15 @@ _CO22B = {
 # On this path: co2 and co2_archive.  The six co2cm* models share the
 # polynomial with their own constants; each would be another ~10 MB of
 # kernel code, and they are left out (their dimers evaluate to 0 here).
-CO2_MODELS = ("co2", "co2_archive")
+CO2_MODELS = ("co2", "co2_archive", "co2cm5100", "co2cm595", "co2cm590", "co2cm585", "co2cm5875", "co2cm580")
+# evaluators that run another evaluator's kernels (and coefficients): the
+# reference's co2cm5100 block (x2b_A1B2_A1B2_v1x.cpp:4657) repeats the co2
+# block's constants and coefficients exactly (:2373), so its dimers run the
+# co2 kernels; water with any CO2 model but co2_archive runs the H2O - CO2
+# evaluator with the co2 constants (energy2b.cpp:140-145, :318-321), one
+# alias per model so that each carries its monomer ids
+KERNEL_ALIASES = {"cm5100co22b": "co2co22b"}
+KERNEL_ALIASES.update({"h2o%sco22b" % m[3:]: "h2oco22b" for m in CO2_MODELS if m.startswith("co2cm")})
 
 
 def _co22b(model):
@@ -604,6 +612,8 @@ H2OCO22B = Spec(
     variables=_vars(_S_H2OCO2, [("exp", a, b) + _hc[key] for a, b, key in _tab]), switch="pair", ri=8.0, rf=9.0,
     skip="pair_gt", nvars=21, ncoef=1653, degree=4, ref="potential/2b/x2b_A1B2Z2_C1D2_v1x.cpp:3635",
 )
+H2OCO2CM2B = tuple(replace(H2OCO22B, name="h2o%sco22b" % m[3:], monomers=("h2o", m), table="h2oco22b")
+                   for m in CO2_MODELS if m.startswith("co2cm"))
 
 # ---------------------------------------------------------------------------
 # Helium: He - He 2b x2b_A1_A1_v1x (potential/2b/x2b_A1_A1_deg23_v1x.cpp:398,
@@ -673,7 +683,7 @@ SPECS = {s.name: s for s in (MBPOL2B, MBPOL3B, CH4H2O2B, CH4CH42B, CH4H2O3B,
                              H2OLI2B, H2ONA2B, H2OK2B, H2ORB2B, H2OCS2B,
                              H2OLI3B, H2ONA3B, H2OK3B, H2ORB3B, H2OCS3B,
                              FH2O2B, CLH2O2B, BRH2O2B, IH2O2B, FH2O3B, CLH2O3B, BRH2O3B, IH2O3B,
-                             ARH2O2B, H2OCO22B, HEHE2B, H2OHE2B, N2O5H2O2B) + ATOM2B + TEMPLATE_SPECS + CO22B}
+                             ARH2O2B, H2OCO22B, HEHE2B, H2OHE2B, N2O5H2O2B) + H2OCO2CM2B + ATOM2B + TEMPLATE_SPECS + CO22B}
 
 # Dispatch by sorted monomer ids (e2b::get_2b_energy, potential/2b/energy2b.cpp:
 # 240-254,258-281,282,323; e3b::get_3b_energy, potential/3b/energy3b.cpp:185-216,
@@ -687,7 +697,10 @@ DISPATCH_2B = {("h2o", "h2o"): "mbpol2b", ("ch4", "h2o"): "ch4h2o2b", ("ch4", "c
                ("h2", "h2"): "h2h22b", ("h2", "h2o"): "h2oh22b", ("cs+", "h2"): "csh22b", ("nh3", "nh3"): "nh3nh32b",
                ("nh3pbe0d3bj", "nh3pbe0d3bj"): "nh3pbe2b", ("ch4", "co2"): "ch4co22b", ("mbpbe", "mbpbe"): "mbpbe2b"}
 DISPATCH_2B.update({(m, m): _CO22B[m][0] for m in CO2_MODELS})
+# water with any CO2 model but co2_archive: the co2 constants
+# (energy2b.cpp:140-145 and :318-321)
 DISPATCH_2B[("co2", "h2o")] = "h2oco22b"
+DISPATCH_2B.update({(m, "h2o"): "h2o%sco22b" % m[3:] for m in CO2_MODELS if m.startswith("co2cm")})
 DISPATCH_2B[("he", "he")] = "hehe2b"
 DISPATCH_2B[("h2o", "he")] = "h2ohe2b"
 DISPATCH_2B[("h2o", "n2o5")] = "n2o5h2o2b"

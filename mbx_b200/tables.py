@@ -61,5 +61,10 @@ def load_pip(name):
 
 @functools.lru_cache(maxsize=None)
 def load_fit(name):
+    """Fitted linear coefficients of an evaluator (an alias evaluator of
+    specs.KERNEL_ALIASES without a fit of its own has its target's)."""
+    from mbx_b200.specs import KERNEL_ALIASES
+    if name in KERNEL_ALIASES and not os.path.exists(os.path.join(DATA, name + ".fit")):
+        name = KERNEL_ALIASES[name]
     with open(os.path.join(DATA, name + ".fit")) as f:
         return np.array([float(v) for v in f.read().split()], np.float64)

@@ -89,6 +89,7 @@ def n2o5_body(r_on=1.50, r_no=1.19, a_non=112.0, a_ono=134.0):
 
 BODIES = {"h2o": water_body, "mbpbe": water_body, "ch4": methane_body, "nh3": ammonia_body,
           "nh3pbe0d3bj": ammonia_body, "co2": co2_body, "co2_archive": co2_body, "h2": h2_body, "n2o5": n2o5_body}
+BODIES.update({m: co2_body for m in ("co2cm5100", "co2cm595", "co2cm590", "co2cm585", "co2cm5875", "co2cm580")})
 
 
 def molecule_box(ids, n_side=7, L=19.72, seed=0, jitter=0.3):

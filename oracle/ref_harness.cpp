@@ -83,7 +83,7 @@ std::vector<std::string> atom_names(const std::string& id) {
     if (id == "ar") return {"Ar"};
     if (id == "h2") return {"H", "H"};
     if (id == "nh3" || id == "nh3pbe0d3bj") return {"N", "H", "H", "H"};
-    if (id == "co2" || id == "co2_archive") return {"C", "O", "O"};
+    if (id == "co2" || id == "co2_archive" || id.rfind("co2cm", 0) == 0) return {"C", "O", "O"};
     if (id == "mbpbe") return {"O", "H", "H"};
     if (id == "he") return {"He"};
     if (id == "n2o5") return {"O", "N", "N", "O", "O", "O", "O"};

@@ -29,8 +29,9 @@ reference checkout, default /root/reference) and writes ``tests/golden/*.json``:
   :1943), ``unittest-energy3b.cpp`` (mbpbe x3 :911, co2 x3 :1386),
   ``unittest-poly-holder-2b.cpp`` (:1019-1546), ``unittest-poly-holder-3b.cpp``
   (:84-173);
-* CO2 - CO2 2b: ``unittest-energy2b.cpp`` (co2_archive :99, co2 :1558),
-  ``unittest-poly-holder-2b.cpp`` (x2b_A1B2_A1B2_v1x :263-560),
+* CO2 - CO2 2b: ``unittest-energy2b.cpp`` (co2_archive :99, co2 :1558, the
+  co2cm* models :1613-1942), ``unittest-poly-holder-2b.cpp``
+  (x2b_A1B2_A1B2_v1x :263-560),
   ``unittest-poly-2b.cpp`` (poly_2b_A1B2_A1B2_v1x :205-993);
 * H2O - CO2 2b: ``unittest-energy2b.cpp`` (h2o-co2 :2000),
   ``unittest-poly-holder-2b.cpp`` (x2b_A1B2Z2_C1D2_v1x h2o-co2 :562),
@@ -153,6 +154,12 @@ BLOCKS += [
      r'SECTION\("h2o-co2"\)'),
     ("poly_h2oco22b", "src/unittests/unittest-poly-2b.cpp", r'TEST_CASE\(":poly_2b_A1B2Z2_C1D2_v1x:struct"\)', None),
 ]
+# CO2 - CO2 2b of the co2cm* models
+CO2CM = ("co2cm5100", "co2cm595", "co2cm590", "co2cm5875", "co2cm585", "co2cm580")
+BLOCKS += [("energy2b_%s" % m, "src/unittests/unittest-energy2b.cpp", r'TEST_CASE\("energy2b::get_2b_energy"\)',
+            r'SECTION\("%s-%s"\)' % (m, m)) for m in CO2CM]
+BLOCKS += [("holder2b_%s" % m, "src/unittests/unittest-poly-holder-2b.cpp", r'TEST_CASE\("x2b_A1B2_A1B2_v1x::struct"\)',
+            r'SECTION\("%s-%s"\)' % (m, m)) for m in CO2CM]
 # N2O5 - H2O 2b and N2O5 - H2O - H2O 3b
 BLOCKS += [
     ("energy2b_n2o5_h2o", "src/unittests/unittest-energy2b.cpp", r'TEST_CASE\("energy2b::get_2b_energy"\)',

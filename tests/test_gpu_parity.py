@@ -25,6 +25,27 @@ G_ABS = 1e-8
 # FP64 evaluations in different orders agree to ~1e-9 kcal/mol per n-mer,
 # not to 1e-10 relative; per-n-mer energies are compared absolutely.
 E_ABS_NMER = 1e-8
+# CO2 models whose intramolecular variables exp(k (d0 - r)) are far above 1
+# (up to 32): their degree-5 polynomials sum terms up to ~1e8 times a
+# dimer's energy, so FP64 evaluation orders differ by ~1e-16 of that sum:
+# up to ~4e-8 kcal/mol per dimer between the oracle's term sums and the
+# reference's Horner program (the trie here lands within 2e-9 of the
+# reference on its co2cm580 golden, the oracle 4e-8 off).  These compare
+# within 1e-6 kcal/mol per dimer (or 1e-8 relative) and 1e-6 kcal/mol/A, or
+# 1e-8 of the largest force.
+ILL_CONDITIONED = {"cm595co22b", "cm590co22b", "cm585co22b", "cm5875co22b", "cm580co22b"}
+ILL_E_REL = 1e-8
+ILL_E_ABS = 1e-6
+
+
+def g_tol(name, go):
+    return max(1e-6, 1e-8 * np.abs(go).max()) if name in ILL_CONDITIONED else G_ABS
+
+
+def e_close(name, e, eo, n=1):
+    if name in ILL_CONDITIONED:
+        return rel(e, eo) < ILL_E_REL or abs(e - eo) < ILL_E_ABS * n
+    return rel(e, eo) < E_REL or abs(e - eo) < E_ABS_NMER
 MIXED_REL = 1e-6          # total 2b+3b energy of a liquid box; also each term's error against |E2B| + |E3B|
 MIXED_REL_TERM = 2e-6     # one term (2b or 3b) of the 2048-water box, relative to itself
 MIXED_REL_GAS = 1e-5      # sums over random gas-phase n-mers
@@ -96,6 +117,8 @@ HOLDERS += [("holder2b_h2_h2", "h2h22b"), ("holder2b_h2_h2o", "h2oh22b"), ("hold
             ("holder3b_co2_co2_co2", "co23b"), ("holder2b_co2a_co2a", "co2a2b"), ("holder2b_co2_co2", "co2co22b"),
             ("holder2b_h2o_co2", "h2oco22b")]
 HOLDERS += [("holder2b_h2o_n2o5", "n2o5h2o2b"), ("holder3b_n2o5_h2o_h2o", "n2o5h2o3b")]
+HOLDERS += [("holder2b_%s" % m, m[3:] + "co22b")
+            for m in ("co2cm5100", "co2cm595", "co2cm590", "co2cm5875", "co2cm585", "co2cm580")]
 # fixtures whose test passes the monomers to the holder in another order
 # (holder slot i <- xyz(order[i] + 1))
 HOLDER_ORDER = {"holder2b_h2_h2o": (1, 0), "holder2b_h2o_n2o5": (1, 0)}
@@ -114,9 +137,9 @@ def test_evaluator_golden(ctx, fixture, name):
     e = ctx.evaluate(name, xyz, grad, vir)
     eo, go, vo, _ = mo.holder_eval(name, xyz)
     assert abs(e - gd["energy_expected"]) < 1e-6
-    assert rel(e, eo) < E_REL or abs(e - eo) < E_ABS_NMER
-    np.testing.assert_allclose(grad, go, rtol=0, atol=G_ABS)
-    np.testing.assert_allclose(vir, vo, rtol=1e-10, atol=G_ABS)
+    assert e_close(name, e, eo)
+    np.testing.assert_allclose(grad, go, rtol=0, atol=g_tol(name, go))
+    np.testing.assert_allclose(vir, vo, rtol=1e-10 if name not in ILL_CONDITIONED else 1e-7, atol=g_tol(name, go))
     off = 0
     for i, k in enumerate(order):
         w = blocks[i].shape[1]
@@ -139,8 +162,9 @@ def random_nmers(name, n, seed=3):
             # first-atom separations from contact (3.2 A for the 2.3 A long CO2) to beyond the cutoff
             # He-He from 6 A: its degree-23 polynomial is ill-conditioned closer in; N2O5 (terminal O
             # 2.25 A from the bridging O) from 3 A
-            rmin = (3.2 if any(m.startswith("co2") for m in s.monomers) else 6.0 if name == "hehe2b" else
-                    3.0 if "n2o5" in s.monomers else 2.4)
+            # the ill-conditioned CO2 models from 4.5 A (ILL_CONDITIONED)
+            rmin = (4.5 if name in ILL_CONDITIONED else 3.2 if any(m.startswith("co2") for m in s.monomers) else
+                    6.0 if name == "hehe2b" else 3.0 if "n2o5" in s.monomers else 2.4)
             c = centre0 if k == 0 else workloads._random_directions(rng, 1)[0] * rng.uniform(rmin, s.rf + 0.5)
             parts.append(workloads.place(rng, bodies[m], c[None, :])[0].reshape(-1))
         out.append(np.concatenate(parts))
@@ -156,10 +180,11 @@ def test_evaluator_random_vs_oracle(ctx, name):
     eper = np.zeros(n)
     e = ctx.evaluate(name, xyz, grad, vir, eper)
     eo, go, vo, epo = mo.holder_eval(name, xyz, per_nmer=True)
-    assert rel(e, eo) < E_REL or abs(e - eo) < E_ABS_NMER
-    np.testing.assert_allclose(eper, epo, rtol=0, atol=E_ABS_NMER)
-    np.testing.assert_allclose(grad, go, rtol=0, atol=G_ABS)
-    np.testing.assert_allclose(vir, vo, rtol=1e-9, atol=1e-8)
+    ill = name in ILL_CONDITIONED
+    assert e_close(name, e, eo, n)
+    np.testing.assert_allclose(eper, epo, rtol=ILL_E_REL if ill else 0, atol=ILL_E_ABS if ill else E_ABS_NMER)
+    np.testing.assert_allclose(grad, go, rtol=0, atol=g_tol(name, go))
+    np.testing.assert_allclose(vir, vo, rtol=1e-7 if ill else 1e-9, atol=1e-6 if ill else 1e-8)
 
 
 @pytest.mark.parametrize("name", ["mbpol2b", "mbpol3b", "ch4h2o2b", "ch4h2o3b"])
@@ -201,7 +226,8 @@ def test_dcoef_vs_oracle(ctx, name):
 
 
 # ------------------------------------------------------------------ systems
-def compare_system(ids, xyz, box, c2, c3, ig2=(), ig3=(), mixed=False, lists=True, g_rtol=0.0):
+def compare_system(ids, xyz, box, c2, c3, ig2=(), ig3=(), mixed=False, lists=True, g_rtol=0.0, e_rtol=E_REL,
+                   g_atol=G_ABS):
     o = mo.OracleSystem(ids, xyz, box, c2, c3, ig2, ig3)
     g = msys.from_arrays(ids, xyz, box, c2, c3, ig2, ig3, precision="mixed" if mixed else "fp64")
     etot, etot_o = 0.0, 0.0
@@ -219,9 +245,9 @@ def compare_system(ids, xyz, box, c2, c3, ig2=(), ig3=(), mixed=False, lists=Tru
         if mixed:
             assert np.abs(np.asarray(gr) - go).max() < MIXED_FORCE, nb
         else:
-            assert rel(e, eo) < E_REL, (nb, e, eo)
-            np.testing.assert_allclose(gr, go, rtol=g_rtol, atol=G_ABS)
-            np.testing.assert_allclose(vr, vo, rtol=1e-9, atol=1e-7)
+            assert rel(e, eo) < e_rtol, (nb, e, eo)
+            np.testing.assert_allclose(gr, go, rtol=g_rtol, atol=g_atol)
+            np.testing.assert_allclose(vr, vo, rtol=1e-9 if e_rtol < 1e-9 else 1e-7, atol=1e-7)
         if lists:
             cut = c2 if nb == 2 else c3
             assert np.array_equal(canon(g.GetPairList(nb, cut)), o.top.nmers_to_input(o.nmers(nb))), nb
@@ -294,7 +320,10 @@ def test_solution_box(ions):
                                    (["h2"] * 60 + ["h2o"] * 150 + ["cs+"] * 2, 19.72), (["mbpbe"] * 220, 19.72),
                                    (["ch4"] + ["h2o"] * 180 + ["na+", "cl-"], 19.72), (["co2"] * 200, 26.0),
                                    (["co2_archive"] * 200, 26.0), (["co2"] * 30 + ["h2o"] * 250, 22.0),
-                                   (["he"] + ["h2o"] * 220, 19.72), (["n2o5"] * 10 + ["h2o"] * 250, 26.0)])
+                                   (["he"] + ["h2o"] * 220, 19.72), (["n2o5"] * 10 + ["h2o"] * 250, 26.0),
+                                   (["co2cm590"] * 100 + ["co2cm585"] * 100, 30.0),
+                                   (["co2cm5875"] * 100 + ["co2cm580"] * 100, 30.0),
+                                   (["co2cm5100"] * 30 + ["co2cm595"] * 30 + ["h2o"] * 220, 22.0)])
 def test_molecule_box(ids, L):
     """Liquids and mixtures of the MB-nrg types beyond water and ions on the
     GPU against the oracle (the boxes the oracle is checked on against the
@@ -303,7 +332,11 @@ def test_molecule_box(ids, L):
     orders differ by ~1e-11 of the force: gradients within 1e-8 absolute
     plus 1e-10 relative."""
     ids, xyz, box = workloads.molecule_box(ids, L=L, seed=3)
-    compare_system(ids, xyz, box, 9.0, 7.0, g_rtol=1e-10)
+    if any(m in ("co2cm595", "co2cm590", "co2cm585", "co2cm5875", "co2cm580") for m in ids):
+        # ill-conditioned CO2 models (ILL_CONDITIONED)
+        compare_system(ids, xyz, box, 9.0, 7.0, e_rtol=ILL_E_REL, g_atol=1e-6)
+    else:
+        compare_system(ids, xyz, box, 9.0, 7.0, g_rtol=1e-10)
 
 
 def test_helium_dilute():
