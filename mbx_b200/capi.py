@@ -25,7 +25,7 @@ EVALUATORS = ("mbpol2b", "mbpol3b", "ch4h2o2b", "ch4ch42b", "ch4h2o3b",
               "co2co22b", "co2a2b", "h2oco22b", "hehe2b", "h2ohe2b", "n2o5h2o2b", "n2o5h2o3b",
               "cm5100co22b", "cm595co22b", "cm590co22b", "cm585co22b", "cm5875co22b", "cm580co22b",
               "h2ocm5100co22b", "h2ocm595co22b", "h2ocm590co22b", "h2ocm585co22b", "h2ocm5875co22b",
-              "h2ocm580co22b")
+              "h2ocm580co22b", "h2oco2a2b")
 
 
 class MBXError(RuntimeError):

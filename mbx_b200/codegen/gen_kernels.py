@@ -785,7 +785,7 @@ int mbx_launch_%(name)s_w(const HolderArgs& A, int grads, int grid, cudaStream_t
 # so their raw-polynomial (mbx_poly) and coefficient-adjoint
 # (mbx_evaluate_dcoef) entries answer MBX_ENOTSUP.
 LEAN_TYPES = {"nh3nh32b", "nh3pbe2b", "ch4co22b", "mbpbe2b", "co23b", "mbpbe3b", "co2co22b", "co2a2b",
-              "n2o5h2o3b", "cm595co22b", "cm590co22b", "cm585co22b", "cm5875co22b", "cm580co22b"}
+              "n2o5h2o3b", "h2oco2a2b", "cm595co22b", "cm590co22b", "cm585co22b", "cm5875co22b", "cm580co22b"}
 
 
 def variants_of(name):

@@ -177,6 +177,9 @@ for _m, _name in (("co2_archive", "co2a2b"), ("co2", "co2co22b"), ("co2cm5100", 
 FITS["h2oco22b"] = ("potential/2b/x2b_A1B2Z2_C1D2_v1x.cpp",
                     r'if \(mon1 == "h2o" && mon2 == "co2"\) \{\s*coefficients\s*=\s*std::vector<double>\s*\{')
 TABLE_OF["h2oco22b"] = "h2oco22b"
+FITS["h2oco2a2b"] = ("potential/2b/x2b_A1B2Z2_C1D2_v1x.cpp",
+                     r'if \(mon1 == "h2o" && mon2 == "co2_archive"\) \{\s*coefficients\s*=\s*std::vector<double>\s*\{')
+TABLE_OF["h2oco2a2b"] = "h2oco22b"
 FITS["n2o5h2o2b"] = ("potential/2b/x2b_A1B2C4_D1E2_deg3_v1x.cpp",
                      r'if \(mon1 == "h2o" && mon2 == "n2o5"\) \{\s*coefficients\s*=\s*std::vector<double>\s*\{')
 TABLE_OF["n2o5h2o2b"] = "n2o5h2o2b"

@@ -593,8 +593,8 @@ CO22B = tuple(_co22b(m) for m in CO2_MODELS)
 # local variable::v_exp(r0, k) = exp(k (r0 - r)) :63-77; MB-pol lone pairs
 # :3683; f_switch :3503-3516 on the O-C distance, dimers beyond r2f skipped
 # :3690; constructor block :1821-3498).  The reference evaluates every CO2
-# model against water with these constants (energy2b.cpp:318-321); its
-# co2_archive block sets no switch radii and is not on this path.
+# model but co2_archive against water with these constants
+# (energy2b.cpp:318-321); co2_archive has a block of its own (H2OCO2A2B).
 # ---------------------------------------------------------------------------
 _S_H2OCO2 = ("A", "B1", "B2", "C", "D1", "D2", "Z1", "Z2")
 _hc = dict(iAB=(4.592278064081765e-01, 4.092695741312179e-01), iBB=(1.797813612275968e+00, 2.515176186264408e+00),
@@ -612,6 +612,16 @@ H2OCO22B = Spec(
     variables=_vars(_S_H2OCO2, [("exp", a, b) + _hc[key] for a, b, key in _tab]), switch="pair", ri=8.0, rf=9.0,
     skip="pair_gt", nvars=21, ncoef=1653, degree=4, ref="potential/2b/x2b_A1B2Z2_C1D2_v1x.cpp:3635",
 )
+# water - co2_archive: the same evaluator with the constants of its own block
+# (x2b_A1B2Z2_C1D2_v1x.cpp:144-1802; the switch radii are the header's
+# defaults 8 and 9 A, x2b_A1B2Z2_C1D2_v1x.h:129-132)
+_hca = dict(iAB=(2.991129377354730e+00, 9.711475336203186e-01), iBB=(1.776076592672980e+00, 2.247507043695376e+00),
+            iCD=(8.784095840943548e-01, 2.930193028642861e+00), iDD=(2.220694581661451e+00, 2.481043684198385e+00),
+            AC=(9.760814515633827e-01, 2.730468459200360e+00), AD=(2.671217176193513e+00, 2.711874357778875e+00),
+            BC=(1.206205856757539e+00, 4.665335309987695e+00), BD=(2.879622692196830e-01, 6.043660542816871e+00),
+            CZ=(1.382134149600439e+00, 4.584956529773560e+00), DZ=(3.624833784927413e+00, 4.021523821428722e+00))
+H2OCO2A2B = replace(H2OCO22B, name="h2oco2a2b", monomers=("h2o", "co2_archive"), table="h2oco22b",
+                    variables=_vars(_S_H2OCO2, [("exp", a, b) + _hca[key] for a, b, key in _tab]))
 H2OCO2CM2B = tuple(replace(H2OCO22B, name="h2o%sco22b" % m[3:], monomers=("h2o", m), table="h2oco22b")
                    for m in CO2_MODELS if m.startswith("co2cm"))
 
@@ -683,7 +693,7 @@ SPECS = {s.name: s for s in (MBPOL2B, MBPOL3B, CH4H2O2B, CH4CH42B, CH4H2O3B,
                              H2OLI2B, H2ONA2B, H2OK2B, H2ORB2B, H2OCS2B,
                              H2OLI3B, H2ONA3B, H2OK3B, H2ORB3B, H2OCS3B,
                              FH2O2B, CLH2O2B, BRH2O2B, IH2O2B, FH2O3B, CLH2O3B, BRH2O3B, IH2O3B,
-                             ARH2O2B, H2OCO22B, HEHE2B, H2OHE2B, N2O5H2O2B) + H2OCO2CM2B + ATOM2B + TEMPLATE_SPECS + CO22B}
+                             ARH2O2B, H2OCO22B, H2OCO2A2B, HEHE2B, H2OHE2B, N2O5H2O2B) + H2OCO2CM2B + ATOM2B + TEMPLATE_SPECS + CO22B}
 
 # Dispatch by sorted monomer ids (e2b::get_2b_energy, potential/2b/energy2b.cpp:
 # 240-254,258-281,282,323; e3b::get_3b_energy, potential/3b/energy3b.cpp:185-216,
@@ -700,6 +710,7 @@ DISPATCH_2B.update({(m, m): _CO22B[m][0] for m in CO2_MODELS})
 # water with any CO2 model but co2_archive: the co2 constants
 # (energy2b.cpp:140-145 and :318-321)
 DISPATCH_2B[("co2", "h2o")] = "h2oco22b"
+DISPATCH_2B[("co2_archive", "h2o")] = "h2oco2a2b"
 DISPATCH_2B.update({(m, "h2o"): "h2o%sco22b" % m[3:] for m in CO2_MODELS if m.startswith("co2cm")})
 DISPATCH_2B[("he", "he")] = "hehe2b"
 DISPATCH_2B[("h2o", "he")] = "h2ohe2b"

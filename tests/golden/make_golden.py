@@ -33,8 +33,9 @@ reference checkout, default /root/reference) and writes ``tests/golden/*.json``:
   co2cm* models :1613-1942), ``unittest-poly-holder-2b.cpp``
   (x2b_A1B2_A1B2_v1x :263-560),
   ``unittest-poly-2b.cpp`` (poly_2b_A1B2_A1B2_v1x :205-993);
-* H2O - CO2 2b: ``unittest-energy2b.cpp`` (h2o-co2 :2000),
-  ``unittest-poly-holder-2b.cpp`` (x2b_A1B2Z2_C1D2_v1x h2o-co2 :562),
+* H2O - CO2 2b: ``unittest-energy2b.cpp`` (h2o-co2 :2000, co2_archive-h2o
+  :428), ``unittest-poly-holder-2b.cpp`` (x2b_A1B2Z2_C1D2_v1x h2o-co2 :562,
+  h2o-co2_archive :596),
   ``unittest-poly-2b.cpp`` (poly_2b_A1B2Z2_C1D2_v1x :994-1580);
 * N2O5 - water 2b and 3b: ``unittest-energy2b.cpp`` (n2o5-h2o :1180),
   ``unittest-poly-holder-2b.cpp`` (x2b_A1B2C4_D1E2_v1x h2o-n2o5 :1407),
@@ -160,6 +161,13 @@ BLOCKS += [("energy2b_%s" % m, "src/unittests/unittest-energy2b.cpp", r'TEST_CAS
             r'SECTION\("%s-%s"\)' % (m, m)) for m in CO2CM]
 BLOCKS += [("holder2b_%s" % m, "src/unittests/unittest-poly-holder-2b.cpp", r'TEST_CASE\("x2b_A1B2_A1B2_v1x::struct"\)',
             r'SECTION\("%s-%s"\)' % (m, m)) for m in CO2CM]
+# H2O - CO2 2b, co2_archive model
+BLOCKS += [
+    ("energy2b_co2a_h2o", "src/unittests/unittest-energy2b.cpp", r'TEST_CASE\("energy2b::get_2b_energy"\)',
+     r'SECTION\("co2-h2o"\)'),
+    ("holder2b_h2o_co2a", "src/unittests/unittest-poly-holder-2b.cpp", r'TEST_CASE\("x2b_A1B2Z2_C1D2_v1x::struct"\)',
+     r'SECTION\("h2o-co2_archive"\)'),
+]
 # N2O5 - H2O 2b and N2O5 - H2O - H2O 3b
 BLOCKS += [
     ("energy2b_n2o5_h2o", "src/unittests/unittest-energy2b.cpp", r'TEST_CASE\("energy2b::get_2b_energy"\)',

@@ -119,6 +119,7 @@ HOLDERS += [("holder2b_h2_h2", "h2h22b"), ("holder2b_h2_h2o", "h2oh22b"), ("hold
 HOLDERS += [("holder2b_h2o_n2o5", "n2o5h2o2b"), ("holder3b_n2o5_h2o_h2o", "n2o5h2o3b")]
 HOLDERS += [("holder2b_%s" % m, m[3:] + "co22b")
             for m in ("co2cm5100", "co2cm595", "co2cm590", "co2cm5875", "co2cm585", "co2cm580")]
+HOLDERS += [("holder2b_h2o_co2a", "h2oco2a2b")]
 # fixtures whose test passes the monomers to the holder in another order
 # (holder slot i <- xyz(order[i] + 1))
 HOLDER_ORDER = {"holder2b_h2_h2o": (1, 0), "holder2b_h2o_n2o5": (1, 0)}
@@ -323,7 +324,8 @@ def test_solution_box(ions):
                                    (["he"] + ["h2o"] * 220, 19.72), (["n2o5"] * 10 + ["h2o"] * 250, 26.0),
                                    (["co2cm590"] * 100 + ["co2cm585"] * 100, 30.0),
                                    (["co2cm5875"] * 100 + ["co2cm580"] * 100, 30.0),
-                                   (["co2cm5100"] * 30 + ["co2cm595"] * 30 + ["h2o"] * 220, 22.0)])
+                                   (["co2cm5100"] * 30 + ["co2cm595"] * 30 + ["h2o"] * 220, 22.0),
+                                   (["co2_archive"] * 30 + ["h2o"] * 250, 22.0)])
 def test_molecule_box(ids, L):
     """Liquids and mixtures of the MB-nrg types beyond water and ions on the
     GPU against the oracle (the boxes the oracle is checked on against the

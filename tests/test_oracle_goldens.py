@@ -81,7 +81,7 @@ DISPATCH += ["energy3b_mbpbe_mbpbe_mbpbe", "energy3b_co2_co2_co2", "energy2b_co2
              "energy2b_h2o_co2"]
 DISPATCH += ["energy2b_n2o5_h2o", "energy3b_n2o5_h2o_h2o"]
 CO2CM = ("co2cm5100", "co2cm595", "co2cm590", "co2cm5875", "co2cm585", "co2cm580")
-DISPATCH += ["energy2b_%s" % m for m in CO2CM]
+DISPATCH += ["energy2b_%s" % m for m in CO2CM] + ["energy2b_co2a_h2o"]
 
 
 @pytest.mark.parametrize("fixture", DISPATCH)
@@ -111,7 +111,7 @@ HOLDERS += [("holder2b_h2_h2", "h2h22b"), ("holder2b_h2_h2o", "h2oh22b"), ("hold
             ("holder3b_co2_co2_co2", "co23b"), ("holder2b_co2a_co2a", "co2a2b"), ("holder2b_co2_co2", "co2co22b"),
             ("holder2b_h2o_co2", "h2oco22b")]
 HOLDERS += [("holder2b_h2o_n2o5", "n2o5h2o2b"), ("holder3b_n2o5_h2o_h2o", "n2o5h2o3b")]
-HOLDERS += [("holder2b_%s" % m, m[3:] + "co22b") for m in CO2CM]
+HOLDERS += [("holder2b_%s" % m, m[3:] + "co22b") for m in CO2CM] + [("holder2b_h2o_co2a", "h2oco2a2b")]
 
 
 # fixtures whose test passes the monomers to the holder in another order
@@ -244,6 +244,8 @@ MOLECULE_BOXES = [
     (["co2cm590"] * 100 + ["co2cm585"] * 100, (2,), 30.0, (1e-8, 1e-6)),
     (["co2cm5875"] * 100 + ["co2cm580"] * 100, (2,), 30.0, (1e-8, 1e-6)),
     (["co2cm5100"] * 30 + ["co2cm580"] * 30 + ["h2o"] * 220, (2,), 22.0, (1e-8, 1e-6)),
+    # co2_archive in water
+    (["co2_archive"] * 30 + ["h2o"] * 250, (2,), 22.0),
     # N2O5 in water (a 26 A box: the molecule spans 4.5 A)
     (["n2o5"] * 10 + ["h2o"] * 250, (2, 3), 26.0),
 ]
@@ -265,7 +267,9 @@ def test_molecule_box_vs_reference(case):
     for nb in nbs:
         e_o, e_r = o.energy(nb), r.energy(nb)
         assert abs(e_o - e_r) < e_rtol * max(1.0, abs(e_r)), (nb, e_o, e_r)
-        np.testing.assert_allclose(o.real_grads(), r.real_grads(), rtol=0, atol=g_atol)
+        # close contacts of randomly oriented molecules carry forces up to
+        # ~1e4 kcal/mol/A: 1e-10 of the force on top of the absolute bound
+        np.testing.assert_allclose(o.real_grads(), r.real_grads(), rtol=1e-10, atol=g_atol)
         np.testing.assert_allclose(o.virial, r.virial(), rtol=1e-9 if e_rtol < 1e-9 else 1e-7, atol=1e-7)
 
 
