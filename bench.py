@@ -43,9 +43,6 @@ sys.path.insert(0, ROOT)
 
 METRIC = "dimers+trimers/s with forces, 2048 H2O; FP32-mixed vs FP64 GPU at <=1e-6 rel E"
 CUT2, CUT3 = 9.0, 7.0
-# DRAM bytes per launch of the mbpol3b gradient kernel on this workload, from one
-# ncu capture of the same command (read + write); the kernel is compute-bound
-TRAFFIC_3B = 5.75e6
 
 
 def workload():
@@ -74,8 +71,9 @@ class Clocks:
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
              "clocks_event_reasons.sw_power_cap")
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+            # line-buffered (stdbuf), so that a sample's arrival time is its time
+            self.proc = subprocess.Popen(["stdbuf", "-oL", "nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -194,8 +192,11 @@ def batched_leg(args, local, flush, fp64_value, dist=None, world=1):
     import torch
     from mbx_b200 import workloads
     from mbx_b200.batch import Batch
+    from mbx_b200 import capi
     cfgs = workloads.batch_beads_clusters(32, 64, seed=0)
-    b = Batch(cfgs, CUT2, CUT3, device=local)
+    stream = torch.cuda.current_stream()
+    bctx = capi.Context(local, stream.cuda_stream)
+    b = Batch(cfgs, CUT2, CUT3, device=local, context=bctx)
     tuned = {}
     for nb in (2, 3):
         knobs, ms = b.tune(nb, mixed=True)
@@ -206,23 +207,24 @@ def batched_leg(args, local, flush, fp64_value, dist=None, world=1):
         b.energy_2b3b(mixed=True)
     listed2, eval2 = b.ctx.counts(2)
     listed3, eval3 = b.ctx.counts(3)
-    stream = torch.cuda.current_stream()
     times = []
     emx = None
     steps = max(3, min(args.steps, 20))
     for _ in range(steps):
         flush.zero_()
+        if dist:
+            dist.barrier()
         torch.cuda.synchronize()
         a = torch.cuda.Event(enable_timing=True)
         z = torch.cuda.Event(enable_timing=True)
         a.record(stream)
         b.grad.zero_()
-        torch.cuda.synchronize()
-        t0, t1 = b.energy_2b3b(mixed=True)
+        t0, t1 = b.energy_2b3b(mixed=True)   # replays the graph on the same stream
         z.record(stream)
         torch.cuda.synchronize()
-        times.append(b.ctx.timing()[1])
+        times.append(a.elapsed_time(z))
         emx = t0 + t1
+    bctx.close()
     from mbx_b200 import replicas
     ms, = replicas.max_over_ranks([sum(times) / len(times)], dist, "cuda")
     units = listed2 + listed3
@@ -234,8 +236,8 @@ def batched_leg(args, local, flush, fp64_value, dist=None, world=1):
             "units_per_step": {"dimers": listed2, "trimers": listed3, "evaluated_dimers": eval2,
                                "evaluated_trimers": eval3},
             "dtype": "mixed (3b paired f32 over a shifted basis; 2b f64)", "cuda_graph": True,
-            "timing": "device time of the replayed graph of both terms (CUDA events around the replay), "
-                      "L2 flushed before each step",
+            "timing": "CUDA events on the bench's stream around the gradient reset and the graph replay of "
+                      "both terms (the library runs on that stream), L2 flushed before each step",
             "autotuned": tuned,
             "max_rel_err_E_per_configuration": float(rel.max()),
             "speedup_vs_fp64_plain": replicas.throughput(units, ms, world) / fp64_value}
@@ -294,7 +296,7 @@ def salt_leg(args, local, flush, cpu=True):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=400)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -374,12 +376,10 @@ def main():
             evs.append(ctx.timing()[1])
         return evs
 
-    with Clocks(local) as clk:
-        clk.wait_first(step)
-        t_begin = time.monotonic()
-        t64, launches, (e2_64, e3_64) = timed(False)
-        clk.window = (t_begin, time.monotonic())
-    clocks = clk.summary()
+    clk = Clocks(local).__enter__()
+    clk.wait_first(step)
+    t_begin = time.monotonic()
+    t64, launches, (e2_64, e3_64) = timed(False)
     g64 = grad.cpu().numpy()
     ev64 = kernel_3b(False, max(3, min(args.steps, 20)))
     if not args.no_mixed:
@@ -433,8 +433,9 @@ def main():
     roofline = {"bound": "fp64-fma", "kernel": "holder_lock_kernel<mbpol3b_T, mbpol3b_CC, HM_GRAD_FP64>",
                 "achieved": achieved,
                 "peak": peaks["fp64_tflops"], "unit": "TFLOP/s", "frac": achieved / peaks["fp64_tflops"],
-                "traffic": TRAFFIC_3B, "traffic_unit": "bytes per launch (ncu dram__bytes, one capture)",
-                "traffic_source": "profiles/holder_kernel_mbpol3b_grad_2048h2o.md",
+                "traffic": None,
+                "traffic_note": "DRAM bytes are not measured inside this run (no profiler here); the kernel's "
+                                "inputs (0.2 MB of coordinates, 0.2 MB of n-mer records) are L2-resident",
                 "note": "algorithmic flops = evaluated trimers x %d (reference gradient program, "
                         "mbx_b200/data/flops.json); peak = FP64 FMA pipe measured on this GPU by "
                         "mbx_fma_peaks (MEASURED_PEAKS.json has no FP64 figure)" % flops["mbpol3b"]["flops"],
@@ -449,7 +450,7 @@ def main():
            "e2e": {"value": world * units / (e2e_ms * 1e-3), "unit": "n-mers/s", "h2d_bytes_per_step": h2d,
                    "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
                    "api": "mbx_b200.system.System.TwoAndThreeBodyEnergy (mbx_energy_2b3b, host arrays)"},
-           "gpu_launches": launches, "roofline": roofline, "clocks": clocks,
+           "gpu_launches": launches, "roofline": roofline,
            "fma_peaks_tflops": peaks}
     if not args.no_mixed:
         g3_64, g3_mx = g64 - g2_64, gmx - g2_mx
@@ -472,6 +473,11 @@ def main():
                                        "bound": "fp32-fma"}
     if not args.no_batch:
         out["batched"] = batched_leg(args, local, flush, value, dist, world)
+    # clocks sampled over the timed legs (FP64, mixed, batched)
+    clk.window = (t_begin, time.monotonic())
+    clk.__exit__()
+    out["clocks"] = clk.summary()
+    out["clocks"]["window"] = "FP64, mixed and batched timed legs"
     if not args.no_salt and rank == 0 and world == 1:
         out["salt"] = salt_leg(args, local, flush, cpu=not args.no_cpu_baseline)
     if rank == 0 and not args.no_cpu_baseline:

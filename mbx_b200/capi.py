@@ -1,8 +1,10 @@
 """ctypes binding of the C ABI in ``include/mbx_b200.h`` (``libmbx_b200.so``).
 
 This is the Python side of the drop-in boundary: every compute call goes to
-the CUDA library.  There is no CPU fallback; loading fails loudly if the
-library has not been built or no CUDA device is present.
+the CUDA library.  There is no CPU fallback: when the library is missing it
+is built on first use (``mbx_b200/build.py``, nvcc for sm_100a, a few
+minutes), and loading fails loudly if that build fails or no CUDA device is
+present.
 """
 import ctypes
 import os
@@ -42,7 +44,11 @@ def lib():
     if _lib is not None:
         return _lib
     if not os.path.exists(LIB_PATH):
-        raise RuntimeError("mbx_b200 CUDA library not built (%s); run python -m mbx_b200.build" % LIB_PATH)
+        from mbx_b200 import build
+        try:
+            build.build(quiet=True)
+        except Exception as e:  # noqa: BLE001 -- re-raised with the library path
+            raise RuntimeError("mbx_b200 CUDA library %s is missing and could not be built: %s" % (LIB_PATH, e))
     L = ctypes.CDLL(LIB_PATH)
     vp, dp, lp, ip = ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_long), ctypes.POINTER(ctypes.c_int)
     cpp = ctypes.POINTER(ctypes.c_char_p)
@@ -61,6 +67,7 @@ def lib():
     L.mbx_nmers.argtypes = [vp, ctypes.c_int, ctypes.c_double, dp, ctypes.c_int, lp, ctypes.c_long, lp]
     L.mbx_evaluate.argtypes = [vp, ctypes.c_char_p, ctypes.c_long, dp, dp, dp, dp, ctypes.POINTER(ctypes.c_double),
                                ctypes.c_int]
+    L.mbx_evaluate_noalloc.argtypes = [ctypes.c_char_p, ctypes.c_long, dp, dp, dp, dp, vp]
     L.mbx_evaluate_dcoef.argtypes = [vp, ctypes.c_char_p, ctypes.c_long, dp, dp, dp, ctypes.c_int]
     L.mbx_poly.argtypes = [vp, ctypes.c_char_p, ctypes.c_long, dp, dp, dp, ctypes.c_int]
     L.mbx_set_coefficients.argtypes = [vp, ctypes.c_char_p, dp, ctypes.c_int]

@@ -87,7 +87,7 @@ def count_program(ref, rel, mode):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("MBX_REFERENCE"), required=not os.environ.get("MBX_REFERENCE"))
     a = ap.parse_args(argv)
     out = {}
     for name, (rel, mode) in PROGRAMS.items():

@@ -10,9 +10,12 @@ For each evaluator in ``mbx_b200.specs.SPECS`` this writes
   multivariate Horner trie over the expanded term table;
 * ``<name>_pip_e``: the energy-only Horner evaluation;
 * ``<name>_pip_s32`` (types in SHIFT_TYPES): the FP32 trie of the type's FP32
-  basis (codegen/shift.py), the mixed-precision polynomial;
-* ``<name>_dcoef``: per-coefficient monomial sums dP/da_k (for the adjoint with
-  respect to the linear coefficients), recomputed from x.
+  basis (codegen/shift.py), the mixed-precision polynomial.
+
+The tries are generated for STRAIGHT_TYPES only; every evaluator also gets a
+table unit ``<name>_t.cu`` (coefficient adjoint and, without a trie, the
+evaluation itself) over the term tables that ``write_term_tables`` packs into
+one binary embedded in the library.
 
 The trie.  Every term is a monomial x_v1 x_v2 ... (variables sorted in a fixed
 order); the monomials form a prefix tree.  With P(n) the product along the path
@@ -43,8 +46,6 @@ from mbx_b200.tables import load_pip  # noqa: E402
 
 OUT = os.path.join(PKG, "csrc", "gen")
 
-# Larger polynomials (CH4-CH4: 201k terms) use the table-driven warp kernel.
-STRAIGHT_LINE_MAX_TERMS = 60000
 
 
 def lit(v):
@@ -438,23 +439,6 @@ def emit_pip_energy(trie, nvars, name, out, nparts=1):
     emit_split(trie, nvars, name, out, nparts, [("x", "double", "in")], body)
 
 
-def emit_dcoef(table, nvars, name, out):
-    """dP/da_k = sum of the monomials of coefficient k; calls SINK(k, value)."""
-    w = out.append
-    w("template <class Sink>")
-    w("__device__ __forceinline__ void %s(const double (&x)[%d], Sink&& SINK) {" % (name, nvars))
-    by_k = collections.defaultdict(list)
-    for t in range(table.nterms):
-        by_k[int(table.k[t])].append((float(table.coef[t]), table.var[t, :table.deg[t]].tolist()))
-    for k in sorted(by_k):
-        terms = []
-        for c, mono in by_k[k]:
-            prod = " * ".join("x[%d]" % v for v in mono) if mono else "1.0"
-            terms.append(prod if c == 1.0 else "%s * %s" % (lit(c), prod))
-        w("    SINK(%d, %s);" % (k, " + ".join(terms)))
-    w("}")
-
-
 def emit_vars(spec, out):
     """Sites (incl. lone pairs), variables and their Cartesian derivative factors."""
     w = out.append
@@ -502,6 +486,8 @@ def emit_traits(spec, table, straight, out):
     w("    static constexpr int SWITCH_TRIPLE = %d, SKIP = %d, STRAIGHT = %d, DEGREE = %d;" %
       ({"pair": 0, "triple": 1, "triple2": 2, "cos2": 3}[spec.switch], {"pair_gt": 0, "two_of_three_gt": 1, "all_three_gt": 2}[spec.skip],
        1 if straight else 0, spec.degree))
+    w("    static constexpr int TPAIRS = %d;  // (variable, exponent) pairs of a term, at most" %
+      term_pairs_max(table))
     w("    static constexpr double RI = %s, RF = %s;" % (lit(spec.ri), lit(spec.rf)))
     w("    static constexpr int VIRIAL_RAW = %d;  // virial of the unswitched polynomial gradient" %
       (1 if spec.virial == "raw" else 0))
@@ -542,8 +528,6 @@ def emit_traits(spec, table, straight, out):
         w("    template <int S, class C> __device__ __forceinline__ static double pip_e_piece(int k, const C& c, "
           "const double* __restrict__ x) { return %s_pip_e_piece<S>(k, c, x); }" % n)
 
-        w("    template <class S> __device__ __forceinline__ static void dcoef(const double (&x)[%d], S&& sink) "
-          "{ %s_dcoef(x, sink); }" % (spec.nvars, n))
     w("};")
 
 
@@ -560,9 +544,9 @@ def generate(name):
     only the units that include it."""
     spec = SPECS[name]
     table = load_pip(name)
-    trie = Trie(table)
-    leaves, inner = trie.counts()
-    straight = table.nterms <= STRAIGHT_LINE_MAX_TERMS
+    straight = name in STRAIGHT_TYPES
+    trie = Trie(table) if straight else None
+    leaves, inner = trie.counts() if straight else (table.nterms, 0)
     head = ["// Generated by mbx_b200/codegen/gen_kernels.py from mbx_b200/specs.py and",
             "// mbx_b200/data/%s.pip.gz -- do not edit." % name]
     out = head + ["// %d terms: %d leaves, %d inner nodes" % (table.nterms, leaves, inner),
@@ -583,8 +567,6 @@ def generate(name):
                 "const double* __restrict__, double* __restrict__);" % name,
                 "template <int S, class Coef> __device__ __forceinline__ double %s_pip_e_piece(int, const Coef&, "
                 "const double* __restrict__);" % name]
-        out += ["template <class Sink> __device__ __forceinline__ void %s_dcoef(const double (&)[%d], Sink&&);" %
-                (name, nv)]
         if name in SHIFT_TYPES:
             sp = shifted_pip(name)
             out.append("template <int S, class Coef> __device__ __forceinline__ double2 %s_pip_s32_lock(const Coef&, "
@@ -605,13 +587,9 @@ def generate(name):
     write_if_changed(os.path.join(OUT, name + ".cuh"), "\n".join(out) + "\n")
     if straight:
         nparts = parts_for(table.nterms, spec.nvars)
-        for suffix, emitter, arg in (("pip", emit_pip, trie), ("pip_e", emit_pip_energy, trie),
-                                     ("dcoef", emit_dcoef, table)):
+        for suffix, emitter, arg in (("pip", emit_pip, trie), ("pip_e", emit_pip_energy, trie)):
             body = head + ["#pragma once", '#include "%s.cuh"' % name]
-            if emitter is emit_dcoef:
-                emitter(arg, nv, "%s_%s" % (name, suffix), body)
-            else:
-                emitter(arg, nv, "%s_%s" % (name, suffix), body, nparts)
+            emitter(arg, nv, "%s_%s" % (name, suffix), body, nparts)
             write_if_changed(os.path.join(OUT, "%s_%s.cuh" % (name, suffix)), "\n".join(body) + "\n")
         if name in SHIFT_TYPES:
             from mbx_b200.codegen.shift import ShiftedTable
@@ -633,6 +611,7 @@ TU_HEAD = """// Generated by mbx_b200/codegen/gen_kernels.py -- do not edit.
 #include <cstring>
 #include <vector>
 #include "../holder_kernel.cuh"
+#include "../launch_cache.cuh"
 #include "%(name)s.cuh"
 %(include)s
 static __constant__ double c_%(name)s[%(ncoef)d];
@@ -655,8 +634,7 @@ int mbx_set_coef_%(name)s_%(v)s(const double* a, int from_device, cudaStream_t s
     } else {
         for (int k = 0; k < %(ncoef)d; ++k) h[k] = a[k];
     }
-    static thread_local std::vector<float> f;
-    f.resize(%(ncoef)d);
+    std::vector<float> f(%(ncoef)d);
     for (int k = 0; k < %(ncoef)d; ++k) f[k] = (float)h[k];
     e = cudaMemcpyToSymbolAsync(cf_%(name)s, f.data(), sizeof(float) * %(ncoef)d, 0, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
@@ -664,138 +642,115 @@ int mbx_set_coef_%(name)s_%(v)s(const double* a, int from_device, cudaStream_t s
 }
 """
 
+LOCK_LAUNCH = """
+int mbx_launch_%(name)s_%(v)s(const HolderArgs& A, int grid, int block, cudaStream_t s) {
+    // persistent grid of lockstep blocks: every resident block slot once
+    // (blocks claim chunks of LOCK_THREADS n-mers dynamically); the
+    // variables%(gtext)s of the block's n-mers in dynamic shared memory
+    auto kern = holder_lock_kernel<%(name)s_T, %(name)s_CC, %(mode)s, false>;
+    block = %(name)s_T::LOCK_THREADS;
+    const int smem = %(ncol)d * %(name)s_T::NVARS * %(name)s_T::LOCK_THREADS * (int)sizeof(double);
+    static LaunchCache lc;
+    int sms = 0, bps = 0;
+    const int r = launch_facts(lc, kern, block, smem, smem, &sms, &bps);
+    if (r) return r;
+    const long need = (A.n + block - 1) / block;
+    grid = (int)(need < (long)sms * bps ? need : (long)sms * bps);
+    if (grid < 1) grid = 1;
+    kern<<<grid, block, smem, s>>>(A);
+    return (int)cudaGetLastError();
+}
+
+int mbx_prime_%(name)s_%(v)s(cudaStream_t s) {
+    // code prefetch of the %(what2)s: a launch of the evaluation kernel itself in its
+    // prefetch mode (prime_pieces), one warp per SM, every piece run by at
+    // least four of them
+    auto kern = holder_lock_kernel<%(name)s_T, %(name)s_CC, %(mode)s, false>;
+    const int smem_full = %(ncol)d * %(name)s_T::NVARS * %(name)s_T::LOCK_THREADS * (int)sizeof(double);
+    const int smem = %(name)s_T::NVARS * %(name)s_T::LOCK_THREADS * (int)sizeof(double);
+    static LaunchCache lc;
+    int sms = 0, bps = 0;
+    const int r = launch_facts(lc, kern, 0, smem_full, 0, &sms, &bps);
+    if (r) return r;
+    HolderArgs A;
+    memset(&A, 0, sizeof(A));
+    A.prime_npieces = %(name)s_%(pipname)s_NPIECES;
+    A.prime_passes = (4 * A.prime_npieces + sms - 1) / sms;
+    kern<<<sms, 32, smem, s>>>(A);
+    return (int)cudaGetLastError();
+}
+"""
+
 VARIANTS = {
     # variant: (description, body)
-    "g": ("FP64 energy + gradient kernel", """
-int mbx_launch_%(name)s_g(const HolderArgs& A, int grid, int block, cudaStream_t s) {
-    // persistent grid of lockstep blocks: every resident block slot once
-    // (blocks claim chunks of LOCK_THREADS n-mers dynamically); the
-    // variables and their gradient accumulators of the block's n-mers in dynamic shared memory
-    auto kern = holder_lock_kernel<%(name)s_T, %(name)s_CC, HM_GRAD_FP64, false>;
-    block = %(name)s_T::LOCK_THREADS;
-    const int smem = 2 * %(name)s_T::NVARS * %(name)s_T::LOCK_THREADS * (int)sizeof(double);
-    static int bps = 0, sms = 0;
-    if (!bps) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, block, smem);
-        if (bps < 1) bps = 1;
-    }
-    const long need = (A.n + block - 1) / block;
-    grid = (int)(need < (long)sms * bps ? need : (long)sms * bps);
-    if (grid < 1) grid = 1;
-    kern<<<grid, block, smem, s>>>(A);
-    return (int)cudaGetLastError();
+    "g": ("FP64 energy + gradient kernel", LOCK_LAUNCH % {
+        "name": "%(name)s", "v": "g", "gtext": " and their gradient accumulators", "mode": "HM_GRAD_FP64",
+        "ncol": 2, "what2": "FP64 gradient trie", "pipname": "pip"}),
+    "e": ("FP64 energy-only kernel", LOCK_LAUNCH % {
+        "name": "%(name)s", "v": "e", "gtext": "", "mode": "HM_ENERGY",
+        "ncol": 1, "what2": "FP64 energy trie", "pipname": "pip_e"}),
 }
 
-int mbx_prime_%(name)s_g(cudaStream_t s) {
-    // code prefetch of the FP64 gradient trie: a launch of the evaluation kernel itself in its
-    // prefetch mode (prime_pieces), one warp per SM, every piece run by at
-    // least four of them
-    auto kern = holder_lock_kernel<%(name)s_T, %(name)s_CC, HM_GRAD_FP64, false>;
-    const int smem_full = 2 * %(name)s_T::NVARS * %(name)s_T::LOCK_THREADS * (int)sizeof(double);
-    const int smem = %(name)s_T::NVARS * %(name)s_T::LOCK_THREADS * (int)sizeof(double);
-    static int sms = 0;
-    if (!sms) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_full);
-    }
-    HolderArgs A;
-    memset(&A, 0, sizeof(A));
-    A.prime_npieces = %(name)s_pip_NPIECES;
-    A.prime_passes = (4 * A.prime_npieces + sms - 1) / sms;
-    kern<<<sms, 32, smem, s>>>(A);
-    return (int)cudaGetLastError();
-}
-"""),
-    "e": ("FP64 energy-only kernel", """
-int mbx_launch_%(name)s_e(const HolderArgs& A, int grid, int block, cudaStream_t s) {
-    // persistent grid of lockstep blocks: every resident block slot once
-    // (blocks claim chunks of LOCK_THREADS n-mers dynamically); the
-    // variables of the block's n-mers in dynamic shared memory
-    auto kern = holder_lock_kernel<%(name)s_T, %(name)s_CC, HM_ENERGY, false>;
-    block = %(name)s_T::LOCK_THREADS;
-    const int smem = 1 * %(name)s_T::NVARS * %(name)s_T::LOCK_THREADS * (int)sizeof(double);
-    static int bps = 0, sms = 0;
-    if (!bps) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, block, smem);
-        if (bps < 1) bps = 1;
-    }
-    const long need = (A.n + block - 1) / block;
-    grid = (int)(need < (long)sms * bps ? need : (long)sms * bps);
-    if (grid < 1) grid = 1;
-    kern<<<grid, block, smem, s>>>(A);
-    return (int)cudaGetLastError();
-}
+# The table unit of every evaluator: the coefficient adjoint and, for the
+# evaluators without straight-line code, the table-driven evaluation, both
+# reading the polynomial's term table (csrc/term_table.cuh) and its
+# coefficients from global memory.
+TABLE_TU = """// Generated by mbx_b200/codegen/gen_kernels.py -- do not edit.
+// Table-driven kernels (term table in global memory) of the %(name)s evaluator.
+#include <cstring>
+#include "../holder_kernel.cuh"
+#include "../launch_cache.cuh"
+#include "%(name)s.cuh"
 
-int mbx_prime_%(name)s_e(cudaStream_t s) {
-    // code prefetch of the FP64 energy trie: a launch of the evaluation kernel itself in its
-    // prefetch mode (prime_pieces), one warp per SM, every piece run by at
-    // least four of them
-    auto kern = holder_lock_kernel<%(name)s_T, %(name)s_CC, HM_ENERGY, false>;
-    const int smem_full = 1 * %(name)s_T::NVARS * %(name)s_T::LOCK_THREADS * (int)sizeof(double);
-    const int smem = %(name)s_T::NVARS * %(name)s_T::LOCK_THREADS * (int)sizeof(double);
-    static int sms = 0;
-    if (!sms) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_full);
-    }
-    HolderArgs A;
-    memset(&A, 0, sizeof(A));
-    A.prime_npieces = %(name)s_pip_e_NPIECES;
-    A.prime_passes = (4 * A.prime_npieces + sms - 1) / sms;
-    kern<<<sms, 32, smem, s>>>(A);
-    return (int)cudaGetLastError();
-}
-"""),
-    "c": ("coefficient-gradient (adjoint) kernel", """
 int mbx_launch_%(name)s_c(const HolderArgs& A, const double* w, double* out, int grid, int block, cudaStream_t s) {
-    holder_dcoef_kernel<%(name)s_T><<<grid, block, 0, s>>>(A, w, out);
+    // coefficient adjoint: dynamic shared memory = per-coefficient sums +
+    // the variable columns of the block's four warps
+    auto kern = holder_dcoef_table_kernel<%(name)s_T>;
+    const int smem = (%(name)s_T::NCOEF + 4 * 32 * %(name)s_T::NVARS) * (int)sizeof(double);
+    static LaunchCache lc;
+    int sms = 0, bps = 0;
+    const int r = launch_facts(lc, kern, 0, smem, 0, &sms, &bps);
+    if (r) return r;
+    kern<<<grid, 128, smem, s>>>(A, w, out);
     return (int)cudaGetLastError();
 }
-"""),
-    "p": ("generated-polynomial (SoA) kernel", """
-int mbx_launch_%(name)s_p(long nd, const double* x, double* g, double* e, int grid, int block, cudaStream_t s) {
-    poly_soa_kernel<%(name)s_T, %(name)s_CC><<<grid, block, 0, s>>>(nd, x, g, e);
-    return (int)cudaGetLastError();
-}
-"""),
-    "w": ("table-driven warp kernel (energy, gradient)", """
+%(warp)s"""
+
+TABLE_WARP = """
 int mbx_launch_%(name)s_w(const HolderArgs& A, int grads, int grid, cudaStream_t s) {
-    holder_warp_kernel<%(name)s_T, 4><<<grid, 128, 0, s>>>(A, grads);
+    if (%(name)s_T::NTERMS > 100000) {
+        // very large table, few n-mers: a warp per n-mer
+        holder_table_kernel<%(name)s_T, 4><<<grid, 128, 0, s>>>(A, grads);
+        return (int)cudaGetLastError();
+    }
+    // a lane per n-mer; x and gradient columns of four warps in dynamic shared memory
+    auto kern = holder_table_lane_kernel<%(name)s_T>;
+    const int smem = 4 * 2 * %(name)s_T::NVARS * 32 * (int)sizeof(double);
+    static LaunchCache lc;
+    int sms = 0, bps = 0;
+    const int r = launch_facts(lc, kern, 128, smem, smem, &sms, &bps);
+    if (r) return r;
+    const long need = (A.n + 127) / 128;
+    const int g = (int)(need < (long)sms * bps ? (need > 0 ? need : 1) : (long)sms * bps);
+    kern<<<g, 128, smem, s>>>(A, grads);
     return (int)cudaGetLastError();
 }
-"""),
-}
+"""
 
 
-# Large template MB-nrg types built with the energy + gradient and the
-# energy-only kernels only: every further kernel of a ~3e4-term trie adds
-# ~10 MB of code (ptxas compiles the trie's pieces once per calling kernel),
-# so their raw-polynomial (mbx_poly) and coefficient-adjoint
-# (mbx_evaluate_dcoef) entries answer MBX_ENOTSUP.
-LEAN_TYPES = {"nh3nh32b", "nh3pbe2b", "ch4co22b", "mbpbe2b", "co23b", "mbpbe3b", "co2co22b", "co2a2b",
-              "n2o5h2o3b", "h2oco2a2b", "cm595co22b", "cm590co22b", "cm585co22b", "cm5875co22b", "cm580co22b"}
+# Evaluators with straight-line (generated Horner trie) kernels: the water
+# and methane-water polynomials of MB-pol / MB-nrg the timed path runs.  All
+# others run the table-driven kernels: their tries would add minutes of
+# compile time each for types no timed workload uses.
+STRAIGHT_TYPES = ("mbpol2b", "mbpol3b", "ch4h2o2b", "ch4h2o3b")
 
 
 def variants_of(name):
     from mbx_b200.specs import KERNEL_ALIASES
     name = KERNEL_ALIASES.get(name, name)
-    if load_pip(name).nterms > STRAIGHT_LINE_MAX_TERMS:
-        return "w"
-    if name in LEAN_TYPES:
-        return "ge"
-    return "gecp" + ("s" if name in SHIFT_TYPES else "")
+    if name in STRAIGHT_TYPES:
+        return "ge" + ("s" if name in SHIFT_TYPES else "") + "t"
+    return "wt"
 
 
 SHIFT_TU = """// Generated by mbx_b200/codegen/gen_kernels.py -- do not edit.
@@ -803,6 +758,7 @@ SHIFT_TU = """// Generated by mbx_b200/codegen/gen_kernels.py -- do not edit.
 #include <cstring>
 #include <vector>
 #include "../holder_kernel.cuh"
+#include "../launch_cache.cuh"
 #include "%(name)s.cuh"
 #include "%(name)s_pip_s32.cuh"
 
@@ -859,15 +815,10 @@ int mbx_launch_%(name)s_s(const HolderArgs& A, int grid, int block, cudaStream_t
     auto kern = holder_pair_kernel<%(name)s_T, %(name)s_CS>;
     block = %(name)s_T::LOCK_THREADS_S;
     const int smem = 2 * %(name)s_T::NVARS * %(name)s_T::LOCK_THREADS_S * (int)sizeof(f2_t);
-    static int bps = 0, sms = 0;
-    if (!bps) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, block, smem);
-        if (bps < 1) bps = 1;
-    }
+    static LaunchCache lc;
+    int sms = 0, bps = 0;
+    const int r = launch_facts(lc, kern, block, smem, smem, &sms, &bps);
+    if (r) return r;
     const long need = (A.n + 2 * block - 1) / (2 * block);
     grid = (int)(need < (long)sms * bps ? need : (long)sms * bps);
     if (grid < 1) grid = 1;
@@ -882,13 +833,10 @@ int mbx_prime_%(name)s_s(cudaStream_t s) {
     auto kern = holder_pair_kernel<%(name)s_T, %(name)s_CS>;
     const int smem_full = 2 * %(name)s_T::NVARS * %(name)s_T::LOCK_THREADS_S * (int)sizeof(f2_t);
     const int smem = %(name)s_T::NVARS * %(name)s_T::LOCK_THREADS_S * (int)sizeof(f2_t);
-    static int sms = 0;
-    if (!sms) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_full);
-    }
+    static LaunchCache lc;
+    int sms = 0, bps = 0;
+    const int r = launch_facts(lc, kern, 0, smem_full, 0, &sms, &bps);
+    if (r) return r;
     HolderArgs A;
     memset(&A, 0, sizeof(A));
     A.prime_npieces = %(name)s_pip_s32_NPIECES;
@@ -927,24 +875,122 @@ def write_tu(path, text):
 def write_kernels_cu(name):
     spec = SPECS[name]
     paths = []
-    inc = {"g": "pip", "e": "pip_e", "c": "dcoef", "p": "pip", "w": None}
+    inc = {"g": "pip", "e": "pip_e"}
     for v in variants_of(name):
+        if v == "w":
+            continue   # part of the table unit
         if v == "s":
             path = os.path.join(OUT, "%s_s.cu" % name)
             write_shift_tu(name, path)
             paths.append(path)
             continue
-        what, body = VARIANTS[v]
-        d = {"name": name, "NAME": name.upper(), "ncoef": spec.ncoef, "v": v, "what": what,
-             "include": ('#include "%s_%s.cuh"\n' % (name, inc[v])) if inc[v] else ""}
         path = os.path.join(OUT, "%s_%s.cu" % (name, v))
-        write_tu(path, (TU_HEAD + body) % d)
+        if v == "t":
+            d = {"name": name, "warp": TABLE_WARP % {"name": name} if "w" in variants_of(name) else ""}
+            write_tu(path, TABLE_TU % d)
+        else:
+            what, body = VARIANTS[v]
+            d = {"name": name, "NAME": name.upper(), "ncoef": spec.ncoef, "v": v, "what": what,
+                 "include": '#include "%s_%s.cuh"\n' % (name, inc[v])}
+            write_tu(path, (TU_HEAD + body) % d)
         paths.append(path)
     return paths
 
 
+def term_runs(vars_):
+    """(variable, exponent) runs of a term's variable list, in order."""
+    runs = []
+    for v in vars_:
+        if runs and runs[-1][0] == v:
+            runs[-1][1] += 1
+        else:
+            runs.append([v, 1])
+    return runs
+
+
+@__import__("functools").lru_cache(maxsize=None)
+def _table_runs(table_name):
+    t = load_pip(table_name)
+    return [term_runs(t.var[q, :t.deg[q]].tolist()) for q in range(t.nterms)]
+
+
+def term_pairs_max(table):
+    return max(1, max(len(r) for r in _table_runs(table.name)))
+
+
+def table_names():
+    """Term tables in registry order (an evaluator sharing another's table
+    refers to the same entry)."""
+    from mbx_b200.specs import KERNEL_ALIASES
+    names = []
+    for n in SPECS:
+        t = SPECS[KERNEL_ALIASES.get(n, n)].pip_table
+        if t not in names:
+            names.append(t)
+    return names
+
+
+def write_term_tables():
+    """Every evaluator's term table (csrc/term_table.cuh encoding) in one
+    binary file, embedded in the library by terms_blob.cpp (.incbin), plus the
+    index of the tables."""
+    blob = bytearray()
+    index = []
+    for tname in table_names():
+        t = load_pip(tname)
+        runs = _table_runs(tname)
+        words = np.zeros((t.nterms, 4), np.int32)
+        words[:, 0] = t.k
+        for q, rr in enumerate(runs):
+            if len(rr) > 6:
+                raise ValueError("%s term %d has more than six distinct variables" % (tname, q))
+            packed = [0, 0, 0]
+            for i in range(6):
+                v, e = (rr[i] if i < len(rr) else (255, 0))
+                if not (0 <= v < 255 and 0 < e < 256) and v != 255:
+                    raise ValueError("%s term %d: variable %d exponent %d out of range" % (tname, q, v, e))
+                packed[i >> 1] |= ((v & 255) | (e << 8)) << (16 * (i & 1))
+            for j in range(3):
+                words[q, 1 + j] = packed[j] - (1 << 32) if packed[j] >= 1 << 31 else packed[j]
+        off_terms = len(blob)
+        blob += words.tobytes()
+        off_coef = len(blob)
+        blob += np.ascontiguousarray(t.coef, np.float64).tobytes()
+        pad = (-len(blob)) % 16
+        blob += b"\0" * pad
+        index.append((tname, off_terms, off_coef, t.nterms, term_pairs_max(t)))
+    bin_path = os.path.join(OUT, "terms.bin")
+    old = open(bin_path, "rb").read() if os.path.exists(bin_path) else None
+    if old != bytes(blob):
+        with open(bin_path, "wb") as f:
+            f.write(bytes(blob))
+    lines = ["// Generated by mbx_b200/codegen/gen_kernels.py -- do not edit.", "#pragma once",
+             "// term tables in terms.bin: (name, byte offset of the int4 terms, of the",
+             "// double multiplicities, number of terms, (variable, exponent) pairs per term at most)",
+             "struct TermTableInfo { const char* name; long off_terms, off_tcoef, nterms; int pairs; };",
+             "static const TermTableInfo mbx_term_tables[] = {"]
+    for tname, ot, oc, nt, npair in index:
+        lines.append('    {"%s", %d, %d, %d, %d},' % (tname, ot, oc, nt, npair))
+    lines.append("};")
+    lines.append("static const int mbx_num_term_tables = %d;" % len(index))
+    lines.append("static const long mbx_terms_bytes = %d;" % len(blob))
+    write_tu(os.path.join(OUT, "terms_index.inc"), "\n".join(lines) + "\n")
+    # the binary is referenced by absolute path (generated per checkout)
+    write_tu(os.path.join(OUT, "terms_blob.cpp"),
+             "// Generated by mbx_b200/codegen/gen_kernels.py -- do not edit.\n"
+             "// The term tables of every evaluator (terms.bin), embedded read-only.\n"
+             "__asm__(\".section .rodata\\n\"\n"
+             "        \".balign 16\\n\"\n"
+             "        \".globl mbx_terms_blob\\n\"\n"
+             "        \".type mbx_terms_blob, @object\\n\"\n"
+             "        \"mbx_terms_blob:\\n\"\n"
+             "        \".incbin \\\"%s\\\"\\n\"\n"
+             "        \".size mbx_terms_blob, %d\\n\"\n"
+             "        \".previous\\n\");\n" % (bin_path, len(blob)))
+
+
 def write_registry():
-    """Host tables: evaluator descriptions, default coefficients, term tables."""
+    """Host tables: evaluator descriptions and default coefficients."""
     from mbx_b200.tables import load_fit
     from mbx_b200.specs import KERNEL_ALIASES
     lines = ["// Generated by mbx_b200/codegen/gen_kernels.py -- do not edit.", "#pragma once",
@@ -953,28 +999,27 @@ def write_registry():
         vs = variants_of(name)
         if name in KERNEL_ALIASES:
             vs = ""   # runs the kernels of KERNEL_ALIASES[name], declared there
-        for v in "gecpws":
+        for v in "gesw":
             if v not in vs:
                 continue
             if v in "ges":
                 lines.append("int mbx_launch_%s_%s(const HolderArgs& A, int grid, int block, cudaStream_t s);" %
                              (name, v))
                 lines.append("int mbx_prime_%s_%s(cudaStream_t s);" % (name, v))
-            elif v == "c":
-                lines.append("int mbx_launch_%s_c(const HolderArgs& A, const double* w, double* out, int grid, "
-                             "int block, cudaStream_t s);" % name)
-            elif v == "p":
-                lines.append("int mbx_launch_%s_p(long nd, const double* x, double* g, double* e, int grid, "
-                             "int block, cudaStream_t s);" % name)
+                lines.append("int mbx_set_coef_%s_%s(const double* a, int from_device, cudaStream_t s);" % (name, v))
             else:
                 lines.append("int mbx_launch_%s_w(const HolderArgs& A, int grads, int grid, cudaStream_t s);" % name)
-            lines.append("int mbx_set_coef_%s_%s(const double* a, int from_device, cudaStream_t s);" % (name, v))
+        if "t" in vs:
+            lines.append("int mbx_launch_%s_c(const HolderArgs& A, const double* w, double* out, int grid, "
+                         "int block, cudaStream_t s);" % name)
         fit = load_fit(name)
         lines.append("static const double mbx_fit_%s[%d] = {" % (name, len(fit)))
         for i in range(0, len(fit), 4):
             lines.append("    " + ", ".join(repr(float(x)) for x in fit[i:i + 4]) + ",")
         lines.append("};")
     lines.append("")
+    names = list(SPECS)
+    tables = table_names()
     lines.append("static const EvaluatorInfo mbx_evaluators[] = {")
     for name, spec in SPECS.items():
         vs = variants_of(name)
@@ -983,14 +1028,17 @@ def write_registry():
         skip = {"pair_gt": 0, "two_of_three_gt": 1, "all_three_gt": 2}[spec.skip]
 
         def fn(v, kind):
-            return ("mbx_%s_%s_%s" % (kind, kern, v)) if v in vs else "nullptr"
-        lines.append('    {"%s", %d, {"%s", "%s", "%s"}, %s, %d, %d, %d, %d, mbx_fit_%s, %s, %s, %s, %s, %s, %s, %s,' %
+            # the table unit ("t") holds the coefficient adjoint ("c")
+            have = ("t" in vs) if v == "c" else (v in vs)
+            return ("mbx_%s_%s_%s" % (kind, kern, v)) if have else "nullptr"
+        lines.append('    {"%s", %d, {"%s", "%s", "%s"}, %s, %d, %d, %d, %d, mbx_fit_%s, %s, %s, %s, %s, %s, %s,' %
                      (name, spec.nbody, ids[0], ids[1], ids[2], lit(spec.rf), skip, spec.ncoef, spec.nreal,
                       spec.nvars, name, fn("g", "launch"), fn("e", "launch"), fn("c", "launch"),
-                      fn("p", "launch"), fn("w", "launch"), fn("s", "launch"),
-                      lit(MIXED_FP64_RADIUS.get(name, 0.0))))
+                      fn("w", "launch"), fn("s", "launch"), lit(MIXED_FP64_RADIUS.get(name, 0.0))))
         lines.append("     %s, %s, %s," % (fn("g", "prime"), fn("e", "prime"), fn("s", "prime")))
-        lines.append("     {%s, nullptr}}," % ", ".join(fn(v, "set_coef") for v in "gecpws"))
+        lines.append("     {%s, nullptr, nullptr, nullptr, nullptr}, %d, %d}," %
+                     (", ".join(fn(v, "set_coef") for v in "ges"), tables.index(SPECS[kern].pip_table),
+                      names.index(kern)))
     lines.append("};")
     lines.append("static const int mbx_num_evaluators = %d;" % len(SPECS))
     # real atoms per monomer id (SetUpMonomers, bblock/sys_tools.cpp:133-254)
@@ -1002,29 +1050,8 @@ def write_registry():
     write_tu(os.path.join(OUT, "registry.inc"), "\n".join(lines) + "\n")
 
 
-def write_term_tables():
-    """Packed term tables for the warp kernel (types without straight-line code)."""
-    lines = ["// Generated by mbx_b200/codegen/gen_kernels.py -- do not edit.", "#pragma once", ""]
-    for name in SPECS:
-        if "w" not in variants_of(name):
-            continue
-        t = load_pip(name)
-        lines.append("static const int mbx_terms_%s[%d][4] = {" % (name, t.nterms))
-        for q in range(t.nterms):
-            packed = 0
-            for i in range(4):
-                v = int(t.var[q, i]) if i < t.deg[q] else 255
-                packed |= (v & 255) << (8 * i)
-            if packed >= 1 << 31:
-                packed -= 1 << 32
-            lines.append("{%d,%d,%d,0}," % (t.k[q], packed, t.deg[q]))
-        lines.append("};")
-        lines.append("static const double mbx_tcoef_%s[%d] = {%s};" %
-                     (name, t.nterms, ",".join(repr(float(c)) for c in t.coef)))
-    write_tu(os.path.join(OUT, "terms.inc"), "\n".join(lines) + "\n")
-
-
-def main(argv=None):
+def main(argv=None, quiet=False):
+    """Writes every generated file; returns the translation units to compile."""
     ap = argparse.ArgumentParser()
     ap.add_argument("names", nargs="*", default=list(SPECS))
     args = ap.parse_args(argv)
@@ -1032,12 +1059,24 @@ def main(argv=None):
     write_registry()
     write_term_tables()
     from mbx_b200.specs import KERNEL_ALIASES
+    keep = {"registry.inc", "terms_index.inc", "terms.bin", "terms_blob.cpp"}
     for n in args.names:
         if n in KERNEL_ALIASES:
             continue
         path, leaves, inner = generate(n)
-        write_kernels_cu(n)
-        print("%s: %d leaves, %d inner -> %s" % (n, leaves, inner, path))
+        keep.add(os.path.basename(path))
+        if n in STRAIGHT_TYPES:
+            for v in ("pip", "pip_e", "pip_s32"):
+                keep.add("%s_%s.cuh" % (n, v))
+        keep.update(os.path.basename(p) for p in write_kernels_cu(n))
+        if not quiet:
+            print("%s: %d leaves, %d inner -> %s" % (n, leaves, inner, path))
+    if args.names == list(SPECS):
+        # drop the units of an earlier generation (other variants or types)
+        for f in os.listdir(OUT):
+            if f not in keep:
+                os.remove(os.path.join(OUT, f))
+    return sorted(os.path.join(OUT, f) for f in os.listdir(OUT) if f.endswith((".cu", ".cpp")))
 
 
 if __name__ == "__main__":

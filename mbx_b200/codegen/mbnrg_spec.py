@@ -22,7 +22,7 @@ and against whole systems evaluated by the compiled reference
 the template evaluators whose specs are written by hand in specs.py and
 compares the two.
 
-Usage: ``python -m mbx_b200.codegen.mbnrg_spec [--ref /root/reference] [names...]``
+Usage: ``python -m mbx_b200.codegen.mbnrg_spec [--ref DIR] (or MBX_REFERENCE) [names...]``
 """
 import argparse
 import json
@@ -227,7 +227,7 @@ def _eval_line(path):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("MBX_REFERENCE"), required=not os.environ.get("MBX_REFERENCE"))
     ap.add_argument("names", nargs="*", default=list(SOURCES))
     args = ap.parse_args(argv)
     os.makedirs(DATA, exist_ok=True)

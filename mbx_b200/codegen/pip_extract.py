@@ -79,7 +79,7 @@ Output (``mbx_b200/data/``): ``<table>.pip.gz`` (term table, gzip) and
 round-trip bit-exactly); an evaluator's table is named after it unless
 several evaluators share one polynomial.
 
-Usage: ``python -m mbx_b200.codegen.pip_extract [--ref /root/reference]``
+Usage: ``python -m mbx_b200.codegen.pip_extract [--ref DIR] (or MBX_REFERENCE)``
 """
 import argparse
 import gzip
@@ -483,7 +483,7 @@ def write_fit(name, fit):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("MBX_REFERENCE"), required=not os.environ.get("MBX_REFERENCE"))
     ap.add_argument("names", nargs="*", default=list(PROGRAMS) + list(MBNRG_PROGRAMS))
     args = ap.parse_args(argv)
     for name in args.names:

@@ -14,10 +14,12 @@
 // scatter steps of System::Get2B/Get3B (bblock/system.cpp:2425-2725,
 // 2769-3073).
 //
-// The CH4-CH4 polynomial (201k terms) is evaluated by a warp per dimer that
-// walks the term table (pip_warp below).
+// The evaluators without straight-line code (the CH4-CH4 polynomial with its
+// 201k terms and the widened MB-nrg types) are evaluated by a warp per n-mer
+// that walks the polynomial's term table (holder_table_kernel below).
 #pragma once
 #include "holder_common.cuh"
+#include "term_table.cuh"
 
 // Precision / output modes.
 // HM_GRAD_SHIFT32 names the paired FP32 kernel (holder_pair_kernel) where a
@@ -43,8 +45,8 @@ struct HolderArgs {
     const BoxParams* conf_bp;  // null: one configuration in bp
     const int* mon_conf;
     double* conf_out;
-    // table-driven polynomial (warp kernel)
-    const int4* terms;         // (k, v0 | v1<<8 | v2<<16 | v3<<24 (255 = none), deg, unused)
+    // term table of the polynomial (term_table.cuh), for the table-driven kernels
+    const int4* terms;         // (k, six (variable, exponent) byte pairs)
     const double* tcoef;       // term multiplicities
     long nterms;
     // code prefetch launch of a lockstep kernel (prime_passes > 0; see
@@ -561,11 +563,14 @@ __global__ void __launch_bounds__(T::LOCK_THREADS_S, 1) holder_pair_kernel(const
     block_reduce_add<7>(acc, A.out);
 }
 
-// Warp-cooperative evaluation for polynomials too large for straight-line
-// code: lane l handles terms l, l+32, ...; variables and gradient
-// accumulators of the warp's n-mer live in shared memory.
+// Table-driven evaluation (evaluators without straight-line code): a warp
+// per n-mer, lane l taking terms l, l+32, ... of the term table
+// (term_table.cuh); the n-mer's variables and gradient accumulators live in
+// shared memory, the gradient summed with shared-memory atomics.  The rest
+// (gather, image, variables, switch, chain rule, scatter) is the same code
+// as the straight-line kernels.
 template <class T, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32) holder_warp_kernel(const HolderArgs A, int grads) {
+__global__ void __launch_bounds__(WARPS * 32) holder_table_kernel(const HolderArgs A, int grads) {
     __shared__ double xs[WARPS][T::NVARS];
     __shared__ double gs[WARPS][T::NVARS];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -588,26 +593,15 @@ __global__ void __launch_bounds__(WARPS * 32) holder_warp_kernel(const HolderArg
             for (int v = 0; v < T::NVARS; ++v) { xs[w][v] = x[v]; gs[w][v] = 0.0; }
         }
         __syncwarp();
+        const auto xv = [&](int v) { return xs[w][v]; };
         double e = 0.0;
         for (long q = lane; q < A.nterms; q += 32) {
             const int4 tm = __ldg(A.terms + q);
-            const double c = (A.coef ? __ldg(A.coef + tm.x) : 0.0) * __ldg(A.tcoef + q);
-            const int deg = tm.z;
-            int v[4];
-            double xv[4];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                v[i] = (tm.y >> (8 * i)) & 255;
-                xv[i] = i < deg ? xs[w][v[i]] : 1.0;
-            }
-            const double p01 = xv[0] * xv[1], p23 = xv[2] * xv[3];
-            e += c * p01 * p23;
-            if (grads) {
-                if (deg > 0) atomicAdd(&gs[w][v[0]], c * xv[1] * p23);
-                if (deg > 1) atomicAdd(&gs[w][v[1]], c * xv[0] * p23);
-                if (deg > 2) atomicAdd(&gs[w][v[2]], c * p01 * xv[3]);
-                if (deg > 3) atomicAdd(&gs[w][v[3]], c * p01 * xv[2]);
-            }
+            const double c = __ldg(A.coef + tm.x) * __ldg(A.tcoef + q);
+            if (grads)
+                e += term_value_grad<T::TPAIRS>(tm, c, xv, [&](int v, double dv) { atomicAdd(&gs[w][v], dv); });
+            else
+                e += term_value<T::TPAIRS>(tm, c, xv);
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
@@ -623,13 +617,86 @@ __global__ void __launch_bounds__(WARPS * 32) holder_warp_kernel(const HolderArg
     block_reduce_add<7>(acc, A.out);
 }
 
+// Table-driven evaluation, a lane per n-mer: the warp walks the whole term
+// table in step, every lane applying each term to its own n-mer, whose
+// variables and gradient accumulators sit in shared-memory columns [v][lane]
+// (conflict-free, no atomics).  This is the form for the many-n-mer buckets
+// of a liquid (a warp per n-mer would serialise on shared-memory atomics of
+// the few variables); the 201k-term CH4-CH4 table, with few dimers per box,
+// keeps the warp-per-n-mer form above.  Dynamic shared memory:
+// 4 warps x 2 x NVARS x 32 doubles.
+template <class T>
+__global__ void __launch_bounds__(128) holder_table_lane_kernel(const HolderArgs A, int grads) {
+    double* xc = reinterpret_cast<double*>(mbx_dyn_smem) + ((threadIdx.x >> 5) * 2 * T::NVARS) * 32 +
+                 (threadIdx.x & 31);
+    double* gc = xc + T::NVARS * 32;
+    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    const long n = nmer_count(A);
+    for (long base = blockIdx.x * (long)blockDim.x; base < n; base += (long)gridDim.x * blockDim.x) {
+        const long t = base + threadIdx.x;
+        bool live = t < n;
+        {
+            double x[T::NVARS];
+#pragma unroll
+            for (int v = 0; v < T::NVARS; ++v) x[v] = 0.0;
+            if (live) {
+                double r[T::NREAL][3];
+                load_nmer<T, false>(A, t, r);
+                double d[3][3], rr[3];
+                if (pair_dists<T>(r, d, rr)) {
+                    if (A.e_per) A.e_per[t] = 0.0;
+                    live = false;
+                } else {
+                    double s[T::NSITES][3];
+                    T::sites(r, s);
+                    T::vars(s, x);
+                }
+            }
+#pragma unroll
+            for (int v = 0; v < T::NVARS; ++v) {
+                xc[v * 32] = x[v];
+                gc[v * 32] = 0.0;
+            }
+        }
+        __syncwarp();
+        double e = 0.0;
+        if (__any_sync(0xffffffffu, live)) {
+            const auto xv = [&](int v) { return xc[v * 32]; };
+            for (long q = 0; q < A.nterms; ++q) {
+                const int4 tm = __ldg(A.terms + q);
+                const double c = __ldg(A.coef + tm.x) * __ldg(A.tcoef + q);
+                if (grads)
+                    e += term_value_grad<T::TPAIRS>(tm, c, xv, [&](int v, double dv) { gc[v * 32] += dv; });
+                else
+                    e += term_value<T::TPAIRS>(tm, c, xv);
+            }
+        }
+        __syncwarp();
+        if (live) {
+            double g[T::NVARS];
+#pragma unroll
+            for (int v = 0; v < T::NVARS; ++v) g[v] = grads ? gc[v * 32] : 0.0;
+            finish_nmer<T>(A, t, e, g, grads != 0, acc);
+        }
+        __syncwarp();
+    }
+    block_reduce_add<7>(acc, A.out);
+}
+
 // Gradient with respect to the linear coefficients: out[k] += sum over n-mers
 // of w[n] * sw(n) * dP/da_k(x(n)), the monomials recomputed from the
-// coordinates (adjoint of E = sum_n sw(n) P(a, x(n)) for refitting).
+// coordinates (adjoint of E = sum_n sw(n) P(a, x(n)) for refitting), from the
+// term table.  A lane per n-mer, its variables in a shared-memory column; the
+// warp walks the table (sorted by coefficient) in step, and at the end of a
+// coefficient's terms the lanes' sums are reduced across the warp into a
+// per-block shared array, added to out at the end.
+// Dynamic shared memory: NCOEF doubles + 4 warps x NVARS x 32 doubles.
 template <class T>
-__global__ void __launch_bounds__(128) holder_dcoef_kernel(const HolderArgs A, const double* __restrict__ w,
-                                                           double* __restrict__ out) {
-    __shared__ double part[T::NCOEF];
+__global__ void __launch_bounds__(128) holder_dcoef_table_kernel(const HolderArgs A, const double* __restrict__ w,
+                                                                 double* __restrict__ out) {
+    double* part = reinterpret_cast<double*>(mbx_dyn_smem);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double* xcol = part + T::NCOEF + (warp * T::NVARS) * 32 + lane;
     for (int k = threadIdx.x; k < T::NCOEF; k += blockDim.x) part[k] = 0.0;
     __syncthreads();
     const long nt = nmer_count(A);
@@ -651,39 +718,29 @@ __global__ void __launch_bounds__(128) holder_dcoef_kernel(const HolderArgs A, c
                 scale = apply_switch<T>(d, rr, 0.0, tg, false) * (w ? w[t] : 1.0);
             }
         }
-        if constexpr (T::STRAIGHT) {
-            const unsigned lane = threadIdx.x & 31;
-            T::dcoef(x, [&](int k, double m) {
-                double v = scale * m;
 #pragma unroll
-                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-                if (lane == 0 && v != 0.0) atomicAdd(&part[k], v);
-            });
+        for (int v = 0; v < T::NVARS; ++v) xcol[v * 32] = x[v];
+        __syncwarp();
+        if (__any_sync(0xffffffffu, scale != 0.0)) {
+            const auto xv = [&](int v) { return xcol[v * 32]; };
+            double sum = 0.0;
+            int4 tm = __ldg(A.terms);
+            for (long q = 0; q < A.nterms; ++q) {
+                const int4 nx = q + 1 < A.nterms ? __ldg(A.terms + q + 1) : make_int4(-1, 0, 0, 0);
+                sum += term_value<T::TPAIRS>(tm, __ldg(A.tcoef + q), xv);
+                if (nx.x != tm.x) {
+                    double v = sum * scale;
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                    if (lane == 0 && v != 0.0) atomicAdd(&part[tm.x], v);
+                    sum = 0.0;
+                }
+                tm = nx;
+            }
         }
+        __syncwarp();
     }
     __syncthreads();
     for (int k = threadIdx.x; k < T::NCOEF; k += blockDim.x)
         if (part[k] != 0.0) atomicAdd(out + k, part[k]);
-}
-
-// The generated-polynomial calling convention of the reference
-// (poly_2b_v6x::eval(nd, a, x, t, g), potential/2b/poly-2b-v6x.h:95): nd
-// configurations, variables and gradients stored variable-major
-// (x[v * nd + i]); energies to e[i].  One configuration per thread, so every
-// load and store is coalesced.
-template <class T, class CC>
-__global__ void __launch_bounds__(128) poly_soa_kernel(long nd, const double* __restrict__ x_soa,
-                                                       double* __restrict__ g_soa, double* __restrict__ e) {
-    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < nd; i += (long)gridDim.x * blockDim.x) {
-        double x[T::NVARS], g[T::NVARS];
-#pragma unroll
-        for (int v = 0; v < T::NVARS; ++v) { x[v] = __ldg(x_soa + v * nd + i); g[v] = 0.0; }
-        const CC coef{};
-        const double ev = T::pip(coef, x, g);
-        e[i] = ev;
-        if (g_soa) {
-#pragma unroll
-            for (int v = 0; v < T::NVARS; ++v) g_soa[v * nd + i] = g[v];
-        }
-    }
 }

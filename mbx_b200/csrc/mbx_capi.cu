@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <mutex>
 
 #include <algorithm>
 #include <cmath>
@@ -23,9 +24,13 @@
 #include "holder_kernel.cuh"
 #include "nmer_build.h"
 
+// Generic table-driven polynomial over caller-supplied variables
+// (table_kernels.cu).
+int mbx_launch_poly_table(long nd, int nvars, const double* x, double* g, double* e, const int4* terms,
+                          const double* tcoef, long nterms, const double* coef, int pairs, int sms, cudaStream_t s);
+
 typedef int (*launch_fn)(const HolderArgs&, int, int, cudaStream_t);
 typedef int (*dcoef_fn)(const HolderArgs&, const double*, double*, int, int, cudaStream_t);
-typedef int (*poly_fn)(long, const double*, double*, double*, int, int, cudaStream_t);
 typedef int (*prime_fn)(cudaStream_t);
 typedef int (*warp_fn)(const HolderArgs&, int, int, cudaStream_t);
 typedef int (*setcoef_fn)(const double*, int, cudaStream_t);
@@ -38,18 +43,20 @@ struct EvaluatorInfo {
     int skip;
     int ncoef, nreal, nvars;
     const double* fit;
-    launch_fn g, e;
-    dcoef_fn c;
-    poly_fn p;
-    warp_fn w;
+    launch_fn g, e;   // straight-line FP64 kernels (energy + gradient, energy only), or null
+    dcoef_fn c;       // coefficient adjoint (table-driven)
+    warp_fn w;        // table-driven evaluation of the types without straight-line kernels, or null
     launch_fn s;      // FP32 kernel of the mixed mode (FP32 basis), or null
     double split_r;   // mixed mode: n-mers with first-atom distance below this run in FP64 (0: none)
     prime_fn pg, pe, ps;   // code prefetch of the g, e and s kernels (holder_prime_kernel), or null
-    setcoef_fn set[7];
+    setcoef_fn set[7];     // constant-memory coefficient setters of the straight-line kernels
+    int table;        // term table (mbx_term_tables)
+    int kern;         // evaluator whose kernels and coefficients this one runs (itself or an alias target)
 };
 
 #include "gen/registry.inc"
-#include "gen/terms.inc"
+#include "gen/terms_index.inc"
+#include "device_state.h"
 
 #define MBX_VERSION_STRING "mbx_b200 0.1 (sm_100a)"
 
@@ -87,6 +94,93 @@ const EvaluatorInfo* find_evaluator(const char* name) {
         if (!strcmp(mbx_evaluators[i].name, name)) return &mbx_evaluators[i];
     return nullptr;
 }
+
+constexpr int kMaxDevices = 64;
+std::mutex g_dev_mu;
+bool g_dev_constants[kMaxDevices] = {false};
+DeviceTables g_dev_tables[kMaxDevices];
+long g_coef_off[256];
+long g_coef_total = -1;
+
+void coef_layout() {
+    if (g_coef_total >= 0) return;
+    long off = 0;
+    for (int i = 0; i < mbx_num_evaluators; ++i) {
+        g_coef_off[i] = off;
+        off += mbx_evaluators[i].ncoef;
+    }
+    g_coef_total = off;
+}
+
+}  // namespace
+
+// The embedded term tables (gen/terms_blob.cpp).
+extern "C" const unsigned char mbx_terms_blob[];
+
+std::mutex& mbx_device_mutex() { return g_dev_mu; }
+
+long mbx_coef_offset(int evaluator) {
+    coef_layout();
+    return g_coef_off[evaluator];
+}
+
+// Caller holds g_dev_mu.
+static int device_constants_locked(int dev) {
+    if (dev < 0 || dev >= kMaxDevices) return MBX_EINVAL;
+    if (g_dev_constants[dev]) return MBX_OK;
+    int cur = 0;
+    if (cudaGetDevice(&cur) != cudaSuccess) return MBX_ENODEV;
+    if (cur != dev && cudaSetDevice(dev) != cudaSuccess) return MBX_ECUDA;
+    int rc = MBX_OK;
+    for (int i = 0; i < mbx_num_evaluators && rc == MBX_OK; ++i) {
+        const EvaluatorInfo& E = mbx_evaluators[i];
+        if (E.kern != i) continue;   // an alias shares its target's kernels and coefficients
+        for (int v = 0; v < 7; ++v)
+            if (E.set[v] && E.set[v](E.fit, 0, nullptr) != 0) rc = MBX_ECUDA;
+    }
+    if (rc == MBX_OK && cudaDeviceSynchronize() != cudaSuccess) rc = MBX_ECUDA;
+    if (rc == MBX_OK) g_dev_constants[dev] = true;
+    if (cur != dev) cudaSetDevice(cur);
+    return rc;
+}
+
+int mbx_device_constants(int dev) {
+    std::lock_guard<std::mutex> lock(g_dev_mu);
+    return device_constants_locked(dev);
+}
+
+int mbx_device_tables(int dev, DeviceTables* out) {
+    std::lock_guard<std::mutex> lock(g_dev_mu);
+    int rc = device_constants_locked(dev);
+    if (rc) return rc;
+    DeviceTables& T = g_dev_tables[dev];
+    if (!T.blob) {
+        coef_layout();
+        int cur = 0;
+        if (cudaGetDevice(&cur) != cudaSuccess) return MBX_ENODEV;
+        if (cur != dev && cudaSetDevice(dev) != cudaSuccess) return MBX_ECUDA;
+        void* blob = nullptr;
+        void* coef = nullptr;
+        cudaError_t e = cudaMalloc(&blob, (size_t)mbx_terms_bytes);
+        if (e == cudaSuccess) e = cudaMalloc(&coef, (size_t)g_coef_total * sizeof(double));
+        if (e == cudaSuccess) e = cudaMemcpy(blob, mbx_terms_blob, (size_t)mbx_terms_bytes, cudaMemcpyHostToDevice);
+        for (int i = 0; i < mbx_num_evaluators && e == cudaSuccess; ++i)
+            e = cudaMemcpy(static_cast<double*>(coef) + g_coef_off[i], mbx_evaluators[i].fit,
+                           mbx_evaluators[i].ncoef * sizeof(double), cudaMemcpyHostToDevice);
+        if (cur != dev) cudaSetDevice(cur);
+        if (e != cudaSuccess) {
+            if (blob) cudaFree(blob);
+            if (coef) cudaFree(coef);
+            return MBX_ECUDA;
+        }
+        T.blob = static_cast<const unsigned char*>(blob);
+        T.coef = static_cast<double*>(coef);
+    }
+    *out = T;
+    return MBX_OK;
+}
+
+namespace {
 
 // Slot order the reference's dispatch sorts the monomer ids into
 // (e2b::get_2b_energy, potential/2b/energy2b.cpp:240-254;
@@ -180,8 +274,7 @@ struct mbx_ctx {
     cudaEvent_t ev_fork = nullptr;
     DevBuf<int4> buckets, list;
     DevBuf<unsigned long long> listed;
-    DevBuf<int4> terms;
-    DevBuf<double> tcoef, warp_coef;
+    DeviceTables tables;   // per-device term tables and coefficients (shared, not owned)
     int nb_cap = 192;
     // runtime launch shapes of the builder (set by mbx_tune)
     struct Knobs {
@@ -275,24 +368,14 @@ int mbx_create(mbx_ctx** out, int device, void* stream) {
     CUCHK(c, c->listed.ensure(4));
     for (int nb = 0; nb < 4; ++nb)
         for (int b = 0; b < MBX_MAX_BUCKETS; ++b) c->bucket_cap[nb][b] = 0;
-    // fitted coefficients into every kernel variant (constant memory, per device)
-    for (int i = 0; i < mbx_num_evaluators; ++i) {
-        const EvaluatorInfo& E = mbx_evaluators[i];
-        for (int v = 0; v < 7; ++v)
-            if (E.set[v]) RCHK(c, E.set[v](E.fit, 0, c->stream));
-    }
-    // the table-driven evaluator reads its terms and coefficients from global memory
+    // the fitted coefficients (constant banks, per device: loaded by the
+    // first context on a device, kept by later ones) and the term tables
     {
-        const EvaluatorInfo* E = find_evaluator("ch4ch42b");
-        const long nt = sizeof(mbx_tcoef_ch4ch42b) / sizeof(double);
-        CUCHK(c, c->terms.ensure(nt));
-        CUCHK(c, c->tcoef.ensure(nt));
-        CUCHK(c, c->warp_coef.ensure(E->ncoef));
-        CUCHK(c, cudaMemcpyAsync(c->terms.p, mbx_terms_ch4ch42b, nt * sizeof(int4), cudaMemcpyHostToDevice, c->stream));
-        CUCHK(c, cudaMemcpyAsync(c->tcoef.p, mbx_tcoef_ch4ch42b, nt * sizeof(double), cudaMemcpyHostToDevice,
-                                 c->stream));
-        CUCHK(c, cudaMemcpyAsync(c->warp_coef.p, E->fit, E->ncoef * sizeof(double), cudaMemcpyHostToDevice,
-                                 c->stream));
+        const int r = mbx_device_tables(device, &c->tables);
+        if (r) {
+            mbx_destroy(c);
+            return r;
+        }
     }
     CUCHK(c, cudaStreamSynchronize(c->stream));
     *out = c;
@@ -306,7 +389,7 @@ int mbx_destroy(mbx_ctx* c) {
     DevBuf<int>* ib[] = {&c->d_first, &c->d_nat, &c->d_tag, &c->d_type, &c->d_members[0], &c->d_members[1],
                          &c->d_query[0], &c->d_query[1], &c->bucket_count, &c->status, &c->counters};
     for (auto* b : ib) b->release();
-    DevBuf<double>* db[] = {&c->xyz, &c->grad, &c->out, &c->coef_ws, &c->tcoef, &c->warp_coef};
+    DevBuf<double>* db[] = {&c->xyz, &c->grad, &c->out, &c->coef_ws};
     for (auto* b : db) b->release();
     for (auto& sc : c->scratch) sc.release();
     for (int i = 1; i < MBX_BUILD_LANES; ++i) {
@@ -325,7 +408,6 @@ int mbx_destroy(mbx_ctx* c) {
     c->buckets.release();
     c->list.release();
     c->listed.release();
-    c->terms.release();
     c->d_conf_bp.release();
     c->d_mon_conf.release();
     c->conf_out.release();
@@ -734,16 +816,23 @@ static HolderArgs base_args(mbx_ctx* c) {
     return A;
 }
 
+// Term table and global-memory coefficients of evaluator E on the context's
+// device, for the table-driven kernels.
+static void table_args(mbx_ctx* c, const EvaluatorInfo* E, HolderArgs& A) {
+    const TermTableInfo& T = mbx_term_tables[E->table];
+    A.terms = reinterpret_cast<const int4*>(c->tables.blob + T.off_terms);
+    A.tcoef = reinterpret_cast<const double*>(c->tables.blob + T.off_tcoef);
+    A.nterms = T.nterms;
+    if (!A.coef) A.coef = c->tables.coef + mbx_coef_offset(E->kern);
+}
+
 static int launch_eval(mbx_ctx* c, const EvaluatorInfo* E, HolderArgs A, int flags, int* kernels,
                        bool near = false) {
     const bool grads = !(flags & MBX_NO_GRADS);
     const bool mixed = (flags & MBX_MIXED) != 0;
     const int block = 128;
     if (E->w) {
-        A.terms = c->terms.p;
-        A.tcoef = c->tcoef.p;
-        A.nterms = (long)(sizeof(mbx_tcoef_ch4ch42b) / sizeof(double));
-        if (!A.coef) A.coef = c->warp_coef.p;
+        table_args(c, E, A);
         long nw = A.n;
         int grid = (int)std::min<long>((nw + 3) / 4, (long)c->sm_count * 8);
         RCHK(c, E->w(A, grads ? 1 : 0, std::max(grid, 1), c->stream));
@@ -946,8 +1035,8 @@ extern "C" int mbx_energy(mbx_ctx* c, int nbody, double* xyz, int use_ghost, dou
 }
 
 // The child context of mbx_energy_2b3b: the 2b term on its own stream and
-// buffers, same topology, configuration, launch shapes and CH4-CH4
-// coefficients as the parent.
+// buffers, same topology, configuration and launch shapes as the parent
+// (coefficients are per device, so shared already).
 static int sync_child(mbx_ctx* c) {
     if (c->child && c->child_gen == c->gen) return MBX_OK;
     if (!c->child) {
@@ -977,9 +1066,6 @@ static int sync_child(mbx_ctx* c) {
         r = mbx_set_batch(k, c->nconf, c->conf_mon.data(), boxes.data(), has.data());
         if (r) return fail(c, r, std::string("child batch: ") + k->err);
     }
-    if (c->warp_coef.p && k->warp_coef.p)
-        CUCHK(c, cudaMemcpy(k->warp_coef.p, c->warp_coef.p, std::min(c->warp_coef.n, k->warp_coef.n) * sizeof(double),
-                            cudaMemcpyDeviceToDevice));
     c->child_gen = c->gen;
     return MBX_OK;
 }
@@ -1216,8 +1302,9 @@ extern "C" int mbx_evaluate_dcoef(mbx_ctx* c, const char* name, long n, const do
     A.n = n;
     A.aos = 1;
     A.xyz = X;
+    table_args(c, E, A);
     if (n > 0) {
-        const int grid = (int)std::max<long>(1, std::min<long>((n + 127) / 128, (long)c->sm_count * 4));
+        const int grid = (int)std::max<long>(1, std::min<long>((n + 127) / 128, (long)c->sm_count * 2));
         RCHK(c, E->c(A, W, O, grid, 128, c->stream));
     }
     if (!dev) {
@@ -1233,7 +1320,6 @@ extern "C" int mbx_poly(mbx_ctx* c, const char* name, long nd, const double* x, 
     if (!c || !name || nd < 0 || (nd > 0 && (!x || !e))) return fail(c, MBX_EINVAL, "bad arguments");
     const EvaluatorInfo* E = find_evaluator(name);
     if (!E) return fail(c, MBX_ENOTSUP, std::string("unknown evaluator ") + name);
-    if (!E->p) return fail(c, MBX_ENOTSUP, std::string("no straight-line polynomial for ") + name);
     CUCHK(c, cudaSetDevice(c->device));
     const bool dev = (flags & MBX_DEVICE_PTRS) != 0;
     const size_t nv = (size_t)nd * E->nvars;
@@ -1249,8 +1335,10 @@ extern "C" int mbx_poly(mbx_ctx* c, const char* name, long nd, const double* x, 
         Ev = eb.p;
     }
     if (nd > 0) {
-        const int grid = (int)std::max<long>(1, std::min<long>((nd + 127) / 128, (long)c->sm_count * 4));
-        RCHK(c, E->p(nd, X, G, Ev, grid, 128, c->stream));
+        HolderArgs A = base_args(c);
+        table_args(c, E, A);
+        RCHK(c, mbx_launch_poly_table(nd, E->nvars, X, G, Ev, A.terms, A.tcoef, A.nterms, A.coef,
+                                      mbx_term_tables[E->table].pairs, c->sm_count, c->stream));
     }
     if (!dev && nd > 0) {
         CUCHK(c, cudaMemcpyAsync(e, Ev, nd * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -1266,14 +1354,16 @@ extern "C" int mbx_set_coefficients(mbx_ctx* c, const char* name, const double* 
     if (!E) return fail(c, MBX_ENOTSUP, std::string("unknown evaluator ") + name);
     CUCHK(c, cudaSetDevice(c->device));
     const bool dev = a && (flags & MBX_DEVICE_PTRS);
-    const double* src = a ? a : E->fit;
+    const EvaluatorInfo* K = &mbx_evaluators[E->kern];
+    const double* src = a ? a : K->fit;
+    // coefficients are per device: wait for all work on the device (any
+    // context's) before changing them, under the device-state lock
+    std::lock_guard<std::mutex> lock(mbx_device_mutex());
+    CUCHK(c, cudaDeviceSynchronize());
     for (int v = 0; v < 7; ++v)
-        if (E->set[v]) RCHK(c, E->set[v](src, dev ? 1 : 0, c->stream));
-    if (E->w) {
-        CUCHK(c, cudaMemcpyAsync(c->warp_coef.p, src, E->ncoef * sizeof(double),
-                                 dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, c->stream));
-        ++c->gen;   // the child context copies them again
-    }
+        if (K->set[v]) RCHK(c, K->set[v](src, dev ? 1 : 0, c->stream));
+    CUCHK(c, cudaMemcpyAsync(c->tables.coef + mbx_coef_offset(E->kern), src, E->ncoef * sizeof(double),
+                             dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, c->stream));
     CUCHK(c, cudaStreamSynchronize(c->stream));
     return MBX_OK;
 }

@@ -21,6 +21,7 @@
 #include <mutex>
 
 #include "../../include/mbx_b200.h"
+#include "device_state.h"
 #include "holder_kernel.cuh"
 
 #define MBX_NOALLOC_HEAD 32   // doubles reserved in front of the per-n-mer energies (slot 0: work counter)
@@ -105,8 +106,13 @@ extern "C" int mbx_evaluate_noalloc(const char* evaluator, long n, const double*
     if (!E) return MBX_ENOTSUP;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return MBX_ENODEV;
+    // the models' fitted coefficients in the kernels' constant banks: loaded
+    // by the first call on a device that no context has loaded them on
+    // (constant-memory copies only, no allocation)
+    int rc = mbx_device_constants(dev);
+    if (rc) return rc;
     double* scratch = nullptr;
-    int rc = scratch_for(dev, &scratch);
+    rc = scratch_for(dev, &scratch);
     if (rc) return rc;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     // the array keeps the previous call's contents: the counter must restart

@@ -16,12 +16,19 @@ N2O5 mini-library), and links them with:
 * ``ref_harness.cpp``: ``extern "C"`` entry points over ``bblock::System``.
 
 Optimisation follows the reference's defaults (``-O2``, no ``-march``,
-``configure.ac:187,222``) for every file the 2-body/3-body path executes; the
-rest of the library (1-body, 4-body, other monomer types, dispersion, ...) is
+``configure.ac:187,222``) for every file the timed water path executes
+(``System::TwoBodyEnergy/ThreeBodyEnergy`` on MB-pol water: the n-mer
+search, the MB-pol 2b/3b holders and polynomials, the dispatch); the rest of
+the library (other monomer types, 1-body, 4-body, dispersion, ...) is
 compiled at ``-O0`` only so that it links quickly, as the reference itself
-does for its N2O5 files (``src/Makefile.am:21-25``).
+does for its N2O5 files (``src/Makefile.am:21-25``).  On x86-64 without
+``-march`` and ``-ffast-math`` the optimisation level does not change a
+double-precision result (SSE2 arithmetic, no FMA contraction, no
+reassociation), so the -O0 files give the same numbers as the reference's
+own build; they are only slower, and they are not timed.
 
-Usage: ``python oracle/build_ref.py [--ref /root/reference] [-j N]``.
+Usage: ``python oracle/build_ref.py [--ref DIR] [-j N]``; the reference root
+is ``--ref``, else the ``MBX_REFERENCE`` environment variable.
 Incremental: an object is rebuilt only when its source is newer.
 """
 import argparse
@@ -30,6 +37,7 @@ import os
 import re
 import subprocess
 import sys
+import time
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
@@ -42,15 +50,12 @@ LISTS = [
     "buck_sources", "ff_sources", "lj_sources",
 ]
 
-# Files the 2-body/3-body path executes: compiled like the reference (-O2).
+# Files the timed water path executes: compiled like the reference (-O2).
 HOT = {
     "potential/2b/energy2b.cpp", "potential/2b/x2b-v9x.cpp", "potential/2b/poly-2b-v6x.cpp",
-    "potential/2b/poly-2b-v6x-nogrd.cpp", "potential/2b/x2b_A1B2Z2_C1D4_deg3_exp0_v1x.cpp",
-    "potential/2b/poly_2b_A1B2Z2_C1D4_deg3_exp0_v1.cpp", "potential/2b/poly_2b_A1B2Z2_C1D4_deg3_exp0_v1x.cpp",
-    "potential/2b/x2b_A1B4_A1B4_deg4_exp0_v1x.cpp", "potential/2b/poly_2b_A1B4_A1B4_deg4_exp0_v1.cpp",
+    "potential/2b/poly-2b-v6x-nogrd.cpp",
     "potential/3b/energy3b.cpp", "potential/3b/x3b-v2x.cpp", "potential/3b/poly-3b-v2x.cpp",
-    "potential/3b/poly-3b-v2x-nogrd.cpp", "potential/3b/mbnrg_3b_A1B4_C1D2_C1D2_deg3_v1.cpp",
-    "potential/3b/poly_3b_A1B4_C1D2_C1D2_deg3_grad_v1.cpp", "potential/3b/poly_3b_A1B4_C1D2_C1D2_deg3_nograd_v1.cpp",
+    "potential/3b/poly-3b-v2x-nogrd.cpp",
     "potential/electrostatics/electrostatics.cpp", "potential/electrostatics/fields.cpp",
 }
 HOT_DIRS = ("tools/", "io_tools/", "bblock/")
@@ -70,19 +75,25 @@ def sources(ref):
 
 def compile_one(cmd, src, obj):
     if os.path.exists(obj) and os.path.getmtime(obj) >= os.path.getmtime(src):
-        return obj, None
-    r = subprocess.run(cmd + ["-c", src, "-o", obj], capture_output=True, text=True)
+        return obj, None, 0.0
+    t0 = time.time()
+    r = subprocess.run(cmd + ["-c", src, "-o", obj + ".tmp"], capture_output=True, text=True)
     if r.returncode != 0:
-        return obj, r.stderr[-4000:]
-    return obj, None
+        return obj, r.stderr[-4000:], time.time() - t0
+    os.replace(obj + ".tmp", obj)
+    return obj, None, time.time() - t0
 
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("MBX_REFERENCE"))
     ap.add_argument("-j", type=int, default=os.cpu_count() or 4)
     ap.add_argument("--cxx", default="/usr/bin/g++")
     args = ap.parse_args(argv)
+    t_start = time.time()
+    if not args.ref:
+        print("no reference root (--ref or MBX_REFERENCE); oracle/_ref not built")
+        return 0
     src_root = os.path.join(args.ref, "src")
     if not os.path.isdir(src_root):
         print("reference sources not found at %s; oracle/_ref not built" % src_root)
@@ -107,9 +118,11 @@ def main(argv=None):
     jobs.sort(key=lambda j: -os.path.getsize(j[1]))
     errors = []
     with cf.ThreadPoolExecutor(max_workers=args.j) as ex:
-        for obj, err in ex.map(lambda j: compile_one(*j), jobs):
+        for obj, err, dt in ex.map(lambda j: compile_one(*j), jobs):
             if err:
                 errors.append((obj, err))
+            elif dt > 20:
+                print("  compiled %s (%.0f s)" % (os.path.basename(obj), dt), flush=True)
     if errors:
         for obj, err in errors:
             sys.stderr.write("FAILED %s\n%s\n" % (obj, err))
@@ -121,7 +134,7 @@ def main(argv=None):
         if r.returncode != 0:
             sys.stderr.write(r.stderr[-4000:])
             return 1
-    print("built %s" % LIB)
+    print("built %s (%.0f s)" % (LIB, time.time() - t_start))
     return 0
 
 

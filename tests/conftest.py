@@ -10,6 +10,12 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 
+# The reference checkout, for the CPU tests that read its sources: the
+# MBX_REFERENCE environment variable, else the build machine's checkout when
+# present (GPU machines have none; those tests skip or use the fixtures).
+if not os.environ.get("MBX_REFERENCE") and os.path.isdir("/root/reference/src"):
+    os.environ["MBX_REFERENCE"] = "/root/reference"
+
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200); runs the CUDA path")
@@ -31,3 +37,20 @@ def ctx():
     c = capi.Context(0)
     yield c
     c.close()
+
+
+# GPU suite order: the path itself first (evaluator goldens, boxes against the
+# reference, lists), then batching and the autograd wrapper; the
+# allocation-free entry point (tests/test_zz_no_alloc.py) stays last.  A run
+# that stops at the first failure has then checked the path before anything
+# built on it.
+_ORDER = ("test_capi_load", "test_gpu_parity", "test_gpu_batch", "test_gpu_autograd", "test_cxx_boundary")
+
+
+def pytest_collection_modifyitems(session, config, items):
+    def rank(item):
+        mod = item.module.__name__.rsplit(".", 1)[-1]
+        if mod.startswith("test_zz"):
+            return len(_ORDER) + 1
+        return _ORDER.index(mod) if mod in _ORDER else len(_ORDER)
+    items.sort(key=rank)   # stable: keeps the order within a file

@@ -2,7 +2,7 @@
 """Extract the reference's golden vectors for the 2b/3b path into JSON fixtures.
 
 Reads the reference's own Catch2 unit tests and timing fixtures (from a
-reference checkout, default /root/reference) and writes ``tests/golden/*.json``:
+reference checkout: --ref or MBX_REFERENCE) and writes ``tests/golden/*.json``:
 
 * evaluator / dispatch goldens: ``unittest-energy2b.cpp`` (h2o-h2o :48-97,
   ch4-ch4 :314-360, ch4-h2o :361-427), ``unittest-energy3b.cpp`` (h2o x3
@@ -54,7 +54,7 @@ reference checkout, default /root/reference) and writes ``tests/golden/*.json``:
   (``timing/*/output:5-6``) and configuration (``mbx.json``).
 
 Every array is copied verbatim (as numbers); nothing else of the reference is
-kept.  Run: ``python tests/golden/make_golden.py [--ref /root/reference]``.
+kept.  Run: ``python tests/golden/make_golden.py [--ref DIR] (or MBX_REFERENCE)``.
 """
 import argparse
 import json
@@ -271,7 +271,7 @@ def extract_systems(ref):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("MBX_REFERENCE"), required=not os.environ.get("MBX_REFERENCE"))
     a = ap.parse_args()
     extract_blocks(a.ref)
     extract_systems(a.ref)

@@ -7,16 +7,20 @@ liquid box within 1e-6 relative, each term within 2e-6, forces within
 1e-3 kcal/mol/A; gas-phase n-mers, away from the basis' reference point,
 within 1e-5.  n-mer lists must be identical after canonicalisation.
 """
+import os
+import sys
+
 import numpy as np
 import pytest
 
 import mbx_oracle as mo
-from conftest import golden
+from conftest import GOLDEN, golden
 from mbx_b200 import system as msys, workloads
 from mbx_b200.specs import ALKALI, HALIDES, SPECS
 from mbx_b200.tables import load_fit
 
 pytestmark = pytest.mark.gpu
+sys.path.insert(0, GOLDEN)
 
 E_REL = 1e-10
 G_ABS = 1e-8
@@ -397,39 +401,56 @@ def test_ghost_monomers():
         np.testing.assert_allclose(g.GetRealGrads(), o.real_grads(), atol=G_ABS)
 
 
-def test_water_2048_full_size():
-    """The bench workload at full size: lists equal to the oracle's, energies to the reference."""
+def ref_fixture(name):
+    """The reference's own results on a seeded workload (tests/golden/ref_<name>.npz,
+    written by tests/golden/make_ref_fixtures.py from the compiled reference)."""
+    from make_ref_fixtures import WORKLOADS, xyz_hash
+    make_fn, c2, c3 = WORKLOADS[name]
+    ids, xyz, box = make_fn()
+    d = np.load(os.path.join(GOLDEN, "ref_%s.npz" % name))
+    assert str(d["xyz_sha256"]) == xyz_hash(xyz), "workload %s no longer matches its fixture" % name
+    return ids, xyz, box, c2, c3, d
+
+
+@pytest.mark.parametrize("name", ["water_256", "water_2048", "methane_water"])
+def test_fp64_vs_reference(name):
+    """The FP64 path against the reference's own TwoBodyEnergy(true) /
+    ThreeBodyEnergy(true) (bblock/system.cpp:2403-2423, 2727-2745): energies
+    within 1e-10 relative, gradients within 1e-8 kcal/mol/A, virials, and the
+    n-mer lists identical to the reference's (same length, same canonical
+    hash).  2048 waters is the bench workload at full size."""
+    from make_ref_fixtures import list_hash
+    ids, xyz, box, c2, c3, d = ref_fixture(name)
+    g = msys.from_arrays(ids, xyz, box, c2, c3)
+    for nb, cut in ((2, c2), (3, c3)):
+        e = g.TwoBodyEnergy(True) if nb == 2 else g.ThreeBodyEnergy(True)
+        gr = np.asarray(g.GetRealGrads())
+        vr = np.asarray(g.GetVirial())
+        er = float(d["e%d" % nb])
+        assert rel(e, er) < E_REL, (nb, e, er)
+        np.testing.assert_allclose(gr, d["g%d" % nb], rtol=0, atol=G_ABS)
+        np.testing.assert_allclose(vr, d["v%d" % nb], rtol=1e-10, atol=1e-7)
+        nm = canon(g.GetPairList(nb, cut))
+        assert len(nm) == int(d["n%d" % nb]) and list_hash(nm) == str(d["l%d_sha256" % nb]), nb
+
+
+def test_water_2048_lists_vs_restatement():
+    """The full-size lists also equal the oracle restatement's, n-mer by n-mer."""
     ids, xyz, box = workloads.water_2048(0)
     g = msys.from_arrays(ids, xyz, box, 9.0, 7.0)
     o = mo.OracleSystem(ids, xyz, box, 9.0, 7.0)
     for nb in (2, 3):
         cut = 9.0 if nb == 2 else 7.0
         assert np.array_equal(canon(g.GetPairList(nb, cut)), o.top.nmers_to_input(o.nmers(nb)))
-    e2 = g.TwoBodyEnergy(True)
-    g2 = g.GetRealGrads()
-    e3 = g.ThreeBodyEnergy(True)
-    g3 = g.GetRealGrads()
-    if mo.RefSystem.available():
-        r = mo.RefSystem(ids, xyz, box, 9.0, 7.0)
-        r2 = r.energy(2)
-        rg2 = r.real_grads()
-        r3 = r.energy(3)
-        rg3 = r.real_grads()
-    else:
-        r2 = o.energy(2)
-        rg2 = o.real_grads()
-        r3 = o.energy(3)
-        rg3 = o.real_grads()
-    assert rel(e2, r2) < E_REL and rel(e3, r3) < E_REL
-    np.testing.assert_allclose(g2, rg2, atol=G_ABS)
-    np.testing.assert_allclose(g3, rg3, atol=G_ABS)
 
 
 def test_water_2048_mixed():
-    ids, xyz, box = workloads.water_2048(0)
-    o = mo.RefSystem(ids, xyz, box, 9.0, 7.0) if mo.RefSystem.available() else mo.OracleSystem(ids, xyz, box, 9.0, 7.0)
-    r2, r3 = o.energy(2), o.energy(3)
-    m = msys.from_arrays(ids, xyz, box, 9.0, 7.0, precision="mixed")
+    """The mixed path (MB-pol 3b in the paired FP32 kernel) on the bench
+    workload against the reference: each term within 2e-6 of itself, the
+    2b+3b total within 1e-6."""
+    ids, xyz, box, c2, c3, d = ref_fixture("water_2048")
+    r2, r3 = float(d["e2"]), float(d["e3"])
+    m = msys.from_arrays(ids, xyz, box, c2, c3, precision="mixed")
     e2 = m.TwoBodyEnergy(True)
     e3 = m.ThreeBodyEnergy(True)
     assert rel(e2, r2) < MIXED_REL_TERM and rel(e3, r3) < MIXED_REL_TERM

@@ -10,7 +10,7 @@ import pytest
 from mbx_b200.codegen import mbnrg_spec as ms
 from mbx_b200.specs import SPECS
 
-REF = "/root/reference"
+REF = os.environ.get("MBX_REFERENCE", "")
 needs_ref = pytest.mark.skipif(not os.path.isdir(os.path.join(REF, "src")), reason="reference sources absent")
 
 

@@ -1,4 +1,7 @@
 """The oracle restatement against the reference's own golden vectors (CPU)."""
+import os
+import sys
+
 import numpy as np
 import pytest
 
@@ -288,3 +291,24 @@ def test_helium_dilute_vs_reference():
     e_o, e_r = o.energy(2), r.energy(2)
     assert abs(e_o - e_r) < 1e-10 * abs(e_r)
     np.testing.assert_allclose(o.real_grads(), r.real_grads(), rtol=0, atol=1e-8)
+
+
+@pytest.mark.parametrize("name", ["water_256", "water_2048", "methane_water"])
+def test_reference_fixtures_match_the_reference(name):
+    """The committed reference fixtures (tests/golden/ref_*.npz) are what the
+    compiled reference computes now, on the workload the recipe makes now."""
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    from make_ref_fixtures import WORKLOADS, list_hash, xyz_hash
+    if not mo.RefSystem.available():
+        pytest.fail("reference library not built here (python oracle/build_ref.py)")
+    make_fn, c2, c3 = WORKLOADS[name]
+    ids, xyz, box = make_fn()
+    d = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref_%s.npz" % name))
+    assert str(d["xyz_sha256"]) == xyz_hash(xyz)
+    r = mo.RefSystem(ids, xyz, box, c2, c3)
+    for nb, cut in ((2, c2), (3, c3)):
+        # the reference's OpenMP reduction order may vary between runs
+        assert abs(r.energy(nb) - float(d["e%d" % nb])) <= 1e-12 * abs(float(d["e%d" % nb]))
+        np.testing.assert_allclose(r.real_grads(), d["g%d" % nb], rtol=0, atol=1e-10)
+        nm = r.pair_list(nb, cut)
+        assert len(nm) == int(d["n%d" % nb]) and list_hash(nm) == str(d["l%d_sha256" % nb])
