@@ -315,6 +315,9 @@ def main():
     from mbx_b200.tables import load_fit  # noqa: F401
 
     torch.cuda.set_device(local)
+    # a stream of our own: the library's kernels and the bench's CUDA events
+    # on the same (non-default) stream
+    torch.cuda.set_stream(torch.cuda.Stream(local))
     dist = None
     if world > 1:
         import datetime

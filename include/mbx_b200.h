@@ -114,8 +114,16 @@ int mbx_evaluate_dcoef(mbx_ctx* ctx, const char* evaluator, long n, const double
 int mbx_poly(mbx_ctx* ctx, const char* evaluator, long nd, const double* x, double* g, double* e, int flags);
 
 /* Replace the linear coefficients of an evaluator (ncoef doubles; NULL
- * restores the fitted ones).  Coefficients live in device constant memory and
- * are shared by every context on the device. */
+ * restores the fitted ones).  Coefficients are per device, not per context:
+ * they live in the kernels' constant memory and in one global-memory copy
+ * for the table-driven kernels, shared by every context on the device, and
+ * an alias evaluator shares its target's.  The call takes a process-wide
+ * lock and waits until the device is idle before writing, so work in flight
+ * on other streams finishes with the old coefficients and later work uses
+ * the new ones; two models that need different coefficients for the same
+ * evaluator at the same time need two devices (or must take turns).  The
+ * first context created on a device loads the fitted coefficients; later
+ * contexts keep whatever is set. */
 int mbx_set_coefficients(mbx_ctx* ctx, const char* evaluator, const double* a, int flags);
 int mbx_evaluator_info(const char* evaluator, int* nbody, int* nreal, int* nvars, int* ncoef);
 
@@ -184,9 +192,12 @@ int mbx_set_knobs(mbx_ctx* ctx, int nbody, const int* in);
  * real-time loops, fixed memory pools, plugins that may not grow the
  * process's device memory).  Same evaluator calling convention as
  * mbx_evaluate, straight-line evaluators only ("mbpol2b", "mbpol3b",
- * "ch4h2o2b", "ch4h2o3b"), coefficients as last set on the device; every
- * pointer is device memory owned by the caller; runs on `stream` on the
- * current device:
+ * "ch4h2o2b", "ch4h2o3b"), with the coefficients last set on the device by
+ * mbx_set_coefficients -- or, where no context and no mbx_set_coefficients
+ * call has set them on this device yet, the models' fitted coefficients,
+ * which the first call copies into the kernels' constant memory itself (a
+ * copy, no allocation); every pointer is device memory owned by the caller;
+ * runs on `stream` on the current device:
  *   xyz[n][nreal*3] in, grad (+=, NULL for energy only) and e_per (n
  *   switched energies, may be NULL) out, result[7] out (overwritten):
  *   energy, then virial xx xy xz yy yz zz.
@@ -194,7 +205,8 @@ int mbx_set_knobs(mbx_ctx* ctx, int nbody, const int* in);
  * call to call).  Scratch lives in one static device array shared by all
  * calls: n must not exceed MBX_NOALLOC_MAX_NMERS (MBX_EINVAL otherwise);
  * calls that overlap on the GPU race on it.  The first call on a device
- * looks up the array's device address; make that call before any stream
+ * looks up the array's device address (and may load the fitted
+ * coefficients, waiting for the device); make that call before any stream
  * capture. */
 #define MBX_NOALLOC_MAX_NMERS 262144
 int mbx_evaluate_noalloc(const char* evaluator, long n, const double* xyz, double* grad, double* e_per,

@@ -136,6 +136,19 @@ class Context:
             raise MBXError(code, "mbx_create failed (no CUDA device?)")
         self.h = h
         self.device = device
+        self.stream = stream or 0   # 0: a stream of the context's own
+
+    def _order(self, dev_ptrs):
+        """Device arrays from torch: when the library runs on another stream
+        than torch's current one, torch's work on them (allocation, zeroing)
+        must be complete before the library's kernels start."""
+        if not dev_ptrs:
+            return
+        import torch
+        cur = torch.cuda.current_stream(self.device)
+        mine = self.stream if self.stream != 1 else 0   # 1: cudaStreamLegacy, torch's default stream
+        if self.stream in (0, None) or mine != cur.cuda_stream:
+            cur.synchronize()
 
     def close(self):
         if getattr(self, "h", None):
@@ -176,6 +189,7 @@ class Context:
     def energy(self, nbody, xyz, grad=None, virial=None, use_ghost=False, mixed=False, grads=True):
         """Get2B/Get3B on site coordinates xyz (numpy or CUDA tensor, wrapped in place)."""
         px, dx = _ptr(xyz)
+        self._order(dx)
         pg, dg = _ptr(grad)
         pv, _ = _ptr(virial)
         flags = (MBX_DEVICE_PTRS if dx else 0) | (MBX_MIXED if mixed else 0) | (0 if grads else MBX_NO_GRADS)
@@ -190,6 +204,7 @@ class Context:
     def energy_2b3b(self, xyz, grad=None, virial=None, use_ghost=False, mixed=False, grads=True):
         """Get2B and Get3B side by side on the GPU; returns (E2B, E3B)."""
         px, dx = _ptr(xyz)
+        self._order(dx)
         pg, dg = _ptr(grad)
         pv, _ = _ptr(virial)
         flags = (MBX_DEVICE_PTRS if dx else 0) | (MBX_MIXED if mixed else 0) | (0 if grads else MBX_NO_GRADS)
@@ -226,6 +241,7 @@ class Context:
     def evaluate(self, name, xyz, grad=None, virial=None, e_per=None, mixed=False, grads=True):
         nb, nreal, nv, nc = evaluator_info(name)
         px, dx = _ptr(xyz)
+        self._order(dx)
         n = (xyz.shape[0] if xyz.ndim > 1 else xyz.size // (3 * nreal))
         pg, _ = _ptr(grad)
         pv, _ = _ptr(virial)
@@ -239,6 +255,7 @@ class Context:
     def evaluate_dcoef(self, name, xyz, w=None, out=None):
         nb, nreal, nv, nc = evaluator_info(name)
         px, dx = _ptr(xyz)
+        self._order(dx)
         n = (xyz.shape[0] if xyz.ndim > 1 else xyz.size // (3 * nreal))
         if out is None:
             out = np.zeros(nc)
@@ -252,6 +269,7 @@ class Context:
         """Generated polynomial, variable-major x[nvars][nd] (poly_*::eval(nd, a, x, t, g))."""
         nb, nreal, nv, nc = evaluator_info(name)
         px, dx = _ptr(x)
+        self._order(dx)
         nd = x.shape[-1] if x.ndim > 1 else x.size // nv
         if e is None:
             e = np.zeros(nd) if not dx else None
@@ -282,6 +300,7 @@ class Context:
         """One term of every configuration (device xyz, device grad +=).
         Returns energies[nconf] (and virials[nconf, 9] when asked)."""
         px, dx = _ptr(xyz)
+        self._order(dx)
         pg, dg = _ptr(grad)
         if not dx or (grad is not None and not dg):
             raise TypeError("batches take CUDA tensors")
@@ -298,6 +317,7 @@ class Context:
         """Both terms of every configuration, side by side on the GPU.
         Returns (e2[nconf], e3[nconf]) (and virials[nconf, 9], summed)."""
         px, dx = _ptr(xyz)
+        self._order(dx)
         pg, dg = _ptr(grad)
         if not dx or (grad is not None and not dg):
             raise TypeError("batches take CUDA tensors")
@@ -315,6 +335,7 @@ class Context:
         """Autotunes the builder's launch shapes of a term on the current batch
         (or system); returns (knobs dict, best ms)."""
         px, dx = _ptr(xyz)
+        self._order(dx)
         pg, _ = _ptr(grad)
         if not dx:
             raise TypeError("tuning takes CUDA tensors")

@@ -206,8 +206,43 @@ def parts_for(nterms, nvars=36):
 # (constant); MB-pol 2b is faster from the constant bank (0.18 vs 0.25 ms).
 SMEM_COEF_TYPES = {"mbpol3b"}
 
+# Types whose tries are generated in the coset form (codegen/coset.py): a
+# polynomial R of ~1/24 of the terms, run once per permutation of a
+# transversal of the symmetry group, so that its code stays in the
+# instruction cache; the kernels' coefficients are scaled on the host.
+# COSET_PIECE_TERMS: terms of R per separately compiled piece.
+# Measured on the 2048-water trimers (L2 flushed between calls, the code
+# prefetch launch in use): MB-pol 3b FP64 1.73 ms in the coset form against
+# 1.36 ms for the full trie, paired FP32 0.96 against 0.91 ms -- with the
+# prefetch the full trie's code is L2-resident already, and the coset form's
+# 10% more arithmetic and per-permutation loads then cost more than its
+# smaller code saves.  No type uses it; the form is kept for polynomials
+# whose trie does not fit in L2.
+COSET_TYPES = set()
+COSET_PIECE_TERMS = 400
 
-def emit_split(trie, nvars, name, out, nparts, arrays, body, ret="double"):
+
+_COSET = {}
+
+
+def coset_of(name, shifted_basis=False):
+    """(coset form, R table) of an evaluator's polynomial, or of its FP32
+    (shifted) basis."""
+    key = (name, shifted_basis)
+    if key not in _COSET:
+        from mbx_b200.codegen.coset import coset_form, CosetTable
+        spec = SPECS[name]
+        if shifted_basis:
+            from mbx_b200.codegen.shift import ShiftedTable
+            sp = shifted_pip(name)
+            cf = coset_form(spec, ShiftedTable(sp, name), sp.group)
+        else:
+            cf = coset_form(spec, load_pip(name))
+        _COSET[key] = (cf, CosetTable(cf, spec.nvars, name))
+    return _COSET[key]
+
+
+def emit_split(trie, nvars, name, out, nparts, arrays, body, ret="double", perms=None):
     """Emits name_partK as __noinline__ functions over strided pointers to the
     caller's arrays, and the wrappers that call them in turn.
 
@@ -219,34 +254,63 @@ def emit_split(trie, nvars, name, out, nparts, arrays, body, ret="double"):
     lockstep kernels keep x and g there: shared memory instead of the
     thread's stack for the values every piece loads and stores).  body(w,
     subtrees) writes the evaluation of the subtrees into the local arrays and
-    into E."""
+    into E.
+
+    perms (coset form, codegen/coset.py): the trie is R and every piece runs
+    its subtrees once per permutation p_t, reading variable v of the caller's
+    arrays at column p_t[v] and adding its gradient there; the permutations
+    sit in a constant-memory table, and a piece's code is reused |T| times in
+    a row while it is in the instruction cache."""
     import re
     w = out.append
     zero = {"float": "0.0f", "double": "0.0", "f2_t": "0ull"}
     e0 = "make_double2(0.0, 0.0)" if ret == "double2" else "0.0"
     pieces = split_terms(trie, nparts) if SPLIT == "terms" else partition(trie, nparts)
     params = ", ".join("%s%s* __restrict__ %sm" % ("const " if role == "in" else "", ct, a) for a, ct, role in arrays)
+    if perms is not None:
+        # the table lives in constant memory and is copied to shared memory
+        # by the lock / piece entry points; the pieces read it with a
+        # non-removable load at every use, so that the 36 column offsets are
+        # not kept in registers across the piece (they would spill)
+        w("// coset form: %d permutations of the %d variables (x_local[v] = x[perm[t][v]])" % (len(perms), nvars))
+        w("static __constant__ int %s_perm[%d] = {%s};" %
+          (name, len(perms) * nvars, ", ".join(str(v) for p in perms for v in p)))
+        w("static __shared__ int %s_sperm[%d];" % (name, len(perms) * nvars))
+        w("__device__ __forceinline__ void %s_load_perm() {" % name)
+        w("    for (int i = threadIdx.x; i < %d; i += blockDim.x) %s_sperm[i] = %s_perm[i];" %
+          (len(perms) * nvars, name, name))
+        w("    __syncthreads();")
+        w("}")
     for i, sub in enumerate(pieces):
         text = []
         body(text.append, sub)
         code = "\n".join(text)
         w("template <class Coef, int S>")
         w("__device__ __noinline__ %s %s_part%d(const Coef& coef, %s) {" % (ret, name, i, params))
+        w("    %s E = %s;" % (ret, e0))
+        pad = "    "
+        if perms is not None:
+            w("#pragma unroll 1")
+            w("    for (int t = 0; t < %d; ++t) {" % len(perms))
+            w("    const int* o = %s_sperm + t * %d;" % (name, nvars))
         for a, ct, role in arrays:
             used = sorted({int(v) for v in re.findall(r"\b%s\[(\d+)\]" % a, code)})
             w("    %s %s[%d];" % (ct, a, nvars))
             for v in used:
-                w("    %s[%d] = %s;" % (a, v, ("%sm[%d * S]" % (a, v)) if role == "in" else zero[ct]))
-        w("    %s E = %s;" % (ret, e0))
+                col = ("lds_pinned(o + %d)" % v) if perms is not None else str(v)
+                w("    %s[%d] = %s;" % (a, v, ("%sm[%s * S]" % (a, col)) if role == "in" else zero[ct]))
         w(code)
         for a, ct, role in arrays:
             if role == "acc":
                 used = sorted({int(v) for v in re.findall(r"\b%s\[(\d+)\]" % a, code)})
                 for v in used:
+                    col = ("lds_pinned(o + %d)" % v) if perms is not None else str(v)
                     if ct == "f2_t":
-                        w("    %sm[%d * S] = f2_add(%sm[%d * S], %s[%d]);" % (a, v, a, v, a, v))
+                        w("    %sm[%s * S] = f2_add(%sm[%s * S], %s[%d]);" % (a, col, a, col, a, v))
                     else:
-                        w("    %sm[%d * S] += %s[%d];" % (a, v, a, v))
+                        w("    %sm[%s * S] += %s[%d];" % (a, col, a, v))
+        if perms is not None:
+            w("    }")
         w("    return E;")
         w("}")
 
@@ -273,6 +337,8 @@ def emit_split(trie, nvars, name, out, nparts, arrays, body, ret="double"):
     # instruction fetches
     w("template <int S, class Coef>")
     w("__device__ __forceinline__ %s %s_lock(const Coef& coef, %s) {" % (ret, name, params))
+    if perms is not None:
+        w("    %s_load_perm();" % name)
     w("    %s E = %s;" % (ret, e0))
     calls(True, "Coef, S", ", ".join("%sm" % a for a, _, _ in arrays))
     w("    return E;")
@@ -283,6 +349,8 @@ def emit_split(trie, nvars, name, out, nparts, arrays, body, ret="double"):
     w("static constexpr int %s_NPIECES = %d;" % (name, len(pieces)))
     w("template <int S, class Coef>")
     w("__device__ __forceinline__ %s %s_piece(int k, const Coef& coef, %s) {" % (ret, name, params))
+    if perms is not None:
+        w("    %s_load_perm();" % name)
     w("    switch (k) {")
     args = ", ".join("%sm" % a for a, _, _ in arrays)
     for i in range(len(pieces)):
@@ -292,7 +360,7 @@ def emit_split(trie, nvars, name, out, nparts, arrays, body, ret="double"):
     w("}")
 
 
-def emit_pip(trie, nvars, name, out, nparts=1):
+def emit_pip(trie, nvars, name, out, nparts=1, perms=None):
     """FP64 value + gradient (multivariate Horner trie, reverse mode)."""
     out.append("// %s: polynomial and reverse-mode gradient (multivariate Horner trie)" % name)
 
@@ -337,10 +405,10 @@ def emit_pip(trie, nvars, name, out, nparts=1):
                 c = coef_expr(ch["coef"])
                 w("    E = fma(%s, x[%d], E); g[%d] += %s;" % (c, var, var, c))
 
-    emit_split(trie, nvars, name, out, nparts, [("x", "double", "in"), ("g", "double", "acc")], body)
+    emit_split(trie, nvars, name, out, nparts, [("x", "double", "in"), ("g", "double", "acc")], body, perms=perms)
 
 
-def emit_pip_f32x2(trie, nvars, name, out, nparts=1):
+def emit_pip_f32x2(trie, nvars, name, out, nparts=1, perms=None):
     """FP32 value + gradient over the trie for two n-mers at once (the low and
     high halves of every f2_t, paired FP32 instructions): monomials,
     coefficients and leaf sums in FP32; the top-level products are added to
@@ -391,7 +459,8 @@ def emit_pip_f32x2(trie, nvars, name, out, nparts=1):
                 w("      E.x = fma((double)f2_lo(c), (double)f2_lo(x[%d]), E.x); "
                   "E.y = fma((double)f2_hi(c), (double)f2_hi(x[%d]), E.y); }" % (var, var))
 
-    emit_split(trie, nvars, name, out, nparts, [("x", "f2_t", "in"), ("g", "f2_t", "acc")], body, ret="double2")
+    emit_split(trie, nvars, name, out, nparts, [("x", "f2_t", "in"), ("g", "f2_t", "acc")], body, ret="double2",
+               perms=perms)
 
 
 def shifted_pip(name):
@@ -415,7 +484,7 @@ def shifted_pip(name):
 _SHIFTED = {}
 
 
-def emit_pip_energy(trie, nvars, name, out, nparts=1):
+def emit_pip_energy(trie, nvars, name, out, nparts=1, perms=None):
     """FP64 value only: plain Horner over the trie."""
     def body(w, subtrees):
         def node(n, var, depth):
@@ -436,7 +505,7 @@ def emit_pip_energy(trie, nvars, name, out, nparts=1):
             else:
                 w("    E = fma(%s, x[%d], E);" % (coef_expr(ch["coef"]), var))
 
-    emit_split(trie, nvars, name, out, nparts, [("x", "double", "in")], body)
+    emit_split(trie, nvars, name, out, nparts, [("x", "double", "in")], body, perms=perms)
 
 
 def emit_vars(spec, out):
@@ -587,21 +656,36 @@ def generate(name):
     write_if_changed(os.path.join(OUT, name + ".cuh"), "\n".join(out) + "\n")
     if straight:
         nparts = parts_for(table.nterms, spec.nvars)
+        perms = None
+        if name in COSET_TYPES:
+            cf, ctab = coset_of(name)
+            trie = Trie(ctab)
+            perms = cf.perms
+            nparts = max(1, (ctab.nterms + COSET_PIECE_TERMS - 1) // COSET_PIECE_TERMS)
         for suffix, emitter, arg in (("pip", emit_pip, trie), ("pip_e", emit_pip_energy, trie)):
             body = head + ["#pragma once", '#include "%s.cuh"' % name]
-            emitter(arg, nv, "%s_%s" % (name, suffix), body, nparts)
+            if perms is not None:
+                body.append("// coset form: %d terms of R x %d permutations (%d terms in the table)" %
+                            (ctab.nterms, len(perms), table.nterms))
+            emitter(arg, nv, "%s_%s" % (name, suffix), body, nparts, perms=perms)
             write_if_changed(os.path.join(OUT, "%s_%s.cuh" % (name, suffix)), "\n".join(body) + "\n")
         if name in SHIFT_TYPES:
             from mbx_b200.codegen.shift import ShiftedTable
             sp = shifted_pip(name)
-            strie = Trie(ShiftedTable(sp, name))
             body = head + ["#pragma once", '#include "%s.cuh"' % name,
                            "// %d monomials of the %s basis, %d coefficient orbits" %
                            (len(sp.monos), SHIFT_TYPES[name], sp.norb)]
-            # ~400 terms per piece: larger pieces spill in the paired form
-            # (2048-water trimers, x/g in shared memory: 0.833/0.818/0.910 ms
-            # at 330/400/480 terms per piece)
-            emit_pip_f32x2(strie, nv, "%s_pip_s32" % name, body, max(1, (len(sp.monos) + 399) // 400))
+            if name in COSET_TYPES:
+                cfs, ctab_s = coset_of(name, shifted_basis=True)
+                body.append("// coset form: %d terms of R x %d permutations" % (ctab_s.nterms, len(cfs.perms)))
+                emit_pip_f32x2(Trie(ctab_s), nv, "%s_pip_s32" % name, body,
+                               max(1, (ctab_s.nterms + COSET_PIECE_TERMS - 1) // COSET_PIECE_TERMS), perms=cfs.perms)
+            else:
+                # ~400 terms per piece: larger pieces spill in the paired form
+                # (2048-water trimers, x/g in shared memory: 0.833/0.818/0.910 ms
+                # at 330/400/480 terms per piece)
+                strie = Trie(ShiftedTable(sp, name))
+                emit_pip_f32x2(strie, nv, "%s_pip_s32" % name, body, max(1, (len(sp.monos) + 399) // 400))
             write_if_changed(os.path.join(OUT, "%s_pip_s32.cuh" % name), "\n".join(body) + "\n")
     return os.path.join(OUT, name + ".cuh"), leaves, inner
 
@@ -621,11 +705,9 @@ struct %(name)s_CC {
     __device__ __forceinline__ float f(int k) const { return cf_%(name)s[k]; }
 };
 
+%(scale_decl)s
 int mbx_set_coef_%(name)s_%(v)s(const double* a, int from_device, cudaStream_t s) {
-    cudaError_t e = cudaMemcpyToSymbolAsync(c_%(name)s, a, sizeof(double) * %(ncoef)d, 0,
-                                            from_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s);
-    if (e != cudaSuccess) return (int)e;
-    // FP32 copy for the mixed-precision leaf sums (a warp-uniform FFMA operand)
+    cudaError_t e = cudaSuccess;
     std::vector<double> h(%(ncoef)d);
     if (from_device) {
         e = cudaMemcpyAsync(h.data(), a, sizeof(double) * %(ncoef)d, cudaMemcpyDeviceToHost, s);
@@ -634,6 +716,9 @@ int mbx_set_coef_%(name)s_%(v)s(const double* a, int from_device, cudaStream_t s
     } else {
         for (int k = 0; k < %(ncoef)d; ++k) h[k] = a[k];
     }
+%(scale_apply)s    e = cudaMemcpyToSymbolAsync(c_%(name)s, h.data(), sizeof(double) * %(ncoef)d, 0, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return (int)e;
+    // FP32 copy for the mixed-precision leaf sums (a warp-uniform FFMA operand)
     std::vector<float> f(%(ncoef)d);
     for (int k = 0; k < %(ncoef)d; ++k) f[k] = (float)h[k];
     e = cudaMemcpyToSymbolAsync(cf_%(name)s, f.data(), sizeof(float) * %(ncoef)d, 0, cudaMemcpyHostToDevice, s);
@@ -778,6 +863,8 @@ static const int sF_k_%(name)s[%(nnz)d] = {%(ks)s};
 static const double sF_f_%(name)s[%(nnz)d] = {%(fs)s};
 static const int sF0_k_%(name)s[%(nnz0)d] = {%(k0)s};
 static const double sF0_f_%(name)s[%(nnz0)d] = {%(f0)s};
+// per-orbit factor of the kernel's coefficients (1, or the coset-form scale)
+static const double sscale_%(name)s[%(norb)d] = {%(sscale)s};
 
 int mbx_set_coef_%(name)s_s(const double* a, int from_device, cudaStream_t s) {
     std::vector<double> h(%(ncoef)d);
@@ -793,7 +880,7 @@ int mbx_set_coef_%(name)s_s(const double* a, int from_device, cudaStream_t s) {
     for (int j = 0; j < %(norb)d; ++j) {
         double acc = 0.0;
         for (int q = sF_row_%(name)s[j]; q < sF_row_%(name)s[j + 1]; ++q) acc += sF_f_%(name)s[q] * h[sF_k_%(name)s[q]];
-        const float f = (float)acc;
+        const float f = (float)(acc * sscale_%(name)s[j]);
         unsigned int u;
         memcpy(&u, &f, sizeof(u));
         b[j] = (unsigned long long)u | ((unsigned long long)u << 32);
@@ -861,6 +948,8 @@ def write_shift_tu(name, path):
          "rows": ",".join(map(str, rows)), "ks": ",".join(map(str, ks)),
          "fs": ",".join(repr(float(f)) for f in fs),
          "k0": ",".join(map(str, k0)) if k0 else "0",
+         "sscale": ",".join(repr(float(x)) for x in (coset_of(name, True)[0].scale if name in COSET_TYPES
+                                                       else np.ones(sp.norb))),
          "f0": ",".join(repr(float(sp.const_F[k])) for k in k0) if k0 else "0.0"}
     write_tu(path, SHIFT_TU % d)
 
@@ -891,7 +980,13 @@ def write_kernels_cu(name):
         else:
             what, body = VARIANTS[v]
             d = {"name": name, "NAME": name.upper(), "ncoef": spec.ncoef, "v": v, "what": what,
-                 "include": '#include "%s_%s.cuh"\n' % (name, inc[v])}
+                 "include": '#include "%s_%s.cuh"\n' % (name, inc[v]), "scale_decl": "", "scale_apply": ""}
+            if name in COSET_TYPES:
+                cf, _ = coset_of(name)
+                d["scale_decl"] = ("// coset form: the kernels take a_k * scale_k (codegen/coset.py)\n"
+                                   "static const double coset_scale_%s[%d] = {%s};\n" %
+                                   (name, spec.ncoef, ", ".join(repr(float(x)) for x in cf.scale)))
+                d["scale_apply"] = "    for (int k = 0; k < %d; ++k) h[k] *= coset_scale_%s[k];\n" % (spec.ncoef, name)
             write_tu(path, (TU_HEAD + body) % d)
         paths.append(path)
     return paths

@@ -38,6 +38,15 @@ __device__ __forceinline__ f2_t f2_pack(float lo, float hi) {
 __device__ __forceinline__ float f2_lo(f2_t a) { return __uint_as_float((unsigned)a); }
 __device__ __forceinline__ float f2_hi(f2_t a) { return __uint_as_float((unsigned)(a >> 32)); }
 
+// A 32-bit shared-memory load the compiler may neither remove nor merge with
+// another (the coset-form pieces re-read their column offsets at each use
+// instead of holding 36 of them in registers).
+__device__ __forceinline__ int lds_pinned(const int* p) {
+    int v;
+    asm volatile("ld.shared.u32 %0, [%1];" : "=r"(v) : "r"((unsigned)__cvta_generic_to_shared(p)));
+    return v;
+}
+
 #define MBX_LP_GAMMA_IN (-9.721486914088159e-02)
 #define MBX_LP_GAMMA_OUT (9.859272078406150e-02)
 

@@ -3,39 +3,59 @@
 ``nmer_energies(name, xyz, coef)`` returns the switched energy of every n-mer
 (``xyz``: [n, nreal*3] float64 CUDA tensor, monomers in evaluator order,
 already imaged; ``coef``: [ncoef] float64 CUDA tensor of linear coefficients).
-Its backward pass gives
 
-* d/dxyz: the analytic reverse pass (the per-n-mer gradients the forward
-  kernel produced), scaled by the upstream gradient;
-* d/dcoef: the adjoint with respect to the linear coefficients,
+* forward: the energy-only kernel (no gradient is formed);
+* backward, d/dxyz: the reverse pass as a kernel of its own -- the gradient
+  kernel recomputes variables and monomials from the coordinates (nothing
+  is stored by the forward pass) and its per-n-mer gradients are scaled by
+  the upstream gradient;
+* backward, d/dcoef: the adjoint with respect to the linear coefficients,
   sum_n w_n dE_n/da, computed by a kernel that recomputes the monomials from
   the coordinates (they are never stored).
 
+With ``virial=True`` the call also returns the virial of the n-mers
+(-sum r (x) dE/dr, 9 components, the evaluators' convention; computed by the
+gradient kernel, not differentiable).
+
+The backward pass is itself not differentiable: a second derivative (for
+instance d loss(forces) / d coef, which a force-matching refit needs) raises
+an error instead of returning a wrong value.
+
 ``system_energy(system, nbody, sites)`` is the same for a whole System term
-(Get2B/Get3B) with respect to the site coordinates.
+(Get2B/Get3B) with respect to the site coordinates: energy-only forward, the
+gradient recomputed by the gradient kernels in backward.
 
 Everything runs on the library's CUDA kernels; the tensors are passed by
-device pointer on the current stream.
+device pointer on torch's current stream.
 """
 import numpy as np
 import torch
+from torch.autograd.function import once_differentiable
 
 from . import capi
 
 _contexts = {}
 
 
+# cudaStreamLegacy: the handle that names the legacy default stream (a null
+# stream handle would make mbx_create give the context a stream of its own,
+# unordered with torch's work on the default stream)
+_LEGACY_STREAM = 1
+
+
 def context(device=None):
+    """The library context of the current device and torch's current stream
+    (kernels are ordered with torch's work on that stream)."""
     dev = torch.cuda.current_device() if device is None else device
     key = (dev, torch.cuda.current_stream(dev).cuda_stream)
     if key not in _contexts:
-        _contexts[key] = capi.Context(dev, key[1])
+        _contexts[key] = capi.Context(dev, key[1] or _LEGACY_STREAM)
     return _contexts[key]
 
 
 class _NmerEnergies(torch.autograd.Function):
     @staticmethod
-    def forward(fctx, xyz, coef, name, mixed):
+    def forward(fctx, xyz, coef, name, mixed, want_virial):
         if not (xyz.is_cuda and coef.is_cuda):
             raise TypeError("xyz and coef must be CUDA tensors")
         xyz = xyz.contiguous()
@@ -44,28 +64,43 @@ class _NmerEnergies(torch.autograd.Function):
         c.set_coefficients(name, coef)
         n = xyz.shape[0]
         e = torch.empty(n, dtype=torch.float64, device=xyz.device)
-        g = torch.zeros_like(xyz)
-        c.evaluate(name, xyz, g, None, e, mixed=mixed, grads=True)
-        fctx.save_for_backward(xyz, coef, g)
+        vir = np.zeros(9)
+        if want_virial:
+            g = torch.zeros_like(xyz)
+            c.evaluate(name, xyz, g, vir, e, mixed=mixed, grads=True)
+        else:
+            c.evaluate(name, xyz, None, None, e, mixed=mixed, grads=False)
+        fctx.save_for_backward(xyz, coef)
         fctx.name = name
-        return e
+        fctx.mixed = mixed
+        v = torch.tensor(vir, dtype=torch.float64, device=xyz.device)
+        fctx.mark_non_differentiable(v)
+        return e, v
 
     @staticmethod
-    def backward(fctx, ge):
-        xyz, coef, g = fctx.saved_tensors
+    @once_differentiable
+    def backward(fctx, ge, gv):
+        xyz, coef = fctx.saved_tensors
         ge = ge.contiguous()
-        dxyz = g * ge[:, None] if fctx.needs_input_grad[0] else None
-        dcoef = None
+        c = context(xyz.device.index)
+        c.set_coefficients(fctx.name, coef)
+        dxyz = dcoef = None
+        if fctx.needs_input_grad[0]:
+            # reverse pass: the gradient kernel, everything recomputed from xyz
+            g = torch.zeros_like(xyz)
+            c.evaluate(fctx.name, xyz, g, None, None, mixed=fctx.mixed, grads=True)
+            dxyz = g * ge[:, None]
         if fctx.needs_input_grad[1]:
-            c = context(xyz.device.index)
-            c.set_coefficients(fctx.name, coef)
             dcoef = torch.zeros_like(coef)
             c.evaluate_dcoef(fctx.name, xyz, ge, dcoef)
-        return dxyz, dcoef, None, None
+        return dxyz, dcoef, None, None, None
 
 
-def nmer_energies(name, xyz, coef, mixed=False):
-    return _NmerEnergies.apply(xyz, coef, name, mixed)
+def nmer_energies(name, xyz, coef, mixed=False, virial=False):
+    """Per-n-mer energies (and, with virial=True, the virial as a second
+    result)."""
+    e, v = _NmerEnergies.apply(xyz, coef, name, mixed, virial)
+    return (e, v) if virial else e
 
 
 def fitted_coefficients(name, device="cuda"):
@@ -75,22 +110,36 @@ def fitted_coefficients(name, device="cuda"):
 
 class _SystemEnergy(torch.autograd.Function):
     @staticmethod
-    def forward(fctx, sites, system, nbody):
+    def forward(fctx, sites, system, nbody, want_virial):
         sites = sites.contiguous()
-        g = torch.zeros_like(sites)
         vir = np.zeros(9)
-        e = system._ctx.energy(nbody, sites, g, vir, mixed=system.precision == "mixed")
-        fctx.save_for_backward(g)
-        return torch.tensor(e, dtype=torch.float64, device=sites.device)
+        mixed = system.precision == "mixed"
+        if want_virial:
+            g = torch.zeros_like(sites)
+            e = system._ctx.energy(nbody, sites, g, vir, mixed=mixed)
+        else:
+            e = system._ctx.energy(nbody, sites, None, None, mixed=mixed, grads=False)
+        fctx.save_for_backward(sites)
+        fctx.system = system
+        fctx.nbody = nbody
+        v = torch.tensor(vir, dtype=torch.float64, device=sites.device)
+        fctx.mark_non_differentiable(v)
+        return torch.tensor(e, dtype=torch.float64, device=sites.device), v
 
     @staticmethod
-    def backward(fctx, ge):
-        (g,) = fctx.saved_tensors
-        return g * ge, None, None
+    @once_differentiable
+    def backward(fctx, ge, gv):
+        (sites,) = fctx.saved_tensors
+        s = fctx.system
+        g = torch.zeros_like(sites)
+        s._ctx.energy(fctx.nbody, sites, g, np.zeros(9), mixed=s.precision == "mixed")
+        return g * ge, None, None, None
 
 
-def system_energy(system, nbody, sites):
-    """Get2B/Get3B of an initialised mbx_b200.system.System on device site coordinates.
+def system_energy(system, nbody, sites, virial=False):
+    """Get2B/Get3B of an initialised mbx_b200.system.System on device site
+    coordinates (and, with virial=True, the term's virial as a second result).
 
     Note: like System::SetPBC, the call wraps the coordinates in place."""
-    return _SystemEnergy.apply(sites, system, nbody)
+    e, v = _SystemEnergy.apply(sites, system, nbody, virial)
+    return (e, v) if virial else e

@@ -34,6 +34,7 @@ from mbx_b200.topology import Topology
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "_build", "libmbx_oracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libmbx_ref.so")
+REF_GPU_LIB = os.path.join(HERE, "_ref", "libmbx_ref_gpu.so")
 
 
 def build(force=False):
@@ -361,15 +362,16 @@ class RefSystem:
     """bblock::System from the reference library (oracle/_ref), via ref_harness.cpp."""
 
     _L = None
+    LIB = REF_LIB
 
     @classmethod
     def available(cls):
-        return os.path.exists(REF_LIB)
+        return os.path.exists(cls.LIB)
 
     @classmethod
     def L(cls):
         if cls._L is None:
-            L = ctypes.CDLL(REF_LIB)
+            L = ctypes.CDLL(cls.LIB)
             dp = ctypes.POINTER(ctypes.c_double)
             L.mbxref_new.argtypes = [ctypes.c_char_p, dp, ctypes.c_char_p]
             L.mbxref_new.restype = ctypes.c_void_p
@@ -455,3 +457,12 @@ class RefSystem:
     @classmethod
     def set_threads(cls, n):
         cls.L().mbxref_set_threads(n)
+
+
+class RefGpuSystem(RefSystem):
+    """The reference's bblock::System with Get2B/Get3B forwarded to the CUDA
+    library over its C ABI (oracle/build_ref_gpu.py, oracle/ref_gpu_glue.cpp):
+    the C++ caller of the drop-in boundary."""
+
+    _L = None
+    LIB = REF_GPU_LIB

@@ -135,7 +135,14 @@ void* mbxref_new(const char* ids, const double* xyz, const char* json) {
     }
 }
 
-void mbxref_free(void* h) { delete static_cast<bblock::System*>(h); }
+// Defined only in the build whose System forwards its 2b/3b terms to the
+// GPU library (ref_gpu_glue.cpp): releases that System's library context.
+void mbxref_gpu_release(const void* sys) __attribute__((weak));
+
+void mbxref_free(void* h) {
+    if (mbxref_gpu_release) mbxref_gpu_release(h);
+    delete static_cast<bblock::System*>(h);
+}
 
 int mbxref_set_real_xyz(void* h, const double* xyz) {
     try {

@@ -21,6 +21,17 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200); runs the CUDA path")
 
 
+def pytest_sessionstart(session):
+    """The compiled reference (oracle/_ref) is the oracle of many CPU tests:
+    build it on demand where its sources are present and it is not built yet
+    (a few minutes, once)."""
+    import subprocess
+    ref = os.environ.get("MBX_REFERENCE")
+    lib = os.path.join(ROOT, "oracle", "_ref", "libmbx_ref.so")
+    if ref and os.path.isdir(os.path.join(ref, "src")) and not os.path.exists(lib):
+        subprocess.call([sys.executable, os.path.join(ROOT, "oracle", "build_ref.py"), "--ref", ref])
+
+
 def golden(name):
     with open(os.path.join(GOLDEN, name + ".json")) as f:
         return json.load(f)

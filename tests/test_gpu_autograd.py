@@ -92,3 +92,64 @@ def test_mixed_refit_forward():
     assert abs(float(e32b.sum() - e64b.sum())) / float(e64b.abs().sum()) < 1e-5
     assert abs(float(e64b.sum()) - 1.01 * float(e64.sum())) < 1e-9 * float(e64.abs().sum())
     torch_ops.context().set_coefficients("mbpol3b", None)
+
+
+@pytest.mark.parametrize("name,maker", [("mbpol2b", workloads.gas_dimers), ("mbpol3b", workloads.gas_trimers)])
+def test_gradcheck(name, maker):
+    """torch.autograd.gradcheck (central differences) of the FP64 n-mer
+    energies with respect to coordinates and coefficients, 16 n-mers."""
+    from mbx_b200 import torch_ops
+    xyz = torch.tensor(maker(16, seed=3), device="cuda", requires_grad=True)
+    coef = torch_ops.fitted_coefficients(name).requires_grad_(True)
+    assert torch.autograd.gradcheck(lambda x, a: torch_ops.nmer_energies(name, x, a), (xyz, coef),
+                                    eps=1e-6, atol=1e-5, rtol=1e-4)
+    torch_ops.context().set_coefficients(name, None)
+
+
+def test_second_derivative_is_refused():
+    """A force-matching refit needs d loss(F) / d a, a second derivative: the
+    backward pass is not differentiable and says so."""
+    from mbx_b200 import torch_ops
+    xyz = torch.tensor(workloads.gas_dimers(8, seed=2), device="cuda", requires_grad=True)
+    coef = torch_ops.fitted_coefficients("mbpol2b").requires_grad_(True)
+    e = torch_ops.nmer_energies("mbpol2b", xyz, coef)
+    (f,) = torch.autograd.grad(e.sum(), xyz, create_graph=True)
+    with pytest.raises(RuntimeError, match="once_differentiable|differentiate"):
+        f.pow(2).sum().backward()
+
+
+@pytest.mark.parametrize("name,maker", [("mbpol2b", workloads.gas_dimers), ("mbpol3b", workloads.gas_trimers)])
+def test_virial_and_energy_only_forward(name, maker):
+    """virial=True gives the evaluators' virial (the oracle's), the plain
+    forward the same energies as the gradient path."""
+    from mbx_b200 import torch_ops
+    xyz_np = maker(100, seed=6)
+    xyz = torch.tensor(xyz_np, device="cuda")
+    coef = torch_ops.fitted_coefficients(name)
+    e, v = torch_ops.nmer_energies(name, xyz, coef, virial=True)
+    e_only = torch_ops.nmer_energies(name, xyz, coef)
+    eo, _, vo, epo = mo.holder_eval(name, xyz_np, per_nmer=True)
+    np.testing.assert_allclose(e.cpu().numpy(), epo, rtol=0, atol=1e-8)
+    np.testing.assert_allclose(e_only.cpu().numpy(), e.cpu().numpy(), rtol=0, atol=1e-8)
+    np.testing.assert_allclose(v.cpu().numpy(), np.asarray(vo).reshape(-1), rtol=1e-9, atol=1e-8)
+    assert not v.requires_grad
+
+
+def test_system_energy_backward_recomputes():
+    """system_energy: energy-only forward, the gradient kernels in backward;
+    equal to the System's own gradient, virial as the second result."""
+    from mbx_b200 import system as msys, torch_ops
+    ids, xyz, box = workloads.water_256(0)
+    s = msys.from_arrays(ids, xyz, box, 9.0, 7.0)
+    e_ref = s.ThreeBodyEnergy(True)
+    g_ref = np.asarray(s.GetRealGrads())
+    v_ref = np.asarray(s.GetVirial())
+    s2 = msys.from_arrays(ids, xyz, box, 9.0, 7.0)
+    sites = torch.tensor(s2.sites, device="cuda", requires_grad=True)
+    e, v = torch_ops.system_energy(s2, 3, sites, virial=True)
+    e.backward()
+    assert abs(float(e) - e_ref) < 1e-10 * abs(e_ref)
+    g = sites.grad.detach().cpu().numpy()
+    s2.grad = g
+    np.testing.assert_allclose(s2.GetRealGrads(), g_ref, rtol=0, atol=1e-8)
+    np.testing.assert_allclose(v.cpu().numpy(), v_ref, rtol=1e-10, atol=1e-8)

@@ -167,7 +167,7 @@ def test_table_vs_reference_program(name):
     variables with the type's fitted coefficients (CH4-CH4: value only, the
     reference ships no gradient program for it)."""
     if not mo.RefSystem.available():
-        pytest.skip("reference library not built here")
+        pytest.fail("reference library not built here (python oracle/build_ref.py)")
     nv = SPECS[name].nvars
     a = load_fit(name)
     rng = np.random.default_rng(11)
@@ -192,7 +192,7 @@ def test_ion_water_vs_reference(ion, nb):
     Cl-, whose like-ion pairs have a polynomial in the reference that is not
     on this path; three of the others)."""
     if not mo.RefSystem.available():
-        pytest.skip("reference library not built here")
+        pytest.fail("reference library not built here (python oracle/build_ref.py)")
     ids, xyz, box = workloads.ion_water_box([ion] * (1 if ion in ("na+", "cl-") else 3), seed=1)
     o = mo.OracleSystem(ids, xyz, box, 9.0, 7.0)
     r = mo.RefSystem(ids, xyz, box, 9.0, 7.0)
@@ -210,7 +210,7 @@ def test_solution_vs_reference(ions, nb):
     evaluator here, ion-ion and atom-atom included): the oracle against the
     compiled reference."""
     if not mo.RefSystem.available():
-        pytest.skip("reference library not built here")
+        pytest.fail("reference library not built here (python oracle/build_ref.py)")
     ids, xyz, box = workloads.ion_water_box(list(ions), seed=4)
     o = mo.OracleSystem(ids, xyz, box, 9.0, 7.0)
     r = mo.RefSystem(ids, xyz, box, 9.0, 7.0)
@@ -260,7 +260,7 @@ def test_molecule_box_vs_reference(case):
     with Cs+, MB-pbe water, CO2 3b) and methane in salt water: the oracle
     against the compiled reference."""
     if not mo.RefSystem.available():
-        pytest.skip("reference library not built here")
+        pytest.fail("reference library not built here (python oracle/build_ref.py)")
     ids, nbs = MOLECULE_BOXES[case][:2]
     L = MOLECULE_BOXES[case][2] if len(MOLECULE_BOXES[case]) > 2 else 19.72
     e_rtol, g_atol = MOLECULE_BOXES[case][3] if len(MOLECULE_BOXES[case]) > 3 else (1e-10, 1e-8)
@@ -284,7 +284,7 @@ def test_helium_dilute_vs_reference():
     relative and neither is closer to the exact value, so parity is pinned
     where x < 1."""
     if not mo.RefSystem.available():
-        pytest.skip("reference library not built here")
+        pytest.fail("reference library not built here (python oracle/build_ref.py)")
     ids, xyz, box = workloads.dilute_box("he", 10, seed=1)
     o = mo.OracleSystem(ids, xyz, box, 9.0, 7.0)
     r = mo.RefSystem(ids, xyz, box, 9.0, 7.0)
@@ -312,3 +312,43 @@ def test_reference_fixtures_match_the_reference(name):
         np.testing.assert_allclose(r.real_grads(), d["g%d" % nb], rtol=0, atol=1e-10)
         nm = r.pair_list(nb, cut)
         assert len(nm) == int(d["n%d" % nb]) and list_hash(nm) == str(d["l%d_sha256" % nb])
+
+
+def _ref_root():
+    r = os.environ.get("MBX_REFERENCE", "")
+    if not os.path.isdir(os.path.join(r, "src")):
+        pytest.skip("reference sources absent (MBX_REFERENCE)")
+    return r
+
+
+def test_fit_files_match_reference_sources():
+    """Every committed fitted-coefficient file (mbx_b200/data/*.fit), which the
+    oracle and the kernels both read, is the coefficient array of the
+    reference's source it names (parsed afresh from the reference's text)."""
+    from mbx_b200.codegen import pip_extract as px
+    ref = _ref_root()
+    for name in sorted(px.FITS):
+        vals = px.extract_fit(ref, name, SPECS[name].ncoef)
+        np.testing.assert_array_equal(load_fit(name), np.array(vals), err_msg=name)
+
+
+@pytest.mark.parametrize("name", list(REF_PROGRAM))
+def test_table_vs_reference_program_random_coefficients(name):
+    """The term tables, which the oracle and the kernels both read, against the
+    compiled reference programs with random coefficients (not the fitted ones
+    the other checks use): agreement at random points pins every term."""
+    if not mo.RefSystem.available():
+        pytest.fail("reference library not built here (python oracle/build_ref.py)")
+    nv = SPECS[name].nvars
+    rng = np.random.default_rng(17)
+    a = rng.normal(size=SPECS[name].ncoef)
+    for _ in range(3):
+        x = rng.uniform(0.05, 1.2, size=nv)
+        if name != "ch4ch42b":
+            e_r, g_r = mo.RefSystem.poly(REF_PROGRAM[name], a, x)
+            e_o, g_o = mo.pip_eval(name, a, x)
+            np.testing.assert_allclose(g_o, g_r, rtol=1e-9, atol=1e-9 * max(1.0, np.abs(g_r).max()))
+        else:
+            e_r = mo.RefSystem.poly(REF_PROGRAM[name], a, x, want_grad=False)
+            e_o = mo.pip_eval(name, a, x, want_grad=False)
+        assert abs(e_o - e_r) < 1e-9 * max(1.0, abs(e_r))
