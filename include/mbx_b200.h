@@ -69,14 +69,36 @@ int mbx_set_topology(mbx_ctx* ctx, int nmon, const char* const* ids, const int* 
 int mbx_set_config(mbx_ctx* ctx, double cutoff2b, double cutoff3b, const double* box, int n2,
                    const char* const* ignore2b, int n3, const char* const* ignore3b);
 
-/* Get2B (nbody 2) / Get3B (nbody 3).  xyz: 3*numsites doubles, wrapped in
- * place as System::SetPBC does (FixMonomerCoordinates, sys_tools.cpp:257).
- * *energy receives the term; grad (3*numsites, may be NULL) and virial (9,
- * may be NULL) are ACCUMULATED (+=) like grad_/virial_ in the reference.
- * flags: MBX_DEVICE_PTRS, MBX_MIXED, MBX_NO_GRADS.  use_ghost as in
- * TwoBodyEnergy(do_grads, use_ghost). */
+/* Get1B (nbody 1, bblock/system.cpp:2269) / Get2B (nbody 2,
+ * system.cpp:2425) / Get3B (nbody 3, system.cpp:2769).  xyz: 3*numsites
+ * doubles, wrapped in place as System::SetPBC does (FixMonomerCoordinates,
+ * sys_tools.cpp:257).  *energy receives the term; grad (3*numsites, may be
+ * NULL) and virial (9, may be NULL) are ACCUMULATED (+=) like grad_/virial_
+ * in the reference.  flags: MBX_DEVICE_PTRS, MBX_MIXED, MBX_NO_GRADS.
+ * use_ghost as in TwoBodyEnergy(do_grads, use_ghost) (ignored by nbody 1).
+ * The 1-body term covers the local waters (MB-pol: the Partridge-Schwenke
+ * surface, ps::pot_nasa, potential/1b/ps.cpp:346); a topology with a
+ * monomer type whose 1-body term the reference computes on the CPU only
+ * here (ch4, co2*, nh3*, h2, n2o5, mbpbe) returns MBX_ENOTSUP for nbody 1
+ * unless that type is in the 1-body ignore list. */
 int mbx_energy(mbx_ctx* ctx, int nbody, double* xyz, int use_ghost, double* energy, double* grad, double* virial,
                int flags);
+
+/* GPU-resident callers (i-PI, LAMMPS: coordinates kept in the caller's
+ * own atom order on the device).  mbx_set_real_order gives the site of
+ * every real atom of the input order (the inverse of the topology's
+ * OrderMonomers, numat entries); mbx_energy_real then takes the real
+ * coordinates in input order (3*numat, not modified: the context wraps its
+ * own site copy, as System::SetRealXyz + SetPBC do, system.cpp:830-846) and
+ * accumulates the gradient in input order (+=, GetRealGrads), for nbody 1, 2
+ * or 3 with the flags of mbx_energy. */
+int mbx_set_real_order(mbx_ctx* ctx, int numat, const int* site_of_atom);
+int mbx_energy_real(mbx_ctx* ctx, int nbody, const double* xyz_real, int use_ghost, double* energy,
+                    double* grad_real, double* virial, int flags);
+
+/* Monomer types skipped by the 1-body term (System ignore_1b_poly_,
+ * system.cpp:2293-2296); replaces the previous list. */
+int mbx_set_ignore_1b(mbx_ctx* ctx, int n, const char* const* ids);
 
 /* Listed n-mers of the last mbx_energy call for nbody (dimers within
  * cutoff2b, trimers by the AddClusters rule within cutoff3b) and the number

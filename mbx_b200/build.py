@@ -33,7 +33,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
          "-I" + os.path.join(ROOT, "include"), "-I" + CSRC]
-HAND = ("mbx_capi.cu", "nmer_build.cu", "peaks.cu", "noalloc.cu", "table_kernels.cu")
+HAND = ("mbx_capi.cu", "nmer_build.cu", "peaks.cu", "noalloc.cu", "table_kernels.cu", "onebody.cu")
 HEADERS = ("holder_common.cuh", "holder_kernel.cuh", "term_table.cuh", "launch_cache.cuh", "device_state.h")
 
 
@@ -50,7 +50,8 @@ def deps(src):
             common.append(os.path.join(GEN, "%s_%s.cuh" % (name, variant)))
     else:
         common += [os.path.join(CSRC, "nmer_build.h"), os.path.join(ROOT, "include", "mbx_b200.h"),
-                   os.path.join(GEN, "registry.inc"), os.path.join(GEN, "terms_index.inc")]
+                   os.path.join(GEN, "registry.inc"), os.path.join(GEN, "terms_index.inc"),
+                   os.path.join(GEN, "ps1b.inc")]
     return [src] + [d for d in common if os.path.exists(d)]
 
 

@@ -58,6 +58,10 @@ def lib():
     L.mbx_last_error.restype = ctypes.c_char_p
     L.mbx_version.restype = ctypes.c_char_p
     L.mbx_set_topology.argtypes = [vp, ctypes.c_int, cpp, ip, ip, ip, ctypes.c_int]
+    L.mbx_set_ignore_1b.argtypes = [vp, ctypes.c_int, cpp]
+    L.mbx_set_real_order.argtypes = [vp, ctypes.c_int, ip]
+    L.mbx_energy_real.argtypes = [vp, ctypes.c_int, dp, ctypes.c_int, ctypes.POINTER(ctypes.c_double), dp, dp,
+                                  ctypes.c_int]
     L.mbx_set_config.argtypes = [vp, ctypes.c_double, ctypes.c_double, dp, ctypes.c_int, cpp, ctypes.c_int, cpp]
     L.mbx_energy.argtypes = [vp, ctypes.c_int, dp, ctypes.c_int, ctypes.POINTER(ctypes.c_double), dp, dp,
                              ctypes.c_int]
@@ -90,7 +94,7 @@ EXPORTED = ("mbx_create", "mbx_destroy", "mbx_last_error", "mbx_version", "mbx_s
             "mbx_energy", "mbx_last_counts", "mbx_nmers", "mbx_evaluate", "mbx_evaluate_dcoef", "mbx_poly",
             "mbx_set_coefficients", "mbx_evaluator_info", "mbx_last_timing", "mbx_fma_peaks", "mbx_set_batch",
             "mbx_batch_energy", "mbx_tune", "mbx_get_knobs", "mbx_set_knobs", "mbx_energy_2b3b",
-            "mbx_batch_energy_2b3b")
+            "mbx_batch_energy_2b3b", "mbx_set_ignore_1b", "mbx_set_real_order", "mbx_energy_real")
 
 KNOBS = ("nb_warps", "nb_unroll", "tri_threads", "dim_threads")
 
@@ -186,8 +190,31 @@ class Context:
         self._check(lib().mbx_set_config(self.h, cutoff2b, cutoff3b, None if b is None else b.ctypes.data,
                                          len(ignore_2b), a2, len(ignore_3b), a3))
 
+    def set_real_order(self, site_of_atom):
+        a = np.ascontiguousarray(site_of_atom, np.int32)
+        self._check(lib().mbx_set_real_order(self.h, len(a), a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))))
+
+    def energy_real(self, nbody, xyz_real, grad_real=None, virial=None, use_ghost=False, mixed=False, grads=True):
+        """A term on real coordinates in input order (numpy or CUDA tensor,
+        not modified); the gradient is accumulated in input order."""
+        px, dx = _ptr(xyz_real)
+        self._order(dx)
+        pg, dg = _ptr(grad_real)
+        pv, _ = _ptr(virial)
+        if grad_real is not None and bool(dg) != bool(dx):
+            raise TypeError("xyz_real and grad_real must both be host or both be device arrays")
+        flags = (MBX_DEVICE_PTRS if dx else 0) | (MBX_MIXED if mixed else 0) | \
+                (0 if (grads and grad_real is not None) else MBX_NO_GRADS)
+        e = ctypes.c_double()
+        self._check(lib().mbx_energy_real(self.h, nbody, px, int(use_ghost), ctypes.byref(e), pg, pv, flags))
+        return e.value
+
+    def set_ignore_1b(self, ids=()):
+        a = (ctypes.c_char_p * max(len(ids), 1))(*[i.encode() for i in ids])
+        self._check(lib().mbx_set_ignore_1b(self.h, len(ids), a))
+
     def energy(self, nbody, xyz, grad=None, virial=None, use_ghost=False, mixed=False, grads=True):
-        """Get2B/Get3B on site coordinates xyz (numpy or CUDA tensor, wrapped in place)."""
+        """Get1B/Get2B/Get3B on site coordinates xyz (numpy or CUDA tensor, wrapped in place)."""
         px, dx = _ptr(xyz)
         self._order(dx)
         pg, dg = _ptr(grad)

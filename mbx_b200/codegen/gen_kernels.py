@@ -1084,6 +1084,43 @@ def write_term_tables():
              "        \".previous\\n\");\n" % (bin_path, len(blob)))
 
 
+def write_ps1b():
+    """The Partridge-Schwenke polynomial sums of the water 1-body term
+    (mbx_b200/data/ps1b.json, extracted by codegen/onebody_extract.py) as
+    straight-line code: for every term j of ps::pot_nasa's loop
+    (potential/1b/ps.cpp:455-476) the four sums with the term's indices and
+    coefficient as literals, every product and sum rounded on its own in the
+    reference's operand order."""
+    import json
+    d = json.load(open(os.path.join(PKG, "data", "ps1b.json")))
+    L = ["// Generated by mbx_b200/codegen/gen_kernels.py from mbx_b200/data/ps1b.json -- do not edit.",
+         "#pragma once",
+         "#define PS1B_REOH %s" % lit(d["reoh"]), "#define PS1B_B1 %s" % lit(d["b1"]),
+         "#define PS1B_ROH %s" % lit(d["roh"]), "#define PS1B_ALPHAOH %s" % lit(d["alphaoh"]),
+         "#define PS1B_PHH2 %s" % lit(d["phh2"]), "#define PS1B_DEOH %s" % lit(d["deoh"]),
+         "#define PS1B_PHH1 %s" % lit(d["phh1"]), "#define PS1B_COSTHE %s" % lit(d["costhe"]),
+         "#define PS1B_OFFSET %s" % lit(d["offset"]), "#define PS1B_CM1_KCALMOL %s" % lit(d["cm1_kcalmol"]),
+         "#define PS1B_C0 %s" % lit(d["c5z"][0]),
+         "__device__ __forceinline__ void ps1b_sums(const double (&f0)[16], const double (&f1)[16], "
+         "const double (&f2)[16], double& s0, double& s1, double& s2, double& s3) {"]
+    M, A = "__dmul_rn", "__dadd_rn"
+    for j in range(1, len(d["c5z"])):
+        I, J, K = d["idx1"][j], d["idx2"][j], d["idx3"][j]
+        c = lit(d["c5z"][j])
+        sym = "%s(%s(f0[%d], f1[%d]), %s(f0[%d], f1[%d]))" % (A, M, I, J, M, J, I)
+        L.append("    { const double sym = %s;" % sym)
+        L.append("      s0 = %s(s0, %s(%s(%s, sym), f2[%d]));" % (A, M, M, c, K))
+        t1 = "%s(%s(%s(%s, f0[%d]), f1[%d]), %s(%s(%s, f0[%d]), f1[%d]))" % (
+            A, M, M, lit(float(I - 1)), I - 1, J, M, M, lit(float(J - 1)), J - 1, I)
+        L.append("      s1 = %s(s1, %s(%s(%s, %s), f2[%d]));" % (A, M, M, c, t1, K))
+        t2 = "%s(%s(%s(%s, f0[%d]), f1[%d]), %s(%s(%s, f0[%d]), f1[%d]))" % (
+            A, M, M, lit(float(J - 1)), I, J - 1, M, M, lit(float(I - 1)), J, I - 1)
+        L.append("      s2 = %s(s2, %s(%s(%s, %s), f2[%d]));" % (A, M, M, c, t2, K))
+        L.append("      s3 = %s(s3, %s(%s(%s(%s, sym), %s), f2[%d])); }" % (A, M, M, M, c, lit(float(K - 1)), K - 1))
+    L.append("}")
+    write_tu(os.path.join(OUT, "ps1b.inc"), "\n".join(L) + "\n")
+
+
 def write_registry():
     """Host tables: evaluator descriptions and default coefficients."""
     from mbx_b200.tables import load_fit
@@ -1153,8 +1190,9 @@ def main(argv=None, quiet=False):
     os.makedirs(OUT, exist_ok=True)
     write_registry()
     write_term_tables()
+    write_ps1b()
     from mbx_b200.specs import KERNEL_ALIASES
-    keep = {"registry.inc", "terms_index.inc", "terms.bin", "terms_blob.cpp"}
+    keep = {"registry.inc", "terms_index.inc", "terms.bin", "terms_blob.cpp", "ps1b.inc"}
     for n in args.names:
         if n in KERNEL_ALIASES:
             continue

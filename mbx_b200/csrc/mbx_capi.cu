@@ -24,6 +24,16 @@
 #include "holder_kernel.cuh"
 #include "nmer_build.h"
 
+// The 1-body term of water (onebody.cu).
+struct OneBodyArgs {
+    const double* xyz;
+    const int* first;
+    long n;
+    double* grad;
+    double* out;
+};
+int mbx_launch_ps1b(const OneBodyArgs& A, int sms, cudaStream_t s);
+
 // Generic table-driven polynomial over caller-supplied variables
 // (table_kernels.cu).
 int mbx_launch_poly_table(long nd, int nvars, const double* x, double* g, double* e, const int4* terms,
@@ -249,6 +259,15 @@ struct mbx_ctx {
     double cutoff[4] = {0, 0, 9.0, 7.0};  // indexed by nbody
     BoxParams bp{};
     std::vector<std::vector<std::string>> ignore[4];
+    std::vector<std::string> ignore1b;   // monomer types without a 1-body term (ignore_1b_poly_)
+    // input (real-atom) order of the caller: site of every real atom (mbx_set_real_order)
+    int numat = 0;
+    DevBuf<int> d_real2site;
+    DevBuf<double> xreal, greal, gsite;
+    // 1-body term: first sites of the local waters, built for topology generation w1b_gen
+    DevBuf<int> d_w1b;
+    long n_w1b = 0;
+    unsigned long w1b_gen = ~0ul;
 
     // per-term dispatch
     int nbucket[4] = {0, 0, 0, 0};
@@ -1015,15 +1034,166 @@ static int unstage_term_io(mbx_ctx* c, double* xyz, double* grad, int flags, dou
     return MBX_OK;
 }
 
+// Monomer types whose 1-body term the reference computes
+// (e1b::get_1b_energy, potential/1b/energy1b.cpp:53-86); the ones other than
+// water have no GPU evaluator here, and a topology holding them (and not
+// ignoring them) gets MBX_ENOTSUP for the 1-body term rather than a silent
+// zero.  Every other type has no 1-body term (0, as in the reference).
+static const char* const k1bCpuOnly[] = {"ch4", "co2_archive", "nh3", "nh3pbe0d3bj", "co2", "co2cm5100", "co2cm595",
+                                         "co2cm590", "co2cm5875", "co2cm585", "co2cm580", "h2", "n2o5", "mbpbe"};
+
+// System::Get1B (bblock/system.cpp:2269-2401) on device coordinates X
+// (wrapped): the local waters through the Partridge-Schwenke kernel.
+static int onebody_term(mbx_ctx* c, double* X, double* G, double* energy, double* virial, int* kernels) {
+    auto ignored = [&](const std::string& t) {
+        return std::find(c->ignore1b.begin(), c->ignore1b.end(), t) != c->ignore1b.end();
+    };
+    for (int t = 0; t < c->ntypes; ++t)
+        for (const char* id : k1bCpuOnly)
+            if (c->type_names[t] == id && !ignored(id))
+                return fail(c, MBX_ENOTSUP, std::string("no GPU 1-body term for monomer type ") + id);
+    if (c->w1b_gen != c->gen) {
+        std::vector<int> first;
+        for (int m = 0; m < c->nmon; ++m)
+            if (c->type_names[c->h_type[m]] == "h2o" && c->h_local[m] && !ignored("h2o")) first.push_back(c->h_first[m]);
+        c->n_w1b = (long)first.size();
+        CUCHK(c, c->d_w1b.ensure(std::max<size_t>(first.size(), 1)));
+        if (!first.empty())
+            CUCHK(c, cudaMemcpyAsync(c->d_w1b.p, first.data(), first.size() * sizeof(int), cudaMemcpyHostToDevice,
+                                     c->stream));
+        CUCHK(c, cudaStreamSynchronize(c->stream));
+        c->w1b_gen = c->gen;
+    }
+    CUCHK(c, cudaEventRecord(c->ev[1], c->stream));
+    CUCHK(c, cudaMemsetAsync(c->out.p, 0, 8 * sizeof(double), c->stream));
+    OneBodyArgs A{X, c->d_w1b.p, c->n_w1b, G, c->out.p};
+    RCHK(c, mbx_launch_ps1b(A, c->sm_count, c->stream));
+    if (c->n_w1b > 0) ++*kernels;
+    CUCHK(c, cudaEventRecord(c->ev[2], c->stream));
+    CUCHK(c, cudaMemcpyAsync(c->h_out, c->out.p, 7 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CUCHK(c, cudaStreamSynchronize(c->stream));
+    *energy = c->h_out[0];
+    if (virial) {
+        virial[0] += c->h_out[1];
+        virial[1] += c->h_out[2];
+        virial[2] += c->h_out[3];
+        virial[4] += c->h_out[4];
+        virial[5] += c->h_out[5];
+        virial[8] += c->h_out[6];
+        virial[3] = virial[1];
+        virial[6] = virial[2];
+        virial[7] = virial[5];
+    }
+    c->last_ms_build = 0;
+    cudaEventElapsedTime(&c->last_ms_eval, c->ev[1], c->ev[2]);
+    c->last_kernels = *kernels;
+    c->last_listed[1] = c->last_evaluated[1] = c->n_w1b;
+    return MBX_OK;
+}
+
+// Input order <-> site order (System::SetRealXyz, bblock/system.cpp:830-846,
+// and GetRealGrads): site of real atom i = real2site[i].
+__global__ void k_gather_real(const double* __restrict__ xr, const int* __restrict__ real2site, int numat,
+                              double* __restrict__ sites) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < numat; i += gridDim.x * blockDim.x) {
+        const int s = real2site[i];
+        sites[3 * s] = xr[3 * i];
+        sites[3 * s + 1] = xr[3 * i + 1];
+        sites[3 * s + 2] = xr[3 * i + 2];
+    }
+}
+
+__global__ void k_scatter_real(const double* __restrict__ gsite, const int* __restrict__ real2site, int numat,
+                               double* __restrict__ greal) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < numat; i += gridDim.x * blockDim.x) {
+        const int s = real2site[i];
+        greal[3 * i] += gsite[3 * s];
+        greal[3 * i + 1] += gsite[3 * s + 1];
+        greal[3 * i + 2] += gsite[3 * s + 2];
+    }
+}
+
+extern "C" int mbx_set_real_order(mbx_ctx* c, int numat, const int* real2site) {
+    if (!c || numat <= 0 || !real2site) return fail(c, MBX_EINVAL, "bad arguments");
+    if (!c->nmon) return fail(c, MBX_EINVAL, "set the topology first");
+    for (int i = 0; i < numat; ++i)
+        if (real2site[i] < 0 || real2site[i] >= c->numsites) return fail(c, MBX_EINVAL, "site index out of range");
+    CUCHK(c, cudaSetDevice(c->device));
+    CUCHK(c, c->d_real2site.ensure(numat));
+    CUCHK(c, cudaMemcpyAsync(c->d_real2site.p, real2site, numat * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    CUCHK(c, cudaStreamSynchronize(c->stream));
+    c->numat = numat;
+    return MBX_OK;
+}
+
+extern "C" int mbx_energy_real(mbx_ctx* c, int nbody, const double* xyz_real, int use_ghost, double* energy,
+                               double* grad_real, double* virial, int flags) {
+    if (!c || nbody < 1 || nbody > 3 || !xyz_real || !energy) return fail(c, MBX_EINVAL, "bad arguments");
+    if (!c->numat) return fail(c, MBX_EINVAL, "no input order (mbx_set_real_order)");
+    CUCHK(c, cudaSetDevice(c->device));
+    const bool dev = (flags & MBX_DEVICE_PTRS) != 0;
+    const bool grads = !(flags & MBX_NO_GRADS) && grad_real;
+    const size_t na3 = 3 * (size_t)c->numat, ns3 = 3 * (size_t)c->numsites;
+    const double* XR = xyz_real;
+    if (!dev) {
+        CUCHK(c, c->xreal.ensure(na3));
+        CUCHK(c, cudaMemcpyAsync(c->xreal.p, xyz_real, na3 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        XR = c->xreal.p;
+    }
+    CUCHK(c, c->xyz.ensure(ns3));
+    const int grid = std::max(1, std::min((c->numat + 255) / 256, c->sm_count * 4));
+    k_gather_real<<<grid, 256, 0, c->stream>>>(XR, c->d_real2site.p, c->numat, c->xyz.p);
+    CUCHK(c, cudaGetLastError());
+    if (grads) {
+        CUCHK(c, c->gsite.ensure(ns3));
+        CUCHK(c, cudaMemsetAsync(c->gsite.p, 0, ns3 * sizeof(double), c->stream));
+    }
+    // the term on the internal (device) site array; mbx_energy wraps it in place
+    int r = mbx_energy(c, nbody, c->xyz.p, use_ghost, energy, grads ? c->gsite.p : nullptr, virial,
+                       flags | MBX_DEVICE_PTRS | (grads ? 0 : MBX_NO_GRADS));
+    if (r) return r;
+    if (!grads) return MBX_OK;
+    double* GR = grad_real;
+    if (!dev) {
+        CUCHK(c, c->greal.ensure(na3));
+        CUCHK(c, cudaMemsetAsync(c->greal.p, 0, na3 * sizeof(double), c->stream));
+        GR = c->greal.p;
+    }
+    k_scatter_real<<<grid, 256, 0, c->stream>>>(c->gsite.p, c->d_real2site.p, c->numat, GR);
+    CUCHK(c, cudaGetLastError());
+    if (!dev) {
+        std::vector<double> h(na3);
+        CUCHK(c, cudaMemcpyAsync(h.data(), GR, na3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CUCHK(c, cudaStreamSynchronize(c->stream));
+        for (size_t i = 0; i < na3; ++i) grad_real[i] += h[i];
+    } else {
+        CUCHK(c, cudaStreamSynchronize(c->stream));
+    }
+    return MBX_OK;
+}
+
+extern "C" int mbx_set_ignore_1b(mbx_ctx* c, int n, const char* const* ids) {
+    if (!c || n < 0 || (n > 0 && !ids)) return fail(c, MBX_EINVAL, "bad arguments");
+    c->ignore1b.clear();
+    for (int i = 0; i < n; ++i) c->ignore1b.push_back(ids[i]);
+    ++c->gen;
+    return MBX_OK;
+}
+
 extern "C" int mbx_energy(mbx_ctx* c, int nbody, double* xyz, int use_ghost, double* energy, double* grad,
                           double* virial, int flags) {
-    if (!c || (nbody != 2 && nbody != 3) || !xyz || !energy) return fail(c, MBX_EINVAL, "bad arguments");
+    if (!c || nbody < 1 || nbody > 3 || !xyz || !energy) return fail(c, MBX_EINVAL, "bad arguments");
     if (!c->nmon) return fail(c, MBX_EINVAL, "System has not been initialized (no topology)");
     CUCHK(c, cudaSetDevice(c->device));
     int kernels = 0;
     double *X, *G;
     int r = stage_term_io(c, xyz, grad, flags, &X, &G, &kernels);
     if (r) return r;
+    if (nbody == 1) {
+        r = onebody_term(c, X, G, energy, virial, &kernels);
+        if (r) return r;
+        return unstage_term_io(c, xyz, grad, flags, X, G);
+    }
     for (int attempt = 0; attempt < 4; ++attempt) {
         r = term_enqueue(c, nbody, use_ghost, X, G, flags, &kernels);
         if (r) return r;
@@ -1123,7 +1293,7 @@ extern "C" int mbx_energy_2b3b(mbx_ctx* c, double* xyz, int use_ghost, double* e
 }
 
 extern "C" int mbx_last_counts(const mbx_ctx* c, int nbody, long* listed, long* evaluated) {
-    if (!c || (nbody != 2 && nbody != 3)) return MBX_EINVAL;
+    if (!c || nbody < 1 || nbody > 3) return MBX_EINVAL;
     if (listed) *listed = c->last_listed[nbody];
     if (evaluated) *evaluated = c->last_evaluated[nbody];
     return MBX_OK;

@@ -35,6 +35,7 @@ class System:
         self.cutoff2b = 100.0   # System::System defaults (bblock/system.cpp:63-133)
         self.cutoff3b = 5.0
         self.box = []
+        self.ignore_1b = []
         self.ignore_2b = []
         self.ignore_3b = []
         self.precision = "fp64"
@@ -72,6 +73,7 @@ class System:
             self._ctx = capi.Context(self.device)
         t = self.top
         self._ctx.set_topology(t.ids, t.first_index, t.tag, t.is_local, t.numsites)
+        self._ctx.set_real_order(t.site_of_input_atom)
         self.initialized = True
         self._push_config()
 
@@ -84,6 +86,7 @@ class System:
         self.box = list(m.get("box", []))
         self.cutoff2b = float(m.get("twobody_cutoff", 100.0))
         self.cutoff3b = float(m.get("threebody_cutoff", 5.0))
+        self.ignore_1b = [str(t) for t in m.get("ignore_1b_poly", [])]
         self.ignore_2b = [list(t) for t in m.get("ignore_2b_poly", [])]
         self.ignore_3b = [list(t) for t in m.get("ignore_3b_poly", [])]
         if not self.initialized:
@@ -111,6 +114,7 @@ class System:
         box = np.asarray(self.box, np.float64) if len(self.box) else None
         try:
             self._ctx.set_config(self.cutoff2b, self.cutoff3b, box, self.ignore_2b, self.ignore_3b)
+            self._ctx.set_ignore_1b(self.ignore_1b)
         except capi.MBXError as e:
             raise CUException(str(e))
 
@@ -130,11 +134,31 @@ class System:
                                        use_ghost=use_ghost, mixed=self.precision == "mixed", grads=do_grads)
         return self.energy
 
+    def OneBodyEnergy(self, do_grads):
+        """System::OneBodyEnergy (bblock/system.cpp:2140): the 1-body term of
+        the local monomers (water: Partridge-Schwenke) on the GPU."""
+        return self._term(1, do_grads, False)
+
     def TwoBodyEnergy(self, do_grads, use_ghost=False):
         return self._term(2, do_grads, use_ghost)
 
     def ThreeBodyEnergy(self, do_grads, use_ghost=False):
         return self._term(3, do_grads, use_ghost)
+
+    def EnergyFromRealXyz(self, nbody, xyz_real, grad_real=None, do_grads=True, use_ghost=False):
+        """The nbody term (1, 2, 3) on real coordinates in input order -- a
+        CUDA tensor for a GPU-resident caller (i-PI, LAMMPS) or a numpy
+        array -- without copying them into the System (SetRealXyz followed
+        by OneBody/TwoBody/ThreeBodyEnergy, with the gradient accumulated
+        into grad_real in input order, GetRealGrads).  The System's own
+        coordinates, gradient and virial are not touched; returns (energy,
+        virial)."""
+        if not self.initialized:
+            raise CUException("System has not been initialized. %dB Energy calculation not possible." % nbody)
+        vir = np.zeros(9)
+        e = self._ctx.energy_real(nbody, xyz_real, grad_real if do_grads else None, vir, use_ghost=use_ghost,
+                                  mixed=self.precision == "mixed", grads=do_grads)
+        return e, vir
 
     def TwoAndThreeBodyEnergy(self, do_grads, use_ghost=False):
         """Both terms in one call (no counterpart in the reference, whose

@@ -30,7 +30,6 @@ device pointer on torch's current stream.
 """
 import numpy as np
 import torch
-from torch.autograd.function import once_differentiable
 
 from . import capi
 
@@ -51,6 +50,16 @@ def context(device=None):
     if key not in _contexts:
         _contexts[key] = capi.Context(dev, key[1] or _LEGACY_STREAM)
     return _contexts[key]
+
+
+def _no_second_derivative():
+    """The backward kernels are not themselves differentiable: a backward
+    pass that builds a graph (create_graph=True, e.g. for d loss(forces) /
+    d coef) is refused here instead of silently dropping the second-order
+    terms."""
+    if torch.is_grad_enabled():
+        raise RuntimeError("mbx_b200: second derivatives of the 2b/3b energies are not supported "
+                           "(the backward pass is a kernel, not a differentiable graph; use create_graph=False)")
 
 
 class _NmerEnergies(torch.autograd.Function):
@@ -78,8 +87,8 @@ class _NmerEnergies(torch.autograd.Function):
         return e, v
 
     @staticmethod
-    @once_differentiable
     def backward(fctx, ge, gv):
+        _no_second_derivative()
         xyz, coef = fctx.saved_tensors
         ge = ge.contiguous()
         c = context(xyz.device.index)
@@ -127,8 +136,8 @@ class _SystemEnergy(torch.autograd.Function):
         return torch.tensor(e, dtype=torch.float64, device=sites.device), v
 
     @staticmethod
-    @once_differentiable
     def backward(fctx, ge, gv):
+        _no_second_derivative()
         (sites,) = fctx.saved_tensors
         s = fctx.system
         g = torch.zeros_like(sites)

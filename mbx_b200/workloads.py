@@ -173,6 +173,14 @@ def beads(xyz, n, sigma=0.05, seed=0):
     return [xyz + rng.normal(0.0, sigma, size=xyz.shape) for _ in range(n)]
 
 
+def water_256_bead(seed=0, sigma=0.05):
+    """One path-integral bead of the 256-water box: every atom displaced by
+    independent Gaussian noise (sigma in A), so that the waters are no longer
+    rigid (the 1-body term sees stretched and bent molecules)."""
+    ids, xyz, box = water_256(seed)
+    return ids, beads(xyz, 1, sigma=sigma, seed=seed + 1)[0], box
+
+
 def water_cluster(n, seed=0, density=0.0334, dmin=2.5):
     rng = np.random.default_rng(seed)
     radius = (3.0 * n / (4.0 * np.pi * density)) ** (1.0 / 3.0)

@@ -162,7 +162,9 @@ int mbxref_num_real_sites(void* h) { return (int)static_cast<bblock::System*>(h)
 int mbxref_energy(void* h, int nbody, int do_grads, double* e) {
     try {
         auto* sys = static_cast<bblock::System*>(h);
-        *e = (nbody == 2) ? sys->TwoBodyEnergy(do_grads != 0) : sys->ThreeBodyEnergy(do_grads != 0);
+        *e = nbody == 1   ? sys->OneBodyEnergy(do_grads != 0)
+             : nbody == 2 ? sys->TwoBodyEnergy(do_grads != 0)
+                          : sys->ThreeBodyEnergy(do_grads != 0);
         return 0;
     } catch (const std::exception& e) {
         g_err = e.what();

@@ -9,6 +9,8 @@ built by oracle/build_ref.py from the reference's sources) through
 ``tests/golden/ref_<workload>.npz``:
 
 * ``xyz_sha256``: the input coordinates' hash (the workload recipe must not drift);
+* ``e1`` (water workloads): the 1-body energy, ``g1``, ``v1`` its gradient
+  and virial (``OneBodyEnergy(true)``, bblock/system.cpp:2140);
 * ``e2``, ``e3``: the 2-body and 3-body energies (kcal/mol);
 * ``g2``, ``g3``: the gradients of real atoms, input order (kcal/mol/A);
 * ``v2``, ``v3``: the virials (9 each);
@@ -42,7 +44,12 @@ WORKLOADS = {
     "water_256": (lambda: workloads.water_256(0), 9.0, 7.0),
     "water_2048": (lambda: workloads.water_2048(0), 9.0, 7.0),
     "methane_water": (lambda: workloads.methane_water_box(seed=0), 9.0, 7.0),
+    "water_256_bead": (lambda: workloads.water_256_bead(0), 9.0, 7.0),
 }
+
+
+# workloads whose monomers all have a GPU 1-body term (water)
+ONEBODY = ("water_256", "water_2048", "water_256_bead")
 
 
 def list_hash(nm):
@@ -59,6 +66,11 @@ def make(name):
     ids, xyz, box = make_fn()
     r = mo.RefSystem(ids, xyz, box, c2, c3)
     out = {"xyz_sha256": xyz_hash(xyz)}
+    if name in ONEBODY:
+        # System::OneBodyEnergy(true) (bblock/system.cpp:2140)
+        out["e1"] = r.energy(1)
+        out["g1"] = r.real_grads()
+        out["v1"] = r.virial()
     for nb, cut in ((2, c2), (3, c3)):
         out["e%d" % nb] = r.energy(nb)
         out["g%d" % nb] = r.real_grads()

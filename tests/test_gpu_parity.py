@@ -434,6 +434,69 @@ def test_fp64_vs_reference(name):
         assert len(nm) == int(d["n%d" % nb]) and list_hash(nm) == str(d["l%d_sha256" % nb]), nb
 
 
+@pytest.mark.parametrize("name", ["water_256", "water_256_bead", "water_2048"])
+def test_onebody_vs_reference(name):
+    """System::OneBodyEnergy(true) (bblock/system.cpp:2140): the GPU
+    Partridge-Schwenke term against the reference's, energy within 1e-10
+    relative (or 1e-9 kcal/mol per water: a near-equilibrium water's energy
+    is a small difference of terms ~10^5 times larger), gradients within
+    1e-8 kcal/mol/A, virial."""
+    ids, xyz, box, c2, c3, d = ref_fixture(name)
+    g = msys.from_arrays(ids, xyz, box, c2, c3)
+    for do_grads in (True, False):
+        e = g.OneBodyEnergy(do_grads)
+        er = float(d["e1"])
+        assert rel(e, er) < E_REL or abs(e - er) < 1e-9 * len(ids), (e, er)
+    g.OneBodyEnergy(True)
+    np.testing.assert_allclose(g.GetRealGrads(), d["g1"], rtol=0, atol=G_ABS)
+    np.testing.assert_allclose(g.GetVirial(), d["v1"], rtol=1e-10, atol=1e-8)
+    assert g.NmerCounts(1)[0] == len(ids)
+
+
+def test_onebody_refuses_cpu_only_types():
+    """A monomer type whose 1-body term the reference has but the GPU path
+    does not (CH4) makes the 1-body call fail loudly, unless ignored."""
+    ids, xyz, box = workloads.methane_water_box(seed=0)
+    g = msys.from_arrays(ids, xyz, box, 9.0, 7.0)
+    with pytest.raises(Exception, match="1-body"):
+        g.OneBodyEnergy(True)
+    g.ignore_1b = ["ch4"]
+    g._push_config()
+    e = g.OneBodyEnergy(True)
+    w = msys.from_arrays([i for i in ids if i == "h2o"],
+                         np.concatenate([x for i, x in zip(ids, np.split(np.asarray(xyz).reshape(-1),
+                                                                         np.cumsum([9 if i == "h2o" else 15
+                                                                                    for i in ids])[:-1]))
+                                         if i == "h2o"]), box, 9.0, 7.0)
+    assert abs(e - w.OneBodyEnergy(True)) < 1e-9 * abs(e)
+
+
+@pytest.mark.parametrize("name", ["water_256_bead", "methane_water"])
+def test_real_order_device_path(name):
+    """GPU-resident callers (i-PI, LAMMPS): real coordinates in input order as
+    a CUDA tensor, gradient accumulated in input order, against the
+    reference; the caller's coordinates are left untouched."""
+    torch = pytest.importorskip("torch")
+    ids, xyz, box, c2, c3, d = ref_fixture(name)
+    g = msys.from_arrays(ids, xyz, box, c2, c3)
+    xr = torch.tensor(np.asarray(xyz).reshape(-1), device="cuda")
+    x0 = xr.clone()
+    terms = (1, 2, 3) if "e1" in d else (2, 3)
+    for nb in terms:
+        gr = torch.full_like(xr, 0.5)
+        e, v = g.EnergyFromRealXyz(nb, xr, gr)
+        er = float(d["e%d" % nb])
+        assert rel(e, er) < E_REL or abs(e - er) < 1e-9 * len(ids), (nb, e, er)
+        np.testing.assert_allclose(gr.cpu().numpy() - 0.5, d["g%d" % nb], rtol=0, atol=G_ABS)
+        np.testing.assert_allclose(v, d["v%d" % nb], rtol=1e-10, atol=1e-7)
+    assert torch.equal(xr, x0)
+    # host arrays
+    gh = np.zeros(xr.numel())
+    e, _ = g.EnergyFromRealXyz(3, np.asarray(xyz, np.float64).reshape(-1).copy(), gh)
+    assert rel(e, float(d["e3"])) < E_REL
+    np.testing.assert_allclose(gh, d["g3"], rtol=0, atol=G_ABS)
+
+
 def test_water_2048_lists_vs_restatement():
     """The full-size lists also equal the oracle restatement's, n-mer by n-mer."""
     ids, xyz, box = workloads.water_2048(0)

@@ -293,7 +293,7 @@ def test_helium_dilute_vs_reference():
     np.testing.assert_allclose(o.real_grads(), r.real_grads(), rtol=0, atol=1e-8)
 
 
-@pytest.mark.parametrize("name", ["water_256", "water_2048", "methane_water"])
+@pytest.mark.parametrize("name", ["water_256", "water_2048", "methane_water", "water_256_bead"])
 def test_reference_fixtures_match_the_reference(name):
     """The committed reference fixtures (tests/golden/ref_*.npz) are what the
     compiled reference computes now, on the workload the recipe makes now."""
@@ -306,6 +306,9 @@ def test_reference_fixtures_match_the_reference(name):
     d = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref_%s.npz" % name))
     assert str(d["xyz_sha256"]) == xyz_hash(xyz)
     r = mo.RefSystem(ids, xyz, box, c2, c3)
+    if "e1" in d:
+        assert abs(r.energy(1) - float(d["e1"])) <= 1e-12 * abs(float(d["e1"])) + 1e-12
+        np.testing.assert_allclose(r.real_grads(), d["g1"], rtol=0, atol=1e-10)
     for nb, cut in ((2, c2), (3, c3)):
         # the reference's OpenMP reduction order may vary between runs
         assert abs(r.energy(nb) - float(d["e%d" % nb])) <= 1e-12 * abs(float(d["e%d" % nb]))
