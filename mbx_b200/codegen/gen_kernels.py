@@ -41,7 +41,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.dirname(HERE)
 sys.path.insert(0, os.path.dirname(PKG))
 
-from mbx_b200.specs import SPECS, LP_GAMMA_IN, LP_GAMMA_OUT  # noqa: E402
+from mbx_b200.specs import SPECS, ONEBODY_SPECS, LP_GAMMA_IN, LP_GAMMA_OUT  # noqa: E402
 from mbx_b200.tables import load_pip  # noqa: E402
 
 OUT = os.path.join(PKG, "csrc", "gen")
@@ -553,7 +553,8 @@ def emit_traits(spec, table, straight, out):
     w("    static constexpr int NAT0 = %d, NAT1 = %d, NAT2 = %d;" % tuple(nat))
     w("    static constexpr int FIRST0 = %d, FIRST1 = %d, FIRST2 = %d;" % tuple(first))
     w("    static constexpr int SWITCH_TRIPLE = %d, SKIP = %d, STRAIGHT = %d, DEGREE = %d;" %
-      ({"pair": 0, "triple": 1, "triple2": 2, "cos2": 3}[spec.switch], {"pair_gt": 0, "two_of_three_gt": 1, "all_three_gt": 2}[spec.skip],
+      ({"pair": 0, "triple": 1, "triple2": 2, "cos2": 3, "none": 0}[spec.switch],
+       {"pair_gt": 0, "two_of_three_gt": 1, "all_three_gt": 2, "none": 0}[spec.skip],
        1 if straight else 0, spec.degree))
     w("    static constexpr int TPAIRS = %d;  // (variable, exponent) pairs of a term, at most" %
       term_pairs_max(table))
@@ -611,7 +612,7 @@ def generate(name):
     """Writes <name>.cuh (sizes, sites, variables, chain rule, traits) and one
     header per polynomial variant, so that a change to one variant rebuilds
     only the units that include it."""
-    spec = SPECS[name]
+    spec = SPECS[name] if name in SPECS else ONEBODY_SPECS[name]
     table = load_pip(name)
     straight = name in STRAIGHT_TYPES
     trie = Trie(table) if straight else None
@@ -823,6 +824,30 @@ int mbx_launch_%(name)s_w(const HolderArgs& A, int grads, int grid, cudaStream_t
 """
 
 
+ONEBODY_TU = """// Generated by mbx_b200/codegen/gen_kernels.py -- do not edit.
+// Table-driven 1-body kernel of the %(name)s evaluator.
+#include <cstring>
+#include "../holder_kernel.cuh"
+#include "../launch_cache.cuh"
+#include "%(name)s.cuh"
+
+int mbx_launch_%(name)s_o(const HolderArgs& A, int grid, int block, cudaStream_t s) {
+    // a lane per monomer; x and gradient columns of four warps in dynamic shared memory
+    auto kern = onebody_table_kernel<%(name)s_T>;
+    const int smem = 4 * 2 * %(name)s_T::NVARS * 32 * (int)sizeof(double);
+    static LaunchCache lc;
+    int sms = 0, bps = 0;
+    const int r = launch_facts(lc, kern, 128, smem, smem, &sms, &bps);
+    if (r) return r;
+    if (A.n <= 0) return 0;
+    const long need = (A.n + 127) / 128;
+    const int g = (int)(need < (long)sms * bps ? need : (long)sms * bps);
+    kern<<<g, 128, smem, s>>>(A);
+    return (int)cudaGetLastError();
+}
+"""
+
+
 # Evaluators with straight-line (generated Horner trie) kernels: the water
 # and methane-water polynomials of MB-pol / MB-nrg the timed path runs.  All
 # others run the table-driven kernels: their tries would add minutes of
@@ -832,6 +857,8 @@ STRAIGHT_TYPES = ("mbpol2b", "mbpol3b", "ch4h2o2b", "ch4h2o3b")
 
 def variants_of(name):
     from mbx_b200.specs import KERNEL_ALIASES
+    if name in ONEBODY_SPECS:
+        return "o"
     name = KERNEL_ALIASES.get(name, name)
     if name in STRAIGHT_TYPES:
         return "ge" + ("s" if name in SHIFT_TYPES else "") + "t"
@@ -962,9 +989,13 @@ def write_tu(path, text):
 
 
 def write_kernels_cu(name):
-    spec = SPECS[name]
     paths = []
     inc = {"g": "pip", "e": "pip_e"}
+    if name in ONEBODY_SPECS:
+        path = os.path.join(OUT, "%s_t.cu" % name)
+        write_tu(path, ONEBODY_TU % {"name": name})
+        return [path]
+    spec = SPECS[name]
     for v in variants_of(name):
         if v == "w":
             continue   # part of the table unit
@@ -1015,13 +1046,16 @@ def term_pairs_max(table):
 
 def table_names():
     """Term tables in registry order (an evaluator sharing another's table
-    refers to the same entry)."""
+    refers to the same entry), then the 1-body evaluators' tables."""
     from mbx_b200.specs import KERNEL_ALIASES
     names = []
     for n in SPECS:
         t = SPECS[KERNEL_ALIASES.get(n, n)].pip_table
         if t not in names:
             names.append(t)
+    for n, sp in ONEBODY_SPECS.items():
+        if sp.pip_table not in names:
+            names.append(sp.pip_table)
     return names
 
 
@@ -1173,6 +1207,21 @@ def write_registry():
                       names.index(kern)))
     lines.append("};")
     lines.append("static const int mbx_num_evaluators = %d;" % len(SPECS))
+    # 1-body evaluators (table-driven), by monomer id
+    from mbx_b200.specs import ONEBODY_DISPATCH
+    lines.append("struct OneBodyInfo { const char* name; const char* mon; int ncoef; const double* fit; int table; "
+                 "int (*launch)(const HolderArgs&, int, int, cudaStream_t); };")
+    for name, sp in ONEBODY_SPECS.items():
+        lines.append("int mbx_launch_%s_o(const HolderArgs& A, int grid, int block, cudaStream_t s);" % name)
+        fit = load_fit(name)
+        lines.append("static const double mbx_fit_%s[%d] = {%s};" %
+                     (name, len(fit), ", ".join(repr(float(x)) for x in fit)))
+    mon_of = {v: k for k, v in ONEBODY_DISPATCH.items()}
+    lines.append("static const OneBodyInfo mbx_onebody[] = {%s};" % ", ".join(
+        '{"%s", "%s", %d, mbx_fit_%s, %d, mbx_launch_%s_o}' %
+        (name, mon_of[name], sp.ncoef, name, tables.index(sp.pip_table), name)
+        for name, sp in ONEBODY_SPECS.items()))
+    lines.append("static const int mbx_num_onebody = %d;" % len(ONEBODY_SPECS))
     # real atoms per monomer id (SetUpMonomers, bblock/sys_tools.cpp:133-254)
     from mbx_b200.specs import MONOMER_ATOMS
     lines.append("struct MonomerInfo { const char* id; int nat; };")
@@ -1193,6 +1242,8 @@ def main(argv=None, quiet=False):
     write_ps1b()
     from mbx_b200.specs import KERNEL_ALIASES
     keep = {"registry.inc", "terms_index.inc", "terms.bin", "terms_blob.cpp", "ps1b.inc"}
+    if args.names == list(SPECS):
+        args.names = list(SPECS) + list(ONEBODY_SPECS)
     for n in args.names:
         if n in KERNEL_ALIASES:
             continue
@@ -1204,7 +1255,7 @@ def main(argv=None, quiet=False):
         keep.update(os.path.basename(p) for p in write_kernels_cu(n))
         if not quiet:
             print("%s: %d leaves, %d inner -> %s" % (n, leaves, inner, path))
-    if args.names == list(SPECS):
+    if args.names == list(SPECS) + list(ONEBODY_SPECS):
         # drop the units of an earlier generation (other variants or types)
         for f in os.listdir(OUT):
             if f not in keep:

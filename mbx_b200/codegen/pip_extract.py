@@ -109,9 +109,11 @@ PROGRAMS = {
     "hehe2b": ("potential/2b/poly_2b_A1_A1_deg23_v1.cpp", 1, 23, 23),
     "h2ohe2b": ("potential/2b/poly_2b_A1B2Z2_C1_deg5_v1.cpp", 8, 496, 5),
     "n2o5h2o2b": ("potential/2b/poly_2b_A1B2C4_D1E2_deg3_v1.cpp", 45, 983, 3),
+    # 1-body: CH4 (x1b_A1B4_deg5_exp0::x1b_A1B4_v1x, potential/1b/x1b_A1B4_deg5_exp0_v1x.cpp:309-419)
+    "ch41b": ("potential/1b/poly_1b_A1B4_deg5_exp0_v1.cpp", 10, 207, 5),
 }
 # programs whose value is assigned to ``double e`` and then returned
-E_ASSIGN = {"co2co22btab"}
+E_ASSIGN = {"co2co22btab", "ch41b"}
 # programs whose value is a named temporary (value + gradient programs)
 RESULT_VAR = {"h2oion3b": r"double e = (t\d+)\s*;"}
 
@@ -180,6 +182,9 @@ TABLE_OF["h2oco22b"] = "h2oco22b"
 FITS["h2oco2a2b"] = ("potential/2b/x2b_A1B2Z2_C1D2_v1x.cpp",
                      r'if \(mon1 == "h2o" && mon2 == "co2_archive"\) \{\s*coefficients\s*=\s*std::vector<double>\s*\{')
 TABLE_OF["h2oco2a2b"] = "h2oco22b"
+FITS["ch41b"] = ("potential/1b/x1b_A1B4_deg5_exp0_v1x.cpp",
+                 r'if \(mon == "ch4"\) \{\s*coefficients\s*=\s*std::vector<double>\s*\{')
+TABLE_OF["ch41b"] = "ch41b"
 FITS["n2o5h2o2b"] = ("potential/2b/x2b_A1B2C4_D1E2_deg3_v1x.cpp",
                      r'if \(mon1 == "h2o" && mon2 == "n2o5"\) \{\s*coefficients\s*=\s*std::vector<double>\s*\{')
 TABLE_OF["n2o5h2o2b"] = "n2o5h2o2b"

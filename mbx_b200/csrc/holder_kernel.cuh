@@ -683,6 +683,88 @@ __global__ void __launch_bounds__(128) holder_table_lane_kernel(const HolderArgs
     block_reduce_add<7>(acc, A.out);
 }
 
+// 1-body MB-nrg evaluation (x1b_*::eval, e.g. x1b_A1B4_v1x::eval,
+// potential/1b/x1b_A1B4_deg5_exp0_v1x.cpp:361-419): no image, no switch, no
+// cutoff.  A lane per monomer, the warp walking the term table in step (as
+// holder_table_lane_kernel); variables, chain rule and the virial
+// -sum r (x) g over the monomer's atoms as the reference's evaluator does.
+// A.first_index: first site of each monomer to evaluate (A.n of them); one
+// thread per monomer writes its gradient, so no atomics.  Dynamic shared
+// memory: 4 warps x 2 x NVARS x 32 doubles.
+template <class T>
+__global__ void __launch_bounds__(128) onebody_table_kernel(const HolderArgs A) {
+    static_assert(T::NBODY == 1, "1-body evaluators only");
+    double* xc = reinterpret_cast<double*>(mbx_dyn_smem) + ((threadIdx.x >> 5) * 2 * T::NVARS) * 32 +
+                 (threadIdx.x & 31);
+    double* gc = xc + T::NVARS * 32;
+    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    const bool grads = A.grad != nullptr;
+    for (long base = blockIdx.x * (long)blockDim.x; base < A.n; base += (long)gridDim.x * blockDim.x) {
+        const long t = base + threadIdx.x;
+        const bool live = t < A.n;
+        double r[T::NREAL][3];
+        double s[T::NSITES][3];
+        {
+            double x[T::NVARS];
+#pragma unroll
+            for (int v = 0; v < T::NVARS; ++v) x[v] = 0.0;
+            if (live) {
+                const double* p = A.xyz + 3 * (size_t)__ldg(A.first_index + t);
+#pragma unroll
+                for (int i = 0; i < T::NREAL; ++i)
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) r[i][c] = p[3 * i + c];
+                T::sites(r, s);
+                T::vars(s, x);
+            }
+#pragma unroll
+            for (int v = 0; v < T::NVARS; ++v) {
+                xc[v * 32] = x[v];
+                gc[v * 32] = 0.0;
+            }
+        }
+        __syncwarp();
+        double e = 0.0;
+        if (__any_sync(0xffffffffu, live)) {
+            const auto xv = [&](int v) { return xc[v * 32]; };
+            for (long q = 0; q < A.nterms; ++q) {
+                const int4 tm = __ldg(A.terms + q);
+                const double c = __ldg(A.coef + tm.x) * __ldg(A.tcoef + q);
+                if (grads)
+                    e += term_value_grad<T::TPAIRS>(tm, c, xv, [&](int v, double dv) { gc[v * 32] += dv; });
+                else
+                    e += term_value<T::TPAIRS>(tm, c, xv);
+            }
+        }
+        __syncwarp();
+        if (live) {
+            acc[0] += e;
+            if (grads) {
+                double g[T::NVARS];
+#pragma unroll
+                for (int v = 0; v < T::NVARS; ++v) g[v] = gc[v * 32];
+                double sg[T::NSITES][3];
+                T::chain(s, g, sg);
+                const int ia[6] = {0, 0, 0, 1, 1, 2}, ib[6] = {0, 1, 2, 1, 2, 2};
+#pragma unroll
+                for (int k = 0; k < 6; ++k) {
+                    double v = 0.0;
+#pragma unroll
+                    for (int i = 0; i < T::NREAL; ++i) v -= r[i][ia[k]] * sg[i][ib[k]];
+                    acc[1 + k] += v;
+                }
+                double* q = A.grad + 3 * (size_t)__ldg(A.first_index + t);
+#pragma unroll
+                for (int i = 0; i < T::NREAL; ++i)
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) q[3 * i + c] += sg[i][c];
+            }
+        }
+        __syncwarp();
+    }
+    block_reduce_add<7>(acc, A.out);
+}
+
 // Gradient with respect to the linear coefficients: out[k] += sum over n-mers
 // of w[n] * sw(n) * dP/da_k(x(n)), the monomials recomputed from the
 // coordinates (adjoint of E = sum_n sw(n) P(a, x(n)) for refitting), from the

@@ -110,6 +110,7 @@ std::mutex g_dev_mu;
 bool g_dev_constants[kMaxDevices] = {false};
 DeviceTables g_dev_tables[kMaxDevices];
 long g_coef_off[256];
+long g_coef_off_1b[16];
 long g_coef_total = -1;
 
 void coef_layout() {
@@ -118,6 +119,10 @@ void coef_layout() {
     for (int i = 0; i < mbx_num_evaluators; ++i) {
         g_coef_off[i] = off;
         off += mbx_evaluators[i].ncoef;
+    }
+    for (int i = 0; i < mbx_num_onebody; ++i) {
+        g_coef_off_1b[i] = off;
+        off += mbx_onebody[i].ncoef;
     }
     g_coef_total = off;
 }
@@ -177,6 +182,9 @@ int mbx_device_tables(int dev, DeviceTables* out) {
         for (int i = 0; i < mbx_num_evaluators && e == cudaSuccess; ++i)
             e = cudaMemcpy(static_cast<double*>(coef) + g_coef_off[i], mbx_evaluators[i].fit,
                            mbx_evaluators[i].ncoef * sizeof(double), cudaMemcpyHostToDevice);
+        for (int i = 0; i < mbx_num_onebody && e == cudaSuccess; ++i)
+            e = cudaMemcpy(static_cast<double*>(coef) + g_coef_off_1b[i], mbx_onebody[i].fit,
+                           mbx_onebody[i].ncoef * sizeof(double), cudaMemcpyHostToDevice);
         if (cur != dev) cudaSetDevice(cur);
         if (e != cudaSuccess) {
             if (blob) cudaFree(blob);
@@ -264,9 +272,12 @@ struct mbx_ctx {
     int numat = 0;
     DevBuf<int> d_real2site;
     DevBuf<double> xreal, greal, gsite;
-    // 1-body term: first sites of the local waters, built for topology generation w1b_gen
+    // 1-body term: first sites of the local waters, then of the local
+    // monomers of each table-driven 1-body evaluator (n1b[i] of them), built
+    // for topology generation w1b_gen
     DevBuf<int> d_w1b;
     long n_w1b = 0;
+    long n1b[16] = {0};
     unsigned long w1b_gen = ~0ul;
 
     // per-term dispatch
@@ -1035,11 +1046,11 @@ static int unstage_term_io(mbx_ctx* c, double* xyz, double* grad, int flags, dou
 }
 
 // Monomer types whose 1-body term the reference computes
-// (e1b::get_1b_energy, potential/1b/energy1b.cpp:53-86); the ones other than
-// water have no GPU evaluator here, and a topology holding them (and not
+// (e1b::get_1b_energy, potential/1b/energy1b.cpp:53-86) but that have no
+// GPU evaluator here (water and CH4 have), and a topology holding them (and not
 // ignoring them) gets MBX_ENOTSUP for the 1-body term rather than a silent
 // zero.  Every other type has no 1-body term (0, as in the reference).
-static const char* const k1bCpuOnly[] = {"ch4", "co2_archive", "nh3", "nh3pbe0d3bj", "co2", "co2cm5100", "co2cm595",
+static const char* const k1bCpuOnly[] = {"co2_archive", "nh3", "nh3pbe0d3bj", "co2", "co2cm5100", "co2cm595",
                                          "co2cm590", "co2cm5875", "co2cm585", "co2cm580", "h2", "n2o5", "mbpbe"};
 
 // System::Get1B (bblock/system.cpp:2269-2401) on device coordinates X
@@ -1057,6 +1068,13 @@ static int onebody_term(mbx_ctx* c, double* X, double* G, double* energy, double
         for (int m = 0; m < c->nmon; ++m)
             if (c->type_names[c->h_type[m]] == "h2o" && c->h_local[m] && !ignored("h2o")) first.push_back(c->h_first[m]);
         c->n_w1b = (long)first.size();
+        for (int i = 0; i < mbx_num_onebody; ++i) {
+            const std::string id = mbx_onebody[i].mon;
+            const size_t before = first.size();
+            for (int m = 0; m < c->nmon; ++m)
+                if (c->type_names[c->h_type[m]] == id && c->h_local[m] && !ignored(id)) first.push_back(c->h_first[m]);
+            c->n1b[i] = (long)(first.size() - before);
+        }
         CUCHK(c, c->d_w1b.ensure(std::max<size_t>(first.size(), 1)));
         if (!first.empty())
             CUCHK(c, cudaMemcpyAsync(c->d_w1b.p, first.data(), first.size() * sizeof(int), cudaMemcpyHostToDevice,
@@ -1069,6 +1087,26 @@ static int onebody_term(mbx_ctx* c, double* X, double* G, double* energy, double
     OneBodyArgs A{X, c->d_w1b.p, c->n_w1b, G, c->out.p};
     RCHK(c, mbx_launch_ps1b(A, c->sm_count, c->stream));
     if (c->n_w1b > 0) ++*kernels;
+    long off = c->n_w1b, n1 = c->n_w1b;
+    for (int i = 0; i < mbx_num_onebody; ++i) {
+        if (c->n1b[i] > 0) {
+            const TermTableInfo& T = mbx_term_tables[mbx_onebody[i].table];
+            HolderArgs H = base_args(c);
+            H.n = c->n1b[i];
+            H.first_index = c->d_w1b.p + off;
+            H.xyz = X;
+            H.grad = G;
+            H.out = c->out.p;
+            H.terms = reinterpret_cast<const int4*>(c->tables.blob + T.off_terms);
+            H.tcoef = reinterpret_cast<const double*>(c->tables.blob + T.off_tcoef);
+            H.nterms = T.nterms;
+            H.coef = c->tables.coef + g_coef_off_1b[i];
+            RCHK(c, mbx_onebody[i].launch(H, 0, 128, c->stream));
+            ++*kernels;
+        }
+        off += c->n1b[i];
+        n1 += c->n1b[i];
+    }
     CUCHK(c, cudaEventRecord(c->ev[2], c->stream));
     CUCHK(c, cudaMemcpyAsync(c->h_out, c->out.p, 7 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     CUCHK(c, cudaStreamSynchronize(c->stream));
@@ -1087,7 +1125,7 @@ static int onebody_term(mbx_ctx* c, double* X, double* G, double* energy, double
     c->last_ms_build = 0;
     cudaEventElapsedTime(&c->last_ms_eval, c->ev[1], c->ev[2]);
     c->last_kernels = *kernels;
-    c->last_listed[1] = c->last_evaluated[1] = c->n_w1b;
+    c->last_listed[1] = c->last_evaluated[1] = n1;
     return MBX_OK;
 }
 

@@ -727,6 +727,27 @@ DISPATCH_3B = {("h2o", "h2o", "h2o"): "mbpol3b", ("ch4", "h2o", "h2o"): "ch4h2o3
 # SetUpMonomers:133-254: h2o has 3 atoms + the M site, ch4 5 atoms, the
 # alkali-metal and halide ions and argon one atom, :210-225, h2 two, nh3
 # four, co2 three, mbpbe like h2o three atoms and four sites, :191-233).
+# ---------------------------------------------------------------------------
+# 1-body MB-nrg: CH4, x1b_A1B4_deg5_exp0::x1b_A1B4_v1x,
+# potential/1b/x1b_A1B4_deg5_exp0_v1x.cpp:309-419 (constants :302-305,
+# variables v_exp0(d0, k) = exp(k (d0 - r)) :67-80, :327-336).  No switch, no
+# cutoff: every local CH4 is evaluated (System::Get1B, system.cpp:2269).
+# ---------------------------------------------------------------------------
+_S = ("A1", "B1", "B2", "B3", "B4")
+_kAB1, _dAB1 = 9.118575345478506e-01, 4.848036021821232e+00
+_kBB1, _dBB1 = 3.397786901029656e-01, 6.999341954887242e+00
+CH41B = Spec(
+    name="ch41b", monomers=("ch4",), nat=(5,), sites=_S, lp=(),
+    variables=_vars(_S, [("exp", "A1", "B%d" % i, _kAB1, _dAB1) for i in range(1, 5)] +
+                    [("exp", "B%d" % i, "B%d" % j, _kBB1, _dBB1) for i in range(1, 5) for j in range(i + 1, 5)]),
+    switch="none", ri=0.0, rf=0.0, skip="none",
+    nvars=10, ncoef=207, degree=5, ref="potential/1b/x1b_A1B4_deg5_exp0_v1x.cpp:361",
+)
+# 1-body evaluators with a GPU kernel other than water's Partridge-Schwenke
+# term, by monomer id (e1b::get_1b_energy, potential/1b/energy1b.cpp:53-56)
+ONEBODY_SPECS = {CH41B.name: CH41B}
+ONEBODY_DISPATCH = {"ch4": "ch41b"}
+
 MONOMER_ATOMS = {"h2o": 3, "ch4": 5, "li+": 1, "na+": 1, "k+": 1, "rb+": 1, "cs+": 1,
                  "f-": 1, "cl-": 1, "br-": 1, "i-": 1, "ar": 1, "h2": 2, "nh3": 4, "nh3pbe0d3bj": 4, "co2": 3,
                  "mbpbe": 3, "co2_archive": 3, "co2cm5100": 3, "co2cm595": 3, "co2cm590": 3, "co2cm585": 3,

@@ -48,8 +48,8 @@ WORKLOADS = {
 }
 
 
-# workloads whose monomers all have a GPU 1-body term (water)
-ONEBODY = ("water_256", "water_2048", "water_256_bead")
+# workloads whose monomers all have a GPU 1-body term (water, CH4)
+ONEBODY = ("water_256", "water_2048", "water_256_bead", "methane_water")
 
 
 def list_hash(nm):

@@ -434,7 +434,7 @@ def test_fp64_vs_reference(name):
         assert len(nm) == int(d["n%d" % nb]) and list_hash(nm) == str(d["l%d_sha256" % nb]), nb
 
 
-@pytest.mark.parametrize("name", ["water_256", "water_256_bead", "water_2048"])
+@pytest.mark.parametrize("name", ["water_256", "water_256_bead", "water_2048", "methane_water"])
 def test_onebody_vs_reference(name):
     """System::OneBodyEnergy(true) (bblock/system.cpp:2140): the GPU
     Partridge-Schwenke term against the reference's, energy within 1e-10
@@ -455,46 +455,23 @@ def test_onebody_vs_reference(name):
 
 def test_onebody_refuses_cpu_only_types():
     """A monomer type whose 1-body term the reference has but the GPU path
-    does not (CH4) makes the 1-body call fail loudly, unless ignored."""
-    ids, xyz, box = workloads.methane_water_box(seed=0)
-    g = msys.from_arrays(ids, xyz, box, 9.0, 7.0)
+    does not (NH3) makes the 1-body call fail loudly, unless ignored; the
+    ignored type then contributes nothing."""
+    rng = np.random.default_rng(4)
+    ids = ["h2o"] * 6 + ["nh3"] * 2
+    parts = []
+    for k, m in enumerate(ids):
+        centre = np.array([4.0 * (k % 4), 4.0 * (k // 4), 0.0])
+        parts.append(workloads.place(rng, workloads.BODIES[m](), centre[None, :])[0].reshape(-1))
+    xyz = np.concatenate(parts)
+    g = msys.from_arrays(ids, xyz, None, 9.0, 7.0)
     with pytest.raises(Exception, match="1-body"):
         g.OneBodyEnergy(True)
-    g.ignore_1b = ["ch4"]
+    g.ignore_1b = ["nh3"]
     g._push_config()
     e = g.OneBodyEnergy(True)
-    w = msys.from_arrays([i for i in ids if i == "h2o"],
-                         np.concatenate([x for i, x in zip(ids, np.split(np.asarray(xyz).reshape(-1),
-                                                                         np.cumsum([9 if i == "h2o" else 15
-                                                                                    for i in ids])[:-1]))
-                                         if i == "h2o"]), box, 9.0, 7.0)
-    assert abs(e - w.OneBodyEnergy(True)) < 1e-9 * abs(e)
-
-
-@pytest.mark.parametrize("name", ["water_256_bead", "methane_water"])
-def test_real_order_device_path(name):
-    """GPU-resident callers (i-PI, LAMMPS): real coordinates in input order as
-    a CUDA tensor, gradient accumulated in input order, against the
-    reference; the caller's coordinates are left untouched."""
-    torch = pytest.importorskip("torch")
-    ids, xyz, box, c2, c3, d = ref_fixture(name)
-    g = msys.from_arrays(ids, xyz, box, c2, c3)
-    xr = torch.tensor(np.asarray(xyz).reshape(-1), device="cuda")
-    x0 = xr.clone()
-    terms = (1, 2, 3) if "e1" in d else (2, 3)
-    for nb in terms:
-        gr = torch.full_like(xr, 0.5)
-        e, v = g.EnergyFromRealXyz(nb, xr, gr)
-        er = float(d["e%d" % nb])
-        assert rel(e, er) < E_REL or abs(e - er) < 1e-9 * len(ids), (nb, e, er)
-        np.testing.assert_allclose(gr.cpu().numpy() - 0.5, d["g%d" % nb], rtol=0, atol=G_ABS)
-        np.testing.assert_allclose(v, d["v%d" % nb], rtol=1e-10, atol=1e-7)
-    assert torch.equal(xr, x0)
-    # host arrays
-    gh = np.zeros(xr.numel())
-    e, _ = g.EnergyFromRealXyz(3, np.asarray(xyz, np.float64).reshape(-1).copy(), gh)
-    assert rel(e, float(d["e3"])) < E_REL
-    np.testing.assert_allclose(gh, d["g3"], rtol=0, atol=G_ABS)
+    w = msys.from_arrays(ids[:6], np.concatenate(parts[:6]), None, 9.0, 7.0)
+    assert abs(e - w.OneBodyEnergy(True)) <= 1e-12 * abs(e)
 
 
 def test_water_2048_lists_vs_restatement():
