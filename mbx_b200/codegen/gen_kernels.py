@@ -923,20 +923,28 @@ int mbx_set_coef_%(name)s_s(const double* a, int from_device, cudaStream_t s) {
 }
 
 int mbx_launch_%(name)s_s(const HolderArgs& A, int grid, int block, cudaStream_t s) {
-    // persistent grid of lockstep blocks (two n-mers per thread): every
-    // resident block slot once; the paired variables and gradient
-    // accumulators of the block in dynamic shared memory
-    auto kern = holder_pair_kernel<%(name)s_T, %(name)s_CS>;
+    // three kernels (holder_kernel.cuh): the FP64 variables at full
+    // occupancy, the paired FP32 trie in a persistent grid of lockstep blocks
+    // (two n-mers per thread, every resident block slot once, the paired
+    // variables and gradient accumulators of the block in dynamic shared
+    // memory), the FP64 chain rule and sums at full occupancy; A.ps holds the
+    // scratch between them (capacity A.ps.cap >= A.n)
+    if (!A.ps.dx || A.ps.cap < A.n) return (int)cudaErrorInvalidValue;
+    auto kern = pair_trie_kernel<%(name)s_T, %(name)s_CS>;
     block = %(name)s_T::LOCK_THREADS_S;
     const int smem = 2 * %(name)s_T::NVARS * %(name)s_T::LOCK_THREADS_S * (int)sizeof(f2_t);
     static LaunchCache lc;
     int sms = 0, bps = 0;
     const int r = launch_facts(lc, kern, block, smem, smem, &sms, &bps);
     if (r) return r;
+    const long wide = (long)sms * 16;
+    const long gv = (A.n + 255) / 256, gf = (A.n + 127) / 128;
+    pair_vars_kernel<%(name)s_T><<<(int)(gv < wide ? (gv > 0 ? gv : 1) : wide), 256, 0, s>>>(A);
     const long need = (A.n + 2 * block - 1) / (2 * block);
     grid = (int)(need < (long)sms * bps ? need : (long)sms * bps);
     if (grid < 1) grid = 1;
     kern<<<grid, block, smem, s>>>(A);
+    pair_finish_kernel<%(name)s_T><<<(int)(gf < wide ? (gf > 0 ? gf : 1) : wide), 128, 0, s>>>(A);
     return (int)cudaGetLastError();
 }
 
@@ -944,7 +952,7 @@ int mbx_prime_%(name)s_s(cudaStream_t s) {
     // code prefetch of the paired FP32 trie: a launch of the evaluation kernel itself in its
     // prefetch mode (prime_pieces), one warp per SM, every piece run by at
     // least four of them
-    auto kern = holder_pair_kernel<%(name)s_T, %(name)s_CS>;
+    auto kern = pair_trie_kernel<%(name)s_T, %(name)s_CS>;
     const int smem_full = 2 * %(name)s_T::NVARS * %(name)s_T::LOCK_THREADS_S * (int)sizeof(f2_t);
     const int smem = %(name)s_T::NVARS * %(name)s_T::LOCK_THREADS_S * (int)sizeof(f2_t);
     static LaunchCache lc;

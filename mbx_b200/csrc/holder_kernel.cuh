@@ -22,9 +22,21 @@
 #include "term_table.cuh"
 
 // Precision / output modes.
-// HM_GRAD_SHIFT32 names the paired FP32 kernel (holder_pair_kernel) where a
+// HM_GRAD_SHIFT32 names the paired FP32 kernels (pair_*_kernel) where a
 // template needs to tell the two gradient kernels apart.
 enum { HM_ENERGY = 0, HM_GRAD_FP64 = 1, HM_GRAD_SHIFT32 = 4 };
+
+// Scratch of the mixed-precision evaluation (three kernels: variables, the
+// paired FP32 trie, chain rule), for up to cap n-mers: the shifted FP32
+// variables and the trie's gradient, variable-major ([v * cap + t]), the
+// polynomial's value and whether the n-mer is within the evaluator's cutoff.
+struct PairScratch {
+    float* dx;
+    float* g;
+    double* ep;
+    unsigned char* live;
+    long cap;
+};
 
 struct HolderArgs {
     long n;                    // number of n-mers (capacity when n_dev is set)
@@ -52,6 +64,7 @@ struct HolderArgs {
     // code prefetch launch of a lockstep kernel (prime_passes > 0; see
     // prime_pieces): of the rest only out (null) is read
     int prime_passes, prime_npieces;
+    PairScratch ps;            // mixed precision: scratch of the three kernels
 };
 
 // Coefficient source: a global pointer, read through the read-only path.
@@ -488,10 +501,32 @@ __device__ __forceinline__ bool nmer_vars_f32(const HolderArgs& A, long t, long 
     return live;
 }
 
-// Mixed-precision evaluation: two n-mers per thread, one in each half of the
-// paired FP32 registers, through the type's FP32-basis trie (T::SHIFTED) in
-// lockstep blocks.  Variables, switch, chain rule, virial and all sums stay
-// FP64.  A block claims chunks of 2 x blockDim.x n-mers.
+// Mixed-precision evaluation in three kernels.  The FP64 work around the
+// polynomial (gather, image, variables; later the switch, chain rule,
+// virial and scatter) is latency-bound and needs many warps, the paired FP32
+// trie needs few warps with all registers in lockstep; in one kernel both
+// ran at 8 warps per SM, so the FP64 parts took ~0.2 of the ~0.9 ms the
+// 2048-water trimers take.  Here:
+//   pair_vars_kernel    one n-mer per thread at full occupancy: the FP64
+//                       variables, shifted to the FP32 basis, into A.ps.dx
+//   pair_trie_kernel    the paired FP32 trie in lockstep blocks (two n-mers
+//                       per thread), dx in, gradient and value out
+//   pair_finish_kernel  one n-mer per thread at full occupancy: switch,
+//                       chain rule (FP64), virial, scatter, energy sums
+// The variables, switch, chain rule and sums stay FP64 as before.
+template <class T>
+__global__ void __launch_bounds__(256, 2) pair_vars_kernel(const HolderArgs A) {
+    const long n = nmer_count(A);
+    const long cap = A.ps.cap;
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
+        float xf[T::NVARS];
+        const bool live = nmer_vars_f32<T>(A, t, n, xf);
+#pragma unroll
+        for (int v = 0; v < T::NVARS; ++v) A.ps.dx[v * cap + t] = xf[v];
+        A.ps.live[t] = live ? 1 : 0;
+    }
+}
+
 // Coefficient pairs of the FP32 basis copied from constant to shared memory
 // once per block (a shared-memory operand costs fewer instructions per leaf
 // than a constant-bank one in the paired form).
@@ -502,8 +537,11 @@ struct SharedPairs {
     __device__ __forceinline__ double b0() const { return CC{}.b0(); }
 };
 
+// The paired FP32 trie: two n-mers per thread, one in each half of the
+// paired FP32 registers, through the type's FP32-basis trie (T::SHIFTED) in
+// lockstep blocks; a block claims chunks of 2 x blockDim.x n-mers.
 template <class T, class CC>
-__global__ void __launch_bounds__(T::LOCK_THREADS_S, 1) holder_pair_kernel(const HolderArgs A) {
+__global__ void __launch_bounds__(T::LOCK_THREADS_S, 1) pair_trie_kernel(const HolderArgs A) {
     constexpr int L = T::LOCK_THREADS_S;   // == blockDim.x
     f2_t* xs = reinterpret_cast<f2_t*>(mbx_dyn_smem) + threadIdx.x;
     f2_t* gs = xs + T::NVARS * L;
@@ -519,46 +557,48 @@ __global__ void __launch_bounds__(T::LOCK_THREADS_S, 1) holder_pair_kernel(const
         });
         return;
     }
-    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
     const long n = nmer_count(A);
+    const long cap = A.ps.cap;
     const long chunk = 2L * blockDim.x;
-    long static_next = blockIdx.x * chunk;
     for (;;) {
-        long base;
-        if (A.counter) {
-            if (threadIdx.x == 0) s_base = atomicAdd(A.counter, (int)chunk);
-            __syncthreads();
-            base = s_base;
-            __syncthreads();
-        } else {
-            base = static_next;
-            static_next += (long)gridDim.x * chunk;
-        }
+        if (threadIdx.x == 0) s_base = atomicAdd(A.counter, (int)chunk);
+        __syncthreads();
+        const long base = s_base;
+        __syncthreads();
         if (base >= n) break;
         const long t0 = base + threadIdx.x, t1 = t0 + blockDim.x;
-        bool live0, live1;
-        {
-            float lo[T::NVARS], hi[T::NVARS];
-            live0 = nmer_vars_f32<T>(A, t0, n, lo);
-            live1 = nmer_vars_f32<T>(A, t1, n, hi);
 #pragma unroll
-            for (int v = 0; v < T::NVARS; ++v) {
-                xs[v * L] = f2_pack(lo[v], hi[v]);
-                gs[v * L] = 0ull;
-            }
+        for (int v = 0; v < T::NVARS; ++v) {
+            const float lo = t0 < n ? A.ps.dx[v * cap + t0] : 0.0f;
+            const float hi = t1 < n ? A.ps.dx[v * cap + t1] : 0.0f;
+            xs[v * L] = f2_pack(lo, hi);
+            gs[v * L] = 0ull;
         }
         const double2 ep = T::template pip_s32_lock<L>(coef, xs, gs);
+        if (t0 < n) {
+#pragma unroll
+            for (int v = 0; v < T::NVARS; ++v) A.ps.g[v * cap + t0] = f2_lo(gs[v * L]);
+            A.ps.ep[t0] = coef.b0() + ep.x;
+        }
+        if (t1 < n) {
+#pragma unroll
+            for (int v = 0; v < T::NVARS; ++v) A.ps.g[v * cap + t1] = f2_hi(gs[v * L]);
+            A.ps.ep[t1] = coef.b0() + ep.y;
+        }
+    }
+}
+
+template <class T>
+__global__ void __launch_bounds__(128, 4) pair_finish_kernel(const HolderArgs A) {
+    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    const long n = nmer_count(A);
+    const long cap = A.ps.cap;
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
+        if (!A.ps.live[t]) continue;
         double g[T::NVARS];
-        if (live0) {
 #pragma unroll
-            for (int v = 0; v < T::NVARS; ++v) g[v] = (double)f2_lo(gs[v * L]);
-            finish_nmer<T>(A, t0, coef.b0() + ep.x, g, true, acc);
-        }
-        if (live1) {
-#pragma unroll
-            for (int v = 0; v < T::NVARS; ++v) g[v] = (double)f2_hi(gs[v * L]);
-            finish_nmer<T>(A, t1, coef.b0() + ep.y, g, true, acc);
-        }
+        for (int v = 0; v < T::NVARS; ++v) g[v] = (double)A.ps.g[v * cap + t];
+        finish_nmer<T>(A, t, A.ps.ep[t], g, true, acc);
     }
     block_reduce_add<7>(acc, A.out);
 }

@@ -305,6 +305,7 @@ struct mbx_ctx {
     DevBuf<int4> buckets, list;
     DevBuf<unsigned long long> listed;
     DeviceTables tables;   // per-device term tables and coefficients (shared, not owned)
+    DevBuf<unsigned char> pair_scratch;   // between the three mixed-precision kernels
     int nb_cap = 192;
     // runtime launch shapes of the builder (set by mbx_tune)
     struct Knobs {
@@ -435,6 +436,7 @@ int mbx_destroy(mbx_ctx* c) {
     if (c->prime_fork) cudaEventDestroy(c->prime_fork);
     if (c->prime_join) cudaEventDestroy(c->prime_join);
     if (c->child) mbx_destroy(c->child);
+    c->pair_scratch.release();
     c->buckets.release();
     c->list.release();
     c->listed.release();
@@ -875,11 +877,25 @@ static int launch_eval(mbx_ctx* c, const EvaluatorInfo* E, HolderArgs A, int fla
     const bool fp32 = mixed && !near && E->s && !(A.aos && E->split_r > 0);
     launch_fn fn = !grads ? E->e : fp32 ? E->s : E->g;
     if (!fn) return fail(c, MBX_ENOTSUP, std::string("no kernel for ") + E->name);
+    if (fn == E->s) {
+        // scratch of the three mixed-precision kernels for up to A.n n-mers
+        auto up = [](size_t b) { return (b + 255) & ~(size_t)255; };
+        const long cap = std::max<long>(A.n, 1);
+        const size_t vb = up((size_t)E->nvars * cap * sizeof(float));
+        const size_t eb = up((size_t)cap * sizeof(double));
+        CUCHK(c, c->pair_scratch.ensure(2 * vb + eb + up((size_t)cap)));
+        unsigned char* base = c->pair_scratch.p;
+        A.ps.dx = reinterpret_cast<float*>(base);
+        A.ps.g = reinterpret_cast<float*>(base + vb);
+        A.ps.ep = reinterpret_cast<double*>(base + 2 * vb);
+        A.ps.live = base + 2 * vb + eb;
+        A.ps.cap = cap;
+    }
     // persistent grid: a few resident blocks per SM, grid-stride over n-mers
     const long want = (A.n + block - 1) / block;
     const int grid = (int)std::max<long>(1, std::min<long>(want, (long)c->sm_count * 4));
     RCHK(c, fn(A, grid, block, c->stream));
-    ++*kernels;
+    *kernels += fn == E->s ? 3 : 1;   // the mixed path is three kernels
     return MBX_OK;
 }
 
