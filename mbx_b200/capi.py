@@ -8,6 +8,7 @@ present.
 """
 import ctypes
 import os
+import weakref
 
 import numpy as np
 
@@ -129,6 +130,10 @@ def _ptr(a):
     return a.data_ptr(), a.is_cuda
 
 
+# live contexts by handle (weak: a Context is closed when collected)
+_LIVE = weakref.WeakValueDictionary()
+
+
 class Context:
     """One CUDA stream and the device state of the 2b/3b path (mbx_ctx)."""
 
@@ -141,6 +146,16 @@ class Context:
         self.h = h
         self.device = device
         self.stream = stream or 0   # 0: a stream of the context's own
+        _LIVE[h.value] = self
+
+    @staticmethod
+    def from_handle(handle):
+        """The live Context whose mbx_ctx* is handle (torch.ops.mbxgpu ops take
+        the context by its handle)."""
+        c = _LIVE.get(int(handle))
+        if c is None or not getattr(c, "h", None):
+            raise MBXError(22, "no live context with handle %#x" % int(handle))
+        return c
 
     def _order(self, dev_ptrs):
         """Device arrays from torch: when the library runs on another stream
@@ -156,6 +171,7 @@ class Context:
 
     def close(self):
         if getattr(self, "h", None):
+            _LIVE.pop(self.h.value, None)
             lib().mbx_destroy(self.h)
             self.h = None
 

@@ -152,3 +152,86 @@ def system_energy(system, nbody, sites, virial=False):
     Note: like System::SetPBC, the call wraps the coordinates in place."""
     e, v = _SystemEnergy.apply(sites, system, nbody, virial)
     return (e, v) if virial else e
+
+
+# ---------------------------------------------------------------------------
+# Registered torch operators (torch.ops.mbxgpu.*): the same CUDA kernels as
+# dispatcher ops, usable from TorchScript-free graphs and by name from C++
+# torch code.  A context is passed by its handle (capi.Context.h.value).
+
+@torch.library.custom_op("mbxgpu::energy_2b3b", mutates_args=())
+def _op_energy_2b3b(sites: torch.Tensor, handle: int, mixed: bool) -> tuple[torch.Tensor, torch.Tensor,
+                                                                             torch.Tensor, torch.Tensor]:
+    """Get2B and Get3B of a context's system on device site coordinates
+    (System::TwoBodyEnergy/ThreeBodyEnergy): (E2B, E3B, dE/dsites of both
+    terms, virial[9]).  The coordinates are not modified (the op works on a
+    copy, wrapped as SetPBC does)."""
+    c = capi.Context.from_handle(handle)
+    x = sites.detach().clone().contiguous()
+    g = torch.zeros_like(x)
+    vir = np.zeros(9)
+    e2, e3 = c.energy_2b3b(x, g, vir, mixed=mixed)
+    dev = sites.device
+    return (torch.tensor(e2, dtype=torch.float64, device=dev), torch.tensor(e3, dtype=torch.float64, device=dev), g,
+            torch.tensor(vir, dtype=torch.float64, device=dev))
+
+
+@_op_energy_2b3b.register_fake
+def _(sites, handle, mixed):
+    s = sites.new_empty(())
+    return s, sites.new_empty(()), torch.empty_like(sites), sites.new_empty(9)
+
+
+@torch.library.custom_op("mbxgpu::nmer_energies", mutates_args=())
+def _op_nmer_energies(xyz: torch.Tensor, coef: torch.Tensor, name: str, mixed: bool) -> torch.Tensor:
+    """Switched energy of every n-mer (evaluator calling convention, AoS
+    coordinates already imaged), energy-only kernel."""
+    c = context(xyz.device.index)
+    c.set_coefficients(name, coef.contiguous())
+    x = xyz.contiguous()
+    e = torch.empty(x.shape[0], dtype=torch.float64, device=x.device)
+    c.evaluate(name, x, None, None, e, mixed=mixed, grads=False)
+    return e
+
+
+@_op_nmer_energies.register_fake
+def _(xyz, coef, name, mixed):
+    return xyz.new_empty(xyz.shape[0])
+
+
+@torch.library.custom_op("mbxgpu::nmer_energies_backward", mutates_args=())
+def _op_nmer_energies_backward(ge: torch.Tensor, xyz: torch.Tensor, coef: torch.Tensor, name: str,
+                               mixed: bool) -> tuple[torch.Tensor, torch.Tensor]:
+    """Reverse pass of mbxgpu::nmer_energies: (dL/dxyz, dL/dcoef) for upstream
+    dL/dE_n = ge, from the gradient kernel and the coefficient adjoint kernel
+    (monomials recomputed from the coordinates)."""
+    c = context(xyz.device.index)
+    c.set_coefficients(name, coef.contiguous())
+    x = xyz.contiguous()
+    g = torch.zeros_like(x)
+    c.evaluate(name, x, g, None, None, mixed=mixed, grads=True)
+    dcoef = torch.zeros_like(coef)
+    c.evaluate_dcoef(name, x, ge.contiguous(), dcoef)
+    return g * ge[:, None], dcoef
+
+
+@_op_nmer_energies_backward.register_fake
+def _(ge, xyz, coef, name, mixed):
+    return torch.empty_like(xyz), torch.empty_like(coef)
+
+
+def _nmer_setup(ctx, inputs, output):
+    xyz, coef, name, mixed = inputs
+    ctx.save_for_backward(xyz, coef)
+    ctx.name = name
+    ctx.mixed = mixed
+
+
+def _nmer_backward(ctx, ge):
+    _no_second_derivative()
+    xyz, coef = ctx.saved_tensors
+    dxyz, dcoef = torch.ops.mbxgpu.nmer_energies_backward(ge, xyz, coef, ctx.name, ctx.mixed)
+    return dxyz, dcoef, None, None
+
+
+torch.library.register_autograd("mbxgpu::nmer_energies", _nmer_backward, setup_context=_nmer_setup)

@@ -156,3 +156,36 @@ def test_system_energy_backward_recomputes():
     s2.grad = g
     np.testing.assert_allclose(s2.GetRealGrads(), g_ref, rtol=0, atol=1e-8)
     np.testing.assert_allclose(v.cpu().numpy(), v_ref, rtol=1e-10, atol=1e-8)
+
+
+def test_registered_torch_ops():
+    """torch.ops.mbxgpu.* (torch.library custom ops): energy_2b3b against the
+    System path, nmer_energies with its registered autograd against the
+    autograd.Function path."""
+    from mbx_b200 import capi, system as msys, torch_ops
+    ids, xyz, box = workloads.water_256(0)
+    a = msys.from_arrays(ids, xyz, box, 9.0, 7.0)
+    e2, e3 = a.TwoAndThreeBodyEnergy(True)
+    g_ref = np.asarray(a.GetGrads())
+    ctx = capi.Context(0)
+    b = msys.from_arrays(ids, xyz, box, 9.0, 7.0, context=ctx)
+    sites = torch.tensor(b.sites, device="cuda")
+    s0 = sites.clone()
+    o2, o3, g, v = torch.ops.mbxgpu.energy_2b3b(sites, ctx.h.value, False)
+    assert torch.equal(sites, s0)
+    assert abs(float(o2) - e2) < 1e-10 * abs(e2) and abs(float(o3) - e3) < 1e-10 * abs(e3)
+    np.testing.assert_allclose(g.cpu().numpy(), g_ref, rtol=0, atol=1e-9)
+    np.testing.assert_allclose(v.cpu().numpy(), a.GetVirial(), rtol=1e-10, atol=1e-8)
+    # nmer_energies as a registered op with autograd
+    x = torch.tensor(workloads.gas_trimers(32, seed=8), device="cuda", requires_grad=True)
+    coef = torch_ops.fitted_coefficients("mbpol3b").requires_grad_(True)
+    e = torch.ops.mbxgpu.nmer_energies(x, coef, "mbpol3b", False)
+    (e * torch.linspace(0.5, 1.5, 32, dtype=torch.float64, device="cuda")).sum().backward()
+    x2 = x.detach().clone().requires_grad_(True)
+    c2 = coef.detach().clone().requires_grad_(True)
+    e_ref = torch_ops.nmer_energies("mbpol3b", x2, c2)
+    (e_ref * torch.linspace(0.5, 1.5, 32, dtype=torch.float64, device="cuda")).sum().backward()
+    np.testing.assert_allclose(e.detach().cpu().numpy(), e_ref.detach().cpu().numpy(), rtol=0, atol=1e-12)
+    np.testing.assert_allclose(x.grad.cpu().numpy(), x2.grad.cpu().numpy(), rtol=0, atol=1e-12)
+    np.testing.assert_allclose(coef.grad.cpu().numpy(), c2.grad.cpu().numpy(), rtol=1e-12, atol=1e-12)
+    ctx.close()

@@ -37,3 +37,22 @@ def test_nmers_to_input_canonical():
     nm = np.array([[2, 0], [1, 0]])
     out = t.nmers_to_input(nm)
     assert out.tolist() == sorted(out.tolist())
+
+
+def test_registered_torch_ops_shapes():
+    """torch.ops.mbxgpu.* are registered at import and their fake (meta)
+    implementations give the shapes of the CUDA ones, so graph capture and
+    tracing see the right outputs without a GPU."""
+    import torch
+    from torch._subclasses.fake_tensor import FakeTensorMode
+    from mbx_b200 import torch_ops  # noqa: F401  (registers the ops)
+    with FakeTensorMode():
+        s = torch.empty(100, 3, dtype=torch.float64)
+        e2, e3, g, v = torch.ops.mbxgpu.energy_2b3b(s, 0, False)
+        assert (e2.shape, e3.shape, g.shape, v.shape) == ((), (), (100, 3), (9,))
+        x = torch.empty(32, 27, dtype=torch.float64)
+        c = torch.empty(1163, dtype=torch.float64)
+        e = torch.ops.mbxgpu.nmer_energies(x, c, "mbpol3b", False)
+        assert e.shape == (32,) and e.dtype == torch.float64
+        gx, gc = torch.ops.mbxgpu.nmer_energies_backward(e, x, c, "mbpol3b", False)
+        assert gx.shape == x.shape and gc.shape == c.shape
