@@ -14,8 +14,10 @@ n-mers (dimers within 9 A + trimers by the reference's AddClusters rule within
 * e2e: the same through the public API (mbx_b200.system.System,
   TwoAndThreeBodyEnergy) with pinned host buffers, host<->device copies
   inside, wall clock per step;
-* mixed: the FP32-monomial / FP64-accumulate path, its throughput and its
-  energy error against the FP64 path;
+* mixed: MB-pol 3b on the tensor cores (the shifted-basis polynomial as a
+  quadratic form, FP16 split operands, FP32 accumulation; variables, chain
+  rule and sums FP64), its throughput and its energy and force errors
+  against the FP64 path;
 * roofline: the MB-pol 3b evaluation kernel launched alone (3b-only calls,
   L2 flushed), algorithmic flops counted from the reference's gradient
   program (mbx_b200/data/flops.json) over its CUDA-event duration, against
@@ -240,7 +242,8 @@ def batched_leg(args, local, flush, fp64_value, dist=None, world=1):
             "value": replicas.throughput(units, ms, world), "unit": "n-mers/s", "ms_per_step": ms,
             "units_per_step": {"dimers": listed2, "trimers": listed3, "evaluated_dimers": eval2,
                                "evaluated_trimers": eval3},
-            "dtype": "mixed (3b paired f32 over a shifted basis; 2b f64)", "cuda_graph": True,
+            "dtype": "mixed (3b: quadratic form over a shifted basis on the tensor cores, FP16 split operands, "
+                     "FP32 accumulation; 2b f64)", "cuda_graph": True,
             "timing": "CUDA events on the bench's stream around the gradient reset and the graph replay of "
                       "both terms (the library runs on that stream), L2 flushed before each step",
             "autotuned": tuned,
@@ -463,7 +466,8 @@ def main():
     if not args.no_mixed:
         g3_64, g3_mx = g64 - g2_64, gmx - g2_mx
         out["mixed"] = {"value": world * units / (ms_mx * 1e-3), "ms_per_step": ms_mx,
-                        "dtype": "3b: paired f32 trie over a shifted basis, f64 variables, switch, chain rule "
+                        "dtype": "3b: quadratic form over a shifted FP32 basis on the tensor cores (tcgen05, FP16 "
+                                 "split operands, FP32 accumulation), f64 variables, switch, chain rule "
                                  "and sums; 2b: f64",
                         "error_vs": "FP64 path of the same run (within 1e-10 of the reference)",
                         "rel_err_E2B": abs(e2_mx - e2_64) / abs(e2_64), "rel_err_E3B": abs(e3_mx - e3_64) / abs(e3_64),
@@ -475,7 +479,7 @@ def main():
                         "speedup_vs_fp64": ms / ms_mx}
         kmx = sum(evmx) / len(evmx)
         amx = eval3 * flops["mbpol3b"]["flops"] / (kmx * 1e-3) / 1e12
-        out["mixed"]["roofline_3b"] = {"kernel": "pair_vars_kernel + pair_trie_kernel<mbpol3b_T, mbpol3b_CS> + "
+        out["mixed"]["roofline_3b"] = {"kernel": "pair_vars_kernel + qf_eval_kernel<mbpol3b_T, mbpol3b_Q> + "
                                                  "pair_finish_kernel (one evaluation, events around all three)",
                                        "kernel_ms": kmx,
                                        "achieved": amx, "unit": "TFLOP/s (reference flops)",

@@ -135,6 +135,18 @@ int mbx_evaluate_dcoef(mbx_ctx* ctx, const char* evaluator, long n, const double
  * current ones (mbx_set_coefficients). */
 int mbx_poly(mbx_ctx* ctx, const char* evaluator, long nd, const double* x, double* g, double* e, int flags);
 
+/* Operands of the tensor-core kernel of the mixed mode (MBX_MIXED) for the
+ * evaluators that have one ("mbpol3b"): the polynomial in the FP32 basis as a
+ * quadratic form m^T C m over a basis of monomials of degree <= 2, C scaled
+ * by powers of two and split into FP16 parts in the kernel's shared-memory
+ * layout.  Host only (no device needed): *image_bytes and *nb get the image
+ * size and the padded basis size; with image, colf and b0 non-NULL the image,
+ * the nb per-column factors and the constant term are written for the
+ * coefficients coef (ncoef doubles; NULL: the fitted ones), exactly as
+ * mbx_set_coefficients uploads them.  MBX_ENOTSUP for other evaluators. */
+int mbx_qf_image(const char* evaluator, const double* coef, long* image_bytes, int* nb, unsigned char* image,
+                 float* colf, double* b0);
+
 /* Replace the linear coefficients of an evaluator (ncoef doubles; NULL
  * restores the fitted ones).  Coefficients are per device, not per context:
  * they live in the kernels' constant memory and in one global-memory copy

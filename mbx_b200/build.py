@@ -34,7 +34,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
          "-I" + os.path.join(ROOT, "include"), "-I" + CSRC]
 HAND = ("mbx_capi.cu", "nmer_build.cu", "peaks.cu", "noalloc.cu", "table_kernels.cu", "onebody.cu")
-HEADERS = ("holder_common.cuh", "holder_kernel.cuh", "term_table.cuh", "launch_cache.cuh", "device_state.h")
+HEADERS = ("holder_common.cuh", "holder_kernel.cuh", "term_table.cuh", "launch_cache.cuh", "device_state.h",
+           "qf_kernel.cuh")
 
 
 def deps(src):
@@ -45,8 +46,7 @@ def deps(src):
     if os.path.dirname(src) == GEN:
         name, v = base[:-3].rsplit("_", 1)
         common.append(os.path.join(GEN, name + ".cuh"))
-        variant = {"g": "pip", "e": "pip_e", "s": "pip_s32"}.get(v)
-        if variant:
+        for variant in {"g": ("pip",), "e": ("pip_e",), "s": ("pip_s32", "qf")}.get(v, ()):
             common.append(os.path.join(GEN, "%s_%s.cuh" % (name, variant)))
     else:
         common += [os.path.join(CSRC, "nmer_build.h"), os.path.join(ROOT, "include", "mbx_b200.h"),

@@ -87,6 +87,7 @@ def lib():
                                         ctypes.POINTER(ctypes.c_double), ctypes.c_int]
     L.mbx_get_knobs.argtypes = [vp, ctypes.c_int, ip]
     L.mbx_set_knobs.argtypes = [vp, ctypes.c_int, ip]
+    L.mbx_qf_image.argtypes = [ctypes.c_char_p, dp, lp, ip, ctypes.c_void_p, ctypes.POINTER(ctypes.c_float), dp]
     _lib = L
     return L
 
@@ -95,7 +96,7 @@ EXPORTED = ("mbx_create", "mbx_destroy", "mbx_last_error", "mbx_version", "mbx_s
             "mbx_energy", "mbx_last_counts", "mbx_nmers", "mbx_evaluate", "mbx_evaluate_dcoef", "mbx_poly",
             "mbx_set_coefficients", "mbx_evaluator_info", "mbx_last_timing", "mbx_fma_peaks", "mbx_set_batch",
             "mbx_batch_energy", "mbx_tune", "mbx_get_knobs", "mbx_set_knobs", "mbx_energy_2b3b",
-            "mbx_batch_energy_2b3b", "mbx_set_ignore_1b", "mbx_set_real_order", "mbx_energy_real")
+            "mbx_batch_energy_2b3b", "mbx_set_ignore_1b", "mbx_set_real_order", "mbx_energy_real", "mbx_qf_image")
 
 KNOBS = ("nb_warps", "nb_unroll", "tri_threads", "dim_threads")
 
@@ -106,6 +107,26 @@ def evaluator_info(name):
                                 ctypes.byref(nc)) != 0:
         raise MBXError(95, "unknown evaluator %s" % name)
     return nb.value, nr.value, nv.value, nc.value
+
+
+def qf_image(name, coef=None):
+    """Host-built operands of the tensor-core mixed kernel (mbx_qf_image): the
+    B image (bytes), the per-column factors (float32) and the constant term,
+    for coefficients coef (None: the fitted ones).  No device needed."""
+    nbytes, nb = ctypes.c_long(), ctypes.c_int()
+    r = lib().mbx_qf_image(name.encode(), None, ctypes.byref(nbytes), ctypes.byref(nb), None, None, None)
+    if r:
+        raise RuntimeError("mbx_qf_image(%s): %d" % (name, r))
+    img = np.zeros(nbytes.value, np.uint8)
+    colf = np.zeros(nb.value, np.float32)
+    b0 = ctypes.c_double()
+    c = None if coef is None else np.ascontiguousarray(coef, np.float64)
+    r = lib().mbx_qf_image(name.encode(), None if c is None else c.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                           ctypes.byref(nbytes), ctypes.byref(nb), img.ctypes.data,
+                           colf.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), ctypes.byref(b0))
+    if r:
+        raise RuntimeError("mbx_qf_image(%s): %d" % (name, r))
+    return img.tobytes(), colf, b0.value
 
 
 def fma_peaks(device=0):

@@ -108,6 +108,10 @@ ACC_CHAINS = 1
 # 2048-water box is off by 1.1e-5 even with the dimers below 4.5 A in FP64
 # (the shifted basis does not condition it either).
 SHIFT_TYPES = {"mbpol3b": "median"}
+# Types of SHIFT_TYPES whose mixed kernel is the quadratic form on the tensor
+# cores (codegen/qf.py, csrc/qf_kernel.cuh) instead of the paired FP32 trie:
+# MB-pol 3b, 442 products of degree 2 in the basis (data/mbpol3b.qf.json).
+QF_TYPES = {"mbpol3b"}
 # Optional: n-mers whose first-atom distance is below this radius (A) run the
 # FP64 kernel in the mixed mode (a type of SHIFT_TYPES whose short-range
 # n-mers cancel too strongly for FP32); the builder puts them in a bucket of
@@ -574,6 +578,7 @@ def emit_traits(spec, table, straight, out):
     if shifted_type:
         w("    __device__ __forceinline__ static void shift(const double (&x)[%d], float (&xf)[%d]) "
           "{ %s_shift(x, xf); }" % (spec.nvars, spec.nvars, n))
+    if shifted_type and n not in QF_TYPES:
         w("    template <int S, class C> __device__ __forceinline__ static double2 pip_s32_lock(const C& c, "
           "const f2_t* __restrict__ x, f2_t* __restrict__ g) { return %s_pip_s32_lock<S>(c, x, g); }" % n)
         w("    template <int S, class C> __device__ __forceinline__ static double2 pip_s32_piece(int k, const C& c, "
@@ -639,10 +644,11 @@ def generate(name):
                 "const double* __restrict__);" % name]
         if name in SHIFT_TYPES:
             sp = shifted_pip(name)
-            out.append("template <int S, class Coef> __device__ __forceinline__ double2 %s_pip_s32_lock(const Coef&, "
-                       "const f2_t* __restrict__, f2_t* __restrict__);" % name)
-            out.append("template <int S, class Coef> __device__ __forceinline__ double2 %s_pip_s32_piece(int, "
-                       "const Coef&, const f2_t* __restrict__, f2_t* __restrict__);" % name)
+            if name not in QF_TYPES:
+                out.append("template <int S, class Coef> __device__ __forceinline__ double2 %s_pip_s32_lock("
+                           "const Coef&, const f2_t* __restrict__, f2_t* __restrict__);" % name)
+                out.append("template <int S, class Coef> __device__ __forceinline__ double2 %s_pip_s32_piece(int, "
+                           "const Coef&, const f2_t* __restrict__, f2_t* __restrict__);" % name)
             out.append("// dx = x - x0, the reference point of the FP32 basis (%s)" % SHIFT_TYPES[name])
             out.append("__device__ __forceinline__ void %s_shift(const double (&x)[%d], float (&xf)[%d]) {" %
                        (name, nv, nv))
@@ -670,7 +676,11 @@ def generate(name):
                             (ctab.nterms, len(perms), table.nterms))
             emitter(arg, nv, "%s_%s" % (name, suffix), body, nparts, perms=perms)
             write_if_changed(os.path.join(OUT, "%s_%s.cuh" % (name, suffix)), "\n".join(body) + "\n")
-        if name in SHIFT_TYPES:
+        if name in QF_TYPES:
+            from mbx_b200.codegen import qf
+            write_if_changed(os.path.join(OUT, "%s_qf.cuh" % name),
+                             qf.emit_cuda(qf.QuadForm(name, shifted_pip(name)), name, nv))
+        elif name in SHIFT_TYPES:
             from mbx_b200.codegen.shift import ShiftedTable
             sp = shifted_pip(name)
             body = head + ["#pragma once", '#include "%s.cuh"' % name,
@@ -969,6 +979,185 @@ int mbx_prime_%(name)s_s(cudaStream_t s) {
 """
 
 
+QF_TU = """// Generated by mbx_b200/codegen/gen_kernels.py -- do not edit.
+// Mixed-precision evaluation of the %(name)s polynomial on the tensor cores
+// (quadratic form over the %(basis)s FP32 basis, csrc/qf_kernel.cuh).
+#include <cmath>
+#include <cstring>
+#include <vector>
+#include "../holder_kernel.cuh"
+#include "../launch_cache.cuh"
+#include "%(name)s.cuh"
+#include "%(name)s_qf.cuh"
+
+// b = F a: the basis coefficients are linear in the fitted ones.  Row j of F
+// (entries sF_row[j] .. sF_row[j+1]) lists (k, factor); sF0 is the constant.
+static const int sF_row_%(name)s[%(norb1)d] = {%(rows)s};
+static const int sF_k_%(name)s[%(nnz)d] = {%(ks)s};
+static const double sF_f_%(name)s[%(nnz)d] = {%(fs)s};
+static const int sF0_k_%(name)s[%(nnz0)d] = {%(k0)s};
+static const double sF0_f_%(name)s[%(nnz0)d] = {%(f0)s};
+%(tables)s
+// IEEE binary16 of x, rounded to nearest even (subnormals kept; |x| < 65504 here)
+static unsigned short qf_half(double x) {
+    const unsigned short sign = std::signbit(x) ? 0x8000 : 0;
+    const double a = std::fabs(x);
+    if (a == 0.0) return sign;
+    int e;
+    const double f = std::frexp(a, &e);   // a = f 2^e, f in [0.5, 1)
+    if (e >= -13) {                        // normal: a >= 2^-14
+        double m = std::nearbyint(std::ldexp(f, 11));
+        if (m == 2048.0) {
+            m = 1024.0;
+            ++e;
+        }
+        return (unsigned short)(sign | ((e + 14) << 10) | ((int)m - 1024));
+    }
+    return (unsigned short)(sign | (int)std::nearbyint(std::ldexp(a, 24)));   // subnormal: m 2^-24
+}
+
+static double qf_half_value(unsigned short h) {
+    const int e = (h >> 10) & 0x1f, m = h & 0x3ff;
+    const double v = e ? std::ldexp(1024.0 + m, e - 25) : std::ldexp((double)m, -24);
+    return (h & 0x8000) ? -v : v;
+}
+
+// The tensor-core operands for fitted coefficients a: the C' image in the
+// kernel's layout (%(name)s_Q::IMAGE_BYTES bytes), the column factors
+// 2^-(s_j + t_j) (NB floats) and the constant term.  Host only.
+int mbx_qf_image_%(name)s(const double* a, unsigned char* img, float* colf, double* b0_out) {
+    constexpr int NB = %(name)s_Q::NB;
+    std::vector<double> b(%(norb)d);
+    for (int j = 0; j < %(norb)d; ++j) {
+        double acc = 0.0;
+        for (int q = sF_row_%(name)s[j]; q < sF_row_%(name)s[j + 1]; ++q) acc += sF_f_%(name)s[q] * a[sF_k_%(name)s[q]];
+        b[j] = acc;
+    }
+    double b0 = 0.0;
+    for (int q = 0; q < %(nnz0)d; ++q) b0 += sF0_f_%(name)s[q] * a[sF0_k_%(name)s[q]];
+    *b0_out = b0;
+    // C (symmetric), then C' = D C D, D = diag(2^t)
+    std::vector<double> C((size_t)NB * NB, 0.0);
+    for (int q = 0; q < qf_nmono_%(name)s; ++q) {
+        const int i = qf_mi_%(name)s[q], j = qf_mj_%(name)s[q];
+        const double c = b[qf_mo_%(name)s[q]];
+        if (i == j) {
+            C[(size_t)i * NB + i] += c;
+        } else {
+            C[(size_t)i * NB + j] += 0.5 * c;
+            C[(size_t)j * NB + i] += 0.5 * c;
+        }
+    }
+    for (int i = 0; i < NB; ++i)
+        for (int j = 0; j < NB; ++j) C[(size_t)i * NB + j] = std::ldexp(C[(size_t)i * NB + j], qf_t_%(name)s[i] + qf_t_%(name)s[j]);
+    // column exponents: largest |C'_ij 2^s_j| of a column below 2^14
+    std::vector<int> sj(NB, 0);
+    for (int j = 0; j < NB; ++j) {
+        double m = 0.0;
+        for (int i = 0; i < NB; ++i) m = std::fmax(m, std::fabs(C[(size_t)i * NB + j]));
+        if (m > 0.0) {
+            int e;
+            std::frexp(m, &e);        // floor(log2 m) = e - 1
+            sj[j] = 14 - e;
+        }
+        colf[j] = (float)std::ldexp(1.0, -(sj[j] + qf_t_%(name)s[j]));
+    }
+    // K block s, N half hf (columns 240 hf ..): B[n][k] = C'_kn 2^s_n in hi,
+    // mid[, lo] FP16 parts of 240 rows x 16, core matrix (n' / 8, k / 8) of a
+    // part at (n' / 8) 256 + (k / 8) 128, row n' %% 8 at 16 (n' %% 8), n' = n - 240 hf
+    memset(img, 0, (size_t)%(name)s_Q::IMAGE_BYTES);
+    for (int s = 0; s < %(name)s_Q::KS; ++s) {
+        const int parts = s < %(name)s_Q::KT ? 3 : 2;
+        for (int n = 0; n < NB; ++n) {
+            const int hf = n / (NB / 2), nn = n - hf * (NB / 2);
+            unsigned char* st = img + %(name)s_Q::chunk_offset(s, hf);
+            for (int kk = 0; kk < 16; ++kk) {
+                const int k = 16 * s + kk;
+                double x = std::ldexp(C[(size_t)k * NB + n], sj[n]);
+                const size_t off = (size_t)(nn / 8) * 256 + (kk / 8) * 128 + (nn %% 8) * 16 + (kk %% 8) * 2;
+                for (int p = 0; p < parts; ++p) {
+                    const unsigned short h = qf_half(x);
+                    memcpy(st + (size_t)p * (NB / 2) * 32 + off, &h, 2);
+                    x -= qf_half_value(h);
+                }
+            }
+        }
+    }
+    return 0;
+}
+
+int mbx_set_coef_%(name)s_s(const double* a, int from_device, cudaStream_t s) {
+    std::vector<double> h(%(ncoef)d);
+    cudaError_t e = cudaSuccess;
+    if (from_device) {
+        e = cudaMemcpyAsync(h.data(), a, sizeof(double) * %(ncoef)d, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return (int)e;
+    } else {
+        for (int k = 0; k < %(ncoef)d; ++k) h[k] = a[k];
+    }
+    std::vector<unsigned char> img((size_t)%(name)s_Q::IMAGE_BYTES);
+    std::vector<float> colf(%(name)s_Q::NB);
+    double b0 = 0.0;
+    mbx_qf_image_%(name)s(h.data(), img.data(), colf.data(), &b0);
+    e = cudaMemcpyToSymbolAsync(qf_img_%(name)s, img.data(), img.size(), 0, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyToSymbolAsync(qf_colf_%(name)s, colf.data(), sizeof(float) * colf.size(), 0,
+                                    cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyToSymbolAsync(qf_b0_%(name)s, &b0, sizeof(double), 0, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    return (int)e;
+}
+
+int mbx_launch_%(name)s_s(const HolderArgs& A, int grid, int block, cudaStream_t s) {
+    // three kernels: the FP64 variables shifted to the FP32 basis at full
+    // occupancy (pair_vars_kernel), the quadratic form on the tensor cores
+    // (qf_eval_kernel: one CTA per SM, persistent over tiles of 128 n-mers),
+    // the FP64 chain rule and sums at full occupancy (pair_finish_kernel);
+    // A.ps holds the scratch between them (capacity A.ps.cap >= A.n)
+    if (!A.ps.dx || A.ps.cap < A.n) return (int)cudaErrorInvalidValue;
+    auto kern = qf_eval_kernel<%(name)s_T, %(name)s_Q>;
+    static LaunchCache lc;
+    int sms = 0, bps = 0;
+    const int r = launch_facts(lc, kern, qf::THREADS, qf::SMEM, qf::SMEM, &sms, &bps);
+    if (r) return r;
+    const long wide = (long)sms * 16;
+    const long gv = (A.n + 255) / 256, gf = (A.n + 127) / 128;
+    pair_vars_kernel<%(name)s_T><<<(int)(gv < wide ? (gv > 0 ? gv : 1) : wide), 256, 0, s>>>(A);
+    const long tiles = (A.n + 127) / 128;
+    grid = (int)(tiles < (long)sms ? (tiles > 0 ? tiles : 1) : sms);
+    kern<<<grid, qf::THREADS, qf::SMEM, s>>>(A);
+    pair_finish_kernel<%(name)s_T><<<(int)(gf < wide ? (gf > 0 ? gf : 1) : wide), 128, 0, s>>>(A);
+    return (int)cudaGetLastError();
+}
+
+int mbx_prime_%(name)s_s(cudaStream_t) {
+    return 0;   // the tensor-core kernel's code is small: nothing to prefetch
+}
+"""
+
+
+def write_qf_tu(name, path):
+    from mbx_b200.codegen import qf
+    sp = shifted_pip(name)
+    q = qf.QuadForm(name, sp)
+    rows, ks, fs = [0], [], []
+    for row in sp.F:
+        for k, f in sorted(row.items()):
+            ks.append(k)
+            fs.append(f)
+        rows.append(len(ks))
+    k0 = sorted(sp.const_F)
+    d = {"name": name, "basis": SHIFT_TYPES[name], "norb": sp.norb, "norb1": sp.norb + 1,
+         "ncoef": SPECS[name].ncoef, "nnz": len(ks), "nnz0": max(1, len(k0)),
+         "rows": ",".join(map(str, rows)), "ks": ",".join(map(str, ks)),
+         "fs": ",".join(repr(float(f)) for f in fs),
+         "k0": ",".join(map(str, k0)) if k0 else "0",
+         "f0": ",".join(repr(float(sp.const_F[k])) for k in k0) if k0 else "0.0",
+         "tables": qf.emit_host_tables(q, name)}
+    write_tu(path, QF_TU % d)
+
+
 def write_shift_tu(name, path):
     sp = shifted_pip(name)
     rows, ks, fs = [0], [], []
@@ -1009,7 +1198,10 @@ def write_kernels_cu(name):
             continue   # part of the table unit
         if v == "s":
             path = os.path.join(OUT, "%s_s.cu" % name)
-            write_shift_tu(name, path)
+            if name in QF_TYPES:
+                write_qf_tu(name, path)
+            else:
+                write_shift_tu(name, path)
             paths.append(path)
             continue
         path = os.path.join(OUT, "%s_%s.cu" % (name, v))
@@ -1215,6 +1407,18 @@ def write_registry():
                       names.index(kern)))
     lines.append("};")
     lines.append("static const int mbx_num_evaluators = %d;" % len(SPECS))
+    # host builders of the tensor-core operands of the mixed mode (QF_TYPES)
+    from mbx_b200.codegen import qf as qfmod
+    lines.append("struct QfInfo { const char* name; long image_bytes; int nb; "
+                 "int (*build)(const double*, unsigned char*, float*, double*); };")
+    for name in sorted(QF_TYPES):
+        lines.append("int mbx_qf_image_%s(const double* a, unsigned char* img, float* colf, double* b0);" % name)
+    lines.append("static const QfInfo mbx_qf_types[] = {")
+    for name in sorted(QF_TYPES):
+        q = qfmod.QuadForm(name, shifted_pip(name))
+        lines.append('    {"%s", %dL, %d, mbx_qf_image_%s},' % (name, qfmod.image_bytes(q), q.npad, name))
+    lines.append("};")
+    lines.append("static const int mbx_num_qf_types = %d;" % len(QF_TYPES))
     # 1-body evaluators (table-driven), by monomer id
     from mbx_b200.specs import ONEBODY_DISPATCH
     lines.append("struct OneBodyInfo { const char* name; const char* mon; int ncoef; const double* fit; int table; "
@@ -1258,7 +1462,7 @@ def main(argv=None, quiet=False):
         path, leaves, inner = generate(n)
         keep.add(os.path.basename(path))
         if n in STRAIGHT_TYPES:
-            for v in ("pip", "pip_e", "pip_s32"):
+            for v in ("pip", "pip_e", "qf" if n in QF_TYPES else "pip_s32"):
                 keep.add("%s_%s.cuh" % (n, v))
         keep.update(os.path.basename(p) for p in write_kernels_cu(n))
         if not quiet:

@@ -36,6 +36,7 @@ struct PairScratch {
     double* ep;
     unsigned char* live;
     long cap;
+    int* err;   // status word: kernels that wait on barriers report a timeout here (bit 8)
 };
 
 struct HolderArgs {

@@ -890,6 +890,7 @@ static int launch_eval(mbx_ctx* c, const EvaluatorInfo* E, HolderArgs A, int fla
         A.ps.ep = reinterpret_cast<double*>(base + 2 * vb);
         A.ps.live = base + 2 * vb + eb;
         A.ps.cap = cap;
+        A.ps.err = c->status.p;   // status word: MBX_STATUS_WAIT_TIMEOUT
     }
     // persistent grid: a few resident blocks per SM, grid-stride over n-mers
     const long want = (A.n + block - 1) / block;
@@ -971,13 +972,16 @@ static int term_enqueue(mbx_ctx* c, int nbody, int use_ghost, double* X, double*
 
 // After the stream of a term_enqueue has completed: 1 when the build did not
 // fit its buffers (capacities grown; the evaluators saw the status word and
-// added nothing: enqueue again), else 0 with the energy, the virial (+=),
-// the counts and the timing recorded.
+// added nothing: enqueue again), a negative value when a kernel reported a
+// timeout (error set), else 0 with the energy, the virial (+=), the counts
+// and the timing recorded.
 static int term_finish(mbx_ctx* c, int nbody, double* energy, double* virial, int kernels) {
     int status[2];
     memcpy(status, c->h_out + MBX_H_STATUS, sizeof(status));
     int counts[MBX_MAX_BUCKETS];
     memcpy(counts, c->h_out + MBX_H_COUNTS, sizeof(counts));
+    if (status[0] & MBX_STATUS_WAIT_TIMEOUT)
+        return -fail(c, MBX_ECUDA, "an evaluation kernel's barrier wait timed out (results discarded)");
     if (status[0]) {
         if (status[0] & MBX_STATUS_NB_OVERFLOW) c->nb_cap = std::max(c->nb_cap * 2, status[1] + 32);
         for (int b = 0; b < c->nbucket[nbody]; ++b)
@@ -1252,7 +1256,9 @@ extern "C" int mbx_energy(mbx_ctx* c, int nbody, double* xyz, int use_ghost, dou
         r = term_enqueue(c, nbody, use_ghost, X, G, flags, &kernels);
         if (r) return r;
         CUCHK(c, cudaStreamSynchronize(c->stream));
-        if (term_finish(c, nbody, energy, virial, kernels) == 0) return unstage_term_io(c, xyz, grad, flags, X, G);
+        const int f = term_finish(c, nbody, energy, virial, kernels);
+        if (f < 0) return MBX_ECUDA;
+        if (f == 0) return unstage_term_io(c, xyz, grad, flags, X, G);
         kernels = 0;
     }
     return fail(c, MBX_ECUDA, "n-mer buffers did not converge");
@@ -1317,6 +1323,8 @@ extern "C" int mbx_energy_2b3b(mbx_ctx* c, double* xyz, int use_ghost, double* e
     CUCHK(c, cudaStreamSynchronize(c->stream));
     int again3 = term_finish(c, 3, e3, virial, kernels);
     int again2 = term_finish(k, 2, e2, virial, kk);
+    if (again3 < 0) return MBX_ECUDA;
+    if (again2 < 0) return fail(c, MBX_ECUDA, std::string("2b term: ") + k->err);
     // a term whose n-mers did not fit its buffers added nothing: run it again
     for (int attempt = 0; (again2 || again3) && attempt < 4; ++attempt) {
         if (again3) {
@@ -1335,6 +1343,8 @@ extern "C" int mbx_energy_2b3b(mbx_ctx* c, double* xyz, int use_ghost, double* e
         CUCHK(c, cudaStreamSynchronize(c->stream));
         if (again3) again3 = term_finish(c, 3, e3, virial, kernels);
         if (again2) again2 = term_finish(k, 2, e2, virial, kk);
+        if (again3 < 0) return MBX_ECUDA;
+        if (again2 < 0) return fail(c, MBX_ECUDA, std::string("2b term: ") + k->err);
     }
     if (again2 || again3) return fail(c, MBX_ECUDA, "n-mer buffers did not converge");
     c->last_listed[2] = k->last_listed[2];
@@ -1466,6 +1476,7 @@ extern "C" int mbx_evaluate(mbx_ctx* c, const char* name, long n, const double* 
     A.out = c->out.p;
     A.e_per = EP;
     int kernels = 0;
+    CUCHK(c, cudaMemsetAsync(c->status.p, 0, sizeof(int), c->stream));
     CUCHK(c, cudaEventRecord(c->ev[1], c->stream));
     if (n > 0) {
         r = launch_eval(c, E, A, grads ? (flags & MBX_MIXED) : (flags | MBX_NO_GRADS), &kernels);
@@ -1473,6 +1484,7 @@ extern "C" int mbx_evaluate(mbx_ctx* c, const char* name, long n, const double* 
     }
     CUCHK(c, cudaEventRecord(c->ev[2], c->stream));
     CUCHK(c, cudaMemcpyAsync(c->h_out, c->out.p, 8 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CUCHK(c, cudaMemcpyAsync(c->h_out + MBX_H_STATUS, c->status.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     std::vector<double> gt, et;
     if (grads && !dev) {
         gt.resize(nx);
@@ -1480,6 +1492,10 @@ extern "C" int mbx_evaluate(mbx_ctx* c, const char* name, long n, const double* 
     }
     if (e_per && !dev && n > 0) CUCHK(c, cudaMemcpyAsync(e_per, EP, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     CUCHK(c, cudaStreamSynchronize(c->stream));
+    int status0;
+    memcpy(&status0, c->h_out + MBX_H_STATUS, sizeof(int));
+    if (status0 & MBX_STATUS_WAIT_TIMEOUT)
+        return fail(c, MBX_ECUDA, "an evaluation kernel's barrier wait timed out (results discarded)");
     if (grads && !dev)
         for (size_t i = 0; i < nx; ++i) grad[i] += gt[i];
     c->last_ms_build = 0;
@@ -1538,6 +1554,23 @@ extern "C" int mbx_evaluate_dcoef(mbx_ctx* c, const char* name, long n, const do
         for (int k = 0; k < E->ncoef; ++k) out[k] += tmp[k];
     }
     return MBX_OK;
+}
+
+extern "C" int mbx_qf_image(const char* name, const double* coef, long* image_bytes, int* nb, unsigned char* image,
+                            float* colf, double* b0) {
+    if (!name) return MBX_EINVAL;
+    const EvaluatorInfo* E = find_evaluator(name);
+    if (!E) return MBX_ENOTSUP;
+    const char* kern = mbx_evaluators[E->kern].name;
+    for (int i = 0; i < mbx_num_qf_types; ++i) {
+        const QfInfo& Q = mbx_qf_types[i];
+        if (strcmp(Q.name, kern) != 0) continue;
+        if (image_bytes) *image_bytes = Q.image_bytes;
+        if (nb) *nb = Q.nb;
+        if (image && colf && b0) return Q.build(coef ? coef : E->fit, image, colf, b0);
+        return MBX_OK;
+    }
+    return MBX_ENOTSUP;
 }
 
 extern "C" int mbx_poly(mbx_ctx* c, const char* name, long nd, const double* x, double* g, double* e, int flags) {
@@ -1723,13 +1756,16 @@ static int batch_sequence(mbx_ctx* c, int nbody, double* X, double* G, bool grad
     return MBX_OK;
 }
 
-// After a sequence: 0 when the build fit its buffers (counts recorded), else
-// the capacities are grown and 1 is returned (run it again).
+// After a sequence: 0 when the build fit its buffers (counts recorded), a
+// negative value when a kernel reported a timeout (error set), else the
+// capacities are grown and 1 is returned (run it again).
 static int batch_check(mbx_ctx* c, int nbody) {
     int status[2];
     memcpy(status, c->h_out + MBX_H_STATUS, sizeof(status));
     int counts[MBX_MAX_BUCKETS];
     memcpy(counts, c->h_out + MBX_H_COUNTS, sizeof(counts));
+    if (status[0] & MBX_STATUS_WAIT_TIMEOUT)
+        return -fail(c, MBX_ECUDA, "an evaluation kernel's barrier wait timed out (results discarded)");
     if (status[0]) {
         if (status[0] & MBX_STATUS_NB_OVERFLOW) c->nb_cap = std::max(c->nb_cap * 2, status[1] + 32);
         for (int b = 0; b < c->nbucket[nbody]; ++b) {
@@ -1766,7 +1802,9 @@ extern "C" int mbx_batch_energy(mbx_ctx* c, int nbody, double* xyz, double* grad
         CUCHK(c, cudaGraphLaunch(gr.exec, c->stream));
         CUCHK(c, cudaEventRecord(c->ev[2], c->stream));
         CUCHK(c, cudaStreamSynchronize(c->stream));
-        if (batch_check(c, nbody) == 0) {
+        const int f = batch_check(c, nbody);
+        if (f < 0) return MBX_ECUDA;
+        if (f == 0) {
             done = true;
             kernels = 1;
         } else {
@@ -1782,7 +1820,9 @@ extern "C" int mbx_batch_energy(mbx_ctx* c, int nbody, double* xyz, double* grad
             if (r) return r;
             CUCHK(c, cudaEventRecord(c->ev[2], c->stream));
             CUCHK(c, cudaStreamSynchronize(c->stream));
-            if (batch_check(c, nbody) == 0) break;
+            const int f = batch_check(c, nbody);
+            if (f < 0) return MBX_ECUDA;
+            if (f == 0) break;
             // the failed pass added nothing (the evaluators saw the status
             // word), so it can simply run again with the larger buffers
         }
@@ -1967,8 +2007,11 @@ extern "C" int mbx_batch_energy_2b3b(mbx_ctx* c, double* xyz, double* grad, doub
         CUCHK(c, cudaEventRecord(c->ev[2], c->stream));
         CUCHK(c, cudaStreamSynchronize(c->stream));
         kernels = 1;
-        need3 = batch_check(c, 3) != 0;
-        need2 = batch_check(k, 2) != 0;
+        const int f3 = batch_check(c, 3), f2 = batch_check(k, 2);
+        if (f3 < 0) return MBX_ECUDA;
+        if (f2 < 0) return fail(c, MBX_ECUDA, std::string("2b term: ") + k->err);
+        need3 = f3 != 0;
+        need2 = f2 != 0;
         if (need3 || need2) drop_graphs(c);   // buffers grow: capture again after a plain run
     }
     if (need3 || need2) {
@@ -1980,8 +2023,11 @@ extern "C" int mbx_batch_energy_2b3b(mbx_ctx* c, double* xyz, double* grad, doub
             if (r) return r;
             CUCHK(c, cudaEventRecord(c->ev[2], c->stream));
             CUCHK(c, cudaStreamSynchronize(c->stream));
-            if (need3) need3 = batch_check(c, 3) != 0;
-            if (need2) need2 = batch_check(k, 2) != 0;
+            const int f3 = need3 ? batch_check(c, 3) : 0, f2 = need2 ? batch_check(k, 2) : 0;
+            if (f3 < 0) return MBX_ECUDA;
+            if (f2 < 0) return fail(c, MBX_ECUDA, std::string("2b term: ") + k->err);
+            need3 = f3 != 0;
+            need2 = f2 != 0;
         }
         if (flags & MBX_GRAPH) {
             if (gr.exec) cudaGraphExecDestroy(gr.exec);

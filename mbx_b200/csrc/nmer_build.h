@@ -13,6 +13,8 @@
 #define MBX_STATUS_NB_OVERFLOW 1
 #define MBX_STATUS_BUCKET_OVERFLOW 2
 #define MBX_STATUS_LIST_OVERFLOW 4
+// a kernel's bounded barrier wait ran out (results discarded; an error, not a retry)
+#define MBX_STATUS_WAIT_TIMEOUT 8
 
 // shared-memory bytes per staged match of k_trimers (3 + 1 doubles, 4 ints)
 #define MBX_TRIMATCH_BYTES 48
