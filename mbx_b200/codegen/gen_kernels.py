@@ -1062,25 +1062,28 @@ int mbx_qf_image_%(name)s(const double* a, unsigned char* img, float* colf, doub
         }
         colf[j] = (float)std::ldexp(1.0, -(sj[j] + qf_t_%(name)s[j]));
     }
-    // K block s, N half hf (columns 240 hf ..): B[n][k] = C'_kn 2^s_n in hi,
-    // mid[, lo] FP16 parts of 240 rows x 16, core matrix (n' / 8, k / 8) of a
-    // part at (n' / 8) 256 + (k / 8) 128, row n' %% 8 at 16 (n' %% 8), n' = n - 240 hf
+    // K block s, pass p (columns pass_col(p) .. + pass_n(p)): B[n][k] =
+    // C'_kn 2^s_n in hi, mid[, lo] FP16 parts of pass_n(p) rows x 16, core
+    // matrix (n' / 8, k / 8) of a part at (n' / 8) 128 + (k / 8) (pass_n / 8) 128
+    // (row groups contiguous), row n' %% 8 at 16 (n' %% 8), n' = n - pass_col(p)
     memset(img, 0, (size_t)%(name)s_Q::IMAGE_BYTES);
     for (int s = 0; s < %(name)s_Q::KS; ++s) {
-        const int parts = s < %(name)s_Q::KT ? 3 : 2;
-        for (int n = 0; n < NB; ++n) {
-            const int hf = n / (NB / 2), nn = n - hf * (NB / 2);
-            unsigned char* st = img + %(name)s_Q::chunk_offset(s, hf);
-            for (int kk = 0; kk < 16; ++kk) {
-                const int k = 16 * s + kk;
-                double x = std::ldexp(C[(size_t)k * NB + n], sj[n]);
-                const size_t off = (size_t)(nn / 8) * 256 + (kk / 8) * 128 + (nn %% 8) * 16 + (kk %% 8) * 2;
-                for (int p = 0; p < parts; ++p) {
-                    const unsigned short h = qf_half(x);
-                    memcpy(st + (size_t)p * (NB / 2) * 32 + off, &h, 2);
-                    x -= qf_half_value(h);
+        const int parts = %(name)s_Q::parts(s);
+        for (int p = 0; p < %(name)s_Q::NPASS; ++p) {
+            const int width = %(name)s_Q::pass_n(p), c0 = %(name)s_Q::pass_col(p);
+            unsigned char* st = img + %(name)s_Q::chunk_offset(s, p);
+            for (int nn = 0; nn < width; ++nn)
+                for (int kk = 0; kk < 16; ++kk) {
+                    const int k = 16 * s + kk, n = c0 + nn;
+                    double x = std::ldexp(C[(size_t)k * NB + n], sj[n]);
+                    const size_t off = (size_t)(nn / 8) * 128 + (size_t)(kk / 8) * (width / 8) * 128 + (nn %% 8) * 16 +
+                                       (kk %% 8) * 2;
+                    for (int pt = 0; pt < parts; ++pt) {
+                        const unsigned short h = qf_half(x);
+                        memcpy(st + (size_t)pt * width * 32 + off, &h, 2);
+                        x -= qf_half_value(h);
+                    }
                 }
-            }
         }
     }
     return 0;
@@ -1119,14 +1122,15 @@ int mbx_launch_%(name)s_s(const HolderArgs& A, int grid, int block, cudaStream_t
     auto kern = qf_eval_kernel<%(name)s_T, %(name)s_Q>;
     static LaunchCache lc;
     int sms = 0, bps = 0;
-    const int r = launch_facts(lc, kern, qf::THREADS, qf::SMEM, qf::SMEM, &sms, &bps);
+    const int r = launch_facts(lc, kern, qf::THREADS, qf::Layout<%(name)s_Q>::SMEM, qf::Layout<%(name)s_Q>::SMEM, &sms,
+                               &bps);
     if (r) return r;
     const long wide = (long)sms * 16;
     const long gv = (A.n + 255) / 256, gf = (A.n + 127) / 128;
     pair_vars_kernel<%(name)s_T><<<(int)(gv < wide ? (gv > 0 ? gv : 1) : wide), 256, 0, s>>>(A);
     const long tiles = (A.n + 127) / 128;
     grid = (int)(tiles < (long)sms ? (tiles > 0 ? tiles : 1) : sms);
-    kern<<<grid, qf::THREADS, qf::SMEM, s>>>(A);
+    kern<<<grid, qf::THREADS, qf::Layout<%(name)s_Q>::SMEM, s>>>(A);
     pair_finish_kernel<%(name)s_T><<<(int)(gf < wide ? (gf > 0 ? gf : 1) : wide), 128, 0, s>>>(A);
     return (int)cudaGetLastError();
 }

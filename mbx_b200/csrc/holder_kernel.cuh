@@ -523,7 +523,11 @@ __global__ void __launch_bounds__(256, 2) pair_vars_kernel(const HolderArgs A) {
         float xf[T::NVARS];
         const bool live = nmer_vars_f32<T>(A, t, n, xf);
 #pragma unroll
-        for (int v = 0; v < T::NVARS; ++v) A.ps.dx[v * cap + t] = xf[v];
+        for (int v = 0; v < T::NVARS; ++v) {
+            A.ps.dx[v * cap + t] = xf[v];
+            A.ps.g[v * cap + t] = 0.0f;   // the tensor-core kernel adds into g and ep
+        }
+        A.ps.ep[t] = 0.0;
         A.ps.live[t] = live ? 1 : 0;
     }
 }

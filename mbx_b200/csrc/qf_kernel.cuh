@@ -8,35 +8,37 @@
 //
 // One CTA per SM, persistent over tiles of 128 n-mers.  For a tile, Y = M C
 // (128 x NB, NB = 480) is a product of FP16 operands accumulated in FP32 in
-// tensor memory by tcgen05.mma (M = 128, N = 240, K = 16), in two passes
-// over the N halves (columns 240 h .. 240 h + 239):
+// tensor memory by tcgen05.mma (M = 128, K = 16), in four passes over the
+// output columns (128, 128, 128, 96):
 //   A operand  the tile's basis values, split hi + lo, written to shared
-//              memory by the 128 row threads, K block by K block (again in
-//              the second pass);
+//              memory by the row threads, K block by K block (the same blocks
+//              in every pass);
 //   B operand  C split hi + mid + lo, prepared on the host in the canonical
-//              no-swizzle K-major layout (8 x 16-byte core matrices), one
-//              bulk copy (cp.async.bulk) per K block and N half from the
-//              type's image;
-//   products   hi.hi into the main accumulator (TMEM columns 0..239),
-//              hi.mid + lo.hi, and hi.lo on the first Q::KT blocks, into the
-//              correction accumulator (columns 256..495).  FP32 accumulation
-//              rounds after every MMA; the main accumulator's partial sums are
-//              large next to its final value (the polynomial cancels), so
-//              keeping the corrections out of it cuts the rounding steps of
-//              the large sums from 98 to 30 per output (9x less error of the
-//              summed energy over a liquid box).
-// Warps 0-3 are the row threads (thread i owns n-mer i of the tile and TMEM
-// lane i): they generate the A blocks and, once a pass's MMAs have
-// completed, read both accumulators back (tcgen05.ld) for the energy m . y
-// and the gradient 2 sum_j y_j dm_j/dd of that half.  Warp 4 lane 0 issues
-// the bulk copies, warp 5 lane 0 the MMAs; warp 5 also owns the TMEM
-// allocation.  Shared-memory slots of one K block each (A and B) cycle
-// through NS stages with mbarriers:
-//   afull[s]  128 row-thread arrivals (A written, proxy-fenced)
-//   bfull[s]  the producer's expect_tx + the copy's bytes
-//   empty[s]  tcgen05.commit after the block's MMAs
-//   tfull     tcgen05.commit after a pass's last block (its half of Y done)
-//   tempty    128 row-thread arrivals (that half read out)
+//              no-swizzle K-major layout (8 x 16-byte core matrices, row
+//              groups contiguous, see sdesc), one bulk copy (cp.async.bulk)
+//              per K block and pass from the type's image;
+//   products   hi.hi into the pass's main accumulator, hi.mid + lo.hi, and
+//              hi.lo on the first Q::KT blocks, into its correction
+//              accumulator.  The tensor core's FP32 accumulation aligns the
+//              addends of an MMA to the largest and truncates; the main
+//              partial sums are large next to their final values (the
+//              polynomial cancels), so keeping the corrections out of them
+//              cuts the truncation steps of the large sums from 98 to 30.
+// A pass takes 256 TMEM columns (main + correction), so two buffers fit in
+// the 512: the MMAs of pass q + 1 run while pass q is read back.
+// Warps 0-7 are the row threads, in two sets of 128 (thread i of a set owns
+// n-mer i of the tile and reads TMEM lane i): set 0 generates the even K
+// blocks of A and reads back the even chunks of 16 columns of both
+// accumulators (tcgen05.ld) for the energy m . y and the gradient
+// 2 sum_j y_j dm_j/dd; set 1 the odd ones.  Warp 8 lane 0 issues the bulk
+// copies, warp 9 lane 0 the MMAs; warp 9 also owns the TMEM allocation.
+// Shared-memory slots of one K block each (A and B) cycle through NS stages
+// with mbarriers:
+//   afull[s]   128 arrivals of the set that writes the block (A written, proxy-fenced)
+//   bfull[s]   the producer's expect_tx + the copy's bytes
+//   empty[s]   tcgen05.commit after the block's MMAs
+//   tfull[b]   tcgen05.commit after a pass's last block (buffer b complete)
+//   tempty[b]  256 row-thread arrivals (buffer b read out)
 // Every wait is bounded (QF_WAIT_NS of %globaltimer): on a timeout the CTA
 // sets an abort flag that ends every role's loop, drains its MMAs and
 // copies, frees its TMEM and reports MBX_STATUS_WAIT_TIMEOUT in *A.ps.err.
@@ -48,21 +50,39 @@
 
 namespace qf {
 
-constexpr int NS = 6;                 // shared-memory stages
 constexpr int A_PART = 128 * 16 * 2;  // bytes of one FP16 part of an A block (128 rows x K 16)
-constexpr int B_PART = 240 * 16 * 2;  // bytes of one FP16 part of a B chunk (240 rows x K 16)
 constexpr int A_BYTES = 2 * A_PART;
-constexpr int SLOT = 31 * 1024;              // A (8 KiB) + 3 B parts (22.5 KiB), rounded to 1 KiB
-static_assert(A_BYTES + 3 * B_PART <= SLOT, "slot too small");
-constexpr int PARK = 128 * (36 + 2) * 4;     // first pass's gradient (36 floats) and energy of each row
-constexpr int SMEM = NS * SLOT + 1024 + PARK; // + alignment of the first slot
-constexpr int THREADS = 192;
+constexpr int PARK_SET = 128 * (36 + 2) * 4; // one row set's gradient (36 floats) and energy of each row
+constexpr int PARK = 2 * PARK_SET;
+constexpr int SMEM_MAX = 232448;
+constexpr int ROW_WARPS = 8;                  // two sets of 4 warps over the 128 rows
+constexpr int PRODUCER_WARP = ROW_WARPS, MMA_WARP = ROW_WARPS + 1;
+constexpr int THREADS = 32 * (ROW_WARPS + 2);
 constexpr unsigned long long QF_WAIT_NS = 4000000000ull;
 // tcgen05 instruction descriptor, kind::f16: F32 accumulator (bits 4-5 = 1),
-// F16 A and B (formats 0), both K-major, N = 240 (bits 17-22: N >> 3),
-// M = 128 (bits 24-28: M >> 4)
-constexpr uint32_t IDESC = (1u << 4) | ((240u >> 3) << 17) | ((128u >> 4) << 24);
-constexpr int CORR_COL = 256;         // TMEM column of the correction accumulator
+// F16 A and B (formats 0), both K-major, N (bits 17-22: N >> 3), M = 128
+// (bits 24-28: M >> 4)
+__host__ __device__ constexpr uint32_t idesc(int n) {
+    return (1u << 4) | ((uint32_t)(n >> 3) << 17) | ((128u >> 4) << 24);
+}
+// Shared memory and tensor memory of a quadratic form Q: a slot holds one
+// K block of A and the widest pass's B chunk; passes of at most 128 columns
+// get two TMEM buffers of 256 columns (main + correction accumulator of 128
+// each: the MMAs of a pass run while the previous one is read back), wider
+// ones (up to 256) one buffer, the correction accumulator at column 256.
+template <class Q>
+struct Layout {
+    static constexpr int MAXN = Q::pass_n(0);   // passes are widest first
+    static constexpr int SLOT = ((A_BYTES + 3 * MAXN * 32) + 1023) / 1024 * 1024;
+    static constexpr int NS_FIT = (SMEM_MAX - 1024 - PARK) / SLOT;
+    static constexpr int NS = NS_FIT < 9 ? NS_FIT : 9;   // shared-memory stages
+    static constexpr int SMEM = NS * SLOT + 1024 + PARK;  // + alignment of the first slot
+    static constexpr bool DB = MAXN <= 128;              // double-buffered tensor memory
+    static constexpr int CORR_COL = DB ? 128 : 256;
+    static_assert(MAXN <= 256 && NS >= 4 && SMEM <= SMEM_MAX, "quadratic form does not fit");
+    __host__ __device__ static constexpr int buf(long q) { return DB ? (int)(q & 1) : 0; }
+    __host__ __device__ static constexpr long use(long q) { return DB ? q >> 1 : q; }   // uses of buf(q) before pass q
+};
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -150,21 +170,27 @@ __device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
 }
 
 // Shared-memory matrix descriptor: K-major, no swizzle (core matrices of
-// 8 rows x 16 bytes stored as 128 contiguous bytes), the two core matrices of
-// a K block 128 bytes apart (leading byte offset), successive 8-row groups
-// 256 bytes apart (stride byte offset); descriptor version 1 (bit 46).
-__device__ __forceinline__ uint64_t sdesc(uint32_t saddr) {
-    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128u >> 4) << 16) | ((uint64_t)(256u >> 4) << 32) |
-           (1ull << 46);
+// 8 rows x 16 bytes stored as 128 contiguous bytes), successive 8-row groups
+// 128 bytes apart (stride byte offset), the second core-matrix column of the
+// K block (k 8..15) lbo bytes after the first (leading byte offset); version
+// 1 (bit 46).  With the row groups contiguous, the groups that the tensor
+// core reads together sit in distinct shared-memory banks (groups 256 bytes
+// apart, the K block's two columns interleaved, put them in the same banks:
+// the kernel ran at a third of the tensor rate).
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)(128u >> 4) << 32) | (1ull << 46);
 }
+constexpr uint32_t A_LBO = 16 * 128;   // A block: 16 row groups (128 rows) per core-matrix column
+// a B chunk of n rows: n / 8 row groups per core-matrix column
 
 // D[tmem] (+)= A[smem] B[smem]^T, one thread issues.
-__device__ __forceinline__ void mma(uint32_t d, uint64_t a, uint64_t b, uint32_t accumulate) {
+__device__ __forceinline__ void mma(uint32_t d, uint64_t a, uint64_t b, uint32_t id, uint32_t accumulate) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d),
-        "l"(a), "l"(b), "r"(IDESC), "r"(accumulate)
+        "l"(a), "l"(b), "r"(id), "r"(accumulate)
         : "memory");
 }
 
@@ -209,34 +235,107 @@ __device__ __forceinline__ void split2(float a, float b, uint32_t& hi, uint32_t&
 
 }  // namespace qf
 
-// One pass's half of the epilogue: main + correction accumulator of the 240
-// columns, then Q::epi on each chunk of 16 (the chunk index a constant).
-template <class Q, int H, int NV>
-__device__ __forceinline__ double qf_epilogue_half(uint32_t trow, const float (&d)[NV], float (&g)[NV]) {
+// One pass's epilogue for one row set: main + correction accumulator of
+// the set's chunks of 16 columns (chunks SET, SET + 2, ... of the pass),
+// Q::epi on each (the chunk index a constant).  The TMEM loads of the next
+// chunk are in flight while the current chunk's arithmetic runs.
+template <class Q, int PASS, int SET, int NV>
+__device__ __forceinline__ double qf_epilogue_pass(uint32_t tbuf, const float (&d)[NV], float (&g)[NV]) {
+    constexpr int HC = Q::pass_n(PASS) / 16;   // chunks of 16 columns in the pass
+    constexpr int NCH = (HC - SET + 1) / 2;    // this set's chunks
+    constexpr int C0 = Q::pass_col(PASS) / 16;
     double P = 0.0;
+    uint32_t ym[2][16], yc[2][16];
+    qf::tmem_ld16(tbuf + (uint32_t)(SET * 16), ym[0]);
+    constexpr uint32_t CC = (uint32_t)qf::Layout<Q>::CORR_COL;
+    qf::tmem_ld16(tbuf + CC + (uint32_t)(SET * 16), yc[0]);
+    qf::tmem_wait_ld(ym[0]);
+    qf::tmem_wait_ld(yc[0]);
 #pragma unroll
-    for (int cc = 0; cc < Q::KS / 2; ++cc) {
-        uint32_t ym[16], yc[16];
-        qf::tmem_ld16(trow + (uint32_t)(cc * 16), ym);
-        qf::tmem_ld16(trow + (uint32_t)(qf::CORR_COL + cc * 16), yc);
-        qf::tmem_wait_ld(ym);
-        qf::tmem_wait_ld(yc);
+    for (int k = 0; k < NCH; ++k) {
+        const int b = k & 1, cc = SET + 2 * k;
+        if (k + 1 < NCH) {
+            qf::tmem_ld16(tbuf + (uint32_t)((cc + 2) * 16), ym[b ^ 1]);
+            qf::tmem_ld16(tbuf + CC + (uint32_t)((cc + 2) * 16), yc[b ^ 1]);
+        }
+        uint32_t y[16];
 #pragma unroll
-        for (int i = 0; i < 16; ++i) ym[i] = __float_as_uint(__uint_as_float(ym[i]) + __uint_as_float(yc[i]));
-        P += (double)Q::epi(H * (Q::KS / 2) + cc, ym, d, g);
+        for (int i = 0; i < 16; ++i) y[i] = __float_as_uint(__uint_as_float(ym[b][i]) + __uint_as_float(yc[b][i]));
+        P += (double)Q::epi(C0 + cc, y, d, g);
+        if (k + 1 < NCH) {
+            qf::tmem_wait_ld(ym[b ^ 1]);
+            qf::tmem_wait_ld(yc[b ^ 1]);
+        }
     }
     return P;
 }
 
+template <class Q, int SET, int NV>
+__device__ __forceinline__ double qf_epilogue(int pass, uint32_t tbuf, const float (&d)[NV], float (&g)[NV]) {
+    switch (pass) {
+        case 0: return qf_epilogue_pass<Q, 0, SET>(tbuf, d, g);
+        case 1: return qf_epilogue_pass<Q, 1, SET>(tbuf, d, g);
+        case 2: return qf_epilogue_pass<Q, 2, SET>(tbuf, d, g);
+        default: return qf_epilogue_pass<Q, 3, SET>(tbuf, d, g);
+    }
+}
+
+// K block s of pass q (ring index q KS + s) of A for one row: wait for the
+// slot, generate the row's 16 values (hi and lo parts) from the variables d
+// and row scales sc, store, fence for the tensor core, arrive.  false (warp-
+// uniform) when the CTA aborted.  Every pass of a tile generates the same
+// blocks (the passes differ in the columns of C).
+template <class Q, int NV>
+__device__ __forceinline__ bool qf_gen_block(int s, long q, float (&d)[NV], float (&sc)[Q::NT], uint32_t arow,
+                                             uint64_t* bar_empty, uint64_t* bar_afull, volatile int* abort_flag) {
+    using namespace qf;
+    constexpr int NS = Layout<Q>::NS, SLOT = Layout<Q>::SLOT;
+    const long it = q * Q::KS + s;
+    const int slot = (int)(it % NS);
+    const long use = it / NS;
+    const bool free_slot = use == 0 || wait(smem_u32(&bar_empty[slot]), (uint32_t)((use - 1) & 1), abort_flag);
+    if (!__all_sync(0xffffffffu, free_slot)) return false;
+    // generate this block here, not earlier: the same blocks recur in every
+    // pass, and hoisting them costs registers
+#pragma unroll
+    for (int v = 0; v < NV; ++v) asm volatile("" : "+f"(d[v]));
+#pragma unroll
+    for (int k = 0; k < Q::NT; ++k) asm volatile("" : "+f"(sc[k]));
+    uint32_t hi[8], lo[8];
+    Q::gen(s, d, sc, hi, lo);
+    const uint32_t a = arow + (uint32_t)(slot * SLOT);
+    st_shared_v4(a, make_uint4(hi[0], hi[1], hi[2], hi[3]));
+    st_shared_v4(a + A_LBO, make_uint4(hi[4], hi[5], hi[6], hi[7]));
+    st_shared_v4(a + A_PART, make_uint4(lo[0], lo[1], lo[2], lo[3]));
+    st_shared_v4(a + A_PART + A_LBO, make_uint4(lo[4], lo[5], lo[6], lo[7]));
+    fence_proxy_async();
+    mbar_arrive(smem_u32(&bar_afull[slot]));
+    return true;
+}
+
+// All K blocks of one set's parity for pass q.
+template <class Q, int NV>
+__device__ __forceinline__ bool qf_gen_pass(int set, long q, float (&d)[NV], float (&sc)[Q::NT], uint32_t arow,
+                                            uint64_t* bar_empty, uint64_t* bar_afull, volatile int* abort_flag) {
+#pragma unroll
+    for (int s = 0; s < Q::KS; ++s)
+        if ((s & 1) == set && !qf_gen_block<Q, NV>(s, q, d, sc, arow, bar_empty, bar_afull, abort_flag)) return false;
+    return true;
+}
+
 // T: the evaluator traits (NVARS); Q: the generated quadratic form
 // (<name>_qf.cuh): KS K blocks of 16, the first KT with the third C part,
-// stage image offsets/bytes, the row-scale classes, gen(s) and epi(c).
+// NPASS passes over the columns, the (block, pass) chunks of the image, the
+// row-scale classes, gen(s) and epi(c).
 template <class T, class Q>
 __global__ void __launch_bounds__(qf::THREADS, 1) qf_eval_kernel(const HolderArgs A) {
     using namespace qf;
+    using L = Layout<Q>;
     constexpr int NV = T::NVARS;
+    constexpr int NP = Q::NPASS;
+    constexpr int NS = L::NS, SLOT = L::SLOT;
     __shared__ __align__(8) uint64_t bar_afull[NS], bar_bfull[NS], bar_empty[NS];
-    __shared__ __align__(8) uint64_t bar_tfull, bar_tempty, bar_drain;
+    __shared__ __align__(8) uint64_t bar_tfull[2], bar_tempty[2], bar_drain;
     __shared__ uint32_t s_tmem;
     __shared__ volatile int s_abort;
     __shared__ long s_n;
@@ -254,13 +353,15 @@ __global__ void __launch_bounds__(qf::THREADS, 1) qf_eval_kernel(const HolderArg
             mbar_init(smem_u32(&bar_bfull[s]), 1);
             mbar_init(smem_u32(&bar_empty[s]), 1);
         }
-        mbar_init(smem_u32(&bar_tfull), 1);
-        mbar_init(smem_u32(&bar_tempty), 128);
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(smem_u32(&bar_tfull[b]), 1);
+            mbar_init(smem_u32(&bar_tempty[b]), 32 * ROW_WARPS);
+        }
         mbar_init(smem_u32(&bar_drain), 1);
         s_abort = 0;
         fence_mbar_init();
     }
-    if (warp == 5) {
+    if (warp == MMA_WARP) {
         tmem_alloc(smem_u32(&s_tmem), 512);
         tmem_relinquish();
     }
@@ -270,141 +371,156 @@ __global__ void __launch_bounds__(qf::THREADS, 1) qf_eval_kernel(const HolderArg
     const uint32_t tmem = s_tmem;
     const long n = s_n;
     const long ntiles = (n + 127) / 128;
+    // passes of this CTA: NP per tile, tiles blockIdx.x, + gridDim.x, ...
+    const long my_tiles = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+    const long npasses = my_tiles * NP;
 
-    if (warp < 4) {
-        // ---- row threads: A blocks of both passes, then each pass's epilogue ----
-        const int row = tid;
-        const uint32_t arow = base + (uint32_t)((row >> 3) * 256 + (row & 7) * 16);
-        const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
-        float* park_g = reinterpret_cast<float*>(mbx_dyn_smem + (base - smem_u32(mbx_dyn_smem)) + NS * SLOT);
+    if (warp < ROW_WARPS) {
+        // ---- row threads.  Two sets of 128 threads, thread i of a set on
+        // row i: set 0 (warps 0-3) generates the even K blocks and reads the
+        // even 16-column chunks of a pass back, set 1 (warps 4-7) the odd
+        // ones.  Software pipeline over the passes: generate pass q + 1, then
+        // read pass q back from its TMEM buffer while the MMAs of pass q + 1
+        // fill the other buffer.  Each set sums its share of a tile's energy
+        // and gradient over the passes in shared memory and adds the totals
+        // to the outputs (zeroed by pair_vars_kernel; two addends onto zero,
+        // so the result does not depend on their order).
+        const int set = warp / 4;
+        const int row = tid & 127;
+        const uint32_t arow = base + (uint32_t)((row >> 3) * 128 + (row & 7) * 16);
+        const uint32_t trow = tmem + ((uint32_t)((warp & 3) * 32) << 16);   // the warp's TMEM lane quarter
+        float* park_g = reinterpret_cast<float*>(mbx_dyn_smem + (base - smem_u32(mbx_dyn_smem)) + NS * SLOT) +
+                        set * (PARK_SET / 4);
         double* park_p = reinterpret_cast<double*>(park_g + 36 * 128);
-        long it = 0, tp = 0;
-        for (long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-            const long t = tile * 128 + row;
-            const bool valid = t < n;
-            float d[NV];
+        static_assert(NV <= 36, "park area holds 36 gradient entries");
+        auto load_vars = [&](long tl, float (&dv)[NV], float (&sv)[Q::NT]) -> float {
+            const long tt = tl * 128 + row;
 #pragma unroll
-            for (int v = 0; v < NV; ++v) d[v] = valid ? A.ps.dx[v * cap + t] : 0.0f;
-            float sc[Q::NT];
-            const float rinv = Q::row_scales(d, sc);
-            double P = 0.0;
-            float g[NV];
+            for (int v = 0; v < NV; ++v) dv[v] = tt < n ? A.ps.dx[v * cap + tt] : 0.0f;
+            return Q::row_scales(dv, sv);
+        };
+        float de_[NV], dg[NV], sg[Q::NT];   // variables of the tile read back / being generated
+        float (&de)[NV] = L::DB ? de_ : dg;  // one buffer: the same tile
+        float rinv_e = 1.0f, rinv_g = 1.0f;
+        if (npasses > 0) {
+            rinv_g = load_vars(blockIdx.x, dg, sg);
+            if (L::DB) {
 #pragma unroll
-            for (int v = 0; v < NV; ++v) g[v] = 0.0f;
-            static_assert(NV <= 36, "park area holds 36 gradient entries");
-            for (int h = 0; h < 2; ++h, ++tp) {
-                // (both passes generate the same A blocks: the opaque inputs in
-                // the stage loop keep the compiler from hoisting them)
-#pragma unroll
-                for (int s = 0; s < Q::KS; ++s, ++it) {
-                    const int slot = (int)(it % NS);
-                    const long use = it / NS;
-                    const bool free_slot =
-                        use == 0 || wait(smem_u32(&bar_empty[slot]), (uint32_t)((use - 1) & 1), &s_abort);
-                    if (!__all_sync(0xffffffffu, free_slot)) goto rows_done;   // warp-uniform exit
-                    // generate this block here, not earlier (register pressure)
-#pragma unroll
-                    for (int v = 0; v < NV; ++v) asm volatile("" : "+f"(d[v]));
-#pragma unroll
-                    for (int k = 0; k < Q::NT; ++k) asm volatile("" : "+f"(sc[k]));
-                    uint32_t hi[8], lo[8];
-                    Q::gen(s, d, sc, hi, lo);
-                    const uint32_t a = arow + (uint32_t)(slot * SLOT);
-                    st_shared_v4(a, make_uint4(hi[0], hi[1], hi[2], hi[3]));
-                    st_shared_v4(a + 128, make_uint4(hi[4], hi[5], hi[6], hi[7]));
-                    st_shared_v4(a + A_PART, make_uint4(lo[0], lo[1], lo[2], lo[3]));
-                    st_shared_v4(a + A_PART + 128, make_uint4(lo[4], lo[5], lo[6], lo[7]));
-                    fence_proxy_async();
-                    mbar_arrive(smem_u32(&bar_afull[slot]));
-                }
-                // warp-uniform: the TMEM loads below are warp-collective
-                if (!__all_sync(0xffffffffu, wait(smem_u32(&bar_tfull), (uint32_t)(tp & 1), &s_abort)))
-                    goto rows_done;
-                tc_after();
-                P += h == 0 ? qf_epilogue_half<Q, 0>(trow, d, g) : qf_epilogue_half<Q, 1>(trow, d, g);
-                tc_before();
-                mbar_arrive(smem_u32(&bar_tempty));
-                if (h == 0) {
-                    // park the first pass's sums in shared memory: registers are
-                    // short while the second pass generates its A blocks
-#pragma unroll
-                    for (int v = 0; v < NV; ++v) {
-                        park_g[v * 128 + row] = g[v];
-                        g[v] = 0.0f;
-                    }
-                    park_p[row] = P;
-                    P = 0.0;
-                }
+                for (int v = 0; v < NV; ++v) de_[v] = dg[v];
             }
+            rinv_e = rinv_g;
+            if (L::DB && !qf_gen_pass<Q, NV>(set, 0, dg, sg, arow, bar_empty, bar_afull, &s_abort)) goto rows_done;
+        }
+        for (long q = 0; q < npasses; ++q) {
+            const int p = (int)(q % NP);
+            const long tile = blockIdx.x + (q / NP) * gridDim.x;
+            if (L::DB) {
+                // double-buffered: generate the next pass before reading this one back
+                if (q + 1 < npasses) {
+                    if (p == NP - 1) rinv_g = load_vars(tile + gridDim.x, dg, sg);
+                    if (!qf_gen_pass<Q, NV>(set, q + 1, dg, sg, arow, bar_empty, bar_afull, &s_abort)) goto rows_done;
+                }
+            } else {
+                // one buffer: this pass's MMAs cannot start before the previous
+                // pass is read back, so generate it first
+                if (p == 0 && q > 0) rinv_e = rinv_g = load_vars(tile, dg, sg);
+                if (!qf_gen_pass<Q, NV>(set, q, dg, sg, arow, bar_empty, bar_afull, &s_abort)) goto rows_done;
+            }
+            const int bi = L::buf(q);
+            // warp-uniform: the TMEM loads below are warp-collective
+            if (!__all_sync(0xffffffffu, wait(smem_u32(&bar_tfull[bi]), (uint32_t)(L::use(q) & 1), &s_abort)))
+                goto rows_done;
+            tc_after();
+            {
+                float g[NV];
 #pragma unroll
-            for (int v = 0; v < NV; ++v) g[v] += park_g[v * 128 + row];
-            P += park_p[row];
-            if (valid) {
-                const float gs = 2.0f * rinv;
+                for (int v = 0; v < NV; ++v) g[v] = 0.0f;
+                const uint32_t tbuf = trow + (uint32_t)(bi * 256);
+                const double P = set == 0 ? qf_epilogue<Q, 0>(p, tbuf, de, g) : qf_epilogue<Q, 1>(p, tbuf, de, g);
+                tc_before();
+                mbar_arrive(smem_u32(&bar_tempty[bi]));
+                // the set's running sums of the tile
 #pragma unroll
-                for (int v = 0; v < NV; ++v) A.ps.g[v * cap + t] = g[v] * gs;
-                A.ps.ep[t] = Q::b0() + P * (double)rinv;
+                for (int v = 0; v < NV; ++v) park_g[v * 128 + row] = (p == 0 ? 0.0f : park_g[v * 128 + row]) + g[v];
+                park_p[row] = (p == 0 ? 0.0 : park_p[row]) + P;
+            }
+            if (p == NP - 1) {
+                const long t = tile * 128 + row;
+                if (t < n) {
+                    const float gs = 2.0f * rinv_e;
+#pragma unroll
+                    for (int v = 0; v < NV; ++v) atomicAdd(A.ps.g + v * cap + t, park_g[v * 128 + row] * gs);
+                    atomicAdd(A.ps.ep + t, (set == 0 ? Q::b0() : 0.0) + park_p[row] * (double)rinv_e);
+                }
+                if (L::DB) {
+#pragma unroll
+                    for (int v = 0; v < NV; ++v) de_[v] = dg[v];
+                    rinv_e = rinv_g;
+                }
             }
         }
     rows_done:;
-    } else if (warp == 4) {
-        // ---- producer: one bulk copy of C's (K block, N half) chunk per stage ----
+    } else if (warp == PRODUCER_WARP) {
+        // ---- producer: one bulk copy of C's (K block, pass) chunk per stage ----
         if (lane == 0) {
             long it = 0;
-            for (long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-                for (int h = 0; h < 2; ++h) {
-                    for (int s = 0; s < Q::KS; ++s, ++it) {
-                        const int slot = (int)(it % NS);
-                        const long use = it / NS;
-                        if (use > 0 && !wait(smem_u32(&bar_empty[slot]), (uint32_t)((use - 1) & 1), &s_abort))
-                            goto producer_done;
-                        const uint32_t bytes = (uint32_t)Q::chunk_bytes(s);
-                        const uint32_t bar = smem_u32(&bar_bfull[slot]);
-                        mbar_arrive_tx(bar, bytes);
-                        bulk_g2s(base + (uint32_t)(slot * SLOT + A_BYTES), Q::image() + Q::chunk_offset(s, h), bytes,
-                                 bar);
-                    }
+            for (long q = 0; q < npasses; ++q) {
+                const int p = (int)(q % NP);
+                for (int s = 0; s < Q::KS; ++s, ++it) {
+                    const int slot = (int)(it % NS);
+                    const long use = it / NS;
+                    if (use > 0 && !wait(smem_u32(&bar_empty[slot]), (uint32_t)((use - 1) & 1), &s_abort))
+                        goto producer_done;
+                    const uint32_t bytes = (uint32_t)Q::chunk_bytes(s, p);
+                    const uint32_t bar = smem_u32(&bar_bfull[slot]);
+                    mbar_arrive_tx(bar, bytes);
+                    bulk_g2s(base + (uint32_t)(slot * SLOT + A_BYTES), Q::image() + Q::chunk_offset(s, p), bytes, bar);
                 }
             }
         producer_done:
             // copies in flight complete on their own: wait for them before the
             // shared memory goes away (the last use of every slot)
             for (int k = 0; k < NS && k < it; ++k) {
-                const long q = it - 1 - k;   // stage iteration of the last copy into slot q % NS
-                wait_drain(smem_u32(&bar_bfull[q % NS]), (uint32_t)((q / NS) & 1));
+                const long qq = it - 1 - k;   // stage iteration of the last copy into slot qq % NS
+                wait_drain(smem_u32(&bar_bfull[qq % NS]), (uint32_t)((qq / NS) & 1));
             }
         }
     } else {
         // ---- MMA issuer ----
         if (lane == 0) {
-            long it = 0, tp = 0;
+            long it = 0;
             bool issued = false;
-            for (long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-                for (int h = 0; h < 2; ++h, ++tp) {
-                    if (tp > 0) {
-                        if (!wait(smem_u32(&bar_tempty), (uint32_t)((tp - 1) & 1), &s_abort)) goto mma_done;
-                        tc_after();
-                    }
-                    for (int s = 0; s < Q::KS; ++s, ++it) {
-                        const int slot = (int)(it % NS);
-                        const uint32_t par = (uint32_t)((it / NS) & 1);
-                        if (!wait(smem_u32(&bar_afull[slot]), par, &s_abort)) goto mma_done;
-                        if (!wait(smem_u32(&bar_bfull[slot]), par, &s_abort)) goto mma_done;
-                        tc_after();
-                        const uint32_t sa = base + (uint32_t)(slot * SLOT);
-                        const uint32_t sb = sa + A_BYTES;
-                        const uint64_t a_hi = sdesc(sa), a_lo = sdesc(sa + A_PART);
-                        const uint64_t b_hi = sdesc(sb), b_mid = sdesc(sb + B_PART);
-                        const uint32_t acc = s > 0 ? 1u : 0u;
-                        mma(tmem, a_hi, b_hi, acc);                      // main: hi.hi
-                        mma(tmem + CORR_COL, a_hi, b_mid, acc);          // corrections
-                        mma(tmem + CORR_COL, a_lo, b_hi, 1u);
-                        if (s < Q::KT) mma(tmem + CORR_COL, a_hi, sdesc(sb + 2 * B_PART), 1u);
-                        commit(smem_u32(&bar_empty[slot]));
-                        issued = true;
-                    }
-                    commit(smem_u32(&bar_tfull));
+            for (long q = 0; q < npasses; ++q) {
+                const int p = (int)(q % NP);
+                const int b = L::buf(q);
+                const long u = L::use(q);
+                if (u >= 1) {
+                    // the buffer's previous pass has been read back
+                    if (!wait(smem_u32(&bar_tempty[b]), (uint32_t)((u - 1) & 1), &s_abort)) goto mma_done;
+                    tc_after();
                 }
+                const int nn = Q::pass_n(p);
+                const uint32_t id = idesc(nn), blbo = (uint32_t)(nn / 8) * 128, bpart = (uint32_t)nn * 32;
+                const uint32_t dmain = tmem + (uint32_t)(b * 256), dcorr = dmain + (uint32_t)L::CORR_COL;
+                for (int s = 0; s < Q::KS; ++s, ++it) {
+                    const int slot = (int)(it % NS);
+                    const uint32_t par = (uint32_t)((it / NS) & 1);
+                    if (!wait(smem_u32(&bar_afull[slot]), par, &s_abort)) goto mma_done;
+                    if (!wait(smem_u32(&bar_bfull[slot]), par, &s_abort)) goto mma_done;
+                    tc_after();
+                    const uint32_t sa = base + (uint32_t)(slot * SLOT);
+                    const uint32_t sb = sa + A_BYTES;
+                    const uint64_t a_hi = sdesc(sa, A_LBO), a_lo = sdesc(sa + A_PART, A_LBO);
+                    const uint64_t b_hi = sdesc(sb, blbo), b_mid = sdesc(sb + bpart, blbo);
+                    const uint32_t acc = s > 0 ? 1u : 0u;
+                    mma(dmain, a_hi, b_hi, id, acc);          // main: hi.hi
+                    mma(dcorr, a_hi, b_mid, id, acc);         // corrections
+                    mma(dcorr, a_lo, b_hi, id, 1u);
+                    if (s < Q::KT) mma(dcorr, a_hi, sdesc(sb + 2 * bpart, blbo), id, 1u);
+                    commit(smem_u32(&bar_empty[slot]));
+                    issued = true;
+                }
+                commit(smem_u32(&bar_tfull[b]));
             }
         mma_done:
             if (issued) {
@@ -417,7 +533,7 @@ __global__ void __launch_bounds__(qf::THREADS, 1) qf_eval_kernel(const HolderArg
     __syncwarp();
     tc_before();
     __syncthreads();
-    if (warp == 5) {
+    if (warp == MMA_WARP) {
         tc_after();
         tmem_dealloc(tmem, 512);
     }
