@@ -224,10 +224,14 @@ def batched_leg(args, local, flush, fp64_value, dist=None, world=1):
         torch.cuda.synchronize()
         a = torch.cuda.Event(enable_timing=True)
         z = torch.cuda.Event(enable_timing=True)
+        # an NVTX range per timed step, so that a profiler can select the
+        # step's launches (ncu --nvtx --nvtx-include "mbx_batched_step/")
+        torch.cuda.nvtx.range_push("mbx_batched_step")
         a.record(stream)
         b.grad.zero_()
         t0, t1 = b.energy_2b3b(mixed=True)   # replays the graph on the same stream
         z.record(stream)
+        torch.cuda.nvtx.range_pop()
         torch.cuda.synchronize()
         times.append(a.elapsed_time(z))
         emx = t0 + t1

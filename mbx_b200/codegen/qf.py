@@ -460,7 +460,10 @@ def emit_cuda(q, name, nvars):
     w("    }")
     # epilogue
     w("    // columns 16 c .. 16 c + 15 of Y: z_j = y_j 2^-(s_j + t_j) (y / r, scaled back by the caller);")
-    w("    // returns sum_j m_j z_j of the chunk, adds z_j dm_j/dd to g")
+    w("    // adds z_j dm_j/dd to g and returns the chunk's share of the energy that g does not")
+    w("    // carry: by Euler's identity for monomials of degree k, sum_u d_u dm/dd_u = k m, so")
+    w("    // sum_j m_j z_j = z_const + (sum_{deg 1} d_u z_j + sum_u d_u g_u) / 2 over the pass,")
+    w("    // and the degree-2 columns (all but 37) need no energy term of their own")
     w("    __device__ __forceinline__ static float epi(int c, const uint32_t (&y)[16], const float (&d)[%d], "
       "float (&g)[%d]) {" % (nvars, nvars))
     w("        float p = 0.0f, z;")
@@ -476,11 +479,10 @@ def emit_cuda(q, name, nvars):
             if len(b) == 0:
                 w("            p += z;")
             elif len(b) == 1:
-                w("            p = fmaf(d[%d], z, p);" % b[0])
+                w("            p = fmaf(0.5f * d[%d], z, p);" % b[0])
                 w("            g[%d] += z;" % b[0])
             else:
                 u, v = b
-                w("            p = fmaf(d[%d] * d[%d], z, p);" % (u, v))
                 w("            g[%d] = fmaf(z, d[%d], g[%d]);" % (u, v, u))
                 w("            g[%d] = fmaf(z, d[%d], g[%d]);" % (v, u, v))
         w("            break;")

@@ -8,8 +8,10 @@
 //
 // One CTA per SM, persistent over tiles of 128 n-mers.  For a tile, Y = M C
 // (128 x NB, NB = 480) is a product of FP16 operands accumulated in FP32 in
-// tensor memory by tcgen05.mma (M = 128, K = 16), in four passes over the
-// output columns (128, 128, 128, 96):
+// tensor memory by tcgen05.mma (M = 128, K = 16), in Q::NPASS passes over
+// the output columns (two of 240 for MB-pol 3b: an MMA of M = 128, K = 16
+// takes the same ~130 SM cycles for N = 128 and N = 256, so the widest
+// passes take the fewest):
 //   A operand  the tile's basis values, split hi + lo, written to shared
 //              memory by the row threads, K block by K block (the same blocks
 //              in every pass);
@@ -24,20 +26,21 @@
 //              partial sums are large next to their final values (the
 //              polynomial cancels), so keeping the corrections out of them
 //              cuts the truncation steps of the large sums from 98 to 30.
-// A pass takes 256 TMEM columns (main + correction), so two buffers fit in
-// the 512: the MMAs of pass q + 1 run while pass q is read back.
+// A pass of 240 columns takes 480 TMEM columns (main + correction), so the
+// 512 hold one buffer: the MMAs of pass q + 1 start once pass q is read
+// back (passes of at most 128 columns get two buffers, see Layout).
 // Warps 0-7 are the row threads, in two sets of 128 (thread i of a set owns
-// n-mer i of the tile and reads TMEM lane i): set 0 generates the even K
-// blocks of A and reads back the even chunks of 16 columns of both
+// n-mer i of the tile and reads TMEM lane i): set 0 generates the even
+// stages of A and reads back the even chunks of 16 columns of both
 // accumulators (tcgen05.ld) for the energy m . y and the gradient
 // 2 sum_j y_j dm_j/dd; set 1 the odd ones.  Warp 8 lane 0 issues the bulk
 // copies, warp 9 lane 0 the MMAs; warp 9 also owns the TMEM allocation.
-// Shared-memory slots of one K block each (A and B) cycle through NS stages
-// with mbarriers:
-//   afull[s]   128 arrivals of the set that writes the block (A written, proxy-fenced)
-//   bfull[s]   the producer's expect_tx + the copy's bytes
-//   empty[s]   tcgen05.commit after the block's MMAs
-//   tfull[b]   tcgen05.commit after a pass's last block (buffer b complete)
+// Shared-memory slots of one stage each (Layout::BPS K blocks of A and B)
+// cycle through NS slots with mbarriers:
+//   afull[s]   128 arrivals of the set that writes the stage (A written, proxy-fenced)
+//   bfull[s]   the producer's expect_tx + the copies' bytes
+//   empty[s]   tcgen05.commit after the stage's MMAs
+//   tfull[b]   tcgen05.commit after a pass's last stage (buffer b complete)
 //   tempty[b]  256 row-thread arrivals (buffer b read out)
 // Every wait is bounded (QF_WAIT_NS of %globaltimer): on a timeout the CTA
 // sets an abort flag that ends every role's loop, drains its MMAs and
@@ -59,27 +62,39 @@ constexpr int ROW_WARPS = 8;                  // two sets of 4 warps over the 12
 constexpr int PRODUCER_WARP = ROW_WARPS, MMA_WARP = ROW_WARPS + 1;
 constexpr int THREADS = 32 * (ROW_WARPS + 2);
 constexpr unsigned long long QF_WAIT_NS = 4000000000ull;
+// Suspend-time hint of every wait: a thread whose phase is not complete
+// sleeps until it completes (or this many ns pass) instead of spinning, so
+// that waiting warps take no issue slots from the MMA issuer and the row
+// threads that share their SM sub-partition.
+constexpr uint32_t QF_SUSPEND_NS = 1000000;
 // tcgen05 instruction descriptor, kind::f16: F32 accumulator (bits 4-5 = 1),
 // F16 A and B (formats 0), both K-major, N (bits 17-22: N >> 3), M = 128
 // (bits 24-28: M >> 4)
 __host__ __device__ constexpr uint32_t idesc(int n) {
     return (1u << 4) | ((uint32_t)(n >> 3) << 17) | ((128u >> 4) << 24);
 }
-// Shared memory and tensor memory of a quadratic form Q: a slot holds one
-// K block of A and the widest pass's B chunk; passes of at most 128 columns
-// get two TMEM buffers of 256 columns (main + correction accumulator of 128
-// each: the MMAs of a pass run while the previous one is read back), wider
-// ones (up to 256) one buffer, the correction accumulator at column 256.
+// Shared memory and tensor memory of a quadratic form Q: a stage is BPS
+// consecutive K blocks, and its slot holds their A blocks (A_BYTES each) and
+// the widest pass's B chunks (BCHUNK each); passes of at most 128 columns get
+// two TMEM buffers of 256 columns (main + correction accumulator of 128 each:
+// the MMAs of a pass run while the previous one is read back), wider ones
+// (up to 256) one buffer, the correction accumulator at column 256.  Two
+// blocks per stage halve the barrier waits of the MMA issuer per MMA: the
+// issuer's waits, not the tensor core, bounded the one-block stages.
 template <class Q>
 struct Layout {
     static constexpr int MAXN = Q::pass_n(0);   // passes are widest first
-    static constexpr int SLOT = ((A_BYTES + 3 * MAXN * 32) + 1023) / 1024 * 1024;
+    static constexpr int BPS = 2;               // K blocks per stage
+    static constexpr int NSTAGE = Q::KS / BPS;  // stages per pass
+    static constexpr int BCHUNK = 3 * MAXN * 32;
+    static constexpr int BOFF = BPS * A_BYTES;  // B chunks after the A blocks
+    static constexpr int SLOT = (BPS * (A_BYTES + BCHUNK) + 1023) / 1024 * 1024;
     static constexpr int NS_FIT = (SMEM_MAX - 1024 - PARK) / SLOT;
     static constexpr int NS = NS_FIT < 9 ? NS_FIT : 9;   // shared-memory stages
     static constexpr int SMEM = NS * SLOT + 1024 + PARK;  // + alignment of the first slot
     static constexpr bool DB = MAXN <= 128;              // double-buffered tensor memory
     static constexpr int CORR_COL = DB ? 128 : 256;
-    static_assert(MAXN <= 256 && NS >= 4 && SMEM <= SMEM_MAX, "quadratic form does not fit");
+    static_assert(MAXN <= 256 && NS >= 3 && SMEM <= SMEM_MAX && Q::KS % BPS == 0, "quadratic form does not fit");
     __host__ __device__ static constexpr int buf(long q) { return DB ? (int)(q & 1) : 0; }
     __host__ __device__ static constexpr long use(long q) { return DB ? q >> 1 : q; }   // uses of buf(q) before pass q
 };
@@ -104,10 +119,10 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(ok)
-        : "r"(bar), "r"(parity)
+        : "r"(bar), "r"(parity), "r"(QF_SUSPEND_NS)
         : "memory");
     return ok != 0;
 }
@@ -238,7 +253,8 @@ __device__ __forceinline__ void split2(float a, float b, uint32_t& hi, uint32_t&
 // One pass's epilogue for one row set: main + correction accumulator of
 // the set's chunks of 16 columns (chunks SET, SET + 2, ... of the pass),
 // Q::epi on each (the chunk index a constant).  The TMEM loads of the next
-// chunk are in flight while the current chunk's arithmetic runs.
+// chunk are in flight while the current chunk's arithmetic runs.  g must
+// enter zeroed: the energy is completed from it.
 template <class Q, int PASS, int SET, int NV>
 __device__ __forceinline__ double qf_epilogue_pass(uint32_t tbuf, const float (&d)[NV], float (&g)[NV]) {
     constexpr int HC = Q::pass_n(PASS) / 16;   // chunks of 16 columns in the pass
@@ -267,7 +283,12 @@ __device__ __forceinline__ double qf_epilogue_pass(uint32_t tbuf, const float (&
             qf::tmem_wait_ld(yc[b ^ 1]);
         }
     }
-    return P;
+    // the degree-2 columns' energy, sum_j m_j z_j = (sum_u d_u g_u) / 2 over
+    // them (Q::epi), here with the degree-1 columns' share (also in g)
+    double dg = 0.0;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) dg = fma((double)d[v], (double)g[v], dg);
+    return P + 0.5 * dg;
 }
 
 template <class Q, int SET, int NV>
@@ -280,46 +301,54 @@ __device__ __forceinline__ double qf_epilogue(int pass, uint32_t tbuf, const flo
     }
 }
 
-// K block s of pass q (ring index q KS + s) of A for one row: wait for the
-// slot, generate the row's 16 values (hi and lo parts) from the variables d
-// and row scales sc, store, fence for the tensor core, arrive.  false (warp-
-// uniform) when the CTA aborted.  Every pass of a tile generates the same
-// blocks (the passes differ in the columns of C).
-template <class Q, int NV>
-__device__ __forceinline__ bool qf_gen_block(int s, long q, float (&d)[NV], float (&sc)[Q::NT], uint32_t arow,
+// Stage st of pass q (ring index q NSTAGE + st) of A for one row: wait for
+// the slot, generate the row's 16 values (hi and lo parts) of each of the
+// stage's K blocks from the variables d and row scales sc, store, fence for
+// the tensor core, arrive.  false (warp-uniform) when the CTA aborted.  Every
+// pass of a tile generates the same blocks (the passes differ in the columns
+// of C).
+template <class Q, int NV, int ST>
+__device__ __forceinline__ bool qf_gen_stage(long q, float (&d)[NV], float (&sc)[Q::NT], uint32_t arow,
                                              uint64_t* bar_empty, uint64_t* bar_afull, volatile int* abort_flag) {
     using namespace qf;
-    constexpr int NS = Layout<Q>::NS, SLOT = Layout<Q>::SLOT;
-    const long it = q * Q::KS + s;
-    const int slot = (int)(it % NS);
-    const long use = it / NS;
-    const bool free_slot = use == 0 || wait(smem_u32(&bar_empty[slot]), (uint32_t)((use - 1) & 1), abort_flag);
+    using L = Layout<Q>;
+    constexpr int NS = L::NS, SLOT = L::SLOT;
+    const uint32_t it = (uint32_t)q * L::NSTAGE + (uint32_t)ST;   // ring index (32 bits: see the kernel)
+    const uint32_t slot = it % NS, use = it / NS;
+    const bool free_slot = use == 0 || wait(smem_u32(&bar_empty[slot]), (use - 1) & 1u, abort_flag);
     if (!__all_sync(0xffffffffu, free_slot)) return false;
-    // generate this block here, not earlier: the same blocks recur in every
-    // pass, and hoisting them costs registers
 #pragma unroll
-    for (int v = 0; v < NV; ++v) asm volatile("" : "+f"(d[v]));
+    for (int j = 0; j < L::BPS; ++j) {
+        // generate each block here, not earlier: the same blocks recur in
+        // every pass, and hoisting them costs registers
 #pragma unroll
-    for (int k = 0; k < Q::NT; ++k) asm volatile("" : "+f"(sc[k]));
-    uint32_t hi[8], lo[8];
-    Q::gen(s, d, sc, hi, lo);
-    const uint32_t a = arow + (uint32_t)(slot * SLOT);
-    st_shared_v4(a, make_uint4(hi[0], hi[1], hi[2], hi[3]));
-    st_shared_v4(a + A_LBO, make_uint4(hi[4], hi[5], hi[6], hi[7]));
-    st_shared_v4(a + A_PART, make_uint4(lo[0], lo[1], lo[2], lo[3]));
-    st_shared_v4(a + A_PART + A_LBO, make_uint4(lo[4], lo[5], lo[6], lo[7]));
+        for (int v = 0; v < NV; ++v) asm volatile("" : "+f"(d[v]));
+#pragma unroll
+        for (int k = 0; k < Q::NT; ++k) asm volatile("" : "+f"(sc[k]));
+        uint32_t hi[8], lo[8];
+        Q::gen(ST * L::BPS + j, d, sc, hi, lo);
+        const uint32_t a = arow + slot * SLOT + (uint32_t)(j * A_BYTES);
+        st_shared_v4(a, make_uint4(hi[0], hi[1], hi[2], hi[3]));
+        st_shared_v4(a + A_LBO, make_uint4(hi[4], hi[5], hi[6], hi[7]));
+        st_shared_v4(a + A_PART, make_uint4(lo[0], lo[1], lo[2], lo[3]));
+        st_shared_v4(a + A_PART + A_LBO, make_uint4(lo[4], lo[5], lo[6], lo[7]));
+    }
     fence_proxy_async();
     mbar_arrive(smem_u32(&bar_afull[slot]));
     return true;
 }
 
-// All K blocks of one set's parity for pass q.
-template <class Q, int NV>
-__device__ __forceinline__ bool qf_gen_pass(int set, long q, float (&d)[NV], float (&sc)[Q::NT], uint32_t arow,
-                                            uint64_t* bar_empty, uint64_t* bar_afull, volatile int* abort_flag) {
-#pragma unroll
-    for (int s = 0; s < Q::KS; ++s)
-        if ((s & 1) == set && !qf_gen_block<Q, NV>(s, q, d, sc, arow, bar_empty, bar_afull, abort_flag)) return false;
+// The stages lo <= st < hi of one set's parity for pass q.
+template <class Q, int NV, int ST = 0>
+__device__ __forceinline__ bool qf_gen_pass(int set, long q, int lo, int hi, float (&d)[NV], float (&sc)[Q::NT],
+                                            uint32_t arow, uint64_t* bar_empty, uint64_t* bar_afull,
+                                            volatile int* abort_flag) {
+    if constexpr (ST < qf::Layout<Q>::NSTAGE) {
+        if ((ST & 1) == set && ST >= lo && ST < hi &&
+            !qf_gen_stage<Q, NV, ST>(q, d, sc, arow, bar_empty, bar_afull, abort_flag))
+            return false;
+        return qf_gen_pass<Q, NV, ST + 1>(set, q, lo, hi, d, sc, arow, bar_empty, bar_afull, abort_flag);
+    }
     return true;
 }
 
@@ -374,17 +403,23 @@ __global__ void __launch_bounds__(qf::THREADS, 1) qf_eval_kernel(const HolderArg
     // passes of this CTA: NP per tile, tiles blockIdx.x, + gridDim.x, ...
     const long my_tiles = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
     const long npasses = my_tiles * NP;
+    // the shared-memory ring index (pass x KS + block) is kept in 32 bits:
+    // 2^32 / KS passes per CTA, far above any box (2 x 10^9 n-mers are
+    // 2 x 10^5 passes per CTA on 148 SMs)
 
     if (warp < ROW_WARPS) {
         // ---- row threads.  Two sets of 128 threads, thread i of a set on
-        // row i: set 0 (warps 0-3) generates the even K blocks and reads the
+        // row i: set 0 (warps 0-3) generates the even stages and reads the
         // even 16-column chunks of a pass back, set 1 (warps 4-7) the odd
-        // ones.  Software pipeline over the passes: generate pass q + 1, then
-        // read pass q back from its TMEM buffer while the MMAs of pass q + 1
-        // fill the other buffer.  Each set sums its share of a tile's energy
-        // and gradient over the passes in shared memory and adds the totals
-        // to the outputs (zeroed by pair_vars_kernel; two addends onto zero,
-        // so the result does not depend on their order).
+        // ones.  Software pipeline over the passes: generate the first AHEAD
+        // stages of pass q + 1, then read pass q back.  With two TMEM buffers
+        // that is all of pass q + 1, whose MMAs fill the other buffer
+        // meanwhile; with one, the NS stages that fit the ring, written while
+        // the last MMAs of pass q run, so that the MMAs of pass q + 1 start
+        // as soon as pass q is read back.  Each set sums its share of a
+        // tile's energy and gradient over the passes in shared memory and
+        // adds the totals to the outputs (zeroed by pair_vars_kernel; two
+        // addends onto zero, so the result does not depend on their order).
         const int set = warp / 4;
         const int row = tid & 127;
         const uint32_t arow = base + (uint32_t)((row >> 3) * 128 + (row & 7) * 16);
@@ -399,32 +434,29 @@ __global__ void __launch_bounds__(qf::THREADS, 1) qf_eval_kernel(const HolderArg
             for (int v = 0; v < NV; ++v) dv[v] = tt < n ? A.ps.dx[v * cap + tt] : 0.0f;
             return Q::row_scales(dv, sv);
         };
-        float de_[NV], dg[NV], sg[Q::NT];   // variables of the tile read back / being generated
-        float (&de)[NV] = L::DB ? de_ : dg;  // one buffer: the same tile
+        // stages of pass q + 1 generated before pass q is read back (with one
+        // buffer, more would wait for ring slots that only the MMAs of pass
+        // q + 1 free, and those wait for the read-back)
+        constexpr int AHEAD = L::DB ? L::NSTAGE : (NS < L::NSTAGE ? NS : L::NSTAGE);
+        float de[NV], dg[NV], sg[Q::NT];   // variables of the tile read back / being generated
         float rinv_e = 1.0f, rinv_g = 1.0f;
         if (npasses > 0) {
             rinv_g = load_vars(blockIdx.x, dg, sg);
-            if (L::DB) {
 #pragma unroll
-                for (int v = 0; v < NV; ++v) de_[v] = dg[v];
-            }
+            for (int v = 0; v < NV; ++v) de[v] = dg[v];
             rinv_e = rinv_g;
-            if (L::DB && !qf_gen_pass<Q, NV>(set, 0, dg, sg, arow, bar_empty, bar_afull, &s_abort)) goto rows_done;
+            if (!qf_gen_pass<Q, NV>(set, 0, 0, AHEAD, dg, sg, arow, bar_empty, bar_afull, &s_abort)) goto rows_done;
         }
         for (long q = 0; q < npasses; ++q) {
             const int p = (int)(q % NP);
             const long tile = blockIdx.x + (q / NP) * gridDim.x;
-            if (L::DB) {
-                // double-buffered: generate the next pass before reading this one back
-                if (q + 1 < npasses) {
-                    if (p == NP - 1) rinv_g = load_vars(tile + gridDim.x, dg, sg);
-                    if (!qf_gen_pass<Q, NV>(set, q + 1, dg, sg, arow, bar_empty, bar_afull, &s_abort)) goto rows_done;
-                }
-            } else {
-                // one buffer: this pass's MMAs cannot start before the previous
-                // pass is read back, so generate it first
-                if (p == 0 && q > 0) rinv_e = rinv_g = load_vars(tile, dg, sg);
-                if (!qf_gen_pass<Q, NV>(set, q, dg, sg, arow, bar_empty, bar_afull, &s_abort)) goto rows_done;
+            // the rest of pass q, then the first stages of pass q + 1
+            if (!qf_gen_pass<Q, NV>(set, q, AHEAD, L::NSTAGE, dg, sg, arow, bar_empty, bar_afull, &s_abort))
+                goto rows_done;
+            if (q + 1 < npasses) {
+                if (p == NP - 1) rinv_g = load_vars(tile + gridDim.x, dg, sg);
+                if (!qf_gen_pass<Q, NV>(set, q + 1, 0, AHEAD, dg, sg, arow, bar_empty, bar_afull, &s_abort))
+                    goto rows_done;
             }
             const int bi = L::buf(q);
             // warp-uniform: the TMEM loads below are warp-collective
@@ -452,43 +484,44 @@ __global__ void __launch_bounds__(qf::THREADS, 1) qf_eval_kernel(const HolderArg
                     for (int v = 0; v < NV; ++v) atomicAdd(A.ps.g + v * cap + t, park_g[v * 128 + row] * gs);
                     atomicAdd(A.ps.ep + t, (set == 0 ? Q::b0() : 0.0) + park_p[row] * (double)rinv_e);
                 }
-                if (L::DB) {
 #pragma unroll
-                    for (int v = 0; v < NV; ++v) de_[v] = dg[v];
-                    rinv_e = rinv_g;
-                }
+                for (int v = 0; v < NV; ++v) de[v] = dg[v];
+                rinv_e = rinv_g;
             }
         }
     rows_done:;
     } else if (warp == PRODUCER_WARP) {
         // ---- producer: one bulk copy of C's (K block, pass) chunk per stage ----
         if (lane == 0) {
-            long it = 0;
+            uint32_t it = 0, slot = 0, phase = 0;   // ring index, its slot and use parity
             for (long q = 0; q < npasses; ++q) {
                 const int p = (int)(q % NP);
-                for (int s = 0; s < Q::KS; ++s, ++it) {
-                    const int slot = (int)(it % NS);
-                    const long use = it / NS;
-                    if (use > 0 && !wait(smem_u32(&bar_empty[slot]), (uint32_t)((use - 1) & 1), &s_abort))
-                        goto producer_done;
-                    const uint32_t bytes = (uint32_t)Q::chunk_bytes(s, p);
+                for (int st = 0; st < L::NSTAGE; ++st, ++it) {
+                    if (it >= NS && !wait(smem_u32(&bar_empty[slot]), phase ^ 1u, &s_abort)) goto producer_done;
+                    uint32_t bytes = 0;
+                    for (int j = 0; j < L::BPS; ++j) bytes += (uint32_t)Q::chunk_bytes(st * L::BPS + j, p);
                     const uint32_t bar = smem_u32(&bar_bfull[slot]);
                     mbar_arrive_tx(bar, bytes);
-                    bulk_g2s(base + (uint32_t)(slot * SLOT + A_BYTES), Q::image() + Q::chunk_offset(s, p), bytes, bar);
+                    for (int j = 0; j < L::BPS; ++j) {
+                        const int s = st * L::BPS + j;
+                        bulk_g2s(base + slot * SLOT + (uint32_t)(L::BOFF + j * L::BCHUNK),
+                                 Q::image() + Q::chunk_offset(s, p), (uint32_t)Q::chunk_bytes(s, p), bar);
+                    }
+                    if (++slot == NS) slot = 0, phase ^= 1u;
                 }
             }
         producer_done:
             // copies in flight complete on their own: wait for them before the
             // shared memory goes away (the last use of every slot)
-            for (int k = 0; k < NS && k < it; ++k) {
-                const long qq = it - 1 - k;   // stage iteration of the last copy into slot qq % NS
-                wait_drain(smem_u32(&bar_bfull[qq % NS]), (uint32_t)((qq / NS) & 1));
+            for (uint32_t k = 0; k < NS && k < it; ++k) {
+                const uint32_t qq = it - 1 - k;   // ring index of the last copy into slot qq % NS
+                wait_drain(smem_u32(&bar_bfull[qq % NS]), (qq / NS) & 1u);
             }
         }
     } else {
         // ---- MMA issuer ----
         if (lane == 0) {
-            long it = 0;
+            uint32_t slot = 0, phase = 0;   // ring slot and use parity
             bool issued = false;
             for (long q = 0; q < npasses; ++q) {
                 const int p = (int)(q % NP);
@@ -502,23 +535,28 @@ __global__ void __launch_bounds__(qf::THREADS, 1) qf_eval_kernel(const HolderArg
                 const int nn = Q::pass_n(p);
                 const uint32_t id = idesc(nn), blbo = (uint32_t)(nn / 8) * 128, bpart = (uint32_t)nn * 32;
                 const uint32_t dmain = tmem + (uint32_t)(b * 256), dcorr = dmain + (uint32_t)L::CORR_COL;
-                for (int s = 0; s < Q::KS; ++s, ++it) {
-                    const int slot = (int)(it % NS);
-                    const uint32_t par = (uint32_t)((it / NS) & 1);
-                    if (!wait(smem_u32(&bar_afull[slot]), par, &s_abort)) goto mma_done;
-                    if (!wait(smem_u32(&bar_bfull[slot]), par, &s_abort)) goto mma_done;
+                // descriptors of slot 0; a slot's are these plus its offset
+                // (the 14-bit address field holds every shared address >> 4)
+                const uint64_t da0 = sdesc(base, A_LBO), db0 = sdesc(base + L::BOFF, blbo);
+                for (int st = 0; st < L::NSTAGE; ++st) {
+                    if (!wait(smem_u32(&bar_afull[slot]), phase, &s_abort)) goto mma_done;
+                    if (!wait(smem_u32(&bar_bfull[slot]), phase, &s_abort)) goto mma_done;
                     tc_after();
-                    const uint32_t sa = base + (uint32_t)(slot * SLOT);
-                    const uint32_t sb = sa + A_BYTES;
-                    const uint64_t a_hi = sdesc(sa, A_LBO), a_lo = sdesc(sa + A_PART, A_LBO);
-                    const uint64_t b_hi = sdesc(sb, blbo), b_mid = sdesc(sb + bpart, blbo);
-                    const uint32_t acc = s > 0 ? 1u : 0u;
-                    mma(dmain, a_hi, b_hi, id, acc);          // main: hi.hi
-                    mma(dcorr, a_hi, b_mid, id, acc);         // corrections
-                    mma(dcorr, a_lo, b_hi, id, 1u);
-                    if (s < Q::KT) mma(dcorr, a_hi, sdesc(sb + 2 * bpart, blbo), id, 1u);
+                    const uint64_t off = (uint64_t)((slot * SLOT) >> 4);
+#pragma unroll
+                    for (int j = 0; j < L::BPS; ++j) {
+                        const int s = st * L::BPS + j;
+                        const uint64_t a_hi = da0 + off + (uint64_t)(j * A_BYTES >> 4), a_lo = a_hi + (A_PART >> 4);
+                        const uint64_t b_hi = db0 + off + (uint64_t)(j * L::BCHUNK >> 4), b_mid = b_hi + (bpart >> 4);
+                        const uint32_t acc = s > 0 ? 1u : 0u;
+                        mma(dmain, a_hi, b_hi, id, acc);          // main: hi.hi
+                        mma(dcorr, a_hi, b_mid, id, acc);         // corrections
+                        mma(dcorr, a_lo, b_hi, id, 1u);
+                        if (s < Q::KT) mma(dcorr, a_hi, b_mid + (bpart >> 4), id, 1u);
+                    }
                     commit(smem_u32(&bar_empty[slot]));
                     issued = true;
+                    if (++slot == NS) slot = 0, phase ^= 1u;
                 }
                 commit(smem_u32(&bar_tfull[b]));
             }
