@@ -530,9 +530,33 @@ def emit_vars(spec, out):
         fn = "var_exp" if kind == "exp" else "var_coul"
         w("    x[%d] = %s(s[%d], s[%d], %s, %s);" % (v, fn, a, b, lit(k), lit(d0)))
     w("}")
-    # chain rule: site gradients from dP/dv (g), scaled by sw
-    w("__device__ __forceinline__ void %s_chain(const double (&s)[%d][3], const double (&g)[%d], "
-      "double (&sg)[%d][3]) {" % (spec.name, ns, nv, ns))
+    # the variables with their radial factors, for a chain rule in another
+    # kernel that reads the factors back (NAME_chain_q); q.put(v, factor)
+    # stores each as soon as it is known
+    w("template <class QW>")
+    w("__device__ __forceinline__ void %s_vars_q(const double (&s)[%d][3], double (&x)[%d], QW& q) {" %
+      (spec.name, ns, nv))
+    for v, (kind, a, b, k, d0) in enumerate(spec.variables):
+        fn = "var_exp_q" if kind == "exp" else "var_coul_q"
+        w("    { double f; x[%d] = %s(s[%d], s[%d], %s, %s, f); q.put(%d, f); }" % (v, fn, a, b, lit(k), lit(d0), v))
+    w("}")
+    w("template <class G, class Q>")
+    w("__device__ __forceinline__ void %s_chain_q(const double (&s)[%d][3], const G& g, const Q& q, "
+      "double (&sg)[%d][3]) {" % (spec.name, ns, ns))
+    w("#pragma unroll")
+    w("    for (int i = 0; i < %d; ++i) { sg[i][0] = 0.0; sg[i][1] = 0.0; sg[i][2] = 0.0; }" % ns)
+    for v, (kind, a, b, k, d0) in enumerate(spec.variables):
+        w("    dvar_q(s[%d], s[%d], g[%d], q[%d], sg[%d], sg[%d]);" % (a, b, v, v, a, b))
+    for (m, o, xp, xm) in spec.lp:
+        w("    lp_grads(s[%d], s[%d], s[%d], sg[%d], sg[%d], sg[%d], sg[%d], sg[%d]);" %
+          (o, o + 1, o + 2, xp, xm, o, o + 1, o + 2))
+    w("}")
+    # chain rule: site gradients from dP/dv (g, an array of NVARS doubles or
+    # anything indexable the same way, e.g. a reader of the FP32 gradients in
+    # global memory that loads each where it is used), scaled by sw
+    w("template <class G>")
+    w("__device__ __forceinline__ void %s_chain(const double (&s)[%d][3], const G& g, "
+      "double (&sg)[%d][3]) {" % (spec.name, ns, ns))
     w("#pragma unroll")
     w("    for (int i = 0; i < %d; ++i) { sg[i][0] = 0.0; sg[i][1] = 0.0; sg[i][2] = 0.0; }" % ns)
     for v, (kind, a, b, k, d0) in enumerate(spec.variables):
@@ -587,8 +611,12 @@ def emit_traits(spec, table, straight, out):
       (spec.nreal, ns, n))
     w("    __device__ __forceinline__ static void vars(const double (&s)[%d][3], double (&x)[%d]) { %s_vars(s, x); }" %
       (ns, spec.nvars, n))
-    w("    __device__ __forceinline__ static void chain(const double (&s)[%d][3], const double (&g)[%d], double (&sg)[%d][3]) "
-      "{ %s_chain(s, g, sg); }" % (ns, spec.nvars, ns, n))
+    w("    template <class G> __device__ __forceinline__ static void chain(const double (&s)[%d][3], const G& g, "
+      "double (&sg)[%d][3]) { %s_chain(s, g, sg); }" % (ns, ns, n))
+    w("    template <class QW> __device__ __forceinline__ static void vars_q(const double (&s)[%d][3], "
+      "double (&x)[%d], QW& q) { %s_vars_q(s, x, q); }" % (ns, spec.nvars, n))
+    w("    template <class G, class Q> __device__ __forceinline__ static void chain_q(const double (&s)[%d][3], "
+      "const G& g, const Q& q, double (&sg)[%d][3]) { %s_chain_q(s, g, q, sg); }" % (ns, ns, n))
     if straight:
         w("    template <class C> __device__ __forceinline__ static double pip(const C& c, const double (&x)[%d], "
           "double (&g)[%d]) { return %s_pip(c, x, g); }" % (spec.nvars, spec.nvars, n))
@@ -939,7 +967,7 @@ int mbx_launch_%(name)s_s(const HolderArgs& A, int grid, int block, cudaStream_t
     // variables and gradient accumulators of the block in dynamic shared
     // memory), the FP64 chain rule and sums at full occupancy; A.ps holds the
     // scratch between them (capacity A.ps.cap >= A.n)
-    if (!A.ps.dx || A.ps.cap < A.n) return (int)cudaErrorInvalidValue;
+    if (!A.ps.dx || !A.ps.q || A.ps.cap < A.n) return (int)cudaErrorInvalidValue;
     auto kern = pair_trie_kernel<%(name)s_T, %(name)s_CS>;
     block = %(name)s_T::LOCK_THREADS_S;
     const int smem = 2 * %(name)s_T::NVARS * %(name)s_T::LOCK_THREADS_S * (int)sizeof(f2_t);
@@ -1118,7 +1146,7 @@ int mbx_launch_%(name)s_s(const HolderArgs& A, int grid, int block, cudaStream_t
     // (qf_eval_kernel: one CTA per SM, persistent over tiles of 128 n-mers),
     // the FP64 chain rule and sums at full occupancy (pair_finish_kernel);
     // A.ps holds the scratch between them (capacity A.ps.cap >= A.n)
-    if (!A.ps.dx || A.ps.cap < A.n) return (int)cudaErrorInvalidValue;
+    if (!A.ps.dx || !A.ps.q || A.ps.cap < A.n) return (int)cudaErrorInvalidValue;
     auto kern = qf_eval_kernel<%(name)s_T, %(name)s_Q>;
     static LaunchCache lc;
     int sms = 0, bps = 0;

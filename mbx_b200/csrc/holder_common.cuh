@@ -100,6 +100,38 @@ __device__ __forceinline__ void dvar_coul(const double (&p1)[3], const double (&
     sg2[0] -= f * a; sg2[1] -= f * b; sg2[2] -= f * c;
 }
 
+// The variable together with its radial factor q, dv/d(p1 - p2) = q (p1 - p2),
+// by the same operations as var_exp / dvar_exp (var_coul / dvar_coul), so that
+// a chain rule from a stored q (dvar_q) gives the same bits as dvar_exp does.
+__device__ __forceinline__ double var_exp_q(const double (&p1)[3], const double (&p2)[3], double k, double d0,
+                                           double& q) {
+    double a, b, c;
+    const double r = dist3(p1, p2, a, b, c);
+    const double v = exp(k * (d0 - r));
+    q = -k * v / r;
+    return v;
+}
+
+__device__ __forceinline__ double var_coul_q(const double (&p1)[3], const double (&p2)[3], double k, double d0,
+                                            double& q) {
+    double a, b, c;
+    const double r = dist3(p1, p2, a, b, c);
+    const double rinv = 1.0 / r;
+    const double v = exp(k * (d0 - r)) * rinv;
+    q = -(k + rinv) * v * rinv;
+    return v;
+}
+
+// Adds gv q (p1 - p2) to sg1 and subtracts it from sg2 (dvar_exp / dvar_coul
+// with the radial factor q already known).
+__device__ __forceinline__ void dvar_q(const double (&p1)[3], const double (&p2)[3], double gv, double q,
+                                       double (&sg1)[3], double (&sg2)[3]) {
+    const double a = p1[0] - p2[0], b = p1[1] - p2[1], c = p1[2] - p2[2];
+    const double f = gv * q;
+    sg1[0] += f * a; sg1[1] += f * b; sg1[2] += f * c;
+    sg2[0] -= f * a; sg2[1] -= f * b; sg2[2] -= f * c;
+}
+
 // The two lone-pair sites of a water (O, H1, H2).
 __device__ __forceinline__ void lp_sites(const double (&o)[3], const double (&h1)[3], const double (&h2)[3],
                                          double (&xp)[3], double (&xm)[3]) {

@@ -32,6 +32,7 @@ enum { HM_ENERGY = 0, HM_GRAD_FP64 = 1, HM_GRAD_SHIFT32 = 4 };
 // polynomial's value and whether the n-mer is within the evaluator's cutoff.
 struct PairScratch {
     float* dx;
+    double* q;    // radial factor of each variable (var_exp_q), for the chain rule of pair_finish_kernel
     float* g;
     double* ep;
     unsigned char* live;
@@ -244,10 +245,41 @@ __device__ __forceinline__ void conf_accumulate(double* dst, const double (&v)[7
     }
 }
 
-// Everything after the polynomial: chain rule, switch, virial, scatter.
+// The chain rule from dP/dv: g is an array of T::NVARS doubles, or a reader
+// indexed the same way; PairFactors (below) also brings the variables'
+// radial factors, so that nothing is recomputed.
+template <class T, class G>
+__device__ __forceinline__ void chain_rule(const double (&s)[T::NSITES][3], const G& g, double (&sg)[T::NSITES][3]) {
+    T::chain(s, g, sg);
+}
+
+// dP/dv (FP32) and the radial factors (FP64) of n-mer t in the mixed path's
+// scratch, read where the chain rule uses them
+struct PairGrad {
+    const float* __restrict__ g;
+    long cap, t;
+    __device__ __forceinline__ double operator[](int v) const { return (double)__ldg(g + v * cap + t); }
+};
+struct PairQ {
+    const double* __restrict__ q;
+    long cap, t;
+    __device__ __forceinline__ double operator[](int v) const { return __ldcs(q + v * cap + t); }
+};
+struct PairFactors {
+    PairGrad g;
+    PairQ q;
+};
 template <class T>
-__device__ __forceinline__ void finish_nmer(const HolderArgs& A, long t, double ep, const double (&g)[T::NVARS],
-                                            bool grads, double (&acc)[7]) {
+__device__ __forceinline__ void chain_rule(const double (&s)[T::NSITES][3], const PairFactors& f,
+                                           double (&sg)[T::NSITES][3]) {
+    T::chain_q(s, f.g, f.q, sg);
+}
+
+// Everything after the polynomial: chain rule, switch, virial, scatter.  g:
+// dP/dv as chain_rule takes it.
+template <class T, class G>
+__device__ __forceinline__ void finish_nmer(const HolderArgs& A, long t, double ep, const G& g, bool grads,
+                                            double (&acc)[7]) {
     double r[T::NREAL][3];
     load_nmer<T, true>(A, t, r);
     double d[3][3], rr[3];
@@ -256,7 +288,7 @@ __device__ __forceinline__ void finish_nmer(const HolderArgs& A, long t, double 
     if (grads) {
         double s[T::NSITES][3], sg[T::NSITES][3];
         T::sites(r, s);
-        T::chain(s, g, sg);
+        chain_rule<T>(s, g, sg);
 #pragma unroll
         for (int i = 0; i < T::NREAL; ++i)
 #pragma unroll
@@ -480,7 +512,8 @@ __global__ void __launch_bounds__(T::LOCK_THREADS, 1) holder_lock_kernel(const H
 // to FP32 (x itself is built in FP64).  Returns false, with x = 0, for t >= n
 // or an n-mer beyond the evaluator's cutoff.
 template <class T>
-__device__ __forceinline__ bool nmer_vars_f32(const HolderArgs& A, long t, long n, float (&xf)[T::NVARS]) {
+__device__ __forceinline__ bool nmer_vars_f32(const HolderArgs& A, long t, long n, float (&xf)[T::NVARS],
+                                              double* q = nullptr) {
     double x[T::NVARS];
 #pragma unroll
     for (int v = 0; v < T::NVARS; ++v) x[v] = 0.0;
@@ -495,7 +528,19 @@ __device__ __forceinline__ bool nmer_vars_f32(const HolderArgs& A, long t, long 
         } else {
             double s[T::NSITES][3];
             T::sites(r, s);
-            T::vars(s, x);
+            if (q) {
+                // with the radial factors, stored for pair_finish_kernel as
+                // they are computed (streaming stores: read once, by that
+                // kernel, they should not push other data out of L2)
+                struct {
+                    double* p;
+                    long cap, t;
+                    __device__ __forceinline__ void put(int v, double f) { __stcs(p + v * cap + t, f); }
+                } qw{q, A.ps.cap, t};
+                T::vars_q(s, x, qw);
+            } else {
+                T::vars(s, x);
+            }
         }
     }
     T::shift(x, xf);
@@ -521,7 +566,7 @@ __global__ void __launch_bounds__(256, 2) pair_vars_kernel(const HolderArgs A) {
     const long cap = A.ps.cap;
     for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
         float xf[T::NVARS];
-        const bool live = nmer_vars_f32<T>(A, t, n, xf);
+        const bool live = nmer_vars_f32<T>(A, t, n, xf, A.ps.q);
 #pragma unroll
         for (int v = 0; v < T::NVARS; ++v) {
             A.ps.dx[v * cap + t] = xf[v];
@@ -600,10 +645,9 @@ __global__ void __launch_bounds__(128, 4) pair_finish_kernel(const HolderArgs A)
     const long cap = A.ps.cap;
     for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
         if (!A.ps.live[t]) continue;
-        double g[T::NVARS];
-#pragma unroll
-        for (int v = 0; v < T::NVARS; ++v) g[v] = (double)A.ps.g[v * cap + t];
-        finish_nmer<T>(A, t, A.ps.ep[t], g, true, acc);
+        // the chain rule from the radial factors pair_vars_kernel stored: no
+        // square root, exponential or division per variable here
+        finish_nmer<T>(A, t, A.ps.ep[t], PairFactors{{A.ps.g, cap, t}, {A.ps.q, cap, t}}, true, acc);
     }
     block_reduce_add<7>(acc, A.out);
 }

@@ -882,13 +882,15 @@ static int launch_eval(mbx_ctx* c, const EvaluatorInfo* E, HolderArgs A, int fla
         auto up = [](size_t b) { return (b + 255) & ~(size_t)255; };
         const long cap = std::max<long>(A.n, 1);
         const size_t vb = up((size_t)E->nvars * cap * sizeof(float));
+        const size_t qb = 2 * vb;   // FP64 radial factors
         const size_t eb = up((size_t)cap * sizeof(double));
-        CUCHK(c, c->pair_scratch.ensure(2 * vb + eb + up((size_t)cap)));
+        CUCHK(c, c->pair_scratch.ensure(qb + 2 * vb + eb + up((size_t)cap)));
         unsigned char* base = c->pair_scratch.p;
-        A.ps.dx = reinterpret_cast<float*>(base);
-        A.ps.g = reinterpret_cast<float*>(base + vb);
-        A.ps.ep = reinterpret_cast<double*>(base + 2 * vb);
-        A.ps.live = base + 2 * vb + eb;
+        A.ps.q = reinterpret_cast<double*>(base);
+        A.ps.dx = reinterpret_cast<float*>(base + qb);
+        A.ps.g = reinterpret_cast<float*>(base + qb + vb);
+        A.ps.ep = reinterpret_cast<double*>(base + qb + 2 * vb);
+        A.ps.live = base + qb + 2 * vb + eb;
         A.ps.cap = cap;
         A.ps.err = c->status.p;   // status word: MBX_STATUS_WAIT_TIMEOUT
     }
@@ -1272,6 +1274,17 @@ static int sync_child(mbx_ctx* c) {
     if (!c->child) {
         int r = mbx_create(&c->child, c->device, nullptr);
         if (r) return fail(c, r, "child context");
+        // the 2b term's stream at the device's highest priority: the 3b
+        // term is enqueued first and its tensor-core kernel takes whole SMs,
+        // so at equal priority the 2b evaluation waits for SMs behind the
+        // 3b kernels and ends the step; first pick of the SMs that free up
+        // lets the two terms end closer together
+        int lo = 0, hi = 0;
+        cudaStream_t hs = nullptr;
+        CUCHK(c, cudaDeviceGetStreamPriorityRange(&lo, &hi));
+        CUCHK(c, cudaStreamCreateWithPriority(&hs, cudaStreamNonBlocking, hi));
+        CUCHK(c, cudaStreamDestroy(c->child->stream));
+        c->child->stream = hs;
     }
     mbx_ctx* k = c->child;
     std::vector<const char*> ids(c->nmon);
