@@ -227,10 +227,11 @@ void sorted_slots(int nb, const std::string* ids, int* idx) {
 // side on their own streams.
 struct BuildScratch {
     DevBuf<double> cloud;
-    DevBuf<int> cell_of, cell_count, cell_start, cell_fill, cell_items, cell_sorted, nb_count;
+    DevBuf<int> cell_of, cell_count, cell_start, cell_fill, cell_items, cell_sorted, nb_count, copy_dir;
     DevBuf<NbEntry> nb;
     void release() {
         cloud.release();
+        copy_dir.release();
         cell_of.release();
         cell_count.release();
         cell_start.release();
@@ -241,7 +242,6 @@ struct BuildScratch {
         nb.release();
     }
 };
-#define MBX_BUILD_LANES 4   // concurrent searches of a batch (streams + scratch sets)
 // pinned result block (h_out, 64 doubles): [0..7) term energy + virial, [8]
 // listed n-mers, then the bucket counts (ints) and the status words (2 ints)
 #define MBX_H_COUNTS 9
@@ -291,9 +291,7 @@ struct mbx_ctx {
     // work buffers
     DevBuf<double> xyz, grad, out, coef_ws;
     DevBuf<int> bucket_count, status, counters;
-    BuildScratch scratch[MBX_BUILD_LANES];   // [0]: every single-system search
-    cudaStream_t lane_stream[MBX_BUILD_LANES] = {nullptr};   // [0] unused (the context stream)
-    cudaEvent_t lane_fork = nullptr, lane_join[MBX_BUILD_LANES] = {nullptr};
+    BuildScratch scratch;   // of every search (a batch searches all its configurations at once)
     // code prefetch of a term's evaluation kernels, beside its n-mer search
     cudaStream_t prime_stream = nullptr;
     cudaEvent_t prime_fork = nullptr, prime_join = nullptr;
@@ -321,6 +319,12 @@ struct mbx_ctx {
     std::vector<int> conf_mon;
     std::vector<BoxParams> conf_bp;
     DevBuf<BoxParams> d_conf_bp;
+    // batched search: every configuration's grid for the term's cutoff, its
+    // cells concatenated (ncell in all), built for context generation gen
+    DevBuf<BatchGrid> d_bgrid[4];
+    int bgrid_ncell[4] = {0, 0, 0, 0};
+    unsigned long bgrid_gen[4] = {0, 0, 0, 0};
+    double bgrid_cut[4] = {0, 0, 0, 0};
     DevBuf<int> d_mon_conf;
     DevBuf<double> conf_out;
     double* h_conf = nullptr;   // pinned, 8 per configuration
@@ -383,15 +387,10 @@ int mbx_create(mbx_ctx** out, int device, void* stream) {
     }
     CUCHK(c, cudaMallocHost(&c->h_out, 64 * sizeof(double)));
     for (int i = 0; i < 3; ++i) CUCHK(c, cudaEventCreate(&c->ev[i]));
-    CUCHK(c, cudaEventCreateWithFlags(&c->lane_fork, cudaEventDisableTiming));
     CUCHK(c, cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
     CUCHK(c, cudaStreamCreateWithFlags(&c->prime_stream, cudaStreamNonBlocking));
     CUCHK(c, cudaEventCreateWithFlags(&c->prime_fork, cudaEventDisableTiming));
     CUCHK(c, cudaEventCreateWithFlags(&c->prime_join, cudaEventDisableTiming));
-    for (int i = 1; i < MBX_BUILD_LANES; ++i) {
-        CUCHK(c, cudaStreamCreateWithFlags(&c->lane_stream[i], cudaStreamNonBlocking));
-        CUCHK(c, cudaEventCreateWithFlags(&c->lane_join[i], cudaEventDisableTiming));
-    }
 
     CUCHK(c, c->out.ensure(64));
     CUCHK(c, c->status.ensure(4));
@@ -422,12 +421,7 @@ int mbx_destroy(mbx_ctx* c) {
     for (auto* b : ib) b->release();
     DevBuf<double>* db[] = {&c->xyz, &c->grad, &c->out, &c->coef_ws};
     for (auto* b : db) b->release();
-    for (auto& sc : c->scratch) sc.release();
-    for (int i = 1; i < MBX_BUILD_LANES; ++i) {
-        if (c->lane_stream[i]) cudaStreamDestroy(c->lane_stream[i]);
-        if (c->lane_join[i]) cudaEventDestroy(c->lane_join[i]);
-    }
-    if (c->lane_fork) cudaEventDestroy(c->lane_fork);
+    c->scratch.release();
     if (c->ev_fork) cudaEventDestroy(c->ev_fork);
     if (c->prime_stream) {
         cudaStreamSynchronize(c->prime_stream);
@@ -442,6 +436,7 @@ int mbx_destroy(mbx_ctx* c) {
     c->listed.release();
     c->d_conf_bp.release();
     c->d_mon_conf.release();
+    for (auto& g : c->d_bgrid) g.release();
     c->conf_out.release();
     if (c->h_out) cudaFreeHost(c->h_out);
     for (int i = 0; i < 3; ++i) cudaEventDestroy(c->ev[i]);
@@ -723,6 +718,12 @@ static CellGrid make_grid(const BoxParams& bp, double rc, int nmem) {
                              vol / std::sqrt(ca[0] * ca[0] + ca[1] * ca[1] + ca[2] * ca[2]),
                              vol / std::sqrt(ab[0] * ab[0] + ab[1] * ab[1] + ab[2] * ab[2])};
         for (int k = 0; k < 3; ++k) g.n[k] = std::max(1, std::min(64, (int)std::floor(h[k] / rc)));
+        // one cloud point per candidate when every axis has 3 or more cells,
+        // each wider than the cutoff by a margin far above rounding (the
+        // search then tests only the copy the cell's wrap implies)
+        g.one_copy = 1;
+        for (int k = 0; k < 3; ++k)
+            if (g.n[k] < 3 || h[k] / g.n[k] < rc * (1.0 + 1e-9)) g.one_copy = 0;
     } else {
         // hashed grid: cell = floor(x / rc) mod n on every axis
         const int n = std::max(3, std::min(32, (int)std::ceil(std::cbrt((double)nmem / 2.0))));
@@ -772,9 +773,9 @@ struct BuildScope {
 // the counters are zeroed by prepare_buckets) and, when list_cap > 0, into
 // c->list.  Asynchronous; status and counts on device.
 static int launch_build_scope(mbx_ctx* c, int nbody, const BuildScope& S, const double* xyz, long list_cap,
-                              int* kernels, bool mixed, int lane = 0) {
-    BuildScratch& B = c->scratch[lane];
-    cudaStream_t st = lane ? c->lane_stream[lane] : c->stream;
+                              int* kernels, bool mixed) {
+    BuildScratch& B = c->scratch;
+    cudaStream_t st = c->stream;
     const int nmem = S.nmem, nq = S.nq;
     if (nmem < 2 || (nbody == 3 && nmem < 3) || nq == 0) return MBX_OK;
     const double rc = c->cutoff[nbody];
@@ -782,6 +783,7 @@ static int launch_build_scope(mbx_ctx* c, int nbody, const BuildScope& S, const 
     CellGrid cg = make_grid(S.bp, rc, nmem);
     const int ncell = cg.n[0] * cg.n[1] * cg.n[2];
     CUCHK(c, B.cloud.ensure((size_t)std::max(nmem, 1) * 24));
+    CUCHK(c, B.copy_dir.ensure(std::max(nmem, 1)));
     CUCHK(c, B.cell_of.ensure(std::max(nmem, 1)));
     CUCHK(c, B.cell_items.ensure(std::max(nmem, 1)));
     CUCHK(c, B.cell_sorted.ensure(std::max(nmem, 1)));
@@ -793,7 +795,7 @@ static int launch_build_scope(mbx_ctx* c, int nbody, const BuildScope& S, const 
     CUCHK(c, cudaMemsetAsync(B.cell_count.p, 0, (ncell + 1) * sizeof(int), st));
     const int T = 128;
     k_cloud<<<(nmem + T - 1) / T, T, 0, st>>>(xyz, c->d_first.p, S.members, nmem, S.bp, cg, B.cloud.p,
-                                                     B.cell_of.p);
+                                                     B.cell_of.p, B.copy_dir.p);
     k_cell_count<<<(nmem + T - 1) / T, T, 0, st>>>(B.cell_of.p, nmem, B.cell_count.p);
     k_cell_scan<<<1, 1024, 0, st>>>(B.cell_count.p, ncell, B.cell_start.p, B.cell_fill.p);
     k_cell_fill<<<(nmem + T - 1) / T, T, 0, st>>>(B.cell_of.p, nmem, B.cell_fill.p, B.cell_items.p);
@@ -804,7 +806,7 @@ static int launch_build_scope(mbx_ctx* c, int nbody, const BuildScope& S, const 
     const auto& K = c->knobs[nbody];
     const int nbw = (size_t)4 * c->nb_cap * sizeof(NbEntry) <= 160 * 1024 ? K.nb_warps : 1;
     if ((size_t)c->nb_cap * sizeof(NbEntry) > 227 * 1024) return fail(c, MBX_ENOMEM, "neighbour staging");
-    RCHK(c, launch_neighbors(nbw, K.nb_unroll, B.cloud.p, B.cell_of.p, B.cell_start.p, B.cell_sorted.p,
+    RCHK(c, launch_neighbors(nbw, K.nb_unroll, B.cloud.p, B.copy_dir.p, B.cell_of.p, B.cell_start.p, B.cell_sorted.p,
                              S.query, nq, cg, S.bp.use_pbc, rc2, c->nb_cap, B.nb_count.p, B.nb.p, c->status.p,
                              st));
     if (nbody == 2) {
@@ -839,6 +841,98 @@ static int launch_build(mbx_ctx* c, int nbody, int use_ghost, const double* xyz,
     if (r) return r;
     BuildScope S{c->d_members[g].p, c->nmem[g], c->d_query[g].p, c->nquery[g], c->bp};
     return launch_build_scope(c, nbody, S, xyz, list_cap, kernels, mixed);
+}
+
+// The grids of a batched search for term nbody (BatchGrid per configuration,
+// cells concatenated), uploaded when the batch or the cutoff changed.  The
+// upload is synchronous, so it must not happen inside a graph capture; every
+// capture follows a plain run of the same sequence, which leaves them fresh.
+static int ensure_batch_grids(mbx_ctx* c, int nbody) {
+    const double rc = c->cutoff[nbody];
+    if (c->d_bgrid[nbody].p && c->bgrid_gen[nbody] == c->gen && c->bgrid_cut[nbody] == rc) return MBX_OK;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CUCHK(c, cudaStreamIsCapturing(c->stream, &cs));
+    if (cs != cudaStreamCaptureStatusNone) return fail(c, MBX_EINVAL, "batch grids changed inside a graph capture");
+    std::vector<BatchGrid> g(c->nconf);
+    long ncell = 0;
+    for (int k = 0; k < c->nconf; ++k) {
+        g[k].bp = c->conf_bp[k];
+        g[k].cg = make_grid(c->conf_bp[k], rc, std::max(c->conf_mon[k + 1] - c->conf_mon[k], 1));
+        g[k].cell_off = (int)ncell;
+        ncell += (long)g[k].cg.n[0] * g[k].cg.n[1] * g[k].cg.n[2];
+    }
+    if (ncell >= (1L << 30)) return fail(c, MBX_ENOMEM, "batched cell grid too large");
+    CUCHK(c, c->d_bgrid[nbody].ensure(c->nconf));
+    CUCHK(c, cudaMemcpy(c->d_bgrid[nbody].p, g.data(), c->nconf * sizeof(BatchGrid), cudaMemcpyHostToDevice));
+    c->bgrid_ncell[nbody] = (int)ncell;
+    c->bgrid_gen[nbody] = c->gen;
+    c->bgrid_cut[nbody] = rc;
+    return MBX_OK;
+}
+
+// A whole batch as one search: members and queries are the batch's monomers
+// (the identity list of its all-local topology), each searching the cells of
+// its own configuration (k_cloud_batch, k_neighbors_batch); the cell kernels
+// run once over every configuration's cells, the dimer and trimer rules once
+// over every query.  One launch per kernel for the batch, where a search per
+// configuration took ~8 small launches each.
+static int launch_build_batch(mbx_ctx* c, int nbody, const double* xyz, int* kernels, bool mixed) {
+    int r = ensure_batch_grids(c, nbody);
+    if (r) return r;
+    BuildScratch& B = c->scratch;
+    cudaStream_t st = c->stream;
+    const int nmem = c->nmon, nq = c->nmon;
+    if (nmem < 2 || (nbody == 3 && nmem < 3)) return MBX_OK;
+    const double rc = c->cutoff[nbody];
+    const double rc2 = rc * rc;
+    const int ncell = c->bgrid_ncell[nbody];
+    const int* ids = c->d_members[0].p;   // identity: member position = monomer = query
+    CUCHK(c, B.cloud.ensure((size_t)nmem * 24));
+    CUCHK(c, B.copy_dir.ensure(nmem));
+    CUCHK(c, B.cell_of.ensure(nmem));
+    CUCHK(c, B.cell_items.ensure(nmem));
+    CUCHK(c, B.cell_sorted.ensure(nmem));
+    CUCHK(c, B.cell_count.ensure(ncell + 1));
+    CUCHK(c, B.cell_start.ensure(ncell + 1));
+    CUCHK(c, B.cell_fill.ensure(ncell + 1));
+    CUCHK(c, B.nb_count.ensure(nq));
+    CUCHK(c, B.nb.ensure((size_t)nq * c->nb_cap));
+    CUCHK(c, cudaMemsetAsync(B.cell_count.p, 0, (ncell + 1) * sizeof(int), st));
+    const int T = 128;
+    k_cloud_batch<<<(nmem + T - 1) / T, T, 0, st>>>(xyz, c->d_first.p, nmem, c->d_mon_conf.p, c->d_bgrid[nbody].p,
+                                                    B.cloud.p, B.cell_of.p, B.copy_dir.p);
+    k_cell_count<<<(nmem + T - 1) / T, T, 0, st>>>(B.cell_of.p, nmem, B.cell_count.p);
+    k_cell_scan<<<1, 1024, 0, st>>>(B.cell_count.p, ncell, B.cell_start.p, B.cell_fill.p);
+    k_cell_fill<<<(nmem + T - 1) / T, T, 0, st>>>(B.cell_of.p, nmem, B.cell_fill.p, B.cell_items.p);
+    k_cell_sort<<<(int)(((long)ncell * 32 + T - 1) / T), T, 0, st>>>(B.cell_start.p, ncell, B.cell_items.p,
+                                                                      B.cell_sorted.p);
+    const auto& K = c->knobs[nbody];
+    const int nbw = (size_t)4 * c->nb_cap * sizeof(NbEntry) <= 160 * 1024 ? K.nb_warps : 1;
+    if ((size_t)c->nb_cap * sizeof(NbEntry) > 227 * 1024) return fail(c, MBX_ENOMEM, "neighbour staging");
+    RCHK(c, launch_neighbors_batch(nbw, K.nb_unroll, B.cloud.p, B.copy_dir.p, B.cell_of.p, B.cell_start.p,
+                                   B.cell_sorted.p, ids, nq,
+                                   c->d_mon_conf.p, c->d_bgrid[nbody].p, rc2, c->nb_cap, B.nb_count.p, B.nb.p,
+                                   c->status.p, st));
+    if (nbody == 2) {
+        DimerRules R = c->drules;
+        if (!mixed)
+            for (int b = 0; b < MBX_MAX_BUCKETS; ++b) R.split2[b] = 0.0;   // no short-range split
+        const int DT = K.dim_threads;
+        k_dimers<<<(int)(((long)nq * 32 + DT - 1) / DT), DT, 0, st>>>(
+            ids, nq, ids, c->d_tag.p, c->d_type.p, B.nb_count.p, B.nb.p, c->nb_cap, rc2, R, c->listed.p, nullptr, 0,
+            c->buckets.p, c->bucket_count.p, c->status.p);
+    } else {
+        const size_t smem = (size_t)c->nb_cap * MBX_TRIMATCH_BYTES;
+        if (smem > 227 * 1024) return fail(c, MBX_ENOMEM, "trimer staging exceeds shared memory");
+        if (smem > 48 * 1024)
+            CUCHK(c, cudaFuncSetAttribute(k_trimers, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_trimers<<<nq, K.tri_threads, smem, st>>>(ids, nq, ids, c->d_tag.p, c->d_type.p, B.cloud.p, B.nb_count.p,
+                                                    B.nb.p, c->nb_cap, rc2, c->trules, c->listed.p, nullptr, 0,
+                                                    c->buckets.p, c->bucket_count.p, c->status.p);
+    }
+    CUCHK(c, cudaGetLastError());
+    *kernels += 8;
+    return MBX_OK;
 }
 
 static HolderArgs base_args(mbx_ctx* c) {
@@ -1716,24 +1810,9 @@ static int batch_sequence(mbx_ctx* c, int nbody, double* X, double* G, bool grad
     if (r) return r;
     r = launch_prime(c, nbody, (mixed ? MBX_MIXED : 0) | (grads ? 0 : MBX_NO_GRADS), kernels);
     if (r) return r;
-    // the configurations' searches on MBX_BUILD_LANES streams (each with its
-    // own scratch; configuration k on lane k mod lanes), joined before the
-    // evaluation; they append to the same buckets through atomics
-    const int lanes = std::min(MBX_BUILD_LANES, c->nconf);
-    CUCHK(c, cudaEventRecord(c->lane_fork, c->stream));
-    for (int l = 1; l < lanes; ++l) CUCHK(c, cudaStreamWaitEvent(c->lane_stream[l], c->lane_fork, 0));
-    for (int k = 0; k < c->nconf; ++k) {
-        const int b = c->conf_mon[k], n = c->conf_mon[k + 1] - b;
-        // members: global ids b..b+n-1 (the identity list of the all-local
-        // topology, offset); queries: positions 0..n-1 in it
-        BuildScope S{c->d_members[0].p + b, n, c->d_members[0].p, n, c->conf_bp[k]};
-        r = launch_build_scope(c, nbody, S, X, 0, kernels, mixed, k % lanes);
-        if (r) return r;
-    }
-    for (int l = 1; l < lanes; ++l) {
-        CUCHK(c, cudaEventRecord(c->lane_join[l], c->lane_stream[l]));
-        CUCHK(c, cudaStreamWaitEvent(c->stream, c->lane_join[l], 0));
-    }
+    // every configuration's search in one set of launches
+    r = launch_build_batch(c, nbody, X, kernels, mixed);
+    if (r) return r;
     CUCHK(c, cudaStreamWaitEvent(c->stream, c->prime_join, 0));
     CUCHK(c, cudaMemsetAsync(c->conf_out.p, 0, 8 * (size_t)c->nconf * sizeof(double), c->stream));
     CUCHK(c, cudaMemsetAsync(c->out.p, 0, 16 * sizeof(double), c->stream));

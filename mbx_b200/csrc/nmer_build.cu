@@ -79,12 +79,15 @@ __global__ void k_fix_monomers(double* __restrict__ xyz, const int* __restrict__
 // atom, slots 1..7 its periodic copies in the reference's shift categories
 // (m,n,l nonzero pattern: 1 = z, 2 = y, 3 = x, 4 = xyz, 5 = yz, 6 = xz, 7 = xy).
 // Also assigns the monomer's cell.
-__global__ void k_cloud(const double* __restrict__ xyz, const int* __restrict__ first_index,
-                        const int* __restrict__ members, int nmem, BoxParams bp, CellGrid cg,
-                        double* __restrict__ cloud, int* __restrict__ cell_of) {
-    const int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= nmem) return;
-    const int i = members[q];
+namespace {
+
+// Cloud point q (monomer i) in the grid cg of box bp; returns its cell, and
+// in dir the directions of its periodic copies (bit a set: the copies along
+// axis a are at +1 box, else at -1).
+__device__ __forceinline__ int cloud_point(const double* __restrict__ xyz, const int* __restrict__ first_index, int i,
+                                           int q, const BoxParams& bp, const CellGrid& cg,
+                                           double* __restrict__ cloud, int& dir) {
+    dir = 0;
     const double* p0 = xyz + 3 * (size_t)first_index[i];
     double p[3] = {p0[0], p0[1], p0[2]};
     double* out = cloud + (size_t)q * 24;
@@ -102,6 +105,7 @@ __global__ void k_cloud(const double* __restrict__ xyz, const int* __restrict__ 
         // uvw == 0 both are made and the +1 copy overwrites (loop order 0,-1,1)
         int sgn[3];
         for (int a = 0; a < 3; ++a) sgn[a] = (uvw[a] > 0.0) ? -1 : 1;
+        dir = (sgn[0] > 0 ? 1 : 0) | (sgn[1] > 0 ? 2 : 0) | (sgn[2] > 0 ? 4 : 0);
         for (int cat = 1; cat < 8; ++cat) {
             // category -> which axes are shifted
             const int mx = (cat == 3 || cat == 4 || cat == 6 || cat == 7);
@@ -138,8 +142,32 @@ __global__ void k_cloud(const double* __restrict__ xyz, const int* __restrict__ 
             c[a] = (int)((v + cg.n[a]) % cg.n[a]);
         }
     }
-    cell_of[q] = (c[2] * cg.n[1] + c[1]) * cg.n[0] + c[0];
+    return (c[2] * cg.n[1] + c[1]) * cg.n[0] + c[0];
 }
+
+}  // namespace
+
+__global__ void k_cloud(const double* __restrict__ xyz, const int* __restrict__ first_index,
+                        const int* __restrict__ members, int nmem, BoxParams bp, CellGrid cg,
+                        double* __restrict__ cloud, int* __restrict__ cell_of, int* __restrict__ copy_dir) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nmem) return;
+    int dir;
+    cell_of[q] = cloud_point(xyz, first_index, members[q], q, bp, cg, cloud, dir);
+    copy_dir[q] = dir;
+}
+
+__global__ void k_cloud_batch(const double* __restrict__ xyz, const int* __restrict__ first_index, int nmem,
+                              const int* __restrict__ conf_of, const BatchGrid* __restrict__ grids,
+                              double* __restrict__ cloud, int* __restrict__ cell_of, int* __restrict__ copy_dir) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nmem) return;
+    const BatchGrid& G = grids[conf_of[q]];
+    int dir;
+    cell_of[q] = G.cell_off + cloud_point(xyz, first_index, q, q, G.bp, G.cg, cloud, dir);
+    copy_dir[q] = dir;
+}
+
 
 __global__ void k_cell_count(const int* __restrict__ cell_of, int nmem, int* __restrict__ cell_count) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
@@ -218,18 +246,19 @@ __global__ void k_cell_sort(const int* __restrict__ cell_start, int ncell, const
 namespace {
 
 template <int NW, int U>
-__device__ __forceinline__ void neighbors_block(const double* __restrict__ cloud, const int* __restrict__ cell_of,
+__device__ __forceinline__ void neighbors_block(const double* __restrict__ cloud, const int* __restrict__ copy_dir,
+                            const int* __restrict__ cell_of,
                             const int* __restrict__ cell_start, const int* __restrict__ cell_items,
-                            const int* __restrict__ query, int nquery, CellGrid cg, int use_pbc, double rc2,
-                            int cap, int* __restrict__ nb_count, NbEntry* __restrict__ nb, int* __restrict__ status,
-                            NbEntry* stage, int* wcount) {
+                            const int* __restrict__ query, int nquery, const CellGrid& cg, int use_pbc,
+                            int cell_off, double rc2, int cap, int* __restrict__ nb_count, NbEntry* __restrict__ nb,
+                            int* __restrict__ status, NbEntry* stage, int* wcount) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int wq = blockIdx.x;
     if (wq >= nquery) return;
     const int qi = query[wq];
     const double* pi = cloud + (size_t)qi * 24;
     const double x0 = pi[0], x1 = pi[1], x2 = pi[2];
-    const int c = cell_of[qi];
+    const int c = cell_of[qi] - cell_off;   // the cell in the query's own grid
     const int cx = c % cg.n[0], cy = (c / cg.n[0]) % cg.n[1], cz = c / (cg.n[0] * cg.n[1]);
     // neighbouring cells; an axis with fewer than 3 cells is scanned once
     const int rx = cg.n[0] >= 3 ? 1 : 0, ry = cg.n[1] >= 3 ? 1 : 0, rz = cg.n[2] >= 3 ? 1 : 0;
@@ -237,6 +266,17 @@ __device__ __forceinline__ void neighbors_block(const double* __restrict__ cloud
     const int ncell = sx * sy * sz;
     const int k0 = w * ncell / NW, k1 = (w + 1) * ncell / NW;
     const int ncopy = use_pbc ? 8 : 1;
+    // One copy per member (cg.one_copy): a point within the cutoff of the
+    // query lies in the 3 x 3 x 3 block of cells around it in real space
+    // (every cell is wider than the cutoff), so a member of a scanned cell can
+    // only match through the copy that moves it into that block, the one the
+    // cell's wrap names (-1 / 0 / +1 box per axis); if the member has no copy
+    // in that direction, it cannot match at all.  The hits, and their order,
+    // are those of the full eight-point test.
+    const bool one = use_pbc && cg.one_copy;
+    const int npts = one ? 1 : ncopy;
+    // cloud category of a shift pattern (x, y, z shifted) -> copy index (k_cloud's order)
+    const int cat_of[8] = {0, 1, 2, 5, 3, 6, 7, 4};
     NbEntry* mine = stage + (size_t)w * cap;
     int count = 0;
     for (int k = k0; k < k1; ++k) {
@@ -244,10 +284,17 @@ __device__ __forceinline__ void neighbors_block(const double* __restrict__ cloud
         // periodic in index space both with PBC and for the hashed grid
         // without PBC (n >= 3 there, so the 27 cells are distinct)
         int ax = rx ? cx + dx - 1 : dx, ay = ry ? cy + dy - 1 : dy, az = rz ? cz + dz - 1 : dz;
+        // wrap of the cell in real space (one-copy mode: n >= 3, rx = ry = rz = 1)
+        const int tx = ax < 0 ? -1 : (ax >= cg.n[0] ? 1 : 0);
+        const int ty = ay < 0 ? -1 : (ay >= cg.n[1] ? 1 : 0);
+        const int tz = az < 0 ? -1 : (az >= cg.n[2] ? 1 : 0);
+        const int need = (tx != 0 ? 1 : 0) | (ty != 0 ? 2 : 0) | (tz != 0 ? 4 : 0);   // axes that must be shifted
+        const int dirs = (tx > 0 ? 1 : 0) | (ty > 0 ? 2 : 0) | (tz > 0 ? 4 : 0);       // and their directions
+        const int cat = cat_of[(tx != 0 ? 4 : 0) | (ty != 0 ? 2 : 0) | (tz != 0 ? 1 : 0)];
         ax = (ax + cg.n[0]) % cg.n[0];
         ay = (ay + cg.n[1]) % cg.n[1];
         az = (az + cg.n[2]) % cg.n[2];
-        const int cell = (az * cg.n[1] + ay) * cg.n[0] + ax;
+        const int cell = cell_off + (az * cg.n[1] + ay) * cg.n[0] + ax;
         const int b = cell_start[cell], e = cell_start[cell + 1];
         // the cell's items in chunks of 32 (one load per lane, then shuffled);
         // its (item, copy) points in item-major order, lanes over consecutive
@@ -255,19 +302,19 @@ __device__ __forceinline__ void neighbors_block(const double* __restrict__ cloud
         for (int c0 = b; c0 < e; c0 += 32) {
             const int nit = e - c0 < 32 ? e - c0 : 32;
             const int my_item = lane < nit ? cell_items[c0 + lane] : 0;
-            const int total = nit * ncopy;
+            const int total = nit * npts;
             for (int base = 0; base < total; base += 32 * U) {
                 bool hit[U];
                 NbEntry ent[U];
 #pragma unroll
                 for (int h = 0; h < U; ++h) {
                     const int t = base + 32 * h + lane;
-                    const bool ok = t < total;
-                    const int it = ok ? t / ncopy : 0;
+                    const int it = t < total ? t / npts : 0;
                     const int qj = __shfl_sync(0xffffffffu, my_item, it);
+                    const bool ok = t < total && (!one || (copy_dir[qj] & need) == dirs);
                     hit[h] = false;
                     if (ok) {
-                        const int s = t - it * ncopy;
+                        const int s = one ? cat : t - it * npts;
                         const double* pj = cloud + (size_t)qj * 24 + 3 * s;
                         const double d2 = dist2_rn(x0, x1, x2, pj[0], pj[1], pj[2]);
                         if (d2 < rc2) {
@@ -313,6 +360,7 @@ __device__ __forceinline__ void neighbors_block(const double* __restrict__ cloud
 
 template <int NW, int U>
 __global__ void __launch_bounds__(NW * 32) k_neighbors(const double* __restrict__ cloud,
+                                                       const int* __restrict__ copy_dir,
                                                        const int* __restrict__ cell_of,
                                                        const int* __restrict__ cell_start,
                                                        const int* __restrict__ cell_items,
@@ -321,16 +369,36 @@ __global__ void __launch_bounds__(NW * 32) k_neighbors(const double* __restrict_
                                                        NbEntry* __restrict__ nb, int* __restrict__ status) {
     extern __shared__ unsigned char smem[];
     __shared__ int wcount[NW];
-    neighbors_block<NW, U>(cloud, cell_of, cell_start, cell_items, query, nquery, cg, use_pbc, rc2, cap, nb_count,
-                           nb, status, reinterpret_cast<NbEntry*>(smem), wcount);
+    neighbors_block<NW, U>(cloud, copy_dir, cell_of, cell_start, cell_items, query, nquery, cg, use_pbc, 0, rc2, cap,
+                           nb_count, nb, status, reinterpret_cast<NbEntry*>(smem), wcount);
+}
+
+// The same over a batch: each query searches its own configuration's grid.
+template <int NW, int U>
+__global__ void __launch_bounds__(NW * 32) k_neighbors_batch(const double* __restrict__ cloud,
+                                                             const int* __restrict__ copy_dir,
+                                                             const int* __restrict__ cell_of,
+                                                             const int* __restrict__ cell_start,
+                                                             const int* __restrict__ cell_items,
+                                                             const int* __restrict__ query, int nquery,
+                                                             const int* __restrict__ conf_of,
+                                                             const BatchGrid* __restrict__ grids, double rc2, int cap,
+                                                             int* __restrict__ nb_count, NbEntry* __restrict__ nb,
+                                                             int* __restrict__ status) {
+    extern __shared__ unsigned char smem[];
+    __shared__ int wcount[NW];
+    if (blockIdx.x >= nquery) return;
+    const BatchGrid& G = grids[conf_of[query[blockIdx.x]]];
+    neighbors_block<NW, U>(cloud, copy_dir, cell_of, cell_start, cell_items, query, nquery, G.cg, G.bp.use_pbc,
+                           G.cell_off, rc2, cap, nb_count, nb, status, reinterpret_cast<NbEntry*>(smem), wcount);
 }
 
 // Host side: one block of `warps` warps per query (1 or 4), U = `unroll`
 // independent 32-point blocks per iteration (1, 2 or 4); the hits of each
 // warp are staged in warps x cap NbEntry of dynamic shared memory.
-int launch_neighbors(int warps, int unroll, const double* cloud, const int* cell_of, const int* cell_start,
-                     const int* cell_items, const int* query, int nquery, CellGrid cg, int use_pbc, double rc2,
-                     int cap, int* nb_count, NbEntry* nb, int* status, cudaStream_t s) {
+int launch_neighbors(int warps, int unroll, const double* cloud, const int* copy_dir, const int* cell_of,
+                     const int* cell_start, const int* cell_items, const int* query, int nquery, CellGrid cg,
+                     int use_pbc, double rc2, int cap, int* nb_count, NbEntry* nb, int* status, cudaStream_t s) {
     if (nquery <= 0) return 0;
     const size_t smem = (size_t)warps * cap * sizeof(NbEntry);
     if (smem > 227 * 1024) return (int)cudaErrorInvalidValue;
@@ -341,8 +409,40 @@ int launch_neighbors(int warps, int unroll, const double* cloud, const int* cell
                                                  (int)smem);                                                    \
             if (e != cudaSuccess) return (int)e;                                                                 \
         }                                                                                                        \
-        k_neighbors<NW, UU><<<nquery, NW * 32, smem, s>>>(cloud, cell_of, cell_start, cell_items, query, nquery, \
+        k_neighbors<NW, UU><<<nquery, NW * 32, smem, s>>>(cloud, copy_dir, cell_of, cell_start, cell_items, query, \
+                                                           nquery,                                                \
                                                            cg, use_pbc, rc2, cap, nb_count, nb, status);          \
+        return (int)cudaGetLastError();                                                                          \
+    }
+    MBX_NB_CASE(4, 1)
+    MBX_NB_CASE(4, 2)
+    MBX_NB_CASE(4, 4)
+    MBX_NB_CASE(1, 1)
+    MBX_NB_CASE(1, 2)
+    MBX_NB_CASE(1, 4)
+#undef MBX_NB_CASE
+    return (int)cudaErrorInvalidValue;
+}
+
+int launch_neighbors_batch(int warps, int unroll, const double* cloud, const int* copy_dir, const int* cell_of,
+                           const int* cell_start,
+                           const int* cell_items, const int* query, int nquery, const int* conf_of,
+                           const BatchGrid* grids, double rc2, int cap, int* nb_count, NbEntry* nb, int* status,
+                           cudaStream_t s) {
+    if (nquery <= 0) return 0;
+    const size_t smem = (size_t)warps * cap * sizeof(NbEntry);
+    if (smem > 227 * 1024) return (int)cudaErrorInvalidValue;
+#define MBX_NB_CASE(NW, UU)                                                                                      \
+    if (warps == NW && unroll == UU) {                                                                           \
+        if (smem > 48 * 1024) {                                                                                  \
+            cudaError_t e = cudaFuncSetAttribute(k_neighbors_batch<NW, UU>,                                      \
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);       \
+            if (e != cudaSuccess) return (int)e;                                                                 \
+        }                                                                                                        \
+        k_neighbors_batch<NW, UU><<<nquery, NW * 32, smem, s>>>(cloud, copy_dir, cell_of, cell_start, cell_items, \
+                                                                 query,                                          \
+                                                                 nquery, conf_of, grids, rc2, cap, nb_count, nb, \
+                                                                 status);                                        \
         return (int)cudaGetLastError();                                                                          \
     }
     MBX_NB_CASE(4, 1)

@@ -21,6 +21,8 @@
 
 struct CellGrid {
     int n[3];
+    int one_copy;          // PBC, n >= 3 on every axis and cells wider than the cutoff (with a margin):
+                           // of a member's eight cloud points only the one its cell's wrap implies can match
     double lo[3];          // unused
     double inv_extent[3];  // no PBC: 1 / cell edge of the hashed grid
 };
@@ -50,18 +52,39 @@ struct TrimerRules {
     long offset[MBX_MAX_BUCKETS];
 };
 
+// One configuration of a batched search (all configurations of a batch in
+// one set of launches): its box, its cell grid, and the index of its first
+// cell in the batch's concatenated cell array.
+struct BatchGrid {
+    BoxParams bp;
+    CellGrid cg;
+    int cell_off;
+};
+
 __global__ void k_fix_monomers(double* xyz, const int* first_index, const int* nat, int nmon, BoxParams bp);
 __global__ void k_cloud(const double* xyz, const int* first_index, const int* members, int nmem, BoxParams bp,
-                        CellGrid cg, double* cloud, int* cell_of);
+                        CellGrid cg, double* cloud, int* cell_of, int* copy_dir);
+// The same for a batch: members are the batch's monomers in order (member
+// position = monomer), each with the grid of its configuration conf_of[q].
+__global__ void k_cloud_batch(const double* xyz, const int* first_index, int nmem, const int* conf_of,
+                              const BatchGrid* grids, double* cloud, int* cell_of, int* copy_dir);
 __global__ void k_cell_count(const int* cell_of, int nmem, int* cell_count);
 __global__ void k_cell_scan(const int* cell_count, int ncell, int* cell_start, int* cell_fill);
 __global__ void k_cell_fill(const int* cell_of, int nmem, int* cell_fill, int* cell_items);
 __global__ void k_cell_sort(const int* cell_start, int ncell, const int* items, int* sorted);
 // Matches of every query monomer (k_neighbors): `warps` warps per query (1 or
 // 4), `unroll` independent 32-point blocks per iteration (1, 2 or 4).
-int launch_neighbors(int warps, int unroll, const double* cloud, const int* cell_of, const int* cell_start,
-                     const int* cell_items, const int* query, int nquery, CellGrid cg, int use_pbc, double rc2,
+int launch_neighbors(int warps, int unroll, const double* cloud, const int* copy_dir, const int* cell_of,
+                     const int* cell_start, const int* cell_items, const int* query, int nquery, CellGrid cg,
+                     int use_pbc, double rc2,
                      int cap, int* nb_count, NbEntry* nb, int* status, cudaStream_t s);
+// The same over a batch (queries are member positions, conf_of and grids as
+// for k_cloud_batch).
+int launch_neighbors_batch(int warps, int unroll, const double* cloud, const int* copy_dir, const int* cell_of,
+                           const int* cell_start,
+                           const int* cell_items, const int* query, int nquery, const int* conf_of,
+                           const BatchGrid* grids, double rc2, int cap, int* nb_count, NbEntry* nb, int* status,
+                           cudaStream_t s);
 __global__ void k_dimers(const int* query, int nquery, const int* members, const int* tag, const int* type,
                          const int* nb_count, const NbEntry* nb, int cap, double rc2, DimerRules R,
                          unsigned long long* listed, int4* list, long list_cap, int4* bucket_data,
