@@ -391,7 +391,7 @@ def emit_cuda(q, name, nvars):
     w("// C' image (hi, mid[, lo] FP16 parts of every K block, K-major no-swizzle core")
     w("// matrices), written by mbx_set_coef_%s_s; per-column factors 2^-(s_j + t_j)" % name)
     w("__device__ __align__(128) unsigned char qf_img_%s[%d];" % (name, image_bytes(q)))
-    w("__constant__ float qf_colf_%s[%d];" % (name, q.npad))
+    w("__constant__ __align__(8) float qf_colf_%s[%d];   // read in pairs (colf2)" % (name, q.npad))
     w("__constant__ double qf_b0_%s[1];" % name)
     w("")
     w("struct %s_Q {" % name)
@@ -417,6 +417,9 @@ def emit_cuda(q, name, nvars):
     w("    __host__ __device__ static constexpr int chunk_bytes(int s, int p) { return parts(s) * pass_n(p) * 32; }")
     w("    __device__ __forceinline__ static const unsigned char* image() { return qf_img_%s; }" % name)
     w("    __device__ __forceinline__ static double b0() { return qf_b0_%s[0]; }" % name)
+    w("    // column scales of columns 2k and 2k + 1, for the paired FP32 multiply")
+    w("    __device__ __forceinline__ static f2_t colf2(int k) { return reinterpret_cast<const f2_t*>(qf_colf_%s)[k]; }"
+      % name)
     w("    // r = 2^(14 - e) with e = floor(log2(max(1, max|d|)^2 2^-TMIN)) + 1, so that every")
     w("    // |m_j(d) 2^-t_j| r < 2^14; sc[k] = r 2^-(TMIN + k); returns 1/r")
     w("    __device__ __forceinline__ static float row_scales(const float (&d)[%d], float (&sc)[NT]) {" % nvars)
@@ -459,14 +462,14 @@ def emit_cuda(q, name, nvars):
     w("        for (int i = 0; i < 8; ++i) qf::split2(a[2 * i], a[2 * i + 1], hi[i], lo[i]);")
     w("    }")
     # epilogue
-    w("    // columns 16 c .. 16 c + 15 of Y: z_j = y_j 2^-(s_j + t_j) (y / r, scaled back by the caller);")
-    w("    // adds z_j dm_j/dd to g and returns the chunk's share of the energy that g does not")
+    w("    // columns 16 c .. 16 c + 15 of Y, scaled: z_j = y_j 2^-(s_j + t_j) (y / r, scaled back by the")
+    w("    // caller); adds z_j dm_j/dd to g and returns the chunk's share of the energy that g does not")
     w("    // carry: by Euler's identity for monomials of degree k, sum_u d_u dm/dd_u = k m, so")
     w("    // sum_j m_j z_j = z_const + (sum_{deg 1} d_u z_j + sum_u d_u g_u) / 2 over the pass,")
     w("    // and the degree-2 columns (all but 37) need no energy term of their own")
-    w("    __device__ __forceinline__ static float epi(int c, const uint32_t (&y)[16], const float (&d)[%d], "
+    w("    __device__ __forceinline__ static float epi(int c, const float (&z)[16], const float (&d)[%d], "
       "float (&g)[%d]) {" % (nvars, nvars))
-    w("        float p = 0.0f, z;")
+    w("        float p = 0.0f;")
     w("        switch (c) {")
     for c in range(ks):
         w("        case %d:" % c)
@@ -475,16 +478,15 @@ def emit_cuda(q, name, nvars):
             if j >= q.nb:
                 continue
             b = q.basis[j]
-            w("            z = __uint_as_float(y[%d]) * qf_colf_%s[%d];" % (i, name, j))
             if len(b) == 0:
-                w("            p += z;")
+                w("            p += z[%d];" % i)
             elif len(b) == 1:
-                w("            p = fmaf(0.5f * d[%d], z, p);" % b[0])
-                w("            g[%d] += z;" % b[0])
+                w("            p = fmaf(0.5f * d[%d], z[%d], p);" % (b[0], i))
+                w("            g[%d] += z[%d];" % (b[0], i))
             else:
                 u, v = b
-                w("            g[%d] = fmaf(z, d[%d], g[%d]);" % (u, v, u))
-                w("            g[%d] = fmaf(z, d[%d], g[%d]);" % (v, u, v))
+                w("            g[%d] = fmaf(z[%d], d[%d], g[%d]);" % (u, i, v, u))
+                w("            g[%d] = fmaf(z[%d], d[%d], g[%d]);" % (v, i, u, v))
         w("            break;")
     w("        default:")
     w("            break;")

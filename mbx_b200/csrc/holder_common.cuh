@@ -101,22 +101,24 @@ __device__ __forceinline__ void dvar_coul(const double (&p1)[3], const double (&
 }
 
 // The variable together with its radial factor q, dv/d(p1 - p2) = q (p1 - p2),
-// by the same operations as var_exp / dvar_exp (var_coul / dvar_coul), so that
-// a chain rule from a stored q (dvar_q) gives the same bits as dvar_exp does.
+// for the mixed path (pair_vars_kernel): 1 / r from one reciprocal square
+// root instead of a square root and a division (1-2 ulp, far below what the
+// FP32 shifted variables and the FP32-accurate gradient keep).
 __device__ __forceinline__ double var_exp_q(const double (&p1)[3], const double (&p2)[3], double k, double d0,
                                            double& q) {
-    double a, b, c;
-    const double r = dist3(p1, p2, a, b, c);
+    const double a = p1[0] - p2[0], b = p1[1] - p2[1], c = p1[2] - p2[2];
+    const double d2 = a * a + b * b + c * c;
+    const double rinv = rsqrt(d2), r = d2 * rinv;
     const double v = exp(k * (d0 - r));
-    q = -k * v / r;
+    q = -k * v * rinv;
     return v;
 }
 
 __device__ __forceinline__ double var_coul_q(const double (&p1)[3], const double (&p2)[3], double k, double d0,
                                             double& q) {
-    double a, b, c;
-    const double r = dist3(p1, p2, a, b, c);
-    const double rinv = 1.0 / r;
+    const double a = p1[0] - p2[0], b = p1[1] - p2[1], c = p1[2] - p2[2];
+    const double d2 = a * a + b * b + c * c;
+    const double rinv = rsqrt(d2), r = d2 * rinv;
     const double v = exp(k * (d0 - r)) * rinv;
     q = -(k + rinv) * v * rinv;
     return v;

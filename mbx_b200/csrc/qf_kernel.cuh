@@ -274,10 +274,18 @@ __device__ __forceinline__ double qf_epilogue_pass(uint32_t tbuf, const float (&
             qf::tmem_ld16(tbuf + (uint32_t)((cc + 2) * 16), ym[b ^ 1]);
             qf::tmem_ld16(tbuf + CC + (uint32_t)((cc + 2) * 16), yc[b ^ 1]);
         }
-        uint32_t y[16];
+        // z = (main + correction) x column scale, two columns per paired
+        // FP32 instruction (the same roundings as one column at a time)
+        float z[16];
 #pragma unroll
-        for (int i = 0; i < 16; ++i) y[i] = __float_as_uint(__uint_as_float(ym[b][i]) + __uint_as_float(yc[b][i]));
-        P += (double)Q::epi(C0 + cc, y, d, g);
+        for (int i = 0; i < 8; ++i) {
+            const f2_t y2 = f2_add(f2_pack(__uint_as_float(ym[b][2 * i]), __uint_as_float(ym[b][2 * i + 1])),
+                                   f2_pack(__uint_as_float(yc[b][2 * i]), __uint_as_float(yc[b][2 * i + 1])));
+            const f2_t z2 = f2_mul(y2, Q::colf2((C0 + cc) * 8 + i));
+            z[2 * i] = f2_lo(z2);
+            z[2 * i + 1] = f2_hi(z2);
+        }
+        P += (double)Q::epi(C0 + cc, z, d, g);
         if (k + 1 < NCH) {
             qf::tmem_wait_ld(ym[b ^ 1]);
             qf::tmem_wait_ld(yc[b ^ 1]);
