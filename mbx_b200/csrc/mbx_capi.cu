@@ -310,6 +310,8 @@ struct mbx_ctx {
         int nb_warps = 4, nb_unroll = 2, tri_threads = 128, dim_threads = 128;
     } knobs[4];         // per term (indexed by nbody)
     double* h_out = nullptr;  // pinned: [0..7] term outputs, [8..15] counters
+    double* h_grad = nullptr;  // pinned staging of the gradient of a call with host arrays
+    size_t h_grad_n = 0;
     cudaEvent_t ev[3];
 
 
@@ -439,6 +441,7 @@ int mbx_destroy(mbx_ctx* c) {
     for (auto& g : c->d_bgrid) g.release();
     c->conf_out.release();
     if (c->h_out) cudaFreeHost(c->h_out);
+    if (c->h_grad) cudaFreeHost(c->h_grad);
     for (int i = 0; i < 3; ++i) cudaEventDestroy(c->ev[i]);
     for (auto& gr : c->graph)
         if (gr.exec) cudaGraphExecDestroy(gr.exec);
@@ -1151,9 +1154,18 @@ static int unstage_term_io(mbx_ctx* c, double* xyz, double* grad, int flags, dou
     if (dev) return MBX_OK;
     if (c->bp.use_pbc) CUCHK(c, cudaMemcpyAsync(xyz, X, nx * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     if (grads && grad) {
-        std::vector<double> tmp(nx);
-        CUCHK(c, cudaMemcpyAsync(tmp.data(), G, nx * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        // through a pinned staging buffer of the context (a DMA copy, no
+        // allocation per call), then += into the caller's array
+        if (c->h_grad_n < nx) {
+            if (c->h_grad) CUCHK(c, cudaFreeHost(c->h_grad));
+            c->h_grad = nullptr;
+            c->h_grad_n = 0;
+            CUCHK(c, cudaMallocHost(&c->h_grad, nx * sizeof(double)));
+            c->h_grad_n = nx;
+        }
+        CUCHK(c, cudaMemcpyAsync(c->h_grad, G, nx * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
         CUCHK(c, cudaStreamSynchronize(c->stream));
+        const double* tmp = c->h_grad;
         for (size_t i = 0; i < nx; ++i) grad[i] += tmp[i];
     } else {
         CUCHK(c, cudaStreamSynchronize(c->stream));

@@ -511,6 +511,16 @@ def test_onebody_refuses_cpu_only_types():
     assert abs(e - w.OneBodyEnergy(True)) <= 1e-12 * abs(e)
 
 
+def test_water_box_three_cells_per_axis():
+    """A box with exactly 3 cells per axis for both cutoffs (27.5 A: 9.17 A
+    cells), the tightest case of the neighbour search's one-copy test (every
+    cell a neighbour of every other, each member reached through exactly the
+    copy its cell's wrap names): lists, energies, gradients and virials
+    against the restatement."""
+    ids, xyz, box = workloads.water_box(n_side=9, n_mol=694, L=27.5, seed=5)
+    compare_system(ids, xyz, box, 9.0, 7.0)
+
+
 def test_water_2048_lists_vs_restatement():
     """The full-size lists also equal the oracle restatement's, n-mer by n-mer."""
     ids, xyz, box = workloads.water_2048(0)
