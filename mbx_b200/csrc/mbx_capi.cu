@@ -1145,17 +1145,15 @@ static int stage_term_io(mbx_ctx* c, double* xyz, double* grad, int flags, doubl
     return MBX_OK;
 }
 
-// Host outputs of a call with host arrays: the wrapped coordinates and the
-// gradient (+=) back into the caller's arrays.
-static int unstage_term_io(mbx_ctx* c, double* xyz, double* grad, int flags, double* X, double* G) {
-    const bool dev = (flags & MBX_DEVICE_PTRS) != 0;
+// The device-to-host copies of a call with host arrays, enqueued on the
+// context stream: the wrapped coordinates into the caller's array, the
+// gradient into a pinned staging buffer of the context (a DMA copy, no
+// allocation per call).
+static int copy_term_outputs(mbx_ctx* c, double* xyz, double* grad, int flags, double* X, double* G) {
     const bool grads = !(flags & MBX_NO_GRADS);
     const size_t nx = 3 * (size_t)c->numsites;
-    if (dev) return MBX_OK;
     if (c->bp.use_pbc) CUCHK(c, cudaMemcpyAsync(xyz, X, nx * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     if (grads && grad) {
-        // through a pinned staging buffer of the context (a DMA copy, no
-        // allocation per call), then += into the caller's array
         if (c->h_grad_n < nx) {
             if (c->h_grad) CUCHK(c, cudaFreeHost(c->h_grad));
             c->h_grad = nullptr;
@@ -1164,11 +1162,27 @@ static int unstage_term_io(mbx_ctx* c, double* xyz, double* grad, int flags, dou
             c->h_grad_n = nx;
         }
         CUCHK(c, cudaMemcpyAsync(c->h_grad, G, nx * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    }
+    return MBX_OK;
+}
+
+// Host outputs of a call with host arrays: the wrapped coordinates and the
+// gradient (+=) back into the caller's arrays.  copied: copy_term_outputs
+// already ran behind the call's last kernels (and the stream was waited for).
+static int unstage_term_io(mbx_ctx* c, double* xyz, double* grad, int flags, double* X, double* G,
+                           bool copied = false) {
+    const bool dev = (flags & MBX_DEVICE_PTRS) != 0;
+    const bool grads = !(flags & MBX_NO_GRADS);
+    const size_t nx = 3 * (size_t)c->numsites;
+    if (dev) return MBX_OK;
+    if (!copied) {
+        int r = copy_term_outputs(c, xyz, grad, flags, X, G);
+        if (r) return r;
         CUCHK(c, cudaStreamSynchronize(c->stream));
+    }
+    if (grads && grad) {
         const double* tmp = c->h_grad;
         for (size_t i = 0; i < nx; ++i) grad[i] += tmp[i];
-    } else {
-        CUCHK(c, cudaStreamSynchronize(c->stream));
     }
     return MBX_OK;
 }
@@ -1438,6 +1452,16 @@ extern "C" int mbx_energy_2b3b(mbx_ctx* c, double* xyz, int use_ghost, double* e
     if (r) return r;
     r = term_enqueue(k, 2, use_ghost, X, G, flags, &kk);
     if (r) return fail(c, r, std::string("2b term: ") + k->err);
+    // host arrays: the output copies behind both terms, before the host
+    // waits (redone below if a term has to run again)
+    bool copied = false;
+    if (!(flags & MBX_DEVICE_PTRS)) {
+        CUCHK(c, cudaEventRecord(k->ev[2], k->stream));
+        CUCHK(c, cudaStreamWaitEvent(c->stream, k->ev[2], 0));
+        r = copy_term_outputs(c, xyz, grad, flags, X, G);
+        if (r) return r;
+        copied = true;
+    }
     CUCHK(c, cudaStreamSynchronize(k->stream));
     CUCHK(c, cudaStreamSynchronize(c->stream));
     int again3 = term_finish(c, 3, e3, virial, kernels);
@@ -1446,6 +1470,7 @@ extern "C" int mbx_energy_2b3b(mbx_ctx* c, double* xyz, int use_ghost, double* e
     if (again2 < 0) return fail(c, MBX_ECUDA, std::string("2b term: ") + k->err);
     // a term whose n-mers did not fit its buffers added nothing: run it again
     for (int attempt = 0; (again2 || again3) && attempt < 4; ++attempt) {
+        copied = false;
         if (again3) {
             kernels = 0;
             r = term_enqueue(c, 3, use_ghost, X, G, flags, &kernels);
@@ -1472,7 +1497,7 @@ extern "C" int mbx_energy_2b3b(mbx_ctx* c, double* xyz, int use_ghost, double* e
     // the 2b term also waited for the wrap: make the caller's stream see its work
     CUCHK(c, cudaEventRecord(k->ev[2], k->stream));
     CUCHK(c, cudaStreamWaitEvent(c->stream, k->ev[2], 0));
-    return unstage_term_io(c, xyz, grad, flags, X, G);
+    return unstage_term_io(c, xyz, grad, flags, X, G, copied);
 }
 
 extern "C" int mbx_last_counts(const mbx_ctx* c, int nbody, long* listed, long* evaluated) {
