@@ -60,7 +60,7 @@ MIXED_FORCE = 1e-3        # kcal/mol/A, largest force error of a liquid box
 # two waters are closer than liquid water ever brings them.
 MIXED_RMIN = 2.5           # A: first-atom separations at and above this are "accessible" (liquid, clusters)
 MIXED_NMER_ABS = 1.5e-4    # kcal/mol, one trimer of accessible geometry (B200: at most 8.8e-5 measured)
-MIXED_NMER_ABS_CLOSE = 5e-4  # kcal/mol, one trimer with waters closer than MIXED_RMIN (B200: 2.4e-4 measured)
+MIXED_NMER_ABS_CLOSE = 5e-4  # kcal/mol, one trimer with waters closer than MIXED_RMIN (B200: 2.1e-4 measured)
 MIXED_NMER_GRAD = 3e-4     # kcal/mol/A, gradient of one trimer of accessible geometry (B200: at most 2.0e-4
                            # measured, a trimer at 2.51 A; 1.3e-6 on average)
 FP32_TYPES = ("mbpol3b",)  # types with a mixed-precision kernel; the rest run FP64 when mixed
