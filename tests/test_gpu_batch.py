@@ -51,6 +51,33 @@ def test_batch_matches_single_configurations(nbody):
         np.testing.assert_allclose(v[k], vs, rtol=1e-9, atol=1e-7)
 
 
+@pytest.mark.parametrize("nbody", [2, 3])
+def test_batch_tiny_configurations(nbody):
+    """Configurations too small for some terms (one water, two waters, three
+    waters) between larger ones and a periodic box: the batched search runs
+    over all of them at once, and each must still give what it gives alone
+    (no dimer or trimer across configurations, zero where none exists)."""
+    ids0, x0, box = workloads.water_256(0)
+    one = workloads.water_cluster(1, seed=21)
+    two = workloads.water_cluster(2, seed=22)
+    three = workloads.water_cluster(3, seed=23)
+    c = workloads.water_cluster(30, seed=24)
+    cfgs = [(one[0], one[1], None), (c[0], c[1], None), (two[0], two[1], None), (ids0, x0, box),
+            (three[0], three[1], None), (one[0], one[1], None)]
+    b = Batch(cfgs)
+    e, v = b.energy(nbody, graph=False, virials=True)
+    for k, cfg in enumerate(cfgs):
+        n = len(cfg[0])
+        if n < nbody:
+            assert e[k] == 0.0, (k, e[k])
+            assert not np.any(b.real_grads(k)), k
+            continue
+        es, gs, vs = single(cfg, nbody)
+        assert abs(e[k] - es) <= E_REL * abs(es) + 1e-9, (k, e[k], es)
+        np.testing.assert_allclose(b.real_grads(k), gs, rtol=0, atol=G_ABS)
+        np.testing.assert_allclose(v[k], vs, rtol=1e-9, atol=1e-7)
+
+
 def test_batch_cluster_vs_oracle():
     cfgs = small_batch()
     b = Batch(cfgs)
