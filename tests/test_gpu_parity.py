@@ -521,6 +521,30 @@ def test_water_box_three_cells_per_axis():
     compare_system(ids, xyz, box, 9.0, 7.0)
 
 
+def triclinic_water_box(n_side=9, n_mol=700, L=30.0, shear=(0.15, 0.1, 0.12), seed=6, jitter=0.3):
+    """Waters on a lattice in the fractional coordinates of a triclinic box
+    (lattice vectors a = (L, 0, 0), b = (s0 L, L, 0), c = (s1 L, s2 L, L), the
+    lower-triangular form the reference's fractional coordinates assume), so
+    that periodic images keep the lattice spacing."""
+    rng = np.random.default_rng(seed)
+    B = np.array([[L, 0, 0], [shear[0] * L, L, 0], [shear[1] * L, shear[2] * L, L]], float)
+    g = (np.arange(n_side) + 0.5) / n_side - 0.5
+    frac = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+    pick = rng.choice(len(frac), size=n_mol, replace=False)
+    centres = frac[pick] @ B + rng.uniform(-jitter, jitter, size=(n_mol, 3))
+    xyz = workloads.place(rng, workloads.water_body(), centres)
+    return ["h2o"] * n_mol, xyz.reshape(-1), B.reshape(-1)
+
+
+def test_water_box_triclinic():
+    """A triclinic box (perpendicular widths 29.6-30 A: 3 cells per axis for
+    the 2b cutoff, 4 for the 3b one), where the neighbour search's cells are
+    parallelepipeds and its one-copy test rests on their perpendicular
+    widths: lists, energies, gradients and virials against the restatement."""
+    ids, xyz, box = triclinic_water_box()
+    compare_system(ids, xyz, box, 9.0, 7.0)
+
+
 def test_water_2048_lists_vs_restatement():
     """The full-size lists also equal the oracle restatement's, n-mer by n-mer."""
     ids, xyz, box = workloads.water_2048(0)
