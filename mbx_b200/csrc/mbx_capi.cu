@@ -684,6 +684,8 @@ static int make_box(mbx_ctx* c, const double* box, double rc, BoxParams* out) {
     return MBX_OK;
 }
 
+static void drop_graphs(mbx_ctx* c);
+
 extern "C" int mbx_set_config(mbx_ctx* c, double cutoff2b, double cutoff3b, const double* box, int n2,
                               const char* const* ignore2b, int n3, const char* const* ignore3b) {
     if (!c || !(cutoff2b >= 0) || !(cutoff3b >= 0)) return fail(c, MBX_EINVAL, "bad cutoffs");
@@ -692,6 +694,8 @@ extern "C" int mbx_set_config(mbx_ctx* c, double cutoff2b, double cutoff3b, cons
     int r = make_box(c, box, std::max(cutoff2b, cutoff3b), &c->bp);
     if (r) return r;
     ++c->gen;
+    // captured batch graphs hold the old cutoffs, rules and search grids
+    drop_graphs(c);
     c->ignore[2].clear();
     c->ignore[3].clear();
     for (int i = 0; i < n2; ++i) c->ignore[2].push_back({ignore2b[2 * i], ignore2b[2 * i + 1]});

@@ -122,6 +122,20 @@ def test_graph_recaptures_after_coordinates_move():
     b.sites.copy_(x0)
 
 
+def test_graph_follows_a_cutoff_change():
+    """A replayed graph must not keep the cutoffs it was captured with: after
+    set_config, the next graph call gives the plain sequence's result for the
+    new cutoffs."""
+    b = Batch(small_batch())
+    e_old = b.energy(2, grads=False, graph=True)
+    e_old = b.energy(2, grads=False, graph=True)   # replayed
+    b.ctx.set_config(5.0, 7.0, None)   # drops dimers the 2b switch still weighs
+    e_graph = b.energy(2, grads=False, graph=True)
+    e_plain = b.energy(2, grads=False, graph=False)
+    np.testing.assert_allclose(e_graph, e_plain, rtol=1e-12, atol=1e-10)
+    assert np.abs(np.asarray(e_graph) - np.asarray(e_old)).max() > 1e-6
+
+
 def test_batch_mixed_errors():
     cfgs = small_batch()[:3]
     b = Batch(cfgs)
